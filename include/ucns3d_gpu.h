@@ -1,0 +1,196 @@
+/*
+ * ucns3d_gpu.h - C ABI of the B200 explicit residual engine.
+ *
+ * The engine replaces, for one GPU, the per-cell / per-face work of one
+ * SSP-RK3 step of UCNS3D:
+ *
+ *   RUNGE_KUTTA3              src/time_p.f90:885-1027   -> ucg_rk3_step / ucg_step
+ *   CALCULATE_CFL             src/time_p.f90:27-191     -> ucg_compute_dt
+ *   CALL_FLUX_SUBROUTINES_3D  src/time_p.f90:2253-2497  -> ucg_residual
+ *     LEAST_SQUARES / ALLGRADS_INNER/MIX   src/reconstruct_p.f90:2702, src/gradients.f90:10-706
+ *     WENOWEIGHTS / CP_RECONSTRUCTION      src/reconstruct_p.f90:407-1250
+ *     CHECKSOL / MUSCL / CHECKSOLX         src/reconstruct_p.f90:3126-3406, 2286-2352
+ *     SOLUTIONTRIAV2                        src/reconstruct_p.f90:2358
+ *     CALCULATE_FLUXESHI_CONVECTIVE         src/flux_p.f90:478-1030
+ *     CALCULATE_FLUXESHI_DIFFUSIVE          src/flux_p.f90:1520-2107
+ *   TGV kinetic energy sum     src/time_p.f90:4145-4198  -> ucg_reduce(UCG_REDUCE_KE)
+ *
+ * The Fortran driver keeps the mesh, the partitioning, UCNS3D.DAT and all
+ * set-up (geometry, stencils, pseudo-inverses).  It packs the set-up tables
+ * once (ucg_upload_geometry, ucg_upload_recon), then calls the engine from the
+ * master thread in place of the SELECT CASE(RUNGEKUTTA) of TIME_MARCHING
+ * (src/time_p.f90:4229-4263).
+ *
+ * Conventions
+ *   - Every entry point returns 0 (UCG_OK) or a positive UCG_E* code; the
+ *     engine never aborts.  ucg_last_error() gives the message.
+ *   - Host pointers are borrowed for the duration of the call only.
+ *   - Array shapes are written C-order, e.g. [n][5] is 5 contiguous doubles
+ *     per cell, which is Fortran U(1:5, 1:n).  Cell and face indices are
+ *     0-based.
+ *   - A handle is not re-entrant: call it from one host thread.  All device
+ *     work of a handle runs on one CUDA stream (ucg_get_stream).
+ *   - There is no CPU fallback: without a usable sm_100 device ucg_create
+ *     fails with UCG_ECUDA.
+ */
+#ifndef UCNS3D_GPU_H
+#define UCNS3D_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UCG_NV 5          /* conserved variables rho, rho*u, rho*v, rho*w, E   */
+#define UCG_MAX_FACES 6   /* hexahedra                                           */
+#define UCG_MAX_QP 16     /* face quadrature points (4x4 Gauss on quadrilaterals) */
+
+enum {
+  UCG_OK = 0,
+  UCG_EINVAL = 1,     /* bad argument or size                                    */
+  UCG_ECUDA = 2,      /* CUDA runtime error (message has the CUDA error string)   */
+  UCG_ENONPHYS = 3,   /* NaN, or non-positive density or pressure in the state    */
+  UCG_ESTATE = 4,     /* call out of order (e.g. a step before the tables)        */
+  UCG_ENOMEM = 5,     /* device allocation failed                                 */
+  UCG_ETIMEOUT = 6    /* a bounded device wait gave up                            */
+};
+
+enum { UCG_FP64 = 0, UCG_MIXED = 1 };
+enum { UCG_REDUCE_KE = 1, UCG_REDUCE_MASS = 2, UCG_REDUCE_ENERGY = 3 };
+
+/* Scheme and fluid parameters.  Field names follow UCNS3D's module globals
+ * (src/parameters.f90, src/declarations.f90).                               */
+typedef struct ucg_config {
+  int32_t governing;   /* 1 Navier-Stokes (ITESTCASE 4), 2 Euler (ITESTCASE 3)        */
+  int32_t scheme;      /* 2 MUSCL (IWENO=-1), 3 WENO/CWENO (IWENO=1)                    */
+  int32_t iorder;      /* reconstruction degree IORDER = spatialorder-1, 1..4           */
+  int32_t ees;         /* 0 WENO, 5 CWENO (parameters.f90:1340-1372)                    */
+  int32_t wenwrt;      /* 1 conserved-variable WENO                                    */
+  int32_t limiter;     /* MUSCL limiter code, 7 = Venkatakrishnan                       */
+  int32_t riemann;     /* 1 = HLLC                                                      */
+  int32_t precision;   /* UCG_FP64 or UCG_MIXED                                         */
+  int32_t wenoz;       /* WENO-Z weights for CWENO (reconstruct_p.f90:1021-1029)         */
+  int32_t ideg;        /* IDEGFREE: basis functions without the mean                    */
+  int32_t imax;        /* cells of a full stencil without the cell itself               */
+  int32_t admis_max;   /* stencil slots per cell (TYPESTEN)                             */
+  int32_t ideg2;       /* CWENO directional stencils: IDEGFREE2 (0 otherwise)           */
+  int32_t imax2;       /* CWENO directional stencils: NUMNEIGHBOURS2-1 (0 otherwise)    */
+  int32_t nq_quad;     /* quadrature points on a quadrilateral face                     */
+  int32_t nq_tri;      /* quadrature points on a triangular face                        */
+  double gamma;        /* GAMMA                                                         */
+  double prandtl;      /* PRANDTL                                                       */
+  double visc;         /* VISC: free-stream dynamic viscosity (parameters.f90:1241)     */
+  double r_gas;        /* R_gas (parameters.f90:1223-1227)                             */
+  double pres;         /* PRES: free-stream pressure (Sutherland reference T0)          */
+  double rres;         /* RRES: free-stream density                                    */
+  double lwci;         /* wenocentralweight (LWCI1)                                     */
+  double weno_eps;     /* DIVBYZERO of WENOWEIGHTS, 10E-12 (reconstruct_p.f90:437)       */
+  double kappa_ven;    /* KAPPA_VEN of SLOPE_LIMITERS, 10 (reconstruct_p.f90:3436)       */
+  double lamx;         /* jump damping of the viscous face gradient (LAMX, 1)           */
+  double quad_w[UCG_MAX_QP];  /* face weights, summing to 1 (QUADRATUREQUAD3D)          */
+  double tri_w[UCG_MAX_QP];   /* face weights, summing to 1 (QUADRATURETRIANG)          */
+  double bc_state[UCG_NV];    /* free-stream primitive state rho,u,v,w,p for the BCs    */
+} ucg_config;
+
+/* Per-cell geometry (IELEM(N,I) and the small parts of ILOCAL_RECON3(I),
+ * src/declarations.f90:461-510, 644-704).  [n][F] arrays have UCG_MAX_FACES
+ * entries per cell; unused faces are ignored.                                */
+typedef struct ucg_geometry {
+  int64_t ncells;
+  const int32_t* nfaces;      /* [n]      IFCA                                          */
+  const int32_t* face_type;   /* [n][F]   types_faces: 5 quadrilateral, 6 triangle      */
+  const int32_t* neigh;       /* [n][F]   INEIGH, -1 on a physical boundary face        */
+  const int32_t* neigh_face;  /* [n][F]   INEIGHN                                      */
+  const int32_t* bc;          /* [n][F]   boundary code (0 interior or periodic)        */
+  const int32_t* qperm;       /* [n][F][Q] quadrature point of the neighbour's face that
+                                 coincides with this face's point q                     */
+  const double* face_angle;   /* [n][F][2] FACEANGLEX, FACEANGLEY                       */
+  const double* face_area;    /* [n][F]   SURF                                          */
+  const double* dih;          /* [n][F]   DIH: centre-to-centre distance               */
+  const double* qpoints;      /* [n][F][Q][3] QPOINTS in the cell's reference frame    */
+  const double* volume;       /* [n]      TOTVOLUME                                     */
+  const double* minedge;      /* [n]      MINEDGE                                       */
+  const double* invccjac;     /* [n][3][3] INVCCJAC                                     */
+  const double* basis_mean;   /* [n][ideg] INTEG_BASIS / VOLUME(1,1): basis cell means  */
+  const int32_t* admis;       /* [n]      ADMIS                                         */
+  const int32_t* full;        /* [n]      FULL                                          */
+} ucg_geometry;
+
+/* Reconstruction tables of cells [first, first+count): stencils and the
+ * FP64 pseudo-inverses of PRESTORE_RECONSTRUCTION3 (src/prestore.f90:167-818)
+ * and the smoothness matrices of INDICATORMATRIX (src/prestore.f90:1529-1673).
+ * With table_id == NULL the matrices are given per cell (ntables ignored);
+ * otherwise cell c uses matrix set table_id[c] out of ntables sets, which
+ * lets meshes with repeated cell geometry upload each set once.             */
+typedef struct ucg_recon {
+  int64_t first, count;
+  const int32_t* stencil;     /* [count][admis_max][imax+1] IHEXL, slot 0 = the cell,
+                                 -1 = unused                                           */
+  int64_t ntables;
+  const int32_t* table_id;    /* [count] or NULL                                        */
+  const double* invmat;       /* [ntab][admis_max][imax][ideg] invmat_stencilt          */
+  const double* invmat2;      /* [ntab][admis_max][imax2][ideg2] invmat_stenciltC (CWENO,
+                                 slot 0 unused) or NULL                                 */
+  const double* indicator;    /* [ntab][ideg][ideg] INDICATOR (WENO) or NULL           */
+  const double* indicator2;   /* [ntab][ideg2][ideg2] INDICATORC (CWENO) or NULL       */
+} ucg_recon;
+
+typedef struct ucg_engine ucg_engine;
+
+/* Create an engine on CUDA device `device` for meshes of `ncells` cells. */
+int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** out);
+void ucg_destroy(ucg_engine* e);
+
+int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g);
+int ucg_upload_recon(ucg_engine* e, const ucg_recon* r);
+
+/* Conserved state U_C(I)%VAL(1,1:5), [n][5]. */
+int ucg_set_state(ucg_engine* e, const double* u, int64_t n);
+int ucg_get_state(ucg_engine* e, double* u, int64_t n);
+
+/* CALCULATE_CFL: dt = min over cells, CCFL = cfl/3 (time_p.f90:46). */
+int ucg_compute_dt(ucg_engine* e, double cfl, double* dt);
+
+/* One CALL_FLUX_SUBROUTINES_3D on the current state; writes RHS(I)%VAL
+ * (net outward flux, convective minus viscous) to rhs [n][5] if non-NULL. */
+int ucg_residual(ucg_engine* e, double* rhs);
+
+/* One RUNGE_KUTTA3 step with the given dt (asynchronous on the stream). */
+int ucg_rk3_step(ucg_engine* e, double dt);
+
+/* nsteps of (CALCULATE_CFL + RUNGE_KUTTA3), dt kept on the device; no host
+ * synchronisation.  The dt of the last step is readable with ucg_last_dt.  */
+int ucg_step(ucg_engine* e, double cfl, int32_t nsteps);
+int ucg_last_dt(ucg_engine* e, double* dt);
+
+/* Domain sums over cells: UCG_REDUCE_KE = sum V*rho*|u|^2/2 (time_p.f90:4145),
+ * UCG_REDUCE_MASS = sum V*rho, UCG_REDUCE_ENERGY = sum V*E.                 */
+int ucg_reduce(ucg_engine* e, int32_t what, double* out);
+
+/* Synchronise, then report UCG_ENONPHYS if a kernel met a NaN or a
+ * non-positive density/pressure since the last call (and clear the flag). */
+int ucg_check_health(ucg_engine* e);
+int ucg_synchronize(ucg_engine* e);
+
+/* Average device time of the stage kernels over `reps` residual
+ * evaluations of the current state, measured with CUDA events on the
+ * handle's stream: ms[0] reconstruction, ms[1] face fluxes, ms[2] time step
+ * (CALCULATE_CFL).  For profiling; it leaves the state unchanged.          */
+int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms);
+
+/* The cudaStream_t of the handle, as an opaque pointer. */
+void* ucg_get_stream(ucg_engine* e);
+/* Kernel launches issued by the handle since creation. */
+int64_t ucg_launch_count(const ucg_engine* e);
+/* Device bytes held by the handle. */
+int64_t ucg_device_bytes(const ucg_engine* e);
+
+int ucg_last_error(const ucg_engine* e, char* buf, int32_t len);
+/* Message of the last failure of ucg_create (no handle exists then). */
+const char* ucg_create_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,106 @@
+"""ORACLE - test infrastructure only (tests/, __graft_entry__.smoke and the
+cpu_baseline leg of bench.py).  ctypes wrapper of oracle/_build/liboracle.so,
+the FP64 CPU restatement of the reference hot path (see
+oracle/ucns3d_oracle.cpp).  Nothing in the ucns3d_b200 package imports this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        from ucns3d_b200 import _native as N
+        L = C.CDLL(LIB)
+        cfgp, geop, recp = C.POINTER(N.UcgConfig), C.POINTER(N.UcgGeometry), C.POINTER(N.UcgRecon)
+        f64p = C.POINTER(C.c_double)
+        L.orc_residual.restype = C.c_int
+        L.orc_residual.argtypes = [cfgp, geop, recp, f64p, f64p]
+        L.orc_face_values.restype = C.c_int
+        L.orc_face_values.argtypes = [cfgp, geop, recp, f64p, f64p]
+        L.orc_compute_dt.restype = C.c_int
+        L.orc_compute_dt.argtypes = [cfgp, geop, f64p, C.c_double, f64p]
+        L.orc_rk3_step.restype = C.c_int
+        L.orc_rk3_step.argtypes = [cfgp, geop, recp, C.c_double, f64p]
+        L.orc_hllc.restype = C.c_int
+        L.orc_hllc.argtypes = [C.c_double, f64p, f64p, f64p]
+        L.orc_reduce.restype = C.c_int
+        L.orc_reduce.argtypes = [geop, f64p, C.c_int, f64p]
+        _lib = L
+    return _lib
+
+
+def hllc(gamma, cl, cr):
+    cl = np.ascontiguousarray(cl, dtype=np.float64)
+    cr = np.ascontiguousarray(cr, dtype=np.float64)
+    out = np.zeros(5)
+    lib().orc_hllc(gamma, _p(cl), _p(cr), _p(out))
+    return out
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """CPU restatement bound to one prepared mesh and configuration."""
+
+    def __init__(self, mesh, cfg):
+        self.mesh = mesh
+        self.cfg = cfg
+        self.geo = mesh.geometry_struct()
+        self.rec = mesh.recon_struct()
+        self.n = mesh.ncells
+
+    def residual(self, U: np.ndarray) -> np.ndarray:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = np.zeros_like(U)
+        rc = lib().orc_residual(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U), _p(out))
+        if rc:
+            raise RuntimeError(f"orc_residual failed: {rc}")
+        return out
+
+    def face_values(self, U: np.ndarray) -> np.ndarray:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = np.zeros((self.n, 6, 16, 5))
+        rc = lib().orc_face_values(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U), _p(out))
+        if rc:
+            raise RuntimeError(f"orc_face_values failed: {rc}")
+        return out
+
+    def compute_dt(self, U: np.ndarray, cfl: float) -> float:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        dt = C.c_double()
+        rc = lib().orc_compute_dt(C.byref(self.cfg), C.byref(self.geo), _p(U), cfl, C.byref(dt))
+        if rc:
+            raise RuntimeError(f"orc_compute_dt failed: {rc}")
+        return dt.value
+
+    def rk3_step(self, U: np.ndarray, dt: float) -> np.ndarray:
+        U = np.array(U, dtype=np.float64, copy=True, order="C")
+        rc = lib().orc_rk3_step(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), dt, _p(U))
+        if rc:
+            raise RuntimeError(f"orc_rk3_step failed: {rc}")
+        return U
+
+    def reduce(self, U: np.ndarray, what: int) -> float:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = C.c_double()
+        lib().orc_reduce(C.byref(self.geo), _p(U), what, C.byref(out))
+        return out.value

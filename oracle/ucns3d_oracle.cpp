@@ -1,0 +1,666 @@
+// ORACLE - test infrastructure only.
+//
+// A plain FP64 CPU restatement of UCNS3D's explicit residual and SSP-RK3
+// step, used by tests/ as the checker of the CUDA engine and by bench.py as
+// the timed CPU baseline ("port": the Fortran reference cannot be built
+// here - no Fortran compiler, no MPI).  It is never linked into, loaded by or
+// called from the engine.  Parity is UNPINNED at the reference-test level:
+// the reference ships no golden vectors or known-answer tests (its only test
+// mesh is missing), so this restatement is pinned by the property tests in
+// tests/ (free-stream preservation, exactness, conservation, consistency).
+//
+// It follows the reference's operation order, per cell:
+//   LEAST_SQUARES -> COMPUTE_GRADIENTS_MEAN_LSQ      src/gradients.f90:253-497
+//   COMPUTE_GRADIENTS_INNER_MEAN_LSQ_VISCOUS         src/gradients.f90:502-706
+//   WENOWEIGHTS / CP_RECONSTRUCTION / EXTRAPOLATE_BOUND
+//                                                    src/reconstruct_p.f90:407-1250, 1556
+//   CHECKSOL                                         src/reconstruct_p.f90:3126-3242
+//   MUSCL / FIND_BOUNDS / COMPUTE_MUSCL_RECONSTRUCTION / SLOPE_LIMITERS(7)
+//                                                    src/reconstruct_p.f90:2286, 1821, 2044, 3421
+//   CHECKSOLX                                        src/reconstruct_p.f90:3245-3406
+//   SOLUTIONTRIAV2                                   src/reconstruct_p.f90:2358
+//   CALCULATE_FLUXESHI_CONVECTIVE + HLLC_RIEMANN_SOLVER + ROTATEF/ROTATEB
+//                                                    src/flux_p.f90:478, riemann.f90:221, grid_t.f90:4217
+//   CALCULATE_FLUXESHI_DIFFUSIVE + SUTHERLAND        src/flux_p.f90:1520, flow_operations.f90:2609
+//   BOUNDARYS (inflow/outflow/symmetry/wall)         src/flow_operations.f90:2860-3230
+//   RUNGE_KUTTA3, CALCULATE_CFL                      src/time_p.f90:885-1027, 27-191
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "ucns3d_gpu.h"
+
+namespace {
+
+const int F = UCG_MAX_FACES, Q = UCG_MAX_QP, NV = 5;
+const double TOLSMALL = 1.0e-13, TOLBIG = 1.0e13;  // grid_p.f90:18-19
+
+struct Mono {
+  int e[3];
+};
+std::vector<Mono> monos(int order) {
+  std::vector<Mono> m;
+  for (int n = 1; n <= order; ++n)
+    for (int c = 0; c <= n; ++c)
+      for (int b = 0; b <= n - c; ++b) m.push_back({{n - c - b, b, c}});
+  return m;
+}
+double pw(double x, int e) {
+  double r = 1.0;
+  for (int i = 0; i < e; ++i) r *= x;
+  return r;
+}
+
+struct Ctx {
+  const ucg_config* cfg;
+  const ucg_geometry* g;
+  const ucg_recon* r;
+  int64_t n;
+  std::vector<Mono> mono;
+};
+
+void cons2prim(const Ctx& x, const double* u, double* p) {
+  double oo = 1.0 / u[0];
+  p[0] = u[0];
+  p[1] = u[1] * oo;
+  p[2] = u[2] * oo;
+  p[3] = u[3] * oo;
+  p[4] = (x.cfg->gamma - 1.0) * (u[4] - 0.5 * u[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]));
+}
+
+// basis at a local point: monomial minus its cell mean (BASIS_REC, icompwrt 0/1)
+void basis(const Ctx& x, int64_t c, const double* xi, int nd, double* b) {
+  for (int d = 0; d < nd; ++d) {
+    const Mono& m = x.mono[d];
+    b[d] = pw(xi[0], m.e[0]) * pw(xi[1], m.e[1]) * pw(xi[2], m.e[2]) - x.g->basis_mean[c * x.cfg->ideg + d];
+  }
+}
+// d/dxi_k of the monomials (DFX, DFY, DFZ)
+void dbasis(const Ctx& x, const double* xi, int nd, double* dx, double* dy, double* dz) {
+  for (int d = 0; d < nd; ++d) {
+    const Mono& m = x.mono[d];
+    double X = xi[0], Y = xi[1], Z = xi[2];
+    dx[d] = m.e[0] ? m.e[0] * pw(X, m.e[0] - 1) * pw(Y, m.e[1]) * pw(Z, m.e[2]) : 0.0;
+    dy[d] = m.e[1] ? m.e[1] * pw(X, m.e[0]) * pw(Y, m.e[1] - 1) * pw(Z, m.e[2]) : 0.0;
+    dz[d] = m.e[2] ? m.e[2] * pw(X, m.e[0]) * pw(Y, m.e[1]) * pw(Z, m.e[2] - 1) : 0.0;
+  }
+}
+
+inline int nq_of(const Ctx& x, int64_t c, int f) {
+  return x.g->face_type[c * F + f] == 5 ? x.cfg->nq_quad : x.cfg->nq_tri;
+}
+inline double wq_of(const Ctx& x, int64_t c, int f, int q) {
+  return x.g->face_type[c * F + f] == 5 ? x.cfg->quad_w[q] : x.cfg->tri_w[q];
+}
+inline int tab(const Ctx& x, int64_t c) { return x.r->table_id ? x.r->table_id[c] : (int)c; }
+
+// Venkatakrishnan limiter (SLOPE_LIMITERS case 7)
+double venkat(double usol, double u0, double umin, double umax, double minedge, double kappa) {
+  double d2 = usol - u0;
+  if (std::fabs(d2) <= 0.0) return 1.0;
+  double dmin = d2;
+  dmin = std::copysign(1.0, dmin) * (std::fabs(dmin) + TOLSMALL);
+  double dplus = (d2 > 0.0) ? umax - u0 : umin - u0;
+  double epsi2 = std::pow(kappa * minedge, 3);
+  return (1.0 / dmin) * ((((dplus * dplus) + epsi2) * dmin + (2.0 * (dmin * dmin) * dplus)) /
+                         ((dplus * dplus) + (2.0 * dmin * dmin) + (dmin * dplus) + epsi2));
+}
+
+// MUSCL on one cell: ULEFT from the central-stencil polynomial G0 [ideg][5]
+void muscl_cell(const Ctx& x, int64_t c, const double* U, const double* G0, double* ul /*[F][Q][5]*/) {
+  const ucg_geometry* g = x.g;
+  const int ideg = x.cfg->ideg;
+  const double* u0 = U + c * NV;
+  double umin[NV], umax[NV];
+  for (int v = 0; v < NV; ++v) umin[v] = umax[v] = u0[v];
+  for (int f = 0; f < g->nfaces[c]; ++f) {
+    int64_t nb = g->neigh[c * F + f];
+    if (nb < 0) continue;  // physical boundary faces add no bound (FIND_BOUNDS)
+    for (int v = 0; v < NV; ++v) {
+      umin[v] = std::min(umin[v], U[nb * NV + v]);
+      umax[v] = std::max(umax[v], U[nb * NV + v]);
+    }
+  }
+  double usol[F][Q][NV], slope[NV];
+  for (int v = 0; v < NV; ++v) slope[v] = TOLBIG;
+  std::vector<double> b(ideg);
+  for (int f = 0; f < g->nfaces[c]; ++f)
+    for (int q = 0; q < nq_of(x, c, f); ++q) {
+      basis(x, c, &g->qpoints[((c * F + f) * Q + q) * 3], ideg, b.data());
+      for (int v = 0; v < NV; ++v) {
+        double res = 0.0;
+        for (int d = 0; d < ideg; ++d) res += b[d] * G0[d * NV + v];
+        usol[f][q][v] = u0[v] + res;
+        double psi = venkat(usol[f][q][v], u0[v], umin[v], umax[v], g->minedge[c], x.cfg->kappa_ven);
+        slope[v] = std::min(slope[v], psi);
+      }
+    }
+  for (int f = 0; f < g->nfaces[c]; ++f)
+    for (int q = 0; q < nq_of(x, c, f); ++q)
+      for (int v = 0; v < NV; ++v) {
+        double du = usol[f][q][v] - u0[v];
+        ul[(f * Q + q) * NV + v] = u0[v] + du * slope[v];
+      }
+}
+
+// CHECKSOL / CHECKSOLX test of one cell's face values against its mean
+bool jump_check(const Ctx& x, int64_t c, const double* u0, const double* ul, double jump) {
+  double pr[NV], pl[NV];
+  cons2prim(x, u0, pr);
+  for (int f = 0; f < x.g->nfaces[c]; ++f)
+    for (int q = 0; q < nq_of(x, c, f); ++q) {
+      cons2prim(x, &ul[(f * Q + q) * NV], pl);
+      if (std::fabs(pl[0] - pr[0]) >= jump * pr[0]) return true;
+      if (std::fabs(pl[4] - pr[4]) >= jump * pr[4]) return true;
+      if (pl[4] < 0.0 || pl[0] < 0.0) return true;
+    }
+  return false;
+}
+
+// reconstruction of one cell: face values ul [F][Q][5] and, for
+// Navier-Stokes, face gradients ulv [F][Q][4][3] of (T, u, v, w)
+void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, double* ulv) {
+  const ucg_config* cfg = x.cfg;
+  const ucg_geometry* g = x.g;
+  const ucg_recon* r = x.r;
+  const int ideg = cfg->ideg, imax = cfg->imax, A = cfg->admis_max, W = imax + 1;
+  const int ideg2 = cfg->ideg2, imax2 = cfg->imax2;
+  const int t = tab(x, c);
+  const int32_t* st = &r->stencil[c * A * W];
+  const double* u0 = U + c * NV;
+  const int admis = g->admis[c];
+  // ---- least squares, every admissible stencil
+  std::vector<double> G((size_t)A * ideg * NV, 0.0);  // [ll][d][v]
+  for (int ll = 0; ll < admis; ++ll) {
+    bool low = (cfg->ees == 5 && ll > 0);
+    int nk = low ? imax2 : imax, nd = low ? ideg2 : ideg;
+    const double* M = low ? &r->invmat2[((int64_t)t * A + ll) * imax2 * ideg2] : &r->invmat[((int64_t)t * A + ll) * imax * ideg];
+    for (int d = 0; d < nd; ++d)
+      for (int v = 0; v < NV; ++v) {
+        double s = 0.0;
+        for (int k = 0; k < nk; ++k) {
+          int64_t y = st[ll * W + k + 1];
+          s += M[k * nd + d] * (U[y * NV + v] - u0[v]);
+        }
+        G[((size_t)ll * ideg + d) * NV + v] = s;
+      }
+  }
+  bool reduce = false;
+  if (cfg->scheme == 3) {
+    // ---- CP_RECONSTRUCTION
+    std::vector<double> w((size_t)A * NV);
+    std::vector<double> g1((size_t)ideg * NV, 0.0);  // central polynomial (CWENO)
+    for (int v = 0; v < NV; ++v) {
+      std::vector<double> is(admis), lam(admis), wt(admis);
+      if (cfg->ees == 5) {
+        double lc1 = 1.0 - 1.0 / cfg->lwci;
+        lam[0] = lc1;
+        for (int ll = 1; ll < admis; ++ll) lam[ll] = (1.0 - lc1) / (admis - 1);
+        std::vector<double> g3(ideg, 0.0);
+        for (int ll = 1; ll < admis; ++ll)
+          for (int d = 0; d < ideg2; ++d) g3[d] = g3[d] + lam[ll] * G[((size_t)ll * ideg + d) * NV + v];
+        std::vector<double> gg(ideg);
+        for (int d = 0; d < ideg; ++d) {
+          gg[d] = (1.0 / lam[0]) * (G[(size_t)d * NV + v] - g3[d]);
+          g1[d * NV + v] = gg[d];
+        }
+        const double* S = &r->indicator[(int64_t)t * ideg * ideg];
+        double acc = 0.0;
+        for (int d = 0; d < ideg; ++d) {
+          double sg = 0.0;
+          for (int e = 0; e < ideg; ++e) sg += S[d * ideg + e] * gg[e];
+          acc += gg[d] * sg;
+        }
+        is[0] = acc;
+        const double* S2 = &r->indicator2[(int64_t)t * ideg2 * ideg2];
+        for (int ll = 1; ll < admis; ++ll) {
+          double a2 = 0.0;
+          for (int d = 0; d < ideg2; ++d) {
+            double sg = 0.0;
+            for (int e = 0; e < ideg2; ++e) sg += S2[d * ideg2 + e] * G[((size_t)ll * ideg + e) * NV + v];
+            a2 += G[((size_t)ll * ideg + d) * NV + v] * sg;
+          }
+          is[ll] = a2;
+        }
+      } else {
+        const double* S = &r->indicator[(int64_t)t * ideg * ideg];
+        for (int ll = 0; ll < admis; ++ll) {
+          double acc = 0.0;
+          for (int d = 0; d < ideg; ++d) {
+            double sg = 0.0;
+            for (int e = 0; e < ideg; ++e) sg += S[d * ideg + e] * G[((size_t)ll * ideg + e) * NV + v];
+            acc += G[((size_t)ll * ideg + d) * NV + v] * sg;
+          }
+          is[ll] = acc;
+        }
+        for (int ll = 0; ll < admis; ++ll) lam[ll] = 1.0;
+        lam[0] = cfg->lwci;
+      }
+      const double eps = cfg->weno_eps;
+      if (cfg->ees == 5 && cfg->wenoz) {
+        double tau = 0.0;
+        for (int ll = 0; ll < admis; ++ll) tau = tau + std::fabs(is[0] - is[ll]);
+        tau = tau / (admis - 1);
+        for (int ll = 0; ll < admis; ++ll) wt[ll] = lam[ll] * (1.0 + std::pow(tau / (eps + is[ll]), 4));
+      } else {
+        for (int ll = 0; ll < admis; ++ll) wt[ll] = lam[ll] / std::pow(eps + is[ll], 4);
+      }
+      double sum = 0.0;
+      for (int ll = 0; ll < admis; ++ll) sum = sum + wt[ll];
+      for (int ll = 0; ll < admis; ++ll) w[(size_t)ll * NV + v] = wt[ll] / sum;
+    }
+    // face values: sum over stencils of weight * (U + basis . g)
+    for (int i = 0; i < F * Q * NV; ++i) ul[i] = 0.0;
+    std::vector<double> b(ideg);
+    for (int ll = 0; ll < admis; ++ll) {
+      bool low = (cfg->ees == 5 && ll > 0);
+      int nd = low ? ideg2 : ideg;
+      for (int f = 0; f < g->nfaces[c]; ++f)
+        for (int q = 0; q < nq_of(x, c, f); ++q) {
+          basis(x, c, &g->qpoints[((c * F + f) * Q + q) * 3], ideg, b.data());
+          for (int v = 0; v < NV; ++v) {
+            double res = 0.0;
+            for (int d = 0; d < nd; ++d) {
+              double gv = (cfg->ees == 5 && ll == 0) ? g1[d * NV + v] : G[((size_t)ll * ideg + d) * NV + v];
+              res += b[d] * gv;
+            }
+            double* o = &ul[(f * Q + q) * NV + v];
+            *o = *o + (u0[v] + res) * w[(size_t)ll * NV + v];
+          }
+        }
+    }
+    // CHECKSOL
+    if (!g->full[c]) reduce = true;
+    else reduce = jump_check(x, c, u0, ul, 0.85);
+  }
+  // MUSCL (all cells for scheme 2; flagged cells for WENO)
+  if (cfg->scheme == 2 || reduce || !g->full[c]) muscl_cell(x, c, U, G.data(), ul);
+  // CHECKSOLX: first order where the face values jump too far
+  if (jump_check(x, c, u0, ul, 0.95)) {
+    for (int f = 0; f < F; ++f)
+      for (int q = 0; q < Q; ++q)
+        for (int v = 0; v < NV; ++v) ul[(f * Q + q) * NV + v] = u0[v];
+  }
+  // ---- SOLUTIONTRIAV2: face gradients of (T, u, v, w) from stencil 1
+  if (cfg->governing == 1) {
+    double p0[NV];
+    cons2prim(x, u0, p0);
+    double s1[4] = {p0[4] / (p0[0] * cfg->r_gas), p0[1], p0[2], p0[3]};
+    std::vector<double> Gv((size_t)ideg * 4, 0.0);
+    const double* M = &r->invmat[((int64_t)t * A + 0) * imax * ideg];
+    for (int d = 0; d < ideg; ++d)
+      for (int v = 0; v < 4; ++v) {
+        double s = 0.0;
+        for (int k = 0; k < imax; ++k) {
+          int64_t y = st[k + 1];
+          double py[NV];
+          cons2prim(x, &U[y * NV], py);
+          double s2[4] = {py[4] / (py[0] * cfg->r_gas), py[1], py[2], py[3]};
+          s += M[k * ideg + d] * (s2[v] - s1[v]);
+        }
+        Gv[d * 4 + v] = s;
+      }
+    const double* J = &g->invccjac[c * 9];
+    std::vector<double> bx(ideg), by(ideg), bz(ideg);
+    for (int f = 0; f < g->nfaces[c]; ++f)
+      for (int q = 0; q < nq_of(x, c, f); ++q) {
+        dbasis(x, &g->qpoints[((c * F + f) * Q + q) * 3], ideg, bx.data(), by.data(), bz.data());
+        for (int v = 0; v < 4; ++v) {
+          double gl[3] = {0.0, 0.0, 0.0};
+          for (int d = 0; d < ideg; ++d) gl[0] += Gv[d * 4 + v] * bx[d];
+          for (int d = 0; d < ideg; ++d) gl[1] += Gv[d * 4 + v] * by[d];
+          for (int d = 0; d < ideg; ++d) gl[2] += Gv[d * 4 + v] * bz[d];
+          // AINVJT = INVCCJAC^T
+          for (int k = 0; k < 3; ++k)
+            ulv[((f * Q + q) * 4 + v) * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
+        }
+      }
+  }
+}
+
+void rotf(const double* a, const double* v, double* o) {
+  // ROTATEF; a = (cos a1, sin a1, cos a2, sin a2)
+  double ca1 = a[0], sa1 = a[1], ca2 = a[2], sa2 = a[3];
+  o[0] = v[0];
+  o[1] = ca1 * sa2 * v[1] + sa1 * sa2 * v[2] + ca2 * v[3];
+  o[2] = ca1 * ca2 * v[1] + sa1 * ca2 * v[2] - sa2 * v[3];
+  o[3] = -sa1 * v[1] + ca1 * v[2];
+  o[4] = v[4];
+}
+void rotb(const double* a, const double* v, double* o) {
+  double ca1 = a[0], sa1 = a[1], ca2 = a[2], sa2 = a[3];
+  o[0] = v[0];
+  o[1] = ca1 * sa2 * v[1] + ca1 * ca2 * v[2] - sa1 * v[3];
+  o[2] = sa1 * sa2 * v[1] + sa1 * ca2 * v[2] + ca1 * v[3];
+  o[3] = ca2 * v[1] - sa2 * v[2];
+  o[4] = v[4];
+}
+
+void hllc(double gamma, const double* cl, const double* cr, double* flux) {
+  double rl = cl[0], ul = cl[1] / rl, vl = cl[2] / rl, wl = cl[3] / rl;
+  double pl = (gamma - 1.0) * (cl[4] - 0.5 * rl * (ul * ul + vl * vl + wl * wl));
+  double rr = cr[0], ur = cr[1] / rr, vr = cr[2] / rr, wr = cr[3] / rr;
+  double pr = (gamma - 1.0) * (cr[4] - 0.5 * rr * (ur * ur + vr * vr + wr * wr));
+  double el = cl[4], er = cr[4];
+  double ccl = std::sqrt(gamma * pl / rl), ccr = std::sqrt(gamma * pr / rr);
+  double srl = std::sqrt(rl), srr = std::sqrt(rr);
+  double cc2 = std::sqrt((((ccl * ccl) * srl) + ((ccr * ccr) * srr)) / (srl + srr) +
+                         0.5 * ((srl * srr) / ((srl + srr) * (srl + srr))) * ((ur - ul) * (ur - ul)));
+  double uu2 = ((ul * srl) + (ur * srr)) / (srl + srr);
+  double sl = std::min(ul - ccl, uu2 - cc2), sr = std::max(ur + ccr, uu2 + cc2);
+  sl = std::min(sl, 0.0);
+  sr = std::max(sr, 0.0);
+  double sm = (pr - pl + (rl * ul * (sl - ul)) - (rr * ur * (sr - ur))) / ((rl * (sl - ul)) - (rr * (sr - ur)));
+  double fl[5] = {rl * ul, rl * ul * ul + pl, rl * ul * vl, rl * ul * wl, ul * (el + pl)};
+  double fr[5] = {rr * ur, rr * ur * ur + pr, rr * ur * vr, rr * ur * wr, ur * (er + pr)};
+  double mul = rl * ((sl - ul) / (sl - sm)), mur = rr * ((sr - ur) / (sr - sm));
+  double lastl = (el / rl) + ((sm - ul) * (sm + (pl / (rl * (sl - ul)))));
+  double lastr = (er / rr) + ((sm - ur) * (sm + (pr / (rr * (sr - ur)))));
+  double ls[5] = {mul, mul * sm, mul * vl, mul * wl, mul * lastl};
+  double rs[5] = {mur, mur * sm, mur * vr, mur * wr, mur * lastr};
+  double sg = std::copysign(1.0, sm);
+  for (int k = 0; k < 5; ++k)
+    flux[k] = (((1.0 + sg) / 2.0) * (fl[k] + sl * (ls[k] - cl[k]))) + (((1.0 - sg) / 2.0) * (fr[k] + sr * (rs[k] - cr[k])));
+}
+
+// ghost state of a physical boundary face (BOUNDARYS, boundtype 1 = subsonic
+// treatment, src/flow_operations.f90:2860-3230).  cfg->bc_state holds the
+// free-stream primitive state (rho, u, v, w, p) that INFLOW/OUTFLOW return.
+void prim2cons(double gm, const double* p, double* u) {
+  double skin = 0.5 * ((p[1] * p[1]) + (p[2] * p[2]) + (p[3] * p[3]));
+  double ie = p[4] / ((gm - 1.0) * p[0]);
+  u[0] = p[0];
+  u[1] = p[1] * p[0];
+  u[2] = p[2] * p[0];
+  u[3] = p[3] * p[0];
+  u[4] = (p[0] * ie) + (p[0] * skin);
+}
+void boundary_state(const Ctx& x, int code, const double* ang, const double* cl, double* cr) {
+  const ucg_config* cfg = x.cfg;
+  const double gm = cfg->gamma;
+  double nx = ang[0] * ang[3], ny = ang[1] * ang[3], nz = ang[2];
+  if (code == 3 || code == 4) {  // symmetry; inviscid wall (ITESTCASE 3)
+    double rl[NV], rr[NV];
+    rotf(ang, cl, rl);
+    rr[0] = rl[0];
+    rr[1] = -rl[1];
+    rr[2] = rl[2];
+    rr[3] = rl[3];
+    rr[4] = rl[4];
+    rotb(ang, rr, cr);
+    return;
+  }
+  double s1[NV], s2[NV], s3[NV];
+  for (int k = 0; k < NV; ++k) s1[k] = cfg->bc_state[k];
+  cons2prim(x, cl, s2);
+  double sps = std::sqrt((gm * s2[4]) / (s2[0]));
+  double vel = std::sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+  bool super = vel / (sps + TOLSMALL) > 1.0;
+  if (code == 1) {  // inflow
+    if (super) {
+      prim2cons(gm, s1, cr);
+      return;
+    }
+    s3[4] = 0.5 * ((s1[4]) + (s2[4]) - (s2[0] * sps * ((nx * (s1[1] - s2[1])) + (ny * (s1[2] - s2[2])) + (nz * (s1[3] - s2[3])))));
+    s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
+    s3[1] = s1[1] - (nx * (s1[4] - s3[4])) / (sps * s2[0]);
+    s3[2] = s1[2] - (ny * (s1[4] - s3[4])) / (sps * s2[0]);
+    s3[3] = s1[3] - (nz * (s1[4] - s3[4])) / (sps * s2[0]);
+  } else if (code == 2) {  // outflow
+    if (super) {
+      for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+      return;
+    }
+    s3[4] = s1[4];
+    s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
+    s3[1] = s2[1] + (nx * (s2[4] - s3[4])) / (sps * s2[0]);
+    s3[2] = s2[2] + (ny * (s2[4] - s3[4])) / (sps * s2[0]);
+    s3[3] = s2[3] + (nz * (s2[4] - s3[4])) / (sps * s2[0]);
+  } else {  // any other code: free stream
+    prim2cons(gm, s1, cr);
+    return;
+  }
+  prim2cons(gm, s3, cr);
+}
+
+void sutherland(const ucg_config* cfg, double rho, double p, double* mu, double* lam) {
+  double t1 = p / (rho * cfg->r_gas);
+  double t0 = cfg->pres / (cfg->rres * cfg->r_gas);
+  const double betaas = 1.5, suther = 0.412158681;  // parameters.f90:1220-1221
+  *mu = cfg->visc * std::pow(t1 / t0, betaas) * ((t0 + (suther * t0)) / (t1 + (suther * t0)));
+  *lam = (*mu) * cfg->r_gas * cfg->gamma / (cfg->prandtl * (cfg->gamma - 1.0));
+}
+
+// CALL_FLUX_SUBROUTINES_3D: rhs [n][5]
+void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& UL, std::vector<double>& ULV) {
+  const int64_t n = x.n;
+  const bool ns = x.cfg->governing == 1;
+  UL.assign((size_t)n * F * Q * NV, 0.0);
+  if (ns) ULV.assign((size_t)n * F * Q * 12, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) reconstruct_cell(x, c, U, &UL[(size_t)c * F * Q * NV], ns ? &ULV[(size_t)c * F * Q * 12] : nullptr);
+  const ucg_geometry* g = x.g;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) {
+    double R[NV] = {0, 0, 0, 0, 0};
+    // convective
+    for (int f = 0; f < g->nfaces[c]; ++f) {
+      double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+      double ang[4] = {std::cos(a1), std::sin(a1), std::cos(a2), std::sin(a2)};
+      double god[NV] = {0, 0, 0, 0, 0};
+      int64_t nb = g->neigh[c * F + f];
+      int nf = g->neigh_face[c * F + f];
+      for (int q = 0; q < nq_of(x, c, f); ++q) {
+        const double* cl = &UL[(((size_t)c * F + f) * Q + q) * NV];
+        double crb[NV];
+        const double* cr;
+        if (nb >= 0) {
+          int qq = g->qperm[(c * F + f) * Q + q];
+          cr = &UL[(((size_t)nb * F + nf) * Q + qq) * NV];
+        } else {
+          boundary_state(x, g->bc[c * F + f], ang, cl, crb);
+          cr = crb;
+        }
+        double clr[NV], crr[NV], hf[NV], fl[NV];
+        rotf(ang, cr, crr);
+        rotf(ang, cl, clr);
+        hllc(x.cfg->gamma, clr, crr, hf);
+        rotb(ang, hf, fl);
+        double ws = wq_of(x, c, f, q) * g->face_area[c * F + f];
+        for (int v = 0; v < NV; ++v) god[v] = god[v] + (fl[v] * ws);
+      }
+      for (int v = 0; v < NV; ++v) R[v] = R[v] + god[v];
+    }
+    // diffusive
+    if (ns) {
+      const ucg_config* cfg = x.cfg;
+      for (int f = 0; f < g->nfaces[c]; ++f) {
+        double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+        double nx = std::cos(a1) * std::sin(a2), ny = std::sin(a1) * std::sin(a2), nz = std::cos(a2);
+        double nn[3] = {nx, ny, nz};
+        double god[NV] = {0, 0, 0, 0, 0};
+        int64_t nb = g->neigh[c * F + f];
+        int nf = g->neigh_face[c * F + f];
+        for (int q = 0; q < nq_of(x, c, f); ++q) {
+          int qq = g->qperm[(c * F + f) * Q + q];
+          const double* cl = &UL[(((size_t)c * F + f) * Q + q) * NV];
+          const double* cr = &UL[(((size_t)nb * F + nf) * Q + qq) * NV];
+          const double* gl = &ULV[(((size_t)c * F + f) * Q + q) * 12];
+          const double* gr = &ULV[(((size_t)nb * F + nf) * Q + qq) * 12];
+          double lv[NV], rv[NV];
+          cons2prim(x, cl, lv);
+          cons2prim(x, cr, rv);
+          double mul, mur, laml, lamr;
+          sutherland(cfg, lv[0], lv[4], &mul, &laml);
+          sutherland(cfg, rv[0], rv[4], &mur, &lamr);
+          // LCVGRAD rows: u, v, w, T (ULEFTV components 2,3,4,1)
+          double lg[4][3], rg[4][3];
+          for (int k = 0; k < 3; ++k) {
+            lg[0][k] = gl[1 * 3 + k]; lg[1][k] = gl[2 * 3 + k]; lg[2][k] = gl[3 * 3 + k]; lg[3][k] = gl[0 * 3 + k];
+            rg[0][k] = gr[1 * 3 + k]; rg[1][k] = gr[2 * 3 + k]; rg[2][k] = gr[3 * 3 + k]; rg[3][k] = gr[0 * 3 + k];
+          }
+          double damp = cfg->lamx, vdamp = 4.0 / 3.0;
+          double dih = std::fabs(g->dih[c * F + f]);
+          double jump[4] = {rv[1] - lv[1], rv[2] - lv[2], rv[3] - lv[3],
+                            (rv[4] / (rv[0] * cfg->r_gas)) - (lv[4] / (lv[0] * cfg->r_gas))};
+          double gg[4][3];
+          for (int a = 0; a < 4; ++a)
+            for (int k = 0; k < 3; ++k) gg[a][k] = ((lg[a][k] + rg[a][k]) / 2.0) + damp * ((vdamp / dih) * nn[k] * jump[a]);
+          double fxv[5] = {0, 0, 0, 0, 0}, fyv[5] = {0, 0, 0, 0, 0}, fzv[5] = {0, 0, 0, 0, 0};
+          double qh[3];
+          for (int k = 0; k < 3; ++k) qh[k] = -0.5 * ((laml + lamr) * gg[3][k]);
+          fxv[4] = fxv[4] - qh[0];
+          fyv[4] = fyv[4] - qh[1];
+          fzv[4] = fzv[4] - qh[2];
+          double ux = gg[0][0], uy = gg[0][1], uz = gg[0][2];
+          double vx = gg[1][0], vy = gg[1][1], vz = gg[1][2];
+          double wx = gg[2][0], wy = gg[2][1], wz = gg[2][2];
+          double tl[3][3];
+          tl[0][0] = (4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz;
+          tl[1][1] = (4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz;
+          tl[2][2] = (4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy;
+          tl[0][1] = tl[1][0] = (uy + vx);
+          tl[0][2] = tl[2][0] = (wx + uz);
+          tl[1][2] = tl[2][1] = (vz + wy);
+          double mu2 = 0.5 * (mul + mur);
+          double tau[3][3];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) tau[a][b] = mu2 * tl[a][b];
+          for (int k = 1; k <= 3; ++k) {
+            fxv[k] = fxv[k] + tau[0][k - 1];
+            fyv[k] = fyv[k] + tau[1][k - 1];
+            fzv[k] = fzv[k] + tau[2][k - 1];
+          }
+          double rho12 = 0.5 * (cl[0] + cr[0]);
+          double u12 = 0.5 * (cl[1] + cr[1]) / rho12, v12 = 0.5 * (cl[2] + cr[2]) / rho12, w12 = 0.5 * (cl[3] + cr[3]) / rho12;
+          fxv[4] = fxv[4] + u12 * tau[0][0] + v12 * tau[0][1] + w12 * tau[0][2];
+          fyv[4] = fyv[4] + u12 * tau[1][0] + v12 * tau[1][1] + w12 * tau[1][2];
+          fzv[4] = fzv[4] + u12 * tau[2][0] + v12 * tau[2][1] + w12 * tau[2][2];
+          double ws = wq_of(x, c, f, q) * g->face_area[c * F + f];
+          for (int v = 0; v < NV; ++v) god[v] = god[v] + ((nx * fxv[v] + ny * fyv[v] + nz * fzv[v]) * ws);
+        }
+        for (int v = 0; v < NV; ++v) R[v] = R[v] - god[v];
+      }
+    }
+    for (int v = 0; v < NV; ++v) rhs[c * NV + v] = R[v];
+  }
+}
+
+bool check_ctx(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r) {
+  if (!cfg || !g || !r) return false;
+  if (r->first != 0 || r->count != g->ncells) return false;
+  if (cfg->governing == 1) {
+    for (int64_t c = 0; c < g->ncells; ++c)
+      for (int f = 0; f < g->nfaces[c]; ++f)
+        if (g->neigh[c * F + f] < 0) return false;  // viscous walls are not restated
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One CALL_FLUX_SUBROUTINES_3D: RHS(I)%VAL for every cell.
+int orc_residual(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, const double* U, double* rhs) {
+  if (!check_ctx(cfg, g, r) || !U || !rhs) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  std::vector<double> UL, ULV;
+  residual(x, U, rhs, UL, ULV);
+  return UCG_OK;
+}
+
+// Face values ULEFT [n][F][Q][5] after reconstruction (for kernel-level tests).
+int orc_face_values(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, const double* U, double* ul) {
+  if (!check_ctx(cfg, g, r) || !U || !ul) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const bool ns = cfg->governing == 1;
+  std::vector<double> tmp;
+#pragma omp parallel for schedule(dynamic, 64) private(tmp)
+  for (int64_t c = 0; c < g->ncells; ++c) {
+    tmp.assign(ns ? F * Q * 12 : 1, 0.0);
+    for (int i = 0; i < F * Q * NV; ++i) ul[(size_t)c * F * Q * NV + i] = 0.0;
+    reconstruct_cell(x, c, U, &ul[(size_t)c * F * Q * NV], ns ? tmp.data() : nullptr);
+  }
+  return UCG_OK;
+}
+
+// CALCULATE_CFL (time_p.f90:27-191), CCFL = CFL/3.
+int orc_compute_dt(const ucg_config* cfg, const ucg_geometry* g, const double* U, double cfl, double* dt) {
+  if (!cfg || !g || !U || !dt) return UCG_EINVAL;
+  double ccfl = cfl / 3.0, best = TOLBIG;
+  Ctx x{cfg, g, nullptr, g->ncells, {}};
+  for (int64_t c = 0; c < g->ncells; ++c) {
+    double p[NV];
+    cons2prim(x, &U[c * NV], p);
+    double agrt = std::sqrt(p[4] * cfg->gamma / p[0]);
+    double veln = std::max(std::max(std::fabs(p[1]), std::fabs(p[2])), std::fabs(p[3])) + agrt;
+    double me = g->minedge[c];
+    double d;
+    if (cfg->governing == 1) {
+      double mu, lam;
+      sutherland(cfg, p[0], p[4], &mu, &lam);
+      d = ccfl * (1.0 / ((std::fabs(veln) / me) + (0.5 * (lam + mu) / (me * me))));
+    } else {
+      d = ccfl * (me / std::fabs(veln));
+    }
+    best = std::min(best, d);
+  }
+  *dt = best;
+  return UCG_OK;
+}
+
+// RUNGE_KUTTA3 (time_p.f90:885-1027) in place on U [n][5].
+int orc_rk3_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt, double* U) {
+  if (!check_ctx(cfg, g, r) || !U) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const int64_t n = g->ncells;
+  std::vector<double> U0(U, U + n * NV), U1, rhs(n * NV), UL, ULV;
+  const double to4 = 3.0 / 4.0, oo4 = 1.0 / 4.0, to3 = 2.0 / 3.0, oo3 = 1.0 / 3.0;
+  residual(x, U, rhs.data(), UL, ULV);
+  for (int64_t c = 0; c < n; ++c) {
+    double oov = 1.0 / g->volume[c];
+    for (int v = 0; v < NV; ++v) U[c * NV + v] = U0[c * NV + v] - (dt * (rhs[c * NV + v] * oov));
+  }
+  residual(x, U, rhs.data(), UL, ULV);
+  for (int64_t c = 0; c < n; ++c) {
+    double oov = 1.0 / g->volume[c];
+    for (int v = 0; v < NV; ++v) {
+      double u3 = U[c * NV + v];
+      U[c * NV + v] = (to4 * U0[c * NV + v]) + (oo4 * u3) - ((oo4) * ((dt) * ((rhs[c * NV + v]) * (oov))));
+    }
+  }
+  residual(x, U, rhs.data(), UL, ULV);
+  for (int64_t c = 0; c < n; ++c) {
+    double oov = 1.0 / g->volume[c];
+    for (int v = 0; v < NV; ++v)
+      U[c * NV + v] = ((oo3)*U0[c * NV + v]) + ((to3)*U[c * NV + v]) - (((to3)) * ((dt) * ((rhs[c * NV + v]) * (oov))));
+  }
+  return UCG_OK;
+}
+
+// HLLC flux of two conserved states in the face frame (known-answer tests).
+int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
+  hllc(gamma, cl, cr, flux);
+  return UCG_OK;
+}
+
+// Domain sums (time_p.f90:4145-4198): 1 = kinetic energy, 2 = mass, 3 = energy.
+int orc_reduce(const ucg_geometry* g, const double* U, int what, double* out) {
+  if (!g || !U || !out) return UCG_EINVAL;
+  double s = 0.0;
+  for (int64_t c = 0; c < g->ncells; ++c) {
+    const double* u = &U[c * NV];
+    double v;
+    if (what == UCG_REDUCE_KE) v = 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
+    else if (what == UCG_REDUCE_MASS) v = u[0];
+    else v = u[4];
+    s += g->volume[c] * v;
+  }
+  *out = s;
+  return UCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,190 @@
+"""CUDA engine against the oracle, through the C ABI, on a B200.
+
+Tolerances (FP64 engine): the residual agrees with the oracle to 1e-12
+relative to the largest flux magnitude of the cell's faces (per variable,
+max over cells); after several RK3 steps the state agrees to 1e-10 relative.
+Differences come only from floating-point contraction/ordering (the GPU fuses
+multiply-adds).  The mixed form (FP32 tables and reconstruction on
+differences, FP64 fluxes/accumulation/update) agrees with the FP64 engine to
+2e-5 relative in the residual."""
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from ucns3d_b200 import _native as N
+from ucns3d_b200.config import EULER, NAVIER_STOKES, make_config
+from ucns3d_b200.engine import Engine, EngineError
+from ucns3d_b200.mesh import IC_TGV, IC_VORTEX, SCHEME_MUSCL, SCHEME_WENO, Mesh
+from ucns3d_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {
+    "muscl_ns_hex": (lambda: Mesh.box_hex(10, 10, 10), SCHEME_MUSCL, 1, 0, NAVIER_STOKES),
+    "muscl_euler_tet": (lambda: Mesh.box_tet(5, 5, 5, seed=9), SCHEME_MUSCL, 1, 0, EULER),
+    "weno3_tet": (lambda: Mesh.box_tet(5, 5, 5, seed=3), SCHEME_WENO, 2, 0, EULER),
+    "weno5_hex": (lambda: Mesh.box_hex(12, 12, 12), SCHEME_WENO, 4, 0, EULER),
+    "cweno4_tet": (lambda: Mesh.box_tet(5, 5, 5, seed=5), SCHEME_WENO, 3, 5, EULER),
+    "cweno4_ns_mixed": (lambda: Mesh.mixed_box(8, seed=4), SCHEME_WENO, 3, 5, NAVIER_STOKES),
+    "weno3_ns_hex": (lambda: Mesh.box_hex(8, 8, 8), SCHEME_WENO, 2, 0, NAVIER_STOKES),
+    "muscl_bump": (lambda: Mesh.bump_channel(24, 10, 2, seed=2), SCHEME_MUSCL, 1, 0, EULER),
+    "muscl_p2_hex": (lambda: Mesh.box_hex(8, 8, 8), SCHEME_MUSCL, 2, 0, EULER),
+}
+
+
+def _setup(name, precision=N.UCG_FP64):
+    mk, scheme, iorder, ees, gov = SMALL[name]
+    m = mk().prepare(scheme, iorder, ees)
+    p0 = 71.43
+    bc = (1.0, 0.675 * np.sqrt(1.4), 0.0, 0.0, 1.0)
+    cfg = make_config(m, governing=gov, precision=precision, reynolds=1600.0, pres=p0 if gov == NAVIER_STOKES else 1.0,
+                      prandtl=0.71, bc_state=bc)
+    if name == "muscl_bump":
+        U = m.initial_condition(1, [1.4, *bc])
+        # a smooth disturbance so that every branch sees non-trivial data
+        c = m.centres()
+        U[:, 0] *= 1.0 + 0.05 * np.sin(2 * np.pi * c[:, 0] / 3.0) * np.sin(np.pi * c[:, 1])
+    else:
+        U = m.initial_condition(IC_TGV, [1.4, p0 if gov == NAVIER_STOKES else 5.0, 1.0])
+    return m, cfg, U
+
+
+def _flux_scale(o, m, U):
+    # magnitude of the face fluxes of a cell: |R| of a one-sided evaluation is
+    # not available, so use the uniform-state flux scale of each cell
+    g = m.geometry()
+    r, u = U[:, 0], U[:, 1:4] / U[:, :1]
+    p = 0.4 * (U[:, 4] - 0.5 * r * (u * u).sum(1))
+    area = (g["face_area"] * (np.arange(6)[None, :] < g["nfaces"][:, None])).sum(1)
+    s = np.abs(U).max(1) * (np.abs(u).max(1) + np.sqrt(1.4 * p / r)) + p
+    return (s * area)[:, None]
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_residual_matches_oracle(name):
+    m, cfg, U = _setup(name)
+    o = Oracle(m, cfg)
+    e = Engine(m, cfg)
+    e.set_state(U)
+    Rg = e.call_flux_subroutines_3d()
+    Ro = o.residual(U)
+    scale = _flux_scale(o, m, U)
+    err = (np.abs(Rg - Ro) / scale).max()
+    print(f"{name}: residual rel err {err:.3e}")
+    assert err < 1e-12
+
+
+@pytest.mark.parametrize("name", ["muscl_ns_hex", "weno3_tet", "weno5_hex", "cweno4_tet", "muscl_bump"])
+def test_rk3_steps_match_oracle(name):
+    m, cfg, U = _setup(name)
+    o = Oracle(m, cfg)
+    e = Engine(m, cfg)
+    e.set_state(U)
+    Uo = U.copy()
+    for _ in range(3):
+        dt_g = e.calculate_cfl(0.5)
+        dt_o = o.compute_dt(Uo, 0.5)
+        assert abs(dt_g - dt_o) <= 1e-14 * dt_o
+        e.runge_kutta3(dt_o)
+        Uo = o.rk3_step(Uo, dt_o)
+    Ug = e.get_state()
+    err = (np.abs(Ug - Uo) / np.abs(Uo).max(0)).max()
+    print(f"{name}: 3-step state rel err {err:.3e}")
+    assert err < 1e-10
+    e.check_health()
+
+
+def test_device_dt_stepping_matches_host_dt():
+    m, cfg, U = _setup("weno3_tet")
+    a, b = Engine(m, cfg), Engine(m, cfg)
+    a.set_state(U)
+    b.set_state(U)
+    for _ in range(2):
+        dt = b.calculate_cfl(0.5)
+        b.runge_kutta3(dt)
+    a.time_marching(2, 0.5)
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+
+
+def test_bitwise_deterministic():
+    m, cfg, U = _setup("weno3_tet")
+    out = []
+    for _ in range(2):
+        e = Engine(m, cfg)
+        e.set_state(U)
+        e.time_marching(3, 0.5)
+        out.append(e.get_state())
+        e.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_reductions_match_oracle():
+    m, cfg, U = _setup("weno5_hex")
+    o = Oracle(m, cfg)
+    e = Engine(m, cfg)
+    e.set_state(U)
+    for what in (N.UCG_REDUCE_KE, N.UCG_REDUCE_MASS, N.UCG_REDUCE_ENERGY):
+        a, b = e.reduce(what), o.reduce(U, what)
+        assert abs(a - b) <= 1e-13 * abs(b)
+
+
+@pytest.mark.parametrize("name", ["weno5_hex", "weno3_tet", "muscl_ns_hex", "cweno4_tet"])
+def test_mixed_precision_close_to_fp64(name):
+    m, cfg64, U = _setup(name, N.UCG_FP64)
+    _, cfg32, _ = _setup(name, N.UCG_MIXED)
+    cfg32 = make_config(m, governing=cfg64.governing, precision=N.UCG_MIXED, reynolds=1600.0, pres=cfg64.pres,
+                        prandtl=0.71)
+    a, b = Engine(m, cfg64), Engine(m, cfg32)
+    a.set_state(U)
+    b.set_state(U)
+    Ra, Rb = a.call_flux_subroutines_3d(), b.call_flux_subroutines_3d()
+    err = (np.abs(Ra - Rb) / _flux_scale(None, m, U)).max()
+    print(f"{name}: mixed vs fp64 residual rel err {err:.3e}")
+    assert err < 2e-5
+
+
+def test_mixed_weno5_vortex_density_error():
+    """Isentropic vortex, WENO5: after 20 RK3 steps the mixed form's density
+    stays within 1e-6 relative L2 of the FP64 form."""
+    c64 = cases.vortex_hex_weno5(n=16)
+    c32 = cases.vortex_hex_weno5(n=16, precision=N.UCG_MIXED)
+    a, b = Engine(c64.mesh, c64.cfg), Engine(c32.mesh, c32.cfg)
+    a.set_state(c64.U0)
+    b.set_state(c32.U0)
+    a.time_marching(20, 0.5)
+    b.time_marching(20, 0.5)
+    ra, rb = a.get_state()[:, 0], b.get_state()[:, 0]
+    l2 = np.sqrt(np.mean((ra - rb) ** 2)) / np.sqrt(np.mean(ra ** 2))
+    print(f"vortex mixed vs fp64 density L2 {l2:.3e}")
+    assert l2 < 1e-6
+
+
+def test_nonphysical_state_is_reported_not_trapped():
+    m, cfg, U = _setup("muscl_ns_hex")
+    e = Engine(m, cfg)
+    bad = U.copy()
+    bad[5, 0] = -1.0
+    e.set_state(bad)
+    e.runge_kutta3(1e-3)
+    with pytest.raises(EngineError) as ei:
+        e.check_health()
+    assert ei.value.code == N.UCG_ENONPHYS
+    # the context stays usable
+    e.set_state(U)
+    e.runge_kutta3(1e-3)
+    e.check_health()
+
+
+def test_call_order_is_checked():
+    m, cfg, U = _setup("weno3_tet")
+    e = Engine(m, cfg, upload=False)
+    with pytest.raises(EngineError) as ei:
+        e.runge_kutta3(1e-3)
+    assert ei.value.code == N.UCG_ESTATE
+    import ctypes as C
+    assert e.lib.ucg_set_state(e._h, N.ptr(U, C.c_double), m.ncells - 1) == N.UCG_EINVAL
+    e.upload_geometry(m.geometry_struct())
+    e.upload_recon(m.recon_struct())
+    e.set_state(U)
+    e.runge_kutta3(1e-3)
+    e.check_health()

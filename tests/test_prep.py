@@ -1,0 +1,117 @@
+"""Host set-up library: meshes, connectivity, geometry and reconstruction
+tables (CPU only)."""
+import numpy as np
+import pytest
+
+from ucns3d_b200.mesh import SCHEME_MUSCL, SCHEME_WENO, Mesh
+
+L = 2 * np.pi
+
+
+def _normals(g):
+    a = g["face_angle"]
+    return np.stack([np.cos(a[..., 0]) * np.sin(a[..., 1]), np.sin(a[..., 0]) * np.sin(a[..., 1]),
+                     np.cos(a[..., 1])], -1)
+
+
+MESHES = {
+    "hex": lambda: Mesh.box_hex(6, 5, 4),
+    "tet": lambda: Mesh.box_tet(4, 4, 3, jitter=0.15, seed=7),
+    "bump": lambda: Mesh.bump_channel(12, 6, 2, seed=3),
+    "mixed": lambda: Mesh.mixed_box(8, seed=5),
+}
+
+
+@pytest.mark.parametrize("kind", list(MESHES))
+def test_connectivity_and_closure(kind):
+    m = MESHES[kind]().prepare(SCHEME_MUSCL, 1)
+    g = m.geometry()
+    n = g["ncells"]
+    assert n == m.ncells > 0
+    assert (g["volume"] > 0).all()
+    # neighbour relation is symmetric and normals/areas match across faces
+    nrm = _normals(g)
+    for c in range(n):
+        for f in range(g["nfaces"][c]):
+            nb, nf = g["neigh"][c, f], g["neigh_face"][c, f]
+            if nb < 0:
+                assert g["bc"][c, f] in (1, 2, 3, 4)
+                continue
+            assert g["neigh"][nb, nf] == c and g["neigh_face"][nb, nf] == f
+            assert abs(g["face_area"][c, f] - g["face_area"][nb, nf]) < 1e-12 * g["face_area"][c, f]
+            np.testing.assert_allclose(nrm[c, f], -nrm[nb, nf], atol=1e-12)
+    # closed cells: sum of n A over the faces vanishes
+    mask = np.arange(6)[None, :] < g["nfaces"][:, None]
+    s = (nrm * (g["face_area"] * mask)[..., None]).sum(1)
+    assert np.abs(s).max() < 1e-13 * g["face_area"].max()
+
+
+def test_box_volume_and_periodic_pairing():
+    m = Mesh.box_tet(3, 3, 3, jitter=0.15, seed=11).prepare(SCHEME_WENO, 2)
+    g = m.geometry()
+    assert abs(g["volume"].sum() - L ** 3) < 1e-10 * L ** 3
+    assert (g["neigh"][:, :4] >= 0).all()  # periodic box: no boundary faces
+    # quadrature point pairing is an involution
+    for c in range(g["ncells"]):
+        for f in range(4):
+            nb, nf = g["neigh"][c, f], g["neigh_face"][c, f]
+            for q in range(3):
+                qq = g["qperm"][c, f, q]
+                assert g["qperm"][nb, nf, qq] == q
+
+
+def test_mixed_box_has_all_shapes():
+    m = Mesh.mixed_box(8, seed=5).prepare(SCHEME_MUSCL, 1)
+    g = m.geometry()
+    nf = np.bincount(g["nfaces"])
+    assert nf[4] > 0 and nf[5] > 0 and nf[6] > 0  # tets; pyramids+prisms; hexahedra
+    assert abs(g["volume"].sum() - L ** 3) < 1e-9 * L ** 3
+
+
+@pytest.mark.parametrize("kind,scheme,iorder,ees", [
+    ("hex", SCHEME_MUSCL, 1, 0), ("tet", SCHEME_WENO, 2, 0), ("hex12", SCHEME_WENO, 4, 0), ("tet", SCHEME_WENO, 3, 5)])
+def test_lsq_reproduces_linear_fields(kind, scheme, iorder, ees):
+    """invmat_stencilt recovers the exact coefficients of a linear field from
+    cell averages (LSQ exactness, prestore.f90:434-523)."""
+    mk = {"hex": lambda: Mesh.box_hex(8, 8, 8), "tet": lambda: Mesh.box_tet(4, 4, 4, seed=3),
+          "hex12": lambda: Mesh.box_hex(12, 12, 12)}[kind]
+    m = mk().prepare(scheme, iorder, ees)
+    g, r, c = m.geometry(), m.recon(), m.centres()
+    worst = 0.0
+    for i in range(g["ncells"]):
+        J = np.linalg.inv(g["invccjac"][i])
+        t = r["table_id"][i]
+        for ll in range(g["admis"][i]):
+            low = ees == 5 and ll > 0
+            M = r["invmat2"][t, ll] if low else r["invmat"][t, ll]
+            nk = M.shape[0]
+            st = r["stencil"][i, ll, 1:nk + 1]
+            d = c[st] - c[i]
+            d -= L * np.round(d / L)
+            for comp in range(3):
+                gg = M.T @ d[:, comp]
+                worst = max(worst, np.abs(gg[:3] - J[comp]).max(), np.abs(gg[3:]).max() if gg.size > 3 else 0.0)
+    assert worst < 1e-8
+
+
+def test_weno_stencils_admissible_and_shared_tables():
+    m = Mesh.box_hex(12, 12, 12).prepare(SCHEME_WENO, 4)
+    g, r = m.geometry(), m.recon()
+    assert (g["admis"] == 7).all() and (g["full"] == 1).all()
+    assert r["ntables"] == 1  # translation-invariant stencils share one matrix set
+    st = r["stencil"]
+    assert (st[:, :, 0] == np.arange(g["ncells"])[:, None]).all()
+    assert (st >= 0).all()
+    # indicator matrices are symmetric positive semi-definite
+    S = r["indicator"][0]
+    np.testing.assert_allclose(S, S.T, rtol=1e-12, atol=1e-12 * np.abs(S).max())
+    assert np.linalg.eigvalsh(S).min() > -1e-10 * np.abs(S).max()
+
+
+def test_initial_condition_averages():
+    m = Mesh.box_hex(16, 16, 16).prepare(SCHEME_MUSCL, 1)
+    U = m.initial_condition(95, [1.4, 100.0, 1.0])
+    g = m.geometry()
+    assert abs((U[:, 0] * g["volume"]).sum() - L ** 3) < 1e-9
+    # TGV momentum integrates to zero
+    assert np.abs((U[:, 1:4] * g["volume"][:, None]).sum(0)).max() < 1e-9

@@ -1,0 +1,65 @@
+"""In-tree build of the native libraries.
+
+    python -m ucns3d_b200.build
+
+* ``ucns3d_b200/lib/libucns3d_gpu.so``  - CUDA engine, sm_100a (nvcc)
+* ``ucns3d_b200/lib/libucns3d_prep.so`` - host set-up library (g++, OpenMP)
+
+nvcc cross-compiles for sm_100a without a GPU.  The libraries are built
+in-tree so that they travel with the source tree.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "lib")
+INC = os.path.join(ROOT, "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build_prep(force=False):
+    src = os.path.join(PKG, "csrc", "prep", "prep.cpp")
+    out = os.path.join(LIB, "libucns3d_prep.so")
+    deps = [src, os.path.join(INC, "ucns3d_prep.h"), os.path.join(INC, "ucns3d_gpu.h")]
+    if force or _stale(out, deps):
+        os.makedirs(LIB, exist_ok=True)
+        # the system g++ (the environment's CXX wrapper has no OpenMP runtime)
+        _run(["g++", "-O3", "-march=x86-64-v2", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-I", INC, src,
+              "-o", out])
+    return out
+
+
+def build_engine(force=False, extra=()):
+    d = os.path.join(PKG, "csrc", "engine")
+    srcs = [os.path.join(d, f) for f in ("engine.cu", "kernels.cuh", "device.cuh")] + [os.path.join(INC, "ucns3d_gpu.h")]
+    out = os.path.join(LIB, "libucns3d_gpu.so")
+    if force or _stale(out, srcs):
+        os.makedirs(LIB, exist_ok=True)
+        _run([NVCC, *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-shared", "-I", INC, *extra, os.path.join(d, "engine.cu"), "-o", out])
+    return out
+
+
+def build_all(force=False):
+    return build_prep(force), build_engine(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)

@@ -1,0 +1,52 @@
+"""Engine configuration (ucg_config) from UCNS3D.DAT-style parameters.
+
+Derived quantities follow src/parameters.f90: VISC = rho*U*L/Re
+(parameters.f90:1241), R_gas = 1 when the free-stream speed is below 10
+(parameters.f90:1223-1227), IORDER = spatialorder - 1 (parameters.f90:1276),
+the WENO epsilon 10E-12 (reconstruct_p.f90:437) and KAPPA_VEN = 10
+(reconstruct_p.f90:3436).
+"""
+from __future__ import annotations
+
+from . import _native as N
+
+NAVIER_STOKES = 1
+EULER = 2
+
+
+def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma: float = 1.4,
+                prandtl: float = 0.72, reynolds: float | None = None, rres: float = 1.0,
+                ufreestream: float = 1.0, pres: float = 1.0, char_length: float = 1.0,
+                lwci: float = 1000.0, wenoz: int = 0, limiter: int = 7,
+                bc_state=(1.0, 0.0, 0.0, 0.0, 1.0), lamx: float = 1.0) -> N.UcgConfig:
+    """A ucg_config for a prepared mesh.  ``reynolds`` sets VISC for
+    Navier-Stokes; ``bc_state`` is the free-stream primitive state used by
+    inflow/outflow boundaries."""
+    if not getattr(mesh, "prepared", False):
+        raise ValueError("mesh must be prepared first")
+    cfg = N.UcgConfig()
+    mesh.fill_config(cfg)
+    cfg.governing = governing
+    cfg.wenwrt = 1
+    cfg.limiter = limiter
+    cfg.riemann = 1
+    cfg.precision = precision
+    cfg.wenoz = wenoz
+    cfg.gamma = gamma
+    cfg.prandtl = prandtl
+    cfg.rres = rres
+    cfg.pres = pres
+    cfg.r_gas = 1.0 if ufreestream < 10.0 else 287.052874
+    if governing == NAVIER_STOKES:
+        if not reynolds:
+            raise ValueError("Navier-Stokes needs a Reynolds number")
+        cfg.visc = rres * ufreestream * char_length / reynolds
+    else:
+        cfg.visc = 0.0
+    cfg.lwci = lwci
+    cfg.weno_eps = 10e-12
+    cfg.kappa_ven = 10.0
+    cfg.lamx = lamx
+    for k in range(5):
+        cfg.bc_state[k] = bc_state[k]
+    return cfg

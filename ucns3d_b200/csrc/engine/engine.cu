@@ -1,0 +1,707 @@
+// C ABI of the engine (include/ucns3d_gpu.h): handle, uploads, stage
+// driver.  The stage sequence mirrors CALL_FLUX_SUBROUTINES_3D
+// (src/time_p.f90:2253-2497) and RUNGE_KUTTA3 (src/time_p.f90:885-1027).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "ucns3d_gpu.h"
+
+using namespace ucg;
+
+namespace {
+
+std::string g_create_err;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct ucg_engine {
+  ucg_config cfg;
+  int64_t n = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool mixed = false;
+  int QS = 1;
+  std::string err;
+  int64_t launches = 0;
+  int64_t bytes = 0;
+  bool have_geometry = false, have_state = false;
+  int64_t recon_cells = 0;
+  std::vector<DevBuf*> owned;
+  // geometry
+  DevBuf nfaces, ftype, neigh, nface, bc, qperm, rot, area, dih, vol, minedge, jinv, admis, full, qpts, bmean;
+  // tables
+  DevBuf sten, invmat, invmat2, ind, ind2;
+  // scratch and state
+  DevBuf dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging;
+  std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
+};
+
+namespace {
+
+int fail(ucg_engine* e, int code, const std::string& msg) {
+  if (e) e->err = msg;
+  return code;
+}
+
+int cuda_fail(ucg_engine* e, cudaError_t st, const char* where) {
+  return fail(e, UCG_ECUDA, std::string(where) + ": " + cudaGetErrorString(st));
+}
+
+#define CK(call)                                               \
+  do {                                                         \
+    cudaError_t st_ = (call);                                  \
+    if (st_ != cudaSuccess) return cuda_fail(e, st_, #call);   \
+  } while (0)
+
+int alloc(ucg_engine* e, DevBuf& b, size_t bytes) {
+  if (b.p && b.bytes >= bytes) return UCG_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    e->bytes -= (int64_t)b.bytes;
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  if (bytes == 0) return UCG_OK;
+  cudaError_t st = cudaMalloc(&b.p, bytes);
+  if (st != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e, UCG_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(st));
+  }
+  b.bytes = bytes;
+  e->bytes += (int64_t)bytes;
+  return UCG_OK;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+size_t tsize(const ucg_engine* e) { return e->mixed ? sizeof(float) : sizeof(double); }
+
+template <typename H>
+int upload(ucg_engine* e, DevBuf& b, const std::vector<H>& h) {
+  int rc = alloc(e, b, h.size() * sizeof(H));
+  if (rc) return rc;
+  if (!h.empty()) CK(cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(H), cudaMemcpyHostToDevice, e->stream));
+  return UCG_OK;
+}
+
+Problem make_problem(ucg_engine* e) {
+  Problem p;
+  std::memset(&p, 0, sizeof(p));
+  const ucg_config& c = e->cfg;
+  p.n = e->n;
+  p.iorder = c.iorder;
+  p.ideg = c.ideg;
+  p.imax = c.imax;
+  p.admis_max = c.admis_max;
+  p.ideg2 = c.ideg2;
+  p.imax2 = c.imax2;
+  p.ees = c.ees;
+  p.scheme = c.scheme;
+  p.governing = c.governing;
+  p.wenoz = c.wenoz;
+  p.nq_quad = c.nq_quad;
+  p.nq_tri = c.nq_tri;
+  p.gamma = c.gamma;
+  p.prandtl = c.prandtl;
+  p.visc = c.visc;
+  p.r_gas = c.r_gas;
+  p.pres = c.pres;
+  p.rres = c.rres;
+  p.lwci = c.lwci;
+  p.weno_eps = c.weno_eps;
+  p.kappa_ven = c.kappa_ven;
+  p.lamx = c.lamx;
+  for (int q = 0; q < MQ; ++q) {
+    p.quad_w[q] = c.quad_w[q];
+    p.tri_w[q] = c.tri_w[q];
+  }
+  for (int v = 0; v < NV; ++v) p.bc_state[v] = c.bc_state[v];
+  p.nfaces = (const int8_t*)e->nfaces.p;
+  p.ftype = (const int8_t*)e->ftype.p;
+  p.neigh = (const int32_t*)e->neigh.p;
+  p.nface = (const int8_t*)e->nface.p;
+  p.bc = (const int8_t*)e->bc.p;
+  p.qperm = (const uint8_t*)e->qperm.p;
+  p.rot = (const double*)e->rot.p;
+  p.area = (const double*)e->area.p;
+  p.dih = (const double*)e->dih.p;
+  p.vol = (const double*)e->vol.p;
+  p.minedge = (const double*)e->minedge.p;
+  p.jinv = (const double*)e->jinv.p;
+  p.admis = (const int8_t*)e->admis.p;
+  p.full = (const int8_t*)e->full.p;
+  p.qpts = e->qpts.p;
+  p.bmean = e->bmean.p;
+  p.sten = (const int32_t*)e->sten.p;
+  p.invmat = e->invmat.p;
+  p.invmat2 = e->invmat2.p;
+  p.ind = e->ind.p;
+  p.ind2 = e->ind2.p;
+  p.dul = e->dul.p;
+  p.ulv = (double*)e->ulv.p;
+  p.gv = (double*)e->gv.p;
+  p.rhs = (double*)e->rhs.p;
+  p.health = (unsigned*)e->health.p;
+  p.dt_dev = nullptr;
+  return p;
+}
+
+bool ready(ucg_engine* e) { return e->have_geometry && e->recon_cells == e->n; }
+
+// ------------------------------------------------------------ launching
+template <int P, typename T>
+int launch_weno(ucg_engine* e, const Problem& p, const double* U) {
+  const ucg_config& c = e->cfg;
+  const bool cw = c.ees == 5;
+  int cpc = 256 / (c.admis_max * c.ideg);
+  if (cpc < 1) cpc = 1;
+  if (cpc > 16) cpc = 16;
+  WenoSmem L = weno_smem_layout<T>(cpc, c.admis_max, c.imax, c.ideg, c.ideg2, e->QS, cw);
+  while (cpc > 1 && L.total > 100 * 1024) {
+    --cpc;
+    L = weno_smem_layout<T>(cpc, c.admis_max, c.imax, c.ideg, c.ideg2, e->QS, cw);
+  }
+  if (L.total > 200 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
+  CK(cudaFuncSetAttribute(k_weno<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total));
+  int64_t blocks = (e->n + cpc - 1) / cpc;
+  k_weno<P, T><<<(unsigned)blocks, 256, L.total, e->stream>>>(p, U, cpc);
+  e->launches++;
+  if (c.governing == 1) {
+    k_visc_lsq<P, T><<<(unsigned)((e->n * 4 + 127) / 128), 128, 0, e->stream>>>(p, U);
+    int64_t nf = e->n * MF * e->QS;
+    k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, e->stream>>>(p);
+    e->launches += 2;
+  }
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+template <typename T>
+int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
+  const ucg_config& c = e->cfg;
+  if (c.scheme == 2 && c.iorder == 1) {
+    unsigned blocks = (unsigned)((e->n + 127) / 128);
+    if (c.governing == 1) k_muscl<T, true><<<blocks, 128, 0, e->stream>>>(p, U);
+    else k_muscl<T, false><<<blocks, 128, 0, e->stream>>>(p, U);
+    e->launches++;
+    CK(cudaGetLastError());
+    return UCG_OK;
+  }
+  switch (c.iorder) {
+    case 1: return launch_weno<1, T>(e, p, U);
+    case 2: return launch_weno<2, T>(e, p, U);
+    case 3: return launch_weno<3, T>(e, p, U);
+    case 4: return launch_weno<4, T>(e, p, U);
+  }
+  return fail(e, UCG_EINVAL, "iorder out of range");
+}
+
+int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
+  return e->mixed ? launch_recon_t<float>(e, p, U) : launch_recon_t<double>(e, p, U);
+}
+
+template <typename T, bool NS>
+int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
+                  double dt) {
+  int64_t threads = e->n * 8;
+  unsigned blocks = (unsigned)((threads + 255) / 256);
+  switch (mode) {
+    case 0: k_flux<T, NS, 0><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 1: k_flux<T, NS, 1><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 2: k_flux<T, NS, 2><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    default: k_flux<T, NS, 3><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+  }
+  e->launches++;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int launch_flux(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo, double dt) {
+  bool ns = e->cfg.governing == 1;
+  if (e->mixed) return ns ? launch_flux_t<float, true>(e, p, mode, Uc, Un, Uo, dt) : launch_flux_t<float, false>(e, p, mode, Uc, Un, Uo, dt);
+  return ns ? launch_flux_t<double, true>(e, p, mode, Uc, Un, Uo, dt) : launch_flux_t<double, false>(e, p, mode, Uc, Un, Uo, dt);
+}
+
+// one RUNGE_KUTTA3 step; dt from the host value or, if dt_dev, from device memory
+int rk3(ucg_engine* e, double dt, bool dt_dev) {
+  Problem p = make_problem(e);
+  if (dt_dev) p.dt_dev = (double*)e->dt.p;
+  double* Un = (double*)e->Un.p;
+  double* Ua = (double*)e->Ua.p;
+  double* Ub = (double*)e->Ub.p;
+  int rc;
+  if ((rc = launch_recon(e, p, Un))) return rc;
+  if ((rc = launch_flux(e, p, 1, Un, Un, Ua, dt))) return rc;
+  if ((rc = launch_recon(e, p, Ua))) return rc;
+  if ((rc = launch_flux(e, p, 2, Ua, Un, Ub, dt))) return rc;
+  if ((rc = launch_recon(e, p, Ub))) return rc;
+  if ((rc = launch_flux(e, p, 3, Ub, Un, Un, dt))) return rc;
+  return UCG_OK;
+}
+
+int cfl_device(ucg_engine* e, double cfl) {
+  Problem p = make_problem(e);
+  k_dt_init<<<1, 1, 0, e->stream>>>((double*)e->dt.p);
+  k_cfl<<<(unsigned)((e->n + 255) / 256), 256, 0, e->stream>>>(p, (const double*)e->Un.p, cfl / 3.0, (double*)e->dt.p);
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+}  // namespace
+
+// =================================================================== ABI
+extern "C" {
+
+const char* ucg_create_error(void) { return g_create_err.c_str(); }
+
+int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** out) {
+  g_create_err.clear();
+  if (!cfg || !out || ncells <= 0) {
+    g_create_err = "null argument or ncells <= 0";
+    return UCG_EINVAL;
+  }
+  *out = nullptr;
+  const ucg_config& c = *cfg;
+  bool okscheme = (c.scheme == 2 || c.scheme == 3) && c.iorder >= 1 && c.iorder <= 4 && (c.ees == 0 || c.ees == 5) &&
+                  (c.governing == 1 || c.governing == 2) && (c.precision == UCG_FP64 || c.precision == UCG_MIXED);
+  int ideg = (c.iorder + 1) * (c.iorder + 2) * (c.iorder + 3) / 6 - 1;
+  if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
+      c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && (c.ideg2 < 1 || c.imax2 < c.ideg2)) ||
+      c.gamma <= 1.0 || c.limiter != 7 || c.riemann != 1 || c.wenwrt != 1) {
+    g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC, limiter 7, "
+                   "conserved-variable WENO)";
+    return UCG_EINVAL;
+  }
+  if (c.scheme == 2 && c.admis_max != 1) {
+    g_create_err = "MUSCL uses one stencil (admis_max 1)";
+    return UCG_EINVAL;
+  }
+  int ndev = 0;
+  cudaError_t st = cudaGetDeviceCount(&ndev);
+  if (st != cudaSuccess || ndev <= device || device < 0) {
+    g_create_err = std::string("no usable CUDA device: ") + (st != cudaSuccess ? cudaGetErrorString(st) : "index out of range");
+    return UCG_ECUDA;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major < 10) {
+    g_create_err = "the engine is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor);
+    return UCG_ECUDA;
+  }
+  auto* e = new ucg_engine;
+  e->cfg = c;
+  e->n = ncells;
+  e->device = device;
+  e->mixed = c.precision == UCG_MIXED;
+  e->QS = c.nq_quad > c.nq_tri ? c.nq_quad : c.nq_tri;
+  cudaSetDevice(device);
+  st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (st != cudaSuccess) {
+    g_create_err = std::string("cudaStreamCreate: ") + cudaGetErrorString(st);
+    delete e;
+    return UCG_ECUDA;
+  }
+  const int64_t n = ncells;
+  int rc = UCG_OK;
+  const size_t T = tsize(e);
+  rc = rc ? rc : alloc(e, e->Un, n * NV * 8);
+  rc = rc ? rc : alloc(e, e->Ua, n * NV * 8);
+  rc = rc ? rc : alloc(e, e->Ub, n * NV * 8);
+  rc = rc ? rc : alloc(e, e->rhs, n * NV * 8);
+  rc = rc ? rc : alloc(e, e->dul, (size_t)n * MF * e->QS * NV * T);
+  if (c.governing == 1) {
+    rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
+    rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
+  }
+  rc = rc ? rc : alloc(e, e->health, 64);
+  rc = rc ? rc : alloc(e, e->dt, 64);
+  rc = rc ? rc : alloc(e, e->partial, ((n + 255) / 256 + 1) * 8);
+  rc = rc ? rc : alloc(e, e->red, 64);
+  if (rc) {
+    g_create_err = e->err;
+    ucg_destroy(e);
+    return rc;
+  }
+  cudaMemsetAsync(e->health.p, 0, 64, e->stream);
+  cudaMemsetAsync(e->dul.p, 0, e->dul.bytes, e->stream);
+  if (e->ulv.p) cudaMemsetAsync(e->ulv.p, 0, e->ulv.bytes, e->stream);
+  e->recon_done.assign(n, 0);
+  *out = e;
+  return UCG_OK;
+}
+
+void ucg_destroy(ucg_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
+                   &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
+                   &e->invmat2, &e->ind, &e->ind2, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
+                   &e->health, &e->dt, &e->partial, &e->red, &e->staging};
+  for (DevBuf* b : all) release(*b);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
+  if (!e || !g) return fail(e, UCG_EINVAL, "null argument");
+  if (g->ncells != e->n) return fail(e, UCG_EINVAL, "geometry has " + std::to_string(g->ncells) + " cells, engine " + std::to_string(e->n));
+  if (!g->nfaces || !g->face_type || !g->neigh || !g->neigh_face || !g->bc || !g->qperm || !g->face_angle ||
+      !g->face_area || !g->dih || !g->qpoints || !g->volume || !g->minedge || !g->invccjac || !g->basis_mean ||
+      !g->admis || !g->full)
+    return fail(e, UCG_EINVAL, "a geometry array is NULL");
+  cudaSetDevice(e->device);
+  const int64_t n = e->n;
+  const int QS = e->QS, ideg = e->cfg.ideg;
+  const bool ns = e->cfg.governing == 1;
+  std::vector<int8_t> nfaces(n), ftype(n * MF), nface(n * MF), bc(n * MF), admis(n), full(n);
+  std::vector<int32_t> neigh(n * MF);
+  std::vector<uint8_t> qperm((size_t)n * MF * QS);
+  std::vector<double> rot((size_t)n * MF * 4), area(n * MF), dih(n * MF), vol(n), minedge(n), jinv(n * 9);
+  for (int64_t c = 0; c < n; ++c) {
+    int nf = g->nfaces[c];
+    if (nf < 4 || nf > MF) return fail(e, UCG_EINVAL, "cell " + std::to_string(c) + " has " + std::to_string(nf) + " faces");
+    if (!(g->volume[c] > 0.0)) return fail(e, UCG_EINVAL, "non-positive cell volume at cell " + std::to_string(c));
+    int adm = g->admis[c];
+    if (adm < 1 || adm > e->cfg.admis_max) return fail(e, UCG_EINVAL, "ADMIS out of range at cell " + std::to_string(c));
+    nfaces[c] = (int8_t)nf;
+    admis[c] = (int8_t)adm;
+    full[c] = (int8_t)(g->full[c] ? 1 : 0);
+    vol[c] = g->volume[c];
+    minedge[c] = g->minedge[c];
+    for (int k = 0; k < 9; ++k) jinv[c * 9 + k] = g->invccjac[c * 9 + k];
+    for (int f = 0; f < MF; ++f) {
+      int64_t i = c * MF + f;
+      ftype[i] = (int8_t)g->face_type[i];
+      neigh[i] = f < nf ? g->neigh[i] : -1;
+      nface[i] = (int8_t)(f < nf ? g->neigh_face[i] : -1);
+      bc[i] = (int8_t)(f < nf ? g->bc[i] : 0);
+      area[i] = g->face_area[i];
+      dih[i] = g->dih[i];
+      double a1 = g->face_angle[i * 2], a2 = g->face_angle[i * 2 + 1];
+      rot[i * 4 + 0] = cos(a1);
+      rot[i * 4 + 1] = sin(a1);
+      rot[i * 4 + 2] = cos(a2);
+      rot[i * 4 + 3] = sin(a2);
+      if (f < nf) {
+        int ft = g->face_type[i];
+        if (ft != 5 && ft != 6) return fail(e, UCG_EINVAL, "face type must be 5 or 6");
+        int64_t nb = g->neigh[i];
+        if (nb >= n || nb < -1) return fail(e, UCG_EINVAL, "neighbour index out of range at cell " + std::to_string(c));
+        if (nb >= 0 && (g->neigh_face[i] < 0 || g->neigh_face[i] >= MF))
+          return fail(e, UCG_EINVAL, "neighbour face out of range at cell " + std::to_string(c));
+        if (nb < 0) {
+          int code = g->bc[i];
+          if (ns) return fail(e, UCG_EINVAL, "Navier-Stokes with physical boundary faces is not supported");
+          if (code != 1 && code != 2 && code != 3 && code != 4 && code != 6)
+            return fail(e, UCG_EINVAL, "unsupported boundary code " + std::to_string(code));
+        }
+        int nq = ft == 5 ? e->cfg.nq_quad : e->cfg.nq_tri;
+        for (int q = 0; q < QS; ++q) {
+          int qq = q < nq ? g->qperm[i * UCG_MAX_QP + q] : 0;
+          if (qq < 0 || qq >= nq) return fail(e, UCG_EINVAL, "qperm out of range at cell " + std::to_string(c));
+          qperm[(size_t)i * QS + q] = (uint8_t)qq;
+        }
+      }
+    }
+  }
+  int rc = UCG_OK;
+  rc = rc ? rc : upload(e, e->nfaces, nfaces);
+  rc = rc ? rc : upload(e, e->ftype, ftype);
+  rc = rc ? rc : upload(e, e->neigh, neigh);
+  rc = rc ? rc : upload(e, e->nface, nface);
+  rc = rc ? rc : upload(e, e->bc, bc);
+  rc = rc ? rc : upload(e, e->qperm, qperm);
+  rc = rc ? rc : upload(e, e->rot, rot);
+  rc = rc ? rc : upload(e, e->area, area);
+  rc = rc ? rc : upload(e, e->dih, dih);
+  rc = rc ? rc : upload(e, e->vol, vol);
+  rc = rc ? rc : upload(e, e->minedge, minedge);
+  rc = rc ? rc : upload(e, e->jinv, jinv);
+  rc = rc ? rc : upload(e, e->admis, admis);
+  rc = rc ? rc : upload(e, e->full, full);
+  if (rc) return rc;
+  // reference-frame quadrature points and basis means, in table precision
+  std::vector<double> qp((size_t)n * MF * QS * 3, 0.0), bm((size_t)n * ideg);
+  for (int64_t c = 0; c < n; ++c) {
+    for (int f = 0; f < MF; ++f)
+      for (int q = 0; q < QS; ++q)
+        for (int k = 0; k < 3; ++k)
+          qp[(((size_t)c * MF + f) * QS + q) * 3 + k] = g->qpoints[((c * MF + f) * UCG_MAX_QP + q) * 3 + k];
+    for (int d = 0; d < ideg; ++d) bm[(size_t)c * ideg + d] = g->basis_mean[(size_t)c * ideg + d];
+  }
+  if (e->mixed) {
+    std::vector<float> qf(qp.begin(), qp.end()), bf(bm.begin(), bm.end());
+    rc = rc ? rc : upload(e, e->qpts, qf);
+    rc = rc ? rc : upload(e, e->bmean, bf);
+  } else {
+    rc = rc ? rc : upload(e, e->qpts, qp);
+    rc = rc ? rc : upload(e, e->bmean, bm);
+  }
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  e->have_geometry = true;
+  return UCG_OK;
+}
+
+int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
+  if (!e || !r) return fail(e, UCG_EINVAL, "null argument");
+  const ucg_config& c = e->cfg;
+  if (r->first < 0 || r->count <= 0 || r->first + r->count > e->n) return fail(e, UCG_EINVAL, "cell range out of bounds");
+  if (!r->stencil || !r->invmat) return fail(e, UCG_EINVAL, "stencil and invmat are required");
+  const bool weno = c.scheme == 3, cw = c.ees == 5;
+  if (weno && !r->indicator) return fail(e, UCG_EINVAL, "WENO needs the INDICATOR matrices");
+  if (cw && (!r->invmat2 || !r->indicator2)) return fail(e, UCG_EINVAL, "CWENO needs invmat2 and INDICATORC");
+  cudaSetDevice(e->device);
+  const int64_t n = e->n, first = r->first, count = r->count;
+  const int A = c.admis_max, W = c.imax + 1;
+  const int64_t ntab = r->table_id ? r->ntables : count;
+  if (r->table_id) {
+    if (ntab <= 0) return fail(e, UCG_EINVAL, "ntables must be positive with table_id");
+    for (int64_t i = 0; i < count; ++i)
+      if (r->table_id[i] < 0 || r->table_id[i] >= ntab) return fail(e, UCG_EINVAL, "table_id out of range");
+  }
+  // stencils (validated; slot 0 must be the cell itself)
+  for (int64_t i = 0; i < count; ++i) {
+    int64_t cell = first + i;
+    for (int ll = 0; ll < A; ++ll)
+      for (int k = 0; k < W; ++k) {
+        int32_t y = r->stencil[(i * A + ll) * W + k];
+        if (y >= n || y < -1) return fail(e, UCG_EINVAL, "stencil index out of range at cell " + std::to_string(cell));
+      }
+    if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
+  }
+  const size_t T = tsize(e);
+  int rc = UCG_OK;
+  rc = rc ? rc : alloc(e, e->sten, (size_t)n * A * W * 4);
+  const int64_t lmat = (int64_t)A * c.imax * c.ideg, lmat2 = cw ? (int64_t)A * c.imax2 * c.ideg2 : 0;
+  const int64_t lind = weno ? (int64_t)c.ideg * c.ideg : 0, lind2 = cw ? (int64_t)c.ideg2 * c.ideg2 : 0;
+  rc = rc ? rc : alloc(e, e->invmat, (size_t)n * lmat * T);
+  if (cw) rc = rc ? rc : alloc(e, e->invmat2, (size_t)n * lmat2 * T);
+  if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)n * lind * T);
+  if (cw) rc = rc ? rc : alloc(e, e->ind2, (size_t)n * lind2 * T);
+  if (rc) return rc;
+  // any cell referenced by a stencil must exist; then copy the stencil rows
+  CK(cudaMemcpyAsync((char*)e->sten.p + (size_t)first * A * W * 4, r->stencil, (size_t)count * A * W * 4,
+                     cudaMemcpyHostToDevice, e->stream));
+  // matrices: staged in chunks of tables, expanded per cell on the device
+  int32_t* d_tid = nullptr;
+  DevBuf tidbuf;
+  if (r->table_id) {
+    CK(cudaMalloc(&tidbuf.p, count * 4));
+    CK(cudaMemcpyAsync(tidbuf.p, r->table_id, count * 4, cudaMemcpyHostToDevice, e->stream));
+    d_tid = (int32_t*)tidbuf.p;
+  }
+  struct Part {
+    const double* src;
+    int64_t len;
+    DevBuf* dst;
+  } parts[4] = {{r->invmat, lmat, &e->invmat}, {r->invmat2, lmat2, &e->invmat2}, {r->indicator, lind, &e->ind},
+                {r->indicator2, lind2, &e->ind2}};
+  const size_t stage_bytes = (size_t)1 << 30;
+  for (auto& pt : parts) {
+    if (pt.len == 0) continue;
+    int64_t per = (int64_t)(stage_bytes / (pt.len * 8));
+    if (per < 1) per = 1;
+    for (int64_t t0 = 0; t0 < ntab; t0 += per) {
+      int64_t t1 = t0 + per < ntab ? t0 + per : ntab;
+      size_t bytes = (size_t)(t1 - t0) * pt.len * 8;
+      rc = alloc(e, e->staging, bytes);
+      if (rc) {
+        if (tidbuf.p) cudaFree(tidbuf.p);
+        return rc;
+      }
+      CK(cudaMemcpyAsync(e->staging.p, pt.src + t0 * pt.len, bytes, cudaMemcpyHostToDevice, e->stream));
+      int64_t total = count * pt.len;
+      unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
+      if (e->mixed)
+        k_expand<float><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, (const double*)e->staging.p, d_tid, first,
+                                                      count, pt.len, t0, t1);
+      else
+        k_expand<double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, (const double*)e->staging.p, d_tid, first,
+                                                       count, pt.len, t0, t1);
+      e->launches++;
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(e->stream));
+    }
+  }
+  if (tidbuf.p) cudaFree(tidbuf.p);
+  e->bytes -= (int64_t)e->staging.bytes;
+  release(e->staging);
+  CK(cudaStreamSynchronize(e->stream));
+  int64_t newly = 0;
+  for (int64_t i = 0; i < count; ++i)
+    if (!e->recon_done[first + i]) {
+      e->recon_done[first + i] = 1;
+      ++newly;
+    }
+  e->recon_cells += newly;
+  return UCG_OK;
+}
+
+int ucg_set_state(ucg_engine* e, const double* u, int64_t n) {
+  if (!e || !u) return fail(e, UCG_EINVAL, "null argument");
+  if (n != e->n) return fail(e, UCG_EINVAL, "state size mismatch");
+  cudaSetDevice(e->device);
+  CK(cudaMemcpyAsync(e->Un.p, u, n * NV * 8, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->have_state = true;
+  return UCG_OK;
+}
+
+int ucg_get_state(ucg_engine* e, double* u, int64_t n) {
+  if (!e || !u) return fail(e, UCG_EINVAL, "null argument");
+  if (n != e->n) return fail(e, UCG_EINVAL, "state size mismatch");
+  if (!e->have_state) return fail(e, UCG_ESTATE, "no state set");
+  cudaSetDevice(e->device);
+  CK(cudaMemcpyAsync(u, e->Un.p, n * NV * 8, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_compute_dt(ucg_engine* e, double cfl, double* dt) {
+  if (!e || !dt || !(cfl > 0)) return fail(e, UCG_EINVAL, "bad argument");
+  if (!e->have_geometry || !e->have_state) return fail(e, UCG_ESTATE, "geometry and state are needed");
+  cudaSetDevice(e->device);
+  int rc = cfl_device(e, cfl);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(dt, e->dt.p, 8, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_residual(ucg_engine* e, double* rhs) {
+  if (!e) return fail(e, UCG_EINVAL, "null argument");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  int rc = launch_recon(e, p, (const double*)e->Un.p);
+  if (rc) return rc;
+  rc = launch_flux(e, p, 0, (const double*)e->Un.p, (const double*)e->Un.p, nullptr, 0.0);
+  if (rc) return rc;
+  if (rhs) {
+    CK(cudaMemcpyAsync(rhs, e->rhs.p, e->n * NV * 8, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  }
+  return UCG_OK;
+}
+
+int ucg_rk3_step(ucg_engine* e, double dt) {
+  if (!e || !(dt > 0)) return fail(e, UCG_EINVAL, "bad argument");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  cudaSetDevice(e->device);
+  return rk3(e, dt, false);
+}
+
+int ucg_step(ucg_engine* e, double cfl, int32_t nsteps) {
+  if (!e || !(cfl > 0) || nsteps < 0) return fail(e, UCG_EINVAL, "bad argument");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  cudaSetDevice(e->device);
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = cfl_device(e, cfl);
+    if (rc) return rc;
+    rc = rk3(e, 0.0, true);
+    if (rc) return rc;
+  }
+  return UCG_OK;
+}
+
+int ucg_last_dt(ucg_engine* e, double* dt) {
+  if (!e || !dt) return fail(e, UCG_EINVAL, "null argument");
+  cudaSetDevice(e->device);
+  CK(cudaMemcpyAsync(dt, e->dt.p, 8, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_reduce(ucg_engine* e, int32_t what, double* out) {
+  if (!e || !out || what < 1 || what > 3) return fail(e, UCG_EINVAL, "bad argument");
+  if (!e->have_geometry || !e->have_state) return fail(e, UCG_ESTATE, "geometry and state are needed");
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  int64_t nb = (e->n + 255) / 256;
+  k_reduce_partial<<<(unsigned)nb, 256, 0, e->stream>>>(p, (const double*)e->Un.p, what, (double*)e->partial.p);
+  k_reduce_final<<<1, 1024, 0, e->stream>>>((const double*)e->partial.p, nb, (double*)e->red.p);
+  e->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, e->red.p, 8, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_check_health(ucg_engine* e) {
+  if (!e) return UCG_EINVAL;
+  cudaSetDevice(e->device);
+  unsigned h = 0;
+  CK(cudaMemcpyAsync(&h, e->health.p, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaMemsetAsync(e->health.p, 0, sizeof(unsigned), e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (h & HEALTH_NONPHYS) return fail(e, UCG_ENONPHYS, "a stage produced NaN or non-positive density/pressure");
+  return UCG_OK;
+}
+
+int ucg_synchronize(ucg_engine* e) {
+  if (!e) return UCG_EINVAL;
+  cudaSetDevice(e->device);
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
+  if (!e || !ms || reps < 1) return fail(e, UCG_EINVAL, "bad argument");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  cudaEvent_t ev[4];
+  for (auto& x : ev) CK(cudaEventCreate(&x));
+  double acc[3] = {0, 0, 0};
+  int rc = UCG_OK;
+  for (int r = 0; r < reps && !rc; ++r) {
+    cudaEventRecord(ev[0], e->stream);
+    rc = launch_recon(e, p, (const double*)e->Un.p);
+    cudaEventRecord(ev[1], e->stream);
+    if (!rc) rc = launch_flux(e, p, 0, (const double*)e->Un.p, (const double*)e->Un.p, nullptr, 0.0);
+    cudaEventRecord(ev[2], e->stream);
+    if (!rc) rc = cfl_device(e, 0.5);
+    cudaEventRecord(ev[3], e->stream);
+    cudaEventSynchronize(ev[3]);
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / reps;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+void* ucg_get_stream(ucg_engine* e) { return e ? (void*)e->stream : nullptr; }
+int64_t ucg_launch_count(const ucg_engine* e) { return e ? e->launches : 0; }
+int64_t ucg_device_bytes(const ucg_engine* e) { return e ? e->bytes : 0; }
+
+int ucg_last_error(const ucg_engine* e, char* buf, int32_t len) {
+  if (!e || !buf || len <= 0) return UCG_EINVAL;
+  std::snprintf(buf, (size_t)len, "%s", e->err.c_str());
+  return UCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+"""Host-side mirror of UCNS3D's explicit time-stepping interface over the
+CUDA engine's C ABI (include/ucns3d_gpu.h).
+
+Method names follow the Fortran routines they replace:
+
+    calculate_cfl(cfl)            CALCULATE_CFL             src/time_p.f90:27-191
+    call_flux_subroutines_3d()    CALL_FLUX_SUBROUTINES_3D  src/time_p.f90:2253-2497
+    runge_kutta3(dt)              RUNGE_KUTTA3              src/time_p.f90:885-1027
+    time_marching(nsteps, cfl)    the CFL + RK3 part of TIME_MARCHING (src/time_p.f90:4026)
+
+Errors come back as ``EngineError`` carrying the UCG_* code; there is no CPU
+fallback: creating an Engine without a B200 raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{N.ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Engine:
+    def __init__(self, mesh, cfg: N.UcgConfig, device: int = 0, upload: bool = True):
+        self.lib = N.engine()
+        self.mesh = mesh
+        self.cfg = cfg
+        self.n = mesh.ncells
+        h = C.c_void_p()
+        rc = self.lib.ucg_create(C.byref(cfg), self.n, device, C.byref(h))
+        if rc:
+            raise EngineError(rc, self.lib.ucg_create_error().decode())
+        self._h = h
+        if upload:
+            self.upload_geometry(mesh.geometry_struct())
+            self.upload_recon(mesh.recon_struct())
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self.lib.ucg_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc:
+            buf = C.create_string_buffer(1024)
+            self.lib.ucg_last_error(self._h, buf, 1024)
+            raise EngineError(rc, buf.value.decode())
+
+    # ------------------------------------------------------------ set-up
+    def upload_geometry(self, g: N.UcgGeometry):
+        self._check(self.lib.ucg_upload_geometry(self._h, C.byref(g)))
+
+    def upload_recon(self, r: N.UcgRecon):
+        self._check(self.lib.ucg_upload_recon(self._h, C.byref(r)))
+
+    # ------------------------------------------------------------- state
+    def set_state(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (self.n, 5):
+            raise ValueError(f"state must have shape ({self.n}, 5)")
+        self._check(self.lib.ucg_set_state(self._h, N.ptr(U, C.c_double), self.n))
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.n, 5))
+        self._check(self.lib.ucg_get_state(self._h, N.ptr(out, C.c_double), self.n))
+        return out
+
+    # ----------------------------------------------------------- stepping
+    def calculate_cfl(self, cfl: float) -> float:
+        dt = C.c_double()
+        self._check(self.lib.ucg_compute_dt(self._h, cfl, C.byref(dt)))
+        return dt.value
+
+    def call_flux_subroutines_3d(self) -> np.ndarray:
+        """RHS(I)%VAL of the current state, shape (n, 5)."""
+        out = np.empty((self.n, 5))
+        self._check(self.lib.ucg_residual(self._h, N.ptr(out, C.c_double)))
+        return out
+
+    residual = call_flux_subroutines_3d
+
+    def runge_kutta3(self, dt: float):
+        self._check(self.lib.ucg_rk3_step(self._h, dt))
+
+    def time_marching(self, nsteps: int, cfl: float):
+        """nsteps of CALCULATE_CFL + RUNGE_KUTTA3 with dt kept on the device."""
+        self._check(self.lib.ucg_step(self._h, cfl, nsteps))
+
+    def last_dt(self) -> float:
+        dt = C.c_double()
+        self._check(self.lib.ucg_last_dt(self._h, C.byref(dt)))
+        return dt.value
+
+    def reduce(self, what: int) -> float:
+        out = C.c_double()
+        self._check(self.lib.ucg_reduce(self._h, what, C.byref(out)))
+        return out.value
+
+    def kinetic_energy(self) -> float:
+        return self.reduce(N.UCG_REDUCE_KE)
+
+    def time_kernels(self, reps: int = 5) -> dict:
+        """Average device ms of the reconstruction, flux and time-step
+        kernels (CUDA events on the engine stream)."""
+        ms = (C.c_double * 3)()
+        self._check(self.lib.ucg_time_kernels(self._h, reps, ms))
+        return dict(recon=ms[0], flux=ms[1], cfl=ms[2])
+
+    def check_health(self):
+        self._check(self.lib.ucg_check_health(self._h))
+
+    def synchronize(self):
+        self._check(self.lib.ucg_synchronize(self._h))
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.ucg_get_stream(self._h) or 0)
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.ucg_launch_count(self._h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.ucg_device_bytes(self._h))

@@ -1,0 +1,177 @@
+"""Synthetic meshes and their set-up tables (wrapper of libucns3d_prep).
+
+UCNS3D builds these tables in its Fortran set-up (src/main.f90:151-767); a
+driver that keeps that set-up passes its own tables to the engine.  This
+module is the standalone path: seeded synthetic meshes for the benchmark and
+the tests, with geometry, stencils, pseudo-inverses and smoothness matrices
+computed in FP64 on the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+SCHEME_MUSCL = 2
+SCHEME_WENO = 3
+
+IC_TGV = 95
+IC_VORTEX = 201
+IC_UNIFORM = 1
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = N.prep().ucp_last_error().decode()
+        raise RuntimeError(f"{what} failed ({N.ERROR_NAMES.get(rc, rc)}): {msg}")
+
+
+class Mesh:
+    """A mesh owned by the set-up library.  Build with one of the class
+    methods, then ``prepare`` it for a scheme."""
+
+    def __init__(self, handle, kind: str, params: dict):
+        if not handle:
+            raise RuntimeError("mesh construction failed: " + N.prep().ucp_last_error().decode())
+        self._h = C.c_void_p(handle)
+        self.kind = kind
+        self.params = params
+        self.prepared = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            N.prep().ucp_free(h)
+            self._h = None
+
+    # -------------------------------------------------------- constructors
+    @classmethod
+    def box_hex(cls, nx, ny, nz, L=(2 * np.pi,) * 3, origin=(0.0, 0.0, 0.0), periodic=(1, 1, 1),
+                bc=(0, 0, 0, 0, 0, 0)):
+        Ls = (C.c_double * 3)(*L)
+        o = (C.c_double * 3)(*origin)
+        p = (C.c_int32 * 3)(*periodic)
+        b = (C.c_int32 * 6)(*bc)
+        h = N.prep().ucp_box_hex(nx, ny, nz, Ls, o, p, b)
+        return cls(h, "box_hex", dict(n=(nx, ny, nz), L=tuple(L), periodic=tuple(periodic)))
+
+    @classmethod
+    def box_tet(cls, nx, ny, nz, L=(2 * np.pi,) * 3, origin=(0.0, 0.0, 0.0), periodic=(1, 1, 1),
+                bc=(0, 0, 0, 0, 0, 0), jitter=0.15, seed=1234):
+        Ls = (C.c_double * 3)(*L)
+        o = (C.c_double * 3)(*origin)
+        p = (C.c_int32 * 3)(*periodic)
+        b = (C.c_int32 * 6)(*bc)
+        h = N.prep().ucp_box_tet(nx, ny, nz, Ls, o, p, b, float(jitter), int(seed))
+        return cls(h, "box_tet", dict(n=(nx, ny, nz), L=tuple(L), periodic=tuple(periodic),
+                                      jitter=jitter, seed=seed))
+
+    @classmethod
+    def bump_channel(cls, nx=240, ny=80, nlayers=4, bump=0.1, dz=None, split_frac=0.5, seed=1234):
+        dz = (1.0 / ny) if dz is None else dz
+        h = N.prep().ucp_bump_channel(nx, ny, nlayers, bump, dz, split_frac, int(seed))
+        return cls(h, "bump_channel", dict(nx=nx, ny=ny, nlayers=nlayers, bump=bump, seed=seed))
+
+    @classmethod
+    def mixed_box(cls, n, L=2 * np.pi, seed=1234):
+        h = N.prep().ucp_mixed_box(n, L, int(seed))
+        return cls(h, "mixed_box", dict(n=n, L=L, seed=seed))
+
+    # ------------------------------------------------------------- set-up
+    @property
+    def ncells(self) -> int:
+        return int(N.prep().ucp_ncells(self._h))
+
+    def prepare(self, scheme: int, iorder: int, ees: int = 0, nthreads: int = 0) -> "Mesh":
+        s = N.UcpScheme(scheme, iorder, ees, nthreads)
+        _check(N.prep().ucp_prepare(self._h, C.byref(s)), "ucp_prepare")
+        self.prepared = True
+        self.scheme, self.iorder, self.ees = scheme, iorder, ees
+        cfg = N.UcgConfig()
+        _check(N.prep().ucp_fill_config(self._h, C.byref(cfg)), "ucp_fill_config")
+        self.sizes = dict(ideg=cfg.ideg, imax=cfg.imax, admis_max=cfg.admis_max, ideg2=cfg.ideg2,
+                          imax2=cfg.imax2, nq_quad=cfg.nq_quad, nq_tri=cfg.nq_tri,
+                          quad_w=list(cfg.quad_w), tri_w=list(cfg.tri_w))
+        return self
+
+    def fill_config(self, cfg: N.UcgConfig) -> N.UcgConfig:
+        _check(N.prep().ucp_fill_config(self._h, C.byref(cfg)), "ucp_fill_config")
+        return cfg
+
+    def geometry_struct(self) -> N.UcgGeometry:
+        g = N.UcgGeometry()
+        _check(N.prep().ucp_geometry(self._h, C.byref(g)), "ucp_geometry")
+        return g
+
+    def recon_struct(self) -> N.UcgRecon:
+        r = N.UcgRecon()
+        _check(N.prep().ucp_recon(self._h, C.byref(r)), "ucp_recon")
+        return r
+
+    @property
+    def ntables(self) -> int:
+        return int(N.prep().ucp_ntables(self._h))
+
+    # ------------------------------------------------ numpy views (copies)
+    def geometry(self) -> dict:
+        """Copies of the geometry arrays as numpy arrays (for tests)."""
+        g = self.geometry_struct()
+        n = g.ncells
+        F, Q = N.UCG_MAX_FACES, N.UCG_MAX_QP
+        ideg = self.sizes["ideg"]
+
+        def arr(p, shape, dt):
+            count = int(np.prod(shape))
+            ct = C.c_int32 if dt == np.int32 else C.c_double
+            buf = (ct * count).from_address(C.cast(p, C.c_void_p).value)
+            return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+        return dict(
+            ncells=n,
+            nfaces=arr(g.nfaces, (n,), np.int32), face_type=arr(g.face_type, (n, F), np.int32),
+            neigh=arr(g.neigh, (n, F), np.int32), neigh_face=arr(g.neigh_face, (n, F), np.int32),
+            bc=arr(g.bc, (n, F), np.int32), qperm=arr(g.qperm, (n, F, Q), np.int32),
+            face_angle=arr(g.face_angle, (n, F, 2), np.float64), face_area=arr(g.face_area, (n, F), np.float64),
+            dih=arr(g.dih, (n, F), np.float64), qpoints=arr(g.qpoints, (n, F, Q, 3), np.float64),
+            volume=arr(g.volume, (n,), np.float64), minedge=arr(g.minedge, (n,), np.float64),
+            invccjac=arr(g.invccjac, (n, 3, 3), np.float64), basis_mean=arr(g.basis_mean, (n, ideg), np.float64),
+            admis=arr(g.admis, (n,), np.int32), full=arr(g.full, (n,), np.int32),
+        )
+
+    def recon(self) -> dict:
+        """Copies of the reconstruction tables (for tests)."""
+        r = self.recon_struct()
+        s = self.sizes
+        n, nt = r.count, r.ntables
+        A, W, D = s["admis_max"], s["imax"] + 1, s["ideg"]
+
+        def arr(p, shape, dt):
+            if not p:
+                return None
+            count = int(np.prod(shape))
+            ct = C.c_int32 if dt == np.int32 else C.c_double
+            buf = (ct * count).from_address(C.cast(p, C.c_void_p).value)
+            return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+        out = dict(stencil=arr(r.stencil, (n, A, W), np.int32), table_id=arr(r.table_id, (n,), np.int32),
+                   ntables=nt, invmat=arr(r.invmat, (nt, A, s["imax"], D), np.float64),
+                   indicator=arr(r.indicator, (nt, D, D), np.float64))
+        if s["ideg2"]:
+            out["invmat2"] = arr(r.invmat2, (nt, A, s["imax2"], s["ideg2"]), np.float64)
+            out["indicator2"] = arr(r.indicator2, (nt, s["ideg2"], s["ideg2"]), np.float64)
+        return out
+
+    def centres(self) -> np.ndarray:
+        out = np.zeros((self.ncells, 3))
+        _check(N.prep().ucp_cell_centres(self._h, N.ptr(out, C.c_double)), "ucp_cell_centres")
+        return out
+
+    def initial_condition(self, kind: int, params) -> np.ndarray:
+        """Cell averages of the conserved variables, shape (n, 5)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        out = np.zeros((self.ncells, 5))
+        _check(N.prep().ucp_initial_condition(self._h, kind, N.ptr(p, C.c_double), len(p),
+                                              N.ptr(out, C.c_double)), "ucp_initial_condition")
+        return out
