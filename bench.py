@@ -1,0 +1,354 @@
+"""Benchmark: cell-RK-stage updates per second of the explicit residual
+engine on one B200 (or N independent replicas under torchrun).
+
+Default workload: the isentropic vortex on a periodic 64^3 hexahedral box
+(262,144 cells), Euler, 5th-order WENO + HLLC, SSP-RK3 - the mixed-precision
+form (FP32 tables/reconstruction on differences, FP64 fluxes/accumulation/
+update) is the headline `value`; the all-FP64 form is measured in the same
+run and the two are compared by their relative L2 density difference.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device-resident throughput (dt kept on the device, no host sync
+inside the timed region); `e2e` goes through the public API with host
+buffers (pinned), the host->device copy of the state and the device->host
+read of the result inside every timed step.  Inputs are larger than L2 (the
+reconstruction tables alone are tens of GB), so no L2 flush is needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-RK-stage updates/s"
+UNIT = "cell-stage/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default="vortex_hex_weno5")
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_init():
+    """One process per GPU under torchrun; replicas only (no data exchange)."""
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws, local):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def recon_bytes_per_cell(cfg):
+    """Algorithmic bytes the reconstruction kernel must move per cell: the
+    pseudo-inverses, stencil indices, smoothness matrix, face quadrature
+    points and basis means of the cell, its own state and its face values
+    written (neighbour state counted once, in the flux kernel)."""
+    from ucns3d_b200 import _native as N
+    s = 4 if cfg.precision == N.UCG_MIXED else 8
+    nq = max(cfg.nq_quad, cfg.nq_tri)
+    b = s * cfg.ideg * cfg.imax * cfg.admis_max + 4 * (cfg.imax + 1) * cfg.admis_max
+    if cfg.scheme == 3:
+        b += s * cfg.ideg * cfg.ideg
+    b += s * 6 * nq * 3 + s * cfg.ideg + 5 * 8
+    b += s * 6 * nq * 5  # face values written
+    return b
+
+
+def make_case(args, precision):
+    from ucns3d_b200 import cases
+    fn = cases.CASES[args.case]
+    kw = {"precision": precision}
+    if args.case in ("tgv_hex_muscl", "tgv_tet_weno3", "vortex_hex_weno5", "mixed_cweno4"):
+        kw["n"] = args.n
+    return fn(**kw)
+
+
+def run_gpu(args, case, ws, local, timed_e2e=True):
+    import numpy as np
+    import torch
+    from ucns3d_b200.engine import Engine
+
+    eng = Engine(case.mesh, case.cfg, device=local)
+    eng.set_state(case.U0)
+    # warm-up (also JIT/allocations)
+    eng.time_marching(args.warmup, case.cfl)
+    eng.synchronize()
+    eng.check_health()
+    stream = torch.cuda.ExternalStream(eng.stream_ptr, device=f"cuda:{local}")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize(local)
+    sampler.start()
+    l0 = eng.launch_count
+    ev0.record(stream)
+    eng.time_marching(args.steps, case.cfl)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize(local)
+    launches = eng.launch_count - l0
+    clocks = sampler.stop()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    eng.check_health()
+    kern = eng.time_kernels(reps=3)
+    state = eng.get_state()
+    e2e = None
+    if timed_e2e:
+        # public API with pinned host buffers: H2D of the state, one step, D2H
+        hin = torch.from_numpy(state).pin_memory()
+        hout = torch.empty_like(hin).pin_memory()
+        nin, nout = hin.numpy(), hout.numpy()
+        eng.set_state(nin)
+        eng.time_marching(1, case.cfl)
+        eng.get_state(nout)
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            eng.set_state(nin)
+            eng.time_marching(1, case.cfl)
+            eng.get_state(nout)
+        t1 = time.perf_counter()
+        e2e = dict(seconds=t1 - t0, bytes_in=nin.nbytes, bytes_out=nout.nbytes)
+    nbytes_dev = eng.device_bytes
+    eng.close()
+    return dict(ms=ms, kern=kern, state=state, clocks=clocks, launches=launches, e2e=e2e, device_bytes=nbytes_dev)
+
+
+def cpu_sample(args, steps=1):
+    """The oracle (CPU restatement) on a bounded sample of the workload: the
+    same scheme on a smaller mesh, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    from ucns3d_b200 import _native as N
+    from ucns3d_b200 import cases
+    fn = cases.CASES[args.case]
+    kw = {"precision": N.UCG_FP64}
+    if args.case in ("tgv_hex_muscl", "tgv_tet_weno3", "vortex_hex_weno5", "mixed_cweno4"):
+        kw["n"] = args.cpu_n
+    c = fn(**kw)
+    o = Oracle(c.mesh, c.cfg)
+    U = c.U0.copy()
+    dt = o.compute_dt(U, c.cfl)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        U = o.rk3_step(U, dt)
+    t = time.perf_counter() - t0
+    cores = os.cpu_count()
+    thr = os.environ.get("OMP_NUM_THREADS")
+    if thr:
+        cores = int(thr)
+    return dict(value=c.mesh.ncells * 3 * steps / t, cores=cores, seconds=t, ncells=c.mesh.ncells,
+                sample=f"{args.case} with n={args.cpu_n} ({c.mesh.ncells} cells), {steps} RK3 step(s), "
+                       f"oracle FP64 CPU restatement, OpenMP")
+
+
+def main_reference(args, ws, rank, local):
+    """The reference arm: the CPU restatement of the reference path (the
+    Fortran reference cannot be built on this image) on the host cores,
+    each step one RK3 step of a bounded sample of the workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    for _ in range(max(args.warmup, 0)):
+        cpu_sample(args, steps=1)
+    t = 0.0
+    cells = 0
+    info = None
+    for _ in range(args.steps):
+        info = cpu_sample(args, steps=1)
+        t += info["seconds"]
+        cells += info["ncells"] * 3
+    value = cells / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.case, "n": args.cpu_n, "note": "bounded CPU sample of the workload"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        main_reference(args, ws, rank, local)
+        return
+    import numpy as np
+    from ucns3d_b200 import _native as N
+
+    peak, peak_kind = load_peaks()
+    c32 = make_case(args, N.UCG_MIXED)
+    ncells = c32.mesh.ncells
+    r32 = run_gpu(args, c32, ws, local, timed_e2e=True)
+    cfg32 = c32.cfg
+    r64 = None
+    if not args.no_fp64:
+        # same mesh, tables and initial state; FP64 engine
+        from ucns3d_b200.cases import Case
+        cfg64 = N.UcgConfig.from_buffer_copy(cfg32)
+        cfg64.precision = N.UCG_FP64
+        c64 = Case(c32.name, c32.mesh, cfg64, c32.U0, c32.cfl, c32.steps, c32.meta)
+        r64 = run_gpu(args, c64, ws, local, timed_e2e=False)
+        del c64
+    ms = max_over_ranks(r32["ms"], ws, local)
+    value = ws * ncells * 3 * args.steps / (ms / 1000.0)
+    e2e_s = max_over_ranks(r32["e2e"]["seconds"], ws, local)
+    e2e_value = ws * ncells * 3 * args.steps / e2e_s
+    # roofline of the dominant kernel (reconstruction), achieved from its
+    # CUDA-event duration on the engine stream
+    bpc = recon_bytes_per_cell(cfg32)
+    rec_ms = r32["kern"]["recon"]
+    achieved = bpc * ncells / (rec_ms / 1000.0) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "mixed: f32 tables/reconstruction, f64 flux/accumulate/update",
+        "data": "synthetic (seeded mesh and analytic initial condition)",
+        "config": {"workload": args.case, "cells": ncells, "n": args.n, "scheme": "WENO5+HLLC SSP-RK3",
+                   "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (tables)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": None, "kernel": "k_weno (reconstruction)",
+                     "bytes_per_cell": bpc, "kernel_ms": rec_ms},
+        "kernel_ms": r32["kern"],
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": r32["e2e"]["bytes_in"],
+                "d2h_bytes_per_step": r32["e2e"]["bytes_out"]},
+        "gpu_launches": r32["launches"],
+        "clocks": r32["clocks"],
+        "device_bytes": r32["device_bytes"],
+    }
+    if r64 is not None:
+        ms64 = max_over_ranks(r64["ms"], ws, local)
+        v64 = ws * ncells * 3 * args.steps / (ms64 / 1000.0)
+        ra, rb = r64["state"][:, 0], r32["state"][:, 0]
+        l2 = float(np.sqrt(np.mean((ra - rb) ** 2)) / np.sqrt(np.mean(ra ** 2)))
+        linf = float(np.abs(ra - rb).max() / np.abs(ra).max())
+        bpc64 = recon_bytes_per_cell(cfg64)
+        out["fp64"] = {"value": v64, "ms_per_step": ms64 / args.steps, "kernel_ms": r64["kern"],
+                       "roofline_frac": bpc64 * ncells / (r64["kern"]["recon"] / 1000.0) / 1e9 / peak,
+                       "mixed_speedup": value / v64,
+                       "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
+                       "after_steps": args.warmup + args.steps}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cb = cpu_sample(args, steps=1)
+        out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                               "sample": cb["sample"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
