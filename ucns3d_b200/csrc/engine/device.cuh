@@ -16,7 +16,7 @@ constexpr double TOLSMALL = 1.0e-13;  // grid_p.f90:18
 constexpr double TOLBIG = 1.0e13;     // grid_p.f90:19
 
 // Health word bits set by kernels (read by ucg_check_health).
-enum : unsigned { HEALTH_NONPHYS = 1u };
+enum : unsigned { HEALTH_NONPHYS = 1u };  // HEALTH_TIMEOUT = 2 below
 
 // Problem description passed by value to every kernel.  Arrays are device
 // pointers; "[c]" means one entry per cell, cell index fastest where noted.
@@ -46,10 +46,19 @@ struct Problem {
   const void* qpts;         // [n][MF][MQ][3]
   const void* bmean;        // [n][ideg]
   const int32_t* sten;      // [n][A][imax+1]
-  const void* invmat;       // [n][A][imax][ideg]
-  const void* invmat2;      // [n][A][imax2][ideg2]
-  const void* ind;          // [n][ideg][ideg]
-  const void* ind2;         // [n][ideg2][ideg2]
+  // pseudo-inverses: one block of `tstride` elements per cell; slice ll
+  // (stencil ll, [nk][nd] with nk = imax or imax2, nd = ideg or ideg2)
+  // starts at element soff[ll] and is padded to a multiple of 16 bytes so
+  // that it can be moved by one bulk copy
+  const void* invmat;
+  int64_t tstride;
+  int soff[8], sbytes[8];
+  // smoothness matrices: one block of `istride` elements per cell, S
+  // [ideg][ideg] at 0 and the CWENO S2 [ideg2][ideg2] at i2off; `ibytes`
+  // is the padded size of the block
+  const void* ind;
+  int64_t istride;
+  int i2off, ibytes;
   // scratch
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
@@ -217,6 +226,153 @@ __device__ __forceinline__ void sutherland(const Problem& p, double rho, double 
   double r = t1 / t0;
   *mu = p.visc * (r * sqrt(r)) * ((t0 + suther * t0) / (t1 + suther * t0));
   *lam = (*mu) * p.r_gas * p.gamma / (p.prandtl * (p.gamma - 1.0));
+}
+
+}  // namespace ucg
+
+namespace ucg {
+
+// ------------------------------------------------ async bulk copy helpers
+// 1-D bulk copies global -> shared completed on an mbarrier (sm_90+ PTX),
+// without cluster multicast.  Waits are bounded: a wait that gives up
+// returns false and the caller records UCG_ETIMEOUT in the health word.
+enum : unsigned { HEALTH_TIMEOUT = 2u };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: about a second at most, then give up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (long it = 0; it < (1L << 22); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 64) __nanosleep(256);
+  }
+  return false;
+}
+
+}  // namespace ucg
+
+namespace ucg {
+
+// Ghost state of a physical boundary face (BOUNDARYS, src/flow_operations.f90:2860-3230)
+// and the viscous face flux (CALCULATE_FLUXESHI_DIFFUSIVE, src/flux_p.f90:1614-1779).
+__device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const double* cl,
+                                               double* cr) {
+  const double gm = p.gamma;
+  const double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
+  if (code == 3 || code == 4) {  // symmetry / inviscid wall: mirror the normal momentum
+    double a[NV], b[NV];
+    rot_f(r, cl, a);
+    b[0] = a[0];
+    b[1] = -a[1];
+    b[2] = a[2];
+    b[3] = a[3];
+    b[4] = a[4];
+    rot_b(r, b, cr);
+    return;
+  }
+  double s1[NV], s2[NV], s3[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) s1[k] = p.bc_state[k];
+  cons2prim(gm, cl, s2);
+  double sps = sqrt(gm * s2[4] / s2[0]);
+  double vel = sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+  bool super = vel / (sps + TOLSMALL) > 1.0;
+  if (code == 1) {  // inflow (BOUNDARYS case 1, subsonic characteristic treatment)
+    if (super) {
+      prim2cons(gm, s1, cr);
+      return;
+    }
+    s3[4] = 0.5 * (s1[4] + s2[4] - s2[0] * sps * (nx * (s1[1] - s2[1]) + ny * (s1[2] - s2[2]) + nz * (s1[3] - s2[3])));
+    s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
+    s3[1] = s1[1] - nx * (s1[4] - s3[4]) / (sps * s2[0]);
+    s3[2] = s1[2] - ny * (s1[4] - s3[4]) / (sps * s2[0]);
+    s3[3] = s1[3] - nz * (s1[4] - s3[4]) / (sps * s2[0]);
+  } else if (code == 2) {  // outflow (case 2)
+    if (super) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+      return;
+    }
+    s3[4] = s1[4];
+    s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
+    s3[1] = s2[1] + nx * (s2[4] - s3[4]) / (sps * s2[0]);
+    s3[2] = s2[2] + ny * (s2[4] - s3[4]) / (sps * s2[0]);
+    s3[3] = s2[3] + nz * (s2[4] - s3[4]) / (sps * s2[0]);
+  } else {
+    prim2cons(gm, s1, cr);
+    return;
+  }
+  prim2cons(gm, s3, cr);
+}
+
+__device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, double dih, const double* cl,
+                                             const double* cr, const double* gl, const double* gr, double* fv) {
+  double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
+  double nn[3] = {nx, ny, nz};
+  double lv[NV], rv[NV];
+  cons2prim(p.gamma, cl, lv);
+  cons2prim(p.gamma, cr, rv);
+  double mul, mur, laml, lamr;
+  sutherland(p, lv[0], lv[4], &mul, &laml);
+  sutherland(p, rv[0], rv[4], &mur, &lamr);
+  // gradient rows u, v, w, T; stored components are T, u, v, w
+  const int src[4] = {1, 2, 3, 0};
+  double jump[4] = {rv[1] - lv[1], rv[2] - lv[2], rv[3] - lv[3],
+                    rv[4] / (rv[0] * p.r_gas) - lv[4] / (lv[0] * p.r_gas)};
+  const double vd = (4.0 / 3.0) / fabs(dih);
+  double gg[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      gg[a][k] = (gl[src[a] * 3 + k] + gr[src[a] * 3 + k]) / 2.0 + p.lamx * (vd * nn[k] * jump[a]);
+  double lam2 = 0.5 * (laml + lamr), mu2 = 0.5 * (mul + mur);
+  double ux = gg[0][0], uy = gg[0][1], uz = gg[0][2];
+  double vx = gg[1][0], vy = gg[1][1], vz = gg[1][2];
+  double wx = gg[2][0], wy = gg[2][1], wz = gg[2][2];
+  double txx = mu2 * ((4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz);
+  double tyy = mu2 * ((4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz);
+  double tzz = mu2 * ((4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy);
+  double txy = mu2 * (uy + vx), txz = mu2 * (wx + uz), tyz = mu2 * (vz + wy);
+  double rho12 = 0.5 * (cl[0] + cr[0]);
+  double u12 = 0.5 * (cl[1] + cr[1]) / rho12, v12 = 0.5 * (cl[2] + cr[2]) / rho12, w12 = 0.5 * (cl[3] + cr[3]) / rho12;
+  double qx = lam2 * gg[3][0], qy = lam2 * gg[3][1], qz = lam2 * gg[3][2];  // -Q
+  double fx4 = qx + u12 * txx + v12 * txy + w12 * txz;
+  double fy4 = qy + u12 * txy + v12 * tyy + w12 * tyz;
+  double fz4 = qz + u12 * txz + v12 * tyz + w12 * tzz;
+  fv[0] = 0.0;
+  fv[1] = nx * txx + ny * txy + nz * txz;
+  fv[2] = nx * txy + ny * tyy + nz * tyz;
+  fv[3] = nx * txz + ny * tyz + nz * tzz;
+  fv[4] = nx * fx4 + ny * fy4 + nz * fz4;
 }
 
 }  // namespace ucg

@@ -25,8 +25,16 @@ struct DevBuf {
 
 }  // namespace
 
+// Device layout of the per-cell table blocks (see Problem in device.cuh).
+struct Layout {
+  int64_t tstride = 0, istride = 0;
+  int soff[8] = {0}, sbytes[8] = {0};
+  int i2off = 0, ibytes = 0;
+};
+
 struct ucg_engine {
   ucg_config cfg;
+  Layout layout;
   int64_t n = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -41,7 +49,7 @@ struct ucg_engine {
   // geometry
   DevBuf nfaces, ftype, neigh, nface, bc, qperm, rot, area, dih, vol, minedge, jinv, admis, full, qpts, bmean;
   // tables
-  DevBuf sten, invmat, invmat2, ind, ind2;
+  DevBuf sten, invmat, ind;
   // scratch and state
   DevBuf dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging;
   std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
@@ -149,9 +157,15 @@ Problem make_problem(ucg_engine* e) {
   p.bmean = e->bmean.p;
   p.sten = (const int32_t*)e->sten.p;
   p.invmat = e->invmat.p;
-  p.invmat2 = e->invmat2.p;
   p.ind = e->ind.p;
-  p.ind2 = e->ind2.p;
+  p.tstride = e->layout.tstride;
+  p.istride = e->layout.istride;
+  p.i2off = e->layout.i2off;
+  p.ibytes = e->layout.ibytes;
+  for (int k = 0; k < 8; ++k) {
+    p.soff[k] = e->layout.soff[k];
+    p.sbytes[k] = e->layout.sbytes[k];
+  }
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.gv = (double*)e->gv.p;
@@ -168,18 +182,11 @@ template <int P, typename T>
 int launch_weno(ucg_engine* e, const Problem& p, const double* U) {
   const ucg_config& c = e->cfg;
   const bool cw = c.ees == 5;
-  int cpc = 256 / (c.admis_max * c.ideg);
-  if (cpc < 1) cpc = 1;
-  if (cpc > 16) cpc = 16;
-  WenoSmem L = weno_smem_layout<T>(cpc, c.admis_max, c.imax, c.ideg, c.ideg2, e->QS, cw);
-  while (cpc > 1 && L.total > 100 * 1024) {
-    --cpc;
-    L = weno_smem_layout<T>(cpc, c.admis_max, c.imax, c.ideg, c.ideg2, e->QS, cw);
-  }
-  if (L.total > 200 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
-  CK(cudaFuncSetAttribute(k_weno<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total));
-  int64_t blocks = (e->n + cpc - 1) / cpc;
-  k_weno<P, T><<<(unsigned)blocks, 256, L.total, e->stream>>>(p, U, cpc);
+  W2Plan w = w2_plan<T>(c.admis_max, c.imax, c.ideg, c.imax2, c.ideg2, e->QS, cw, e->layout.sbytes,
+                        e->layout.ibytes);
+  if (w.total > 227 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
+  CK(cudaFuncSetAttribute(k_weno2<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, w.total));
+  k_weno2<P, T><<<(unsigned)e->n, W2_THREADS, w.total, e->stream>>>(p, U, w);
   e->launches++;
   if (c.governing == 1) {
     k_visc_lsq<P, T><<<(unsigned)((e->n * 4 + 127) / 128), 128, 0, e->stream>>>(p, U);
@@ -310,6 +317,24 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   e->device = device;
   e->mixed = c.precision == UCG_MIXED;
   e->QS = c.nq_quad > c.nq_tri ? c.nq_quad : c.nq_tri;
+  {
+    // slices and smoothness blocks padded to 16 bytes (bulk-copy granularity)
+    const int64_t ts = e->mixed ? 4 : 8, pad = 16 / ts;
+    auto up = [&](int64_t x) { return (x + pad - 1) / pad * pad; };
+    Layout& L = e->layout;
+    int64_t off = 0;
+    for (int ll = 0; ll < c.admis_max; ++ll) {
+      bool low = c.ees == 5 && ll > 0;
+      int64_t el = low ? (int64_t)c.imax2 * c.ideg2 : (int64_t)c.imax * c.ideg;
+      L.soff[ll] = (int)off;
+      L.sbytes[ll] = (int)(up(el) * ts);
+      off += up(el);
+    }
+    L.tstride = off;
+    L.i2off = (int)up((int64_t)c.ideg * c.ideg);
+    L.istride = L.i2off + (c.ees == 5 ? up((int64_t)c.ideg2 * c.ideg2) : 0);
+    L.ibytes = (int)(L.istride * ts);
+  }
   cudaSetDevice(device);
   st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
   if (st != cudaSuccess) {
@@ -352,7 +377,7 @@ void ucg_destroy(ucg_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
-                   &e->invmat2, &e->ind, &e->ind2, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
+                   &e->ind, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging};
   for (DevBuf* b : all) release(*b);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -477,7 +502,6 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     for (int64_t i = 0; i < count; ++i)
       if (r->table_id[i] < 0 || r->table_id[i] >= ntab) return fail(e, UCG_EINVAL, "table_id out of range");
   }
-  // stencils (validated; slot 0 must be the cell itself)
   for (int64_t i = 0; i < count; ++i) {
     int64_t cell = first + i;
     for (int ll = 0; ll < A; ++ll)
@@ -487,34 +511,48 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       }
     if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
   }
+  const Layout& Ly = e->layout;
   const size_t T = tsize(e);
   int rc = UCG_OK;
   rc = rc ? rc : alloc(e, e->sten, (size_t)n * A * W * 4);
-  const int64_t lmat = (int64_t)A * c.imax * c.ideg, lmat2 = cw ? (int64_t)A * c.imax2 * c.ideg2 : 0;
-  const int64_t lind = weno ? (int64_t)c.ideg * c.ideg : 0, lind2 = cw ? (int64_t)c.ideg2 * c.ideg2 : 0;
-  rc = rc ? rc : alloc(e, e->invmat, (size_t)n * lmat * T);
-  if (cw) rc = rc ? rc : alloc(e, e->invmat2, (size_t)n * lmat2 * T);
-  if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)n * lind * T);
-  if (cw) rc = rc ? rc : alloc(e, e->ind2, (size_t)n * lind2 * T);
+  rc = rc ? rc : alloc(e, e->invmat, (size_t)n * Ly.tstride * T);
+  if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)n * Ly.istride * T);
   if (rc) return rc;
-  // any cell referenced by a stencil must exist; then copy the stencil rows
   CK(cudaMemcpyAsync((char*)e->sten.p + (size_t)first * A * W * 4, r->stencil, (size_t)count * A * W * 4,
                      cudaMemcpyHostToDevice, e->stream));
-  // matrices: staged in chunks of tables, expanded per cell on the device
-  int32_t* d_tid = nullptr;
   DevBuf tidbuf;
+  int32_t* d_tid = nullptr;
   if (r->table_id) {
     CK(cudaMalloc(&tidbuf.p, count * 4));
     CK(cudaMemcpyAsync(tidbuf.p, r->table_id, count * 4, cudaMemcpyHostToDevice, e->stream));
     d_tid = (int32_t*)tidbuf.p;
   }
+  // pack matrix sets into the engine's per-cell block layout on the host
+  // (FP64, padding zeroed), stage them in chunks, expand per cell on the GPU
+  const int ideg = c.ideg, imax = c.imax, ideg2 = c.ideg2, imax2 = c.imax2;
+  auto pack_mat = [&](int64_t t, double* dst) {
+    for (int64_t j = 0; j < Ly.tstride; ++j) dst[j] = 0.0;
+    for (int ll = 0; ll < A; ++ll) {
+      bool low = cw && ll > 0;
+      int nk = low ? imax2 : imax, nd = low ? ideg2 : ideg;
+      const double* src = low ? r->invmat2 + ((t * A + ll) * (int64_t)imax2) * ideg2
+                              : r->invmat + ((t * A + ll) * (int64_t)imax) * ideg;
+      for (int j = 0; j < nk * nd; ++j) dst[Ly.soff[ll] + j] = src[j];
+    }
+  };
+  auto pack_ind = [&](int64_t t, double* dst) {
+    for (int64_t j = 0; j < Ly.istride; ++j) dst[j] = 0.0;
+    for (int j = 0; j < ideg * ideg; ++j) dst[j] = r->indicator[t * ideg * ideg + j];
+    if (cw)
+      for (int j = 0; j < ideg2 * ideg2; ++j) dst[Ly.i2off + j] = r->indicator2[t * ideg2 * ideg2 + j];
+  };
   struct Part {
-    const double* src;
     int64_t len;
     DevBuf* dst;
-  } parts[4] = {{r->invmat, lmat, &e->invmat}, {r->invmat2, lmat2, &e->invmat2}, {r->indicator, lind, &e->ind},
-                {r->indicator2, lind2, &e->ind2}};
-  const size_t stage_bytes = (size_t)1 << 30;
+    int which;
+  } parts[2] = {{Ly.tstride, &e->invmat, 0}, {weno ? Ly.istride : 0, &e->ind, 1}};
+  const size_t stage_bytes = (size_t)512 << 20;
+  std::vector<double> host;
   for (auto& pt : parts) {
     if (pt.len == 0) continue;
     int64_t per = (int64_t)(stage_bytes / (pt.len * 8));
@@ -522,12 +560,18 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     for (int64_t t0 = 0; t0 < ntab; t0 += per) {
       int64_t t1 = t0 + per < ntab ? t0 + per : ntab;
       size_t bytes = (size_t)(t1 - t0) * pt.len * 8;
+      host.resize((size_t)(t1 - t0) * pt.len);
+      for (int64_t t = t0; t < t1; ++t) {
+        double* d = host.data() + (t - t0) * pt.len;
+        if (pt.which == 0) pack_mat(t, d);
+        else pack_ind(t, d);
+      }
       rc = alloc(e, e->staging, bytes);
       if (rc) {
         if (tidbuf.p) cudaFree(tidbuf.p);
         return rc;
       }
-      CK(cudaMemcpyAsync(e->staging.p, pt.src + t0 * pt.len, bytes, cudaMemcpyHostToDevice, e->stream));
+      CK(cudaMemcpyAsync(e->staging.p, host.data(), bytes, cudaMemcpyHostToDevice, e->stream));
       int64_t total = count * pt.len;
       unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
       if (e->mixed)
