@@ -126,7 +126,8 @@ typedef struct ucg_geometry {
 typedef struct ucg_recon {
   int64_t first, count;
   const int32_t* stencil;     /* [count][admis_max][imax+1] IHEXL, slot 0 = the cell,
-                                 -1 = unused                                           */
+                                 -1 = unused (only outside the rows 1..imax (imax2 for
+                                 CWENO stencils ll > 0) of stencils ll < admis[c])     */
   int64_t ntables;
   const int32_t* table_id;    /* [count] or NULL                                        */
   const double* invmat;       /* [ntab][admis_max][imax][ideg] invmat_stencilt          */
@@ -142,6 +143,9 @@ typedef struct ucg_engine ucg_engine;
 int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** out);
 void ucg_destroy(ucg_engine* e);
 
+/* Upload order: geometry first (ADMIS decides which stencil rows are
+ * checked), then the reconstruction tables, in one or more cell ranges;
+ * ucg_upload_recon before ucg_upload_geometry returns UCG_ESTATE. */
 int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g);
 int ucg_upload_recon(ucg_engine* e, const ucg_recon* r);
 

@@ -48,7 +48,8 @@ def build_prep(force=False):
 
 def build_engine(force=False, extra=()):
     d = os.path.join(PKG, "csrc", "engine")
-    srcs = [os.path.join(d, f) for f in ("engine.cu", "kernels.cuh", "device.cuh")] + [os.path.join(INC, "ucns3d_gpu.h")]
+    srcs = [os.path.join(d, f) for f in ("engine.cu", "kernels.cuh", "recon2.cuh", "device.cuh")]
+    srcs.append(os.path.join(INC, "ucns3d_gpu.h"))
     out = os.path.join(LIB, "libucns3d_gpu.so")
     if force or _stale(out, srcs):
         os.makedirs(LIB, exist_ok=True)

@@ -45,11 +45,12 @@ struct Problem {
   // reconstruction tables, per cell contiguous, precision T
   const void* qpts;         // [n][MF][MQ][3]
   const void* bmean;        // [n][ideg]
-  const int32_t* sten;      // [n][A][imax+1]
-  // pseudo-inverses: one block of `tstride` elements per cell; slice ll
-  // (stencil ll, [nk][nd] with nk = imax or imax2, nd = ideg or ideg2)
-  // starts at element soff[ll] and is padded to a multiple of 16 bytes so
-  // that it can be moved by one bulk copy
+  // stencils and pseudo-inverses are interleaved over groups of 32 cells:
+  // element j of cell c is at ((c / 32) * len + j) * 32 + c % 32, with
+  // len = A*(imax+1) for the stencils and `tstride` for the pseudo-inverses.
+  // Slice ll of a cell's pseudo-inverse block ([nk][nd], nk = imax or imax2,
+  // nd = ideg or ideg2) starts at element soff[ll].
+  const int32_t* sten;
   const void* invmat;
   int64_t tstride;
   int soff[8], sbytes[8];
@@ -60,10 +61,15 @@ struct Problem {
   int64_t istride;
   int i2off, ibytes;
   // scratch
+  void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the tables
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
   double* gv;               // [n][ideg][4]  viscous LSQ coefficients
   double* rhs;              // [n][NV] residual output (residual-only mode)
+  const int32_t* own;       // owned faces, code cell*8 + face
+  int64_t nown;
+  double* fflux;            // [n][MF][NV] convective face sums (owner and negated copy)
+  double* vflux;            // [n][MF][NV] viscous face sums
   unsigned* health;
   double* dt_dev;           // device dt (ucg_step)
 };

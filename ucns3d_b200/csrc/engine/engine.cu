@@ -51,8 +51,10 @@ struct ucg_engine {
   // tables
   DevBuf sten, invmat, ind;
   // scratch and state
-  DevBuf dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging;
+  DevBuf gbuf, dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux;
+  int64_t nown = 0;
   std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
+  std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
 };
 
 namespace {
@@ -166,10 +168,15 @@ Problem make_problem(ucg_engine* e) {
     p.soff[k] = e->layout.soff[k];
     p.sbytes[k] = e->layout.sbytes[k];
   }
+  p.gbuf = e->gbuf.p;
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.gv = (double*)e->gv.p;
   p.rhs = (double*)e->rhs.p;
+  p.own = (const int32_t*)e->own.p;
+  p.nown = e->nown;
+  p.fflux = (double*)e->fflux.p;
+  p.vflux = (double*)e->vflux.p;
   p.health = (unsigned*)e->health.p;
   p.dt_dev = nullptr;
   return p;
@@ -182,12 +189,24 @@ template <int P, typename T>
 int launch_weno(ucg_engine* e, const Problem& p, const double* U) {
   const ucg_config& c = e->cfg;
   const bool cw = c.ees == 5;
-  W2Plan w = w2_plan<T>(c.admis_max, c.imax, c.ideg, c.imax2, c.ideg2, e->QS, cw, e->layout.sbytes,
-                        e->layout.ibytes);
-  if (w.total > 227 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
-  CK(cudaFuncSetAttribute(k_weno2<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, w.total));
-  k_weno2<P, T><<<(unsigned)e->n, W2_THREADS, w.total, e->stream>>>(p, U, w);
-  e->launches++;
+#if UCG_LSQ_BULK
+  {
+    const LsqBulkPlan pl = lsq_bulk_plan<P, T>(3);
+    CK(cudaFuncSetAttribute(k_lsq_bulk<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.total));
+    const int64_t ngrp = (e->n + 31) / 32;
+    k_lsq_bulk<P, T><<<(unsigned)((ngrp + pl.nw - 1) / pl.nw), pl.nw * 32, pl.total, e->stream>>>(p, U, pl);
+  }
+#else
+  k_lsq<P, T><<<(unsigned)((e->n + 127) / 128), 128, 0, e->stream>>>(p, U);
+#endif
+  int cpc = 512 / (c.admis_max * c.ideg);
+  cpc = cpc < 1 ? 1 : (cpc > 16 ? 16 : cpc);
+  WPPlan w = wpost_plan<T>(cpc, c.admis_max, c.ideg, c.ideg2, e->QS, cw, (int)e->layout.istride);
+  while (cpc > 1 && w.total > 64 * 1024) w = wpost_plan<T>(--cpc, c.admis_max, c.ideg, c.ideg2, e->QS, cw, (int)e->layout.istride);
+  if (w.total > 200 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
+  CK(cudaFuncSetAttribute(k_wpost<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, w.total));
+  k_wpost<P, T><<<(unsigned)((e->n + cpc - 1) / cpc), 256, w.total, e->stream>>>(p, U, w);
+  e->launches += 2;
   if (c.governing == 1) {
     k_visc_lsq<P, T><<<(unsigned)((e->n * 4 + 127) / 128), 128, 0, e->stream>>>(p, U);
     int64_t nf = e->n * MF * e->QS;
@@ -225,15 +244,15 @@ int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
 template <typename T, bool NS>
 int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
                   double dt) {
-  int64_t threads = e->n * 8;
-  unsigned blocks = (unsigned)((threads + 255) / 256);
+  k_face<T, NS><<<(unsigned)((e->nown + 255) / 256), 256, 0, e->stream>>>(p, Uc);
+  unsigned blocks = (unsigned)((e->n + 255) / 256);
   switch (mode) {
-    case 0: k_flux<T, NS, 0><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    case 1: k_flux<T, NS, 1><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    case 2: k_flux<T, NS, 2><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    default: k_flux<T, NS, 3><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 0: k_update<NS, 0><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 1: k_update<NS, 1><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 2: k_update<NS, 2><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    default: k_update<NS, 3><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
   }
-  e->launches++;
+  e->launches += 2;
   CK(cudaGetLastError());
   return UCG_OK;
 }
@@ -289,7 +308,7 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
                   (c.governing == 1 || c.governing == 2) && (c.precision == UCG_FP64 || c.precision == UCG_MIXED);
   int ideg = (c.iorder + 1) * (c.iorder + 2) * (c.iorder + 3) / 6 - 1;
   if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
-      c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && (c.ideg2 < 1 || c.imax2 < c.ideg2)) ||
+      c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && (c.ideg2 < 1 || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
       c.gamma <= 1.0 || c.limiter != 7 || c.riemann != 1 || c.wenwrt != 1) {
     g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC, limiter 7, "
                    "conserved-variable WENO)";
@@ -349,7 +368,12 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   rc = rc ? rc : alloc(e, e->Ua, n * NV * 8);
   rc = rc ? rc : alloc(e, e->Ub, n * NV * 8);
   rc = rc ? rc : alloc(e, e->rhs, n * NV * 8);
+  rc = rc ? rc : alloc(e, e->fflux, (size_t)n * MF * NV * 8);
+  if (c.governing == 1) rc = rc ? rc : alloc(e, e->vflux, (size_t)n * MF * NV * 8);
   rc = rc ? rc : alloc(e, e->dul, (size_t)n * MF * e->QS * NV * T);
+  const int64_t ngrp = (n + 31) / 32;
+  if (!(c.scheme == 2 && c.iorder == 1))
+    rc = rc ? rc : alloc(e, e->gbuf, (size_t)ngrp * 32 * c.admis_max * c.ideg * NV * T);
   if (c.governing == 1) {
     rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
     rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
@@ -378,7 +402,7 @@ void ucg_destroy(ucg_engine* e) {
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
-                   &e->health, &e->dt, &e->partial, &e->red, &e->staging};
+                   &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux};
   for (DevBuf* b : all) release(*b);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -446,7 +470,17 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
       }
     }
   }
+  if (n >= (int64_t(1) << 28)) return fail(e, UCG_EINVAL, "too many cells (face codes are 32-bit)");
+  std::vector<int32_t> own;
+  own.reserve(n * 3);
+  for (int64_t c = 0; c < n; ++c)
+    for (int f = 0; f < nfaces[c]; ++f) {
+      int64_t nb = neigh[c * MF + f];
+      if (nb < 0 || c < nb || (c == nb && f < nface[c * MF + f])) own.push_back((int32_t)(c * 8 + f));
+    }
   int rc = UCG_OK;
+  rc = rc ? rc : upload(e, e->own, own);
+  e->nown = (int64_t)own.size();
   rc = rc ? rc : upload(e, e->nfaces, nfaces);
   rc = rc ? rc : upload(e, e->ftype, ftype);
   rc = rc ? rc : upload(e, e->neigh, neigh);
@@ -481,6 +515,7 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   }
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
+  e->admis_h = std::move(admis);
   e->have_geometry = true;
   return UCG_OK;
 }
@@ -493,6 +528,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   const bool weno = c.scheme == 3, cw = c.ees == 5;
   if (weno && !r->indicator) return fail(e, UCG_EINVAL, "WENO needs the INDICATOR matrices");
   if (cw && (!r->invmat2 || !r->indicator2)) return fail(e, UCG_EINVAL, "CWENO needs invmat2 and INDICATORC");
+  if (!e->have_geometry) return fail(e, UCG_ESTATE, "upload the geometry before the reconstruction tables");
   cudaSetDevice(e->device);
   const int64_t n = e->n, first = r->first, count = r->count;
   const int A = c.admis_max, W = c.imax + 1;
@@ -508,18 +544,35 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       for (int k = 0; k < W; ++k) {
         int32_t y = r->stencil[(i * A + ll) * W + k];
         if (y >= n || y < -1) return fail(e, UCG_EINVAL, "stencil index out of range at cell " + std::to_string(cell));
+        // rows 1..nk of the admissible stencils are read by the kernels
+        const int nk = cw && ll > 0 ? c.imax2 : c.imax;
+        if (y < 0 && ll < e->admis_h[cell] && k >= 1 && k <= nk)
+          return fail(e, UCG_EINVAL, "unused slot (-1) inside admissible stencil " + std::to_string(ll) + " of cell " +
+                                         std::to_string(cell));
       }
     if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
   }
   const Layout& Ly = e->layout;
   const size_t T = tsize(e);
   int rc = UCG_OK;
-  rc = rc ? rc : alloc(e, e->sten, (size_t)n * A * W * 4);
-  rc = rc ? rc : alloc(e, e->invmat, (size_t)n * Ly.tstride * T);
+  const int64_t ngrp = (n + 31) / 32;
+  rc = rc ? rc : alloc(e, e->sten, (size_t)ngrp * 32 * A * W * 4);
+  rc = rc ? rc : alloc(e, e->invmat, (size_t)ngrp * 32 * Ly.tstride * T);
   if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)n * Ly.istride * T);
   if (rc) return rc;
-  CK(cudaMemcpyAsync((char*)e->sten.p + (size_t)first * A * W * 4, r->stencil, (size_t)count * A * W * 4,
-                     cudaMemcpyHostToDevice, e->stream));
+  {
+    // stencils: staged per cell, interleaved on the device
+    rc = alloc(e, e->staging, (size_t)count * A * W * 4);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(e->staging.p, r->stencil, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
+    int64_t total = count * A * W;
+    unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
+    k_expand_il<int32_t, int32_t><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
+                                                                nullptr, first, count, (int64_t)A * W, 0, count);
+    e->launches++;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(e->stream));
+  }
   DevBuf tidbuf;
   int32_t* d_tid = nullptr;
   if (r->table_id) {
@@ -574,12 +627,18 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       CK(cudaMemcpyAsync(e->staging.p, host.data(), bytes, cudaMemcpyHostToDevice, e->stream));
       int64_t total = count * pt.len;
       unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
-      if (e->mixed)
-        k_expand<float><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, (const double*)e->staging.p, d_tid, first,
-                                                      count, pt.len, t0, t1);
-      else
-        k_expand<double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, (const double*)e->staging.p, d_tid, first,
-                                                       count, pt.len, t0, t1);
+      const double* sp = (const double*)e->staging.p;
+      if (pt.which == 0) {  // pseudo-inverses: interleaved over 32-cell groups
+        if (e->mixed)
+          k_expand_il<float, double><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+        else
+          k_expand_il<double, double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      } else {  // smoothness matrices: one contiguous block per cell
+        if (e->mixed)
+          k_expand<float><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+        else
+          k_expand<double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      }
       e->launches++;
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(e->stream));

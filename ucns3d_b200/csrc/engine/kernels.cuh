@@ -27,8 +27,10 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
   cons2prim(p.gamma, u0, pm);
   const double t0 = NS ? pm[4] / (pm[0] * p.r_gas) : 0.0;
   // least squares on stencil 1
-  const int32_t* st = p.sten + c * (int64_t)p.admis_max * W;
-  const T* M = (const T*)p.invmat + c * p.tstride + p.soff[0];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;  // row j at st[j * 32]
+  const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
   T g[3][NV];
   double gvv[3][4];
 #pragma unroll
@@ -39,11 +41,11 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
     for (int v = 0; v < 4; ++v) gvv[d][v] = 0.0;
   }
   for (int k = 0; k < IM; ++k) {
-    const int64_t y = st[k + 1];
+    const int64_t y = st[(k + 1) * 32];
     double uy[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) uy[v] = U[y * NV + v];
-    T m0 = M[k * 3 + 0], m1 = M[k * 3 + 1], m2 = M[k * 3 + 2];
+    T m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       T du = T(uy[v] - u0[v]);
@@ -80,36 +82,30 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
   const T* qp = (const T*)p.qpts + c * (int64_t)MF * QS * 3;
   const T* bm = (const T*)p.bmean + c * 3;
   const double epsi2 = (p.kappa_ven * p.minedge[c]) * (p.kappa_ven * p.minedge[c]) * (p.kappa_ven * p.minedge[c]);
-  double d2[MF][NV], slope[NV];
+  // unlimited face value minus the mean (recomputed rather than stored: three terms)
+  auto face_d = [&](int f, int v) -> double {
+    T b0 = qp[f * QS * 3 + 0] - bm[0], b1 = qp[f * QS * 3 + 1] - bm[1], b2 = qp[f * QS * 3 + 2] - bm[2];
+    T res = b0 * g[0][v] + b1 * g[1][v] + b2 * g[2][v];
+    return (u0[v] + (double)res) - u0[v];
+  };
+  double slope[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) slope[v] = TOLBIG;
-  for (int f = 0; f < MF; ++f) {
-    if (f >= nf) break;
-    T b0 = qp[f * QS * 3 + 0] - bm[0], b1 = qp[f * QS * 3 + 1] - bm[1], b2 = qp[f * QS * 3 + 2] - bm[2];
+  for (int f = 0; f < nf; ++f)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      T res = b0 * g[0][v] + b1 * g[1][v] + b2 * g[2][v];
-      double usol = u0[v] + (double)res;
-      double dd = usol - u0[v];
-      d2[f][v] = dd;
-      slope[v] = fmin(slope[v], venkat(dd, umin[v] - u0[v], umax[v] - u0[v], epsi2));
-    }
-  }
+    for (int v = 0; v < NV; ++v) slope[v] = fmin(slope[v], venkat(face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2));
   // limited face values and CHECKSOLX
   bool first = false;
   for (int f = 0; f < nf; ++f) {
     double uf[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      d2[f][v] = d2[f][v] * slope[v];
-      uf[v] = u0[v] + d2[f][v];
-    }
+    for (int v = 0; v < NV; ++v) uf[v] = u0[v] + face_d(f, v) * slope[v];
     first = first || jump_bad(p.gamma, pm, uf, 0.95);
   }
   T* out = (T*)p.dul + c * (int64_t)MF * QS * NV;
   for (int f = 0; f < nf; ++f)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) out[f * QS * NV + v] = first ? T(0) : T(d2[f][v]);
+    for (int v = 0; v < NV; ++v) out[f * QS * NV + v] = first ? T(0) : T(face_d(f, v) * slope[v]);
   if (NS) {
     // face gradients: d/dxi of the linear basis is the unit vector, then
     // AINVJT = INVCCJAC^T (SOLUTIONTRIAV2)
@@ -143,17 +139,19 @@ __global__ void k_visc_lsq(Problem p, const double* __restrict__ U) {
   double pm[NV];
   cons2prim(p.gamma, U + c * NV, pm);
   const double s0 = var == 0 ? pm[4] / (pm[0] * p.r_gas) : pm[var];
-  const int32_t* st = p.sten + c * (int64_t)p.admis_max * W;
-  const T* M = (const T*)p.invmat + c * p.tstride + p.soff[0];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
   double acc[ID];
 #pragma unroll
   for (int d = 0; d < ID; ++d) acc[d] = 0.0;
   for (int k = 0; k < IM; ++k) {
     double py[NV];
-    cons2prim(p.gamma, U + (int64_t)st[k + 1] * NV, py);
+    cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
     double ds = (var == 0 ? py[4] / (py[0] * p.r_gas) : py[var]) - s0;
 #pragma unroll
-    for (int d = 0; d < ID; ++d) acc[d] += (double)M[k * ID + d] * ds;
+    for (int d = 0; d < ID; ++d) acc[d] += (double)M[(k * ID + d) * 32] * ds;
   }
 #pragma unroll
   for (int d = 0; d < ID; ++d) p.gv[(c * ID + d) * 4 + var] = acc[d];
@@ -195,77 +193,105 @@ __global__ void k_visc_face(Problem p) {
 // flux_p.f90:1520), then RUNGE_KUTTA3 (time_p.f90:885-1027).
 // MODE 0: write the residual; MODE 1/2/3: RK stage 1/2/3.
 // ======================================================================
-template <typename T, bool NS, int MODE>
-__global__ void __launch_bounds__(256) k_flux(Problem p, const double* __restrict__ Uc, const double* Un,
-                                              double* Uout, double dt_host) {
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t c = gid >> 3;
-  const int f = (int)(gid & 7);
-  const int lane = threadIdx.x & 31, base = lane & ~7;
+// One thread per owned face (the cell with the smaller index, or the only
+// cell of a boundary face): HLLC and viscous fluxes over the face's points,
+// weighted by w_q * area.  The neighbour's face gets the negated sums: HLLC
+// and the viscous flux are antisymmetric under swapping the two states and
+// flipping the normal, so each interior face is evaluated once instead of
+// twice as in the reference's per-cell loop.
+template <typename T, bool NS>
+__global__ void __launch_bounds__(256) k_face(Problem p, const double* __restrict__ Uc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nown) return;
+  const int32_t code = p.own[i];
+  const int64_t c = code >> 3;
+  const int f = code & 7;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  double u0[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = Uc[c * NV + v];
+  const int ft = p.ftype[c * MF + f];
+  const int nq = face_nq(p, ft);
+  const int64_t nb = p.neigh[c * MF + f];
+  const int nf = p.nface[c * MF + f];
+  double r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
+  const double area = p.area[c * MF + f];
+  double un[NV];
+  if (nb >= 0)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) un[v] = Uc[nb * NV + v];
+  const T* dl = (const T*)p.dul + (c * MF + f) * QS * NV;
+  const T* dr = nb >= 0 ? (const T*)p.dul + (nb * MF + nf) * QS * NV : nullptr;
+  const uint8_t* qpm = p.qperm + (c * MF + f) * QS;
   double god[NV] = {0, 0, 0, 0, 0}, gvis[NV] = {0, 0, 0, 0, 0};
-  const bool live = c < p.n && f < p.nfaces[c];
-  if (live) {
-    double u0[NV];
+  for (int q = 0; q < nq; ++q) {
+    double cl[NV], cr[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) u0[v] = Uc[c * NV + v];
-    const int ft = p.ftype[c * MF + f];
-    const int nq = face_nq(p, ft);
-    const int64_t nb = p.neigh[c * MF + f];
-    const int nf = p.nface[c * MF + f];
-    double r[4];
+    for (int v = 0; v < NV; ++v) cl[v] = u0[v] + (double)dl[q * NV + v];
+    const int qq = qpm[q];
+    if (nb >= 0) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
-    const double area = p.area[c * MF + f];
-    double un[NV];
-    if (nb >= 0)
+      for (int v = 0; v < NV; ++v) cr[v] = un[v] + (double)dr[qq * NV + v];
+    } else {
+      boundary_ghost(p, p.bc[c * MF + f], r, cl, cr);
+    }
+    double a[NV], b[NV], h[NV], fl[NV];
+    rot_f(r, cr, b);
+    rot_f(r, cl, a);
+    hllc(p.gamma, a, b, h);
+    rot_b(r, h, fl);
+    const double ws = face_weight(p, ft, q) * area;
 #pragma unroll
-      for (int v = 0; v < NV; ++v) un[v] = Uc[nb * NV + v];
-    const T* dl = (const T*)p.dul + (c * MF + f) * QS * NV;
-    const T* dr = nb >= 0 ? (const T*)p.dul + (nb * MF + nf) * QS * NV : nullptr;
-    const uint8_t* qpm = p.qperm + (c * MF + f) * QS;
-    for (int q = 0; q < nq; ++q) {
-      double cl[NV], cr[NV];
+    for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
+    if (NS && nb >= 0) {
+      const double* gl = p.ulv + ((c * MF + f) * QS + q) * 12;
+      const double* gr = p.ulv + ((nb * MF + nf) * QS + qq) * 12;
+      double fv[NV];
+      viscous_flux(p, r, p.dih[c * MF + f], cl, cr, gl, gr, fv);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) cl[v] = u0[v] + (double)dl[q * NV + v];
-      int qq = qpm[q];
-      if (nb >= 0) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) cr[v] = un[v] + (double)dr[qq * NV + v];
-      } else {
-        boundary_ghost(p, p.bc[c * MF + f], r, cl, cr);
-      }
-      double a[NV], b[NV], h[NV], fl[NV];
-      rot_f(r, cr, b);
-      rot_f(r, cl, a);
-      hllc(p.gamma, a, b, h);
-      rot_b(r, h, fl);
-      const double ws = face_weight(p, ft, q) * area;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
-      if (NS && nb >= 0) {
-        const double* gl = p.ulv + ((c * MF + f) * QS + q) * 12;
-        const double* gr = p.ulv + ((nb * MF + nf) * QS + qq) * 12;
-        double fv[NV];
-        viscous_flux(p, r, p.dih[c * MF + f], cl, cr, gl, gr, fv);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) gvis[v] = gvis[v] + fv[v] * ws;
-      }
+      for (int v = 0; v < NV; ++v) gvis[v] = gvis[v] + fv[v] * ws;
     }
   }
-  // face sums in face order: convective first, then viscous (subtracted)
-  double R[NV] = {0, 0, 0, 0, 0};
+  double* o = p.fflux + (c * MF + f) * NV;
 #pragma unroll
-  for (int k = 0; k < MF; ++k)
-#pragma unroll
-    for (int v = 0; v < NV; ++v) R[v] = R[v] + __shfl_sync(0xffffffffu, god[v], base + k);
+  for (int v = 0; v < NV; ++v) o[v] = god[v];
   if (NS) {
+    double* ov = p.vflux + (c * MF + f) * NV;
 #pragma unroll
-    for (int k = 0; k < MF; ++k)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) R[v] = R[v] - __shfl_sync(0xffffffffu, gvis[v], base + k);
+    for (int v = 0; v < NV; ++v) ov[v] = gvis[v];
   }
-  if (f != 0 || c >= p.n) return;
+  if (nb >= 0) {
+    double* o2 = p.fflux + (nb * MF + nf) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o2[v] = -god[v];
+    if (NS) {
+      double* ov2 = p.vflux + (nb * MF + nf) * NV;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ov2[v] = -gvis[v];
+    }
+  }
+}
+
+// Per-cell sum of the face fluxes in face order (convective first, then the
+// viscous ones subtracted, as CALCULATE_FLUXESHI_CONVECTIVE/_DIFFUSIVE add
+// them to RHS) and the RUNGE_KUTTA3 stage update (time_p.f90:885-1027).
+// MODE 0: write the residual; MODE 1/2/3: RK stage 1/2/3.
+template <bool NS, int MODE>
+__global__ void __launch_bounds__(256) k_update(Problem p, const double* __restrict__ Uc, const double* Un,
+                                                double* Uout, double dt_host) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const int nf = p.nfaces[c];
+  double R[NV] = {0, 0, 0, 0, 0};
+  for (int f = 0; f < nf; ++f)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) R[v] = R[v] + p.fflux[(c * MF + f) * NV + v];
+  if (NS)
+    for (int f = 0; f < nf; ++f)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) R[v] = R[v] - p.vflux[(c * MF + f) * NV + v];
   if (MODE == 0) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) p.rhs[c * NV + v] = R[v];
@@ -360,6 +386,20 @@ __global__ void k_reduce_final(const double* partial, int64_t np, double* out) {
 // Table upload: per-cell rows dst[c][0..len) from src[table_id[c]] (or
 // src[c - first] without ids), converted to the engine precision.
 // ======================================================================
+// Interleaved variant: row j of cell c goes to ((c/32)*len + j)*32 + c%32.
+template <typename D, typename S>
+__global__ void k_expand_il(D* __restrict__ dst, const S* __restrict__ src, const int32_t* __restrict__ tid,
+                            int64_t first, int64_t count, int64_t len, int64_t tlo, int64_t thi) {
+  const int64_t total = count * len;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t cl = i / len, j = i - cl * len;
+    int64_t t = tid ? tid[cl] : cl;
+    if (t < tlo || t >= thi) continue;
+    int64_t c = first + cl;
+    dst[((c >> 5) * len + j) * 32 + (c & 31)] = D(src[(t - tlo) * len + j]);
+  }
+}
+
 template <typename T>
 __global__ void k_expand(T* __restrict__ dst, const double* __restrict__ src, const int32_t* __restrict__ tid,
                          int64_t first, int64_t count, int64_t len, int64_t tlo, int64_t thi) {

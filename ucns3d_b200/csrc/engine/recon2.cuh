@@ -1,115 +1,402 @@
-// WENO / CWENO / high-order MUSCL reconstruction, one thread block per cell,
-// with the cell's pseudo-inverse streamed into shared memory by 1-D bulk
-// asynchronous copies (two ring slots, mbarrier completion, no multicast).
+// Reconstruction for WENO / CWENO / high-order MUSCL in two kernels.
 //
-// Per cell, in the order of ARBITRARY_ORDER (src/reconstruct_p.f90:2954):
-//   LEAST_SQUARES      G[ll] = invmat[ll] . (U_k - U_i)      gradients.f90:253-497
-//   CP_RECONSTRUCTION  IS = g^T S g, weights, face values    reconstruct_p.f90:920-1250
-//   CHECKSOL -> MUSCL on flagged cells -> CHECKSOLX          reconstruct_p.f90:3126, 2286, 3245
+// k_lsq      LEAST_SQUARES (src/gradients.f90:253-497): one lane per cell.
+//            Tables are interleaved over groups of 32 cells, so every table
+//            load of a warp is one contiguous 128/256-byte row; each gathered
+//            difference U_k - U_i is reused across DH rows held in registers.
+//            Output: the stencil polynomials G[ll][d][v], interleaved.
+// k_wpost    CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), CHECKSOL,
+//            MUSCL fall-back, CHECKSOLX (3126-3406): a block reconstructs
+//            `cpc` cells cooperatively in shared memory.
 #pragma once
 
 #include "device.cuh"
 
 namespace ucg {
 
-constexpr int W2_THREADS = 256;
-constexpr int W2_MAXITEM = 16;
+// Tuning of k_lsq (compile-time): rows of G held in registers per pass for
+// IORDER 4/3 in FP32/FP64, software pipelining of the index/state chain,
+// minimum resident blocks per SM for the register budget.
+#ifndef UCG_LSQ_ROWS_P4F
+#define UCG_LSQ_ROWS_P4F 17
+#endif
+#ifndef UCG_LSQ_ROWS_P4D
+#define UCG_LSQ_ROWS_P4D 12
+#endif
+#ifndef UCG_LSQ_ROWS_P3F
+#define UCG_LSQ_ROWS_P3F 19
+#endif
+#ifndef UCG_LSQ_ROWS_P3D
+#define UCG_LSQ_ROWS_P3D 10
+#endif
+#ifndef UCG_LSQ_PIPE
+#define UCG_LSQ_PIPE 0
+#endif
+#ifndef UCG_LSQ_MINB
+#define UCG_LSQ_MINB 1
+#endif
+// 1: k_lsq_bulk (tables streamed through shared memory), 0: k_lsq
+#ifndef UCG_LSQ_BULK
+#define UCG_LSQ_BULK 1
+#endif
 
-// Host-computed description of the stream of table chunks and of the
-// shared-memory carve-up (offsets in bytes).
-struct W2Plan {
-  int nch[8];      // chunks of slice ll (1 or 2)
-  int rc[8];       // rows per chunk of slice ll (last chunk: the rest)
-  int slot_bytes;  // one ring slot
-  int kp;          // row partitions of the LSQ product
-  int db;          // rows of G per thread (d block)
-  int o_bar, o_slot, o_S, o_du, o_part, o_G, o_g1, o_gh, o_w, o_dul, o_psi, o_u0, o_bnd, o_slope, o_flag,
-      o_sten, total;
+// rows of G held in registers per pass
+template <int P, typename T>
+struct LsqRows {
+  static constexpr int ID = Deg<P>::ideg;
+  static constexpr int value = P == 4   ? (sizeof(T) == 4 ? UCG_LSQ_ROWS_P4F : UCG_LSQ_ROWS_P4D)
+                               : P == 3 ? (sizeof(T) == 4 ? UCG_LSQ_ROWS_P3F : UCG_LSQ_ROWS_P3D)
+                                        : ID;
 };
 
-template <typename T>
-inline W2Plan w2_plan(int A, int IM, int ID, int IM2, int ID2, int QS, bool cw, const int* sbytes, int ibytes) {
-  W2Plan w{};
-  const int s = (int)sizeof(T);
-  int slot = 0;
+template <int P, typename T>
+__global__ void __launch_bounds__(128, UCG_LSQ_MINB) k_lsq(Problem p, const double* __restrict__ U) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int DH = LsqRows<P, T>::value;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int A = p.admis_max, W = p.imax + 1;
+  const bool cw = p.ees == 5;
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const bool live = c < p.n;
+  const int adm = live ? p.admis[c] : 0;
+  double u0[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = live ? U[c * NV + v] : 0.0;
+  const T* Mi = (const T*)p.invmat + grp * p.tstride * 32 + lane;
+  const int32_t* Si = p.sten + grp * (int64_t)(A * W) * 32 + lane;
+  T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
   for (int ll = 0; ll < A; ++ll) {
-    bool low = cw && ll > 0;
-    int nk = low ? IM2 : IM, nd = low ? ID2 : ID;
-    int rb = nd * s;
-    int g = 16;
-    for (int x = rb; x % 2 == 0 && g > 1; x /= 2) g /= 2;  // rows per 16-byte granule
-    if (sbytes[ll] <= 16 * 1024 || nk < 2 * g) {
-      w.nch[ll] = 1;
-      w.rc[ll] = nk;
-      slot = slot > sbytes[ll] ? slot : sbytes[ll];
-    } else {
-      int rc = (nk + 1) / 2;
-      rc = (rc + g - 1) / g * g;
-      w.nch[ll] = 2;
-      w.rc[ll] = rc;
-      int b0 = rc * rb, b1 = sbytes[ll] - b0;
-      slot = slot > b0 ? slot : b0;
-      slot = slot > b1 ? slot : b1;
+    const bool low = cw && ll > 0;
+    const int nk = low ? p.imax2 : p.imax, nd = low ? p.ideg2 : ID;
+    const bool act = ll < adm;
+    for (int d0 = 0; d0 < nd; d0 += DH) {
+      T acc[DH][NV];
+#pragma unroll
+      for (int j = 0; j < DH; ++j)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
+      if (act) {
+        const T* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
+        const int32_t* S = Si + (ll * W + 1) * 32;
+#if UCG_LSQ_PIPE
+        // software pipeline of the dependent chain index -> state -> FMA:
+        // indices two rows ahead, neighbour state one row ahead
+        int y1 = nk > 1 ? S[32] : 0;
+        double ua[NV];
+        {
+          const double* uy = U + (int64_t)S[0] * NV;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ua[v] = uy[v];
+        }
+        for (int k = 0; k < nk; ++k) {
+          const int y2 = k + 2 < nk ? S[(k + 2) * 32] : 0;
+          double ub[NV];
+          const double* un = U + (int64_t)y1 * NV;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ub[v] = k + 1 < nk ? un[v] : 0.0;
+          T du[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) du[v] = T(ua[v] - u0[v]);
+          const T* Mk = M + (int64_t)k * nd * 32;
+#pragma unroll
+          for (int j = 0; j < DH; ++j)
+            if (d0 + j < nd) {
+              T m = Mk[j * 32];
+#pragma unroll
+              for (int v = 0; v < NV; ++v) acc[j][v] += m * du[v];
+            }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ua[v] = ub[v];
+          y1 = y2;
+        }
+      }
+#else
+#pragma unroll 2
+        for (int k = 0; k < nk; ++k) {
+          const double* uy = U + (int64_t)S[k * 32] * NV;
+          T du[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) du[v] = T(uy[v] - u0[v]);
+          const T* Mk = M + (int64_t)k * nd * 32;
+#pragma unroll
+          for (int j = 0; j < DH; ++j)
+            if (d0 + j < nd) {
+              T m = Mk[j * 32];
+#pragma unroll
+              for (int v = 0; v < NV; ++v) acc[j][v] += m * du[v];
+            }
+        }
+      }
+#endif
+      if (live)
+#pragma unroll
+        for (int j = 0; j < DH; ++j)
+          if (d0 + j < nd)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] = acc[j][v];
     }
   }
-  w.slot_bytes = (slot + 127) / 128 * 128;
-  w.db = ID >= 19 ? 4 : 3;
-  int ndb = (ID + w.db - 1) / w.db;
-  w.kp = W2_THREADS / ndb;
-  if (w.kp > 16) w.kp = 16;
-  if (w.kp > IM) w.kp = IM;
-  int off = 0;
-  auto take = [&](int bytes) {
-    int o = off;
-    off += (bytes + 127) / 128 * 128;
-    return o;
+}
+
+// ------------------------------------------------------------- k_lsq_bulk
+// The same product G = invmat * (U_k - U_i) with the pseudo-inverse rows
+// streamed through shared memory.  Each warp owns one 32-cell group; lane 0
+// keeps `stages` chunks of bulk copies in flight (table rows and stencil
+// indices), so the DRAM requests outstanding per SM do not depend on the
+// register budget.  A chunk is KR stencil rows x dc columns [d0, d0+dc) of
+// stencil ll; LsqBulk<P,T>::DH columns are accumulated in registers over all
+// rows of a stencil.  The neighbour states of chunk i+1 are gathered while
+// chunk i is multiplied.  No block-wide barrier: warps run independently.
+template <int P, typename T>
+struct LsqBulk {
+  static constexpr int ID = Deg<P>::ideg;
+  // columns per pass: 170 accumulator registers at most
+  static constexpr int DH = sizeof(T) == 4 ? (ID <= 34 ? ID : 34) : (ID <= 17 ? ID : (ID + 1) / 2);
+  static constexpr int KR = 2;  // stencil rows per chunk
+  static constexpr int stage_bytes = KR * DH * 32 * (int)sizeof(T) + KR * 128;
+};
+
+struct LsqBulkPlan {
+  int nw;      // warps (32-cell groups) per block
+  int stages;  // chunks in flight per warp
+  int total;   // dynamic shared memory per block
+};
+
+template <int P, typename T>
+LsqBulkPlan lsq_bulk_plan(int nw) {
+  constexpr int sb = LsqBulk<P, T>::stage_bytes;
+  int st = 36 * 1024 / sb;
+  st = st < 3 ? 3 : (st > 16 ? 16 : st);
+  return LsqBulkPlan{nw, st, nw * st * (sb + 8)};
+}
+
+struct LsqChunk {
+  int ll, d0, k0;
+};
+
+template <int P, typename T>
+__global__ void __launch_bounds__(96, 2) k_lsq_bulk(Problem p, const double* __restrict__ U, LsqBulkPlan pl) {
+  using B = LsqBulk<P, T>;
+  constexpr int ID = B::ID, DH = B::DH, KR = B::KR, SB = B::stage_bytes;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t grp = (int64_t)blockIdx.x * pl.nw + w;
+  if (grp * 32 >= p.n) return;  // warp-uniform
+  const int S = pl.stages;
+  unsigned char* stage0 = smem + (size_t)w * S * SB;
+  uint64_t* bar = (uint64_t*)(smem + (size_t)pl.nw * S * SB) + w * S;
+  const int A = p.admis_max, W = p.imax + 1;
+  const bool cw = p.ees == 5;
+  const int64_t c = grp * 32 + lane;
+  const bool live = c < p.n;
+  const int adm = live ? p.admis[c] : 0;
+  const int amax = __reduce_max_sync(0xffffffffu, adm);  // stencils any lane of the group uses
+  const T* Mg = (const T*)p.invmat + grp * p.tstride * 32;
+  const int32_t* Sg = p.sten + grp * (int64_t)(A * W) * 32;
+  T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto nk_of = [&](int ll) { return cw && ll > 0 ? p.imax2 : p.imax; };
+  auto nd_of = [&](int ll) { return cw && ll > 0 ? p.ideg2 : ID; };
+  auto next = [&](LsqChunk& q) {
+    q.k0 += KR;
+    if (q.k0 >= nk_of(q.ll)) {
+      q.k0 = 0;
+      q.d0 += DH;
+      if (q.d0 >= nd_of(q.ll)) {
+        q.d0 = 0;
+        ++q.ll;
+      }
+    }
   };
-  const int NVv = 5, MFv = 6;
-  w.o_bar = take(4 * 8);
-  w.o_slot = take(2 * w.slot_bytes);
-  w.o_S = take(ibytes);
-  w.o_du = take(A * IM * NVv * s);
-  int part = w.kp * ndb * w.db * NVv * s, psi = MFv * QS * NVv * 8, tmp = A * ID * NVv * s;
-  if (psi > part) part = psi;
-  if (tmp > part) part = tmp;
-  w.o_part = take(part);
-  w.o_psi = w.o_part;  // partial sums are dead once G is formed
-  w.o_G = take(A * ID * NVv * s);
-  w.o_g1 = take(cw ? ID * NVv * s : 0);
-  w.o_gh = take(ID * NVv * s);
-  w.o_w = take(A * NVv * 8);
-  w.o_dul = take(MFv * QS * NVv * s);
-  w.o_u0 = take(NVv * 8);
-  w.o_bnd = take(2 * NVv * 8);
-  w.o_slope = take(NVv * 8);
-  w.o_flag = take(2 * 4);
-  w.o_sten = take(A * (IM + 1) * 4);
-  w.total = off;
-  return w;
+  // lane 0: copy chunk q into stage s
+  auto issue = [&](const LsqChunk& q, int s) {
+    const int nk = nk_of(q.ll), nd = nd_of(q.ll);
+    const int kc = min(KR, nk - q.k0), dc = min(DH, nd - q.d0);
+    unsigned char* st = stage0 + (size_t)s * SB;
+    T* tab = (T*)st;
+    int32_t* idx = (int32_t*)(st + KR * DH * 32 * sizeof(T));
+    const T* M = Mg + (int64_t)p.soff[q.ll] * 32;
+    mbar_expect_tx(&bar[s], (unsigned)(kc * dc * 32 * sizeof(T) + kc * 128));
+    if (dc == nd) {
+      bulk_g2s(tab, M + (int64_t)q.k0 * nd * 32, (unsigned)(kc * nd * 32 * sizeof(T)), &bar[s]);
+    } else {
+      for (int r = 0; r < kc; ++r)
+        bulk_g2s(tab + r * dc * 32, M + ((int64_t)(q.k0 + r) * nd + q.d0) * 32, (unsigned)(dc * 32 * sizeof(T)),
+                 &bar[s]);
+    }
+    bulk_g2s(idx, Sg + (int64_t)(q.ll * W + 1 + q.k0) * 32, (unsigned)(kc * 128), &bar[s]);
+  };
+  if (lane == 0)
+    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+  mbar_fence_init();
+  __syncwarp();
+
+  double u0[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = live ? U[c * NV + v] : 0.0;
+
+  // chunk indices: waited < issued; chunk i lives in stage i % S
+  int64_t issued = 0, waited = 0;
+  LsqChunk prod{0, 0, 0};
+  for (int s = 0; s < S && prod.ll < amax; ++s) {
+    if (lane == 0) issue(prod, s);
+    next(prod);
+    ++issued;
+  }
+  bool ok = true;
+  auto wait_chunk = [&](int64_t i) {
+    const bool r = __all_sync(0xffffffffu, mbar_wait(&bar[i % S], (unsigned)((i / S) & 1)));
+    ok = ok && r;
+    if (r) waited = i + 1;
+  };
+
+  LsqChunk cur{0, 0, 0};
+  double un[KR][NV];  // neighbour states of the current chunk
+  // gather the rows of chunk q (its indices are in stage s)
+  auto gather = [&](const LsqChunk& q, int s) {
+    const int kc = min(KR, nk_of(q.ll) - q.k0);
+    const bool act = q.ll < adm;
+    const int32_t* idx = (const int32_t*)(stage0 + (size_t)s * SB + KR * DH * 32 * sizeof(T));
+#pragma unroll
+    for (int r = 0; r < KR; ++r) {
+      const bool on = act && r < kc;
+      const int y = on ? idx[r * 32 + lane] : 0;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) un[r][v] = on ? U[(int64_t)y * NV + v] : 0.0;
+    }
+  };
+  if (issued > 0) {
+    wait_chunk(0);
+    if (ok) gather(cur, 0);
+  }
+  T acc[DH][NV];
+#pragma unroll
+  for (int j = 0; j < DH; ++j)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
+
+  for (int64_t i = 0; ok && cur.ll < amax; ++i) {
+    const int s = (int)(i % S);
+    const int nk = nk_of(cur.ll), nd = nd_of(cur.ll);
+    const int kc = min(KR, nk - cur.k0), dc = min(DH, nd - cur.d0);
+    const bool act = cur.ll < adm;
+    T du[KR][NV];
+#pragma unroll
+    for (int r = 0; r < KR; ++r)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) du[r][v] = T(un[r][v] - u0[v]);
+    // start the gathers of the next chunk
+    LsqChunk nx = cur;
+    next(nx);
+    if (nx.ll < amax) {
+      wait_chunk(i + 1);
+      if (!ok) break;
+      gather(nx, (int)((i + 1) % S));
+    }
+    const T* tab = (const T*)(stage0 + (size_t)s * SB);
+    if (act) {
+#pragma unroll
+      for (int r = 0; r < KR; ++r)
+        if (r < kc) {
+#pragma unroll
+          for (int j = 0; j < DH; ++j)
+            if (j < dc) {
+              const T m = tab[(r * dc + j) * 32 + lane];
+#pragma unroll
+              for (int v = 0; v < NV; ++v) acc[j][v] += m * du[r][v];
+            }
+        }
+    }
+    if (cur.k0 + kc >= nk) {  // last rows of this column pass: write G
+      if (live)
+#pragma unroll
+        for (int j = 0; j < DH; ++j)
+          if (j < dc)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              Gi[(int64_t)((cur.ll * ID + cur.d0 + j) * NV + v) * 32] = acc[j][v];
+              acc[j][v] = T(0);
+            }
+    }
+    // stage s is free again: refill it with chunk i + S
+    __syncwarp();
+    if (prod.ll < amax) {
+      if (lane == 0) {
+        fence_proxy_async();
+        issue(prod, s);
+      }
+      next(prod);
+      ++issued;
+    }
+    cur = nx;
+  }
+  if (!ok) {
+    // record the timeout and let the copies in flight land before leaving
+    if (lane == 0) atomicOr(p.health, HEALTH_TIMEOUT);
+    for (int64_t i = waited; i < issued; ++i) mbar_wait(&bar[i % S], (unsigned)((i / S) & 1));
+    return;
+  }
+  // stencils no lane of the group uses
+  if (live)
+    for (int ll = amax; ll < A; ++ll)
+      for (int j = 0; j < nd_of(ll); ++j)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + j) * NV + v) * 32] = T(0);
 }
 
 }  // namespace ucg
 
 namespace ucg {
 
+struct WPPlan {
+  int cpc;
+  int o_G, o_g1, o_S, o_tmp, o_gh, o_w, o_dul, o_u0, o_bnd, o_slope, o_flag, total;
+};
+
+template <typename T>
+inline WPPlan wpost_plan(int cpc, int A, int ID, int ID2, int QS, bool cw, int istride) {
+  WPPlan w{};
+  w.cpc = cpc;
+  const int s = (int)sizeof(T);
+  int off = 0;
+  auto take = [&](int bytes) {
+    int o = off;
+    off += (bytes + 15) / 16 * 16;
+    return o;
+  };
+  w.o_G = take(cpc * A * ID * NV * s);
+  w.o_g1 = take(cw ? cpc * ID * NV * s : 0);
+  w.o_S = take(cpc * istride * s);
+  int tmp = cpc * A * ID * NV * s, psi = cpc * MF * QS * NV * 8;
+  w.o_tmp = take(tmp > psi ? tmp : psi);  // indicator partials, later the limiter values
+  w.o_gh = take(cpc * ID * NV * s);
+  w.o_w = take(cpc * A * NV * 8);
+  w.o_dul = take(cpc * MF * QS * NV * s);
+  w.o_u0 = take(cpc * NV * 8);
+  w.o_bnd = take(cpc * 2 * NV * 8);
+  w.o_slope = take(cpc * NV * 8);
+  w.o_flag = take(cpc * 2 * 4);
+  w.total = off;
+  return w;
+}
+
 template <int P, typename T>
-__global__ void __launch_bounds__(W2_THREADS, 2) k_weno2(Problem p, const double* __restrict__ U, W2Plan w) {
+__global__ void __launch_bounds__(256) k_wpost(Problem p, const double* __restrict__ U, WPPlan w) {
   constexpr int ID = Deg<P>::ideg;
-  const int A = p.admis_max, IM = p.imax, W = IM + 1;
+  const int A = p.admis_max;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
   const bool cw = p.ees == 5;
   const bool weno = p.scheme == 3;
-  const int ID2 = p.ideg2, IM2 = p.imax2;
-  const int tid = threadIdx.x;
-  const int64_t c = blockIdx.x;
-  extern __shared__ __align__(128) unsigned char sm[];
-  uint64_t* bar = (uint64_t*)(sm + w.o_bar);  // [0],[1] ring slots, [2] smoothness block
-  T* s_S = (T*)(sm + w.o_S);
-  T* s_du = (T*)(sm + w.o_du);
-  T* s_part = (T*)(sm + w.o_part);
-  double* s_psi = (double*)(sm + w.o_psi);
+  const int ID2 = p.ideg2;
+  const int cpc = w.cpc, tid = threadIdx.x, NT = blockDim.x;
+  const int64_t c0 = (int64_t)blockIdx.x * cpc;
+  const int nc = (int)((p.n - c0) < cpc ? (p.n - c0) : cpc);
+  extern __shared__ __align__(16) unsigned char sm[];
   T* s_G = (T*)(sm + w.o_G);
   T* s_g1 = (T*)(sm + w.o_g1);
+  T* s_S = (T*)(sm + w.o_S);
+  T* s_tmp = (T*)(sm + w.o_tmp);
+  double* s_psi = (double*)(sm + w.o_tmp);
   T* s_gh = (T*)(sm + w.o_gh);
   double* s_w = (double*)(sm + w.o_w);
   T* s_dul = (T*)(sm + w.o_dul);
@@ -117,165 +404,46 @@ __global__ void __launch_bounds__(W2_THREADS, 2) k_weno2(Problem p, const double
   double* s_bnd = (double*)(sm + w.o_bnd);
   double* s_slope = (double*)(sm + w.o_slope);
   int* s_flag = (int*)(sm + w.o_flag);
-  int32_t* s_sten = (int32_t*)(sm + w.o_sten);
 
-  const int adm = p.admis[c];
-  const char* tab = (const char*)p.invmat + (size_t)c * p.tstride * sizeof(T);
-  // stream items: (slice, chunk) in order
-  int it_ll[W2_MAXITEM], it_r0[W2_MAXITEM], it_r1[W2_MAXITEM];
-  int nitem = 0;
-  for (int ll = 0; ll < adm; ++ll) {
-    int nk = (cw && ll > 0) ? IM2 : IM;
-    for (int j = 0; j < w.nch[ll]; ++j) {
-      it_ll[nitem] = ll;
-      it_r0[nitem] = j * w.rc[ll];
-      it_r1[nitem] = (j + 1 == w.nch[ll]) ? nk : (j + 1) * w.rc[ll];
-      ++nitem;
-    }
+  const int GS = A * ID * NV;
+  const T* Gi = (const T*)p.gbuf;
+  for (int i = tid; i < nc * NV; i += NT) s_u0[i] = U[c0 * NV + i];
+  for (int i = tid; i < nc * 2; i += NT) s_flag[i] = 0;
+  // stencil polynomials: consecutive threads read consecutive cells (lanes)
+  for (int i = tid; i < nc * GS; i += NT) {
+    int r = i / nc, cl = i - r * nc;
+    int64_t c = c0 + cl;
+    s_G[cl * GS + r] = Gi[((c >> 5) * GS + r) * 32 + (c & 31)];
   }
-  auto item_src = [&](int it, unsigned& bytes) -> const char* {
-    int ll = it_ll[it];
-    int nd = (cw && ll > 0) ? ID2 : ID;
-    int rb = nd * (int)sizeof(T);
-    int off = it_r0[it] * rb;
-    bytes = (it_r1[it] == ((cw && ll > 0) ? IM2 : IM)) ? (unsigned)(p.sbytes[ll] - off) : (unsigned)((it_r1[it] - it_r0[it]) * rb);
-    return tab + (size_t)p.soff[ll] * sizeof(T) + off;
-  };
-  auto issue = [&](int it) {
-    unsigned bytes;
-    const char* src = item_src(it, bytes);
-    int slot = it & 1;
-    mbar_expect_tx(&bar[slot], bytes);
-    bulk_g2s(sm + w.o_slot + slot * w.slot_bytes, src, bytes, &bar[slot]);
-  };
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    mbar_init(&bar[2], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  if (tid == 0) {
-    if (weno) {
-      mbar_expect_tx(&bar[2], (unsigned)p.ibytes);
-      bulk_g2s(s_S, (const char*)p.ind + (size_t)c * p.istride * sizeof(T), (unsigned)p.ibytes, &bar[2]);
-    }
-    if (nitem > 0) issue(0);
-    if (nitem > 1) issue(1);
-  }
-  // own state and stencil indices
-  if (tid < NV) s_u0[tid] = U[c * NV + tid];
-  for (int i = tid; i < A * W; i += W2_THREADS) s_sten[i] = p.sten[c * A * W + i];
-  if (tid < 2) s_flag[tid] = 0;
-  __syncthreads();
-  // gather U_k - U_i for every stencil cell (FP64 difference, rounded to T)
-  for (int i = tid; i < adm * IM; i += W2_THREADS) {
-    int ll = i / IM, k = i - ll * IM;
-    int nk = (cw && ll > 0) ? IM2 : IM;
-    T* o = s_du + (size_t)i * NV;
-    if (k < nk) {
-      const double* uy = U + (int64_t)s_sten[ll * W + k + 1] * NV;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) o[v] = T(uy[v] - s_u0[v]);
-    }
-  }
-  __syncthreads();
-
-  // ---- least squares, slice by slice as the chunks arrive
-  bool ok = true;
-  const int DB = w.db, KP = w.kp;
-  for (int it = 0; it < nitem; ++it) {
-    const int ll = it_ll[it];
-    const bool low = cw && ll > 0;
-    const int nd = low ? ID2 : ID;
-    const int ndb = (nd + DB - 1) / DB;
-    const int slot = it & 1;
-    if (!mbar_wait(&bar[slot], (it >> 1) & 1)) ok = false;
-    const T* M = (const T*)(sm + w.o_slot + slot * w.slot_bytes) - it_r0[it] * nd;  // row-indexed
-    const int db = tid % ndb, kp = tid / ndb;
-    const bool first_chunk = it == 0 || it_ll[it - 1] != ll;
-    const bool last_chunk = it + 1 == nitem || it_ll[it + 1] != ll;
-    if (kp < KP) {
-      T acc[4][NV];
-      // partial sums of this slice live in s_part between chunks
-      if (first_chunk) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-          for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-          for (int v = 0; v < NV; ++v)
-            acc[j][v] = j < DB ? s_part[((size_t)kp * ndb * DB + db * DB + j) * NV + v] : T(0);
-      }
-      const T* du = s_du + (size_t)ll * IM * NV;
-      for (int k = it_r0[it] + kp; k < it_r1[it]; k += KP) {
-        T dv[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) dv[v] = du[k * NV + v];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          int d = db * DB + j;
-          if (j < DB && d < nd) {
-            T m = M[k * nd + d];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) acc[j][v] += m * dv[v];
-          }
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < DB)
-#pragma unroll
-          for (int v = 0; v < NV; ++v) s_part[((size_t)kp * ndb * DB + db * DB + j) * NV + v] = acc[j][v];
-    }
-    __syncthreads();  // slot consumed, partials written
-    if (tid == 0 && it + 2 < nitem) {
-      fence_proxy_async();
-      issue(it + 2);
-    }
-    if (last_chunk) {
-      // G[ll][d][v] = sum over row partitions, in partition order
-      const int npart = KP < ((low ? IM2 : IM)) ? KP : (low ? IM2 : IM);
-      for (int i = tid; i < ID * NV; i += W2_THREADS) {
-        int d = i / NV, v = i - d * NV;
-        T s = T(0);
-        if (d < nd)
-          for (int q = 0; q < npart; ++q) s += s_part[((size_t)q * ndb * DB + d) * NV + v];
-        s_G[((size_t)ll * ID + d) * NV + v] = s;
-      }
-      __syncthreads();
-    }
-  }
-  if (!ok) atomicOr(p.health, HEALTH_TIMEOUT);
-
-  T* s_tmp = s_part;  // [A][ID][NV] scratch for the indicator reduction
   if (weno) {
-    if (!mbar_wait(&bar[2], 0)) atomicOr(p.health, HEALTH_TIMEOUT);
-    // CWENO: central polynomial with the low-order stencils removed (reconstruct_p.f90:956-965)
-    if (cw) {
-      const double lc1 = 1.0 - 1.0 / p.lwci;
-      const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-      for (int i = tid; i < ID * NV; i += W2_THREADS) {
-        int d = i / NV, v = i - d * NV;
+    const T* IND = (const T*)p.ind + c0 * p.istride;
+    for (int i = tid; i < nc * (int)p.istride; i += NT) s_S[i] = IND[i];
+  }
+  __syncthreads();
+
+  if (weno) {
+    if (cw) {  // central polynomial with the low-order stencils removed (reconstruct_p.f90:956-965)
+      for (int i = tid; i < nc * ID * NV; i += NT) {
+        int cl = i / (ID * NV), r = i - cl * ID * NV, d = r / NV, v = r - d * NV;
+        int adm = p.admis[c0 + cl];
+        const double lc1 = 1.0 - 1.0 / p.lwci;
+        const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
         T g3 = T(0);
         if (d < ID2)
-          for (int ll = 1; ll < adm; ++ll) g3 = g3 + T(lk) * s_G[((size_t)ll * ID + d) * NV + v];
-        s_g1[i] = T(1.0 / lc1) * (s_G[(size_t)d * NV + v] - g3);
+          for (int ll = 1; ll < adm; ++ll) g3 = g3 + T(lk) * s_G[cl * GS + (ll * ID + d) * NV + v];
+        s_g1[i] = T(1.0 / lc1) * (s_G[cl * GS + d * NV + v] - g3);
       }
       __syncthreads();
     }
-    // IS = g^T S g: thread (ll, e) forms (S g)_e g_e for the five variables
-    for (int i = tid; i < adm * ID; i += W2_THREADS) {
-      int ll = i / ID, e = i - ll * ID;
+    // IS = g^T S g: thread (cell, ll, e) forms (S g)_e g_e for the five variables
+    for (int i = tid; i < nc * A * ID; i += NT) {
+      int cl = i / (A * ID), r = i - cl * A * ID, ll = r / ID, e = r - ll * ID;
       bool low = cw && ll > 0;
       int nd = low ? ID2 : ID;
       T t[NV] = {T(0), T(0), T(0), T(0), T(0)};
-      if (e < nd) {
-        const T* S = low ? s_S + p.i2off : s_S;
-        const T* g = (cw && ll == 0) ? s_g1 : s_G + (size_t)ll * ID * NV;
+      if (ll < p.admis[c0 + cl] && e < nd) {
+        const T* S = s_S + cl * (int)p.istride + (low ? p.i2off : 0);
+        const T* g = (cw && ll == 0) ? s_g1 + cl * ID * NV : s_G + cl * GS + ll * ID * NV;
         T acc[NV] = {T(0), T(0), T(0), T(0), T(0)};
         for (int d = 0; d < nd; ++d) {
           T sde = S[d * nd + e];
@@ -289,17 +457,19 @@ __global__ void __launch_bounds__(W2_THREADS, 2) k_weno2(Problem p, const double
       for (int v = 0; v < NV; ++v) s_tmp[(size_t)i * NV + v] = t[v];
     }
     __syncthreads();
-    for (int i = tid; i < adm * NV; i += W2_THREADS) {
-      int ll = i / NV, v = i - ll * NV;
+    for (int i = tid; i < nc * A * NV; i += NT) {
+      int cl = i / (A * NV), r = i - cl * A * NV, ll = r / NV, v = r - ll * NV;
       int nd = (cw && ll > 0) ? ID2 : ID;
       T is = T(0);
-      for (int e = 0; e < nd; ++e) is += s_tmp[((size_t)ll * ID + e) * NV + v];
-      s_w[ll * NV + v] = (double)is;
+      for (int e = 0; e < nd; ++e) is += s_tmp[((size_t)(cl * A + ll) * ID + e) * NV + v];
+      s_w[i] = (double)is;
     }
     __syncthreads();
     // nonlinear weights in FP64 ((10E-12)^4 underflows FP32)
-    if (tid < NV) {
-      const int v = tid;
+    for (int i = tid; i < nc * NV; i += NT) {
+      int cl = i / NV, v = i - cl * NV;
+      int adm = p.admis[c0 + cl];
+      double* ws = s_w + cl * A * NV;
       double lam0, lamk;
       if (cw) {
         lam0 = 1.0 - 1.0 / p.lwci;
@@ -310,11 +480,11 @@ __global__ void __launch_bounds__(W2_THREADS, 2) k_weno2(Problem p, const double
       }
       double tau = 0.0, sum = 0.0;
       if (cw && p.wenoz) {
-        for (int ll = 0; ll < adm; ++ll) tau += fabs(s_w[v] - s_w[ll * NV + v]);
+        for (int ll = 0; ll < adm; ++ll) tau += fabs(ws[v] - ws[ll * NV + v]);
         tau = tau / (adm - 1);
       }
       for (int ll = 0; ll < adm; ++ll) {
-        double e = p.weno_eps + s_w[ll * NV + v];
+        double e = p.weno_eps + ws[ll * NV + v];
         double lam = ll == 0 ? lam0 : lamk, wt;
         if (cw && p.wenoz) {
           double q = tau / e;
@@ -324,124 +494,143 @@ __global__ void __launch_bounds__(W2_THREADS, 2) k_weno2(Problem p, const double
           double e2 = e * e;
           wt = lam / (e2 * e2);
         }
-        s_w[ll * NV + v] = wt;
+        ws[ll * NV + v] = wt;
         sum += wt;
       }
-      for (int ll = 0; ll < adm; ++ll) s_w[ll * NV + v] = s_w[ll * NV + v] / sum;
+      for (int ll = 0; ll < adm; ++ll) ws[ll * NV + v] = ws[ll * NV + v] / sum;
     }
     __syncthreads();
     // combined polynomial
-    for (int i = tid; i < ID * NV; i += W2_THREADS) {
-      int d = i / NV, v = i - d * NV;
-      const T* g0 = cw ? s_g1 : s_G;
-      T acc = T(s_w[v]) * g0[d * NV + v];
+    for (int i = tid; i < nc * ID * NV; i += NT) {
+      int cl = i / (ID * NV), r = i - cl * ID * NV, d = r / NV, v = r - d * NV;
+      int adm = p.admis[c0 + cl];
+      const double* ws = s_w + cl * A * NV;
+      const T* g0 = cw ? s_g1 + cl * ID * NV : s_G + cl * GS;
+      T acc = T(ws[v]) * g0[d * NV + v];
       for (int ll = 1; ll < adm; ++ll)
-        if (!cw || d < ID2) acc += T(s_w[ll * NV + v]) * s_G[((size_t)ll * ID + d) * NV + v];
+        if (!cw || d < ID2) acc += T(ws[ll * NV + v]) * s_G[cl * GS + (ll * ID + d) * NV + v];
       s_gh[i] = acc;
     }
     __syncthreads();
   }
 
   // ---- face values and CHECKSOL
-  const T* QP = (const T*)p.qpts + (size_t)c * MF * QS * 3;
-  const T* BM = (const T*)p.bmean + (size_t)c * ID;
-  const int nfc = p.nfaces[c];
-  const bool full = p.full[c] != 0;
-  for (int i = tid; i < MF * QS; i += W2_THREADS) {
-    int f = i / QS, q = i - f * QS;
+  const T* QPa = (const T*)p.qpts;
+  const T* BMa = (const T*)p.bmean;
+  const int FQ = MF * QS;
+  for (int i = tid; i < nc * FQ; i += NT) {
+    int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
+    int64_t c = c0 + cl;
     T* o = s_dul + (size_t)i * NV;
 #pragma unroll
     for (int v = 0; v < NV; ++v) o[v] = T(0);
-    if (f >= nfc || q >= face_nq(p, p.ftype[c * MF + f])) continue;
-    if (!weno || !full) {  // MUSCL everywhere / CHECKSOL: FULL = 0 -> REDUCE
-      s_flag[0] = 1;
+    if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) continue;
+    if (!weno || !p.full[c]) {  // MUSCL everywhere / CHECKSOL: FULL = 0 -> REDUCE
+      s_flag[cl * 2] = 1;
       continue;
     }
+    const T* xi = QPa + ((size_t)c * FQ + j) * 3;
     T b[ID];
-    monomials<P, T>(QP[i * 3 + 0], QP[i * 3 + 1], QP[i * 3 + 2], b);
+    monomials<P, T>(xi[0], xi[1], xi[2], b);
 #pragma unroll
-    for (int d = 0; d < ID; ++d) b[d] -= BM[d];
+    for (int d = 0; d < ID; ++d) b[d] -= BMa[c * ID + d];
+    const T* gh = s_gh + cl * ID * NV;
     double uf[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       T res = T(0);
 #pragma unroll
-      for (int d = 0; d < ID; ++d) res += b[d] * s_gh[d * NV + v];
+      for (int d = 0; d < ID; ++d) res += b[d] * gh[d * NV + v];
       o[v] = res;
-      uf[v] = s_u0[v] + (double)res;
+      uf[v] = s_u0[cl * NV + v] + (double)res;
     }
     double pm[NV];
-    cons2prim(p.gamma, s_u0, pm);
-    if (jump_bad(p.gamma, pm, uf, 0.85)) s_flag[0] = 1;
+    cons2prim(p.gamma, s_u0 + cl * NV, pm);
+    if (jump_bad(p.gamma, pm, uf, 0.85)) s_flag[cl * 2] = 1;
   }
   __syncthreads();
-
-  // ---- MUSCL with the central stencil polynomial on flagged cells
-  if (s_flag[0]) {
-    if (tid < NV) {
-      const int v = tid;
-      double u0 = s_u0[v], mn = u0, mx = u0;
-      for (int f = 0; f < nfc; ++f) {
+  const int any = __syncthreads_or((tid < nc) ? s_flag[tid * 2] : 0);
+  if (any) {
+    // ---- MUSCL with the central stencil polynomial on flagged cells
+    for (int i = tid; i < nc * NV; i += NT) {
+      int cl = i / NV, v = i - cl * NV;
+      if (!s_flag[cl * 2]) continue;
+      int64_t c = c0 + cl;
+      double u0 = s_u0[i], mn = u0, mx = u0;
+      for (int f = 0; f < p.nfaces[c]; ++f) {
         int64_t nb = p.neigh[c * MF + f];
         if (nb < 0) continue;
         double un = U[nb * NV + v];
         mn = fmin(mn, un);
         mx = fmax(mx, un);
       }
-      s_bnd[v] = mn - u0;
-      s_bnd[NV + v] = mx - u0;
+      s_bnd[(cl * 2 + 0) * NV + v] = mn - u0;
+      s_bnd[(cl * 2 + 1) * NV + v] = mx - u0;
     }
     __syncthreads();
-    const double e3 = p.kappa_ven * p.minedge[c];
-    const double epsi2 = e3 * e3 * e3;
-    for (int i = tid; i < MF * QS; i += W2_THREADS) {
-      int f = i / QS, q = i - f * QS;
+    for (int i = tid; i < nc * FQ; i += NT) {
+      int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
+      if (!s_flag[cl * 2]) continue;
+      int64_t c = c0 + cl;
       double* ps = s_psi + (size_t)i * NV;
-      if (f >= nfc || q >= face_nq(p, p.ftype[c * MF + f])) {
+      if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) ps[v] = TOLBIG;
         continue;
       }
+      const T* xi = QPa + ((size_t)c * FQ + j) * 3;
       T b[ID];
-      monomials<P, T>(QP[i * 3 + 0], QP[i * 3 + 1], QP[i * 3 + 2], b);
+      monomials<P, T>(xi[0], xi[1], xi[2], b);
 #pragma unroll
-      for (int d = 0; d < ID; ++d) b[d] -= BM[d];
+      for (int d = 0; d < ID; ++d) b[d] -= BMa[c * ID + d];
+      const T* g0 = s_G + cl * GS;
+      const double e3 = p.kappa_ven * p.minedge[c];
+      const double epsi2 = e3 * e3 * e3;
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         T res = T(0);
 #pragma unroll
-        for (int d = 0; d < ID; ++d) res += b[d] * s_G[d * NV + v];
-        double dd = (s_u0[v] + (double)res) - s_u0[v];
+        for (int d = 0; d < ID; ++d) res += b[d] * g0[d * NV + v];
+        double u0 = s_u0[cl * NV + v];
+        double dd = (u0 + (double)res) - u0;
         s_dul[(size_t)i * NV + v] = T(dd);
-        ps[v] = venkat(dd, s_bnd[v], s_bnd[NV + v], epsi2);
+        ps[v] = venkat(dd, s_bnd[(cl * 2 + 0) * NV + v], s_bnd[(cl * 2 + 1) * NV + v], epsi2);
       }
     }
     __syncthreads();
-    if (tid < NV) {
+    for (int i = tid; i < nc * NV; i += NT) {
+      int cl = i / NV, v = i - cl * NV;
+      if (!s_flag[cl * 2]) continue;
       double mn = TOLBIG;
-      for (int j = 0; j < MF * QS; ++j) mn = fmin(mn, s_psi[(size_t)j * NV + tid]);
-      s_slope[tid] = mn;
+      for (int j = 0; j < FQ; ++j) mn = fmin(mn, s_psi[((size_t)cl * FQ + j) * NV + v]);
+      s_slope[i] = mn;
     }
     __syncthreads();
-    for (int i = tid; i < MF * QS * NV; i += W2_THREADS)
-      s_dul[i] = T((double)s_dul[i] * s_slope[i % NV]);
+    for (int i = tid; i < nc * FQ * NV; i += NT) {
+      int cl = i / (FQ * NV);
+      if (!s_flag[cl * 2]) continue;
+      s_dul[i] = T((double)s_dul[i] * s_slope[cl * NV + i % NV]);
+    }
     __syncthreads();
   }
 
   // ---- CHECKSOLX: first order where a face value jumps by 95 %
-  for (int i = tid; i < MF * QS; i += W2_THREADS) {
-    int f = i / QS, q = i - f * QS;
-    if (f >= nfc || q >= face_nq(p, p.ftype[c * MF + f])) continue;
+  for (int i = tid; i < nc * FQ; i += NT) {
+    int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
+    int64_t c = c0 + cl;
+    if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) continue;
     double uf[NV], pm[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) uf[v] = s_u0[v] + (double)s_dul[(size_t)i * NV + v];
-    cons2prim(p.gamma, s_u0, pm);
-    if (jump_bad(p.gamma, pm, uf, 0.95)) s_flag[1] = 1;
+    for (int v = 0; v < NV; ++v) uf[v] = s_u0[cl * NV + v] + (double)s_dul[(size_t)i * NV + v];
+    cons2prim(p.gamma, s_u0 + cl * NV, pm);
+    if (jump_bad(p.gamma, pm, uf, 0.95)) s_flag[cl * 2 + 1] = 1;
   }
   __syncthreads();
-  T* out = (T*)p.dul + (size_t)c * MF * QS * NV;
-  const bool first = s_flag[1] != 0;
-  for (int i = tid; i < MF * QS * NV; i += W2_THREADS) out[i] = first ? T(0) : s_dul[i];
+  T* out = (T*)p.dul + c0 * FQ * NV;
+  for (int i = tid; i < nc * FQ * NV; i += NT) {
+    int cl = i / (FQ * NV);
+    out[i] = s_flag[cl * 2 + 1] ? T(0) : s_dul[i];
+  }
 }
 
 }  // namespace ucg
