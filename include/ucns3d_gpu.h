@@ -191,6 +191,34 @@ int64_t ucg_launch_count(const ucg_engine* e);
 int64_t ucg_device_bytes(const ucg_engine* e);
 
 int ucg_last_error(const ucg_engine* e, char* buf, int32_t len);
+
+/* Residual of a MUSCL configuration (scheme 2, iorder 1: Euler or
+ * Navier-Stokes) that allocates no memory at all.  No counterpart in the
+ * reference.  It is for callers that cannot call cudaMalloc: code that only
+ * receives buffers from its own caller (a plug-in inside a host application
+ * that owns the device pool), runs where the allocator is locked or
+ * unavailable, or must not grow the process's device footprint.  Such a
+ * caller passes everything in device-accessible memory: `geo` and `rec`
+ * hold device pointers to the arrays of the layouts documented above (all
+ * cells, first = 0), `u` is the state [n][5] and `rhs` receives RHS(I)%VAL
+ * [n][5]; the work is queued on `stream` (a cudaStream_t, NULL = the default
+ * stream) and the call returns without synchronising.
+ * Scratch: the face values (and, for Navier-Stokes, the face gradients) live
+ * in one fixed 64 MiB device array inside this library, which every GPU that
+ * loads the library holds until the process exits; meshes of more than
+ * 279,620 cells (Euler) or 82,241 cells (Navier-Stokes) are rejected with
+ * UCG_EINVAL.  Every call writes all the scratch it later reads, so nothing
+ * needs clearing, but all calls in the process share the array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Indices read from `geo` and `rec` on the device are
+ * bounds-checked, not followed: a cell with an index out of range gets a NaN
+ * row in rhs (and so may its face neighbours).  Returns UCG_OK, UCG_EINVAL
+ * (unsupported configuration, NULL argument or too many cells) or
+ * UCG_ECUDA.                                                              */
+int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, const ucg_recon* rec,
+                              const double* u, double* rhs, void* stream);
 /* Message of the last failure of ucg_create (no handle exists then). */
 const char* ucg_create_error(void);
 

@@ -48,13 +48,13 @@ def build_prep(force=False):
 
 def build_engine(force=False, extra=()):
     d = os.path.join(PKG, "csrc", "engine")
-    srcs = [os.path.join(d, f) for f in ("engine.cu", "kernels.cuh", "recon2.cuh", "device.cuh")]
+    srcs = [os.path.join(d, f) for f in ("engine.cu", "kernels.cuh", "recon2.cuh", "device.cuh", "static_scratch.cu")]
     srcs.append(os.path.join(INC, "ucns3d_gpu.h"))
     out = os.path.join(LIB, "libucns3d_gpu.so")
     if force or _stale(out, srcs):
         os.makedirs(LIB, exist_ok=True)
         _run([NVCC, *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-shared", "-I", INC, *extra, os.path.join(d, "engine.cu"), "-o", out])
+              "-shared", "-I", INC, *extra, os.path.join(d, "engine.cu"), os.path.join(d, "static_scratch.cu"), "-o", out])
     return out
 
 
