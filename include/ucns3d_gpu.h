@@ -179,8 +179,10 @@ int ucg_synchronize(ucg_engine* e);
 
 /* Average device time of the stage kernels over `reps` residual
  * evaluations of the current state, measured with CUDA events on the
- * handle's stream: ms[0] reconstruction, ms[1] face fluxes, ms[2] time step
- * (CALCULATE_CFL).  For profiling; it leaves the state unchanged.          */
+ * handle's stream, into ms[4]: ms[0] reconstruction, ms[1] face fluxes,
+ * ms[2] time step (CALCULATE_CFL), ms[3] the stencil least-squares kernel
+ * alone (part of ms[0]; all of it for MUSCL IORDER 1).  For profiling; it
+ * leaves the state unchanged.                                              */
 int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms);
 
 /* The cudaStream_t of the handle, as an opaque pointer. */

@@ -53,13 +53,13 @@ struct Problem {
   const int32_t* sten;
   const void* invmat;
   int64_t tstride;
-  int soff[8], sbytes[8];
-  // smoothness matrices: one block of `istride` elements per cell, S
-  // [ideg][ideg] at 0 and the CWENO S2 [ideg2][ideg2] at i2off; `ibytes`
-  // is the padded size of the block
+  int soff[8];
+  // smoothness matrices, interleaved the same way with len = `istride`:
+  // packed upper triangle of S [ideg][ideg] at element 0 and of the CWENO
+  // S2 [ideg2][ideg2] at i2off, off-diagonal entries S_de + S_ed
   const void* ind;
   int64_t istride;
-  int i2off, ibytes;
+  int i2off;
   // scratch
   void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the tables
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)

@@ -28,8 +28,8 @@ struct DevBuf {
 // Device layout of the per-cell table blocks (see Problem in device.cuh).
 struct Layout {
   int64_t tstride = 0, istride = 0;
-  int soff[8] = {0}, sbytes[8] = {0};
-  int i2off = 0, ibytes = 0;
+  int soff[8] = {0};
+  int i2off = 0;
 };
 
 struct ucg_engine {
@@ -53,6 +53,7 @@ struct ucg_engine {
   // scratch and state
   DevBuf gbuf, dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux;
   int64_t nown = 0;
+  cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs
   std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
   std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
 };
@@ -163,10 +164,8 @@ Problem make_problem(ucg_engine* e) {
   p.tstride = e->layout.tstride;
   p.istride = e->layout.istride;
   p.i2off = e->layout.i2off;
-  p.ibytes = e->layout.ibytes;
   for (int k = 0; k < 8; ++k) {
     p.soff[k] = e->layout.soff[k];
-    p.sbytes[k] = e->layout.sbytes[k];
   }
   p.gbuf = e->gbuf.p;
   p.dul = e->dul.p;
@@ -185,38 +184,6 @@ Problem make_problem(ucg_engine* e) {
 bool ready(ucg_engine* e) { return e->have_geometry && e->recon_cells == e->n; }
 
 // ------------------------------------------------------------ launching
-template <int P, typename T>
-int launch_weno(ucg_engine* e, const Problem& p, const double* U) {
-  const ucg_config& c = e->cfg;
-  const bool cw = c.ees == 5;
-#if UCG_LSQ_BULK
-  {
-    const LsqBulkPlan pl = lsq_bulk_plan<P, T>(3);
-    CK(cudaFuncSetAttribute(k_lsq_bulk<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.total));
-    const int64_t ngrp = (e->n + 31) / 32;
-    k_lsq_bulk<P, T><<<(unsigned)((ngrp + pl.nw - 1) / pl.nw), pl.nw * 32, pl.total, e->stream>>>(p, U, pl);
-  }
-#else
-  k_lsq<P, T><<<(unsigned)((e->n + 127) / 128), 128, 0, e->stream>>>(p, U);
-#endif
-  int cpc = 512 / (c.admis_max * c.ideg);
-  cpc = cpc < 1 ? 1 : (cpc > 16 ? 16 : cpc);
-  WPPlan w = wpost_plan<T>(cpc, c.admis_max, c.ideg, c.ideg2, e->QS, cw, (int)e->layout.istride);
-  while (cpc > 1 && w.total > 64 * 1024) w = wpost_plan<T>(--cpc, c.admis_max, c.ideg, c.ideg2, e->QS, cw, (int)e->layout.istride);
-  if (w.total > 200 * 1024) return fail(e, UCG_EINVAL, "reconstruction does not fit in shared memory");
-  CK(cudaFuncSetAttribute(k_wpost<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, w.total));
-  k_wpost<P, T><<<(unsigned)((e->n + cpc - 1) / cpc), 256, w.total, e->stream>>>(p, U, w);
-  e->launches += 2;
-  if (c.governing == 1) {
-    k_visc_lsq<P, T><<<(unsigned)((e->n * 4 + 127) / 128), 128, 0, e->stream>>>(p, U);
-    int64_t nf = e->n * MF * e->QS;
-    k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, e->stream>>>(p);
-    e->launches += 2;
-  }
-  CK(cudaGetLastError());
-  return UCG_OK;
-}
-
 template <typename T>
 int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
   const ucg_config& c = e->cfg;
@@ -228,13 +195,11 @@ int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
     CK(cudaGetLastError());
     return UCG_OK;
   }
-  switch (c.iorder) {
-    case 1: return launch_weno<1, T>(e, p, U);
-    case 2: return launch_weno<2, T>(e, p, U);
-    case 3: return launch_weno<3, T>(e, p, U);
-    case 4: return launch_weno<4, T>(e, p, U);
-  }
-  return fail(e, UCG_EINVAL, "iorder out of range");
+  if (c.iorder < 1 || c.iorder > 4) return fail(e, UCG_EINVAL, "iorder out of range");
+  const bool ns = c.governing == 1;
+  CK(sizeof(T) == 4 ? launch_weno_f32(c.iorder, p, U, ns, e->QS, e->stream, &e->launches, e->mark)
+                    : launch_weno_f64(c.iorder, p, U, ns, e->QS, e->stream, &e->launches, e->mark));
+  return UCG_OK;
 }
 
 int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
@@ -308,10 +273,10 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
                   (c.governing == 1 || c.governing == 2) && (c.precision == UCG_FP64 || c.precision == UCG_MIXED);
   int ideg = (c.iorder + 1) * (c.iorder + 2) * (c.iorder + 3) / 6 - 1;
   if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
-      c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && (c.ideg2 < 1 || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
+      c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && ((c.ideg2 != 3 && c.ideg2 != 9) || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
       c.gamma <= 1.0 || c.limiter != 7 || c.riemann != 1 || c.wenwrt != 1) {
     g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC, limiter 7, "
-                   "conserved-variable WENO)";
+                   "conserved-variable WENO, CWENO lower-order degree 3 or 9)";
     return UCG_EINVAL;
   }
   if (c.scheme == 2 && c.admis_max != 1) {
@@ -346,13 +311,13 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
       bool low = c.ees == 5 && ll > 0;
       int64_t el = low ? (int64_t)c.imax2 * c.ideg2 : (int64_t)c.imax * c.ideg;
       L.soff[ll] = (int)off;
-      L.sbytes[ll] = (int)(up(el) * ts);
       off += up(el);
     }
     L.tstride = off;
-    L.i2off = (int)up((int64_t)c.ideg * c.ideg);
-    L.istride = L.i2off + (c.ees == 5 ? up((int64_t)c.ideg2 * c.ideg2) : 0);
-    L.ibytes = (int)(L.istride * ts);
+    // smoothness matrices: packed upper triangles (S and the CWENO S2)
+    auto tri = [](int64_t m) { return m * (m + 1) / 2; };
+    L.i2off = (int)up(tri(c.ideg));
+    L.istride = L.i2off + (c.ees == 5 ? up(tri(c.ideg2)) : 0);
   }
   cudaSetDevice(device);
   st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
@@ -558,7 +523,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   const int64_t ngrp = (n + 31) / 32;
   rc = rc ? rc : alloc(e, e->sten, (size_t)ngrp * 32 * A * W * 4);
   rc = rc ? rc : alloc(e, e->invmat, (size_t)ngrp * 32 * Ly.tstride * T);
-  if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)n * Ly.istride * T);
+  if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)ngrp * 32 * Ly.istride * T);
   if (rc) return rc;
   {
     // stencils: staged per cell, interleaved on the device
@@ -593,11 +558,17 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       for (int j = 0; j < nk * nd; ++j) dst[Ly.soff[ll] + j] = src[j];
     }
   };
+  // upper triangle row by row; off-diagonal entries hold S_de + S_ed, so the
+  // packed form gives the same quadratic form as the full matrix
+  auto pack_tri = [](const double* S, int m, double* dst) {
+    int j = 0;
+    for (int d = 0; d < m; ++d)
+      for (int k = d; k < m; ++k) dst[j++] = k == d ? S[d * m + d] : S[d * m + k] + S[k * m + d];
+  };
   auto pack_ind = [&](int64_t t, double* dst) {
     for (int64_t j = 0; j < Ly.istride; ++j) dst[j] = 0.0;
-    for (int j = 0; j < ideg * ideg; ++j) dst[j] = r->indicator[t * ideg * ideg + j];
-    if (cw)
-      for (int j = 0; j < ideg2 * ideg2; ++j) dst[Ly.i2off + j] = r->indicator2[t * ideg2 * ideg2 + j];
+    pack_tri(r->indicator + t * ideg * ideg, ideg, dst);
+    if (cw) pack_tri(r->indicator2 + t * ideg2 * ideg2, ideg2, dst + Ly.i2off);
   };
   struct Part {
     int64_t len;
@@ -628,17 +599,11 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       int64_t total = count * pt.len;
       unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
       const double* sp = (const double*)e->staging.p;
-      if (pt.which == 0) {  // pseudo-inverses: interleaved over 32-cell groups
-        if (e->mixed)
-          k_expand_il<float, double><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
-        else
-          k_expand_il<double, double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
-      } else {  // smoothness matrices: one contiguous block per cell
-        if (e->mixed)
-          k_expand<float><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
-        else
-          k_expand<double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
-      }
+      // pseudo-inverses and smoothness matrices: interleaved over 32-cell groups
+      if (e->mixed)
+        k_expand_il<float, double><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      else
+        k_expand_il<double, double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
       e->launches++;
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(e->stream));
@@ -771,13 +736,16 @@ int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   cudaSetDevice(e->device);
   Problem p = make_problem(e);
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[5];
   for (auto& x : ev) CK(cudaEventCreate(&x));
-  double acc[3] = {0, 0, 0};
+  double acc[4] = {0, 0, 0, 0};
   int rc = UCG_OK;
+  const bool split = !(e->cfg.scheme == 2 && e->cfg.iorder == 1);  // k_lsq + k_wpost
   for (int r = 0; r < reps && !rc; ++r) {
     cudaEventRecord(ev[0], e->stream);
+    e->mark = split ? ev[4] : nullptr;
     rc = launch_recon(e, p, (const double*)e->Un.p);
+    e->mark = nullptr;
     cudaEventRecord(ev[1], e->stream);
     if (!rc) rc = launch_flux(e, p, 0, (const double*)e->Un.p, (const double*)e->Un.p, nullptr, 0.0);
     cudaEventRecord(ev[2], e->stream);
@@ -789,10 +757,12 @@ int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
       cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
       acc[k] += t;
     }
+    cudaEventElapsedTime(&t, ev[0], split ? ev[4] : ev[1]);
+    acc[3] += t;
   }
   for (auto& x : ev) cudaEventDestroy(x);
   if (rc) return rc;
-  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / reps;
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
   CK(cudaGetLastError());
   return UCG_OK;
 }

@@ -125,68 +125,6 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
 }
 
 // ======================================================================
-// Viscous gradients for WENO/CWENO + Navier-Stokes: LSQ on (T,u,v,w) with
-// stencil 1 (gradients.f90:502-706), then face gradients (SOLUTIONTRIAV2).
-// ======================================================================
-template <int P, typename T>
-__global__ void k_visc_lsq(Problem p, const double* __restrict__ U) {
-  constexpr int ID = Deg<P>::ideg;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n * 4) return;
-  const int64_t c = i >> 2;
-  const int var = (int)(i & 3);
-  const int IM = p.imax, W = IM + 1;
-  double pm[NV];
-  cons2prim(p.gamma, U + c * NV, pm);
-  const double s0 = var == 0 ? pm[4] / (pm[0] * p.r_gas) : pm[var];
-  const int64_t grp = c >> 5;
-  const int lane = (int)(c & 31);
-  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
-  const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
-  double acc[ID];
-#pragma unroll
-  for (int d = 0; d < ID; ++d) acc[d] = 0.0;
-  for (int k = 0; k < IM; ++k) {
-    double py[NV];
-    cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
-    double ds = (var == 0 ? py[4] / (py[0] * p.r_gas) : py[var]) - s0;
-#pragma unroll
-    for (int d = 0; d < ID; ++d) acc[d] += (double)M[(k * ID + d) * 32] * ds;
-  }
-#pragma unroll
-  for (int d = 0; d < ID; ++d) p.gv[(c * ID + d) * 4 + var] = acc[d];
-}
-
-template <int P, typename T>
-__global__ void k_visc_face(Problem p) {
-  constexpr int ID = Deg<P>::ideg;
-  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n * MF * QS) return;
-  const int64_t c = i / (MF * QS);
-  const int r = (int)(i - c * MF * QS), f = r / QS, q = r - f * QS;
-  if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) return;
-  const T* xi = (const T*)p.qpts + ((c * MF + f) * QS + q) * 3;
-  double dx[ID], dy[ID], dz[ID];
-  dmonomials<P>((double)xi[0], (double)xi[1], (double)xi[2], dx, dy, dz);
-  const double* J = p.jinv + c * 9;
-  double* o = p.ulv + ((c * MF + f) * QS + q) * 12;
-#pragma unroll
-  for (int var = 0; var < 4; ++var) {
-    double gl[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < ID; ++d) {
-      double g = p.gv[(c * ID + d) * 4 + var];
-      gl[0] += g * dx[d];
-      gl[1] += g * dy[d];
-      gl[2] += g * dz[d];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
-  }
-}
-
-// ======================================================================
 // Face fluxes fused with the RK stage update.  Eight lanes per cell, lane f
 // integrates face f; the face sums are added in face order
 // (CALCULATE_FLUXESHI_CONVECTIVE flux_p.f90:478, CALCULATE_FLUXESHI_DIFFUSIVE
@@ -386,29 +324,43 @@ __global__ void k_reduce_final(const double* partial, int64_t np, double* out) {
 // Table upload: per-cell rows dst[c][0..len) from src[table_id[c]] (or
 // src[c - first] without ids), converted to the engine precision.
 // ======================================================================
-// Interleaved variant: row j of cell c goes to ((c/32)*len + j)*32 + c%32.
+// Interleaved layout: row j of cell c goes to ((c/32)*len + j)*32 + c%32.
+// One block moves a 32-cell x 64-row tile through shared memory, so both the
+// per-cell source rows and the interleaved destination are accessed in
+// contiguous runs.  Cells outside [first, first+count) or whose table set is
+// outside [tlo, thi) are left untouched.
 template <typename D, typename S>
-__global__ void k_expand_il(D* __restrict__ dst, const S* __restrict__ src, const int32_t* __restrict__ tid,
-                            int64_t first, int64_t count, int64_t len, int64_t tlo, int64_t thi) {
-  const int64_t total = count * len;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t cl = i / len, j = i - cl * len;
-    int64_t t = tid ? tid[cl] : cl;
-    if (t < tlo || t >= thi) continue;
-    int64_t c = first + cl;
-    dst[((c >> 5) * len + j) * 32 + (c & 31)] = D(src[(t - tlo) * len + j]);
-  }
-}
-
-template <typename T>
-__global__ void k_expand(T* __restrict__ dst, const double* __restrict__ src, const int32_t* __restrict__ tid,
-                         int64_t first, int64_t count, int64_t len, int64_t tlo, int64_t thi) {
-  const int64_t total = count * len;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t cl = i / len, j = i - cl * len;
-    int64_t t = tid ? tid[cl] : cl;
-    if (t < tlo || t >= thi) continue;
-    dst[(first + cl) * len + j] = T(src[(t - tlo) * len + j]);
+__global__ void __launch_bounds__(256) k_expand_il(D* __restrict__ dst, const S* __restrict__ src,
+                                                   const int32_t* __restrict__ tid, int64_t first, int64_t count,
+                                                   int64_t len, int64_t tlo, int64_t thi) {
+  __shared__ S tile[32][65];
+  __shared__ int64_t trow[32];
+  const int64_t g0 = first >> 5, g1 = (first + count - 1) >> 5;
+  const int64_t ntile = (len + 63) / 64, nblk = (g1 - g0 + 1) * ntile;
+  for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    const int64_t g = g0 + b / ntile, j0 = (b % ntile) * 64;
+    if (threadIdx.x < 32) {
+      const int64_t c = g * 32 + threadIdx.x;
+      int64_t t = -1;
+      if (c >= first && c < first + count) {
+        const int64_t cl = c - first;
+        t = tid ? tid[cl] : cl;
+        if (t < tlo || t >= thi) t = -1;
+      }
+      trow[threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 32 * 64; i += blockDim.x) {
+      const int cell = i >> 6, jj = i & 63;
+      const int64_t t = trow[cell];
+      if (t >= 0 && j0 + jj < len) tile[cell][jj] = src[(t - tlo) * len + j0 + jj];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 64 * 32; i += blockDim.x) {
+      const int jj = i >> 5, lane = i & 31;
+      if (trow[lane] >= 0 && j0 + jj < len) dst[(g * len + j0 + jj) * 32 + lane] = D(tile[lane][jj]);
+    }
+    __syncthreads();
   }
 }
 

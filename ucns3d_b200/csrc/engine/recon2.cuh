@@ -6,51 +6,23 @@
 //            difference U_k - U_i is reused across DH rows held in registers.
 //            Output: the stencil polynomials G[ll][d][v], interleaved.
 // k_wpost    CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), CHECKSOL,
-//            MUSCL fall-back, CHECKSOLX (3126-3406): a block reconstructs
-//            `cpc` cells cooperatively in shared memory.
+//            MUSCL fall-back, CHECKSOLX (3126-3406): one lane per cell, no
+//            block barriers; smoothness indicators as packed quadratic forms.
 #pragma once
 
 #include "device.cuh"
 
 namespace ucg {
 
-// Tuning of k_lsq (compile-time): rows of G held in registers per pass for
-// IORDER 4/3 in FP32/FP64, software pipelining of the index/state chain,
-// minimum resident blocks per SM for the register budget.
-#ifndef UCG_LSQ_ROWS_P4F
-#define UCG_LSQ_ROWS_P4F 17
-#endif
-#ifndef UCG_LSQ_ROWS_P4D
-#define UCG_LSQ_ROWS_P4D 12
-#endif
-#ifndef UCG_LSQ_ROWS_P3F
-#define UCG_LSQ_ROWS_P3F 19
-#endif
-#ifndef UCG_LSQ_ROWS_P3D
-#define UCG_LSQ_ROWS_P3D 10
-#endif
-#ifndef UCG_LSQ_PIPE
-#define UCG_LSQ_PIPE 0
-#endif
-#ifndef UCG_LSQ_MINB
-#define UCG_LSQ_MINB 1
-#endif
-// 1: k_lsq_bulk (tables streamed through shared memory), 0: k_lsq
-#ifndef UCG_LSQ_BULK
-#define UCG_LSQ_BULK 1
-#endif
-
-// rows of G held in registers per pass
+// rows of G held in registers per pass (accumulators: DH x 5 values of T)
 template <int P, typename T>
 struct LsqRows {
   static constexpr int ID = Deg<P>::ideg;
-  static constexpr int value = P == 4   ? (sizeof(T) == 4 ? UCG_LSQ_ROWS_P4F : UCG_LSQ_ROWS_P4D)
-                               : P == 3 ? (sizeof(T) == 4 ? UCG_LSQ_ROWS_P3F : UCG_LSQ_ROWS_P3D)
-                                        : ID;
+  static constexpr int value = P == 4 ? (sizeof(T) == 4 ? 34 : 17) : P == 3 ? (sizeof(T) == 4 ? 19 : 10) : ID;
 };
 
 template <int P, typename T>
-__global__ void __launch_bounds__(128, UCG_LSQ_MINB) k_lsq(Problem p, const double* __restrict__ U) {
+__global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int DH = LsqRows<P, T>::value;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -79,39 +51,6 @@ __global__ void __launch_bounds__(128, UCG_LSQ_MINB) k_lsq(Problem p, const doub
       if (act) {
         const T* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
         const int32_t* S = Si + (ll * W + 1) * 32;
-#if UCG_LSQ_PIPE
-        // software pipeline of the dependent chain index -> state -> FMA:
-        // indices two rows ahead, neighbour state one row ahead
-        int y1 = nk > 1 ? S[32] : 0;
-        double ua[NV];
-        {
-          const double* uy = U + (int64_t)S[0] * NV;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) ua[v] = uy[v];
-        }
-        for (int k = 0; k < nk; ++k) {
-          const int y2 = k + 2 < nk ? S[(k + 2) * 32] : 0;
-          double ub[NV];
-          const double* un = U + (int64_t)y1 * NV;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) ub[v] = k + 1 < nk ? un[v] : 0.0;
-          T du[NV];
-#pragma unroll
-          for (int v = 0; v < NV; ++v) du[v] = T(ua[v] - u0[v]);
-          const T* Mk = M + (int64_t)k * nd * 32;
-#pragma unroll
-          for (int j = 0; j < DH; ++j)
-            if (d0 + j < nd) {
-              T m = Mk[j * 32];
-#pragma unroll
-              for (int v = 0; v < NV; ++v) acc[j][v] += m * du[v];
-            }
-#pragma unroll
-          for (int v = 0; v < NV; ++v) ua[v] = ub[v];
-          y1 = y2;
-        }
-      }
-#else
 #pragma unroll 2
         for (int k = 0; k < nk; ++k) {
           const double* uy = U + (int64_t)S[k * 32] * NV;
@@ -128,7 +67,6 @@ __global__ void __launch_bounds__(128, UCG_LSQ_MINB) k_lsq(Problem p, const doub
             }
         }
       }
-#endif
       if (live)
 #pragma unroll
         for (int j = 0; j < DH; ++j)
@@ -139,498 +77,425 @@ __global__ void __launch_bounds__(128, UCG_LSQ_MINB) k_lsq(Problem p, const doub
   }
 }
 
-// ------------------------------------------------------------- k_lsq_bulk
-// The same product G = invmat * (U_k - U_i) with the pseudo-inverse rows
-// streamed through shared memory.  Each warp owns one 32-cell group; lane 0
-// keeps `stages` chunks of bulk copies in flight (table rows and stencil
-// indices), so the DRAM requests outstanding per SM do not depend on the
-// register budget.  A chunk is KR stencil rows x dc columns [d0, d0+dc) of
-// stencil ll; LsqBulk<P,T>::DH columns are accumulated in registers over all
-// rows of a stencil.  The neighbour states of chunk i+1 are gathered while
-// chunk i is multiplied.  No block-wide barrier: warps run independently.
-template <int P, typename T>
-struct LsqBulk {
-  static constexpr int ID = Deg<P>::ideg;
-  // columns per pass: 170 accumulator registers at most
-  static constexpr int DH = sizeof(T) == 4 ? (ID <= 34 ? ID : 34) : (ID <= 17 ? ID : (ID + 1) / 2);
-  static constexpr int KR = 2;  // stencil rows per chunk
-  static constexpr int stage_bytes = KR * DH * 32 * (int)sizeof(T) + KR * 128;
-};
+// ------------------------------------------------------------- k_wpost
+// Smoothness matrices are packed upper triangles, interleaved over 32-cell
+// groups like the pseudo-inverses: entry (d, e >= d) of cell c is element
+// tri(d, e) = d*nd - d*(d-1)/2 + (e - d) of the cell's block, and an
+// off-diagonal entry holds S_de + S_ed, so that
+//   g^T S g = sum_d g_d * sum_{e >= d} P_de g_e
+// is the full quadratic form of INDICATORMATRIX (src/prestore.f90:1529-1673)
+// with half the loads and multiplies.
 
-struct LsqBulkPlan {
-  int nw;      // warps (32-cell groups) per block
-  int stages;  // chunks in flight per warp
-  int total;   // dynamic shared memory per block
-};
-
-template <int P, typename T>
-LsqBulkPlan lsq_bulk_plan(int nw) {
-  constexpr int sb = LsqBulk<P, T>::stage_bytes;
-  int st = 36 * 1024 / sb;
-  st = st < 3 ? 3 : (st > 16 ? 16 : st);
-  return LsqBulkPlan{nw, st, nw * st * (sb + 8)};
-}
-
-struct LsqChunk {
-  int ll, d0, k0;
-};
-
-template <int P, typename T>
-__global__ void __launch_bounds__(96, 2) k_lsq_bulk(Problem p, const double* __restrict__ U, LsqBulkPlan pl) {
-  using B = LsqBulk<P, T>;
-  constexpr int ID = B::ID, DH = B::DH, KR = B::KR, SB = B::stage_bytes;
-  extern __shared__ __align__(128) unsigned char smem[];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t grp = (int64_t)blockIdx.x * pl.nw + w;
-  if (grp * 32 >= p.n) return;  // warp-uniform
-  const int S = pl.stages;
-  unsigned char* stage0 = smem + (size_t)w * S * SB;
-  uint64_t* bar = (uint64_t*)(smem + (size_t)pl.nw * S * SB) + w * S;
-  const int A = p.admis_max, W = p.imax + 1;
-  const bool cw = p.ees == 5;
-  const int64_t c = grp * 32 + lane;
-  const bool live = c < p.n;
-  const int adm = live ? p.admis[c] : 0;
-  const int amax = __reduce_max_sync(0xffffffffu, adm);  // stencils any lane of the group uses
-  const T* Mg = (const T*)p.invmat + grp * p.tstride * 32;
-  const int32_t* Sg = p.sten + grp * (int64_t)(A * W) * 32;
-  T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  auto nk_of = [&](int ll) { return cw && ll > 0 ? p.imax2 : p.imax; };
-  auto nd_of = [&](int ll) { return cw && ll > 0 ? p.ideg2 : ID; };
-  auto next = [&](LsqChunk& q) {
-    q.k0 += KR;
-    if (q.k0 >= nk_of(q.ll)) {
-      q.k0 = 0;
-      q.d0 += DH;
-      if (q.d0 >= nd_of(q.ll)) {
-        q.d0 = 0;
-        ++q.ll;
-      }
-    }
-  };
-  // lane 0: copy chunk q into stage s
-  auto issue = [&](const LsqChunk& q, int s) {
-    const int nk = nk_of(q.ll), nd = nd_of(q.ll);
-    const int kc = min(KR, nk - q.k0), dc = min(DH, nd - q.d0);
-    unsigned char* st = stage0 + (size_t)s * SB;
-    T* tab = (T*)st;
-    int32_t* idx = (int32_t*)(st + KR * DH * 32 * sizeof(T));
-    const T* M = Mg + (int64_t)p.soff[q.ll] * 32;
-    mbar_expect_tx(&bar[s], (unsigned)(kc * dc * 32 * sizeof(T) + kc * 128));
-    if (dc == nd) {
-      bulk_g2s(tab, M + (int64_t)q.k0 * nd * 32, (unsigned)(kc * nd * 32 * sizeof(T)), &bar[s]);
-    } else {
-      for (int r = 0; r < kc; ++r)
-        bulk_g2s(tab + r * dc * 32, M + ((int64_t)(q.k0 + r) * nd + q.d0) * 32, (unsigned)(dc * 32 * sizeof(T)),
-                 &bar[s]);
-    }
-    bulk_g2s(idx, Sg + (int64_t)(q.ll * W + 1 + q.k0) * 32, (unsigned)(kc * 128), &bar[s]);
-  };
-  if (lane == 0)
-    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
-  mbar_fence_init();
-  __syncwarp();
-
-  double u0[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) u0[v] = live ? U[c * NV + v] : 0.0;
-
-  // chunk indices: waited < issued; chunk i lives in stage i % S
-  int64_t issued = 0, waited = 0;
-  LsqChunk prod{0, 0, 0};
-  for (int s = 0; s < S && prod.ll < amax; ++s) {
-    if (lane == 0) issue(prod, s);
-    next(prod);
-    ++issued;
-  }
-  bool ok = true;
-  auto wait_chunk = [&](int64_t i) {
-    const bool r = __all_sync(0xffffffffu, mbar_wait(&bar[i % S], (unsigned)((i / S) & 1)));
-    ok = ok && r;
-    if (r) waited = i + 1;
-  };
-
-  LsqChunk cur{0, 0, 0};
-  double un[KR][NV];  // neighbour states of the current chunk
-  // gather the rows of chunk q (its indices are in stage s)
-  auto gather = [&](const LsqChunk& q, int s) {
-    const int kc = min(KR, nk_of(q.ll) - q.k0);
-    const bool act = q.ll < adm;
-    const int32_t* idx = (const int32_t*)(stage0 + (size_t)s * SB + KR * DH * 32 * sizeof(T));
-#pragma unroll
-    for (int r = 0; r < KR; ++r) {
-      const bool on = act && r < kc;
-      const int y = on ? idx[r * 32 + lane] : 0;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) un[r][v] = on ? U[(int64_t)y * NV + v] : 0.0;
-    }
-  };
-  if (issued > 0) {
-    wait_chunk(0);
-    if (ok) gather(cur, 0);
-  }
-  T acc[DH][NV];
-#pragma unroll
-  for (int j = 0; j < DH; ++j)
-#pragma unroll
-    for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
-
-  for (int64_t i = 0; ok && cur.ll < amax; ++i) {
-    const int s = (int)(i % S);
-    const int nk = nk_of(cur.ll), nd = nd_of(cur.ll);
-    const int kc = min(KR, nk - cur.k0), dc = min(DH, nd - cur.d0);
-    const bool act = cur.ll < adm;
-    T du[KR][NV];
-#pragma unroll
-    for (int r = 0; r < KR; ++r)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) du[r][v] = T(un[r][v] - u0[v]);
-    // start the gathers of the next chunk
-    LsqChunk nx = cur;
-    next(nx);
-    if (nx.ll < amax) {
-      wait_chunk(i + 1);
-      if (!ok) break;
-      gather(nx, (int)((i + 1) % S));
-    }
-    const T* tab = (const T*)(stage0 + (size_t)s * SB);
-    if (act) {
-#pragma unroll
-      for (int r = 0; r < KR; ++r)
-        if (r < kc) {
-#pragma unroll
-          for (int j = 0; j < DH; ++j)
-            if (j < dc) {
-              const T m = tab[(r * dc + j) * 32 + lane];
-#pragma unroll
-              for (int v = 0; v < NV; ++v) acc[j][v] += m * du[r][v];
-            }
-        }
-    }
-    if (cur.k0 + kc >= nk) {  // last rows of this column pass: write G
-      if (live)
-#pragma unroll
-        for (int j = 0; j < DH; ++j)
-          if (j < dc)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-              Gi[(int64_t)((cur.ll * ID + cur.d0 + j) * NV + v) * 32] = acc[j][v];
-              acc[j][v] = T(0);
-            }
-    }
-    // stage s is free again: refill it with chunk i + S
-    __syncwarp();
-    if (prod.ll < amax) {
-      if (lane == 0) {
-        fence_proxy_async();
-        issue(prod, s);
-      }
-      next(prod);
-      ++issued;
-    }
-    cur = nx;
-  }
-  if (!ok) {
-    // record the timeout and let the copies in flight land before leaving
-    if (lane == 0) atomicOr(p.health, HEALTH_TIMEOUT);
-    for (int64_t i = waited; i < issued; ++i) mbar_wait(&bar[i % S], (unsigned)((i / S) & 1));
-    return;
-  }
-  // stencils no lane of the group uses
-  if (live)
-    for (int ll = amax; ll < A; ++ll)
-      for (int j = 0; j < nd_of(ll); ++j)
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + j) * NV + v) * 32] = T(0);
-}
-
-}  // namespace ucg
-
-namespace ucg {
-
-struct WPPlan {
-  int cpc;
-  int o_G, o_g1, o_S, o_tmp, o_gh, o_w, o_dul, o_u0, o_bnd, o_slope, o_flag, total;
-};
-
+// variables per register pass of each phase: indicators (IS), combined
+// polynomial + face values (FACE), MUSCL fall-back (FALL); the polynomial
+// of a pass ([ID] x variables) stays in registers
+#ifndef UCG_WV_IS_F
+#define UCG_WV_IS_F 5
+#endif
+#ifndef UCG_WV_FACE_F
+#define UCG_WV_FACE_F 3
+#endif
+#ifndef UCG_WV_FALL_F
+#define UCG_WV_FALL_F 1
+#endif
+#ifndef UCG_WV_IS_D
+#define UCG_WV_IS_D 2
+#endif
+#ifndef UCG_WV_FACE_D
+#define UCG_WV_FACE_D 2
+#endif
+#ifndef UCG_WV_FALL_D
+#define UCG_WV_FALL_D 1
+#endif
 template <typename T>
-inline WPPlan wpost_plan(int cpc, int A, int ID, int ID2, int QS, bool cw, int istride) {
-  WPPlan w{};
-  w.cpc = cpc;
-  const int s = (int)sizeof(T);
-  int off = 0;
-  auto take = [&](int bytes) {
-    int o = off;
-    off += (bytes + 15) / 16 * 16;
-    return o;
-  };
-  w.o_G = take(cpc * A * ID * NV * s);
-  w.o_g1 = take(cw ? cpc * ID * NV * s : 0);
-  w.o_S = take(cpc * istride * s);
-  int tmp = cpc * A * ID * NV * s, psi = cpc * MF * QS * NV * 8;
-  w.o_tmp = take(tmp > psi ? tmp : psi);  // indicator partials, later the limiter values
-  w.o_gh = take(cpc * ID * NV * s);
-  w.o_w = take(cpc * A * NV * 8);
-  w.o_dul = take(cpc * MF * QS * NV * s);
-  w.o_u0 = take(cpc * NV * 8);
-  w.o_bnd = take(cpc * 2 * NV * 8);
-  w.o_slope = take(cpc * NV * 8);
-  w.o_flag = take(cpc * 2 * 4);
-  w.total = off;
-  return w;
+struct WVars {
+  static constexpr int is = sizeof(T) == 4 ? UCG_WV_IS_F : UCG_WV_IS_D;
+  static constexpr int face = sizeof(T) == 4 ? UCG_WV_FACE_F : UCG_WV_FACE_D;
+  static constexpr int fall = sizeof(T) == 4 ? UCG_WV_FALL_F : UCG_WV_FALL_D;
+};
+
+// is[k] += sum_d g[d][k] * sum_{e>=d} P_de g[e][k] over d, e < nd <= NMAX
+template <int NMAX, int VG, typename T>
+__device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[NMAX][VG], int nd, T (&is)[VG]) {
+  int j = 0;
+#pragma unroll
+  for (int d = 0; d < NMAX; ++d) {
+    if (d < nd) {
+      T t[VG];
+#pragma unroll
+      for (int k = 0; k < VG; ++k) t[k] = T(0);
+#pragma unroll
+      for (int e = d; e < NMAX; ++e)
+        if (e < nd) {
+          const T s = P[(int64_t)(j + e - d) * 32];
+#pragma unroll
+          for (int k = 0; k < VG; ++k) t[k] += s * g[e][k];
+        }
+      j += nd - d;
+#pragma unroll
+      for (int k = 0; k < VG; ++k) is[k] += g[d][k] * t[k];
+      // keep the loads of one row together: without this fence the
+      // compiler hoists the whole triangle and spills it
+      asm volatile("" ::: "memory");
+    }
+  }
 }
 
+// k_wpost: one lane per cell, no block barriers.  Indicators and weights of
+// CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), the combined
+// polynomial, its face values and CHECKSOL; flagged cells (and every cell of
+// high-order MUSCL) take the central stencil polynomial limited by
+// Venkatakrishnan, then CHECKSOLX (3126-3406).  Output: dul [n][F][QS][5],
+// face value minus cell mean, 0 in unused slots.
 template <int P, typename T>
-__global__ void __launch_bounds__(256) k_wpost(Problem p, const double* __restrict__ U, WPPlan w) {
+__global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
+  constexpr int VI = WVars<T>::is, VH = WVars<T>::face, VF = WVars<T>::fall;
+  __shared__ double s_w[7 * NV * 128];  // per thread, [ll][v]: indicators, then weights
+  const int tid = threadIdx.x;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + tid;
+  if (c >= p.n) return;
   const int A = p.admis_max;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
-  const bool cw = p.ees == 5;
-  const bool weno = p.scheme == 3;
+  const int FQ = MF * QS;
+  const bool cw = p.ees == 5, weno = p.scheme == 3;
   const int ID2 = p.ideg2;
-  const int cpc = w.cpc, tid = threadIdx.x, NT = blockDim.x;
-  const int64_t c0 = (int64_t)blockIdx.x * cpc;
-  const int nc = (int)((p.n - c0) < cpc ? (p.n - c0) : cpc);
-  extern __shared__ __align__(16) unsigned char sm[];
-  T* s_G = (T*)(sm + w.o_G);
-  T* s_g1 = (T*)(sm + w.o_g1);
-  T* s_S = (T*)(sm + w.o_S);
-  T* s_tmp = (T*)(sm + w.o_tmp);
-  double* s_psi = (double*)(sm + w.o_tmp);
-  T* s_gh = (T*)(sm + w.o_gh);
-  double* s_w = (double*)(sm + w.o_w);
-  T* s_dul = (T*)(sm + w.o_dul);
-  double* s_u0 = (double*)(sm + w.o_u0);
-  double* s_bnd = (double*)(sm + w.o_bnd);
-  double* s_slope = (double*)(sm + w.o_slope);
-  int* s_flag = (int*)(sm + w.o_flag);
-
-  const int GS = A * ID * NV;
-  const T* Gi = (const T*)p.gbuf;
-  for (int i = tid; i < nc * NV; i += NT) s_u0[i] = U[c0 * NV + i];
-  for (int i = tid; i < nc * 2; i += NT) s_flag[i] = 0;
-  // stencil polynomials: consecutive threads read consecutive cells (lanes)
-  for (int i = tid; i < nc * GS; i += NT) {
-    int r = i / nc, cl = i - r * nc;
-    int64_t c = c0 + cl;
-    s_G[cl * GS + r] = Gi[((c >> 5) * GS + r) * 32 + (c & 31)];
-  }
-  if (weno) {
-    const T* IND = (const T*)p.ind + c0 * p.istride;
-    for (int i = tid; i < nc * (int)p.istride; i += NT) s_S[i] = IND[i];
-  }
-  __syncthreads();
-
-  if (weno) {
-    if (cw) {  // central polynomial with the low-order stencils removed (reconstruct_p.f90:956-965)
-      for (int i = tid; i < nc * ID * NV; i += NT) {
-        int cl = i / (ID * NV), r = i - cl * ID * NV, d = r / NV, v = r - d * NV;
-        int adm = p.admis[c0 + cl];
-        const double lc1 = 1.0 - 1.0 / p.lwci;
-        const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-        T g3 = T(0);
-        if (d < ID2)
-          for (int ll = 1; ll < adm; ++ll) g3 = g3 + T(lk) * s_G[cl * GS + (ll * ID + d) * NV + v];
-        s_g1[i] = T(1.0 / lc1) * (s_G[cl * GS + d * NV + v] - g3);
-      }
-      __syncthreads();
-    }
-    // IS = g^T S g: thread (cell, ll, e) forms (S g)_e g_e for the five variables
-    for (int i = tid; i < nc * A * ID; i += NT) {
-      int cl = i / (A * ID), r = i - cl * A * ID, ll = r / ID, e = r - ll * ID;
-      bool low = cw && ll > 0;
-      int nd = low ? ID2 : ID;
-      T t[NV] = {T(0), T(0), T(0), T(0), T(0)};
-      if (ll < p.admis[c0 + cl] && e < nd) {
-        const T* S = s_S + cl * (int)p.istride + (low ? p.i2off : 0);
-        const T* g = (cw && ll == 0) ? s_g1 + cl * ID * NV : s_G + cl * GS + ll * ID * NV;
-        T acc[NV] = {T(0), T(0), T(0), T(0), T(0)};
-        for (int d = 0; d < nd; ++d) {
-          T sde = S[d * nd + e];
+  const int adm = p.admis[c];
+  const int nf = p.nfaces[c];
+  const int lane = (int)(c & 31);
+  const T* Gc = (const T*)p.gbuf + (c >> 5) * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int ll, int d, int v) -> T { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  double u0[NV], pm[NV];
 #pragma unroll
-          for (int v = 0; v < NV; ++v) acc[v] += sde * g[d * NV + v];
+  for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
+  cons2prim(p.gamma, u0, pm);
+  const T* xq = (const T*)p.qpts + c * FQ * 3;
+  const T* bm = (const T*)p.bmean + c * ID;
+  T* out = (T*)p.dul + c * FQ * NV;
+  double* sw = s_w + tid;  // sw[(ll * NV + v) * 128]
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
+  // b = basis at face point (f, q) minus the basis means
+  auto basis = [&](int f, int q, T (&b)[ID]) {
+    const T* xi = xq + (f * QS + q) * 3;
+    monomials<P, T>(xi[0], xi[1], xi[2], b);
+#pragma unroll
+    for (int d = 0; d < ID; ++d) b[d] -= bm[d];
+  };
+  // central stencil polynomial for variables v0, v0+1, ... (as many as g
+  // holds); with `rem`, the CWENO form with the low-order stencils removed
+  // (reconstruct_p.f90:956-965)
+  auto load_g0 = [&](int v0, auto& g, bool rem) {
+    constexpr int VV = sizeof(g[0]) / sizeof(T);
+#pragma unroll
+    for (int d = 0; d < ID; ++d)
+#pragma unroll
+      for (int k = 0; k < VV; ++k) {
+        const int v = v0 + k;
+        T x = v < NV ? G(0, d, v) : T(0);
+        if (rem && v < NV) {
+          T g3 = T(0);
+          if (d < ID2)
+            for (int l2 = 1; l2 < adm; ++l2) g3 = g3 + T(lk) * G(l2, d, v);
+          x = T(1.0 / lc1) * (x - g3);
+        }
+        g[d][k] = x;
+      }
+  };
+
+  bool fall = !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
+  if (!fall) {
+    // ---- smoothness indicators g^T S g per stencil and variable
+    const T* Pc = (const T*)p.ind + (c >> 5) * p.istride * 32 + lane;
+    for (int ll = 0; ll < adm; ++ll) {
+      const bool low = cw && ll > 0;
+      for (int v0 = 0; v0 < NV; v0 += VI) {
+        T is[VI];
+#pragma unroll
+        for (int k = 0; k < VI; ++k) is[k] = T(0);
+        if (low) {  // CWENO lower-order stencil: IDEGFREE2 is 3 or 9 (grid_p.f90:6145-6160)
+          constexpr int L2 = ID < 9 ? ID : 9;
+          T g[L2][VI];
+#pragma unroll
+          for (int d = 0; d < L2; ++d)
+#pragma unroll
+            for (int k = 0; k < VI; ++k) g[d][k] = (v0 + k < NV && d < ID2) ? G(ll, d, v0 + k) : T(0);
+          quad_form<L2, VI>(Pc + (int64_t)p.i2off * 32, g, ID2, is);
+        } else {
+          T g[ID][VI];
+          if (ll == 0) {
+            load_g0(v0, g, cw);
+          } else {
+#pragma unroll
+            for (int d = 0; d < ID; ++d)
+#pragma unroll
+              for (int k = 0; k < VI; ++k) g[d][k] = v0 + k < NV ? G(ll, d, v0 + k) : T(0);
+          }
+          quad_form<ID, VI>(Pc, g, ID, is);
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) t[v] = g[e * NV + v] * acc[v];
+        for (int k = 0; k < VI; ++k)
+          if (v0 + k < NV) sw[(ll * NV + v0 + k) * 128] = (double)is[k];
       }
-#pragma unroll
-      for (int v = 0; v < NV; ++v) s_tmp[(size_t)i * NV + v] = t[v];
     }
-    __syncthreads();
-    for (int i = tid; i < nc * A * NV; i += NT) {
-      int cl = i / (A * NV), r = i - cl * A * NV, ll = r / NV, v = r - ll * NV;
-      int nd = (cw && ll > 0) ? ID2 : ID;
-      T is = T(0);
-      for (int e = 0; e < nd; ++e) is += s_tmp[((size_t)(cl * A + ll) * ID + e) * NV + v];
-      s_w[i] = (double)is;
-    }
-    __syncthreads();
-    // nonlinear weights in FP64 ((10E-12)^4 underflows FP32)
-    for (int i = tid; i < nc * NV; i += NT) {
-      int cl = i / NV, v = i - cl * NV;
-      int adm = p.admis[c0 + cl];
-      double* ws = s_w + cl * A * NV;
-      double lam0, lamk;
-      if (cw) {
-        lam0 = 1.0 - 1.0 / p.lwci;
-        lamk = adm > 1 ? (1.0 - lam0) / (adm - 1) : 0.0;
-      } else {
-        lam0 = p.lwci;
-        lamk = 1.0;
-      }
+    // ---- nonlinear weights in FP64 ((10E-12)^4 underflows FP32)
+    for (int v = 0; v < NV; ++v) {
+      const double lam0 = cw ? lc1 : p.lwci, lamk = cw ? lk : 1.0;
       double tau = 0.0, sum = 0.0;
       if (cw && p.wenoz) {
-        for (int ll = 0; ll < adm; ++ll) tau += fabs(ws[v] - ws[ll * NV + v]);
+        for (int ll = 0; ll < adm; ++ll) tau += fabs(sw[v * 128] - sw[(ll * NV + v) * 128]);
         tau = tau / (adm - 1);
       }
       for (int ll = 0; ll < adm; ++ll) {
-        double e = p.weno_eps + ws[ll * NV + v];
-        double lam = ll == 0 ? lam0 : lamk, wt;
+        const double e = p.weno_eps + sw[(ll * NV + v) * 128];
+        const double lam = ll == 0 ? lam0 : lamk;
+        double wt;
         if (cw && p.wenoz) {
           double q = tau / e;
           q = q * q;
           wt = lam * (1.0 + q * q);
         } else {
-          double e2 = e * e;
+          const double e2 = e * e;
           wt = lam / (e2 * e2);
         }
-        ws[ll * NV + v] = wt;
+        sw[(ll * NV + v) * 128] = wt;
         sum += wt;
       }
-      for (int ll = 0; ll < adm; ++ll) ws[ll * NV + v] = ws[ll * NV + v] / sum;
+      for (int ll = 0; ll < adm; ++ll) sw[(ll * NV + v) * 128] = sw[(ll * NV + v) * 128] / sum;
     }
-    __syncthreads();
-    // combined polynomial
-    for (int i = tid; i < nc * ID * NV; i += NT) {
-      int cl = i / (ID * NV), r = i - cl * ID * NV, d = r / NV, v = r - d * NV;
-      int adm = p.admis[c0 + cl];
-      const double* ws = s_w + cl * A * NV;
-      const T* g0 = cw ? s_g1 + cl * ID * NV : s_G + cl * GS;
-      T acc = T(ws[v]) * g0[d * NV + v];
-      for (int ll = 1; ll < adm; ++ll)
-        if (!cw || d < ID2) acc += T(ws[ll * NV + v]) * s_G[cl * GS + (ll * ID + d) * NV + v];
-      s_gh[i] = acc;
+    // ---- combined polynomial, face values, CHECKSOL (threshold 0.85)
+    bool flag = false;
+    for (int v0 = 0; v0 < NV; v0 += VH) {
+      T gh[ID][VH];
+      load_g0(v0, gh, cw);
+#pragma unroll
+      for (int k = 0; k < VH; ++k) {
+        const T w0 = v0 + k < NV ? T(sw[(v0 + k) * 128]) : T(0);
+#pragma unroll
+        for (int d = 0; d < ID; ++d) gh[d][k] = w0 * gh[d][k];
+      }
+      for (int ll = 1; ll < adm; ++ll) {
+        T wl[VH];
+#pragma unroll
+        for (int k = 0; k < VH; ++k) wl[k] = v0 + k < NV ? T(sw[(ll * NV + v0 + k) * 128]) : T(0);
+#pragma unroll
+        for (int d = 0; d < ID; ++d)
+          if (!cw || d < ID2)
+#pragma unroll
+            for (int k = 0; k < VH; ++k)
+              if (v0 + k < NV) gh[d][k] += wl[k] * G(ll, d, v0 + k);
+      }
+      for (int f = 0; f < MF; ++f) {
+        const int nq = nq_of(f);
+        for (int q = 0; q < QS; ++q) {
+          T* o = out + (f * QS + q) * NV;
+          if (q >= nq) {
+#pragma unroll
+            for (int k = 0; k < VH; ++k)
+              if (v0 + k < NV) o[v0 + k] = T(0);
+            continue;
+          }
+          T b[ID];
+          basis(f, q, b);
+          T res[VH];
+#pragma unroll
+          for (int k = 0; k < VH; ++k) {
+            T r = T(0);
+#pragma unroll
+            for (int d = 0; d < ID; ++d) r += b[d] * gh[d][k];
+            res[k] = r;
+            if (v0 + k < NV) o[v0 + k] = r;
+          }
+          if (VH == NV) {
+            double uf[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) uf[v] = u0[v] + (double)res[v % VH];
+            flag = flag || jump_bad(p.gamma, pm, uf, 0.85);
+          }
+        }
+      }
     }
-    __syncthreads();
+    if (VH < NV) {  // CHECKSOL on the stored face values
+      for (int f = 0; f < nf; ++f) {
+        const int nq = nq_of(f);
+        for (int q = 0; q < nq; ++q) {
+          const T* o = out + (f * QS + q) * NV;
+          double uf[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) uf[v] = u0[v] + (double)o[v];
+          flag = flag || jump_bad(p.gamma, pm, uf, 0.85);
+        }
+      }
+    }
+    fall = flag;
   }
+  // CHECKSOLX (threshold 0.95) cannot fire where the 0.85 test passed on the
+  // same face values
+  if (!fall) return;
 
-  // ---- face values and CHECKSOL
-  const T* QPa = (const T*)p.qpts;
-  const T* BMa = (const T*)p.bmean;
-  const int FQ = MF * QS;
-  for (int i = tid; i < nc * FQ; i += NT) {
-    int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
-    int64_t c = c0 + cl;
-    T* o = s_dul + (size_t)i * NV;
+  // ---- MUSCL with the central stencil polynomial (FIND_BOUNDS + Venkatakrishnan)
+  double lo[NV], hi[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) o[v] = T(0);
-    if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) continue;
-    if (!weno || !p.full[c]) {  // MUSCL everywhere / CHECKSOL: FULL = 0 -> REDUCE
-      s_flag[cl * 2] = 1;
-      continue;
-    }
-    const T* xi = QPa + ((size_t)c * FQ + j) * 3;
-    T b[ID];
-    monomials<P, T>(xi[0], xi[1], xi[2], b);
-#pragma unroll
-    for (int d = 0; d < ID; ++d) b[d] -= BMa[c * ID + d];
-    const T* gh = s_gh + cl * ID * NV;
-    double uf[NV];
+  for (int v = 0; v < NV; ++v) lo[v] = hi[v] = u0[v];
+  for (int f = 0; f < nf; ++f) {
+    const int64_t nb = p.neigh[c * MF + f];
+    if (nb < 0) continue;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      T res = T(0);
-#pragma unroll
-      for (int d = 0; d < ID; ++d) res += b[d] * gh[d * NV + v];
-      o[v] = res;
-      uf[v] = s_u0[cl * NV + v] + (double)res;
+      const double un = U[nb * NV + v];
+      lo[v] = fmin(lo[v], un);
+      hi[v] = fmax(hi[v], un);
     }
-    double pm[NV];
-    cons2prim(p.gamma, s_u0 + cl * NV, pm);
-    if (jump_bad(p.gamma, pm, uf, 0.85)) s_flag[cl * 2] = 1;
   }
-  __syncthreads();
-  const int any = __syncthreads_or((tid < nc) ? s_flag[tid * 2] : 0);
-  if (any) {
-    // ---- MUSCL with the central stencil polynomial on flagged cells
-    for (int i = tid; i < nc * NV; i += NT) {
-      int cl = i / NV, v = i - cl * NV;
-      if (!s_flag[cl * 2]) continue;
-      int64_t c = c0 + cl;
-      double u0 = s_u0[i], mn = u0, mx = u0;
-      for (int f = 0; f < p.nfaces[c]; ++f) {
-        int64_t nb = p.neigh[c * MF + f];
-        if (nb < 0) continue;
-        double un = U[nb * NV + v];
-        mn = fmin(mn, un);
-        mx = fmax(mx, un);
-      }
-      s_bnd[(cl * 2 + 0) * NV + v] = mn - u0;
-      s_bnd[(cl * 2 + 1) * NV + v] = mx - u0;
-    }
-    __syncthreads();
-    for (int i = tid; i < nc * FQ; i += NT) {
-      int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
-      if (!s_flag[cl * 2]) continue;
-      int64_t c = c0 + cl;
-      double* ps = s_psi + (size_t)i * NV;
-      if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) ps[v] = TOLBIG;
-        continue;
-      }
-      const T* xi = QPa + ((size_t)c * FQ + j) * 3;
-      T b[ID];
-      monomials<P, T>(xi[0], xi[1], xi[2], b);
-#pragma unroll
-      for (int d = 0; d < ID; ++d) b[d] -= BMa[c * ID + d];
-      const T* g0 = s_G + cl * GS;
-      const double e3 = p.kappa_ven * p.minedge[c];
-      const double epsi2 = e3 * e3 * e3;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        T res = T(0);
-#pragma unroll
-        for (int d = 0; d < ID; ++d) res += b[d] * g0[d * NV + v];
-        double u0 = s_u0[cl * NV + v];
-        double dd = (u0 + (double)res) - u0;
-        s_dul[(size_t)i * NV + v] = T(dd);
-        ps[v] = venkat(dd, s_bnd[(cl * 2 + 0) * NV + v], s_bnd[(cl * 2 + 1) * NV + v], epsi2);
-      }
-    }
-    __syncthreads();
-    for (int i = tid; i < nc * NV; i += NT) {
-      int cl = i / NV, v = i - cl * NV;
-      if (!s_flag[cl * 2]) continue;
-      double mn = TOLBIG;
-      for (int j = 0; j < FQ; ++j) mn = fmin(mn, s_psi[((size_t)cl * FQ + j) * NV + v]);
-      s_slope[i] = mn;
-    }
-    __syncthreads();
-    for (int i = tid; i < nc * FQ * NV; i += NT) {
-      int cl = i / (FQ * NV);
-      if (!s_flag[cl * 2]) continue;
-      s_dul[i] = T((double)s_dul[i] * s_slope[cl * NV + i % NV]);
-    }
-    __syncthreads();
+  for (int v = 0; v < NV; ++v) {
+    lo[v] -= u0[v];
+    hi[v] -= u0[v];
   }
-
+  const double e3 = p.kappa_ven * p.minedge[c];
+  const double epsi2 = e3 * e3 * e3;
+  for (int v0 = 0; v0 < NV; v0 += VF) {
+    T g0[ID][VF];
+    load_g0(v0, g0, false);
+    double slope[VF];
+#pragma unroll
+    for (int k = 0; k < VF; ++k) slope[k] = TOLBIG;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int f = 0; f < MF; ++f) {
+        const int nq = nq_of(f);
+        for (int q = 0; q < QS; ++q) {
+          T* o = out + (f * QS + q) * NV;
+          if (q >= nq) {
+            if (pass == 1)
+#pragma unroll
+              for (int k = 0; k < VF; ++k)
+                if (v0 + k < NV) o[v0 + k] = T(0);
+            continue;
+          }
+          T b[ID];
+          basis(f, q, b);
+#pragma unroll
+          for (int k = 0; k < VF; ++k) {
+            const int v = v0 + k;
+            if (v >= NV) continue;
+            T r = T(0);
+#pragma unroll
+            for (int d = 0; d < ID; ++d) r += b[d] * g0[d][k];
+            const double dd = (u0[v] + (double)r) - u0[v];
+            if (pass == 0) slope[k] = fmin(slope[k], venkat(dd, lo[v], hi[v], epsi2));
+            else o[v] = T((double)T(dd) * slope[k]);
+          }
+        }
+      }
+    }
+  }
   // ---- CHECKSOLX: first order where a face value jumps by 95 %
-  for (int i = tid; i < nc * FQ; i += NT) {
-    int cl = i / FQ, j = i - cl * FQ, f = j / QS, q = j - f * QS;
-    int64_t c = c0 + cl;
-    if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) continue;
-    double uf[NV], pm[NV];
+  bool bad = false;
+  for (int f = 0; f < nf; ++f) {
+    const int nq = nq_of(f);
+    for (int q = 0; q < nq; ++q) {
+      const T* o = out + (f * QS + q) * NV;
+      double uf[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) uf[v] = s_u0[cl * NV + v] + (double)s_dul[(size_t)i * NV + v];
-    cons2prim(p.gamma, s_u0 + cl * NV, pm);
-    if (jump_bad(p.gamma, pm, uf, 0.95)) s_flag[cl * 2 + 1] = 1;
+      for (int v = 0; v < NV; ++v) uf[v] = u0[v] + (double)o[v];
+      bad = bad || jump_bad(p.gamma, pm, uf, 0.95);
+    }
   }
-  __syncthreads();
-  T* out = (T*)p.dul + c0 * FQ * NV;
-  for (int i = tid; i < nc * FQ * NV; i += NT) {
-    int cl = i / (FQ * NV);
-    out[i] = s_flag[cl * 2 + 1] ? T(0) : s_dul[i];
+  if (bad)
+    for (int i = 0; i < FQ * NV; ++i) out[i] = T(0);
+}
+
+// ======================================================================
+// Viscous gradients for WENO/CWENO + Navier-Stokes: LSQ on (T,u,v,w) with
+// stencil 1 (gradients.f90:502-706), then face gradients (SOLUTIONTRIAV2).
+// ======================================================================
+template <int P, typename T>
+__global__ void k_visc_lsq(Problem p, const double* __restrict__ U) {
+  constexpr int ID = Deg<P>::ideg;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n * 4) return;
+  const int64_t c = i >> 2;
+  const int var = (int)(i & 3);
+  const int IM = p.imax, W = IM + 1;
+  double pm[NV];
+  cons2prim(p.gamma, U + c * NV, pm);
+  const double s0 = var == 0 ? pm[4] / (pm[0] * p.r_gas) : pm[var];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  double acc[ID];
+#pragma unroll
+  for (int d = 0; d < ID; ++d) acc[d] = 0.0;
+  for (int k = 0; k < IM; ++k) {
+    double py[NV];
+    cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
+    double ds = (var == 0 ? py[4] / (py[0] * p.r_gas) : py[var]) - s0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) acc[d] += (double)M[(k * ID + d) * 32] * ds;
+  }
+#pragma unroll
+  for (int d = 0; d < ID; ++d) p.gv[(c * ID + d) * 4 + var] = acc[d];
+}
+
+template <int P, typename T>
+__global__ void k_visc_face(Problem p) {
+  constexpr int ID = Deg<P>::ideg;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n * MF * QS) return;
+  const int64_t c = i / (MF * QS);
+  const int r = (int)(i - c * MF * QS), f = r / QS, q = r - f * QS;
+  if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) return;
+  const T* xi = (const T*)p.qpts + ((c * MF + f) * QS + q) * 3;
+  double dx[ID], dy[ID], dz[ID];
+  dmonomials<P>((double)xi[0], (double)xi[1], (double)xi[2], dx, dy, dz);
+  const double* J = p.jinv + c * 9;
+  double* o = p.ulv + ((c * MF + f) * QS + q) * 12;
+#pragma unroll
+  for (int var = 0; var < 4; ++var) {
+    double gl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      double g = p.gv[(c * ID + d) * 4 + var];
+      gl[0] += g * dx[d];
+      gl[1] += g * dy[d];
+      gl[2] += g * dz[d];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
   }
 }
+
+// One reconstruction: stencil polynomials, WENO post-processing and, for
+// Navier-Stokes, the viscous LSQ and face gradients.  Instantiated per
+// precision and order in recon_*.cu, which nvcc compiles in parallel.
+// `mark`, if not null, is recorded between k_lsq and k_wpost (kernel timing).
+template <int P, typename T>
+cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st, int64_t* launches,
+                          cudaEvent_t mark) {
+  const unsigned b = (unsigned)((p.n + 127) / 128);
+  k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
+  if (mark) cudaEventRecord(mark, st);
+  k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+  *launches += 2;
+  if (ns) {
+    k_visc_lsq<P, T><<<(unsigned)((p.n * 4 + 127) / 128), 128, 0, st>>>(p, U);
+    const int64_t nf = p.n * MF * QS;
+    k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, st>>>(p);
+    *launches += 2;
+  }
+  return cudaGetLastError();
+}
+
+// precision-specific entry points (recon_f32.cu + recon_f32_p4.cu, recon_f64.cu);
+// iorder 1..4, anything else returns cudaErrorInvalidValue
+cudaError_t launch_weno_f32(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                            int64_t* launches, cudaEvent_t mark);
+cudaError_t launch_weno_f32_p4(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                               int64_t* launches, cudaEvent_t mark);
+cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                            int64_t* launches, cudaEvent_t mark);
 
 }  // namespace ucg

@@ -1,0 +1,18 @@
+// Mixed-precision (FP32 tables) reconstruction kernels, IORDER 1-3, and the
+// dispatch over IORDER; IORDER 4 lives in recon_f32_p4.cu.
+#include "recon2.cuh"
+
+namespace ucg {
+
+cudaError_t launch_weno_f32(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                            int64_t* launches, cudaEvent_t mark) {
+  switch (iorder) {
+    case 1: return launch_weno_t<1, float>(p, U, ns, QS, st, launches, mark);
+    case 2: return launch_weno_t<2, float>(p, U, ns, QS, st, launches, mark);
+    case 3: return launch_weno_t<3, float>(p, U, ns, QS, st, launches, mark);
+    case 4: return launch_weno_f32_p4(p, U, ns, QS, st, launches, mark);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace ucg

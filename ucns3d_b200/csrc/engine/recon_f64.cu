@@ -1,0 +1,17 @@
+// FP64 reconstruction kernels, IORDER 1-4.
+#include "recon2.cuh"
+
+namespace ucg {
+
+cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                            int64_t* launches, cudaEvent_t mark) {
+  switch (iorder) {
+    case 1: return launch_weno_t<1, double>(p, U, ns, QS, st, launches, mark);
+    case 2: return launch_weno_t<2, double>(p, U, ns, QS, st, launches, mark);
+    case 3: return launch_weno_t<3, double>(p, U, ns, QS, st, launches, mark);
+    case 4: return launch_weno_t<4, double>(p, U, ns, QS, st, launches, mark);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace ucg

@@ -116,9 +116,9 @@ class Engine:
     def time_kernels(self, reps: int = 5) -> dict:
         """Average device ms of the reconstruction, flux and time-step
         kernels (CUDA events on the engine stream)."""
-        ms = (C.c_double * 3)()
+        ms = (C.c_double * 4)()
         self._check(self.lib.ucg_time_kernels(self._h, reps, ms))
-        return dict(recon=ms[0], flux=ms[1], cfl=ms[2])
+        return dict(recon=ms[0], flux=ms[1], cfl=ms[2], lsq=ms[3])
 
     def check_health(self):
         self._check(self.lib.ucg_check_health(self._h))
