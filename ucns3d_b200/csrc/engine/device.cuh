@@ -42,9 +42,10 @@ struct Problem {
   const double* jinv;       // [n][9]
   const int8_t* admis;      // [n]
   const int8_t* full;       // [n]
-  // reconstruction tables, per cell contiguous, precision T
-  const void* qpts;         // [n][MF][MQ][3]
-  const void* bmean;        // [n][ideg]
+  // reconstruction tables in precision T, interleaved over 32-cell groups
+  // (element j of cell c at ((c / 32) * len + j) * 32 + c % 32)
+  const void* qpts;         // len = MF*QS*3: [f][q][xyz], QS = max(nq_quad, nq_tri)
+  const void* bmean;        // len = ideg
   // stencils and pseudo-inverses are interleaved over groups of 32 cells:
   // element j of cell c is at ((c / 32) * len + j) * 32 + c % 32, with
   // len = A*(imax+1) for the stencils and `tstride` for the pseudo-inverses.
@@ -54,14 +55,15 @@ struct Problem {
   const void* invmat;
   int64_t tstride;
   int soff[8];
-  // smoothness matrices, interleaved the same way with len = `istride`:
+  // smoothness matrices, vector-interleaved (see Vec) with len = `istride`:
   // packed upper triangle of S [ideg][ideg] at element 0 and of the CWENO
-  // S2 [ideg2][ideg2] at i2off, off-diagonal entries S_de + S_ed
+  // S2 [ideg2][ideg2] at i2off, rows padded to whole vectors, off-diagonal
+  // entries S_de + S_ed
   const void* ind;
   int64_t istride;
   int i2off;
   // scratch
-  void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the tables
+  void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the stencils
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
   double* gv;               // [n][ideg][4]  viscous LSQ coefficients
@@ -83,6 +85,27 @@ __constant__ __device__ static const int8_t kExp[34][3] = {
     {3, 0, 0}, {2, 1, 0}, {1, 2, 0}, {0, 3, 0}, {2, 0, 1}, {1, 1, 1}, {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {0, 0, 3},
     {4, 0, 0}, {3, 1, 0}, {2, 2, 0}, {1, 3, 0}, {0, 4, 0}, {3, 0, 1}, {2, 1, 1}, {1, 2, 1}, {0, 3, 1},
     {2, 0, 2}, {1, 1, 2}, {0, 2, 2}, {1, 0, 3}, {0, 1, 3}, {0, 0, 4}};
+
+// 16-byte vectors of the table precision: VEC elements per lane and load.
+// "Vector-interleaved" arrays store element j of cell c at
+// (((c/32)*len/VEC + j/VEC)*32 + c%32)*VEC + j%VEC (len a multiple of VEC),
+// so a warp reads VEC consecutive elements of 32 cells with one 512-byte load.
+template <typename T>
+struct Vec {
+  static constexpr int N = 16 / (int)sizeof(T);
+};
+__device__ __forceinline__ void ldv(const float* p, float (&o)[4]) {
+  const float4 x = *(const float4*)p;
+  o[0] = x.x;
+  o[1] = x.y;
+  o[2] = x.z;
+  o[3] = x.w;
+}
+__device__ __forceinline__ void ldv(const double* p, double (&o)[2]) {
+  const double2 x = *(const double2*)p;
+  o[0] = x.x;
+  o[1] = x.y;
+}
 
 template <int P>
 struct Deg {

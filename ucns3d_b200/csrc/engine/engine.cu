@@ -311,13 +311,18 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
       bool low = c.ees == 5 && ll > 0;
       int64_t el = low ? (int64_t)c.imax2 * c.ideg2 : (int64_t)c.imax * c.ideg;
       L.soff[ll] = (int)off;
-      off += up(el);
+      off += up(el);  // 16-byte aligned slices
     }
     L.tstride = off;
-    // smoothness matrices: packed upper triangles (S and the CWENO S2)
-    auto tri = [](int64_t m) { return m * (m + 1) / 2; };
-    L.i2off = (int)up(tri(c.ideg));
-    L.istride = L.i2off + (c.ees == 5 ? up(tri(c.ideg2)) : 0);
+    // smoothness matrices: packed upper triangles (S and the CWENO S2), each
+    // row padded to whole 16-byte vectors
+    auto tri = [&](int64_t m) {
+      int64_t t = 0;
+      for (int64_t d = 0; d < m; ++d) t += up(m - d);
+      return t;
+    };
+    L.i2off = (int)tri(c.ideg);
+    L.istride = L.i2off + (c.ees == 5 ? tri(c.ideg2) : 0);
   }
   cudaSetDevice(device);
   st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
@@ -462,13 +467,16 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   rc = rc ? rc : upload(e, e->full, full);
   if (rc) return rc;
   // reference-frame quadrature points and basis means, in table precision
-  std::vector<double> qp((size_t)n * MF * QS * 3, 0.0), bm((size_t)n * ideg);
+  // interleaved over 32-cell groups: element j of cell c at ((c/32)*len + j)*32 + c%32
+  const int64_t ngrp = (n + 31) / 32, lq = (int64_t)MF * QS * 3;
+  std::vector<double> qp((size_t)ngrp * 32 * lq, 0.0), bm((size_t)ngrp * 32 * ideg, 0.0);
   for (int64_t c = 0; c < n; ++c) {
+    const int64_t gq = (c >> 5) * lq, gb = (c >> 5) * ideg, ln = c & 31;
     for (int f = 0; f < MF; ++f)
       for (int q = 0; q < QS; ++q)
         for (int k = 0; k < 3; ++k)
-          qp[(((size_t)c * MF + f) * QS + q) * 3 + k] = g->qpoints[((c * MF + f) * UCG_MAX_QP + q) * 3 + k];
-    for (int d = 0; d < ideg; ++d) bm[(size_t)c * ideg + d] = g->basis_mean[(size_t)c * ideg + d];
+          qp[(size_t)((gq + (f * QS + q) * 3 + k) * 32 + ln)] = g->qpoints[((c * MF + f) * UCG_MAX_QP + q) * 3 + k];
+    for (int d = 0; d < ideg; ++d) bm[(size_t)((gb + d) * 32 + ln)] = g->basis_mean[(size_t)c * ideg + d];
   }
   if (e->mixed) {
     std::vector<float> qf(qp.begin(), qp.end()), bf(bm.begin(), bm.end());
@@ -532,7 +540,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     CK(cudaMemcpyAsync(e->staging.p, r->stencil, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
     int64_t total = count * A * W;
     unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
-    k_expand_il<int32_t, int32_t><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
+    k_expand_il<int32_t, int32_t, 1><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
                                                                 nullptr, first, count, (int64_t)A * W, 0, count);
     e->launches++;
     CK(cudaGetLastError());
@@ -548,6 +556,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   // pack matrix sets into the engine's per-cell block layout on the host
   // (FP64, padding zeroed), stage them in chunks, expand per cell on the GPU
   const int ideg = c.ideg, imax = c.imax, ideg2 = c.ideg2, imax2 = c.imax2;
+  const int vec = e->mixed ? 4 : 2;  // elements per 16-byte vector on the device
   auto pack_mat = [&](int64_t t, double* dst) {
     for (int64_t j = 0; j < Ly.tstride; ++j) dst[j] = 0.0;
     for (int ll = 0; ll < A; ++ll) {
@@ -558,12 +567,15 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       for (int j = 0; j < nk * nd; ++j) dst[Ly.soff[ll] + j] = src[j];
     }
   };
-  // upper triangle row by row; off-diagonal entries hold S_de + S_ed, so the
-  // packed form gives the same quadratic form as the full matrix
-  auto pack_tri = [](const double* S, int m, double* dst) {
+  // upper triangle row by row, each row padded with zeros to whole 16-byte
+  // vectors; off-diagonal entries hold S_de + S_ed, so the packed form gives
+  // the same quadratic form as the full matrix
+  auto pack_tri = [vec](const double* S, int m, double* dst) {
     int j = 0;
-    for (int d = 0; d < m; ++d)
-      for (int k = d; k < m; ++k) dst[j++] = k == d ? S[d * m + d] : S[d * m + k] + S[k * m + d];
+    for (int d = 0; d < m; ++d) {
+      for (int k = d; k < m; ++k) dst[j + k - d] = k == d ? S[d * m + d] : S[d * m + k] + S[k * m + d];
+      j += (m - d + vec - 1) / vec * vec;
+    }
   };
   auto pack_ind = [&](int64_t t, double* dst) {
     for (int64_t j = 0; j < Ly.istride; ++j) dst[j] = 0.0;
@@ -575,6 +587,8 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     DevBuf* dst;
     int which;
   } parts[2] = {{Ly.tstride, &e->invmat, 0}, {weno ? Ly.istride : 0, &e->ind, 1}};
+  // pseudo-inverses interleaved element by element, smoothness matrices by
+  // 16-byte vectors
   const size_t stage_bytes = (size_t)512 << 20;
   std::vector<double> host;
   for (auto& pt : parts) {
@@ -599,11 +613,17 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       int64_t total = count * pt.len;
       unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
       const double* sp = (const double*)e->staging.p;
-      // pseudo-inverses and smoothness matrices: interleaved over 32-cell groups
-      if (e->mixed)
-        k_expand_il<float, double><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
-      else
-        k_expand_il<double, double><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      if (e->mixed) {
+        if (pt.which == 0)
+          k_expand_il<float, double, 1><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+        else
+          k_expand_il<float, double, 4><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      } else {
+        if (pt.which == 0)
+          k_expand_il<double, double, 1><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+        else
+          k_expand_il<double, double, 2><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+      }
       e->launches++;
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(e->stream));

@@ -79,12 +79,14 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
       umax[v] = fmax(umax[v], un);
     }
   }
-  const T* qp = (const T*)p.qpts + c * (int64_t)MF * QS * 3;
-  const T* bm = (const T*)p.bmean + c * 3;
+  // interleaved over 32-cell groups: element j at [j * 32]
+  const T* qp = (const T*)p.qpts + (c >> 5) * (int64_t)MF * QS * 3 * 32 + (c & 31);
+  const T* bm = (const T*)p.bmean + (c >> 5) * 3 * 32 + (c & 31);
   const double epsi2 = (p.kappa_ven * p.minedge[c]) * (p.kappa_ven * p.minedge[c]) * (p.kappa_ven * p.minedge[c]);
   // unlimited face value minus the mean (recomputed rather than stored: three terms)
   auto face_d = [&](int f, int v) -> double {
-    T b0 = qp[f * QS * 3 + 0] - bm[0], b1 = qp[f * QS * 3 + 1] - bm[1], b2 = qp[f * QS * 3 + 2] - bm[2];
+    T b0 = qp[(f * QS * 3 + 0) * 32] - bm[0], b1 = qp[(f * QS * 3 + 1) * 32] - bm[32],
+      b2 = qp[(f * QS * 3 + 2) * 32] - bm[64];
     T res = b0 * g[0][v] + b1 * g[1][v] + b2 * g[2][v];
     return (u0[v] + (double)res) - u0[v];
   };
@@ -324,12 +326,14 @@ __global__ void k_reduce_final(const double* partial, int64_t np, double* out) {
 // Table upload: per-cell rows dst[c][0..len) from src[table_id[c]] (or
 // src[c - first] without ids), converted to the engine precision.
 // ======================================================================
-// Interleaved layout: row j of cell c goes to ((c/32)*len + j)*32 + c%32.
-// One block moves a 32-cell x 64-row tile through shared memory, so both the
-// per-cell source rows and the interleaved destination are accessed in
-// contiguous runs.  Cells outside [first, first+count) or whose table set is
-// outside [tlo, thi) are left untouched.
-template <typename D, typename S>
+// Interleaved layout: row j of cell c goes to ((c/32)*len + j)*32 + c%32
+// (VEC = 1), or vector-interleaved to (((c/32)*len/VEC + j/VEC)*32 + c%32)*VEC
+// + j%VEC (len a multiple of VEC).  One block moves a 32-cell x 64-row tile
+// through shared memory, so both the per-cell source rows and the
+// interleaved destination are accessed in contiguous runs.  Cells outside
+// [first, first+count) or whose table set is outside [tlo, thi) are left
+// untouched.
+template <typename D, typename S, int VEC>
 __global__ void __launch_bounds__(256) k_expand_il(D* __restrict__ dst, const S* __restrict__ src,
                                                    const int32_t* __restrict__ tid, int64_t first, int64_t count,
                                                    int64_t len, int64_t tlo, int64_t thi) {
@@ -357,8 +361,9 @@ __global__ void __launch_bounds__(256) k_expand_il(D* __restrict__ dst, const S*
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 64 * 32; i += blockDim.x) {
-      const int jj = i >> 5, lane = i & 31;
-      if (trow[lane] >= 0 && j0 + jj < len) dst[(g * len + j0 + jj) * 32 + lane] = D(tile[lane][jj]);
+      const int r = i % VEC, lane = (i / VEC) & 31, jj = (i / (VEC * 32)) * VEC + r;
+      const int64_t j = j0 + jj;
+      if (trow[lane] >= 0 && j < len) dst[((g * len + j - r) * 32 + lane * VEC) + r] = D(tile[lane][jj]);
     }
     __syncthreads();
   }

@@ -114,10 +114,13 @@ struct WVars {
   static constexpr int fall = sizeof(T) == 4 ? UCG_WV_FALL_F : UCG_WV_FALL_D;
 };
 
-// is[k] += sum_d g[d][k] * sum_{e>=d} P_de g[e][k] over d, e < nd <= NMAX
+// is[k] += sum_d g[d][k] * sum_{e>=d} P_de g[e][k] over d, e < nd <= NMAX.
+// P: the cell's packed triangle, vector-interleaved (rows padded to VEC);
+// entries past nd in a row's last vector are zero, and so is g[e] for e >= nd.
 template <int NMAX, int VG, typename T>
 __device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[NMAX][VG], int nd, T (&is)[VG]) {
-  int j = 0;
+  constexpr int VEC = Vec<T>::N;
+  int rs = 0;  // first vector of row d
 #pragma unroll
   for (int d = 0; d < NMAX; ++d) {
     if (d < nd) {
@@ -125,13 +128,17 @@ __device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[
 #pragma unroll
       for (int k = 0; k < VG; ++k) t[k] = T(0);
 #pragma unroll
-      for (int e = d; e < NMAX; ++e)
-        if (e < nd) {
-          const T s = P[(int64_t)(j + e - d) * 32];
+      for (int q = 0; q < (NMAX - d + VEC - 1) / VEC; ++q)
+        if (d + q * VEC < nd) {
+          T s[VEC];
+          ldv(P + (int64_t)(rs + q) * 32 * VEC, s);
 #pragma unroll
-          for (int k = 0; k < VG; ++k) t[k] += s * g[e][k];
+          for (int i = 0; i < VEC; ++i)
+            if (d + q * VEC + i < NMAX)
+#pragma unroll
+              for (int k = 0; k < VG; ++k) t[k] += s[i] * g[d + q * VEC + i][k];
         }
-      j += nd - d;
+      rs += (nd - d + VEC - 1) / VEC;
 #pragma unroll
       for (int k = 0; k < VG; ++k) is[k] += g[d][k] * t[k];
       // keep the loads of one row together: without this fence the
@@ -146,10 +153,14 @@ __device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[
 // polynomial, its face values and CHECKSOL; flagged cells (and every cell of
 // high-order MUSCL) take the central stencil polynomial limited by
 // Venkatakrishnan, then CHECKSOLX (3126-3406).  Output: dul [n][F][QS][5],
-// face value minus cell mean, 0 in unused slots.
+// face value minus cell mean, 0 in unused slots.  A face value is
+// sum_d m_d(x) g_d - sum_d mean(m_d) g_d: the second sum is formed once per
+// polynomial instead of subtracting the basis means at every face point.
 template <int P, typename T>
 __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
+  constexpr int VEC = Vec<T>::N;
+  constexpr int L2 = ID < 9 ? ID : 9;  // CWENO lower order: IDEGFREE2 3 or 9 (grid_p.f90:6145-6160)
   constexpr int VI = WVars<T>::is, VH = WVars<T>::face, VF = WVars<T>::fall;
   __shared__ double s_w[7 * NV * 128];  // per thread, [ll][v]: indicators, then weights
   const int tid = threadIdx.x;
@@ -162,76 +173,92 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
   const int ID2 = p.ideg2;
   const int adm = p.admis[c];
   const int nf = p.nfaces[c];
+  const int64_t grp = c >> 5;
   const int lane = (int)(c & 31);
-  const T* Gc = (const T*)p.gbuf + (c >> 5) * (int64_t)(A * ID * NV) * 32 + lane;
+  // stencil polynomials G[ll][d][v], interleaved like the tables
+  const T* Gc = (const T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
   auto G = [&](int ll, int d, int v) -> T { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
   double u0[NV], pm[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
   cons2prim(p.gamma, u0, pm);
-  const T* xq = (const T*)p.qpts + c * FQ * 3;
-  const T* bm = (const T*)p.bmean + c * ID;
+  const T* xq = (const T*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;  // interleaved
+  const T* bmv = (const T*)p.bmean + grp * (int64_t)ID * 32 + lane;    // interleaved
   T* out = (T*)p.dul + c * FQ * NV;
   double* sw = s_w + tid;  // sw[(ll * NV + v) * 128]
   const double lc1 = 1.0 - 1.0 / p.lwci;
   const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
   auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
-  // b = basis at face point (f, q) minus the basis means
-  auto basis = [&](int f, int q, T (&b)[ID]) {
-    const T* xi = xq + (f * QS + q) * 3;
-    monomials<P, T>(xi[0], xi[1], xi[2], b);
+  // monomials at face point (f, q)
+  auto mono = [&](int f, int q, T (&m)[ID]) {
+    const T* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+    monomials<P, T>(__ldcs(xi), __ldcs(xi + 32), __ldcs(xi + 64), m);
+  };
+  // g[d][k] = G(ll, d, v0 + k) for d < ndl, else 0
+  auto load_poly = [&](int ll, int v0, auto& g, int ndl) {
+    constexpr int ND = sizeof(g) / sizeof(g[0]);
+    constexpr int VV = sizeof(g[0]) / sizeof(T);
 #pragma unroll
-    for (int d = 0; d < ID; ++d) b[d] -= bm[d];
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+      for (int k = 0; k < VV; ++k) g[d][k] = (v0 + k < NV && d < ndl) ? G(ll, d, v0 + k) : T(0);
   };
   // central stencil polynomial for variables v0, v0+1, ... (as many as g
   // holds); with `rem`, the CWENO form with the low-order stencils removed
   // (reconstruct_p.f90:956-965)
   auto load_g0 = [&](int v0, auto& g, bool rem) {
     constexpr int VV = sizeof(g[0]) / sizeof(T);
+    load_poly(0, v0, g, ID);
+    if (rem) {
+      T g3[L2][VV];
 #pragma unroll
-    for (int d = 0; d < ID; ++d)
+      for (int d = 0; d < L2; ++d)
 #pragma unroll
-      for (int k = 0; k < VV; ++k) {
-        const int v = v0 + k;
-        T x = v < NV ? G(0, d, v) : T(0);
-        if (rem && v < NV) {
-          T g3 = T(0);
-          if (d < ID2)
-            for (int l2 = 1; l2 < adm; ++l2) g3 = g3 + T(lk) * G(l2, d, v);
-          x = T(1.0 / lc1) * (x - g3);
-        }
-        g[d][k] = x;
-      }
+        for (int k = 0; k < VV; ++k) g3[d][k] = T(0);
+      for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+#pragma unroll
+          for (int k = 0; k < VV; ++k)
+            if (v0 + k < NV && d < ID2) g3[d][k] = g3[d][k] + T(lk) * G(l2, d, v0 + k);
+#pragma unroll
+      for (int d = 0; d < ID; ++d)
+#pragma unroll
+        for (int k = 0; k < VV; ++k)
+          if (v0 + k < NV) g[d][k] = T(1.0 / lc1) * (g[d][k] - (d < L2 ? g3[d][k] : T(0)));
+    }
+  };
+  // sum_d mean(m_d) g[d][k]
+  auto mean_term = [&](const auto& g, auto& cb) {
+    constexpr int VV = sizeof(g[0]) / sizeof(T);
+#pragma unroll
+    for (int k = 0; k < VV; ++k) cb[k] = T(0);
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      const T b = bmv[d * 32];
+#pragma unroll
+      for (int k = 0; k < VV; ++k) cb[k] += b * g[d][k];
+    }
   };
 
   bool fall = !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
   if (!fall) {
     // ---- smoothness indicators g^T S g per stencil and variable
-    const T* Pc = (const T*)p.ind + (c >> 5) * p.istride * 32 + lane;
+    const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
     for (int ll = 0; ll < adm; ++ll) {
       const bool low = cw && ll > 0;
       for (int v0 = 0; v0 < NV; v0 += VI) {
         T is[VI];
 #pragma unroll
         for (int k = 0; k < VI; ++k) is[k] = T(0);
-        if (low) {  // CWENO lower-order stencil: IDEGFREE2 is 3 or 9 (grid_p.f90:6145-6160)
-          constexpr int L2 = ID < 9 ? ID : 9;
+        if (low) {
           T g[L2][VI];
-#pragma unroll
-          for (int d = 0; d < L2; ++d)
-#pragma unroll
-            for (int k = 0; k < VI; ++k) g[d][k] = (v0 + k < NV && d < ID2) ? G(ll, d, v0 + k) : T(0);
-          quad_form<L2, VI>(Pc + (int64_t)p.i2off * 32, g, ID2, is);
+          load_poly(ll, v0, g, ID2);
+          quad_form<L2, VI>(Pc + (int64_t)(p.i2off / VEC) * 32 * VEC, g, ID2, is);
         } else {
           T g[ID][VI];
-          if (ll == 0) {
-            load_g0(v0, g, cw);
-          } else {
-#pragma unroll
-            for (int d = 0; d < ID; ++d)
-#pragma unroll
-              for (int k = 0; k < VI; ++k) g[d][k] = v0 + k < NV ? G(ll, d, v0 + k) : T(0);
-          }
+          if (ll == 0) load_g0(v0, g, cw);
+          else load_poly(ll, v0, g, ID);
           quad_form<ID, VI>(Pc, g, ID, is);
         }
 #pragma unroll
@@ -286,6 +313,8 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
             for (int k = 0; k < VH; ++k)
               if (v0 + k < NV) gh[d][k] += wl[k] * G(ll, d, v0 + k);
       }
+      T cb[VH];
+      mean_term(gh, cb);
       for (int f = 0; f < MF; ++f) {
         const int nq = nq_of(f);
         for (int q = 0; q < QS; ++q) {
@@ -296,16 +325,16 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
               if (v0 + k < NV) o[v0 + k] = T(0);
             continue;
           }
-          T b[ID];
-          basis(f, q, b);
+          T m[ID];
+          mono(f, q, m);
           T res[VH];
 #pragma unroll
           for (int k = 0; k < VH; ++k) {
             T r = T(0);
 #pragma unroll
-            for (int d = 0; d < ID; ++d) r += b[d] * gh[d][k];
-            res[k] = r;
-            if (v0 + k < NV) o[v0 + k] = r;
+            for (int d = 0; d < ID; ++d) r += m[d] * gh[d][k];
+            res[k] = r - cb[k];
+            if (v0 + k < NV) o[v0 + k] = res[k];
           }
           if (VH == NV) {
             double uf[NV];
@@ -357,7 +386,9 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
   const double epsi2 = e3 * e3 * e3;
   for (int v0 = 0; v0 < NV; v0 += VF) {
     T g0[ID][VF];
-    load_g0(v0, g0, false);
+    load_poly(0, v0, g0, ID);
+    T cb[VF];
+    mean_term(g0, cb);
     double slope[VF];
 #pragma unroll
     for (int k = 0; k < VF; ++k) slope[k] = TOLBIG;
@@ -373,15 +404,16 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
                 if (v0 + k < NV) o[v0 + k] = T(0);
             continue;
           }
-          T b[ID];
-          basis(f, q, b);
+          T m[ID];
+          mono(f, q, m);
 #pragma unroll
           for (int k = 0; k < VF; ++k) {
             const int v = v0 + k;
             if (v >= NV) continue;
             T r = T(0);
 #pragma unroll
-            for (int d = 0; d < ID; ++d) r += b[d] * g0[d][k];
+            for (int d = 0; d < ID; ++d) r += m[d] * g0[d][k];
+            r = r - cb[k];
             const double dd = (u0[v] + (double)r) - u0[v];
             if (pass == 0) slope[k] = fmin(slope[k], venkat(dd, lo[v], hi[v], epsi2));
             else o[v] = T((double)T(dd) * slope[k]);
@@ -448,9 +480,9 @@ __global__ void k_visc_face(Problem p) {
   const int64_t c = i / (MF * QS);
   const int r = (int)(i - c * MF * QS), f = r / QS, q = r - f * QS;
   if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) return;
-  const T* xi = (const T*)p.qpts + ((c * MF + f) * QS + q) * 3;
+  const T* xi = (const T*)p.qpts + ((c >> 5) * MF * QS * 3 + (f * QS + q) * 3) * 32 + (c & 31);
   double dx[ID], dy[ID], dz[ID];
-  dmonomials<P>((double)xi[0], (double)xi[1], (double)xi[2], dx, dy, dz);
+  dmonomials<P>((double)xi[0], (double)xi[32], (double)xi[64], dx, dy, dz);
   const double* J = p.jinv + c * 9;
   double* o = p.ulv + ((c * MF + f) * QS + q) * 12;
 #pragma unroll
