@@ -142,6 +142,14 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+# DRAM bytes per cell of one k_lsq launch (mixed form, WENO5 on hexahedra),
+# dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the
+# 32^3 case divided by its 32,768 cells (profiles/k_lsq_mixed_vortex_n32.md);
+# the traffic grows in proportion to the cells (no re-reads), so a launch on
+# n^3 cells moves this times n^3.
+LSQ_DRAM_BYTES_PER_CELL_MIXED_WENO5_HEX = 106_700
+
+
 def lsq_bytes_per_cell(cfg):
     """Algorithmic bytes of k_lsq per cell: the pseudo-inverse slices and
     stencil indices of every stencil, the cell's own state, and the stencil
@@ -326,6 +334,8 @@ def main():
     lsq_ms = r32["kern"]["lsq"]
     achieved = bpc * ncells / (lsq_ms / 1000.0) / 1e9
     rbpc = recon_bytes_per_cell(cfg32)
+    traffic = (LSQ_DRAM_BYTES_PER_CELL_MIXED_WENO5_HEX * ncells
+               if args.case == "vortex_hex_weno5" else None)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -334,7 +344,8 @@ def main():
         "config": {"workload": args.case, "cells": ncells, "n": args.n, "scheme": "WENO5+HLLC SSP-RK3",
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (tables)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": None, "kernel": "k_lsq (stencil least squares)",
+                     "peak_kind": peak_kind, "traffic": traffic, "traffic_unit": "bytes per launch",
+                     "kernel": "k_lsq (stencil least squares)",
                      "bytes_per_cell": bpc, "kernel_ms": lsq_ms,
                      "reconstruction": {"kernels": "k_lsq + k_wpost", "bytes_per_cell": rbpc,
                                         "ms": r32["kern"]["recon"],
