@@ -221,6 +221,38 @@ int ucg_last_error(const ucg_engine* e, char* buf, int32_t len);
  * UCG_ECUDA.                                                              */
 int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, const ucg_recon* rec,
                               const double* u, double* rhs, void* stream);
+/* ---------------------------------------------------------------- adjoint
+ * Discrete adjoint (VJP) and tangent (JVP) for the FP64 form of a MUSCL
+ * (scheme 2, IORDER 1) Euler configuration (the adjoint workload is the
+ * bump channel).  p denotes the free-stream state bc_state[5] (primitive:
+ * rho, u, v, w, pressure) used by the inflow, outflow and far-field ghost
+ * states.  Host arrays; [n][5] as everywhere.  Other configurations return
+ * UCG_EINVAL.
+ *
+ * ucg_force: integrated wall pressure force in x at the current state,
+ *   J = sum over faces with BC code 4 of (sum_q w_q p(u_face,q) - pres) * area
+ *   * n_x, with the reconstructed face values (COMPUTEFORCE, src/io.f90:18752,
+ *   inviscid part).
+ * ucg_force_vjp: dJ/dU at the current state.
+ * ucg_residual_vjp: mu = (dR/dU)^T lambda and, if pbar != NULL,
+ *   pbar = (dR/dp)^T lambda, R the residual of ucg_residual.
+ * ucg_residual_jvp: drhs = (dR/dU) du + (dR/dp) dp (dp may be NULL).
+ * ucg_adjoint_run: nsteps RK3 steps of fixed dt from the current state, J at
+ *   the final state, and its gradients w.r.t. the initial state (dJdU0) and
+ *   p (dJdp[5]) by reverse sweeps over segments of `every` steps, each
+ *   segment recomputed from its checkpoint.  The handle's state becomes the
+ *   final state.
+ * ucg_tangent_run: the same steps with tangents dU0 (and dp), J and
+ *   dJ = <dJ/dU0, dU0> + <dJ/dp, dp> by forward mode; state as above.    */
+int ucg_force(ucg_engine* e, double* fx);
+int ucg_force_vjp(ucg_engine* e, double* dJdU);
+int ucg_residual_vjp(ucg_engine* e, const double* lambda, double* mu, double* pbar);
+int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* drhs);
+int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, double* J, double* dJdU0,
+                    double* dJdp);
+int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
+                    double* dJ);
+
 /* Message of the last failure of ucg_create (no handle exists then). */
 const char* ucg_create_error(void);
 

@@ -42,6 +42,8 @@ def lib():
         L.orc_hllc.argtypes = [C.c_double, f64p, f64p, f64p]
         L.orc_reduce.restype = C.c_int
         L.orc_reduce.argtypes = [geop, f64p, C.c_int, f64p]
+        L.orc_force.restype = C.c_int
+        L.orc_force.argtypes = [cfgp, geop, recp, f64p, f64p]
         _lib = L
     return _lib
 
@@ -98,6 +100,15 @@ class Oracle:
         if rc:
             raise RuntimeError(f"orc_rk3_step failed: {rc}")
         return U
+
+    def force(self, U: np.ndarray) -> float:
+        """Wall pressure force in x (COMPUTEFORCE, inviscid part)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = C.c_double()
+        rc = lib().orc_force(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U), C.byref(out))
+        if rc:
+            raise RuntimeError(f"orc_force failed: {rc}")
+        return out.value
 
     def reduce(self, U: np.ndarray, what: int) -> float:
         U = np.ascontiguousarray(U, dtype=np.float64)

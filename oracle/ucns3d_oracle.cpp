@@ -641,6 +641,38 @@ int orc_rk3_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* 
   return UCG_OK;
 }
 
+// Wall force in x (COMPUTEFORCE, src/io.f90:18752-18915, inviscid part):
+// over faces with boundary code 4, SSP = sum_q p(ULEFT_q) * w_q - PRES, then
+// FORCEX += SSP * SURF * NX with NX = cos(angle1) * sin(angle2).
+int orc_force(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, const double* U, double* fx) {
+  if (!check_ctx(cfg, g, r) || !U || !fx) return UCG_EINVAL;
+  const int64_t n = g->ncells;
+  std::vector<double> ul((size_t)n * F * Q * NV);
+  int rc = orc_face_values(cfg, g, r, U, ul.data());
+  if (rc) return rc;
+  Ctx x{cfg, g, r, n, monos(cfg->iorder)};
+  double force = 0.0;
+  for (int64_t c = 0; c < n; ++c)
+    for (int f = 0; f < g->nfaces[c]; ++f) {
+      if (g->neigh[c * F + f] >= 0 || g->bc[c * F + f] != 4) continue;
+      const bool quad = g->face_type[c * F + f] == 5;
+      const int nq = quad ? cfg->nq_quad : cfg->nq_tri;
+      const double* w = quad ? cfg->quad_w : cfg->tri_w;
+      double ssp = 0.0;
+      for (int q = 0; q < nq; ++q) {
+        double pm[NV];
+        cons2prim(x, &ul[(((size_t)c * F + f) * Q + q) * NV], pm);
+        ssp = ssp + (pm[4] * w[q]);
+      }
+      ssp = ssp - cfg->pres;
+      const double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+      const double nx = std::cos(a1) * std::sin(a2);
+      force = force + ((ssp * g->face_area[c * F + f]) * nx);
+    }
+  *fx = force;
+  return UCG_OK;
+}
+
 // HLLC flux of two conserved states in the face frame (known-answer tests).
 int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
   hllc(gamma, cl, cr, flux);

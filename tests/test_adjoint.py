@@ -1,0 +1,227 @@
+"""Discrete adjoint (VJP) and tangent (JVP) of the MUSCL residual, the wall
+force and SSP-RK3 steps on the bump channel (hexahedra + prisms, inflow,
+outflow, slip walls), FP64 form, through the C ABI.
+
+Checks, as the adjoint's contract asks:
+  * force J against the oracle's COMPUTEFORCE restatement (1e-12 relative);
+  * residual JVP against central finite differences of the oracle's FP64
+    residual, in the state and in the free-stream state (FD step 1e-6 of the
+    perturbation scale; truncation error O(eps^2));
+  * dot-product test <lam, JVP(du, dp)> = <VJP_U(lam), du> + <VJP_p(lam), dp>
+    (1e-12 relative: both sides are the same derivatives);
+  * through RK3 steps with checkpoints: tangent run vs adjoint run (dot
+    product), adjoint run vs finite differences of J after the same steps of
+    the oracle, and independence of the checkpoint stride.
+Base states: the free stream marched from the inflow (limiters active at the
+bump) plus a seeded 3D perturbation, so that no two states tie (see
+_generic_state).
+"""
+import numpy as np
+import pytest
+
+from ucns3d_b200 import _native as N
+from ucns3d_b200 import cases
+from ucns3d_b200.engine import Engine, EngineError
+
+pytestmark = pytest.mark.gpu
+
+
+def _generic_state(c, nsteps, seed):
+    """The free stream marched `nsteps` steps (limiters active at the bump),
+    then a 3% perturbation that varies in x, y and z: the base state must be
+    generic, since at exactly equal states (a z-invariant flow on a layered
+    mesh) the Einfeldt wave-speed min/max of HLLC and the FIND_BOUNDS min/max
+    have ties where the residual has no derivative."""
+    e = Engine(c.mesh, c.cfg)
+    e.set_state(c.U0)
+    e.time_marching(nsteps, 0.5)
+    U = e.get_state()
+    rng = np.random.default_rng(seed)
+    cc = c.mesh.centres()
+    U = U * (1.0 + 0.03 * np.sin(3.1 * cc[:, :1] + 1.7 * cc[:, 1:2] + 40.0 * cc[:, 2:3] + rng.uniform(0, 6.3, (1, 5))))
+    e.set_state(U)
+    return e, U
+
+
+@pytest.fixture(scope="module")
+def bump():
+    from oracle import Oracle
+    c = cases.bump_muscl(nx=60, ny=20, nlayers=4)
+    e, U = _generic_state(c, 40, 7)
+    dt = e.calculate_cfl(0.5)
+    yield dict(case=c, engine=e, U=U, dt=dt, oracle=Oracle(c.mesh, c.cfg))
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def short_bump():
+    """A short channel, so that the inflow state reaches the bump within the
+    200 steps of the adjoint runs."""
+    c = cases.bump_muscl(nx=24, ny=8, nlayers=4)
+    e, U = _generic_state(c, 20, 11)
+    dt = e.calculate_cfl(0.5)
+    yield dict(case=c, engine=e, U=U, dt=dt)
+    e.close()
+
+
+def _cfg_with_bc(cfg, bc):
+    out = N.UcgConfig.from_buffer_copy(cfg)
+    for k in range(5):
+        out.bc_state[k] = bc[k]
+    return out
+
+
+def _directions(U, seed):
+    rng = np.random.default_rng(seed)
+    du = rng.standard_normal(U.shape) * np.abs(U).max(0) * 1e-2
+    dp = rng.standard_normal(5) * np.array([1.0, 0.8, 0.0, 0.0, 1.0]) * 1e-2
+    return du, dp
+
+
+def test_force_matches_oracle(bump):
+    e, o, U = bump["engine"], bump["oracle"], bump["U"]
+    e.set_state(U)
+    a, b = e.force(), o.force(U)
+    assert abs(a - b) <= 1e-12 * max(1.0, abs(b)), (a, b)
+
+
+def test_residual_jvp_matches_oracle_fd(bump):
+    from oracle import Oracle
+    c, e, U = bump["case"], bump["engine"], bump["U"]
+    e.set_state(U)
+    du, dp = _directions(U, 1)
+    jvp = e.residual_jvp(du, dp)
+    eps = 1e-6
+    bc = np.array([c.cfg.bc_state[k] for k in range(5)])
+    op = Oracle(c.mesh, _cfg_with_bc(c.cfg, bc + eps * dp))
+    om = Oracle(c.mesh, _cfg_with_bc(c.cfg, bc - eps * dp))
+    fd = (op.residual(U + eps * du) - om.residual(U - eps * du)) / (2 * eps)
+    scale = np.abs(fd).max(0) + 1e-300
+    err = (np.abs(jvp - fd) / scale).max(1)
+    # measured: median 3e-9, max 3e-8 (the FD's own roundoff at this step)
+    assert err.max() < 1e-6, np.sort(err)[-5:]
+    assert np.median(err) < 1e-7
+
+
+def test_vjp_jvp_dot_product(bump):
+    e, U = bump["engine"], bump["U"]
+    e.set_state(U)
+    du, dp = _directions(U, 2)
+    lam = np.random.default_rng(3).standard_normal(U.shape)
+    jvp = e.residual_jvp(du, dp)
+    mu, pbar = e.residual_vjp(lam)
+    a = float(np.sum(lam * jvp))
+    b = float(np.sum(mu * du) + np.sum(pbar * dp))
+    assert abs(a - b) <= 1e-12 * (np.abs(lam * jvp).sum()), (a, b)
+
+
+def test_force_vjp_matches_fd(bump):
+    e, U = bump["engine"], bump["U"]
+    du, _ = _directions(U, 4)
+    e.set_state(U)
+    g = e.force_vjp()
+    eps = 1e-6
+    e.set_state(U + eps * du)
+    jp = e.force()
+    e.set_state(U - eps * du)
+    jm = e.force()
+    e.set_state(U)
+    fd = (jp - jm) / (2 * eps)
+    ad = float(np.sum(g * du))
+    assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-30), (ad, fd)
+
+
+NSTEPS, EVERY = 200, 20
+
+
+def test_adjoint_run_matches_tangent_run(short_bump):
+    e, U, dt = short_bump["engine"], short_bump["U"], short_bump["dt"]
+    du, dp = _directions(U, 5)
+    e.set_state(U)
+    J1, dJ = e.tangent_run(NSTEPS, dt, du, dp)
+    e.set_state(U)
+    J2, g, gp = e.adjoint_run(NSTEPS, dt, every=EVERY)
+    assert J1 == J2
+    ad = float(np.sum(g * du) + np.sum(gp * dp))
+    assert abs(ad - dJ) <= 1e-10 * max(abs(dJ), 1e-30), (ad, dJ)
+
+
+def test_adjoint_run_matches_oracle_fd(short_bump):
+    from oracle import Oracle
+    c, e, U, dt = short_bump["case"], short_bump["engine"], short_bump["U"], short_bump["dt"]
+    e.set_state(U)
+    J, g, gp = e.adjoint_run(NSTEPS, dt, every=EVERY)
+    bc = np.array([c.cfg.bc_state[k] for k in range(5)])
+
+    def J_oracle(U0, bcs):
+        o = Oracle(c.mesh, _cfg_with_bc(c.cfg, bcs))
+        W = U0.copy()
+        for _ in range(NSTEPS):
+            W = o.rk3_step(W, dt)
+        return o.force(W)
+
+    assert abs(J_oracle(U, bc) - J) <= 1e-10 * max(1.0, abs(J))
+    eps = 1e-6
+    du, dp = _directions(U, 6)
+    fd_u = (J_oracle(U + eps * du, bc) - J_oracle(U - eps * du, bc)) / (2 * eps)
+    fd_p = (J_oracle(U, bc + eps * dp) - J_oracle(U, bc - eps * dp)) / (2 * eps)
+    ad_u, ad_p = float(np.sum(g * du)), float(np.sum(gp * dp))
+    assert abs(ad_u - fd_u) <= 1e-5 * max(abs(fd_u), 1e-30), (ad_u, fd_u)
+    assert abs(ad_p - fd_p) <= 1e-5 * max(abs(fd_p), 1e-30), (ad_p, fd_p)
+
+
+def test_checkpoint_stride_does_not_change_gradients(short_bump):
+    e, U, dt = short_bump["engine"], short_bump["U"], short_bump["dt"]
+    out = []
+    for every in (1, 7, EVERY, NSTEPS):
+        e.set_state(U)
+        out.append(e.adjoint_run(NSTEPS, dt, every=every))
+    for J, g, gp in out[1:]:
+        assert J == out[0][0]
+        assert np.array_equal(g, out[0][1]) and np.array_equal(gp, out[0][2])
+
+
+def test_torch_autograd_function(bump):
+    """The residual as a torch.autograd.Function (test harness only):
+    backward is the engine's VJP; the gradient of a scalar built on it
+    matches finite differences."""
+    import torch
+    e, U = bump["engine"], bump["U"]
+
+    class Residual(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, u):
+            e.set_state(u.detach().cpu().numpy())
+            ctx.save_for_backward(u)
+            return torch.from_numpy(e.residual())
+
+        @staticmethod
+        def backward(ctx, g):
+            (u,) = ctx.saved_tensors
+            e.set_state(u.detach().cpu().numpy())
+            mu, _ = e.residual_vjp(g.detach().cpu().numpy())
+            return torch.from_numpy(mu)
+
+    w = torch.from_numpy(np.random.default_rng(8).standard_normal(U.shape))
+    u = torch.from_numpy(U.copy()).requires_grad_(True)
+    Jt = (w * Residual.apply(u)).sum()
+    (gu,) = torch.autograd.grad(Jt, u)
+    du, _ = _directions(U, 9)
+    eps = 1e-6
+    with torch.no_grad():
+        jp = float((w * Residual.apply(torch.from_numpy(U + eps * du))).sum())
+        jm = float((w * Residual.apply(torch.from_numpy(U - eps * du))).sum())
+    fd = (jp - jm) / (2 * eps)
+    ad = float((gu * torch.from_numpy(du)).sum())
+    assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
+    e.set_state(U)
+
+
+def test_adjoint_rejects_other_configurations():
+    c = cases.vortex_hex_weno5(n=8)
+    e = Engine(c.mesh, c.cfg)
+    e.set_state(c.U0)
+    with pytest.raises(EngineError) as ei:
+        e.force()
+    assert ei.value.code == N.UCG_EINVAL
+    e.close()

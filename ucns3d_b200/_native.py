@@ -132,7 +132,8 @@ ENGINE_SYMBOLS = [
     "ucg_set_state", "ucg_get_state", "ucg_compute_dt", "ucg_residual", "ucg_rk3_step",
     "ucg_step", "ucg_last_dt", "ucg_reduce", "ucg_check_health", "ucg_synchronize",
     "ucg_time_kernels", "ucg_get_stream", "ucg_launch_count", "ucg_device_bytes", "ucg_last_error",
-    "ucg_create_error",
+    "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
+    "ucg_tangent_run",
 ]
 
 
@@ -182,6 +183,18 @@ def engine() -> C.CDLL:
         lib.ucg_last_error.argtypes = [vp, C.c_char_p, C.c_int32]
         lib.ucg_create_error.restype = C.c_char_p
         lib.ucg_create_error.argtypes = []
+        lib.ucg_force.restype = C.c_int
+        lib.ucg_force.argtypes = [vp, _f64p]
+        lib.ucg_force_vjp.restype = C.c_int
+        lib.ucg_force_vjp.argtypes = [vp, _f64p]
+        lib.ucg_residual_vjp.restype = C.c_int
+        lib.ucg_residual_vjp.argtypes = [vp, _f64p, _f64p, _f64p]
+        lib.ucg_residual_jvp.restype = C.c_int
+        lib.ucg_residual_jvp.argtypes = [vp, _f64p, _f64p, _f64p]
+        lib.ucg_adjoint_run.restype = C.c_int
+        lib.ucg_adjoint_run.argtypes = [vp, C.c_int32, C.c_double, C.c_int32, _f64p, _f64p, _f64p]
+        lib.ucg_tangent_run.restype = C.c_int
+        lib.ucg_tangent_run.argtypes = [vp, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
         _engine = lib
     return _engine
 

@@ -1,0 +1,919 @@
+// Discrete adjoint (VJP) and tangent (JVP) of the engine's MUSCL residual,
+// of the wall pressure force and of SSP-RK3 steps, for the FP64 form of a
+// MUSCL (scheme 2, IORDER 1) Euler configuration.
+//
+// Residual R(U) = net outward flux (CALL_FLUX_SUBROUTINES_3D,
+// src/time_p.f90:2253-2497); force J(U) = sum over wall faces (BC code 4) of
+// (sum_q w_q p(u_face,q) - PRES) * area * n_x (COMPUTEFORCE,
+// src/io.f90:18752-18915, inviscid part).
+//
+// VJP of R: mu = (dR/dU)^T lambda, pbar = (dR/dp)^T lambda (p: the
+// free-stream state of the inflow/outflow conditions, Problem::bc_state).
+//   1. k_adj_face   one thread per owned face: the 5x10 Jacobian of the face
+//                   flux w.r.t. its two states (or its state and p) from
+//                   dual numbers, applied transposed to lambda_c - lambda_nb;
+//                   gives the adjoint of every face value.
+//   2. k_adj_muscl  one thread per cell: the MUSCL reconstruction (LSQ,
+//                   FIND_BOUNDS, Venkatakrishnan, CHECKSOLX) reversed by
+//                   hand; its contributions to the cell, its stencil cells
+//                   and its face neighbours go to per-slot buffers.
+//   3. k_adj_gather one thread per cell: sums the slots that point at it,
+//                   through a reverse map built on the host in a fixed
+//                   order, so results are deterministic (no atomics).
+// JVP: the same reconstruction and fluxes on Dual<1> numbers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ad.cuh"
+#include "engine_internal.h"
+
+using namespace ucg;
+using namespace ucg_host;
+using ad::Dual;
+
+namespace {
+
+// ------------------------------------------------------------ set-up checks
+int adj_check(ucg_engine* e) {
+  if (!e) return UCG_EINVAL;
+  const ucg_config& c = e->cfg;
+  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64))
+    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1), Euler, FP64 form");
+  if (e->QS != 1) return fail(e, UCG_EINVAL, "the adjoint needs one face point per face (IORDER 1)");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  return UCG_OK;
+}
+
+// elementwise: y = a*x + b*y  (n*5)
+__global__ void k_axpby(int64_t m, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) y[i] = a * x[i] + b * y[i];
+}
+// lam[c][v] = s * x[c][v] / V_c
+__global__ void k_over_vol(Problem p, double s, const double* __restrict__ x, double* __restrict__ lam) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < p.n * NV) lam[i] = s * x[i] / p.vol[i / NV];
+}
+// acc[k] += s * part[k], k < 5
+__global__ void k_pacc(double s, const double* __restrict__ part, double* __restrict__ acc) {
+  if (threadIdx.x < NV) acc[threadIdx.x] += s * part[threadIdx.x];
+}
+
+// deterministic column sums of a [m][5] array: block k sums column k
+__global__ void __launch_bounds__(256) k_colsum5(const double* __restrict__ a, int64_t m, double* __restrict__ out) {
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < m; i += blockDim.x) s += a[i * NV + k];
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = sh[0];
+}
+// deterministic sum of a [m] array
+__global__ void __launch_bounds__(1024) k_sum1(const double* __restrict__ a, int64_t m, double* __restrict__ out) {
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < m; i += blockDim.x) s += a[i];
+  __shared__ double sh[1024];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+// ------------------------------------------------------------ face VJP
+// adjF[c][f] = adjoint of the face value of cell c at face f;
+// pface[c][f] = adjoint of the free-stream state from boundary face (c, f).
+__global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __restrict__ U,
+                                                  const double* __restrict__ lam, double* __restrict__ adjF,
+                                                  double* __restrict__ pface) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nown) return;
+  const int32_t code = p.own[i];
+  const int64_t c = code >> 3;
+  const int f = code & 7;
+  const int64_t nb = p.neigh[c * MF + f];
+  const int nf = p.nface[c * MF + f];
+  double r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
+  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
+  const double* dul = (const double*)p.dul;
+  Dual<10> L[NV], R[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    L[v] = Dual<10>(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
+    L[v].d[v] = 1.0;
+  }
+  double g[NV];
+  if (nb >= 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      R[v] = Dual<10>(U[nb * NV + v] + dul[(nb * MF + nf) * NV + v]);
+      R[v].d[5 + v] = 1.0;
+      g[v] = lam[c * NV + v] - lam[nb * NV + v];
+    }
+  } else {
+    Dual<10> bcs[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      bcs[v] = Dual<10>(p.bc_state[v]);
+      bcs[v].d[5 + v] = 1.0;
+      g[v] = lam[c * NV + v];
+    }
+    boundary_ghost(p, (int)p.bc[c * MF + f], r, L, bcs, R);
+  }
+  Dual<10> a[NV], b[NV], h[NV], fl[NV];
+  rot_f(r, R, b);
+  rot_f(r, L, a);
+  hllc(p.gamma, a, b, h);
+  rot_b(r, h, fl);
+  double out[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    double s = 0.0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[k];
+    out[k] = ws * s;
+  }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = out[k];
+  if (nb >= 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) adjF[(nb * MF + nf) * NV + k] = out[5 + k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) pface[(c * MF + f) * NV + k] = out[5 + k];
+  }
+}
+
+// ------------------------------------------------------------ MUSCL reverse
+// Forward quantities of the MUSCL reconstruction of cell c (k_muscl,
+// IORDER 1, Euler), kept for the reverse sweep.
+struct MusclFwd {
+  double u0[NV];
+  double g[3][NV];
+  double lo[NV], hi[NV];   // bounds relative to u0
+  int amin[NV], amax[NV];  // slot of the bound: 0 the cell, 1 + IMAX + f face neighbour f
+  double slope[NV];
+  int fstar[NV];           // face of the limiting value, -1 if none
+  double epsi2;
+  bool first;              // CHECKSOLX: first order
+};
+
+__device__ __forceinline__ void muscl_basis(const Problem& p, int64_t c, int f, double* b) {
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const double* qp = (const double*)p.qpts + (c >> 5) * (int64_t)MF * QS * 3 * 32 + (c & 31);
+  const double* bm = (const double*)p.bmean + (c >> 5) * 3 * 32 + (c & 31);
+  b[0] = qp[(f * QS * 3 + 0) * 32] - bm[0];
+  b[1] = qp[(f * QS * 3 + 1) * 32] - bm[32];
+  b[2] = qp[(f * QS * 3 + 2) * 32] - bm[64];
+}
+
+__device__ __forceinline__ double muscl_dd(const MusclFwd& m, const double* b, int v) {
+  const double res = b[0] * m.g[0][v] + b[1] * m.g[1][v] + b[2] * m.g[2][v];
+  return (m.u0[v] + res) - m.u0[v];
+}
+
+__device__ void muscl_forward(const Problem& p, const double* __restrict__ U, int64_t c, MusclFwd& m) {
+  const int IM = p.imax, W = IM + 1, nf = p.nfaces[c];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) m.u0[v] = U[c * NV + v];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) m.g[d][v] = 0.0;
+  for (int k = 0; k < IM; ++k) {
+    const int64_t y = st[(k + 1) * 32];
+    const double m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double du = U[y * NV + v] - m.u0[v];
+      m.g[0][v] += m0 * du;
+      m.g[1][v] += m1 * du;
+      m.g[2][v] += m2 * du;
+    }
+  }
+  double mn[NV], mx[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    mn[v] = mx[v] = m.u0[v];
+    m.amin[v] = m.amax[v] = 0;
+  }
+  for (int f = 0; f < nf; ++f) {
+    const int64_t nb = p.neigh[c * MF + f];
+    if (nb < 0) continue;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double un = U[nb * NV + v];
+      if (un < mn[v]) {
+        mn[v] = un;
+        m.amin[v] = 1 + IM + f;
+      }
+      if (un > mx[v]) {
+        mx[v] = un;
+        m.amax[v] = 1 + IM + f;
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    m.lo[v] = mn[v] - m.u0[v];
+    m.hi[v] = mx[v] - m.u0[v];
+  }
+  const double e3 = p.kappa_ven * p.minedge[c];
+  m.epsi2 = e3 * e3 * e3;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    m.slope[v] = TOLBIG;
+    m.fstar[v] = -1;
+  }
+  for (int f = 0; f < nf; ++f) {
+    double b[3];
+    muscl_basis(p, c, f, b);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double ps = venkat(muscl_dd(m, b, v), m.lo[v], m.hi[v], m.epsi2);
+      if (ps < m.slope[v]) {
+        m.slope[v] = ps;
+        m.fstar[v] = f;
+      }
+    }
+  }
+  double pm[NV];
+  cons2prim(p.gamma, m.u0, pm);
+  m.first = false;
+  for (int f = 0; f < nf; ++f) {
+    double b[3], uf[NV];
+    muscl_basis(p, c, f, b);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) uf[v] = m.u0[v] + muscl_dd(m, b, v) * m.slope[v];
+    m.first = m.first || jump_bad(p.gamma, pm, uf, 0.95);
+  }
+}
+
+// contrib[c][slot][v]: slot 0 the cell, 1..IMAX its stencil cells, 1+IMAX+f
+// its face neighbour f.  Face values u_f = u0 + dd_f * slope (or u0 when
+// CHECKSOLX chose first order).
+__global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const double* __restrict__ U,
+                                                   const double* __restrict__ adjF, double* __restrict__ contrib,
+                                                   int slots) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const int IM = p.imax, nf = p.nfaces[c];
+  MusclFwd m;
+  muscl_forward(p, U, c, m);
+  double* out = contrib + c * (int64_t)slots * NV;
+  for (int s = 0; s < slots * NV; ++s) out[s] = 0.0;
+  double self[NV] = {0, 0, 0, 0, 0};
+  if (m.first) {
+    for (int f = 0; f < nf; ++f)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) self[v] += adjF[(c * MF + f) * NV + v];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = self[v];
+    return;
+  }
+  // reverse of u_f = u0 + dd_f * slope, slope = psi_{f*}, dd_f = b_f . g
+  double gbar[3][NV] = {};
+  double lob[NV] = {0, 0, 0, 0, 0}, hib[NV] = {0, 0, 0, 0, 0};
+  double sbar[NV] = {0, 0, 0, 0, 0};
+  for (int f = 0; f < nf; ++f) {
+    double b[3];
+    muscl_basis(p, c, f, b);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double ub = adjF[(c * MF + f) * NV + v];
+      self[v] += ub;
+      sbar[v] += ub * muscl_dd(m, b, v);
+      const double ddb = ub * m.slope[v];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) gbar[d][v] += ddb * b[d];
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const int fs = m.fstar[v];
+    if (fs < 0) continue;
+    double b[3];
+    muscl_basis(p, c, fs, b);
+    Dual<3> dd(muscl_dd(m, b, v)), lo(m.lo[v]), hi(m.hi[v]);
+    dd.d[0] = 1.0;
+    lo.d[1] = 1.0;
+    hi.d[2] = 1.0;
+    const Dual<3> ps = venkat(dd, lo, hi, m.epsi2);
+    const double ddb = sbar[v] * ps.d[0];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gbar[d][v] += ddb * b[d];
+    lob[v] += sbar[v] * ps.d[1];
+    hib[v] += sbar[v] * ps.d[2];
+  }
+  // g = sum_k M_k (u_k - u0)
+  const int W = IM + 1;
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  for (int k = 0; k < IM; ++k) {
+    const double m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const double ck = m0 * gbar[0][v] + m1 * gbar[1][v] + m2 * gbar[2][v];
+      out[(1 + k) * NV + v] += ck;
+      self[v] -= ck;
+    }
+  }
+  (void)W;
+  // lo = min(...) - u0, hi = max(...) - u0
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    self[v] -= lob[v] + hib[v];
+    out[m.amin[v] * NV + v] += lob[v];
+    out[m.amax[v] * NV + v] += hib[v];
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) out[v] += self[v];
+}
+
+// mu[j] = sum over the slots that point at cell j (reverse map, fixed order)
+__global__ void k_adj_gather(int64_t n, const int64_t* __restrict__ rptr, const int64_t* __restrict__ rsrc,
+                             const double* __restrict__ contrib, double* __restrict__ mu) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double s[NV] = {0, 0, 0, 0, 0};
+  for (int64_t e = rptr[j]; e < rptr[j + 1]; ++e) {
+    const double* x = contrib + rsrc[e] * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] += x[v];
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) mu[j * NV + v] = s[v];
+}
+
+// ------------------------------------------------------------ tangent
+struct Dp5 {
+  double v[NV];
+};
+
+// tangent of the face values: tdul[c][f] = d(u_f - u0) along dU
+__global__ void __launch_bounds__(128) k_jvp_muscl(Problem p, const double* __restrict__ U,
+                                                   const double* __restrict__ dU, double* __restrict__ tdul) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  using D = Dual<1>;
+  const int IM = p.imax, W = IM + 1, nf = p.nfaces[c];
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  D u0[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    u0[v] = D(U[c * NV + v]);
+    u0[v].d[0] = dU[c * NV + v];
+  }
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  D g[3][NV];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) g[d][v] = D(0.0);
+  for (int k = 0; k < IM; ++k) {
+    const int64_t y = st[(k + 1) * 32];
+    const double m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      D uy(U[y * NV + v]);
+      uy.d[0] = dU[y * NV + v];
+      const D du = uy - u0[v];
+      g[0][v] = g[0][v] + m0 * du;
+      g[1][v] = g[1][v] + m1 * du;
+      g[2][v] = g[2][v] + m2 * du;
+    }
+  }
+  D mn[NV], mx[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) mn[v] = mx[v] = u0[v];
+  for (int f = 0; f < nf; ++f) {
+    const int64_t nb = p.neigh[c * MF + f];
+    if (nb < 0) continue;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      D un(U[nb * NV + v]);
+      un.d[0] = dU[nb * NV + v];
+      if (un.v < mn[v].v) mn[v] = un;
+      if (un.v > mx[v].v) mx[v] = un;
+    }
+  }
+  const double e3 = p.kappa_ven * p.minedge[c];
+  const double epsi2 = e3 * e3 * e3;
+  const double* qp = (const double*)p.qpts + grp * (int64_t)MF * QS * 3 * 32 + lane;
+  const double* bm = (const double*)p.bmean + grp * 3 * 32 + lane;
+  auto face_d = [&](int f, int v) -> D {
+    const double b0 = qp[(f * QS * 3 + 0) * 32] - bm[0], b1 = qp[(f * QS * 3 + 1) * 32] - bm[32],
+                 b2 = qp[(f * QS * 3 + 2) * 32] - bm[64];
+    const D res = b0 * g[0][v] + b1 * g[1][v] + b2 * g[2][v];
+    return (u0[v] + res) - u0[v];
+  };
+  D slope[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) slope[v] = D(TOLBIG);
+  for (int f = 0; f < nf; ++f)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const D ps = venkat(face_d(f, v), mn[v] - u0[v], mx[v] - u0[v], epsi2);
+      if (ps.v < slope[v].v) slope[v] = ps;
+    }
+  double pm[NV], u0v[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0v[v] = u0[v].v;
+  cons2prim(p.gamma, u0v, pm);
+  bool first = false;
+  for (int f = 0; f < nf; ++f) {
+    double uf[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) uf[v] = u0v[v] + face_d(f, v).v * slope[v].v;
+    first = first || jump_bad(p.gamma, pm, uf, 0.95);
+  }
+  for (int f = 0; f < nf; ++f)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tdul[(c * MF + f) * NV + v] = first ? 0.0 : (face_d(f, v) * slope[v]).d[0];
+}
+
+// tangent of the face fluxes (owner and negated neighbour copy)
+__global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __restrict__ U,
+                                                  const double* __restrict__ dU, const double* __restrict__ tdul,
+                                                  Dp5 dp, double* __restrict__ tflux) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nown) return;
+  using D = Dual<1>;
+  const int32_t code = p.own[i];
+  const int64_t c = code >> 3;
+  const int f = code & 7;
+  const int64_t nb = p.neigh[c * MF + f];
+  const int nf = p.nface[c * MF + f];
+  double r[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
+  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
+  const double* dul = (const double*)p.dul;
+  D L[NV], R[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    L[v] = D(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
+    L[v].d[0] = dU[c * NV + v] + tdul[(c * MF + f) * NV + v];
+  }
+  if (nb >= 0) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      R[v] = D(U[nb * NV + v] + dul[(nb * MF + nf) * NV + v]);
+      R[v].d[0] = dU[nb * NV + v] + tdul[(nb * MF + nf) * NV + v];
+    }
+  } else {
+    D bcs[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      bcs[v] = D(p.bc_state[v]);
+      bcs[v].d[0] = dp.v[v];
+    }
+    boundary_ghost(p, (int)p.bc[c * MF + f], r, L, bcs, R);
+  }
+  D a[NV], b[NV], h[NV], fl[NV];
+  rot_f(r, R, b);
+  rot_f(r, L, a);
+  hllc(p.gamma, a, b, h);
+  rot_b(r, h, fl);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) tflux[(c * MF + f) * NV + v] = fl[v].d[0] * ws;
+  if (nb >= 0)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tflux[(nb * MF + nf) * NV + v] = -(fl[v].d[0] * ws);
+}
+
+// tangent of the residual: face sums in face order
+__global__ void k_jvp_sum(Problem p, const double* __restrict__ tflux, double* __restrict__ dR) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  double s[NV] = {0, 0, 0, 0, 0};
+  for (int f = 0; f < p.nfaces[c]; ++f)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = s[v] + tflux[(c * MF + f) * NV + v];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) dR[c * NV + v] = s[v];
+}
+
+// ------------------------------------------------------------ wall force
+// per cell: sum over its wall faces of (sum_q w_q p_q - PRES) * area * n_x;
+// with dU != null the tangent of the same sum, with adjF != null the
+// adjoint of the face values (jbar * area * n_x * w_q * dp/du), else 0.
+__global__ void k_force_cell(Problem p, const double* __restrict__ U, const double* __restrict__ dU,
+                             const double* __restrict__ tdul, double* __restrict__ fcell, double* __restrict__ adjF,
+                             double jbar) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const int nf = p.nfaces[c];
+  const double* dul = (const double*)p.dul;
+  double sum = 0.0;
+  for (int f = 0; f < nf; ++f) {
+    const bool wall = p.neigh[c * MF + f] < 0 && p.bc[c * MF + f] == 4;
+    if (adjF)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) adjF[(c * MF + f) * NV + v] = 0.0;
+    if (!wall) continue;
+    const double nx = p.rot[(c * MF + f) * 4 + 0] * p.rot[(c * MF + f) * 4 + 3];
+    const double area = p.area[c * MF + f];
+    const double w = face_weight(p, p.ftype[c * MF + f], 0);
+    Dual<NV> u[NV], pr[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      u[v] = Dual<NV>(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
+      u[v].d[v] = 1.0;
+    }
+    cons2prim(p.gamma, u, pr);
+    if (dU) {
+      double t = 0.0;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) t += pr[4].d[v] * (dU[c * NV + v] + tdul[(c * MF + f) * NV + v]);
+      sum += w * t * area * nx;
+    } else {
+      sum += ((pr[4].v * w) - p.pres) * area * nx;
+    }
+    if (adjF)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) adjF[(c * MF + f) * NV + v] = jbar * area * nx * w * pr[4].d[v];
+  }
+  fcell[c] = sum;
+}
+
+unsigned blocks_for(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
+
+}  // namespace
+
+// ====================================================================== host
+namespace ucg_host {
+
+void adjoint_release(ucg_engine* e) {
+  ucg_engine::DevBuf* all[] = {&e->adj_face, &e->adj_contrib, &e->adj_rptr, &e->adj_rsrc, &e->adj_lam,
+                               &e->adj_mu,   &e->adj_pface,   &e->adj_tflux, &e->adj_tdul, &e->adj_tU,
+                               &e->adj_fcell, &e->adj_traj,  &e->adj_bar,  &e->adj_tmp};
+  for (auto* b : all) {
+    if (b->p) e->bytes -= (int64_t)b->bytes;
+    release(*b);
+  }
+  e->adj_ready = false;
+}
+
+}  // namespace ucg_host
+
+namespace {
+
+// reverse map and buffers (once per geometry/tables)
+int adj_setup(ucg_engine* e) {
+  int rc = adj_check(e);
+  if (rc) return rc;
+  if (e->adj_ready) return UCG_OK;
+  const int64_t n = e->n;
+  const int IM = e->cfg.imax, W = IM + 1;
+  const int slots = 1 + IM + MF;
+  if ((int64_t)e->sten1_h.size() != n * W || (int64_t)e->neigh_h.size() != n * MF)
+    return fail(e, UCG_ESTATE, "stencils and neighbours of every cell are needed");
+  // reverse map: for each target cell, the (cell, slot) pairs pointing at it,
+  // ordered by source cell then slot
+  std::vector<int64_t> cnt(n + 1, 0);
+  auto target = [&](int64_t i, int s) -> int64_t {
+    if (s == 0) return i;
+    if (s <= IM) return e->sten1_h[(size_t)i * W + s];
+    return e->neigh_h[(size_t)i * MF + (s - 1 - IM)];
+  };
+  for (int64_t i = 0; i < n; ++i)
+    for (int s = 0; s < slots; ++s) {
+      const int64_t t = target(i, s);
+      if (t >= 0 && t < n) ++cnt[t + 1];
+    }
+  for (int64_t j = 0; j < n; ++j) cnt[j + 1] += cnt[j];
+  std::vector<int64_t> src(cnt[n]), pos(cnt.begin(), cnt.end() - 1);
+  for (int64_t i = 0; i < n; ++i)
+    for (int s = 0; s < slots; ++s) {
+      const int64_t t = target(i, s);
+      if (t >= 0 && t < n) src[pos[t]++] = i * slots + s;
+    }
+  cudaSetDevice(e->device);
+  auto get = [&](ucg_engine::DevBuf& b, size_t bytes) { return alloc(e, b, bytes); };
+  rc = get(e->adj_face, (size_t)n * MF * NV * 8);
+  rc = rc ? rc : get(e->adj_contrib, (size_t)n * slots * NV * 8);
+  rc = rc ? rc : get(e->adj_rptr, (size_t)(n + 1) * 8);
+  rc = rc ? rc : get(e->adj_rsrc, (size_t)std::max<int64_t>(1, cnt[n]) * 8);
+  rc = rc ? rc : get(e->adj_lam, (size_t)n * NV * 8);
+  rc = rc ? rc : get(e->adj_mu, (size_t)n * NV * 8);
+  rc = rc ? rc : get(e->adj_pface, (size_t)n * MF * NV * 8);
+  rc = rc ? rc : get(e->adj_tflux, (size_t)n * MF * NV * 8);
+  rc = rc ? rc : get(e->adj_tdul, (size_t)n * MF * NV * 8);
+  rc = rc ? rc : get(e->adj_tU, (size_t)n * NV * 8);
+  rc = rc ? rc : get(e->adj_fcell, (size_t)n * 8);
+  rc = rc ? rc : get(e->adj_bar, (size_t)4 * n * NV * 8 + 64 * 8);
+  rc = rc ? rc : get(e->adj_tmp, (size_t)2 * n * NV * 8);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(e->adj_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
+  if (cnt[n]) CK(cudaMemcpyAsync(e->adj_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemsetAsync(e->adj_face.p, 0, (size_t)n * MF * NV * 8, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->adj_slots = slots;
+  e->adj_ready = true;
+  return UCG_OK;
+}
+
+// scratch vectors inside adj_bar: 4 state-sized vectors and a few scalars
+double* bar_vec(ucg_engine* e, int k) { return (double*)e->adj_bar.p + (size_t)k * e->n * NV; }
+double* bar_scal(ucg_engine* e) { return (double*)e->adj_bar.p + (size_t)4 * e->n * NV; }
+
+// mu = (dR/dU)^T lam, psum[0..4] = (dR/dp)^T lam, at state U (device)
+int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* lam, double* mu, double* psum) {
+  int rc = launch_recon(e, p, U);
+  if (rc) return rc;
+  const int64_t n = e->n;
+  CK(cudaMemsetAsync(e->adj_pface.p, 0, (size_t)n * MF * NV * 8, e->stream));
+  k_adj_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, lam, (double*)e->adj_face.p,
+                                                              (double*)e->adj_pface.p);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, (const double*)e->adj_face.p,
+                                                         (double*)e->adj_contrib.p, e->adj_slots);
+  k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
+                                                          (const int64_t*)e->adj_rsrc.p,
+                                                          (const double*)e->adj_contrib.p, mu);
+  k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adj_pface.p, n * MF, psum);
+  e->launches += 4;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+// dR = (dR/dU) dU + (dR/dp) dp at state U (device); leaves the primal face
+// values of U in dul and their tangents in adj_tdul
+int jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* dU, const Dp5& dp, double* dR) {
+  int rc = launch_recon(e, p, U);
+  if (rc) return rc;
+  const int64_t n = e->n;
+  k_jvp_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p);
+  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p, dp,
+                                                              (double*)e->adj_tflux.p);
+  k_jvp_sum<<<blocks_for(n, 256), 256, 0, e->stream>>>(p, (const double*)e->adj_tflux.p, dR);
+  e->launches += 3;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+// J at state U into *out (device); with dU the tangent dJ instead
+int force_device(ucg_engine* e, const Problem& p, const double* U, const double* dU, double* out) {
+  int rc = launch_recon(e, p, U);
+  if (rc) return rc;
+  if (dU) {
+    k_jvp_muscl<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p);
+    e->launches++;
+  }
+  k_force_cell<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p,
+                                                              (double*)e->adj_fcell.p, nullptr, 0.0);
+  k_sum1<<<1, 1024, 0, e->stream>>>((const double*)e->adj_fcell.p, e->n, out);
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+// dJ/dU at state U into g (device)
+int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g) {
+  int rc = launch_recon(e, p, U);
+  if (rc) return rc;
+  const int64_t n = e->n;
+  k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p,
+                                                          (double*)e->adj_face.p, 1.0);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, (const double*)e->adj_face.p,
+                                                         (double*)e->adj_contrib.p, e->adj_slots);
+  k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
+                                                          (const int64_t*)e->adj_rsrc.p,
+                                                          (const double*)e->adj_contrib.p, g);
+  e->launches += 3;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int copy_in(ucg_engine* e, double* dst, const double* src, size_t count) {
+  CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyHostToDevice, e->stream));
+  return UCG_OK;
+}
+int copy_out(ucg_engine* e, double* dst, const double* src, size_t count) {
+  CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyDeviceToHost, e->stream));
+  return UCG_OK;
+}
+
+}  // namespace
+
+// =================================================================== ABI
+extern "C" {
+
+int ucg_force(ucg_engine* e, double* fx) {
+  if (!e || !fx) return fail(e, UCG_EINVAL, "null argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  double* s = bar_scal(e);
+  if ((rc = force_device(e, p, (const double*)e->Un.p, nullptr, s))) return rc;
+  if ((rc = copy_out(e, fx, s, 1))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_force_vjp(ucg_engine* e, double* dJdU) {
+  if (!e || !dJdU) return fail(e, UCG_EINVAL, "null argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  if ((rc = force_vjp_device(e, p, (const double*)e->Un.p, (double*)e->adj_mu.p))) return rc;
+  if ((rc = copy_out(e, dJdU, (const double*)e->adj_mu.p, (size_t)e->n * NV))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_residual_vjp(ucg_engine* e, const double* lambda, double* mu, double* pbar) {
+  if (!e || !lambda || !mu) return fail(e, UCG_EINVAL, "null argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  const size_t m = (size_t)e->n * NV;
+  double* s = bar_scal(e);
+  if ((rc = copy_in(e, (double*)e->adj_lam.p, lambda, m))) return rc;
+  if ((rc = vjp_device(e, p, (const double*)e->Un.p, (const double*)e->adj_lam.p, (double*)e->adj_mu.p, s)))
+    return rc;
+  if ((rc = copy_out(e, mu, (const double*)e->adj_mu.p, m))) return rc;
+  if (pbar && (rc = copy_out(e, pbar, s, NV))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* drhs) {
+  if (!e || !du || !drhs) return fail(e, UCG_EINVAL, "null argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  const size_t m = (size_t)e->n * NV;
+  Dp5 d{};
+  if (dp)
+    for (int k = 0; k < NV; ++k) d.v[k] = dp[k];
+  if ((rc = copy_in(e, (double*)e->adj_tU.p, du, m))) return rc;
+  if ((rc = jvp_device(e, p, (const double*)e->Un.p, (const double*)e->adj_tU.p, d, (double*)e->adj_mu.p)))
+    return rc;
+  if ((rc = copy_out(e, drhs, (const double*)e->adj_mu.p, m))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, double* J, double* dJdU0,
+                    double* dJdp) {
+  if (!e || nsteps < 0 || every < 1 || !(dt > 0.0)) return fail(e, UCG_EINVAL, "bad argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  const int64_t n = e->n;
+  const size_t m = (size_t)n * NV, mb = m * 8;
+  const int nseg = (nsteps + every - 1) / every;
+  const int K = std::min<int>(every, std::max(nsteps, 1));
+  // checkpoints [nseg][n][5], stage states of one segment [K][3][n][5], final state
+  if ((rc = alloc(e, e->adj_traj, ((size_t)std::max(nseg, 1) + (size_t)3 * K + 1) * mb))) return rc;
+  double* ckpt = (double*)e->adj_traj.p;
+  double* traj = ckpt + (size_t)std::max(nseg, 1) * m;
+  double* fin = traj + (size_t)3 * K * m;
+  double* Un = (double*)e->Un.p;
+  Problem p = make_problem(e);
+  // forward with checkpoints
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % every == 0) CK(cudaMemcpyAsync(ckpt + (size_t)(s / every) * m, Un, mb, cudaMemcpyDeviceToDevice, e->stream));
+    if ((rc = rk3(e, dt, false))) return rc;
+  }
+  CK(cudaMemcpyAsync(fin, Un, mb, cudaMemcpyDeviceToDevice, e->stream));
+  double* sc = bar_scal(e);  // sc[0] J, sc[8..12] pbar accumulator, sc[16..20] partial
+  double* pacc = sc + 8;
+  double* part = sc + 16;
+  if ((rc = force_device(e, p, Un, nullptr, sc))) return rc;
+  // terminal adjoint: dJ/dU^N
+  double* ub = bar_vec(e, 0);   // adjoint of the current step's output
+  double* u0b = bar_vec(e, 1);  // adjoint of its input
+  double* u1b = bar_vec(e, 2);
+  double* u2b = bar_vec(e, 3);
+  double* mu = (double*)e->adj_mu.p;
+  double* lam = (double*)e->adj_lam.p;
+  if ((rc = force_vjp_device(e, p, Un, ub))) return rc;
+  CK(cudaMemsetAsync(pacc, 0, NV * 8, e->stream));
+  const unsigned bm = blocks_for((int64_t)m, 256), bv = blocks_for((int64_t)m, 256);
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int s0 = seg * every, s1 = std::min(nsteps, s0 + every);
+    CK(cudaMemcpyAsync(Un, ckpt + (size_t)seg * m, mb, cudaMemcpyDeviceToDevice, e->stream));
+    for (int s = s0; s < s1; ++s) {
+      double* t = traj + (size_t)3 * (s - s0) * m;
+      CK(cudaMemcpyAsync(t, Un, mb, cudaMemcpyDeviceToDevice, e->stream));
+      if ((rc = rk3(e, dt, false))) return rc;
+      CK(cudaMemcpyAsync(t + m, e->Ua.p, mb, cudaMemcpyDeviceToDevice, e->stream));
+      CK(cudaMemcpyAsync(t + 2 * m, e->Ub.p, mb, cudaMemcpyDeviceToDevice, e->stream));
+    }
+    for (int s = s1 - 1; s >= s0; --s) {
+      const double* U0 = traj + (size_t)3 * (s - s0) * m;
+      const double* U1 = U0 + m;
+      const double* U2 = U0 + 2 * m;
+      // U3 = 1/3 U0 + 2/3 U2 - 2/3 dt R(U2)/V
+      k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, ub, lam);
+      if ((rc = vjp_device(e, p, U2, lam, mu, part))) return rc;
+      k_pacc<<<1, 32, 0, e->stream>>>(-(2.0 / 3.0) * dt, part, pacc);
+      CK(cudaMemcpyAsync(u2b, ub, mb, cudaMemcpyDeviceToDevice, e->stream));
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -(2.0 / 3.0) * dt, mu, 2.0 / 3.0, u2b);
+      CK(cudaMemcpyAsync(u0b, ub, mb, cudaMemcpyDeviceToDevice, e->stream));
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.0, ub, 1.0 / 3.0, u0b);
+      // U2 = 3/4 U0 + 1/4 U1 - 1/4 dt R(U1)/V
+      k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, u2b, lam);
+      if ((rc = vjp_device(e, p, U1, lam, mu, part))) return rc;
+      k_pacc<<<1, 32, 0, e->stream>>>(-0.25 * dt, part, pacc);
+      CK(cudaMemcpyAsync(u1b, u2b, mb, cudaMemcpyDeviceToDevice, e->stream));
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -0.25 * dt, mu, 0.25, u1b);
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.75, u2b, 1.0, u0b);
+      // U1 = U0 - dt R(U0)/V
+      k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, u1b, lam);
+      if ((rc = vjp_device(e, p, U0, lam, mu, part))) return rc;
+      k_pacc<<<1, 32, 0, e->stream>>>(-dt, part, pacc);
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0, u1b, 1.0, u0b);
+      k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -dt, mu, 1.0, u0b);
+      CK(cudaMemcpyAsync(ub, u0b, mb, cudaMemcpyDeviceToDevice, e->stream));
+      e->launches += 12;
+    }
+  }
+  CK(cudaGetLastError());
+  // the handle's state is the final state
+  CK(cudaMemcpyAsync(Un, fin, mb, cudaMemcpyDeviceToDevice, e->stream));
+  if (J && (rc = copy_out(e, J, sc, 1))) return rc;
+  if (dJdU0 && (rc = copy_out(e, dJdU0, ub, m))) return rc;
+  if (dJdp && (rc = copy_out(e, dJdp, pacc, NV))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
+                    double* dJ) {
+  if (!e || nsteps < 0 || !dU0 || !(dt > 0.0)) return fail(e, UCG_EINVAL, "bad argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  const int64_t n = e->n;
+  const size_t m = (size_t)n * NV, mb = m * 8;
+  Dp5 d{};
+  if (dp)
+    for (int k = 0; k < NV; ++k) d.v[k] = dp[k];
+  Problem p = make_problem(e);
+  double* Un = (double*)e->Un.p;
+  double* t0 = bar_vec(e, 0);  // tangent of the step's input
+  double* t1 = bar_vec(e, 1);
+  double* t2 = bar_vec(e, 2);
+  double* dR = bar_vec(e, 3);
+  double* sc = bar_scal(e);
+  const unsigned bm = blocks_for((int64_t)m, 256);
+  if ((rc = copy_in(e, t0, dU0, m))) return rc;
+  for (int s = 0; s < nsteps; ++s) {
+    // stage 1 at U0 = Un
+    if ((rc = jvp_device(e, p, Un, t0, d, dR))) return rc;
+    if ((rc = launch_flux(e, p, 1, Un, Un, (double*)e->Ua.p, dt))) return rc;
+    k_over_vol<<<bm, 256, 0, e->stream>>>(p, -dt, dR, t1);
+    k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0, t0, 1.0, t1);
+    // stage 2 at U1 = Ua
+    if ((rc = jvp_device(e, p, (const double*)e->Ua.p, t1, d, dR))) return rc;
+    if ((rc = launch_flux(e, p, 2, (const double*)e->Ua.p, Un, (double*)e->Ub.p, dt))) return rc;
+    k_over_vol<<<bm, 256, 0, e->stream>>>(p, -0.25 * dt, dR, t2);
+    k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.75, t0, 1.0, t2);
+    k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.25, t1, 1.0, t2);
+    // stage 3 at U2 = Ub
+    if ((rc = jvp_device(e, p, (const double*)e->Ub.p, t2, d, dR))) return rc;
+    if ((rc = launch_flux(e, p, 3, (const double*)e->Ub.p, Un, Un, dt))) return rc;
+    k_over_vol<<<bm, 256, 0, e->stream>>>(p, -(2.0 / 3.0) * dt, dR, t1);
+    k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0 / 3.0, t0, 1.0, t1);
+    k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 2.0 / 3.0, t2, 1.0, t1);
+    CK(cudaMemcpyAsync(t0, t1, mb, cudaMemcpyDeviceToDevice, e->stream));
+    e->launches += 9;
+  }
+  if ((rc = force_device(e, p, Un, nullptr, sc))) return rc;
+  if ((rc = force_device(e, p, Un, t0, sc + 1))) return rc;
+  CK(cudaGetLastError());
+  if (J && (rc = copy_out(e, J, sc, 1))) return rc;
+  if (dJ && (rc = copy_out(e, dJ, sc + 1, 1))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+}  // extern "C"

@@ -159,8 +159,14 @@ __device__ __forceinline__ void dmonomials(double x, double y, double z, double*
 }
 
 // ------------------------------------------------------------- gas
-__device__ __forceinline__ void cons2prim(double gamma, const double* u, double* p) {
-  double oo = 1.0 / u[0];
+// The gas relations, rotations, HLLC, the limiter and the boundary states
+// are templates over the scalar type S: the engine uses S = double, the
+// discrete adjoint and tangent (adjoint.cu) forward-mode dual numbers.
+__host__ __device__ __forceinline__ double value(double x) { return x; }
+
+template <typename S>
+__host__ __device__ __forceinline__ void cons2prim(double gamma, const S* u, S* p) {
+  S oo = 1.0 / u[0];
   p[0] = u[0];
   p[1] = u[1] * oo;
   p[2] = u[2] * oo;
@@ -168,9 +174,10 @@ __device__ __forceinline__ void cons2prim(double gamma, const double* u, double*
   p[4] = (gamma - 1.0) * (u[4] - 0.5 * u[0] * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]));
 }
 
-__device__ __forceinline__ void prim2cons(double gamma, const double* p, double* u) {
-  double skin = 0.5 * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
-  double ie = p[4] / ((gamma - 1.0) * p[0]);
+template <typename S>
+__host__ __device__ __forceinline__ void prim2cons(double gamma, const S* p, S* u) {
+  S skin = 0.5 * (p[1] * p[1] + p[2] * p[2] + p[3] * p[3]);
+  S ie = p[4] / ((gamma - 1.0) * p[0]);
   u[0] = p[0];
   u[1] = p[1] * p[0];
   u[2] = p[2] * p[0];
@@ -179,14 +186,16 @@ __device__ __forceinline__ void prim2cons(double gamma, const double* p, double*
 }
 
 // ROTATEF / ROTATEB (src/grid_t.f90:4217-4305); r = cos a1, sin a1, cos a2, sin a2
-__device__ __forceinline__ void rot_f(const double* r, const double* v, double* o) {
+template <typename S>
+__host__ __device__ __forceinline__ void rot_f(const double* r, const S* v, S* o) {
   o[0] = v[0];
   o[1] = r[0] * r[3] * v[1] + r[1] * r[3] * v[2] + r[2] * v[3];
   o[2] = r[0] * r[2] * v[1] + r[1] * r[2] * v[2] - r[3] * v[3];
   o[3] = -r[1] * v[1] + r[0] * v[2];
   o[4] = v[4];
 }
-__device__ __forceinline__ void rot_b(const double* r, const double* v, double* o) {
+template <typename S>
+__host__ __device__ __forceinline__ void rot_b(const double* r, const S* v, S* o) {
   o[0] = v[0];
   o[1] = r[0] * r[3] * v[1] + r[0] * r[2] * v[2] - r[1] * v[3];
   o[2] = r[1] * r[3] * v[1] + r[1] * r[2] * v[2] + r[0] * v[3];
@@ -197,26 +206,27 @@ __device__ __forceinline__ void rot_b(const double* r, const double* v, double* 
 // HLLC in the face frame (HLLC_RIEMANN_SOLVER, src/riemann.f90:221-426):
 // Einfeldt-type wave speeds from Roe averages, SL <= 0 <= SR, and the final
 // flux is the sign(SM) blend of the two star fluxes.
-__device__ __forceinline__ void hllc(double gamma, const double* cl, const double* cr, double* flux) {
-  double rl = cl[0], ul = cl[1] / rl, vl = cl[2] / rl, wl = cl[3] / rl;
-  double pl = (gamma - 1.0) * (cl[4] - 0.5 * rl * (ul * ul + vl * vl + wl * wl));
-  double rr = cr[0], ur = cr[1] / rr, vr = cr[2] / rr, wr = cr[3] / rr;
-  double pr = (gamma - 1.0) * (cr[4] - 0.5 * rr * (ur * ur + vr * vr + wr * wr));
-  double el = cl[4], er = cr[4];
-  double ccl = sqrt(gamma * pl / rl), ccr = sqrt(gamma * pr / rr);
-  double srl = sqrt(rl), srr = sqrt(rr), ssum = srl + srr;
-  double cc2 = sqrt((ccl * ccl * srl + ccr * ccr * srr) / ssum +
-                    0.5 * ((srl * srr) / (ssum * ssum)) * ((ur - ul) * (ur - ul)));
-  double uu2 = (ul * srl + ur * srr) / ssum;
-  double sl = fmin(fmin(ul - ccl, uu2 - cc2), 0.0);
-  double sr = fmax(fmax(ur + ccr, uu2 + cc2), 0.0);
-  double sm = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
-  double mul = rl * ((sl - ul) / (sl - sm)), mur = rr * ((sr - ur) / (sr - sm));
-  double lastl = el / rl + (sm - ul) * (sm + pl / (rl * (sl - ul)));
-  double lastr = er / rr + (sm - ur) * (sm + pr / (rr * (sr - ur)));
-  double sg = copysign(1.0, sm);
+template <typename S>
+__host__ __device__ __forceinline__ void hllc(double gamma, const S* cl, const S* cr, S* flux) {
+  S rl = cl[0], ul = cl[1] / rl, vl = cl[2] / rl, wl = cl[3] / rl;
+  S pl = (gamma - 1.0) * (cl[4] - 0.5 * rl * (ul * ul + vl * vl + wl * wl));
+  S rr = cr[0], ur = cr[1] / rr, vr = cr[2] / rr, wr = cr[3] / rr;
+  S pr = (gamma - 1.0) * (cr[4] - 0.5 * rr * (ur * ur + vr * vr + wr * wr));
+  S el = cl[4], er = cr[4];
+  S ccl = sqrt(gamma * pl / rl), ccr = sqrt(gamma * pr / rr);
+  S srl = sqrt(rl), srr = sqrt(rr), ssum = srl + srr;
+  S cc2 = sqrt((ccl * ccl * srl + ccr * ccr * srr) / ssum +
+               0.5 * ((srl * srr) / (ssum * ssum)) * ((ur - ul) * (ur - ul)));
+  S uu2 = (ul * srl + ur * srr) / ssum;
+  S sl = fmin(fmin(ul - ccl, uu2 - cc2), 0.0);
+  S sr = fmax(fmax(ur + ccr, uu2 + cc2), 0.0);
+  S sm = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
+  S mul = rl * ((sl - ul) / (sl - sm)), mur = rr * ((sr - ur) / (sr - sm));
+  S lastl = el / rl + (sm - ul) * (sm + pl / (rl * (sl - ul)));
+  S lastr = er / rr + (sm - ur) * (sm + pr / (rr * (sr - ur)));
+  double sg = copysign(1.0, value(sm));
   double al = 0.5 * (1.0 + sg), ar = 0.5 * (1.0 - sg);
-  double fl0 = rl * ul, fr0 = rr * ur;
+  S fl0 = rl * ul, fr0 = rr * ur;
   flux[0] = al * (fl0 + sl * (mul - cl[0])) + ar * (fr0 + sr * (mur - cr[0]));
   flux[1] = al * (fl0 * ul + pl + sl * (mul * sm - cl[1])) + ar * (fr0 * ur + pr + sr * (mur * sm - cr[1]));
   flux[2] = al * (fl0 * vl + sl * (mul * vl - cl[2])) + ar * (fr0 * vr + sr * (mur * vr - cr[2]));
@@ -225,10 +235,11 @@ __device__ __forceinline__ void hllc(double gamma, const double* cl, const doubl
 }
 
 // Venkatakrishnan limiter, SLOPE_LIMITERS case 7 (src/reconstruct_p.f90:3647-3652)
-__device__ __forceinline__ double venkat(double d2, double umin0, double umax0, double epsi2) {
-  if (fabs(d2) <= 0.0) return 1.0;
-  double dmin = copysign(1.0, d2) * (fabs(d2) + TOLSMALL);
-  double dplus = d2 > 0.0 ? umax0 : umin0;
+template <typename S>
+__host__ __device__ __forceinline__ S venkat(S d2, S umin0, S umax0, double epsi2) {
+  if (fabs(value(d2)) <= 0.0) return S(1.0);
+  S dmin = copysign(1.0, value(d2)) * (fabs(d2) + TOLSMALL);
+  S dplus = value(d2) > 0.0 ? umax0 : umin0;
   return (1.0 / dmin) * (((dplus * dplus + epsi2) * dmin + 2.0 * (dmin * dmin) * dplus) /
                          (dplus * dplus + 2.0 * dmin * dmin + dmin * dplus + epsi2));
 }
@@ -312,12 +323,15 @@ namespace ucg {
 
 // Ghost state of a physical boundary face (BOUNDARYS, src/flow_operations.f90:2860-3230)
 // and the viscous face flux (CALCULATE_FLUXESHI_DIFFUSIVE, src/flux_p.f90:1614-1779).
-__device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const double* cl,
-                                               double* cr) {
+// `bcs` is the free-stream state (primitive) of the inflow/outflow/far-field
+// conditions, normally Problem::bc_state.
+template <typename S>
+__host__ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const S* cl, const S* bcs,
+                                               S* cr) {
   const double gm = p.gamma;
   const double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
   if (code == 3 || code == 4) {  // symmetry / inviscid wall: mirror the normal momentum
-    double a[NV], b[NV];
+    S a[NV], b[NV];
     rot_f(r, cl, a);
     b[0] = a[0];
     b[1] = -a[1];
@@ -327,13 +341,13 @@ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const
     rot_b(r, b, cr);
     return;
   }
-  double s1[NV], s2[NV], s3[NV];
+  S s1[NV], s2[NV], s3[NV];
 #pragma unroll
-  for (int k = 0; k < NV; ++k) s1[k] = p.bc_state[k];
+  for (int k = 0; k < NV; ++k) s1[k] = bcs[k];
   cons2prim(gm, cl, s2);
-  double sps = sqrt(gm * s2[4] / s2[0]);
-  double vel = sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
-  bool super = vel / (sps + TOLSMALL) > 1.0;
+  S sps = sqrt(gm * s2[4] / s2[0]);
+  S vel = sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+  bool super = value(vel / (sps + TOLSMALL)) > 1.0;
   if (code == 1) {  // inflow (BOUNDARYS case 1, subsonic characteristic treatment)
     if (super) {
       prim2cons(gm, s1, cr);
@@ -360,6 +374,11 @@ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const
     return;
   }
   prim2cons(gm, s3, cr);
+}
+
+__device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const double* cl,
+                                               double* cr) {
+  boundary_ghost<double>(p, code, r, cl, p.bc_state, cr);
 }
 
 __device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, double dih, const double* cl,

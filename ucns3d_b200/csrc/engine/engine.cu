@@ -9,8 +9,8 @@
 #include <string>
 #include <vector>
 
+#include "engine_internal.h"
 #include "kernels.cuh"
-#include "ucns3d_gpu.h"
 
 using namespace ucg;
 
@@ -18,47 +18,9 @@ namespace {
 
 std::string g_create_err;
 
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-};
-
 }  // namespace
 
-// Device layout of the per-cell table blocks (see Problem in device.cuh).
-struct Layout {
-  int64_t tstride = 0, istride = 0;
-  int soff[8] = {0};
-  int i2off = 0;
-};
-
-struct ucg_engine {
-  ucg_config cfg;
-  Layout layout;
-  int64_t n = 0;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool mixed = false;
-  int QS = 1;
-  std::string err;
-  int64_t launches = 0;
-  int64_t bytes = 0;
-  bool have_geometry = false, have_state = false;
-  int64_t recon_cells = 0;
-  std::vector<DevBuf*> owned;
-  // geometry
-  DevBuf nfaces, ftype, neigh, nface, bc, qperm, rot, area, dih, vol, minedge, jinv, admis, full, qpts, bmean;
-  // tables
-  DevBuf sten, invmat, ind;
-  // scratch and state
-  DevBuf gbuf, dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux;
-  int64_t nown = 0;
-  cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs
-  std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
-  std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
-};
-
-namespace {
+namespace ucg_host {
 
 int fail(ucg_engine* e, int code, const std::string& msg) {
   if (e) e->err = msg;
@@ -68,12 +30,6 @@ int fail(ucg_engine* e, int code, const std::string& msg) {
 int cuda_fail(ucg_engine* e, cudaError_t st, const char* where) {
   return fail(e, UCG_ECUDA, std::string(where) + ": " + cudaGetErrorString(st));
 }
-
-#define CK(call)                                               \
-  do {                                                         \
-    cudaError_t st_ = (call);                                  \
-    if (st_ != cudaSuccess) return cuda_fail(e, st_, #call);   \
-  } while (0)
 
 int alloc(ucg_engine* e, DevBuf& b, size_t bytes) {
   if (b.p && b.bytes >= bytes) return UCG_OK;
@@ -254,7 +210,9 @@ int cfl_device(ucg_engine* e, double cfl) {
   return UCG_OK;
 }
 
-}  // namespace
+}  // namespace ucg_host
+
+using namespace ucg_host;
 
 // =================================================================== ABI
 extern "C" {
@@ -372,8 +330,9 @@ void ucg_destroy(ucg_engine* e) {
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
-                   &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux};
+                   &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf};
   for (DevBuf* b : all) release(*b);
+  adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -489,6 +448,8 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   e->admis_h = std::move(admis);
+  e->neigh_h = neigh;
+  e->adj_ready = false;
   e->have_geometry = true;
   return UCG_OK;
 }
@@ -524,6 +485,12 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
                                          std::to_string(cell));
       }
     if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
+  }
+  if (c.scheme == 2 && c.iorder == 1) {  // first stencil kept on the host for the adjoint's reverse map
+    e->sten1_h.resize((size_t)n * W, -1);
+    for (int64_t i = 0; i < count; ++i)
+      for (int k = 0; k < W; ++k) e->sten1_h[(size_t)(first + i) * W + k] = r->stencil[(i * A) * W + k];
+    e->adj_ready = false;
   }
   const Layout& Ly = e->layout;
   const size_t T = tsize(e);

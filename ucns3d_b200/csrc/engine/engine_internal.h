@@ -1,0 +1,85 @@
+// Engine handle and host helpers shared by the translation units of the C
+// ABI (engine.cu: handle, uploads, stage driver; adjoint.cu: discrete
+// adjoint and tangent).  Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+#include "ucns3d_gpu.h"
+
+namespace ucg_host {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+// Device layout of the per-cell table blocks (see Problem in device.cuh).
+struct Layout {
+  int64_t tstride = 0, istride = 0;
+  int soff[8] = {0};
+  int i2off = 0;
+};
+
+}  // namespace ucg_host
+
+struct ucg_engine {
+  ucg_config cfg;
+  ucg_host::Layout layout;
+  int64_t n = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool mixed = false;
+  int QS = 1;
+  std::string err;
+  int64_t launches = 0;
+  int64_t bytes = 0;
+  bool have_geometry = false, have_state = false;
+  int64_t recon_cells = 0;
+  using DevBuf = ucg_host::DevBuf;
+  // geometry
+  DevBuf nfaces, ftype, neigh, nface, bc, qperm, rot, area, dih, vol, minedge, jinv, admis, full, qpts, bmean;
+  // tables
+  DevBuf sten, invmat, ind;
+  // scratch and state
+  DevBuf gbuf, dul, ulv, gv, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux;
+  int64_t nown = 0;
+  cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs
+  std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
+  std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
+  std::vector<int32_t> neigh_h;     // [n][6] face neighbours (host copy, adjoint set-up)
+  std::vector<int32_t> sten1_h;     // [n][IMAX+1] first stencil (host copy, MUSCL IORDER 1 only)
+  // discrete adjoint / tangent (adjoint.cu)
+  bool adj_ready = false;
+  int adj_slots = 0;                // contribution slots per cell: self, IMAX stencil cells, 6 face neighbours
+  DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
+      adj_fcell, adj_traj, adj_bar, adj_tmp;
+};
+
+namespace ucg_host {
+
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t st_ = (call);                                \
+    if (st_ != cudaSuccess) return cuda_fail(e, st_, #call); \
+  } while (0)
+
+int fail(ucg_engine* e, int code, const std::string& msg);
+int cuda_fail(ucg_engine* e, cudaError_t st, const char* where);
+int alloc(ucg_engine* e, DevBuf& b, size_t bytes);
+void release(DevBuf& b);
+ucg::Problem make_problem(ucg_engine* e);
+bool ready(ucg_engine* e);
+int launch_recon(ucg_engine* e, const ucg::Problem& p, const double* U);
+int launch_flux(ucg_engine* e, const ucg::Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
+                double dt);
+int rk3(ucg_engine* e, double dt, bool dt_dev);
+// frees the adjoint buffers (adjoint.cu)
+void adjoint_release(ucg_engine* e);
+
+}  // namespace ucg_host

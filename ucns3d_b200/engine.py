@@ -113,6 +113,54 @@ class Engine:
     def kinetic_energy(self) -> float:
         return self.reduce(N.UCG_REDUCE_KE)
 
+    # ------------------------------------------- adjoint and tangent (FP64 MUSCL, Euler)
+    def force(self) -> float:
+        """Wall pressure force in x at the current state (COMPUTEFORCE, src/io.f90:18752)."""
+        out = C.c_double()
+        self._check(self.lib.ucg_force(self._h, C.byref(out)))
+        return out.value
+
+    def force_vjp(self) -> np.ndarray:
+        """dJ/dU of the wall force at the current state, shape (n, 5)."""
+        out = np.empty((self.n, 5))
+        self._check(self.lib.ucg_force_vjp(self._h, N.ptr(out, C.c_double)))
+        return out
+
+    def residual_vjp(self, lam: np.ndarray):
+        """(dR/dU)^T lam, shape (n, 5), and (dR/dp)^T lam, shape (5,)."""
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        mu, pbar = np.empty((self.n, 5)), np.empty(5)
+        self._check(self.lib.ucg_residual_vjp(self._h, N.ptr(lam, C.c_double), N.ptr(mu, C.c_double),
+                                              N.ptr(pbar, C.c_double)))
+        return mu, pbar
+
+    def residual_jvp(self, du: np.ndarray, dp: np.ndarray | None = None) -> np.ndarray:
+        """(dR/dU) du + (dR/dp) dp, shape (n, 5)."""
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        dp = None if dp is None else np.ascontiguousarray(dp, dtype=np.float64)
+        out = np.empty((self.n, 5))
+        self._check(self.lib.ucg_residual_jvp(self._h, N.ptr(du, C.c_double), N.ptr(dp, C.c_double),
+                                              N.ptr(out, C.c_double)))
+        return out
+
+    def adjoint_run(self, nsteps: int, dt: float, every: int = 20):
+        """J after nsteps RK3 steps of fixed dt, dJ/dU0 (n, 5) and dJ/dp (5,);
+        the state becomes the final state."""
+        J, g, gp = C.c_double(), np.empty((self.n, 5)), np.empty(5)
+        self._check(self.lib.ucg_adjoint_run(self._h, nsteps, dt, every, C.byref(J), N.ptr(g, C.c_double),
+                                             N.ptr(gp, C.c_double)))
+        return J.value, g, gp
+
+    def tangent_run(self, nsteps: int, dt: float, dU0: np.ndarray, dp: np.ndarray | None = None):
+        """J and its directional derivative along (dU0, dp) after nsteps
+        RK3 steps of fixed dt; the state becomes the final state."""
+        dU0 = np.ascontiguousarray(dU0, dtype=np.float64)
+        dp = None if dp is None else np.ascontiguousarray(dp, dtype=np.float64)
+        J, dJ = C.c_double(), C.c_double()
+        self._check(self.lib.ucg_tangent_run(self._h, nsteps, dt, N.ptr(dU0, C.c_double), N.ptr(dp, C.c_double),
+                                             C.byref(J), C.byref(dJ)))
+        return J.value, dJ.value
+
     def time_kernels(self, reps: int = 5) -> dict:
         """Average device ms of the reconstruction, flux and time-step
         kernels (CUDA events on the engine stream)."""
