@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--case", default="vortex_hex_weno5")
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing (bump channel)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
     return ap.parse_args()
@@ -301,6 +302,44 @@ def main_reference(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(local, steps=200, every=20):
+    """Adjoint cost on the bump channel (240x80 quads half split into
+    triangles, 4 layers: hexahedra + prisms, MUSCL + HLLC, FP64): device
+    times of the residual, its VJP and JVP at a marched state, then a
+    checkpointed adjoint run of `steps` RK3 steps (checkpoints every
+    `every`) against the same steps of the primal alone."""
+    import torch
+    from ucns3d_b200 import cases
+    from ucns3d_b200.engine import Engine
+    c = cases.bump_muscl()
+    eng = Engine(c.mesh, c.cfg, device=local)
+    eng.set_state(c.U0)
+    eng.time_marching(50, c.cfl)
+    U = eng.get_state()
+    dt = eng.calculate_cfl(c.cfl)
+    t = eng.time_adjoint(reps=10)
+    stream = torch.cuda.ExternalStream(eng.stream_ptr, device=f"cuda:{local}")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    eng.set_state(U)
+    ev[0].record(stream)
+    for _ in range(steps):
+        eng.runge_kutta3(dt)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    eng.set_state(U)
+    ev[2].record(stream)
+    J, g, gp = eng.adjoint_run(steps, dt, every)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    primal, adj = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    eng.close()
+    return {"workload": "bump_muscl", "cells": c.mesh.ncells, "dtype": "f64", "residual_ms": t["residual"],
+            "vjp_ms": t["vjp"], "jvp_ms": t["jvp"], "vjp_over_residual": t["vjp"] / t["residual"],
+            "run_steps": steps, "checkpoint_every": every, "primal_run_ms": primal, "adjoint_run_ms": adj,
+            "adjoint_run_over_primal_run": adj / primal, "J": J,
+            "dJdp": [float(x) for x in gp]}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -369,6 +408,8 @@ def main():
                        "mixed_speedup": value / v64,
                        "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
                        "after_steps": args.warmup + args.steps}
+    if not args.no_adjoint:
+        out["adjoint"] = run_adjoint(local)
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_sample(args, steps=1)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",

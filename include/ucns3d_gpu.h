@@ -252,6 +252,10 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
                     double* dJdp);
 int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
                     double* dJ);
+/* Average device times over `reps` evaluations at the current state (CUDA
+ * events on the handle's stream), into ms[3]: ms[0] residual (reconstruction
+ * + fluxes), ms[1] residual VJP, ms[2] residual JVP.                      */
+int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms);
 
 /* Message of the last failure of ucg_create (no handle exists then). */
 const char* ucg_create_error(void);

@@ -166,5 +166,203 @@ __host__ __device__ __forceinline__ Dual<N> fmax(const Dual<N>& a, double b) {
   return b > a.v ? Dual<N>(b) : a;
 }
 
+// ---------------------------------------------------------------- HLLC adjoint
+// Reverse mode of hllc() (device.cuh) for double states in the face frame:
+// given fb = dJ/dflux, accumulates clb += (dflux/dcl)^T fb and
+// crb += (dflux/dcr)^T fb.  One forward sweep recomputes the intermediates,
+// one backward sweep applies the chain rule in reverse order; the branches
+// (wave-speed selection, clamping at zero, the side picked by the sign of
+// the contact speed) are those of the forward values.
+__host__ __device__ inline void hllc_adj(double gamma, const double* cl, const double* cr, const double* fb,
+                                         double* clb, double* crb) {
+  const double g1 = gamma - 1.0;
+  // ---- forward
+  const double rl = cl[0], ul = cl[1] / rl, vl = cl[2] / rl, wl = cl[3] / rl;
+  const double kl = ul * ul + vl * vl + wl * wl;
+  const double pl = g1 * (cl[4] - 0.5 * rl * kl);
+  const double rr = cr[0], ur = cr[1] / rr, vr = cr[2] / rr, wr = cr[3] / rr;
+  const double kr = ur * ur + vr * vr + wr * wr;
+  const double pr = g1 * (cr[4] - 0.5 * rr * kr);
+  const double el = cl[4], er = cr[4];
+  const double ccl = ::sqrt(gamma * pl / rl), ccr = ::sqrt(gamma * pr / rr);
+  const double srl = ::sqrt(rl), srr = ::sqrt(rr), ssum = srl + srr;
+  const double du = ur - ul;
+  const double T1 = ccl * ccl * srl + ccr * ccr * srr;
+  const double P = (srl * srr) / (ssum * ssum);
+  const double q = T1 / ssum + 0.5 * P * (du * du);
+  const double cc2 = ::sqrt(q);
+  const double uu2 = (ul * srl + ur * srr) / ssum;
+  // sl = min(min(ul - ccl, uu2 - cc2), 0): which term
+  const double sl1 = ul - ccl, sl2 = uu2 - cc2;
+  const double slm = sl2 < sl1 ? sl2 : sl1;
+  const int slb = 0.0 < slm ? 0 : (sl2 < sl1 ? 2 : 1);
+  const double sl = slb == 0 ? 0.0 : slm;
+  const double sr1 = ur + ccr, sr2 = uu2 + cc2;
+  const double srm = sr2 > sr1 ? sr2 : sr1;
+  const int srb = 0.0 > srm ? 0 : (sr2 > sr1 ? 2 : 1);
+  const double sr = srb == 0 ? 0.0 : srm;
+  const double num = pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur);
+  const double den = rl * (sl - ul) - rr * (sr - ur);
+  const double sm = num / den;
+  const bool left = copysign(1.0, sm) > 0.0;
+  // ---- backward: adjoints of the intermediates
+  double rlb = 0, ulb = 0, vlb = 0, wlb = 0, plb = 0, elb = 0;
+  double rrb = 0, urb = 0, vrb = 0, wrb = 0, prb = 0, erb = 0;
+  double slb_ = 0, srb_ = 0, smb = 0;
+  {
+    // active side: F = fs0 + s (mus - c) terms (s = sl or sr)
+    const double rs = left ? rl : rr, us = left ? ul : ur, vs = left ? vl : vr, ws = left ? wl : wr;
+    const double ps = left ? pl : pr, es = left ? el : er, s = left ? sl : sr;
+    const double* cs = left ? cl : cr;
+    double* csb = left ? clb : crb;
+    const double Bq = rs * (s - us);            // rho (s - u)
+    const double D1 = s - sm;
+    const double mus = Bq / D1;                 // star density factor
+    const double A = sm - us, Bt = sm + ps / Bq;
+    const double lasts = es / rs + A * Bt;
+    const double fs0 = rs * us;
+    double rsb = 0, usb = 0, vsb = 0, wsb = 0, psb = 0, esb = 0, sb = 0;
+    // F0 = fs0 + s (mus - c0); F1 = fs0 us + ps + s (mus sm - c1);
+    // F2 = fs0 vs + s (mus vs - c2); F3 = fs0 ws + s (mus ws - c3);
+    // F4 = us (es + ps) + s (mus lasts - c4)
+    const double fs0b = fb[0] + fb[1] * us + fb[2] * vs + fb[3] * ws;
+    sb += fb[0] * (mus - cs[0]) + fb[1] * (mus * sm - cs[1]) + fb[2] * (mus * vs - cs[2]) +
+          fb[3] * (mus * ws - cs[3]) + fb[4] * (mus * lasts - cs[4]);
+    const double musb = s * (fb[0] + fb[1] * sm + fb[2] * vs + fb[3] * ws + fb[4] * lasts);
+    csb[0] -= s * fb[0];
+    csb[1] -= s * fb[1];
+    csb[2] -= s * fb[2];
+    csb[3] -= s * fb[3];
+    csb[4] -= s * fb[4];
+    usb += fb[1] * fs0 + fb[4] * (es + ps);
+    vsb += fb[2] * (fs0 + s * mus);
+    wsb += fb[3] * (fs0 + s * mus);
+    psb += fb[1] + fb[4] * us;
+    esb += fb[4] * us;
+    smb += fb[1] * s * mus;
+    const double lastb = fb[4] * s * mus;
+    // fs0 = rs us
+    rsb += fs0b * us;
+    usb += fs0b * rs;
+    // lasts = es/rs + A Bt, A = sm - us, Bt = sm + ps/Bq
+    esb += lastb / rs;
+    rsb -= lastb * es / (rs * rs);
+    const double Ab = lastb * Bt, Btb = lastb * A;
+    smb += Ab;
+    usb -= Ab;
+    smb += Btb;
+    psb += Btb / Bq;
+    double Bqb = -Btb * ps / (Bq * Bq);
+    // mus = Bq / D1, D1 = s - sm
+    Bqb += musb / D1;
+    const double D1b = -musb * Bq / (D1 * D1);
+    sb += D1b;
+    smb -= D1b;
+    // Bq = rs (s - us)
+    rsb += Bqb * (s - us);
+    sb += Bqb * rs;
+    usb -= Bqb * rs;
+    if (left) {
+      rlb += rsb; ulb += usb; vlb += vsb; wlb += wsb; plb += psb; elb += esb; slb_ += sb;
+    } else {
+      rrb += rsb; urb += usb; vrb += vsb; wrb += wsb; prb += psb; erb += esb; srb_ += sb;
+    }
+  }
+  // sm = num / den
+  const double numb = smb / den, denb = -smb * num / (den * den);
+  prb += numb;
+  plb -= numb;
+  rlb += numb * ul * (sl - ul);
+  ulb += numb * rl * (sl - 2.0 * ul);
+  slb_ += numb * rl * ul;
+  rrb -= numb * ur * (sr - ur);
+  urb -= numb * rr * (sr - 2.0 * ur);
+  srb_ -= numb * rr * ur;
+  rlb += denb * (sl - ul);
+  slb_ += denb * rl;
+  ulb -= denb * rl;
+  rrb -= denb * (sr - ur);
+  srb_ -= denb * rr;
+  urb += denb * rr;
+  // wave speeds
+  double cclb = 0, ccrb = 0, uu2b = 0, cc2b = 0;
+  if (slb == 1) {
+    ulb += slb_;
+    cclb -= slb_;
+  } else if (slb == 2) {
+    uu2b += slb_;
+    cc2b -= slb_;
+  }
+  if (srb == 1) {
+    urb += srb_;
+    ccrb += srb_;
+  } else if (srb == 2) {
+    uu2b += srb_;
+    cc2b += srb_;
+  }
+  // uu2 = (ul srl + ur srr) / ssum
+  double srlb = 0, srrb = 0, ssumb = 0;
+  const double Xb = uu2b / ssum;
+  ssumb -= uu2b * uu2 / ssum;
+  ulb += Xb * srl;
+  srlb += Xb * ul;
+  urb += Xb * srr;
+  srrb += Xb * ur;
+  // cc2 = sqrt(q), q = T1/ssum + 0.5 P du^2
+  const double qb = cc2b / (2.0 * cc2);
+  const double T1b = qb / ssum;
+  ssumb -= qb * T1 / (ssum * ssum);
+  const double Pb = qb * 0.5 * du * du;
+  const double dub = qb * P * du;
+  srlb += Pb * srr / (ssum * ssum);
+  srrb += Pb * srl / (ssum * ssum);
+  ssumb -= Pb * 2.0 * srl * srr / (ssum * ssum * ssum);
+  urb += dub;
+  ulb -= dub;
+  cclb += T1b * 2.0 * ccl * srl;
+  srlb += T1b * ccl * ccl;
+  ccrb += T1b * 2.0 * ccr * srr;
+  srrb += T1b * ccr * ccr;
+  srlb += ssumb;
+  srrb += ssumb;
+  rlb += srlb / (2.0 * srl);
+  rrb += srrb / (2.0 * srr);
+  // ccl = sqrt(gamma pl / rl)
+  {
+    const double zb = cclb / (2.0 * ccl);
+    plb += zb * gamma / rl;
+    rlb -= zb * gamma * pl / (rl * rl);
+    const double zr = ccrb / (2.0 * ccr);
+    prb += zr * gamma / rr;
+    rrb -= zr * gamma * pr / (rr * rr);
+  }
+  // pl = g1 (el - 0.5 rl kl), el = cl[4]
+  elb += plb * g1;
+  rlb -= plb * g1 * 0.5 * kl;
+  const double klb = -plb * g1 * 0.5 * rl;
+  ulb += klb * 2.0 * ul;
+  vlb += klb * 2.0 * vl;
+  wlb += klb * 2.0 * wl;
+  erb += prb * g1;
+  rrb -= prb * g1 * 0.5 * kr;
+  const double krb = -prb * g1 * 0.5 * rr;
+  urb += krb * 2.0 * ur;
+  vrb += krb * 2.0 * vr;
+  wrb += krb * 2.0 * wr;
+  // ul = cl1 / rl, ...; rl = cl0, el = cl4
+  clb[1] += ulb / rl;
+  clb[2] += vlb / rl;
+  clb[3] += wlb / rl;
+  rlb -= (ulb * ul + vlb * vl + wlb * wl) / rl;
+  clb[0] += rlb;
+  clb[4] += elb;
+  crb[1] += urb / rr;
+  crb[2] += vrb / rr;
+  crb[3] += wrb / rr;
+  rrb -= (urb * ur + vrb * vr + wrb * wr) / rr;
+  crb[0] += rrb;
+  crb[4] += erb;
+}
+
 }  // namespace ad
 }  // namespace ucg

@@ -93,10 +93,15 @@ __global__ void __launch_bounds__(1024) k_sum1(const double* __restrict__ a, int
 
 // ------------------------------------------------------------ face VJP
 // adjF[c][f] = adjoint of the face value of cell c at face f;
-// pface[c][f] = adjoint of the free-stream state from boundary face (c, f).
+// pown[i] = adjoint of the free-stream state from owned face i (0 unless an
+// inflow/outflow/far-field face).  Interior and mirror faces take the
+// hand-written reverse sweep of HLLC (ad::hllc_adj); the other boundary
+// faces, whose ghost state depends on the free stream, form the 5x10
+// Jacobian one input direction at a time (Dual<1>).
 __global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __restrict__ U,
                                                   const double* __restrict__ lam, double* __restrict__ adjF,
-                                                  double* __restrict__ pface) {
+                                                  double* __restrict__ pown) {
+  using D = Dual<1>;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   const int32_t code = p.own[i];
@@ -104,57 +109,112 @@ __global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __res
   const int f = code & 7;
   const int64_t nb = p.neigh[c * MF + f];
   const int nf = p.nface[c * MF + f];
+  const int bcode = p.bc[c * MF + f];
   double r[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
   const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
   const double* dul = (const double*)p.dul;
-  Dual<10> L[NV], R[NV];
+  double ul[NV], ur[NV], g[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    L[v] = Dual<10>(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
-    L[v].d[v] = 1.0;
-  }
-  double g[NV];
-  if (nb >= 0) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      R[v] = Dual<10>(U[nb * NV + v] + dul[(nb * MF + nf) * NV + v]);
-      R[v].d[5 + v] = 1.0;
-      g[v] = lam[c * NV + v] - lam[nb * NV + v];
+    ul[v] = U[c * NV + v] + dul[(c * MF + f) * NV + v];
+    if (nb >= 0) {
+      ur[v] = U[nb * NV + v] + dul[(nb * MF + nf) * NV + v];
+      g[v] = ws * (lam[c * NV + v] - lam[nb * NV + v]);
+    } else {
+      ur[v] = p.bc_state[v];  // free-stream state, the second input of a boundary face
+      g[v] = ws * lam[c * NV + v];
     }
-  } else {
-    Dual<10> bcs[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      bcs[v] = Dual<10>(p.bc_state[v]);
-      bcs[v].d[5 + v] = 1.0;
-      g[v] = lam[c * NV + v];
-    }
-    boundary_ghost(p, (int)p.bc[c * MF + f], r, L, bcs, R);
   }
-  Dual<10> a[NV], b[NV], h[NV], fl[NV];
-  rot_f(r, R, b);
-  rot_f(r, L, a);
-  hllc(p.gamma, a, b, h);
-  rot_b(r, h, fl);
   double out[10];
+  if (nb >= 0 || bcode == 3 || bcode == 4) {
+    // interior or mirror face: reverse sweep of HLLC in the face frame.
+    // The rotations are orthogonal (rot_b = rot_f^T), and a mirror ghost is
+    // b = S a in the face frame (S flips the normal momentum).
+    double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
+    rot_f(r, ul, a);
+    if (nb >= 0) {
+      rot_f(r, ur, b);
+    } else {
 #pragma unroll
+      for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
+    }
+    rot_f(r, g, hb);
+    ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
+    if (nb < 0)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
+    rot_b(r, ab, o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = o[v];
+    rot_b(r, bb, o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[5 + v] = nb >= 0 ? o[v] : 0.0;
+  } else {
+#pragma unroll 1
   for (int k = 0; k < 10; ++k) {
+    D L[NV], R[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      L[v] = D(ul[v]);
+      L[v].d[0] = v == k ? 1.0 : 0.0;
+    }
+    if (nb >= 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        R[v] = D(ur[v]);
+        R[v].d[0] = v + 5 == k ? 1.0 : 0.0;
+      }
+    } else {
+      D bcs[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        bcs[v] = D(ur[v]);
+        bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
+      }
+      boundary_ghost(p, bcode, r, L, bcs, R);
+    }
+    D a[NV], b[NV], h[NV], fl[NV];
+    rot_f(r, R, b);
+    rot_f(r, L, a);
+    hllc(p.gamma, a, b, h);
+    rot_b(r, h, fl);
     double s = 0.0;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[k];
-    out[k] = ws * s;
+    for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
+    out[k] = s;
+  }
   }
 #pragma unroll
   for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = out[k];
-  if (nb >= 0) {
+  if (nb >= 0)
 #pragma unroll
     for (int k = 0; k < NV; ++k) adjF[(nb * MF + nf) * NV + k] = out[5 + k];
-  } else {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) pface[(c * MF + f) * NV + k] = out[5 + k];
+  for (int k = 0; k < NV; ++k) pown[i * NV + k] = nb >= 0 ? 0.0 : out[5 + k];
+}
+
+// deterministic column sums of a [m][5] array in two passes: k_colsum5_part
+// sums fixed row ranges per block, k_colsum5 then sums the block partials
+__global__ void __launch_bounds__(256) k_colsum5_part(const double* __restrict__ a, int64_t m, int64_t rows,
+                                                      double* __restrict__ part) {
+  const int64_t r0 = (int64_t)blockIdx.x * rows, r1 = r0 + rows < m ? r0 + rows : m;
+  __shared__ double sh[NV][256];
+  double s[NV] = {0, 0, 0, 0, 0};
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s[k] += a[r * NV + k];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) sh[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
   }
+  if (threadIdx.x < NV) part[blockIdx.x * NV + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // ------------------------------------------------------------ MUSCL reverse
@@ -266,17 +326,35 @@ __device__ void muscl_forward(const Problem& p, const double* __restrict__ U, in
   }
 }
 
+// The reconstruction of every cell with its intermediates kept for the
+// reverse sweep: face values (minus the mean) to dul exactly as k_muscl
+// writes them, the MusclFwd record to fwd[c].
+__global__ void __launch_bounds__(128) k_adj_fwd(Problem p, const double* __restrict__ U,
+                                                 MusclFwd* __restrict__ fwd) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  MusclFwd m;
+  muscl_forward(p, U, c, m);
+  double* out = (double*)p.dul + c * (int64_t)MF * NV;
+  for (int f = 0; f < p.nfaces[c]; ++f) {
+    double b[3];
+    muscl_basis(p, c, f, b);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[f * NV + v] = m.first ? 0.0 : muscl_dd(m, b, v) * m.slope[v];
+  }
+  fwd[c] = m;
+}
+
 // contrib[c][slot][v]: slot 0 the cell, 1..IMAX its stencil cells, 1+IMAX+f
 // its face neighbour f.  Face values u_f = u0 + dd_f * slope (or u0 when
 // CHECKSOLX chose first order).
-__global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const double* __restrict__ U,
+__global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const MusclFwd* __restrict__ fwd,
                                                    const double* __restrict__ adjF, double* __restrict__ contrib,
                                                    int slots) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
   const int IM = p.imax, nf = p.nfaces[c];
-  MusclFwd m;
-  muscl_forward(p, U, c, m);
+  const MusclFwd m = fwd[c];
   double* out = contrib + c * (int64_t)slots * NV;
   for (int s = 0; s < slots * NV; ++s) out[s] = 0.0;
   double self[NV] = {0, 0, 0, 0, 0};
@@ -568,7 +646,7 @@ namespace ucg_host {
 void adjoint_release(ucg_engine* e) {
   ucg_engine::DevBuf* all[] = {&e->adj_face, &e->adj_contrib, &e->adj_rptr, &e->adj_rsrc, &e->adj_lam,
                                &e->adj_mu,   &e->adj_pface,   &e->adj_tflux, &e->adj_tdul, &e->adj_tU,
-                               &e->adj_fcell, &e->adj_traj,  &e->adj_bar,  &e->adj_tmp};
+                               &e->adj_fcell, &e->adj_traj,  &e->adj_bar,  &e->adj_tmp, &e->adj_fwd};
   for (auto* b : all) {
     if (b->p) e->bytes -= (int64_t)b->bytes;
     release(*b);
@@ -625,6 +703,7 @@ int adj_setup(ucg_engine* e) {
   rc = rc ? rc : get(e->adj_fcell, (size_t)n * 8);
   rc = rc ? rc : get(e->adj_bar, (size_t)4 * n * NV * 8 + 64 * 8);
   rc = rc ? rc : get(e->adj_tmp, (size_t)2 * n * NV * 8);
+  rc = rc ? rc : get(e->adj_fwd, (size_t)n * sizeof(MusclFwd));
   if (rc) return rc;
   CK(cudaMemcpyAsync(e->adj_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
   if (cnt[n]) CK(cudaMemcpyAsync(e->adj_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
@@ -640,20 +719,31 @@ double* bar_vec(ucg_engine* e, int k) { return (double*)e->adj_bar.p + (size_t)k
 double* bar_scal(ucg_engine* e) { return (double*)e->adj_bar.p + (size_t)4 * e->n * NV; }
 
 // mu = (dR/dU)^T lam, psum[0..4] = (dR/dp)^T lam, at state U (device)
+// the reconstruction of U with its intermediates (face values to dul)
+int adj_forward(ucg_engine* e, const Problem& p, const double* U) {
+  k_adj_fwd<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, (MusclFwd*)e->adj_fwd.p);
+  e->launches++;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
 int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* lam, double* mu, double* psum) {
-  int rc = launch_recon(e, p, U);
+  int rc = adj_forward(e, p, U);
   if (rc) return rc;
   const int64_t n = e->n;
-  CK(cudaMemsetAsync(e->adj_pface.p, 0, (size_t)n * MF * NV * 8, e->stream));
   k_adj_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, lam, (double*)e->adj_face.p,
                                                               (double*)e->adj_pface.p);
-  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, (const double*)e->adj_face.p,
-                                                         (double*)e->adj_contrib.p, e->adj_slots);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, (const MusclFwd*)e->adj_fwd.p,
+                                                         (const double*)e->adj_face.p, (double*)e->adj_contrib.p,
+                                                         e->adj_slots);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, mu);
-  k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adj_pface.p, n * MF, psum);
-  e->launches += 4;
+  const int64_t rows = 4096, nb = (e->nown + rows - 1) / rows;
+  k_colsum5_part<<<(unsigned)nb, 256, 0, e->stream>>>((const double*)e->adj_pface.p, e->nown, rows,
+                                                       (double*)e->adj_tmp.p);
+  k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adj_tmp.p, nb, psum);
+  e->launches += 5;
   CK(cudaGetLastError());
   return UCG_OK;
 }
@@ -691,13 +781,14 @@ int force_device(ucg_engine* e, const Problem& p, const double* U, const double*
 
 // dJ/dU at state U into g (device)
 int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g) {
-  int rc = launch_recon(e, p, U);
+  int rc = adj_forward(e, p, U);
   if (rc) return rc;
   const int64_t n = e->n;
   k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p,
                                                           (double*)e->adj_face.p, 1.0);
-  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, (const double*)e->adj_face.p,
-                                                         (double*)e->adj_contrib.p, e->adj_slots);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, (const MusclFwd*)e->adj_fwd.p,
+                                                         (const double*)e->adj_face.p, (double*)e->adj_contrib.p,
+                                                         e->adj_slots);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, g);
@@ -777,6 +868,44 @@ int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* 
     return rc;
   if ((rc = copy_out(e, drhs, (const double*)e->adj_mu.p, m))) return rc;
   CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms) {
+  if (!e || !ms || reps < 1) return fail(e, UCG_EINVAL, "bad argument");
+  int rc = adj_setup(e);
+  if (rc) return rc;
+  cudaSetDevice(e->device);
+  Problem p = make_problem(e);
+  const int64_t n = e->n;
+  const double* U = (const double*)e->Un.p;
+  double* x = bar_vec(e, 0);
+  double* y = bar_vec(e, 1);
+  CK(cudaMemsetAsync(x, 0, (size_t)n * NV * 8, e->stream));
+  cudaEvent_t ev[4];
+  for (auto& t : ev) CK(cudaEventCreate(&t));
+  double acc[3] = {0, 0, 0};
+  Dp5 d{};
+  for (int r = 0; r < reps && !rc; ++r) {
+    cudaEventRecord(ev[0], e->stream);
+    rc = launch_recon(e, p, U);
+    if (!rc) rc = launch_flux(e, p, 0, U, U, nullptr, 0.0);
+    cudaEventRecord(ev[1], e->stream);
+    if (!rc) rc = vjp_device(e, p, U, x, y, bar_scal(e));
+    cudaEventRecord(ev[2], e->stream);
+    if (!rc) rc = jvp_device(e, p, U, x, d, y);
+    cudaEventRecord(ev[3], e->stream);
+    cudaEventSynchronize(ev[3]);
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (auto& t : ev) cudaEventDestroy(t);
+  if (rc) return rc;
+  for (int k = 0; k < 3; ++k) ms[k] = acc[k] / reps;
+  CK(cudaGetLastError());
   return UCG_OK;
 }
 

@@ -400,13 +400,25 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
     }
   }
   if (n >= (int64_t(1) << 28)) return fail(e, UCG_EINVAL, "too many cells (face codes are 32-bit)");
-  std::vector<int32_t> own;
+  // owned faces, grouped: interior faces, then mirror boundaries (symmetry,
+  // slip wall), then the other boundaries (each group in cell order), so
+  // that kernels branching on the face kind see uniform warps
+  std::vector<int32_t> own, own_mir, own_bnd;
   own.reserve(n * 3);
   for (int64_t c = 0; c < n; ++c)
     for (int f = 0; f < nfaces[c]; ++f) {
       int64_t nb = neigh[c * MF + f];
-      if (nb < 0 || c < nb || (c == nb && f < nface[c * MF + f])) own.push_back((int32_t)(c * 8 + f));
+      const int32_t code = (int32_t)(c * 8 + f);
+      if (nb >= 0) {
+        if (c < nb || (c == nb && f < nface[c * MF + f])) own.push_back(code);
+      } else if (bc[c * MF + f] == 3 || bc[c * MF + f] == 4) {
+        own_mir.push_back(code);
+      } else {
+        own_bnd.push_back(code);
+      }
     }
+  own.insert(own.end(), own_mir.begin(), own_mir.end());
+  own.insert(own.end(), own_bnd.begin(), own_bnd.end());
   int rc = UCG_OK;
   rc = rc ? rc : upload(e, e->own, own);
   e->nown = (int64_t)own.size();

@@ -58,7 +58,7 @@ struct ucg_engine {
   bool adj_ready = false;
   int adj_slots = 0;                // contribution slots per cell: self, IMAX stencil cells, 6 face neighbours
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
-      adj_fcell, adj_traj, adj_bar, adj_tmp;
+      adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd;
 };
 
 namespace ucg_host {

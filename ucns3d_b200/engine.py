@@ -161,6 +161,12 @@ class Engine:
                                              C.byref(J), C.byref(dJ)))
         return J.value, dJ.value
 
+    def time_adjoint(self, reps: int = 5) -> dict:
+        """Average device ms of the residual, its VJP and its JVP."""
+        ms = (C.c_double * 3)()
+        self._check(self.lib.ucg_time_adjoint(self._h, reps, ms))
+        return dict(residual=ms[0], vjp=ms[1], jvp=ms[2])
+
     def time_kernels(self, reps: int = 5) -> dict:
         """Average device ms of the reconstruction, flux and time-step
         kernels (CUDA events on the engine stream)."""
