@@ -229,6 +229,68 @@ struct MusclFwd {
   int fstar[NV];           // face of the limiting value, -1 if none
   double epsi2;
   bool first;              // CHECKSOLX: first order
+  int fmask;               // bit f: face neighbour f has a slot of its own (not in the stencil)
+};
+
+// The records of all cells, field-major so that a warp's loads and stores of
+// one field are contiguous: double field j of cell c at d[j * n + c], byte
+// field j at b[j * n + c].
+constexpr int FWD_D = 4 * NV + 3 * NV + 1;  // u0, g, lo, hi, slope, epsi2
+constexpr int FWD_B = 3 * NV + 2;           // amin, amax, fstar, first, fmask
+struct FwdStore {
+  double* d;
+  int8_t* b;
+  int64_t n;
+  __device__ void put(int64_t c, const MusclFwd& m) const {
+    int j = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) d[(j++) * n + c] = m.u0[v];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) d[(j++) * n + c] = m.g[k][v];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      d[(j++) * n + c] = m.lo[v];
+      d[(j++) * n + c] = m.hi[v];
+      d[(j++) * n + c] = m.slope[v];
+    }
+    d[j * n + c] = m.epsi2;
+    j = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      b[(j++) * n + c] = (int8_t)m.amin[v];
+      b[(j++) * n + c] = (int8_t)m.amax[v];
+      b[(j++) * n + c] = (int8_t)m.fstar[v];
+    }
+    b[(j++) * n + c] = (int8_t)m.first;
+    b[j * n + c] = (int8_t)m.fmask;
+  }
+  __device__ void get(int64_t c, MusclFwd& m) const {
+    int j = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) m.u0[v] = d[(j++) * n + c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) m.g[k][v] = d[(j++) * n + c];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      m.lo[v] = d[(j++) * n + c];
+      m.hi[v] = d[(j++) * n + c];
+      m.slope[v] = d[(j++) * n + c];
+    }
+    m.epsi2 = d[j * n + c];
+    j = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      m.amin[v] = b[(j++) * n + c];
+      m.amax[v] = b[(j++) * n + c];
+      m.fstar[v] = b[(j++) * n + c];
+    }
+    m.first = b[(j++) * n + c] != 0;
+    m.fmask = b[j * n + c];
+  }
 };
 
 __device__ __forceinline__ void muscl_basis(const Problem& p, int64_t c, int f, double* b) {
@@ -329,41 +391,73 @@ __device__ void muscl_forward(const Problem& p, const double* __restrict__ U, in
 // The reconstruction of every cell with its intermediates kept for the
 // reverse sweep: face values (minus the mean) to dul exactly as k_muscl
 // writes them, the MusclFwd record to fwd[c].
-__global__ void __launch_bounds__(128) k_adj_fwd(Problem p, const double* __restrict__ U,
-                                                 MusclFwd* __restrict__ fwd) {
+// A face neighbour that is also a cell of the stencil shares the stencil
+// cell's slot: the bound slots amin/amax are remapped to it, and fmask keeps
+// the faces whose neighbour has a slot of its own (the reverse map in
+// adj_setup makes the same choice).
+__global__ void __launch_bounds__(128) k_adj_fwd(Problem p, const double* __restrict__ U, FwdStore fwd) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
   MusclFwd m;
   muscl_forward(p, U, c, m);
+  const int IM = p.imax, nf = p.nfaces[c];
   double* out = (double*)p.dul + c * (int64_t)MF * NV;
-  for (int f = 0; f < p.nfaces[c]; ++f) {
+  for (int f = 0; f < nf; ++f) {
     double b[3];
     muscl_basis(p, c, f, b);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[f * NV + v] = m.first ? 0.0 : muscl_dd(m, b, v) * m.slope[v];
   }
-  fwd[c] = m;
+  const int32_t* st = p.sten + (c >> 5) * (int64_t)p.admis_max * (IM + 1) * 32 + (c & 31);
+  int slot_of[MF];
+  m.fmask = 0;
+  for (int f = 0; f < MF; ++f) {
+    const int64_t nb = f < nf ? p.neigh[c * MF + f] : -1;
+    slot_of[f] = 1 + IM + f;
+    if (nb < 0) continue;
+    for (int k = 0; k < IM; ++k)
+      if (st[(k + 1) * 32] == nb) {
+        slot_of[f] = 1 + k;
+        break;
+      }
+    if (slot_of[f] == 1 + IM + f) m.fmask |= 1 << f;
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    if (m.amin[v] > IM) m.amin[v] = slot_of[m.amin[v] - 1 - IM];
+    if (m.amax[v] > IM) m.amax[v] = slot_of[m.amax[v] - 1 - IM];
+  }
+  fwd.put(c, m);
 }
 
-// contrib[c][slot][v]: slot 0 the cell, 1..IMAX its stencil cells, 1+IMAX+f
-// its face neighbour f.  Face values u_f = u0 + dd_f * slope (or u0 when
+// Contributions to mu, slot-major: contrib[(slot * n + c) * NV + v], slot 0
+// the cell, 1..IMAX its stencil cells, 1 + IMAX + f its face neighbour f
+// (only the faces of fmask).  Each slot that the reverse map reads is
+// written exactly once.  Face values u_f = u0 + dd_f * slope (or u0 when
 // CHECKSOLX chose first order).
-__global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const MusclFwd* __restrict__ fwd,
-                                                   const double* __restrict__ adjF, double* __restrict__ contrib,
-                                                   int slots) {
+__global__ void __launch_bounds__(128) k_adj_muscl(Problem p, FwdStore fwd, const double* __restrict__ adjF,
+                                                   double* __restrict__ contrib) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.n) return;
+  const int64_t n = p.n;
+  if (c >= n) return;
   const int IM = p.imax, nf = p.nfaces[c];
-  const MusclFwd m = fwd[c];
-  double* out = contrib + c * (int64_t)slots * NV;
-  for (int s = 0; s < slots * NV; ++s) out[s] = 0.0;
+  MusclFwd m;
+  fwd.get(c, m);
   double self[NV] = {0, 0, 0, 0, 0};
+  for (int f = 0; f < nf; ++f)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) self[v] += adjF[(c * MF + f) * NV + v];
+  auto put = [&](int slot, int v, double x) { contrib[((int64_t)slot * n + c) * NV + v] = x; };
   if (m.first) {
-    for (int f = 0; f < nf; ++f)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) self[v] += adjF[(c * MF + f) * NV + v];
+    for (int v = 0; v < NV; ++v) put(0, v, self[v]);
+    for (int k = 0; k < IM; ++k)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) out[v] = self[v];
+      for (int v = 0; v < NV; ++v) put(1 + k, v, 0.0);
+    for (int f = 0; f < MF; ++f)
+      if (m.fmask >> f & 1)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) put(1 + IM + f, v, 0.0);
     return;
   }
   // reverse of u_f = u0 + dd_f * slope, slope = psi_{f*}, dd_f = b_f . g
@@ -376,7 +470,6 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const MusclFwd* __
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const double ub = adjF[(c * MF + f) * NV + v];
-      self[v] += ub;
       sbar[v] += ub * muscl_dd(m, b, v);
       const double ddb = ub * m.slope[v];
 #pragma unroll
@@ -400,8 +493,11 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const MusclFwd* __
     lob[v] += sbar[v] * ps.d[1];
     hib[v] += sbar[v] * ps.d[2];
   }
+  // lo = min(...) - u0, hi = max(...) - u0: the bound cells get lob/hib
+  auto bounds = [&](int slot, int v) {
+    return (m.amin[v] == slot ? lob[v] : 0.0) + (m.amax[v] == slot ? hib[v] : 0.0);
+  };
   // g = sum_k M_k (u_k - u0)
-  const int W = IM + 1;
   const int64_t grp = c >> 5;
   const int lane = (int)(c & 31);
   const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
@@ -410,20 +506,16 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, const MusclFwd* __
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const double ck = m0 * gbar[0][v] + m1 * gbar[1][v] + m2 * gbar[2][v];
-      out[(1 + k) * NV + v] += ck;
+      put(1 + k, v, ck + bounds(1 + k, v));
       self[v] -= ck;
     }
   }
-  (void)W;
-  // lo = min(...) - u0, hi = max(...) - u0
+  for (int f = 0; f < MF; ++f)
+    if (m.fmask >> f & 1)
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    self[v] -= lob[v] + hib[v];
-    out[m.amin[v] * NV + v] += lob[v];
-    out[m.amax[v] * NV + v] += hib[v];
-  }
+      for (int v = 0; v < NV; ++v) put(1 + IM + f, v, bounds(1 + IM + f, v));
 #pragma unroll
-  for (int v = 0; v < NV; ++v) out[v] += self[v];
+  for (int v = 0; v < NV; ++v) put(0, v, self[v] - (lob[v] + hib[v]) + bounds(0, v));
 }
 
 // mu[j] = sum over the slots that point at cell j (reverse map, fixed order)
@@ -671,10 +763,15 @@ int adj_setup(ucg_engine* e) {
   // reverse map: for each target cell, the (cell, slot) pairs pointing at it,
   // ordered by source cell then slot
   std::vector<int64_t> cnt(n + 1, 0);
+  // a face neighbour that is also in the stencil shares the stencil slot
+  // (k_adj_fwd makes the same choice)
   auto target = [&](int64_t i, int s) -> int64_t {
     if (s == 0) return i;
     if (s <= IM) return e->sten1_h[(size_t)i * W + s];
-    return e->neigh_h[(size_t)i * MF + (s - 1 - IM)];
+    const int64_t nb = e->neigh_h[(size_t)i * MF + (s - 1 - IM)];
+    for (int k = 1; k <= IM; ++k)
+      if (e->sten1_h[(size_t)i * W + k] == nb) return -1;
+    return nb;
   };
   for (int64_t i = 0; i < n; ++i)
     for (int s = 0; s < slots; ++s) {
@@ -686,7 +783,7 @@ int adj_setup(ucg_engine* e) {
   for (int64_t i = 0; i < n; ++i)
     for (int s = 0; s < slots; ++s) {
       const int64_t t = target(i, s);
-      if (t >= 0 && t < n) src[pos[t]++] = i * slots + s;
+      if (t >= 0 && t < n) src[pos[t]++] = s * n + i;
     }
   cudaSetDevice(e->device);
   auto get = [&](ucg_engine::DevBuf& b, size_t bytes) { return alloc(e, b, bytes); };
@@ -703,7 +800,7 @@ int adj_setup(ucg_engine* e) {
   rc = rc ? rc : get(e->adj_fcell, (size_t)n * 8);
   rc = rc ? rc : get(e->adj_bar, (size_t)4 * n * NV * 8 + 64 * 8);
   rc = rc ? rc : get(e->adj_tmp, (size_t)2 * n * NV * 8);
-  rc = rc ? rc : get(e->adj_fwd, (size_t)n * sizeof(MusclFwd));
+  rc = rc ? rc : get(e->adj_fwd, (size_t)n * (FWD_D * 8 + FWD_B));
   if (rc) return rc;
   CK(cudaMemcpyAsync(e->adj_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
   if (cnt[n]) CK(cudaMemcpyAsync(e->adj_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
@@ -719,9 +816,14 @@ double* bar_vec(ucg_engine* e, int k) { return (double*)e->adj_bar.p + (size_t)k
 double* bar_scal(ucg_engine* e) { return (double*)e->adj_bar.p + (size_t)4 * e->n * NV; }
 
 // mu = (dR/dU)^T lam, psum[0..4] = (dR/dp)^T lam, at state U (device)
+FwdStore fwd_store(ucg_engine* e) {
+  double* d = (double*)e->adj_fwd.p;
+  return FwdStore{d, (int8_t*)(d + (size_t)FWD_D * e->n), e->n};
+}
+
 // the reconstruction of U with its intermediates (face values to dul)
 int adj_forward(ucg_engine* e, const Problem& p, const double* U) {
-  k_adj_fwd<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, (MusclFwd*)e->adj_fwd.p);
+  k_adj_fwd<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, fwd_store(e));
   e->launches++;
   CK(cudaGetLastError());
   return UCG_OK;
@@ -733,9 +835,8 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
   const int64_t n = e->n;
   k_adj_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, lam, (double*)e->adj_face.p,
                                                               (double*)e->adj_pface.p);
-  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, (const MusclFwd*)e->adj_fwd.p,
-                                                         (const double*)e->adj_face.p, (double*)e->adj_contrib.p,
-                                                         e->adj_slots);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
+                                                         (double*)e->adj_contrib.p);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, mu);
@@ -786,9 +887,8 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
   const int64_t n = e->n;
   k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p,
                                                           (double*)e->adj_face.p, 1.0);
-  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, (const MusclFwd*)e->adj_fwd.p,
-                                                         (const double*)e->adj_face.p, (double*)e->adj_contrib.p,
-                                                         e->adj_slots);
+  k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
+                                                         (double*)e->adj_contrib.p);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, g);

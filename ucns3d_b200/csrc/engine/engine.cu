@@ -461,6 +461,8 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   CK(cudaStreamSynchronize(e->stream));
   e->admis_h = std::move(admis);
   e->neigh_h = neigh;
+  for (int64_t c = 0; c < n; ++c)  // no neighbour past the cell's last face
+    for (int f = nfaces[c]; f < MF; ++f) e->neigh_h[(size_t)c * MF + f] = -1;
   e->adj_ready = false;
   e->have_geometry = true;
   return UCG_OK;
