@@ -106,6 +106,24 @@ def test_device_dt_stepping_matches_host_dt():
     np.testing.assert_array_equal(a.get_state(), b.get_state())
 
 
+@pytest.mark.parametrize("name", ["weno5_hex", "cweno4_tet", "weno3_tet"])
+@pytest.mark.parametrize("precision", [N.UCG_FP64, N.UCG_MIXED])
+def test_bulk_copy_lsq_is_bitwise_equal(name, precision, monkeypatch):
+    """The opt-in least squares through the shared-memory bulk-copy ring
+    (UCG_LSQ_BULK=1 at engine creation) forms the same products in the same
+    order as the default kernel: residuals equal bit for bit."""
+    m, cfg, U = _setup(name, precision)
+    out = []
+    for bulk in ("0", "1"):
+        monkeypatch.setenv("UCG_LSQ_BULK", bulk)
+        e = Engine(m, cfg)
+        e.set_state(U)
+        out.append(e.residual())
+        e.check_health()
+        e.close()
+    assert np.array_equal(out[0], out[1])
+
+
 def test_bitwise_deterministic():
     m, cfg, U = _setup("weno3_tet")
     out = []

@@ -9,17 +9,25 @@
 //
 // VJP of R: mu = (dR/dU)^T lambda, pbar = (dR/dp)^T lambda (p: the
 // free-stream state of the inflow/outflow conditions, Problem::bc_state).
-//   1. k_adj_face   one thread per owned face: the 5x10 Jacobian of the face
-//                   flux w.r.t. its two states (or its state and p) from
-//                   dual numbers, applied transposed to lambda_c - lambda_nb;
-//                   gives the adjoint of every face value.
-//   2. k_adj_muscl  one thread per cell: the MUSCL reconstruction (LSQ,
-//                   FIND_BOUNDS, Venkatakrishnan, CHECKSOLX) reversed by
-//                   hand; its contributions to the cell, its stencil cells
-//                   and its face neighbours go to per-slot buffers.
-//   3. k_adj_gather one thread per cell: sums the slots that point at it,
-//                   through a reverse map built on the host in a fixed
-//                   order, so results are deterministic (no atomics).
+//   0. k_adj_fwd       one thread per cell: the MUSCL reconstruction (the
+//                      face values k_muscl writes) with its intermediates
+//                      kept, field-major, for step 2.
+//   1. k_adj_face      one thread per interior or mirror face: the reverse
+//                      sweep of HLLC (ad::hllc_adj) applied to
+//                      lambda_c - lambda_nb; k_adj_face_bnd, one thread per
+//                      other boundary face: the 5x10 Jacobian w.r.t. the
+//                      face value and p from dual numbers.  Together they
+//                      give the adjoint of every face value.
+//   2. k_adj_muscl     one thread per cell: the MUSCL reconstruction (LSQ,
+//                      FIND_BOUNDS, Venkatakrishnan, CHECKSOLX) reversed by
+//                      hand; its contributions to the cell, its stencil
+//                      cells and the face neighbours outside the stencil go
+//                      to per-slot buffers, each written once.
+//   3. k_adj_gather    one thread per cell: sums the slots that point at it,
+//                      through a reverse map built on the host in a fixed
+//                      order, so results are deterministic (no atomics).
+//   4. k_colsum5_part, k_colsum5: pbar, summed over the other boundary faces
+//                      in a fixed order.
 // JVP: the same reconstruction and fluxes on Dual<1> numbers.
 #include <cuda_runtime.h>
 
@@ -92,30 +100,22 @@ __global__ void __launch_bounds__(1024) k_sum1(const double* __restrict__ a, int
 }
 
 // ------------------------------------------------------------ face VJP
-// adjF[c][f] = adjoint of the face value of cell c at face f;
-// pown[i] = adjoint of the free-stream state from owned face i (0 unless an
-// inflow/outflow/far-field face).  Interior and mirror faces take the
-// hand-written reverse sweep of HLLC (ad::hllc_adj); the other boundary
-// faces, whose ghost state depends on the free stream, form the 5x10
-// Jacobian one input direction at a time (Dual<1>).
-__global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __restrict__ U,
-                                                  const double* __restrict__ lam, double* __restrict__ adjF,
-                                                  double* __restrict__ pown) {
-  using D = Dual<1>;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.nown) return;
+// adjF[c][f] = adjoint of the face value of cell c at face f.  The owned
+// faces come grouped (interior, mirror boundaries, other boundaries), and
+// the two kinds of kernel below take disjoint ranges of that list.
+__device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* __restrict__ U,
+                                                const double* __restrict__ lam, int64_t i, int64_t& c, int& f,
+                                                int64_t& nb, int& nf, double* r, double* ul, double* ur,
+                                                double* g) {
   const int32_t code = p.own[i];
-  const int64_t c = code >> 3;
-  const int f = code & 7;
-  const int64_t nb = p.neigh[c * MF + f];
-  const int nf = p.nface[c * MF + f];
-  const int bcode = p.bc[c * MF + f];
-  double r[4];
+  c = code >> 3;
+  f = code & 7;
+  nb = p.neigh[c * MF + f];
+  nf = p.nface[c * MF + f];
 #pragma unroll
   for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
   const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
   const double* dul = (const double*)p.dul;
-  double ul[NV], ur[NV], g[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
     ul[v] = U[c * NV + v] + dul[(c * MF + f) * NV + v];
@@ -127,54 +127,70 @@ __global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __res
       g[v] = ws * lam[c * NV + v];
     }
   }
-  double out[10];
-  if (nb >= 0 || bcode == 3 || bcode == 4) {
-    // interior or mirror face: reverse sweep of HLLC in the face frame.
-    // The rotations are orthogonal (rot_b = rot_f^T), and a mirror ghost is
-    // b = S a in the face frame (S flips the normal momentum).
-    double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
-    rot_f(r, ul, a);
-    if (nb >= 0) {
-      rot_f(r, ur, b);
-    } else {
+}
+
+// Interior and mirror faces, owned faces [0, nplain): reverse sweep of HLLC
+// (ad::hllc_adj) in the face frame.  The rotations are orthogonal (rot_b =
+// rot_f^T), and a mirror ghost is b = S a in the face frame (S flips the
+// normal momentum).
+__global__ void __launch_bounds__(128) k_adj_face(Problem p, int64_t nplain, const double* __restrict__ U,
+                                                  const double* __restrict__ lam, double* __restrict__ adjF) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nplain) return;
+  int64_t c, nb;
+  int f, nf;
+  double r[4], ul[NV], ur[NV], g[NV];
+  adj_face_inputs(p, U, lam, i, c, f, nb, nf, r, ul, ur, g);
+  double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
+  rot_f(r, ul, a);
+  if (nb >= 0) {
+    rot_f(r, ur, b);
+  } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
-    }
-    rot_f(r, g, hb);
-    ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
-    if (nb < 0)
+    for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
+  }
+  rot_f(r, g, hb);
+  ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
+  if (nb < 0)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
-    rot_b(r, ab, o);
+    for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
+  rot_b(r, ab, o);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) out[v] = o[v];
+  for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = o[k];
+  if (nb >= 0) {
     rot_b(r, bb, o);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) out[5 + v] = nb >= 0 ? o[v] : 0.0;
-  } else {
+    for (int k = 0; k < NV; ++k) adjF[(nb * MF + nf) * NV + k] = o[k];
+  }
+}
+
+// The other boundary faces, owned faces [nplain, nown): their ghost state
+// depends on the free stream, so the 5x10 Jacobian of the face flux w.r.t.
+// the face value and the free-stream state is formed one input direction at
+// a time (Dual<1>).  pown[i - nplain] = adjoint of the free-stream state.
+__global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain, const double* __restrict__ U,
+                                                      const double* __restrict__ lam, double* __restrict__ adjF,
+                                                      double* __restrict__ pown) {
+  using D = Dual<1>;
+  const int64_t i = nplain + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nown) return;
+  int64_t c, nb;
+  int f, nf;
+  double r[4], ul[NV], ur[NV], g[NV];
+  adj_face_inputs(p, U, lam, i, c, f, nb, nf, r, ul, ur, g);
+  const int bcode = p.bc[c * MF + f];
+  double out[10];
 #pragma unroll 1
   for (int k = 0; k < 10; ++k) {
-    D L[NV], R[NV];
+    D L[NV], R[NV], bcs[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       L[v] = D(ul[v]);
       L[v].d[0] = v == k ? 1.0 : 0.0;
+      bcs[v] = D(ur[v]);
+      bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
     }
-    if (nb >= 0) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        R[v] = D(ur[v]);
-        R[v].d[0] = v + 5 == k ? 1.0 : 0.0;
-      }
-    } else {
-      D bcs[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        bcs[v] = D(ur[v]);
-        bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
-      }
-      boundary_ghost(p, bcode, r, L, bcs, R);
-    }
+    boundary_ghost(p, bcode, r, L, bcs, R);
     D a[NV], b[NV], h[NV], fl[NV];
     rot_f(r, R, b);
     rot_f(r, L, a);
@@ -185,14 +201,10 @@ __global__ void __launch_bounds__(128) k_adj_face(Problem p, const double* __res
     for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
     out[k] = s;
   }
-  }
 #pragma unroll
   for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = out[k];
-  if (nb >= 0)
 #pragma unroll
-    for (int k = 0; k < NV; ++k) adjF[(nb * MF + nf) * NV + k] = out[5 + k];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) pown[i * NV + k] = nb >= 0 ? 0.0 : out[5 + k];
+  for (int k = 0; k < NV; ++k) pown[(i - nplain) * NV + k] = out[5 + k];
 }
 
 // deterministic column sums of a [m][5] array in two passes: k_colsum5_part
@@ -833,18 +845,27 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
   int rc = adj_forward(e, p, U);
   if (rc) return rc;
   const int64_t n = e->n;
-  k_adj_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, lam, (double*)e->adj_face.p,
-                                                              (double*)e->adj_pface.p);
+  const int64_t nplain = e->nown_plain, nbnd = e->nown - nplain;
+  if (nplain)
+    k_adj_face<<<blocks_for(nplain, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p);
+  if (nbnd)
+    k_adj_face_bnd<<<blocks_for(nbnd, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p,
+                                                                 (double*)e->adj_pface.p);
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
                                                          (double*)e->adj_contrib.p);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, mu);
-  const int64_t rows = 4096, nb = (e->nown + rows - 1) / rows;
-  k_colsum5_part<<<(unsigned)nb, 256, 0, e->stream>>>((const double*)e->adj_pface.p, e->nown, rows,
-                                                       (double*)e->adj_tmp.p);
-  k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adj_tmp.p, nb, psum);
-  e->launches += 5;
+  e->launches += 2 + (nplain > 0) + (nbnd > 0);
+  if (nbnd) {
+    const int64_t rows = 1024, nb = (nbnd + rows - 1) / rows;
+    k_colsum5_part<<<(unsigned)nb, 256, 0, e->stream>>>((const double*)e->adj_pface.p, nbnd, rows,
+                                                         (double*)e->adj_tmp.p);
+    k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adj_tmp.p, nb, psum);
+    e->launches += 2;
+  } else {
+    CK(cudaMemsetAsync(psum, 0, NV * sizeof(double), e->stream));
+  }
   CK(cudaGetLastError());
   return UCG_OK;
 }

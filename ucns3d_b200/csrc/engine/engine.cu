@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -134,6 +135,7 @@ Problem make_problem(ucg_engine* e) {
   p.vflux = (double*)e->vflux.p;
   p.health = (unsigned*)e->health.p;
   p.dt_dev = nullptr;
+  p.lsq_bulk = e->lsq_bulk ? 1 : 0;
   return p;
 }
 
@@ -259,6 +261,10 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   e->device = device;
   e->mixed = c.precision == UCG_MIXED;
   e->QS = c.nq_quad > c.nq_tri ? c.nq_quad : c.nq_tri;
+  {
+    const char* bulk = std::getenv("UCG_LSQ_BULK");
+    e->lsq_bulk = bulk && bulk[0] == '1';
+  }
   {
     // slices and smoothness blocks padded to 16 bytes (bulk-copy granularity)
     const int64_t ts = e->mixed ? 4 : 8, pad = 16 / ts;
@@ -418,6 +424,7 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
       }
     }
   own.insert(own.end(), own_mir.begin(), own_mir.end());
+  e->nown_plain = (int64_t)own.size();
   own.insert(own.end(), own_bnd.begin(), own_bnd.end());
   int rc = UCG_OK;
   rc = rc ? rc : upload(e, e->own, own);
@@ -721,6 +728,7 @@ int ucg_check_health(ucg_engine* e) {
   CK(cudaMemcpyAsync(&h, e->health.p, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
   CK(cudaMemsetAsync(e->health.p, 0, sizeof(unsigned), e->stream));
   CK(cudaStreamSynchronize(e->stream));
+  if (h & HEALTH_TIMEOUT) return fail(e, UCG_ETIMEOUT, "a bounded device wait gave up (reconstruction table pipeline)");
   if (h & HEALTH_NONPHYS) return fail(e, UCG_ENONPHYS, "a stage produced NaN or non-positive density/pressure");
   return UCG_OK;
 }
