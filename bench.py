@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing (bump channel)")
+    ap.add_argument("--adjoint-only", action="store_true", help="only the adjoint timing (bump channel)")
+    ap.add_argument("--adjoint-steps", type=int, default=200, help="RK3 steps of the adjoint run")
+    ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint stride of the adjoint run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
     return ap.parse_args()
@@ -349,6 +352,14 @@ def main():
     import numpy as np
     from ucns3d_b200 import _native as N
 
+    if args.adjoint_only:
+        adj = run_adjoint(local, args.adjoint_steps, args.adjoint_every)
+        if rank == 0:
+            print(json.dumps({"adjoint": adj}), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     peak, peak_kind = load_peaks()
     c32 = make_case(args, N.UCG_MIXED)
     ncells = c32.mesh.ncells
@@ -409,7 +420,7 @@ def main():
                        "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
                        "after_steps": args.warmup + args.steps}
     if not args.no_adjoint:
-        out["adjoint"] = run_adjoint(local)
+        out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every)
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_sample(args, steps=1)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",
