@@ -14,6 +14,9 @@
 //   COMPUTE_GRADIENTS_INNER_MEAN_LSQ_VISCOUS         src/gradients.f90:502-706
 //   WENOWEIGHTS / CP_RECONSTRUCTION / EXTRAPOLATE_BOUND
 //                                                    src/reconstruct_p.f90:407-1250, 1556
+//   CHARACTERISTIC_RECONSTRUCTION (WENWRT = 2) + WENO_NEIGHBOUR +
+//   compute_gradcharv_smoothindicator + diag_At_B_A  src/reconstruct_p.f90:497-917, 1608-1818
+//   COMPUTE_EIGENVECTORS                             src/flow_operations.f90:3934-3995
 //   CHECKSOL                                         src/reconstruct_p.f90:3126-3242
 //   MUSCL / FIND_BOUNDS / COMPUTE_MUSCL_RECONSTRUCTION / SLOPE_LIMITERS(7)
 //                                                    src/reconstruct_p.f90:2286, 1821, 2044, 3421
@@ -161,6 +164,8 @@ bool jump_check(const Ctx& x, int64_t c, const double* u0, const double* ul, dou
 
 // reconstruction of one cell: face values ul [F][Q][5] and, for
 // Navier-Stokes, face gradients ulv [F][Q][4][3] of (T, u, v, w)
+void char_faces(const Ctx& x, int64_t c, const double* U, const double* G, double* ul);
+
 void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, double* ulv) {
   const ucg_config* cfg = x.cfg;
   const ucg_geometry* g = x.g;
@@ -188,7 +193,12 @@ void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, doub
       }
   }
   bool reduce = false;
-  if (cfg->scheme == 3) {
+  if (cfg->scheme == 3 && cfg->wenwrt == 2) {
+    // ---- CHARACTERISTIC_RECONSTRUCTION, then CHECKSOL
+    char_faces(x, c, U, G.data(), ul);
+    if (!g->full[c]) reduce = true;
+    else reduce = jump_check(x, c, u0, ul, 0.85);
+  } else if (cfg->scheme == 3) {
     // ---- CP_RECONSTRUCTION
     std::vector<double> w((size_t)A * NV);
     std::vector<double> g1((size_t)ideg * NV, 0.0);  // central polynomial (CWENO)
@@ -423,6 +433,190 @@ void boundary_state(const Ctx& x, int code, const double* ang, const double* cl,
     return;
   }
   prim2cons(gm, s3, cr);
+}
+
+// COMPUTE_EIGENVECTORS (flow_operations.f90:3934-3995): left (EL) and right
+// (ER) eigenvectors of the x-direction Euler flux Jacobian at the arithmetic
+// average of two face-frame states (density, velocity, total energy).
+void eigenvectors(double gamma, const double* rl, const double* rr, double EL[5][5], double ER[5][5]) {
+  const double gm1 = gamma - 1.0, oo2 = 0.5;
+  const double oor1 = 1.0 / rl[0], oor2 = 1.0 / rr[0];
+  const double rs = oo2 * (rl[0] + rr[0]);
+  const double us = oo2 * ((rl[1] * oor1) + (rr[1] * oor2));
+  const double vs = oo2 * ((rl[2] * oor1) + (rr[2] * oor2));
+  const double ws = oo2 * ((rl[3] * oor1) + (rr[3] * oor2));
+  const double es = oo2 * (rl[4] + rr[4]);
+  const double vvs = us * us + vs * vs + ws * ws;
+  const double vsd = oo2 * vvs;
+  const double ps = gm1 * (es - oo2 * rs * vvs);
+  const double as = std::sqrt(gamma * ps / rs);
+  const double hs = (oo2 * vvs) + ((as * as) / gm1);
+  const double R[5][5] = {{1.0, 1.0, 0.0, 0.0, 1.0},
+                          {us - as, us, 0.0, 0.0, us + as},
+                          {vs, vs, 1.0, 0.0, vs},
+                          {ws, ws, 0.0, 1.0, ws},
+                          {hs - us * as, oo2 * vvs, vs, ws, hs + us * as}};
+  const double den = 2.0 * as * hs - 2.0 * as * vsd;
+  const double us2 = us * us, vs2 = vs * vs, ws2 = ws * ws;
+  double L[5][5];
+  L[0][0] = (hs * us + as * us2 + as * vs2 - as * vsd - us * vsd + as * ws2) / den;
+  L[0][1] = (-hs - as * us + vsd) / den;
+  L[0][2] = -((as * vs) / den);
+  L[0][3] = -((as * ws) / den);
+  L[0][4] = as / den;
+  L[1][0] = (2.0 * as * hs - 2.0 * as * us2 - 2.0 * as * vs2 - 2.0 * as * ws2) / den;
+  L[1][1] = (2.0 * as * us) / den;
+  L[1][2] = (2.0 * as * vs) / den;
+  L[1][3] = (2.0 * as * ws) / den;
+  L[1][4] = (-2.0 * as) / den;
+  L[2][0] = (-2.0 * as * hs * vs + 2.0 * as * vs * vsd) / den;
+  L[2][1] = 0.0;
+  L[2][2] = 1.0;
+  L[2][3] = 0.0;
+  L[2][4] = 0.0;
+  L[3][0] = (-2.0 * as * hs * ws + 2.0 * as * vsd * ws) / den;
+  L[3][1] = 0.0;
+  L[3][2] = 0.0;
+  L[3][3] = 1.0;
+  L[3][4] = 0.0;
+  L[4][0] = (-(hs * us) + as * us2 + as * vs2 - as * vsd + us * vsd + as * ws2) / den;
+  L[4][1] = (hs - as * us - vsd) / den;
+  L[4][2] = -((as * vs) / den);
+  L[4][3] = -((as * ws) / den);
+  L[4][4] = as / den;
+  for (int i = 0; i < 5; ++i)
+    for (int j = 0; j < 5; ++j) {
+      EL[i][j] = L[i][j];
+      ER[i][j] = R[i][j];
+    }
+}
+
+// CHARACTERISTIC_RECONSTRUCTION (reconstruct_p.f90:497-758), per face L of
+// cell c: eigenvectors from the cell mean and the face neighbour's mean (or
+// the boundary ghost of the cell mean, WENO_NEIGHBOUR :761-917), both rotated
+// into the face frame; the stencil polynomials (with the mean as row 0)
+// projected on the left eigenvectors, W = gradients * EL^T (the projected
+// quantities are the global-frame conserved variables, as in the
+// reference); smoothness indicators diag(W^T S W) (diag_At_B_A); weights per
+// characteristic variable; LIMITEDDW = sum_ll W_ll * w_ll; back-projection
+// FINDW = ER * LIMITEDDW; face values FINDW(:,0) + basis . FINDW(:,1:).
+// CWENO (EES 5): the central polynomial has the lower-order stencils
+// removed, and the lower-order stencils use INDICATORC over IDEGFREE2
+// (compute_gradcharv_smoothindicator :1723-1760).
+void char_faces(const Ctx& x, int64_t c, const double* U, const double* G, double* ul) {
+  const ucg_config* cfg = x.cfg;
+  const ucg_geometry* g = x.g;
+  const ucg_recon* r = x.r;
+  const int ideg = cfg->ideg, ideg2 = cfg->ideg2;
+  const int t = tab(x, c);
+  const int admis = g->admis[c];
+  const bool cw = cfg->ees == 5;
+  const double* u0 = U + c * NV;
+  // gradients[ll][d][v], d = 0 the cell mean
+  std::vector<double> gr((size_t)admis * (ideg + 1) * NV, 0.0);
+  auto GR = [&](int ll, int d, int v) -> double& { return gr[((size_t)ll * (ideg + 1) + d) * NV + v]; };
+  std::vector<double> lam(admis, 1.0);
+  for (int ll = 0; ll < admis; ++ll)
+    for (int v = 0; v < NV; ++v) GR(ll, 0, v) = u0[v];
+  if (cw) {
+    lam[0] = 1.0 - 1.0 / cfg->lwci;
+    for (int ll = 1; ll < admis; ++ll) lam[ll] = (1.0 - lam[0]) / (admis - 1);
+    std::vector<double> g5((size_t)ideg * NV, 0.0);
+    for (int ll = 1; ll < admis; ++ll)
+      for (int d = 0; d < ideg2; ++d)
+        for (int v = 0; v < NV; ++v) {
+          g5[d * NV + v] = g5[d * NV + v] + lam[ll] * G[((size_t)ll * ideg + d) * NV + v];
+          GR(ll, d + 1, v) = G[((size_t)ll * ideg + d) * NV + v];
+        }
+    for (int d = 0; d < ideg; ++d)
+      for (int v = 0; v < NV; ++v) GR(0, d + 1, v) = (1.0 / lam[0]) * (G[(size_t)d * NV + v] - g5[d * NV + v]);
+  } else {
+    lam[0] = cfg->lwci;
+    for (int ll = 0; ll < admis; ++ll)
+      for (int d = 0; d < ideg; ++d)
+        for (int v = 0; v < NV; ++v) GR(ll, d + 1, v) = G[((size_t)ll * ideg + d) * NV + v];
+  }
+  const double* S = &r->indicator[(int64_t)t * ideg * ideg];
+  const double* S2 = cw ? &r->indicator2[(int64_t)t * ideg2 * ideg2] : nullptr;
+  std::vector<double> W((size_t)admis * (ideg + 1) * NV), b(ideg);
+  for (int f = 0; f < g->nfaces[c]; ++f) {
+    const double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+    const double ang[4] = {std::cos(a1), std::sin(a1), std::cos(a2), std::sin(a2)};
+    double ur[NV], rvl[NV], rvr[NV];
+    const int64_t nb = g->neigh[c * F + f];
+    if (nb >= 0) {
+      for (int v = 0; v < NV; ++v) ur[v] = U[nb * NV + v];
+    } else {
+      boundary_state(x, g->bc[c * F + f], ang, u0, ur);
+    }
+    rotf(ang, u0, rvl);
+    rotf(ang, ur, rvr);
+    double EL[5][5], ER[5][5];
+    eigenvectors(cfg->gamma, rvl, rvr, EL, ER);
+    // W[ll][d][k] = sum_v gradients[ll][d][v] * EL[k][v]
+    for (int ll = 0; ll < admis; ++ll) {
+      const int nd = (cw && ll > 0) ? ideg2 : ideg;
+      for (int d = 0; d <= nd; ++d)
+        for (int k = 0; k < NV; ++k) {
+          double s = 0.0;
+          for (int v = 0; v < NV; ++v) s += GR(ll, d, v) * EL[k][v];
+          W[((size_t)ll * (ideg + 1) + d) * NV + k] = s;
+        }
+    }
+    auto Wv = [&](int ll, int d, int k) { return W[((size_t)ll * (ideg + 1) + d) * NV + k]; };
+    // smoothness indicators and weights per characteristic variable
+    std::vector<double> w((size_t)admis * NV);
+    for (int k = 0; k < NV; ++k) {
+      std::vector<double> is(admis), wt(admis);
+      for (int ll = 0; ll < admis; ++ll) {
+        const bool low = cw && ll > 0;
+        const int nd = low ? ideg2 : ideg;
+        const double* B = low ? S2 : S;
+        double acc = 0.0;
+        for (int i = 0; i < nd; ++i) {
+          double ba = 0.0;
+          for (int j = 0; j < nd; ++j) ba += B[i * nd + j] * Wv(ll, j + 1, k);
+          acc += Wv(ll, i + 1, k) * ba;
+        }
+        is[ll] = acc;
+      }
+      const double eps = cfg->weno_eps;
+      if (cw && cfg->wenoz) {
+        double tau = 0.0;
+        for (int ll = 0; ll < admis; ++ll) tau = tau + std::fabs(is[0] - is[ll]);
+        tau = tau / (admis - 1);
+        for (int ll = 0; ll < admis; ++ll) wt[ll] = lam[ll] * (1.0 + std::pow(tau / (eps + is[ll]), 4));
+      } else {
+        for (int ll = 0; ll < admis; ++ll) wt[ll] = lam[ll] / std::pow(eps + is[ll], 4);
+      }
+      double sum = 0.0;
+      for (int ll = 0; ll < admis; ++ll) sum = sum + wt[ll];
+      for (int ll = 0; ll < admis; ++ll) w[(size_t)ll * NV + k] = wt[ll] / sum;
+    }
+    // LIMITEDDW and its back-projection FINDW[d][v]
+    std::vector<double> fw((size_t)(ideg + 1) * NV);
+    for (int d = 0; d <= ideg; ++d) {
+      double lim[NV] = {0, 0, 0, 0, 0};
+      for (int ll = 0; ll < admis; ++ll) {
+        const int nd = (cw && ll > 0) ? ideg2 : ideg;
+        if (d > nd) continue;
+        for (int k = 0; k < NV; ++k) lim[k] = lim[k] + Wv(ll, d, k) * w[(size_t)ll * NV + k];
+      }
+      for (int v = 0; v < NV; ++v) {
+        double s = 0.0;
+        for (int k = 0; k < NV; ++k) s += ER[v][k] * lim[k];
+        fw[(size_t)d * NV + v] = s;
+      }
+    }
+    for (int q = 0; q < nq_of(x, c, f); ++q) {
+      basis(x, c, &g->qpoints[((c * F + f) * Q + q) * 3], ideg, b.data());
+      for (int v = 0; v < NV; ++v) {
+        double res = 0.0;
+        for (int d = 0; d < ideg; ++d) res += b[d] * fw[(size_t)(d + 1) * NV + v];
+        ul[(f * Q + q) * NV + v] = fw[v] + res;
+      }
+    }
+  }
 }
 
 void sutherland(const ucg_config* cfg, double rho, double p, double* mu, double* lam) {

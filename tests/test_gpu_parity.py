@@ -32,14 +32,20 @@ SMALL = {
 }
 
 
-def _setup(name, precision=N.UCG_FP64):
+# characteristic-variable WENO (WENWRT 2) on the WENO cases, and on a
+# channel with inflow/outflow/slip walls (boundary ghosts in the eigenvectors)
+SMALL["weno3_channel"] = (lambda: Mesh.bump_channel(16, 8, 8, seed=2), SCHEME_WENO, 2, 0, EULER)
+CHAR = ["weno3_tet", "weno5_hex", "cweno4_tet", "cweno4_ns_mixed", "weno3_channel"]
+
+
+def _setup(name, precision=N.UCG_FP64, wenwrt=1):
     mk, scheme, iorder, ees, gov = SMALL[name]
     m = mk().prepare(scheme, iorder, ees)
     p0 = 71.43
     bc = (1.0, 0.675 * np.sqrt(1.4), 0.0, 0.0, 1.0)
     cfg = make_config(m, governing=gov, precision=precision, reynolds=1600.0, pres=p0 if gov == NAVIER_STOKES else 1.0,
-                      prandtl=0.71, bc_state=bc)
-    if name == "muscl_bump":
+                      prandtl=0.71, bc_state=bc, wenwrt=wenwrt)
+    if name in ("muscl_bump", "weno3_channel"):
         U = m.initial_condition(1, [1.4, *bc])
         # a smooth disturbance so that every branch sees non-trivial data
         c = m.centres()
@@ -72,6 +78,41 @@ def test_residual_matches_oracle(name):
     err = (np.abs(Rg - Ro) / scale).max()
     print(f"{name}: residual rel err {err:.3e}")
     assert err < 1e-12
+
+
+@pytest.mark.parametrize("name", CHAR)
+def test_characteristic_weno_residual_matches_oracle(name):
+    """WENWRT 2: per-face eigenvector projection, indicators and weights per
+    characteristic variable (CHARACTERISTIC_RECONSTRUCTION)."""
+    m, cfg, U = _setup(name, wenwrt=2)
+    o = Oracle(m, cfg)
+    e = Engine(m, cfg)
+    e.set_state(U)
+    Rg = e.call_flux_subroutines_3d()
+    Ro = o.residual(U)
+    err = (np.abs(Rg - Ro) / _flux_scale(o, m, U)).max()
+    print(f"{name} (characteristic): residual rel err {err:.3e}")
+    assert err < 1e-12
+    e.check_health()
+    # the characteristic reconstruction is a different scheme: not the conserved one
+    cfg1 = N.UcgConfig.from_buffer_copy(cfg)
+    cfg1.wenwrt = 1
+    assert np.abs(Rg - Oracle(m, cfg1).residual(U)).max() > 1e-10 * np.abs(Rg).max()
+
+
+@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
+def test_characteristic_weno_mixed_close_to_fp64(name):
+    m, cfg, U = _setup(name, wenwrt=2)
+    _, cfgm, _ = _setup(name, precision=N.UCG_MIXED, wenwrt=2)
+    out = []
+    for c in (cfg, cfgm):
+        e = Engine(m, c)
+        e.set_state(U)
+        out.append(e.call_flux_subroutines_3d())
+        e.close()
+    err = (np.abs(out[0] - out[1]) / _flux_scale(None, m, U)).max()
+    print(f"{name} (characteristic): mixed vs fp64 residual rel err {err:.3e}")
+    assert err < 2e-5
 
 
 @pytest.mark.parametrize("name", ["muscl_ns_hex", "weno3_tet", "weno5_hex", "cweno4_tet", "muscl_bump"])

@@ -74,6 +74,7 @@ struct Problem {
   double* vflux;            // [n][MF][NV] viscous face sums
   unsigned* health;
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
+  int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
   double* dt_dev;           // device dt (ucg_step)
 };
 
@@ -237,6 +238,49 @@ __host__ __device__ __forceinline__ void hllc(double gamma, const S* cl, const S
   flux[2] = al * (fl0 * vl + sl * (mul * vl - cl[2])) + ar * (fr0 * vr + sr * (mur * vr - cr[2]));
   flux[3] = al * (fl0 * wl + sl * (mul * wl - cl[3])) + ar * (fr0 * wr + sr * (mur * wr - cr[3]));
   flux[4] = al * (ul * (el + pl) + sl * (mul * lastl - cl[4])) + ar * (ur * (er + pr) + sr * (mur * lastr - cr[4]));
+}
+
+// COMPUTE_EIGENVECTORS (src/flow_operations.f90:3934-3995): left (EL) and
+// right (ER) eigenvectors of the x-direction Euler flux Jacobian at the
+// arithmetic average of two face-frame states, written with stride `st`:
+// EL[(k * 5 + v) * st] (row k), ER[(v * 5 + k) * st] (column k).
+__device__ __forceinline__ void char_eigenvectors(double gamma, const double* rl, const double* rr, double* EL,
+                                                  double* ER, int st) {
+  const double gm1 = gamma - 1.0;
+  const double oor1 = 1.0 / rl[0], oor2 = 1.0 / rr[0];
+  const double rs = 0.5 * (rl[0] + rr[0]);
+  const double us = 0.5 * ((rl[1] * oor1) + (rr[1] * oor2));
+  const double vs = 0.5 * ((rl[2] * oor1) + (rr[2] * oor2));
+  const double ws = 0.5 * ((rl[3] * oor1) + (rr[3] * oor2));
+  const double es = 0.5 * (rl[4] + rr[4]);
+  const double vvs = us * us + vs * vs + ws * ws;
+  const double vsd = 0.5 * vvs;
+  const double ps = gm1 * (es - 0.5 * rs * vvs);
+  const double as = sqrt(gamma * ps / rs);
+  const double hs = (0.5 * vvs) + ((as * as) / gm1);
+  const double R[5][5] = {{1.0, 1.0, 0.0, 0.0, 1.0},
+                          {us - as, us, 0.0, 0.0, us + as},
+                          {vs, vs, 1.0, 0.0, vs},
+                          {ws, ws, 0.0, 1.0, ws},
+                          {hs - us * as, 0.5 * vvs, vs, ws, hs + us * as}};
+  const double iden = 1.0 / (2.0 * as * hs - 2.0 * as * vsd);
+  const double us2 = us * us, vs2 = vs * vs, ws2 = ws * ws;
+  const double L[5][5] = {
+      {(hs * us + as * us2 + as * vs2 - as * vsd - us * vsd + as * ws2) * iden, (-hs - as * us + vsd) * iden,
+       -(as * vs) * iden, -(as * ws) * iden, as * iden},
+      {(2.0 * as * hs - 2.0 * as * us2 - 2.0 * as * vs2 - 2.0 * as * ws2) * iden, (2.0 * as * us) * iden,
+       (2.0 * as * vs) * iden, (2.0 * as * ws) * iden, (-2.0 * as) * iden},
+      {(-2.0 * as * hs * vs + 2.0 * as * vs * vsd) * iden, 0.0, 1.0, 0.0, 0.0},
+      {(-2.0 * as * hs * ws + 2.0 * as * vsd * ws) * iden, 0.0, 0.0, 1.0, 0.0},
+      {(-(hs * us) + as * us2 + as * vs2 - as * vsd + us * vsd + as * ws2) * iden, (hs - as * us - vsd) * iden,
+       -(as * vs) * iden, -(as * ws) * iden, as * iden}};
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      EL[(i * 5 + j) * st] = L[i][j];
+      ER[(i * 5 + j) * st] = R[i][j];
+    }
 }
 
 // Venkatakrishnan limiter, SLOPE_LIMITERS case 7 (src/reconstruct_p.f90:3647-3652)

@@ -300,13 +300,15 @@ __device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[
 // face value minus cell mean, 0 in unused slots.  A face value is
 // sum_d m_d(x) g_d - sum_d mean(m_d) g_d: the second sum is formed once per
 // polynomial instead of subtracting the basis means at every face point.
-template <int P, typename T>
-__global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restrict__ U) {
+template <int P, typename T, bool CH = false>
+__global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<T>::N;
   constexpr int L2 = ID < 9 ? ID : 9;  // CWENO lower order: IDEGFREE2 3 or 9 (grid_p.f90:6145-6160)
   constexpr int VI = WVars<T>::is, VH = WVars<T>::face, VF = WVars<T>::fall;
-  __shared__ double s_w[7 * NV * 128];  // per thread, [ll][v]: indicators, then weights
+  constexpr int BT = CH ? 64 : 128;    // threads per block
+  __shared__ double s_w[7 * NV * BT];  // per thread, [ll][v]: indicators, then weights
+  __shared__ double s_e[CH ? 50 * BT : 1];  // per thread: left then right eigenvectors (characteristic form)
   const int tid = threadIdx.x;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + tid;
   if (c >= p.n) return;
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
   const T* xq = (const T*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;  // interleaved
   const T* bmv = (const T*)p.bmean + grp * (int64_t)ID * 32 + lane;    // interleaved
   T* out = (T*)p.dul + c * FQ * NV;
-  double* sw = s_w + tid;  // sw[(ll * NV + v) * 128]
+  double* sw = s_w + tid;  // sw[(ll * NV + v) * BT]
   const double lc1 = 1.0 - 1.0 / p.lwci;
   const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
   auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
@@ -385,8 +387,36 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
     }
   };
 
+  // nonlinear weights in FP64 ((10E-12)^4 underflows FP32): sw holds the
+  // indicators [ll][v] on entry and the weights on exit
+  auto weights = [&]() {
+    for (int v = 0; v < NV; ++v) {
+      const double lam0 = cw ? lc1 : p.lwci, lamk = cw ? lk : 1.0;
+      double tau = 0.0, sum = 0.0;
+      if (cw && p.wenoz) {
+        for (int ll = 0; ll < adm; ++ll) tau += fabs(sw[v * BT] - sw[(ll * NV + v) * BT]);
+        tau = tau / (adm - 1);
+      }
+      for (int ll = 0; ll < adm; ++ll) {
+        const double e = p.weno_eps + sw[(ll * NV + v) * BT];
+        const double lam = ll == 0 ? lam0 : lamk;
+        double wt;
+        if (cw && p.wenoz) {
+          double q = tau / e;
+          q = q * q;
+          wt = lam * (1.0 + q * q);
+        } else {
+          const double e2 = e * e;
+          wt = lam / (e2 * e2);
+        }
+        sw[(ll * NV + v) * BT] = wt;
+        sum += wt;
+      }
+      for (int ll = 0; ll < adm; ++ll) sw[(ll * NV + v) * BT] = sw[(ll * NV + v) * BT] / sum;
+    }
+  };
   bool fall = !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
-  if (!fall) {
+  if (!CH && !fall) {
     // ---- smoothness indicators g^T S g per stencil and variable
     const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
     for (int ll = 0; ll < adm; ++ll) {
@@ -407,34 +437,10 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
         }
 #pragma unroll
         for (int k = 0; k < VI; ++k)
-          if (v0 + k < NV) sw[(ll * NV + v0 + k) * 128] = (double)is[k];
+          if (v0 + k < NV) sw[(ll * NV + v0 + k) * BT] = (double)is[k];
       }
     }
-    // ---- nonlinear weights in FP64 ((10E-12)^4 underflows FP32)
-    for (int v = 0; v < NV; ++v) {
-      const double lam0 = cw ? lc1 : p.lwci, lamk = cw ? lk : 1.0;
-      double tau = 0.0, sum = 0.0;
-      if (cw && p.wenoz) {
-        for (int ll = 0; ll < adm; ++ll) tau += fabs(sw[v * 128] - sw[(ll * NV + v) * 128]);
-        tau = tau / (adm - 1);
-      }
-      for (int ll = 0; ll < adm; ++ll) {
-        const double e = p.weno_eps + sw[(ll * NV + v) * 128];
-        const double lam = ll == 0 ? lam0 : lamk;
-        double wt;
-        if (cw && p.wenoz) {
-          double q = tau / e;
-          q = q * q;
-          wt = lam * (1.0 + q * q);
-        } else {
-          const double e2 = e * e;
-          wt = lam / (e2 * e2);
-        }
-        sw[(ll * NV + v) * 128] = wt;
-        sum += wt;
-      }
-      for (int ll = 0; ll < adm; ++ll) sw[(ll * NV + v) * 128] = sw[(ll * NV + v) * 128] / sum;
-    }
+    weights();
     // ---- combined polynomial, face values, CHECKSOL (threshold 0.85)
     bool flag = false;
     for (int v0 = 0; v0 < NV; v0 += VH) {
@@ -442,14 +448,14 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
       load_g0(v0, gh, cw);
 #pragma unroll
       for (int k = 0; k < VH; ++k) {
-        const T w0 = v0 + k < NV ? T(sw[(v0 + k) * 128]) : T(0);
+        const T w0 = v0 + k < NV ? T(sw[(v0 + k) * BT]) : T(0);
 #pragma unroll
         for (int d = 0; d < ID; ++d) gh[d][k] = w0 * gh[d][k];
       }
       for (int ll = 1; ll < adm; ++ll) {
         T wl[VH];
 #pragma unroll
-        for (int k = 0; k < VH; ++k) wl[k] = v0 + k < NV ? T(sw[(ll * NV + v0 + k) * 128]) : T(0);
+        for (int k = 0; k < VH; ++k) wl[k] = v0 + k < NV ? T(sw[(ll * NV + v0 + k) * BT]) : T(0);
 #pragma unroll
         for (int d = 0; d < ID; ++d)
           if (!cw || d < ID2)
@@ -501,6 +507,181 @@ __global__ void __launch_bounds__(128) k_wpost(Problem p, const double* __restri
         }
       }
     }
+    fall = flag;
+  }
+  if (CH && !fall) {
+    // ---- CHARACTERISTIC_RECONSTRUCTION (src/reconstruct_p.f90:497-758), per
+    // face: eigenvectors at the average of the cell mean and the face
+    // neighbour's mean (or the boundary ghost of the cell mean), both in the
+    // face frame; stencil polynomials projected on the left eigenvectors
+    // (global-frame conserved variables, as the reference projects them);
+    // indicators and weights per characteristic variable; the face's
+    // polynomial back-projected.  With M_ll = ER diag(w_ll) EL the combined
+    // conserved polynomial is sum_ll M_ll G_ll (rows d >= 1) and its mean
+    // sum_ll M_ll u0, formed in FP64.
+    const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
+    double* EL = s_e + tid;            // EL[(k * NV + v) * BT]
+    double* ER = s_e + 25 * BT + tid;  // ER[(v * NV + k) * BT]
+    // stencil polynomial row d of variable u (CWENO: the central one with the
+    // lower-order stencils removed, reconstruct_p.f90:1723-1737; g3 holds
+    // sum_l2 lk * G(l2) for the rows d < IDEGFREE2)
+    auto Gp = [&](int ll, int d, int u, const T (&g3)[L2][NV]) -> T {
+      if (!(cw && ll == 0)) return G(ll, d, u);
+      return T(1.0 / lc1) * (G(0, d, u) - (d < L2 ? g3[d][u] : T(0)));
+    };
+    auto lower_sum = [&](T (&g3)[L2][NV]) {
+#pragma unroll
+      for (int d = 0; d < L2; ++d)
+#pragma unroll
+        for (int u = 0; u < NV; ++u) g3[d][u] = T(0);
+      if (!cw) return;
+      for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+          if (d < ID2)
+#pragma unroll
+            for (int u = 0; u < NV; ++u) g3[d][u] = g3[d][u] + T(lk) * G(l2, d, u);
+    };
+    bool flag = false;
+    for (int f = 0; f < nf; ++f) {
+      double r[4], ur[NV];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
+      const int64_t nb = p.neigh[c * MF + f];
+      if (nb >= 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ur[v] = U[nb * NV + v];
+      } else {
+        boundary_ghost(p, p.bc[c * MF + f], r, u0, ur);
+      }
+      {
+        double rl[NV], rr[NV];
+        rot_f(r, u0, rl);
+        rot_f(r, ur, rr);
+        char_eigenvectors(p.gamma, rl, rr, EL, ER, BT);
+      }
+      // indicators of the projected polynomials
+#pragma unroll 1
+      for (int ll = 0; ll < adm; ++ll) {
+        const bool low = cw && ll > 0;
+#pragma unroll 1
+        for (int k0 = 0; k0 < NV; k0 += VI) {
+          T is[VI];
+#pragma unroll
+          for (int k = 0; k < VI; ++k) is[k] = T(0);
+          T g3[L2][NV];
+          lower_sum(g3);
+          auto project = [&](auto& g, int nd) {
+            constexpr int ND = sizeof(g) / sizeof(g[0]);
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+              T gu[NV];
+#pragma unroll
+              for (int u = 0; u < NV; ++u) gu[u] = d < nd ? Gp(ll, d, u, g3) : T(0);
+#pragma unroll
+              for (int k = 0; k < VI; ++k) {
+                T a = T(0);
+                if (k0 + k < NV)
+#pragma unroll
+                  for (int u = 0; u < NV; ++u) a += T(EL[((k0 + k) * NV + u) * BT]) * gu[u];
+                g[d][k] = a;
+              }
+            }
+          };
+          if (low) {
+            T g[L2][VI];
+            project(g, ID2);
+            quad_form<L2, VI>(Pc + (int64_t)(p.i2off / VEC) * 32 * VEC, g, ID2, is);
+          } else {
+            T g[ID][VI];
+            project(g, ID);
+            quad_form<ID, VI>(Pc, g, ID, is);
+          }
+#pragma unroll
+          for (int k = 0; k < VI; ++k)
+            if (k0 + k < NV) sw[(ll * NV + k0 + k) * BT] = (double)is[k];
+        }
+      }
+      weights();
+      // the face's polynomial in conserved variables, VH at a time
+      const int nq = face_nq(p, p.ftype[c * MF + f]);
+#pragma unroll 1
+      for (int v0 = 0; v0 < NV; v0 += VH) {
+        T gh[ID][VH];
+        double f0[VH];
+#pragma unroll
+        for (int k = 0; k < VH; ++k) {
+          f0[k] = 0.0;
+#pragma unroll
+          for (int d = 0; d < ID; ++d) gh[d][k] = T(0);
+        }
+#pragma unroll 1
+        for (int ll = 0; ll < adm; ++ll) {
+          const int nd = cw && ll > 0 ? ID2 : ID;
+          T g3[L2][NV];
+          if (ll == 0) lower_sum(g3);
+          double M[VH][NV];
+#pragma unroll
+          for (int k = 0; k < VH; ++k)
+#pragma unroll
+            for (int u = 0; u < NV; ++u) {
+              double a = 0.0;
+              if (v0 + k < NV)
+#pragma unroll
+                for (int j = 0; j < NV; ++j)
+                  a += ER[((v0 + k) * NV + j) * BT] * sw[(ll * NV + j) * BT] * EL[(j * NV + u) * BT];
+              M[k][u] = a;
+            }
+#pragma unroll
+          for (int k = 0; k < VH; ++k)
+#pragma unroll
+            for (int u = 0; u < NV; ++u) f0[k] += M[k][u] * u0[u];
+#pragma unroll
+          for (int d = 0; d < ID; ++d)
+            if (d < nd) {
+              T gu[NV];
+#pragma unroll
+              for (int u = 0; u < NV; ++u) gu[u] = Gp(ll, d, u, g3);
+#pragma unroll
+              for (int k = 0; k < VH; ++k)
+#pragma unroll
+                for (int u = 0; u < NV; ++u) gh[d][k] += T(M[k][u]) * gu[u];
+            }
+        }
+        T cb[VH];
+        mean_term(gh, cb);
+        for (int q = 0; q < QS; ++q) {
+          T* o = out + (f * QS + q) * NV;
+          if (q >= nq) {
+#pragma unroll
+            for (int k = 0; k < VH; ++k)
+              if (v0 + k < NV) o[v0 + k] = T(0);
+            continue;
+          }
+          T m[ID];
+          mono(f, q, m);
+#pragma unroll
+          for (int k = 0; k < VH; ++k) {
+            T rsum = T(0);
+#pragma unroll
+            for (int d = 0; d < ID; ++d) rsum += m[d] * gh[d][k];
+            if (v0 + k < NV) o[v0 + k] = T((f0[k] - u0[v0 + k]) + (double)(rsum - cb[k]));
+          }
+        }
+      }
+      // CHECKSOL on this face's stored values
+      for (int q = 0; q < nq; ++q) {
+        const T* o = out + (f * QS + q) * NV;
+        double uf[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) uf[v] = u0[v] + (double)o[v];
+        flag = flag || jump_bad(p.gamma, pm, uf, 0.85);
+      }
+    }
+    for (int f = nf; f < MF; ++f)
+      for (int q = 0; q < QS; ++q)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[(f * QS + q) * NV + v] = T(0);
     fall = flag;
   }
   // CHECKSOLX (threshold 0.95) cannot fire where the 0.85 test passed on the
@@ -644,6 +825,26 @@ __global__ void k_visc_face(Problem p) {
   }
 }
 
+// Characteristic-variable post-processing (k_wpost<P, T, true>), 64 threads
+// per block for its shared eigenvectors.  Instantiated only in
+// recon_char_*.cu (explicit instantiations), which nvcc compiles in parallel
+// with the other reconstruction units.
+template <int P, typename T>
+cudaError_t launch_wpost_char(const Problem& p, const double* U, cudaStream_t st) {
+  k_wpost<P, T, true><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U);
+  return cudaGetLastError();
+}
+#ifndef UCG_RECON_CHAR_TU
+extern template cudaError_t launch_wpost_char<1, float>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<2, float>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<3, float>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<4, float>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<1, double>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<2, double>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<3, double>(const Problem&, const double*, cudaStream_t);
+extern template cudaError_t launch_wpost_char<4, double>(const Problem&, const double*, cudaStream_t);
+#endif
+
 // One reconstruction: stencil polynomials, WENO post-processing and, for
 // Navier-Stokes, the viscous LSQ and face gradients.  Instantiated per
 // precision and order in recon_*.cu, which nvcc compiles in parallel.
@@ -661,7 +862,12 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
   }
   if (mark) cudaEventRecord(mark, st);
-  k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+  if (p.wenwrt == 2) {
+    const cudaError_t e = launch_wpost_char<P, T>(p, U, st);
+    if (e != cudaSuccess) return e;
+  } else {
+    k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+  }
   *launches += 2;
   if (ns) {
     k_visc_lsq<P, T><<<(unsigned)((p.n * 4 + 127) / 128), 128, 0, st>>>(p, U);
@@ -672,7 +878,8 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   return cudaGetLastError();
 }
 
-// precision-specific entry points (recon_f32.cu + recon_f32_p4.cu, recon_f64.cu);
+// precision-specific entry points (recon_f32.cu + recon_f32_p4.cu, recon_f64.cu +
+// recon_f64_p4.cu; characteristic post-processing in recon_char*.cu);
 // iorder 1..4, anything else returns cudaErrorInvalidValue
 cudaError_t launch_weno_f32(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
                             int64_t* launches, cudaEvent_t mark);
@@ -680,5 +887,7 @@ cudaError_t launch_weno_f32_p4(const Problem& p, const double* U, bool ns, int Q
                                int64_t* launches, cudaEvent_t mark);
 cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
                             int64_t* launches, cudaEvent_t mark);
+cudaError_t launch_weno_f64_p4(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
+                               int64_t* launches, cudaEvent_t mark);
 
 }  // namespace ucg

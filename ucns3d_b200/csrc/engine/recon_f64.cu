@@ -1,4 +1,5 @@
-// FP64 reconstruction kernels, IORDER 1-4.
+// FP64 reconstruction kernels, IORDER 1-3, and the dispatch over IORDER;
+// IORDER 4 lives in recon_f64_p4.cu.
 #include "recon2.cuh"
 
 namespace ucg {
@@ -9,7 +10,7 @@ cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool 
     case 1: return launch_weno_t<1, double>(p, U, ns, QS, st, launches, mark);
     case 2: return launch_weno_t<2, double>(p, U, ns, QS, st, launches, mark);
     case 3: return launch_weno_t<3, double>(p, U, ns, QS, st, launches, mark);
-    case 4: return launch_weno_t<4, double>(p, U, ns, QS, st, launches, mark);
+    case 4: return launch_weno_f64_p4(p, U, ns, QS, st, launches, mark);
   }
   return cudaErrorInvalidValue;
 }
