@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="vortex_hex_weno5")
     ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--wenwrt", type=int, default=1, choices=[1, 2],
+                    help="WENO variables: 1 conserved, 2 characteristic (vortex_hex_weno5)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint timing (bump channel)")
     ap.add_argument("--adjoint-only", action="store_true", help="only the adjoint timing (bump channel)")
@@ -191,6 +193,8 @@ def make_case(args, precision):
     kw = {"precision": precision}
     if args.case in ("tgv_hex_muscl", "tgv_tet_weno3", "vortex_hex_weno5", "mixed_cweno4"):
         kw["n"] = args.n
+    if args.case == "vortex_hex_weno5" and args.wenwrt != 1:
+        kw["wenwrt"] = args.wenwrt
     return fn(**kw)
 
 
@@ -391,7 +395,8 @@ def main():
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "mixed: f32 tables/reconstruction, f64 flux/accumulate/update",
         "data": "synthetic (seeded mesh and analytic initial condition)",
-        "config": {"workload": args.case, "cells": ncells, "n": args.n, "scheme": "WENO5+HLLC SSP-RK3",
+        "config": {"workload": args.case, "cells": ncells, "n": args.n,
+                   "scheme": "WENO5+HLLC SSP-RK3" + (" (characteristic variables)" if args.wenwrt == 2 else ""),
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (tables)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "traffic_unit": "bytes per launch",

@@ -66,7 +66,8 @@ typedef struct ucg_config {
   int32_t scheme;      /* 2 MUSCL (IWENO=-1), 3 WENO/CWENO (IWENO=1)                    */
   int32_t iorder;      /* reconstruction degree IORDER = spatialorder-1, 1..4           */
   int32_t ees;         /* 0 WENO, 5 CWENO (parameters.f90:1340-1372)                    */
-  int32_t wenwrt;      /* 1 conserved-variable WENO                                    */
+  int32_t wenwrt;      /* 1 conserved-variable WENO, 2 characteristic-variable WENO
+                          (WENO only; WENWRT, reconstruct_p.f90:445, 497-758)         */
   int32_t limiter;     /* MUSCL limiter code, 7 = Venkatakrishnan                       */
   int32_t riemann;     /* 1 = HLLC                                                      */
   int32_t precision;   /* UCG_FP64 or UCG_MIXED                                         */

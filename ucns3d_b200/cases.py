@@ -74,9 +74,9 @@ def vortex_params(L=10.0, t=0.0, mach=0.5, strength=5.0):
     return [GAMMA, strength, u, u, 0.0, 0.5 * L, 0.5 * L, 0.5 * L, t, L, L, L]
 
 
-def vortex_hex_weno5(n=64, precision=N.UCG_FP64, L=10.0, nthreads=0) -> Case:
+def vortex_hex_weno5(n=64, precision=N.UCG_FP64, L=10.0, nthreads=0, wenwrt=1) -> Case:
     m = Mesh.box_hex(n, n, n, L=(L, L, L)).prepare(SCHEME_WENO, 4, nthreads=nthreads)
-    cfg = make_config(m, governing=EULER, precision=precision, pres=1.0, lwci=1000.0)
+    cfg = make_config(m, governing=EULER, precision=precision, pres=1.0, lwci=1000.0, wenwrt=wenwrt)
     U0 = m.initial_condition(IC_VORTEX, vortex_params(L))
     return Case("vortex_hex_weno5", m, cfg, U0, 0.5, 200, dict(n=n, L=L, scheme="WENO", order=5, equations="Euler"))
 
