@@ -57,7 +57,7 @@ enum {
 };
 
 enum { UCG_FP64 = 0, UCG_MIXED = 1 };
-enum { UCG_REDUCE_KE = 1, UCG_REDUCE_MASS = 2, UCG_REDUCE_ENERGY = 3 };
+enum { UCG_REDUCE_KE = 1, UCG_REDUCE_MASS = 2, UCG_REDUCE_ENERGY = 3, UCG_REDUCE_ENSTROPHY = 4 };
 
 /* Scheme and fluid parameters.  Field names follow UCNS3D's module globals
  * (src/parameters.f90, src/declarations.f90).                               */
@@ -170,7 +170,12 @@ int ucg_step(ucg_engine* e, double cfl, int32_t nsteps);
 int ucg_last_dt(ucg_engine* e, double* dt);
 
 /* Domain sums over cells: UCG_REDUCE_KE = sum V*rho*|u|^2/2 (time_p.f90:4145),
- * UCG_REDUCE_MASS = sum V*rho, UCG_REDUCE_ENERGY = sum V*E.                 */
+ * UCG_REDUCE_MASS = sum V*rho, UCG_REDUCE_ENERGY = sum V*E,
+ * UCG_REDUCE_ENSTROPHY = sum V*rho*(rho*|grad u - grad u^T|_F^2/2)/2, the
+ * TOTENS of a periodic (BOUNDTYPE 1) TGV run (ENSTROPHY_CALC,
+ * flow_operations.f90:2718-2815; time_p.f90:4311-4320) with the cell-centre
+ * velocity gradients of the viscous least squares; Navier-Stokes MUSCL
+ * (IORDER 1) only, where those gradients are the linear polynomial's.     */
 int ucg_reduce(ucg_engine* e, int32_t what, double* out);
 
 /* Synchronise, then report UCG_ENONPHYS if a kernel met a NaN or a

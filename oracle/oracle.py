@@ -44,6 +44,8 @@ def lib():
         L.orc_reduce.argtypes = [geop, f64p, C.c_int, f64p]
         L.orc_force.restype = C.c_int
         L.orc_force.argtypes = [cfgp, geop, recp, f64p, f64p]
+        L.orc_enstrophy.restype = C.c_int
+        L.orc_enstrophy.argtypes = [cfgp, geop, recp, f64p, f64p]
         _lib = L
     return _lib
 
@@ -108,6 +110,15 @@ class Oracle:
         rc = lib().orc_force(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U), C.byref(out))
         if rc:
             raise RuntimeError(f"orc_force failed: {rc}")
+        return out.value
+
+    def enstrophy(self, U: np.ndarray) -> float:
+        """TOTENS of a periodic TGV run (ENSTROPHY_CALC), Navier-Stokes MUSCL."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = C.c_double()
+        rc = lib().orc_enstrophy(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U), C.byref(out))
+        if rc:
+            raise RuntimeError(f"orc_enstrophy failed: {rc}")
         return out.value
 
     def reduce(self, U: np.ndarray, what: int) -> float:

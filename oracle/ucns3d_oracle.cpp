@@ -874,6 +874,34 @@ int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
 }
 
 // Domain sums (time_p.f90:4145-4198): 1 = kinetic energy, 2 = mass, 3 = energy.
+// ENSTROPHY_CALC (flow_operations.f90:2718-2815, BOUNDTYPE 1) summed as
+// TOTENS (time_p.f90:4311-4320): sum V * rho * 0.5 * (0.5 * ONORM * rho),
+// ONORM = |G - G^T|_F^2 with G the cell-centre velocity gradients
+// (SOLUTIONTRIAV2's GRADS, reconstruct_p.f90:2590-2660), which for IORDER 1
+// equal the face gradients of the linear viscous polynomial.
+int orc_enstrophy(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, const double* U, double* out) {
+  if (!check_ctx(cfg, g, r) || !U || !out || cfg->governing != 1 || cfg->scheme != 2 || cfg->iorder != 1)
+    return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  std::vector<double> UL, ULV;
+  std::vector<double> rhs((size_t)x.n * NV);
+  residual(x, U, rhs.data(), UL, ULV);
+  double s = 0.0;
+  for (int64_t c = 0; c < x.n; ++c) {
+    const double* G = &ULV[(size_t)c * F * Q * 12 + 3];
+    double on = 0.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const double d = G[i * 3 + j] - G[j * 3 + i];
+        on += d * d;
+      }
+    const double rho = U[c * NV];
+    s += g->volume[c] * (rho * 0.5 * (0.5 * (on * rho)));
+  }
+  *out = s;
+  return UCG_OK;
+}
+
 int orc_reduce(const ucg_geometry* g, const double* U, int what, double* out) {
   if (!g || !U || !out) return UCG_EINVAL;
   double s = 0.0;

@@ -177,6 +177,20 @@ def test_bitwise_deterministic():
     assert np.array_equal(out[0], out[1])
 
 
+def test_enstrophy_matches_oracle():
+    m, cfg, U = _setup("muscl_ns_hex")
+    e = Engine(m, cfg)
+    e.set_state(U)
+    a, b = e.enstrophy(), Oracle(m, cfg).enstrophy(U)
+    assert abs(a - b) <= 1e-12 * abs(b), (a, b)
+    m2, cfg2, U2 = _setup("weno3_ns_hex")
+    e2 = Engine(m2, cfg2)
+    e2.set_state(U2)
+    with pytest.raises(EngineError) as ei:
+        e2.enstrophy()
+    assert ei.value.code == N.UCG_EINVAL
+
+
 def test_reductions_match_oracle():
     m, cfg, U = _setup("weno5_hex")
     o = Oracle(m, cfg)

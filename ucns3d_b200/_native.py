@@ -18,7 +18,7 @@ UCG_MAX_QP = 16
 
 UCG_OK, UCG_EINVAL, UCG_ECUDA, UCG_ENONPHYS, UCG_ESTATE, UCG_ENOMEM, UCG_ETIMEOUT = range(7)
 UCG_FP64, UCG_MIXED = 0, 1
-UCG_REDUCE_KE, UCG_REDUCE_MASS, UCG_REDUCE_ENERGY = 1, 2, 3
+UCG_REDUCE_KE, UCG_REDUCE_MASS, UCG_REDUCE_ENERGY, UCG_REDUCE_ENSTROPHY = 1, 2, 3, 4
 
 ERROR_NAMES = {
     UCG_EINVAL: "UCG_EINVAL",

@@ -15,8 +15,9 @@
 //   1. k_adj_face      one thread per interior or mirror face: the reverse
 //                      sweep of HLLC (ad::hllc_adj) applied to
 //                      lambda_c - lambda_nb; k_adj_face_bnd, one thread per
-//                      other boundary face: the 5x10 Jacobian w.r.t. the
-//                      face value and p from dual numbers.  Together they
+//                      other boundary face and input direction: one column
+//                      of the 5x10 Jacobian w.r.t. the face value and p
+//                      from dual numbers.  Together they
 //                      give the adjoint of every face value.
 //   2. k_adj_muscl     one thread per cell: the MUSCL reconstruction (LSQ,
 //                      FIND_BOUNDS, Venkatakrishnan, CHECKSOLX) reversed by
@@ -166,45 +167,42 @@ __global__ void __launch_bounds__(128) k_adj_face(Problem p, int64_t nplain, con
 
 // The other boundary faces, owned faces [nplain, nown): their ghost state
 // depends on the free stream, so the 5x10 Jacobian of the face flux w.r.t.
-// the face value and the free-stream state is formed one input direction at
-// a time (Dual<1>).  pown[i - nplain] = adjoint of the free-stream state.
+// the face value and the free-stream state is formed one input direction
+// at a time (Dual<1>), one thread per face and direction k (k < 5: the face
+// value, k >= 5: the free-stream state).  pown[i - nplain] = adjoint of the
+// free-stream state.
 __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain, const double* __restrict__ U,
                                                       const double* __restrict__ lam, double* __restrict__ adjF,
                                                       double* __restrict__ pown) {
   using D = Dual<1>;
-  const int64_t i = nplain + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = nplain + t / 10;
+  const int k = (int)(t % 10);
   if (i >= p.nown) return;
   int64_t c, nb;
   int f, nf;
   double r[4], ul[NV], ur[NV], g[NV];
   adj_face_inputs(p, U, lam, i, c, f, nb, nf, r, ul, ur, g);
   const int bcode = p.bc[c * MF + f];
-  double out[10];
-#pragma unroll 1
-  for (int k = 0; k < 10; ++k) {
-    D L[NV], R[NV], bcs[NV];
+  D L[NV], R[NV], bcs[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      L[v] = D(ul[v]);
-      L[v].d[0] = v == k ? 1.0 : 0.0;
-      bcs[v] = D(ur[v]);
-      bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
-    }
-    boundary_ghost(p, bcode, r, L, bcs, R);
-    D a[NV], b[NV], h[NV], fl[NV];
-    rot_f(r, R, b);
-    rot_f(r, L, a);
-    hllc(p.gamma, a, b, h);
-    rot_b(r, h, fl);
-    double s = 0.0;
-#pragma unroll
-    for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
-    out[k] = s;
+  for (int v = 0; v < NV; ++v) {
+    L[v] = D(ul[v]);
+    L[v].d[0] = v == k ? 1.0 : 0.0;
+    bcs[v] = D(ur[v]);
+    bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
   }
+  boundary_ghost(p, bcode, r, L, bcs, R);
+  D a[NV], b[NV], h[NV], fl[NV];
+  rot_f(r, R, b);
+  rot_f(r, L, a);
+  hllc(p.gamma, a, b, h);
+  rot_b(r, h, fl);
+  double s = 0.0;
 #pragma unroll
-  for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = out[k];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) pown[(i - nplain) * NV + k] = out[5 + k];
+  for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
+  if (k < NV) adjF[(c * MF + f) * NV + k] = s;
+  else pown[(i - nplain) * NV + (k - NV)] = s;
 }
 
 // deterministic column sums of a [m][5] array in two passes: k_colsum5_part
@@ -849,8 +847,8 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
   if (nplain)
     k_adj_face<<<blocks_for(nplain, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p);
   if (nbnd)
-    k_adj_face_bnd<<<blocks_for(nbnd, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p,
-                                                                 (double*)e->adj_pface.p);
+    k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p,
+                                                                      (double*)e->adj_pface.p);
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
                                                          (double*)e->adj_contrib.p);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,

@@ -708,10 +708,17 @@ int ucg_last_dt(ucg_engine* e, double* dt) {
 }
 
 int ucg_reduce(ucg_engine* e, int32_t what, double* out) {
-  if (!e || !out || what < 1 || what > 3) return fail(e, UCG_EINVAL, "bad argument");
+  if (!e || !out || what < 1 || what > 4) return fail(e, UCG_EINVAL, "bad argument");
   if (!e->have_geometry || !e->have_state) return fail(e, UCG_ESTATE, "geometry and state are needed");
   cudaSetDevice(e->device);
   Problem p = make_problem(e);
+  if (what == UCG_REDUCE_ENSTROPHY) {
+    if (!(e->cfg.governing == 1 && e->cfg.scheme == 2 && e->cfg.iorder == 1))
+      return fail(e, UCG_EINVAL, "enstrophy needs the Navier-Stokes MUSCL (IORDER 1) configuration");
+    if (!ready(e)) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+    int rc = launch_recon(e, p, (const double*)e->Un.p);  // viscous least squares -> ulv
+    if (rc) return rc;
+  }
   int64_t nb = (e->n + 255) / 256;
   k_reduce_partial<<<(unsigned)nb, 256, 0, e->stream>>>(p, (const double*)e->Un.p, what, (double*)e->partial.p);
   k_reduce_final<<<1, 1024, 0, e->stream>>>((const double*)e->partial.p, nb, (double*)e->red.p);

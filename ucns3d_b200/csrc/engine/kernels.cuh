@@ -295,8 +295,24 @@ __global__ void k_reduce_partial(Problem p, const double* __restrict__ U, int wh
   double v = 0.0;
   if (c < p.n) {
     const double* u = U + c * NV;
-    double x = what == UCG_REDUCE_KE ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]
-                                     : (what == UCG_REDUCE_MASS ? u[0] : u[4]);
+    double x;
+    if (what == UCG_REDUCE_ENSTROPHY) {
+      // cell-centre velocity gradients g[i][j] = du_i/dx_j: the viscous
+      // least-squares face gradients of a linear polynomial (face 0, point 0)
+      const double* g = p.ulv + c * (int64_t)MF * 12 + 3;
+      double on = 0.0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const double d = g[i * 3 + j] - g[j * 3 + i];
+          on += d * d;
+        }
+      x = u[0] * 0.5 * (0.5 * (on * u[0]));
+    } else {
+      x = what == UCG_REDUCE_KE ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0]
+                                : (what == UCG_REDUCE_MASS ? u[0] : u[4]);
+    }
     v = p.vol[c] * x;
   }
   __shared__ double s[256];

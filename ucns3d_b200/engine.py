@@ -113,6 +113,10 @@ class Engine:
     def kinetic_energy(self) -> float:
         return self.reduce(N.UCG_REDUCE_KE)
 
+    def enstrophy(self) -> float:
+        """TOTENS of a periodic TGV run (ENSTROPHY_CALC); Navier-Stokes MUSCL."""
+        return self.reduce(N.UCG_REDUCE_ENSTROPHY)
+
     # ------------------------------------------- adjoint and tangent (FP64 MUSCL, Euler)
     def force(self) -> float:
         """Wall pressure force in x at the current state (COMPUTEFORCE, src/io.f90:18752)."""
