@@ -217,6 +217,54 @@ def test_torch_autograd_function(bump):
     e.set_state(U)
 
 
+@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
+def test_weno_vjp_matches_oracle_fd(name):
+    """VJP of the WENO residual (nonlinear weights, smoothness indicators,
+    stencil least squares, HLLC at every face point) against central
+    differences of the oracle's FP64 residual, on periodic meshes whose
+    cells are all on the WENO branch."""
+    from oracle import Oracle
+    from ucns3d_b200.config import make_config
+    from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
+    if name == "weno3_tet":
+        m = Mesh.box_tet(5, 5, 5, seed=3).prepare(SCHEME_WENO, 2)
+    else:
+        m = Mesh.box_hex(10, 10, 10).prepare(SCHEME_WENO, 4)
+    cfg = make_config(m, governing=2)
+    U = m.initial_condition(IC_TGV, [1.4, 5.0, 1.0])
+    rng = np.random.default_rng(12)
+    cc = m.centres()
+    U = U * (1.0 + 0.02 * np.sin(1.3 * cc[:, :1] + 0.7 * cc[:, 1:2] + 2.1 * cc[:, 2:3] + rng.uniform(0, 6.3, (1, 5))))
+    e = Engine(m, cfg)
+    e.set_state(U)
+    lam = rng.standard_normal(U.shape)
+    mu, pbar = e.residual_vjp(lam)
+    assert np.all(pbar == 0.0)  # periodic: no free-stream dependence
+    o = Oracle(m, cfg)
+    eps = 1e-6
+    for trial in range(2):
+        du = rng.standard_normal(U.shape) * np.abs(U).max(0) * 1e-2
+        fd = float(np.sum(lam * (o.residual(U + eps * du) - o.residual(U - eps * du)))) / (2 * eps)
+        ad = float(np.sum(mu * du))
+        assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-30), (trial, ad, fd)
+    e.close()
+
+
+def test_weno_vjp_rejects_the_muscl_fall_back():
+    """Cells next to the channel walls are not FULL (they take the MUSCL
+    fall-back), which the WENO adjoint does not cover."""
+    from ucns3d_b200.config import make_config
+    from ucns3d_b200.mesh import SCHEME_WENO, Mesh
+    m = Mesh.bump_channel(16, 8, 8, seed=2).prepare(SCHEME_WENO, 2)
+    cfg = make_config(m, governing=2, bc_state=(1.0, 0.8, 0.0, 0.0, 1.0))
+    e = Engine(m, cfg)
+    e.set_state(np.tile([1.0, 0.8, 0.0, 0.0, 1.0 / 0.4 + 0.32], (m.ncells, 1)))
+    with pytest.raises(EngineError) as ei:
+        e.residual_vjp(np.ones((m.ncells, 5)))
+    assert ei.value.code == N.UCG_EINVAL
+    e.close()
+
+
 def test_adjoint_rejects_other_configurations():
     c = cases.vortex_hex_weno5(n=8)
     e = Engine(c.mesh, c.cfg)

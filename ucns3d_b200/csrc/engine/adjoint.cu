@@ -101,27 +101,43 @@ __global__ void __launch_bounds__(1024) k_sum1(const double* __restrict__ a, int
 }
 
 // ------------------------------------------------------------ face VJP
-// adjF[c][f] = adjoint of the face value of cell c at face f.  The owned
-// faces come grouped (interior, mirror boundaries, other boundaries), and
-// the two kinds of kernel below take disjoint ranges of that list.
-__device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* __restrict__ U,
-                                                const double* __restrict__ lam, int64_t i, int64_t& c, int& f,
-                                                int64_t& nb, int& nf, double* r, double* ul, double* ur,
-                                                double* g) {
+// adjF[c][f][q] = adjoint of the face value of cell c at point q of face f
+// ([n][F][QS][5]; one point per face for MUSCL IORDER 1).  The owned faces
+// come grouped (interior, mirror boundaries, other boundaries), and the two
+// kinds of kernel below take disjoint ranges of that list.
+struct FaceRef {
+  int64_t c, nb;
+  int f, nf, nq, QS;
+};
+__device__ __forceinline__ FaceRef face_ref(const Problem& p, int64_t i) {
+  FaceRef F;
   const int32_t code = p.own[i];
-  c = code >> 3;
-  f = code & 7;
-  nb = p.neigh[c * MF + f];
-  nf = p.nface[c * MF + f];
+  F.c = code >> 3;
+  F.f = code & 7;
+  F.nb = p.neigh[F.c * MF + F.f];
+  F.nf = p.nface[F.c * MF + F.f];
+  F.nq = face_nq(p, p.ftype[F.c * MF + F.f]);
+  F.QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  return F;
+}
+// inputs of face point q: the two face values (the free-stream state as the
+// second input of a boundary face), the weighted adjoint difference g, and
+// the neighbour's point qq
+__device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* __restrict__ U,
+                                                const double* __restrict__ lam, const FaceRef& F, int q,
+                                                double* r, double* ul, double* ur, double* g, int& qq) {
+  const int64_t c = F.c, nb = F.nb;
+  const int f = F.f;
 #pragma unroll
   for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
-  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
+  const double ws = face_weight(p, p.ftype[c * MF + f], q) * p.area[c * MF + f];
   const double* dul = (const double*)p.dul;
+  qq = nb >= 0 ? p.qperm[(c * MF + f) * F.QS + q] : 0;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    ul[v] = U[c * NV + v] + dul[(c * MF + f) * NV + v];
+    ul[v] = U[c * NV + v] + dul[((c * MF + f) * F.QS + q) * NV + v];
     if (nb >= 0) {
-      ur[v] = U[nb * NV + v] + dul[(nb * MF + nf) * NV + v];
+      ur[v] = U[nb * NV + v] + dul[((nb * MF + F.nf) * F.QS + qq) * NV + v];
       g[v] = ws * (lam[c * NV + v] - lam[nb * NV + v]);
     } else {
       ur[v] = p.bc_state[v];  // free-stream state, the second input of a boundary face
@@ -131,37 +147,39 @@ __device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* 
 }
 
 // Interior and mirror faces, owned faces [0, nplain): reverse sweep of HLLC
-// (ad::hllc_adj) in the face frame.  The rotations are orthogonal (rot_b =
-// rot_f^T), and a mirror ghost is b = S a in the face frame (S flips the
-// normal momentum).
+// (ad::hllc_adj) in the face frame at every face point.  The rotations are
+// orthogonal (rot_b = rot_f^T), and a mirror ghost is b = S a in the face
+// frame (S flips the normal momentum).
 __global__ void __launch_bounds__(128) k_adj_face(Problem p, int64_t nplain, const double* __restrict__ U,
                                                   const double* __restrict__ lam, double* __restrict__ adjF) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nplain) return;
-  int64_t c, nb;
-  int f, nf;
-  double r[4], ul[NV], ur[NV], g[NV];
-  adj_face_inputs(p, U, lam, i, c, f, nb, nf, r, ul, ur, g);
-  double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
-  rot_f(r, ul, a);
-  if (nb >= 0) {
-    rot_f(r, ur, b);
-  } else {
+  const FaceRef F = face_ref(p, i);
+  for (int q = 0; q < F.nq; ++q) {
+    double r[4], ul[NV], ur[NV], g[NV];
+    int qq;
+    adj_face_inputs(p, U, lam, F, q, r, ul, ur, g, qq);
+    double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
+    rot_f(r, ul, a);
+    if (F.nb >= 0) {
+      rot_f(r, ur, b);
+    } else {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
-  }
-  rot_f(r, g, hb);
-  ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
-  if (nb < 0)
+      for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
+    }
+    rot_f(r, g, hb);
+    ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
+    if (F.nb < 0)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
-  rot_b(r, ab, o);
+      for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
+    rot_b(r, ab, o);
 #pragma unroll
-  for (int k = 0; k < NV; ++k) adjF[(c * MF + f) * NV + k] = o[k];
-  if (nb >= 0) {
-    rot_b(r, bb, o);
+    for (int k = 0; k < NV; ++k) adjF[((F.c * MF + F.f) * F.QS + q) * NV + k] = o[k];
+    if (F.nb >= 0) {
+      rot_b(r, bb, o);
 #pragma unroll
-    for (int k = 0; k < NV; ++k) adjF[(nb * MF + nf) * NV + k] = o[k];
+      for (int k = 0; k < NV; ++k) adjF[((F.nb * MF + F.nf) * F.QS + qq) * NV + k] = o[k];
+    }
   }
 }
 
@@ -170,7 +188,7 @@ __global__ void __launch_bounds__(128) k_adj_face(Problem p, int64_t nplain, con
 // the face value and the free-stream state is formed one input direction
 // at a time (Dual<1>), one thread per face and direction k (k < 5: the face
 // value, k >= 5: the free-stream state).  pown[i - nplain] = adjoint of the
-// free-stream state.
+// free-stream state, summed over the face's points.
 __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain, const double* __restrict__ U,
                                                       const double* __restrict__ lam, double* __restrict__ adjF,
                                                       double* __restrict__ pown) {
@@ -179,11 +197,13 @@ __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain,
   const int64_t i = nplain + t / 10;
   const int k = (int)(t % 10);
   if (i >= p.nown) return;
-  int64_t c, nb;
-  int f, nf;
+  const FaceRef F = face_ref(p, i);
+  const int bcode = p.bc[F.c * MF + F.f];
+  double sp = 0.0;
+  for (int q = 0; q < F.nq; ++q) {
   double r[4], ul[NV], ur[NV], g[NV];
-  adj_face_inputs(p, U, lam, i, c, f, nb, nf, r, ul, ur, g);
-  const int bcode = p.bc[c * MF + f];
+  int qq;
+  adj_face_inputs(p, U, lam, F, q, r, ul, ur, g, qq);
   D L[NV], R[NV], bcs[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
@@ -201,8 +221,10 @@ __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain,
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
-  if (k < NV) adjF[(c * MF + f) * NV + k] = s;
-  else pown[(i - nplain) * NV + (k - NV)] = s;
+  if (k < NV) adjF[((F.c * MF + F.f) * F.QS + q) * NV + k] = s;
+  else sp += s;
+  }
+  if (k >= NV) pown[(i - nplain) * NV + (k - NV)] = sp;
 }
 
 // deterministic column sums of a [m][5] array in two passes: k_colsum5_part
@@ -746,14 +768,18 @@ unsigned blocks_for(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
 namespace ucg_host {
 
 void adjoint_release(ucg_engine* e) {
-  ucg_engine::DevBuf* all[] = {&e->adj_face, &e->adj_contrib, &e->adj_rptr, &e->adj_rsrc, &e->adj_lam,
-                               &e->adj_mu,   &e->adj_pface,   &e->adj_tflux, &e->adj_tdul, &e->adj_tU,
-                               &e->adj_fcell, &e->adj_traj,  &e->adj_bar,  &e->adj_tmp, &e->adj_fwd};
+  ucg_engine::DevBuf* all[] = {&e->adj_face,   &e->adj_contrib, &e->adj_rptr,  &e->adj_rsrc,     &e->adj_lam,
+                               &e->adj_mu,     &e->adj_pface,   &e->adj_tflux, &e->adj_tdul,     &e->adj_tU,
+                               &e->adj_fcell,  &e->adj_traj,    &e->adj_bar,   &e->adj_tmp,      &e->adj_fwd,
+                               &e->adjw_face,  &e->adjw_gbar,   &e->adjw_scr,  &e->adjw_self,    &e->adjw_contrib,
+                               &e->adjw_rptr,  &e->adjw_rsrc,   &e->adjw_flag, &e->adjw_lam,     &e->adjw_mu,
+                               &e->adjw_pface, &e->adjw_tmp};
   for (auto* b : all) {
     if (b->p) e->bytes -= (int64_t)b->bytes;
     release(*b);
   }
   e->adj_ready = false;
+  e->adjw_ready = false;
 }
 
 }  // namespace ucg_host
@@ -916,6 +942,100 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
   return UCG_OK;
 }
 
+// ---------------------------------------------------------------- WENO
+// The VJP of the WENO residual: conserved-variable WENO (EES 0), Euler, FP64
+// form, cells off the MUSCL fall-back.
+int adjw_setup(ucg_engine* e) {
+  const ucg_config& c = e->cfg;
+  if (!(c.scheme == 3 && c.ees == 0 && c.wenwrt == 1 && c.governing == 2 && c.precision == UCG_FP64))
+    return fail(e, UCG_EINVAL, "the WENO adjoint covers conserved-variable WENO (EES 0), Euler, FP64 form");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (e->adjw_ready) return UCG_OK;
+  const int64_t n = e->n, ngrp = (n + 31) / 32;
+  const int A = c.admis_max, IM = c.imax, W = IM + 1, ID = c.ideg;
+  const int64_t slots = 1 + (int64_t)A * IM;
+  cudaSetDevice(e->device);
+  // the stencils, back from the device (interleaved over 32-cell groups)
+  std::vector<int32_t> st((size_t)ngrp * 32 * A * W);
+  CK(cudaMemcpyAsync(st.data(), e->sten.p, st.size() * 4, cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  auto target = [&](int64_t i, int64_t s) -> int64_t {
+    if (s == 0) return i;
+    const int ll = (int)((s - 1) / IM), k = (int)((s - 1) % IM);
+    if (ll >= e->admis_h[i]) return -1;
+    return st[(size_t)(((i >> 5) * A * W + ll * W + k + 1) * 32 + (i & 31))];
+  };
+  std::vector<int64_t> cnt(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t s = 0; s < slots; ++s) {
+      const int64_t t = target(i, s);
+      if (t >= 0 && t < n) ++cnt[t + 1];
+    }
+  for (int64_t j = 0; j < n; ++j) cnt[j + 1] += cnt[j];
+  std::vector<int64_t> src(cnt[n]), pos(cnt.begin(), cnt.end() - 1);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t s = 0; s < slots; ++s) {
+      const int64_t t = target(i, s);
+      if (t >= 0 && t < n) src[pos[t]++] = s * n + i;
+    }
+  auto get = [&](ucg_engine::DevBuf& b, size_t bytes) { return alloc(e, b, bytes); };
+  int rc = get(e->adjw_face, (size_t)n * MF * e->QS * NV * 8);
+  rc = rc ? rc : get(e->adjw_gbar, (size_t)ngrp * 32 * A * ID * NV * 8);
+  rc = rc ? rc : get(e->adjw_scr, (size_t)ngrp * 32 * 2 * ID * NV * 8);
+  rc = rc ? rc : get(e->adjw_self, (size_t)n * NV * 8);
+  rc = rc ? rc : get(e->adjw_contrib, (size_t)n * slots * NV * 8);
+  rc = rc ? rc : get(e->adjw_rptr, (size_t)(n + 1) * 8);
+  rc = rc ? rc : get(e->adjw_rsrc, (size_t)std::max<int64_t>(1, cnt[n]) * 8);
+  rc = rc ? rc : get(e->adjw_flag, 64);
+  rc = rc ? rc : get(e->adjw_lam, (size_t)n * NV * 8);
+  rc = rc ? rc : get(e->adjw_mu, (size_t)n * NV * 8 + 64 * 8);
+  rc = rc ? rc : get(e->adjw_pface, (size_t)std::max<int64_t>(1, e->nown - e->nown_plain) * NV * 8);
+  rc = rc ? rc : get(e->adjw_tmp, (size_t)(std::max<int64_t>(1, e->nown - e->nown_plain) / 1024 + 2) * NV * 8);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(e->adjw_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
+  if (cnt[n]) CK(cudaMemcpyAsync(e->adjw_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
+  CK(cudaMemsetAsync(e->adjw_face.p, 0, (size_t)n * MF * e->QS * NV * 8, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->adjw_ready = true;
+  return UCG_OK;
+}
+
+// mu = (dR/dU)^T lam, psum = (dR/dp)^T lam for the WENO residual (device)
+int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* lam, double* mu, double* psum) {
+  int rc = launch_recon(e, p, U);  // stencil polynomials (gbuf) and face values (dul)
+  if (rc) return rc;
+  const int64_t n = e->n, nplain = e->nown_plain, nbnd = e->nown - nplain;
+  double* adjF = (double*)e->adjw_face.p;
+  if (nplain) k_adj_face<<<blocks_for(nplain, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF);
+  if (nbnd)
+    k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF,
+                                                                      (double*)e->adjw_pface.p);
+  e->launches += (nplain > 0) + (nbnd > 0);
+  CK(cudaMemsetAsync(e->adjw_flag.p, 0, sizeof(int), e->stream));
+  if ((rc = launch_weno_adjoint(e, p, U, adjF, (double*)e->adjw_gbar.p, (double*)e->adjw_scr.p,
+                                (double*)e->adjw_self.p, (double*)e->adjw_contrib.p, (int*)e->adjw_flag.p)))
+    return rc;
+  k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adjw_rptr.p,
+                                                          (const int64_t*)e->adjw_rsrc.p,
+                                                          (const double*)e->adjw_contrib.p, mu);
+  e->launches++;
+  if (nbnd) {
+    const int64_t rows = 1024, nb = (nbnd + rows - 1) / rows;
+    k_colsum5_part<<<(unsigned)nb, 256, 0, e->stream>>>((const double*)e->adjw_pface.p, nbnd, rows,
+                                                         (double*)e->adjw_tmp.p);
+    k_colsum5<<<NV, 256, 0, e->stream>>>((const double*)e->adjw_tmp.p, nb, psum);
+    e->launches += 2;
+  } else {
+    CK(cudaMemsetAsync(psum, 0, NV * sizeof(double), e->stream));
+  }
+  CK(cudaGetLastError());
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, e->adjw_flag.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (flag) return fail(e, UCG_EINVAL, "a cell is on the MUSCL fall-back (FULL = 0 or CHECKSOL), which the WENO adjoint does not cover");
+  return UCG_OK;
+}
+
 int copy_in(ucg_engine* e, double* dst, const double* src, size_t count) {
   CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyHostToDevice, e->stream));
   return UCG_OK;
@@ -957,6 +1077,21 @@ int ucg_force_vjp(ucg_engine* e, double* dJdU) {
 
 int ucg_residual_vjp(ucg_engine* e, const double* lambda, double* mu, double* pbar) {
   if (!e || !lambda || !mu) return fail(e, UCG_EINVAL, "null argument");
+  if (e->cfg.scheme == 3) {  // WENO
+    int rc = adjw_setup(e);
+    if (rc) return rc;
+    cudaSetDevice(e->device);
+    Problem p = make_problem(e);
+    const size_t m = (size_t)e->n * NV;
+    double* s = (double*)e->adjw_mu.p + m;
+    if ((rc = copy_in(e, (double*)e->adjw_lam.p, lambda, m))) return rc;
+    if ((rc = weno_vjp_device(e, p, (const double*)e->Un.p, (const double*)e->adjw_lam.p, (double*)e->adjw_mu.p, s)))
+      return rc;
+    if ((rc = copy_out(e, mu, (const double*)e->adjw_mu.p, m))) return rc;
+    if (pbar && (rc = copy_out(e, pbar, s, NV))) return rc;
+    CK(cudaStreamSynchronize(e->stream));
+    return UCG_OK;
+  }
   int rc = adj_setup(e);
   if (rc) return rc;
   cudaSetDevice(e->device);

@@ -1,0 +1,263 @@
+// Discrete adjoint (VJP) of the WENO reconstruction (conserved variables,
+// EES 0, FP64 form): the reverse of CP_RECONSTRUCTION's nonlinear weights
+// and smoothness indicators (src/reconstruct_p.f90:920-1250) and of the
+// stencil least squares (LEAST_SQUARES, src/gradients.f90:253-497).
+//
+// Forward, per cell c and variable v (k_lsq, k_wpost):
+//   G_l  = M_l (U_st(l,k) - U_c)                         l < ADMIS
+//   IS_l = G_l^T S G_l,  wt_l = lam_l / (eps + IS_l)^4,  om_l = wt_l / sum wt
+//   u(x) = U_c + sum_l om_l b(x) . G_l                   at every face point
+// Reverse, given ub(x) = dJ/du(x) at the face points:
+//   Bb      = sum_x ub(x) b(x)                (the basis with its mean removed)
+//   omb_l   = Bb . G_l
+//   wtb_l   = (omb_l - sum_m omb_m om_m) / sum wt
+//   ISb_l   = -4 wtb_l wt_l / (eps + IS_l)
+//   Gb_l    = om_l Bb + ISb_l 2 S G_l
+//   U_c    += sum_x ub(x);  U_st(l,k) += M_l[k]^T Gb_l;  U_c -= sum_k M_l[k]^T Gb_l
+// A cell whose CHECKSOL test (or FULL = 0) put it on the MUSCL fall-back is
+// not covered: the kernel raises a flag and the VJP returns UCG_EINVAL.
+#include <cuda_runtime.h>
+
+#include "engine_internal.h"
+#include "recon2.cuh"
+
+using namespace ucg;
+
+namespace {
+
+// k_adj_wpost: one lane per cell.  Writes Gb (layout of the stencil
+// polynomials G) and the direct adjoint of the cell mean; scr holds Bb and
+// the combined polynomial of the CHECKSOL test (interleaved like G).
+template <int P>
+__global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __restrict__ U,
+                                                  const double* __restrict__ adjF, double* __restrict__ gbar,
+                                                  double* __restrict__ scr, double* __restrict__ selfc,
+                                                  int* __restrict__ flag) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int VEC = Vec<double>::N;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const int A = p.admis_max;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int FQ = MF * QS;
+  const int adm = p.admis[c], nf = p.nfaces[c];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int ll, int d, int v) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  double* Sc = scr + grp * (int64_t)(2 * ID * NV) * 32 + lane;
+  auto BB = [&](int d, int v) -> double& { return Sc[(int64_t)(d * NV + v) * 32]; };
+  auto GH = [&](int d, int v) -> double& { return Sc[(int64_t)((ID + d) * NV + v) * 32]; };
+  const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
+  const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
+  const double* aF = adjF + c * (int64_t)FQ * NV;
+  double u0[NV], pm[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
+  cons2prim(p.gamma, u0, pm);
+  auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
+  auto mono = [&](int f, int q, double (&m)[ID]) {
+    const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+    monomials<P, double>(xi[0], xi[32], xi[64], m);
+  };
+  if (!p.full[c]) {
+    atomicOr(flag, 1);
+    return;
+  }
+  // ---- the direct term and Bb = sum_x ub(x) (m(x) - mean(m))
+  double sadj[NV] = {0, 0, 0, 0, 0};
+  for (int f = 0; f < nf; ++f)
+    for (int q = 0; q < nq_of(f); ++q)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sadj[v] += aF[(f * QS + q) * NV + v];
+#pragma unroll 1
+  for (int v0 = 0; v0 < NV; v0 += 2) {
+    double acc[ID][2];
+#pragma unroll
+    for (int d = 0; d < ID; ++d) acc[d][0] = acc[d][1] = 0.0;
+    for (int f = 0; f < nf; ++f)
+      for (int q = 0; q < nq_of(f); ++q) {
+        double m[ID];
+        mono(f, q, m);
+        const double a0 = aF[(f * QS + q) * NV + v0], a1 = v0 + 1 < NV ? aF[(f * QS + q) * NV + v0 + 1] : 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) {
+          acc[d][0] += m[d] * a0;
+          acc[d][1] += m[d] * a1;
+        }
+      }
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      const double b = bmv[d * 32];
+      BB(d, v0) = acc[d][0] - b * sadj[v0];
+      if (v0 + 1 < NV) BB(d, v0 + 1) = acc[d][1] - b * sadj[v0 + 1];
+    }
+  }
+  // ---- per variable: indicators, weights and their adjoints
+  const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+#pragma unroll 1
+  for (int v = 0; v < NV; ++v) {
+    double is[7], wt[7], om[7], omb[7];
+    double sum = 0.0;
+    for (int ll = 0; ll < adm; ++ll) {
+      double g[ID][1], s1[1] = {0.0};
+#pragma unroll
+      for (int d = 0; d < ID; ++d) g[d][0] = G(ll, d, v);
+      quad_form<ID, 1>(Pc, g, ID, s1);
+      is[ll] = s1[0];
+      const double e = p.weno_eps + is[ll];
+      const double e2 = e * e;
+      wt[ll] = (ll == 0 ? p.lwci : 1.0) / (e2 * e2);
+      sum += wt[ll];
+    }
+    for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
+    // combined polynomial (CHECKSOL) and the weights' adjoints
+    double dot = 0.0;
+    for (int ll = 0; ll < adm; ++ll) {
+      double ob = 0.0;
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        const double gd = G(ll, d, v);
+        ob += BB(d, v) * gd;
+        GH(d, v) = (ll == 0 ? 0.0 : GH(d, v)) + om[ll] * gd;
+      }
+      omb[ll] = ob;
+      dot += ob * om[ll];
+    }
+    for (int ll = 0; ll < adm; ++ll) {
+      const double wtb = (omb[ll] - dot) / sum;
+      const double isb = wtb * (-4.0 * wt[ll] / (p.weno_eps + is[ll]));
+      double g[ID], gr[ID];
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        g[d] = G(ll, d, v);
+        gr[d] = 0.0;
+      }
+      // gr = 2 S g from the packed triangle (P_dd = S_dd, P_de = 2 S_de)
+      int rs = 0;
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+#pragma unroll
+        for (int q = 0; q < (ID - d + VEC - 1) / VEC; ++q) {
+          double sv[VEC];
+          ldv(Pc + (int64_t)(rs + q) * 32 * VEC, sv);
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            const int e = d + q * VEC + i;
+            if (e < ID) {
+              if (e == d) {
+                gr[d] += 2.0 * sv[i] * g[d];
+              } else {
+                gr[d] += sv[i] * g[e];
+                gr[e] += sv[i] * g[d];
+              }
+            }
+          }
+        }
+        rs += (ID - d + VEC - 1) / VEC;
+        asm volatile("" ::: "memory");
+      }
+#pragma unroll
+      for (int d = 0; d < ID; ++d) Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = om[ll] * BB(d, v) + isb * gr[d];
+    }
+  }
+  // ---- CHECKSOL (0.85) on the WENO face values: a flagged cell took the
+  // MUSCL fall-back in the forward, which this adjoint does not cover
+  bool bad = false;
+  double cb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    cb[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) cb[v] += bmv[d * 32] * GH(d, v);
+  }
+  for (int f = 0; f < nf && !bad; ++f)
+    for (int q = 0; q < nq_of(f); ++q) {
+      double m[ID], uf[NV];
+      mono(f, q, m);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) r += m[d] * GH(d, v);
+        uf[v] = u0[v] + (r - cb[v]);
+      }
+      bad = bad || jump_bad(p.gamma, pm, uf, 0.85);
+    }
+  if (bad) atomicOr(flag, 1);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) selfc[c * NV + v] = sadj[v];
+}
+
+// k_adj_lsq: one lane per cell, the transpose of the stencil least squares.
+// Gb of the current stencil sits in shared memory (32 lanes per block);
+// contributions go to slot-major buffers: slot 0 the cell, 1 + l*IMAX + k
+// member k of stencil l, each written once.
+template <int P>
+__global__ void __launch_bounds__(32) k_adj_lsq(Problem p, const double* __restrict__ gbar,
+                                                const double* __restrict__ selfc, double* __restrict__ contrib) {
+  constexpr int ID = Deg<P>::ideg;
+  __shared__ double s_g[ID * NV][32];
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = p.n;
+  if (c >= n) return;
+  const int tid = threadIdx.x;
+  const int A = p.admis_max, IM = p.imax;
+  const int adm = p.admis[c];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  const double* Mi = (const double*)p.invmat + grp * p.tstride * 32 + lane;
+  double self[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) self[v] = selfc[c * NV + v];
+  for (int ll = 0; ll < adm; ++ll) {
+    for (int j = 0; j < ID * NV; ++j) s_g[j][tid] = Gb[(int64_t)(ll * ID * NV + j) * 32];
+    const double* M = Mi + (int64_t)p.soff[ll] * 32;
+    for (int k = 0; k < IM; ++k) {
+      double a[NV] = {0, 0, 0, 0, 0};
+      const double* Mk = M + (int64_t)k * ID * 32;
+#pragma unroll 2
+      for (int d = 0; d < ID; ++d) {
+        const double m = Mk[d * 32];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) a[v] += m * s_g[d * NV + v][tid];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        contrib[((int64_t)(1 + ll * IM + k) * n + c) * NV + v] = a[v];
+        self[v] -= a[v];
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) contrib[(int64_t)c * NV + v] = self[v];
+}
+
+template <int P>
+void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
+              double* contrib, int* flag, cudaStream_t st) {
+  k_adj_wpost<P><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U, adjF, gbar, scr, selfc, flag);
+  k_adj_lsq<P><<<(unsigned)((p.n + 31) / 32), 32, 0, st>>>(p, gbar, selfc, contrib);
+}
+
+}  // namespace
+
+namespace ucg_host {
+
+int launch_weno_adjoint(ucg_engine* e, const Problem& p, const double* U, const double* adjF, double* gbar,
+                        double* scr, double* selfc, double* contrib, int* flag) {
+  switch (e->cfg.iorder) {
+    case 1: launch_t<1>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
+    case 2: launch_t<2>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
+    case 3: launch_t<3>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
+    case 4: launch_t<4>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
+    default: return fail(e, UCG_EINVAL, "iorder out of range");
+  }
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+}  // namespace ucg_host

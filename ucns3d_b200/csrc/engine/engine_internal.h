@@ -61,6 +61,10 @@ struct ucg_engine {
   int adj_slots = 0;                // contribution slots per cell: self, IMAX stencil cells, 6 face neighbours
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
       adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd;
+  // discrete adjoint of the WENO reconstruction (adjoint_weno.cu)
+  bool adjw_ready = false;
+  DevBuf adjw_face, adjw_gbar, adjw_scr, adjw_self, adjw_contrib, adjw_rptr, adjw_rsrc, adjw_flag, adjw_lam, adjw_mu,
+      adjw_pface, adjw_tmp;
 };
 
 namespace ucg_host {
@@ -83,5 +87,8 @@ int launch_flux(ucg_engine* e, const ucg::Problem& p, int mode, const double* Uc
 int rk3(ucg_engine* e, double dt, bool dt_dev);
 // frees the adjoint buffers (adjoint.cu)
 void adjoint_release(ucg_engine* e);
+// reverse of the WENO post-processing and least squares (adjoint_weno.cu)
+int launch_weno_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, const double* adjF, double* gbar,
+                        double* scr, double* selfc, double* contrib, int* flag);
 
 }  // namespace ucg_host
