@@ -219,10 +219,11 @@ def test_torch_autograd_function(bump):
 
 @pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
 def test_weno_vjp_matches_oracle_fd(name):
-    """VJP of the WENO residual (nonlinear weights, smoothness indicators,
-    stencil least squares, HLLC at every face point) against central
-    differences of the oracle's FP64 residual, on periodic meshes whose
-    cells are all on the WENO branch."""
+    """VJP and JVP of the WENO residual (nonlinear weights, smoothness
+    indicators, stencil least squares, HLLC at every face point) against
+    central differences of the oracle's FP64 residual, and the dot-product
+    test between them, on periodic meshes whose cells are all on the WENO
+    branch."""
     from oracle import Oracle
     from ucns3d_b200.config import make_config
     from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
@@ -244,9 +245,17 @@ def test_weno_vjp_matches_oracle_fd(name):
     eps = 1e-6
     for trial in range(2):
         du = rng.standard_normal(U.shape) * np.abs(U).max(0) * 1e-2
-        fd = float(np.sum(lam * (o.residual(U + eps * du) - o.residual(U - eps * du)))) / (2 * eps)
+        fdv = (o.residual(U + eps * du) - o.residual(U - eps * du)) / (2 * eps)
+        fd = float(np.sum(lam * fdv))
         ad = float(np.sum(mu * du))
         assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-30), (trial, ad, fd)
+        # the tangent: against the same differences, and the dot-product test
+        jvp = e.residual_jvp(du)
+        err = (np.abs(jvp - fdv) / (np.abs(fdv).max(0) + 1e-300)).max()
+        print(f"{name}: WENO JVP vs oracle differences {err:.2e}")
+        assert err < 1e-6
+        a, b = float(np.sum(lam * jvp)), ad
+        assert abs(a - b) <= 1e-12 * np.abs(lam * jvp).sum(), (a, b)
     e.close()
 
 

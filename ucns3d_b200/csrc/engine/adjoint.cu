@@ -662,47 +662,51 @@ __global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __res
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   using D = Dual<1>;
-  const int32_t code = p.own[i];
-  const int64_t c = code >> 3;
-  const int f = code & 7;
-  const int64_t nb = p.neigh[c * MF + f];
-  const int nf = p.nface[c * MF + f];
+  const FaceRef F = face_ref(p, i);
+  const int64_t c = F.c, nb = F.nb;
+  const int f = F.f, nf = F.nf, QS = F.QS;
   double r[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) r[k] = p.rot[(c * MF + f) * 4 + k];
-  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
   const double* dul = (const double*)p.dul;
-  D L[NV], R[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    L[v] = D(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
-    L[v].d[0] = dU[c * NV + v] + tdul[(c * MF + f) * NV + v];
-  }
-  if (nb >= 0) {
+  double tf[NV] = {0, 0, 0, 0, 0};
+  for (int q = 0; q < F.nq; ++q) {
+    const double ws = face_weight(p, p.ftype[c * MF + f], q) * p.area[c * MF + f];
+    D L[NV], R[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      R[v] = D(U[nb * NV + v] + dul[(nb * MF + nf) * NV + v]);
-      R[v].d[0] = dU[nb * NV + v] + tdul[(nb * MF + nf) * NV + v];
+      L[v] = D(U[c * NV + v] + dul[((c * MF + f) * QS + q) * NV + v]);
+      L[v].d[0] = dU[c * NV + v] + tdul[((c * MF + f) * QS + q) * NV + v];
     }
-  } else {
-    D bcs[NV];
+    if (nb >= 0) {
+      const int qq = p.qperm[(c * MF + f) * QS + q];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      bcs[v] = D(p.bc_state[v]);
-      bcs[v].d[0] = dp.v[v];
+      for (int v = 0; v < NV; ++v) {
+        R[v] = D(U[nb * NV + v] + dul[((nb * MF + nf) * QS + qq) * NV + v]);
+        R[v].d[0] = dU[nb * NV + v] + tdul[((nb * MF + nf) * QS + qq) * NV + v];
+      }
+    } else {
+      D bcs[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        bcs[v] = D(p.bc_state[v]);
+        bcs[v].d[0] = dp.v[v];
+      }
+      boundary_ghost(p, (int)p.bc[c * MF + f], r, L, bcs, R);
     }
-    boundary_ghost(p, (int)p.bc[c * MF + f], r, L, bcs, R);
+    D a[NV], b[NV], h[NV], fl[NV];
+    rot_f(r, R, b);
+    rot_f(r, L, a);
+    hllc(p.gamma, a, b, h);
+    rot_b(r, h, fl);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) tf[v] = tf[v] + fl[v].d[0] * ws;
   }
-  D a[NV], b[NV], h[NV], fl[NV];
-  rot_f(r, R, b);
-  rot_f(r, L, a);
-  hllc(p.gamma, a, b, h);
-  rot_b(r, h, fl);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) tflux[(c * MF + f) * NV + v] = fl[v].d[0] * ws;
+  for (int v = 0; v < NV; ++v) tflux[(c * MF + f) * NV + v] = tf[v];
   if (nb >= 0)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) tflux[(nb * MF + nf) * NV + v] = -(fl[v].d[0] * ws);
+    for (int v = 0; v < NV; ++v) tflux[(nb * MF + nf) * NV + v] = -tf[v];
 }
 
 // tangent of the residual: face sums in face order
@@ -1036,6 +1040,31 @@ int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   return UCG_OK;
 }
 
+// dR = (dR/dU) dU + (dR/dp) dp for the WENO residual (device)
+int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* dU, const Dp5& dp, double* dR) {
+  int rc = launch_recon(e, p, U);  // G (gbuf) and face values (dul)
+  if (rc) return rc;
+  Problem pt = p;
+  pt.gbuf = e->adjw_gbar.p;  // dG = least squares of dU
+  CK(launch_lsq_f64(e->cfg.iorder, pt, dU, e->stream));
+  e->launches++;
+  CK(cudaMemsetAsync(e->adjw_flag.p, 0, sizeof(int), e->stream));
+  double* tdul = (double*)e->adjw_face.p;
+  double* tflux = (double*)e->adjw_contrib.p;
+  if ((rc = launch_weno_tangent(e, p, U, (const double*)e->adjw_gbar.p, (double*)e->adjw_scr.p, tdul,
+                                (int*)e->adjw_flag.p)))
+    return rc;
+  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux);
+  k_jvp_sum<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, tflux, dR);
+  e->launches += 2;
+  CK(cudaGetLastError());
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, e->adjw_flag.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  if (flag) return fail(e, UCG_EINVAL, "a cell is on the MUSCL fall-back (FULL = 0 or CHECKSOL), which the WENO tangent does not cover");
+  return UCG_OK;
+}
+
 int copy_in(ucg_engine* e, double* dst, const double* src, size_t count) {
   CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyHostToDevice, e->stream));
   return UCG_OK;
@@ -1109,6 +1138,22 @@ int ucg_residual_vjp(ucg_engine* e, const double* lambda, double* mu, double* pb
 
 int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* drhs) {
   if (!e || !du || !drhs) return fail(e, UCG_EINVAL, "null argument");
+  if (e->cfg.scheme == 3) {  // WENO
+    int rc = adjw_setup(e);
+    if (rc) return rc;
+    cudaSetDevice(e->device);
+    Problem p = make_problem(e);
+    const size_t m = (size_t)e->n * NV;
+    Dp5 d{};
+    if (dp)
+      for (int k = 0; k < NV; ++k) d.v[k] = dp[k];
+    if ((rc = copy_in(e, (double*)e->adjw_lam.p, du, m))) return rc;
+    if ((rc = weno_jvp_device(e, p, (const double*)e->Un.p, (const double*)e->adjw_lam.p, d, (double*)e->adjw_mu.p)))
+      return rc;
+    if ((rc = copy_out(e, drhs, (const double*)e->adjw_mu.p, m))) return rc;
+    CK(cudaStreamSynchronize(e->stream));
+    return UCG_OK;
+  }
   int rc = adj_setup(e);
   if (rc) return rc;
   cudaSetDevice(e->device);

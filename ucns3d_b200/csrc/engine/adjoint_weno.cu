@@ -5,6 +5,7 @@
 //
 // Forward, per cell c and variable v (k_lsq, k_wpost):
 //   G_l  = M_l (U_st(l,k) - U_c)                         l < ADMIS
+// (The tangent, k_jvp_wpost, pushes dG = M_l (dU_st - dU_c) forward instead.)
 //   IS_l = G_l^T S G_l,  wt_l = lam_l / (eps + IS_l)^4,  om_l = wt_l / sum wt
 //   u(x) = U_c + sum_l om_l b(x) . G_l                   at every face point
 // Reverse, given ub(x) = dJ/du(x) at the face points:
@@ -235,6 +236,138 @@ __global__ void __launch_bounds__(32) k_adj_lsq(Problem p, const double* __restr
   for (int v = 0; v < NV; ++v) contrib[(int64_t)c * NV + v] = self[v];
 }
 
+// k_jvp_wpost: one lane per cell, the tangent of the WENO face values
+// (minus the cell mean) from the tangent stencil polynomials dG:
+//   dIS_l = d(G_l^T S G_l),  dwt_l = -4 wt_l dIS_l / (eps + IS_l),
+//   dom_l = (dwt_l - om_l sum dwt) / sum wt,
+//   du(x) - dU_c = b(x) . sum_l (dom_l G_l + om_l dG_l).
+// Same fall-back flag as k_adj_wpost.
+template <int P>
+__global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __restrict__ U,
+                                                  const double* __restrict__ dG, double* __restrict__ scr,
+                                                  double* __restrict__ tdul, int* __restrict__ flag) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int VEC = Vec<double>::N;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const int A = p.admis_max;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int FQ = MF * QS;
+  const int adm = p.admis[c], nf = p.nfaces[c];
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  const double* dGc = dG + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int ll, int d, int v) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  auto dGv = [&](int ll, int d, int v) -> double { return dGc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  double* Sc = scr + grp * (int64_t)(2 * ID * NV) * 32 + lane;
+  auto TD = [&](int d, int v) -> double& { return Sc[(int64_t)(d * NV + v) * 32]; };
+  auto GH = [&](int d, int v) -> double& { return Sc[(int64_t)((ID + d) * NV + v) * 32]; };
+  const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
+  const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
+  double* out = tdul + c * (int64_t)FQ * NV;
+  for (int i = 0; i < FQ * NV; ++i) out[i] = 0.0;
+  double u0[NV], pm[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
+  cons2prim(p.gamma, u0, pm);
+  auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
+  auto mono = [&](int f, int q, double (&m)[ID]) {
+    const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+    monomials<P, double>(xi[0], xi[32], xi[64], m);
+  };
+  if (!p.full[c]) {
+    atomicOr(flag, 1);
+    return;
+  }
+  const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+#pragma unroll 1
+  for (int v = 0; v < NV; ++v) {
+    double is[7], dis[7], wt[7], dwt[7];
+    double sum = 0.0, dsum = 0.0;
+    for (int ll = 0; ll < adm; ++ll) {
+      double g[ID], dg[ID];
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        g[d] = G(ll, d, v);
+        dg[d] = dGv(ll, d, v);
+      }
+      // IS = sum_d P_dd g_d^2 + sum_{d<e} P_de g_d g_e and its tangent
+      double a = 0.0, da = 0.0;
+      int rs = 0;
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        double t = 0.0, dt = 0.0;
+#pragma unroll
+        for (int q = 0; q < (ID - d + VEC - 1) / VEC; ++q) {
+          double sv[VEC];
+          ldv(Pc + (int64_t)(rs + q) * 32 * VEC, sv);
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            const int e = d + q * VEC + i;
+            if (e < ID) {
+              t += sv[i] * g[e];
+              dt += sv[i] * dg[e];
+            }
+          }
+        }
+        rs += (ID - d + VEC - 1) / VEC;
+        // IS = sum_d g_d t_d, t_d = sum_{e>=d} P_de g_e: product rule
+        a += g[d] * t;
+        da += dg[d] * t + g[d] * dt;
+        asm volatile("" ::: "memory");
+      }
+      is[ll] = a;
+      dis[ll] = da;
+      const double e = p.weno_eps + a;
+      const double e2 = e * e;
+      wt[ll] = (ll == 0 ? p.lwci : 1.0) / (e2 * e2);
+      dwt[ll] = -4.0 * wt[ll] * dis[ll] / e;
+      sum += wt[ll];
+      dsum += dwt[ll];
+    }
+    for (int ll = 0; ll < adm; ++ll) {
+      const double om = wt[ll] / sum;
+      const double dom = (dwt[ll] - om * dsum) / sum;
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        const double gd = G(ll, d, v);
+        TD(d, v) = (ll == 0 ? 0.0 : TD(d, v)) + (dom * gd + om * dGv(ll, d, v));
+        GH(d, v) = (ll == 0 ? 0.0 : GH(d, v)) + om * gd;
+      }
+    }
+  }
+  double cb[NV], tb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    cb[v] = tb[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      cb[v] += bmv[d * 32] * GH(d, v);
+      tb[v] += bmv[d * 32] * TD(d, v);
+    }
+  }
+  bool bad = false;
+  for (int f = 0; f < nf; ++f)
+    for (int q = 0; q < nq_of(f); ++q) {
+      double m[ID], uf[NV];
+      mono(f, q, m);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        double r = 0.0, t = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) {
+          r += m[d] * GH(d, v);
+          t += m[d] * TD(d, v);
+        }
+        uf[v] = u0[v] + (r - cb[v]);
+        out[(f * QS + q) * NV + v] = t - tb[v];
+      }
+      bad = bad || jump_bad(p.gamma, pm, uf, 0.85);
+    }
+  if (bad) atomicOr(flag, 1);
+}
+
 template <int P>
 void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
               double* contrib, int* flag, cudaStream_t st) {
@@ -242,9 +375,30 @@ void launch_t(const Problem& p, const double* U, const double* adjF, double* gba
   k_adj_lsq<P><<<(unsigned)((p.n + 31) / 32), 32, 0, st>>>(p, gbar, selfc, contrib);
 }
 
+template <int P>
+void launch_jvp_t(const Problem& p, const double* U, const double* dG, double* scr, double* tdul, int* flag,
+                  cudaStream_t st) {
+  k_jvp_wpost<P><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U, dG, scr, tdul, flag);
+}
+
 }  // namespace
 
 namespace ucg_host {
+
+int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dG, double* scr,
+                        double* tdul, int* flag) {
+  switch (e->cfg.iorder) {
+    case 1: launch_jvp_t<1>(p, U, dG, scr, tdul, flag, e->stream); break;
+    case 2: launch_jvp_t<2>(p, U, dG, scr, tdul, flag, e->stream); break;
+    case 3: launch_jvp_t<3>(p, U, dG, scr, tdul, flag, e->stream); break;
+    case 4: launch_jvp_t<4>(p, U, dG, scr, tdul, flag, e->stream); break;
+    default: return fail(e, UCG_EINVAL, "iorder out of range");
+  }
+  e->launches++;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
 
 int launch_weno_adjoint(ucg_engine* e, const Problem& p, const double* U, const double* adjF, double* gbar,
                         double* scr, double* selfc, double* contrib, int* flag) {

@@ -12,6 +12,11 @@
 #include "device.cuh"
 #include "ucns3d_gpu.h"
 
+namespace ucg {
+// the stencil least squares alone, FP64 tables (recon_f64.cu)
+cudaError_t launch_lsq_f64(int iorder, const Problem& p, const double* U, cudaStream_t st);
+}  // namespace ucg
+
 namespace ucg_host {
 
 struct DevBuf {
@@ -90,5 +95,8 @@ void adjoint_release(ucg_engine* e);
 // reverse of the WENO post-processing and least squares (adjoint_weno.cu)
 int launch_weno_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, const double* adjF, double* gbar,
                         double* scr, double* selfc, double* contrib, int* flag);
+// tangent of the WENO face values from the tangent stencil polynomials dG
+int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dG, double* scr,
+                        double* tdul, int* flag);
 
 }  // namespace ucg_host

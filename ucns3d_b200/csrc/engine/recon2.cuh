@@ -889,5 +889,9 @@ cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool 
                             int64_t* launches, cudaEvent_t mark);
 cudaError_t launch_weno_f64_p4(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st,
                                int64_t* launches, cudaEvent_t mark);
+// the stencil least squares alone (FP64 tables) into p.gbuf: G is linear in
+// U, so applied to a tangent dU it gives the tangent dG (adjoint.cu)
+cudaError_t launch_lsq_f64(int iorder, const Problem& p, const double* U, cudaStream_t st);
+cudaError_t launch_lsq_f64_p4(const Problem& p, const double* U, cudaStream_t st);
 
 }  // namespace ucg

@@ -15,4 +15,16 @@ cudaError_t launch_weno_f64(int iorder, const Problem& p, const double* U, bool 
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_lsq_f64(int iorder, const Problem& p, const double* U, cudaStream_t st) {
+  const unsigned b = (unsigned)((p.n + 127) / 128);
+  switch (iorder) {
+    case 1: k_lsq<1, double><<<b, 128, 0, st>>>(p, U); break;
+    case 2: k_lsq<2, double><<<b, 128, 0, st>>>(p, U); break;
+    case 3: k_lsq<3, double><<<b, 128, 0, st>>>(p, U); break;
+    case 4: return launch_lsq_f64_p4(p, U, st);
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace ucg
