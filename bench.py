@@ -340,11 +340,26 @@ def run_adjoint(local, steps=200, every=20):
     ev[3].synchronize()
     primal, adj = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
     eng.close()
-    return {"workload": "bump_muscl", "cells": c.mesh.ncells, "dtype": "f64", "residual_ms": t["residual"],
-            "vjp_ms": t["vjp"], "jvp_ms": t["jvp"], "vjp_over_residual": t["vjp"] / t["residual"],
-            "run_steps": steps, "checkpoint_every": every, "primal_run_ms": primal, "adjoint_run_ms": adj,
-            "adjoint_run_over_primal_run": adj / primal, "J": J,
-            "dJdp": [float(x) for x in gp]}
+    out = {"workload": "bump_muscl", "cells": c.mesh.ncells, "dtype": "f64", "residual_ms": t["residual"],
+           "vjp_ms": t["vjp"], "jvp_ms": t["jvp"], "vjp_over_residual": t["vjp"] / t["residual"],
+           "run_steps": steps, "checkpoint_every": every, "primal_run_ms": primal, "adjoint_run_ms": adj,
+           "adjoint_run_over_primal_run": adj / primal, "J": J,
+           "dJdp": [float(x) for x in gp]}
+    # the WENO residual's VJP/JVP (FP64 form) on the vortex, 32^3 hexahedra
+    from ucns3d_b200 import _native as N
+    from ucns3d_b200.engine import EngineError
+    cw = cases.vortex_hex_weno5(n=32, precision=N.UCG_FP64)
+    ew = Engine(cw.mesh, cw.cfg, device=local)
+    ew.set_state(cw.U0)
+    try:
+        tw = ew.time_adjoint(reps=5)
+        out["weno"] = {"workload": "vortex_hex_weno5", "cells": cw.mesh.ncells, "dtype": "f64",
+                       "residual_ms": tw["residual"], "vjp_ms": tw["vjp"], "jvp_ms": tw["jvp"],
+                       "vjp_over_residual": tw["vjp"] / tw["residual"]}
+    except EngineError as err:
+        out["weno"] = {"unavailable": str(err)}
+    ew.close()
+    return out
 
 
 def main():

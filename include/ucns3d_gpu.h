@@ -230,7 +230,11 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
 /* ---------------------------------------------------------------- adjoint
  * Discrete adjoint (VJP) and tangent (JVP) for the FP64 form of a MUSCL
  * (scheme 2, IORDER 1) Euler configuration (the adjoint workload is the
- * bump channel).  p denotes the free-stream state bc_state[5] (primitive:
+ * bump channel).  ucg_residual_vjp and ucg_residual_jvp also cover
+ * conserved-variable WENO (scheme 3, EES 0, Euler, FP64 form): the
+ * reverse/tangent of the nonlinear weights, smoothness indicators and
+ * stencil least squares; a cell on the MUSCL fall-back (FULL = 0 or
+ * CHECKSOL) makes them return UCG_EINVAL.  p denotes the free-stream state bc_state[5] (primitive:
  * rho, u, v, w, pressure) used by the inflow, outflow and far-field ghost
  * states.  Host arrays; [n][5] as everywhere.  Other configurations return
  * UCG_EINVAL.
@@ -260,7 +264,7 @@ int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0,
                     double* dJ);
 /* Average device times over `reps` evaluations at the current state (CUDA
  * events on the handle's stream), into ms[3]: ms[0] residual (reconstruction
- * + fluxes), ms[1] residual VJP, ms[2] residual JVP.                      */
+ * + fluxes), ms[1] residual VJP, ms[2] residual JVP (MUSCL or WENO).       */
 int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms);
 
 /* Message of the last failure of ucg_create (no handle exists then). */

@@ -1172,14 +1172,16 @@ int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* 
 
 int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms) {
   if (!e || !ms || reps < 1) return fail(e, UCG_EINVAL, "bad argument");
-  int rc = adj_setup(e);
+  const bool weno = e->cfg.scheme == 3;
+  int rc = weno ? adjw_setup(e) : adj_setup(e);
   if (rc) return rc;
   cudaSetDevice(e->device);
   Problem p = make_problem(e);
   const int64_t n = e->n;
   const double* U = (const double*)e->Un.p;
-  double* x = bar_vec(e, 0);
-  double* y = bar_vec(e, 1);
+  double* x = weno ? (double*)e->adjw_lam.p : bar_vec(e, 0);
+  double* y = weno ? (double*)e->adjw_mu.p : bar_vec(e, 1);
+  double* ps = weno ? (double*)e->adjw_mu.p + (size_t)n * NV : bar_scal(e);
   CK(cudaMemsetAsync(x, 0, (size_t)n * NV * 8, e->stream));
   cudaEvent_t ev[4];
   for (auto& t : ev) CK(cudaEventCreate(&t));
@@ -1190,9 +1192,9 @@ int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms) {
     rc = launch_recon(e, p, U);
     if (!rc) rc = launch_flux(e, p, 0, U, U, nullptr, 0.0);
     cudaEventRecord(ev[1], e->stream);
-    if (!rc) rc = vjp_device(e, p, U, x, y, bar_scal(e));
+    if (!rc) rc = weno ? weno_vjp_device(e, p, U, x, y, ps) : vjp_device(e, p, U, x, y, ps);
     cudaEventRecord(ev[2], e->stream);
-    if (!rc) rc = jvp_device(e, p, U, x, d, y);
+    if (!rc) rc = weno ? weno_jvp_device(e, p, U, x, d, y) : jvp_device(e, p, U, x, d, y);
     cudaEventRecord(ev[3], e->stream);
     cudaEventSynchronize(ev[3]);
     float t;
