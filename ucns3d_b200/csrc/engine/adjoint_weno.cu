@@ -115,16 +115,26 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
     // combined polynomial (CHECKSOL) and the weights' adjoints
     double dot = 0.0;
-    for (int ll = 0; ll < adm; ++ll) {
-      double ob = 0.0;
+    {
+      double gh[ID], bb[ID];
 #pragma unroll
       for (int d = 0; d < ID; ++d) {
-        const double gd = G(ll, d, v);
-        ob += BB(d, v) * gd;
-        GH(d, v) = (ll == 0 ? 0.0 : GH(d, v)) + om[ll] * gd;
+        gh[d] = 0.0;
+        bb[d] = BB(d, v);
       }
-      omb[ll] = ob;
-      dot += ob * om[ll];
+      for (int ll = 0; ll < adm; ++ll) {
+        double ob = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) {
+          const double gd = G(ll, d, v);
+          ob += bb[d] * gd;
+          gh[d] = (ll == 0 ? 0.0 : gh[d]) + om[ll] * gd;
+        }
+        omb[ll] = ob;
+        dot += ob * om[ll];
+      }
+#pragma unroll
+      for (int d = 0; d < ID; ++d) GH(d, v) = gh[d];
     }
     for (int ll = 0; ll < adm; ++ll) {
       const double wtb = (omb[ll] - dot) / sum;
@@ -191,19 +201,19 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
   for (int v = 0; v < NV; ++v) selfc[c * NV + v] = sadj[v];
 }
 
-// k_adj_lsq: one lane per cell, the transpose of the stencil least squares.
-// Gb of the current stencil sits in shared memory (32 lanes per block);
-// contributions go to slot-major buffers: slot 0 the cell, 1 + l*IMAX + k
-// member k of stencil l, each written once.
+// k_adj_lsq: one lane per cell, the transpose of the stencil least squares,
+// shaped like k_lsq: DH rows of Gb in registers per pass, the members of
+// the stencil streamed; a member's contribution is the sum of its row
+// passes (the first writes, the next add).  Contributions go to slot-major
+// buffers: slot 0 the cell, 1 + l*IMAX + k member k of stencil l.
 template <int P>
-__global__ void __launch_bounds__(32) k_adj_lsq(Problem p, const double* __restrict__ gbar,
-                                                const double* __restrict__ selfc, double* __restrict__ contrib) {
+__global__ void __launch_bounds__(128) k_adj_lsq(Problem p, const double* __restrict__ gbar,
+                                                 const double* __restrict__ selfc, double* __restrict__ contrib) {
   constexpr int ID = Deg<P>::ideg;
-  __shared__ double s_g[ID * NV][32];
+  constexpr int DH = LsqRows<P, double>::value;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = p.n;
   if (c >= n) return;
-  const int tid = threadIdx.x;
   const int A = p.admis_max, IM = p.imax;
   const int adm = p.admis[c];
   const int64_t grp = c >> 5;
@@ -214,21 +224,30 @@ __global__ void __launch_bounds__(32) k_adj_lsq(Problem p, const double* __restr
 #pragma unroll
   for (int v = 0; v < NV; ++v) self[v] = selfc[c * NV + v];
   for (int ll = 0; ll < adm; ++ll) {
-    for (int j = 0; j < ID * NV; ++j) s_g[j][tid] = Gb[(int64_t)(ll * ID * NV + j) * 32];
-    const double* M = Mi + (int64_t)p.soff[ll] * 32;
-    for (int k = 0; k < IM; ++k) {
-      double a[NV] = {0, 0, 0, 0, 0};
-      const double* Mk = M + (int64_t)k * ID * 32;
+    for (int d0 = 0; d0 < ID; d0 += DH) {
+      double gb[DH][NV];
+#pragma unroll
+      for (int j = 0; j < DH; ++j)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) gb[j][v] = d0 + j < ID ? Gb[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] : 0.0;
+      const double* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
 #pragma unroll 2
-      for (int d = 0; d < ID; ++d) {
-        const double m = Mk[d * 32];
+      for (int k = 0; k < IM; ++k) {
+        const double* Mk = M + (int64_t)k * ID * 32;
+        double a[NV] = {0, 0, 0, 0, 0};
 #pragma unroll
-        for (int v = 0; v < NV; ++v) a[v] += m * s_g[d * NV + v][tid];
-      }
+        for (int j = 0; j < DH; ++j)
+          if (d0 + j < ID) {
+            const double m = Mk[j * 32];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        contrib[((int64_t)(1 + ll * IM + k) * n + c) * NV + v] = a[v];
-        self[v] -= a[v];
+            for (int v = 0; v < NV; ++v) a[v] += m * gb[j][v];
+          }
+        double* o = contrib + ((int64_t)(1 + ll * IM + k) * n + c) * NV;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          o[v] = d0 == 0 ? a[v] : o[v] + a[v];
+          self[v] -= a[v];
+        }
       }
     }
   }
@@ -326,15 +345,23 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
       sum += wt[ll];
       dsum += dwt[ll];
     }
+    double td[ID], gh[ID];
+#pragma unroll
+    for (int d = 0; d < ID; ++d) td[d] = gh[d] = 0.0;
     for (int ll = 0; ll < adm; ++ll) {
       const double om = wt[ll] / sum;
       const double dom = (dwt[ll] - om * dsum) / sum;
 #pragma unroll
       for (int d = 0; d < ID; ++d) {
         const double gd = G(ll, d, v);
-        TD(d, v) = (ll == 0 ? 0.0 : TD(d, v)) + (dom * gd + om * dGv(ll, d, v));
-        GH(d, v) = (ll == 0 ? 0.0 : GH(d, v)) + om * gd;
+        td[d] = (ll == 0 ? 0.0 : td[d]) + (dom * gd + om * dGv(ll, d, v));
+        gh[d] = (ll == 0 ? 0.0 : gh[d]) + om * gd;
       }
+    }
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      TD(d, v) = td[d];
+      GH(d, v) = gh[d];
     }
   }
   double cb[NV], tb[NV];
@@ -372,7 +399,7 @@ template <int P>
 void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
               double* contrib, int* flag, cudaStream_t st) {
   k_adj_wpost<P><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U, adjF, gbar, scr, selfc, flag);
-  k_adj_lsq<P><<<(unsigned)((p.n + 31) / 32), 32, 0, st>>>(p, gbar, selfc, contrib);
+  k_adj_lsq<P><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, gbar, selfc, contrib);
 }
 
 template <int P>
