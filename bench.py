@@ -138,6 +138,11 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# nominal HBM3e bandwidth of a B200 (HGX figure), reported beside the
+# measured copy peak
+NOMINAL_HBM_GBS = 7700.0
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -414,7 +419,8 @@ def main():
                    "scheme": "WENO5+HLLC SSP-RK3" + (" (characteristic variables)" if args.wenwrt == 2 else ""),
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (tables)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": traffic, "traffic_unit": "bytes per launch",
+                     "peak_kind": peak_kind, "nominal_peak": NOMINAL_HBM_GBS, "frac_nominal": achieved / NOMINAL_HBM_GBS,
+                     "traffic": traffic, "traffic_unit": "bytes per launch",
                      "kernel": "k_lsq (stencil least squares)",
                      "bytes_per_cell": bpc, "kernel_ms": lsq_ms,
                      "reconstruction": {"kernels": "k_lsq + k_wpost", "bytes_per_cell": rbpc,

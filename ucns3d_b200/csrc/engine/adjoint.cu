@@ -201,28 +201,28 @@ __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain,
   const int bcode = p.bc[F.c * MF + F.f];
   double sp = 0.0;
   for (int q = 0; q < F.nq; ++q) {
-  double r[4], ul[NV], ur[NV], g[NV];
-  int qq;
-  adj_face_inputs(p, U, lam, F, q, r, ul, ur, g, qq);
-  D L[NV], R[NV], bcs[NV];
+    double r[4], ul[NV], ur[NV], g[NV];
+    int qq;
+    adj_face_inputs(p, U, lam, F, q, r, ul, ur, g, qq);
+    D L[NV], R[NV], bcs[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    L[v] = D(ul[v]);
-    L[v].d[0] = v == k ? 1.0 : 0.0;
-    bcs[v] = D(ur[v]);
-    bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
-  }
-  boundary_ghost(p, bcode, r, L, bcs, R);
-  D a[NV], b[NV], h[NV], fl[NV];
-  rot_f(r, R, b);
-  rot_f(r, L, a);
-  hllc(p.gamma, a, b, h);
-  rot_b(r, h, fl);
-  double s = 0.0;
+    for (int v = 0; v < NV; ++v) {
+      L[v] = D(ul[v]);
+      L[v].d[0] = v == k ? 1.0 : 0.0;
+      bcs[v] = D(ur[v]);
+      bcs[v].d[0] = v + 5 == k ? 1.0 : 0.0;
+    }
+    boundary_ghost(p, bcode, r, L, bcs, R);
+    D a[NV], b[NV], h[NV], fl[NV];
+    rot_f(r, R, b);
+    rot_f(r, L, a);
+    hllc(p.gamma, a, b, h);
+    rot_b(r, h, fl);
+    double s = 0.0;
 #pragma unroll
-  for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
-  if (k < NV) adjF[((F.c * MF + F.f) * F.QS + q) * NV + k] = s;
-  else sp += s;
+    for (int v = 0; v < NV; ++v) s += g[v] * fl[v].d[0];
+    if (k < NV) adjF[((F.c * MF + F.f) * F.QS + q) * NV + k] = s;
+    else sp += s;
   }
   if (k >= NV) pown[(i - nplain) * NV + (k - NV)] = sp;
 }
@@ -846,7 +846,6 @@ int adj_setup(ucg_engine* e) {
   if (cnt[n]) CK(cudaMemcpyAsync(e->adj_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
   CK(cudaMemsetAsync(e->adj_face.p, 0, (size_t)n * MF * NV * 8, e->stream));
   CK(cudaStreamSynchronize(e->stream));
-  e->adj_slots = slots;
   e->adj_ready = true;
   return UCG_OK;
 }

@@ -63,7 +63,6 @@ struct ucg_engine {
   std::vector<int32_t> sten1_h;     // [n][IMAX+1] first stencil (host copy, MUSCL IORDER 1 only)
   // discrete adjoint / tangent (adjoint.cu)
   bool adj_ready = false;
-  int adj_slots = 0;                // contribution slots per cell: self, IMAX stencil cells, 6 face neighbours
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
       adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd;
   // discrete adjoint of the WENO reconstruction (adjoint_weno.cu)

@@ -127,7 +127,6 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
   const T* Mg = (const T*)p.invmat + grp * p.tstride * 32;  // the group's tables
   const int32_t* Si = p.sten + grp * (int64_t)(A * W) * 32 + lane;
   T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  (void)A;
   if (lane == 0) {
     for (int s = 0; s < NSTG; ++s) mbar_init(&bar[s], 1);
     mbar_fence_init();
