@@ -69,7 +69,8 @@ typedef struct ucg_config {
   int32_t wenwrt;      /* 1 conserved-variable WENO, 2 characteristic-variable WENO
                           (WENO only; WENWRT, reconstruct_p.f90:445, 497-758)         */
   int32_t limiter;     /* MUSCL limiter code, 7 = Venkatakrishnan                       */
-  int32_t riemann;     /* 1 = HLLC                                                      */
+  int32_t riemann;     /* iRiemann: 1 HLLC, 2 Rusanov, 9 HLL (flux_p.f90:587-660);
+                          the adjoint covers HLLC                                      */
   int32_t precision;   /* UCG_FP64 or UCG_MIXED                                         */
   int32_t wenoz;       /* WENO-Z weights for CWENO (reconstruct_p.f90:1021-1029)         */
   int32_t ideg;        /* IDEGFREE: basis functions without the mean                    */

@@ -22,8 +22,9 @@
 //                                                    src/reconstruct_p.f90:2286, 1821, 2044, 3421
 //   CHECKSOLX                                        src/reconstruct_p.f90:3245-3406
 //   SOLUTIONTRIAV2                                   src/reconstruct_p.f90:2358
-//   CALCULATE_FLUXESHI_CONVECTIVE + HLLC_RIEMANN_SOLVER + ROTATEF/ROTATEB
-//                                                    src/flux_p.f90:478, riemann.f90:221, grid_t.f90:4217
+//   CALCULATE_FLUXESHI_CONVECTIVE + HLLC / RUSANOV / HLL_RIEMANN_SOLVER + ROTATEF/ROTATEB
+//                                                    src/flux_p.f90:478, riemann.f90:221, 1236, 28,
+//                                                    grid_t.f90:4217
 //   CALCULATE_FLUXESHI_DIFFUSIVE + SUTHERLAND        src/flux_p.f90:1520, flow_operations.f90:2609
 //   BOUNDARYS (inflow/outflow/symmetry/wall)         src/flow_operations.f90:2860-3230
 //   RUNGE_KUTTA3, CALCULATE_CFL                      src/time_p.f90:885-1027, 27-191
@@ -375,6 +376,49 @@ void hllc(double gamma, const double* cl, const double* cr, double* flux) {
     flux[k] = (((1.0 + sg) / 2.0) * (fl[k] + sl * (ls[k] - cl[k]))) + (((1.0 - sg) / 2.0) * (fr[k] + sr * (rs[k] - cr[k])));
 }
 
+// RUSANOV_RIEMANN_SOLVER (riemann.f90:1236-1403) and HLL_RIEMANN_SOLVER
+// (riemann.f90:28-217, Davis wave speeds) in the face frame
+void xflux(double gamma, const double* c, double* f, double& u, double& p) {
+  const double r = c[0];
+  u = c[1] / r;
+  const double v = c[2] / r, w = c[3] / r;
+  p = (gamma - 1.0) * (c[4] - 0.5 * r * (u * u + v * v + w * w));
+  f[0] = r * u;
+  f[1] = (r * (u * u)) + p;
+  f[2] = r * u * v;
+  f[3] = r * u * w;
+  f[4] = u * (c[4] + p);
+}
+void rusanov(double gamma, const double* cl, const double* cr, double* flux) {
+  double fl[5], fr[5], ul, ur, pl, pr;
+  xflux(gamma, cl, fl, ul, pl);
+  xflux(gamma, cr, fr, ur, pr);
+  const double sl = std::fabs(ul) + std::sqrt(gamma * pl / cl[0]);
+  const double sr = std::fabs(ur) + std::sqrt(gamma * pr / cr[0]);
+  const double smax = std::max(std::fabs(sl), std::fabs(sr));
+  for (int k = 0; k < 5; ++k) flux[k] = 0.5 * (fl[k] + fr[k]) - 0.5 * smax * (cr[k] - cl[k]);
+}
+void hll(double gamma, const double* cl, const double* cr, double* flux) {
+  double fl[5], fr[5], ul, ur, pl, pr;
+  xflux(gamma, cl, fl, ul, pl);
+  xflux(gamma, cr, fr, ur, pr);
+  const double ccl = std::sqrt(gamma * pl / cl[0]), ccr = std::sqrt(gamma * pr / cr[0]);
+  const double sl = std::min(ul - ccl, ur - ccr), sr = std::max(ul + ccl, ur + ccr);
+  for (int k = 0; k < 5; ++k) {
+    const double fhll = (sr * fl[k] - sl * fr[k] + (sl * sr * (cr[k] - cl[k]))) / (sr - sl);
+    double f = 0.0;
+    if (sl >= 0.0) f = fl[k];
+    if (sr <= 0.0) f = fr[k];
+    if (sl <= 0.0 && sr >= 0.0) f = fhll;
+    flux[k] = f;
+  }
+}
+void riemann(const ucg_config* cfg, const double* cl, const double* cr, double* flux) {
+  if (cfg->riemann == 2) rusanov(cfg->gamma, cl, cr, flux);
+  else if (cfg->riemann == 9) hll(cfg->gamma, cl, cr, flux);
+  else hllc(cfg->gamma, cl, cr, flux);
+}
+
 // ghost state of a physical boundary face (BOUNDARYS, boundtype 1 = subsonic
 // treatment, src/flow_operations.f90:2860-3230).  cfg->bc_state holds the
 // free-stream primitive state (rho, u, v, w, p) that INFLOW/OUTFLOW return.
@@ -660,7 +704,7 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
         double clr[NV], crr[NV], hf[NV], fl[NV];
         rotf(ang, cr, crr);
         rotf(ang, cl, clr);
-        hllc(x.cfg->gamma, clr, crr, hf);
+        riemann(x.cfg, clr, crr, hf);
         rotb(ang, hf, fl);
         double ws = wq_of(x, c, f, q) * g->face_area[c * F + f];
         for (int v = 0; v < NV; ++v) god[v] = god[v] + (fl[v] * ws);

@@ -100,6 +100,22 @@ def test_characteristic_weno_residual_matches_oracle(name):
     assert np.abs(Rg - Oracle(m, cfg1).residual(U)).max() > 1e-10 * np.abs(Rg).max()
 
 
+@pytest.mark.parametrize("riemann", [2, 9])
+@pytest.mark.parametrize("name", ["weno3_tet", "muscl_bump", "muscl_ns_hex"])
+def test_rusanov_and_hll_match_oracle(name, riemann):
+    """iRiemann 2 (Rusanov) and 9 (HLL) on the same kernels."""
+    m, cfg, U = _setup(name)
+    cfg.riemann = riemann
+    e = Engine(m, cfg)
+    e.set_state(U)
+    Rg = e.call_flux_subroutines_3d()
+    o = Oracle(m, cfg)
+    err = (np.abs(Rg - o.residual(U)) / _flux_scale(o, m, U)).max()
+    print(f"{name} (riemann {riemann}): residual rel err {err:.3e}")
+    assert err < 1e-12
+    e.close()
+
+
 @pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
 def test_characteristic_weno_mixed_close_to_fp64(name):
     m, cfg, U = _setup(name, wenwrt=2)

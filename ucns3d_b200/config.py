@@ -18,11 +18,13 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
                 prandtl: float = 0.72, reynolds: float | None = None, rres: float = 1.0,
                 ufreestream: float = 1.0, pres: float = 1.0, char_length: float = 1.0,
                 lwci: float = 1000.0, wenoz: int = 0, limiter: int = 7,
-                bc_state=(1.0, 0.0, 0.0, 0.0, 1.0), lamx: float = 1.0, wenwrt: int = 1) -> N.UcgConfig:
+                bc_state=(1.0, 0.0, 0.0, 0.0, 1.0), lamx: float = 1.0, wenwrt: int = 1,
+                riemann: int = 1) -> N.UcgConfig:
     """A ucg_config for a prepared mesh.  ``reynolds`` sets VISC for
     Navier-Stokes; ``bc_state`` is the free-stream primitive state used by
     inflow/outflow boundaries; ``wenwrt`` 1 reconstructs the conserved
-    variables, 2 the characteristic variables (WENWRT of UCNS3D.DAT)."""
+    variables, 2 the characteristic variables (WENWRT of UCNS3D.DAT);
+    ``riemann`` 1 HLLC, 2 Rusanov, 9 HLL (iRiemann)."""
     if not getattr(mesh, "prepared", False):
         raise ValueError("mesh must be prepared first")
     cfg = N.UcgConfig()
@@ -30,7 +32,7 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
     cfg.governing = governing
     cfg.wenwrt = wenwrt
     cfg.limiter = limiter
-    cfg.riemann = 1
+    cfg.riemann = riemann
     cfg.precision = precision
     cfg.wenoz = wenoz
     cfg.gamma = gamma

@@ -50,8 +50,8 @@ namespace {
 int adj_check(ucg_engine* e) {
   if (!e) return UCG_EINVAL;
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64))
-    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1), Euler, FP64 form");
+  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64 && c.riemann == 1))
+    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1), HLLC, Euler, FP64 form");
   if (e->QS != 1) return fail(e, UCG_EINVAL, "the adjoint needs one face point per face (IORDER 1)");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   return UCG_OK;
@@ -950,8 +950,9 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
 // form, cells off the MUSCL fall-back.
 int adjw_setup(ucg_engine* e) {
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 3 && c.ees == 0 && c.wenwrt == 1 && c.governing == 2 && c.precision == UCG_FP64))
-    return fail(e, UCG_EINVAL, "the WENO adjoint covers conserved-variable WENO (EES 0), Euler, FP64 form");
+  if (!(c.scheme == 3 && c.ees == 0 && c.wenwrt == 1 && c.governing == 2 && c.precision == UCG_FP64 &&
+        c.riemann == 1))
+    return fail(e, UCG_EINVAL, "the WENO adjoint covers conserved-variable WENO (EES 0), HLLC, Euler, FP64 form");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   if (e->adjw_ready) return UCG_OK;
   const int64_t n = e->n, ngrp = (n + 31) / 32;

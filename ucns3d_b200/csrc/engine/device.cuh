@@ -75,6 +75,7 @@ struct Problem {
   unsigned* health;
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
+  int riemann;   // 1 HLLC, 2 Rusanov, 9 HLL
   double* dt_dev;           // device dt (ucg_step)
 };
 
@@ -281,6 +282,66 @@ __device__ __forceinline__ void char_eigenvectors(double gamma, const double* rl
       EL[(i * 5 + j) * st] = L[i][j];
       ER[(i * 5 + j) * st] = R[i][j];
     }
+}
+
+// Euler flux in the face frame of a conserved state, with its velocity and
+// pressure
+template <typename S>
+__host__ __device__ __forceinline__ void euler_xflux(double gamma, const S* c, S* f, S& u, S& pr) {
+  const S r = c[0], ir = 1.0 / r;
+  u = c[1] * ir;
+  const S v = c[2] * ir, w = c[3] * ir;
+  pr = (gamma - 1.0) * (c[4] - 0.5 * r * (u * u + v * v + w * w));
+  f[0] = r * u;
+  f[1] = r * u * u + pr;
+  f[2] = r * u * v;
+  f[3] = r * u * w;
+  f[4] = u * (c[4] + pr);
+}
+
+// Rusanov flux (RUSANOV_RIEMANN_SOLVER, src/riemann.f90:1236-1403):
+// 0.5 (FL + FR) - 0.5 max(|uL| + cL, |uR| + cR) (UR - UL).
+template <typename S>
+__host__ __device__ __forceinline__ void rusanov(double gamma, const S* cl, const S* cr, S* flux) {
+  S fl[5], fr[5], ul, ur, pl, pr;
+  euler_xflux(gamma, cl, fl, ul, pl);
+  euler_xflux(gamma, cr, fr, ur, pr);
+  const S sl = fabs(ul) + sqrt(gamma * pl / cl[0]), sr = fabs(ur) + sqrt(gamma * pr / cr[0]);
+  const S smax = fmax(fabs(sl), fabs(sr));
+#pragma unroll
+  for (int k = 0; k < 5; ++k) flux[k] = 0.5 * (fl[k] + fr[k]) - 0.5 * smax * (cr[k] - cl[k]);
+}
+
+// HLL flux (HLL_RIEMANN_SOLVER, src/riemann.f90:28-217) with the Davis wave
+// speeds SL = min(uL - cL, uR - cR), SR = max(uL + cL, uR + cR): FL when
+// SL > 0, FR when SR < 0, else (SR FL - SL FR + SL SR (UR - UL)) / (SR - SL).
+template <typename S>
+__host__ __device__ __forceinline__ void hll(double gamma, const S* cl, const S* cr, S* flux) {
+  S fl[5], fr[5], ul, ur, pl, pr;
+  euler_xflux(gamma, cl, fl, ul, pl);
+  euler_xflux(gamma, cr, fr, ur, pr);
+  const S ccl = sqrt(gamma * pl / cl[0]), ccr = sqrt(gamma * pr / cr[0]);
+  const S sl = fmin(ul - ccl, ur - ccr), sr = fmax(ul + ccl, ur + ccr);
+  if (value(sl) <= 0.0 && value(sr) >= 0.0) {
+    const S id = 1.0 / (sr - sl);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) flux[k] = (sr * fl[k] - sl * fr[k] + (sl * sr * (cr[k] - cl[k]))) * id;
+  } else if (value(sr) <= 0.0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) flux[k] = fr[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) flux[k] = fl[k];
+  }
+}
+
+// The face-frame flux of the configured Riemann solver (iRiemann of
+// UCNS3D.DAT, src/flux_p.f90:587-660): 1 HLLC, 2 Rusanov, 9 HLL.
+template <typename S>
+__host__ __device__ __forceinline__ void riemann_flux(int kind, double gamma, const S* cl, const S* cr, S* flux) {
+  if (kind == 2) rusanov(gamma, cl, cr, flux);
+  else if (kind == 9) hll(gamma, cl, cr, flux);
+  else hllc(gamma, cl, cr, flux);
 }
 
 // Venkatakrishnan limiter, SLOPE_LIMITERS case 7 (src/reconstruct_p.f90:3647-3652)

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) k_face(Problem p, const double* __restric
     double a[NV], b[NV], h[NV], fl[NV];
     rot_f(r, cr, b);
     rot_f(r, cl, a);
-    hllc(p.gamma, a, b, h);
+    riemann_flux(p.riemann, p.gamma, a, b, h);
     rot_b(r, h, fl);
     const double ws = face_weight(p, ft, q) * area;
 #pragma unroll
