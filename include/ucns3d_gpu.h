@@ -68,7 +68,9 @@ typedef struct ucg_config {
   int32_t ees;         /* 0 WENO, 5 CWENO (parameters.f90:1340-1372)                    */
   int32_t wenwrt;      /* 1 conserved-variable WENO, 2 characteristic-variable WENO
                           (WENO only; WENWRT, reconstruct_p.f90:445, 497-758)         */
-  int32_t limiter;     /* MUSCL limiter code, 7 = Venkatakrishnan                       */
+  int32_t limiter;     /* MUSCL limiter code (SLOPE_LIMITERS): 1 Barth-Jespersen,
+                          2/3/9 Michalak, 4/8 Venkatakrishnan blended, 5 van Albada,
+                          6 van Leer, 7 Venkatakrishnan; the adjoint covers 7           */
   int32_t riemann;     /* iRiemann: 1 HLLC, 2 Rusanov, 9 HLL (flux_p.f90:587-660);
                           the adjoint covers HLLC                                      */
   int32_t precision;   /* UCG_FP64 or UCG_MIXED                                         */

@@ -18,7 +18,7 @@
 //   compute_gradcharv_smoothindicator + diag_At_B_A  src/reconstruct_p.f90:497-917, 1608-1818
 //   COMPUTE_EIGENVECTORS                             src/flow_operations.f90:3934-3995
 //   CHECKSOL                                         src/reconstruct_p.f90:3126-3242
-//   MUSCL / FIND_BOUNDS / COMPUTE_MUSCL_RECONSTRUCTION / SLOPE_LIMITERS(7)
+//   MUSCL / FIND_BOUNDS / COMPUTE_MUSCL_RECONSTRUCTION / SLOPE_LIMITERS(1-9)
 //                                                    src/reconstruct_p.f90:2286, 1821, 2044, 3421
 //   CHECKSOLX                                        src/reconstruct_p.f90:3245-3406
 //   SOLUTIONTRIAV2                                   src/reconstruct_p.f90:2358
@@ -112,6 +112,37 @@ double venkat(double usol, double u0, double umin, double umax, double minedge, 
                          ((dplus * dplus) + (2.0 * dmin * dmin) + (dmin * dplus) + epsi2));
 }
 
+// SLOPE_LIMITERS (reconstruct_p.f90:3421-3945) for limiter codes 1-9
+double slope_limiter(int kind, double usol, double u0, double umin, double umax, double minedge, double kappa) {
+  if (kind == 7) return venkat(usol, u0, umin, umax, minedge, kappa);
+  const double d2 = usol - u0;
+  if (std::fabs(d2) <= 0.0) return 1.0;
+  double psi;
+  if (kind == 4 || kind == 8) {
+    psi = venkat(usol, u0, umin, umax, minedge, kappa);
+  } else {
+    const double sfd = ((d2 > 0.0) ? (umax - u0) : (umin - u0)) / d2;
+    if (kind == 1) psi = std::min(1.0, sfd);
+    else if (kind == 5) psi = (sfd * sfd + sfd) / (sfd * sfd + 1.0);
+    else if (kind == 6) psi = 2.0 * sfd / (sfd + 1.0);
+    else psi = (sfd < 1.5) ? -((4.0 / 27.0) * std::pow(sfd, 3)) + sfd : 1.0;
+  }
+  if (kind == 2 || kind == 3 || kind == 9 || kind == 4 || kind == 8) {
+    const double delu = umax - umin, e3 = std::pow(kappa * minedge, 3);
+    double sig;
+    if (delu * delu <= e3) {
+      sig = 1.0;
+    } else if (delu * delu < 2.0 * e3) {
+      const double y = (delu * delu - e3) / e3;
+      sig = (2.0 * std::pow(y, 3)) - (3.0 * std::pow(y, 2)) + 1.0;
+    } else {
+      sig = 0.0;
+    }
+    psi = sig + (1.0 - sig) * psi;
+  }
+  return psi;
+}
+
 // MUSCL on one cell: ULEFT from the central-stencil polynomial G0 [ideg][5]
 void muscl_cell(const Ctx& x, int64_t c, const double* U, const double* G0, double* ul /*[F][Q][5]*/) {
   const ucg_geometry* g = x.g;
@@ -137,7 +168,8 @@ void muscl_cell(const Ctx& x, int64_t c, const double* U, const double* G0, doub
         double res = 0.0;
         for (int d = 0; d < ideg; ++d) res += b[d] * G0[d * NV + v];
         usol[f][q][v] = u0[v] + res;
-        double psi = venkat(usol[f][q][v], u0[v], umin[v], umax[v], g->minedge[c], x.cfg->kappa_ven);
+        double psi = slope_limiter(x.cfg->limiter, usol[f][q][v], u0[v], umin[v], umax[v], g->minedge[c],
+                                   x.cfg->kappa_ven);
         slope[v] = std::min(slope[v], psi);
       }
     }

@@ -116,6 +116,23 @@ def test_rusanov_and_hll_match_oracle(name, riemann):
     e.close()
 
 
+@pytest.mark.parametrize("limiter", [1, 2, 4, 5, 6, 9])
+@pytest.mark.parametrize("name", ["muscl_euler_tet", "muscl_bump", "muscl_p2_hex"])
+def test_slope_limiters_match_oracle(name, limiter):
+    """SLOPE_LIMITERS codes 1-9 in the MUSCL kernels (IORDER 1 and the
+    high-order MUSCL of k_wpost)."""
+    m, cfg, U = _setup(name)
+    cfg.limiter = limiter
+    e = Engine(m, cfg)
+    e.set_state(U)
+    Rg = e.call_flux_subroutines_3d()
+    o = Oracle(m, cfg)
+    err = (np.abs(Rg - o.residual(U)) / _flux_scale(o, m, U)).max()
+    print(f"{name} (limiter {limiter}): residual rel err {err:.3e}")
+    assert err < 1e-12
+    e.close()
+
+
 @pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
 def test_characteristic_weno_mixed_close_to_fp64(name):
     m, cfg, U = _setup(name, wenwrt=2)

@@ -50,8 +50,9 @@ namespace {
 int adj_check(ucg_engine* e) {
   if (!e) return UCG_EINVAL;
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64 && c.riemann == 1))
-    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1), HLLC, Euler, FP64 form");
+  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64 && c.riemann == 1 &&
+        c.limiter == 7))
+    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1, Venkatakrishnan), HLLC, Euler, FP64 form");
   if (e->QS != 1) return fail(e, UCG_EINVAL, "the adjoint needs one face point per face (IORDER 1)");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   return UCG_OK;

@@ -76,6 +76,7 @@ struct Problem {
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
   int riemann;   // 1 HLLC, 2 Rusanov, 9 HLL
+  int limiter;   // SLOPE_LIMITERS code (7 Venkatakrishnan)
   double* dt_dev;           // device dt (ucg_step)
 };
 
@@ -352,6 +353,42 @@ __host__ __device__ __forceinline__ S venkat(S d2, S umin0, S umax0, double epsi
   S dplus = value(d2) > 0.0 ? umax0 : umin0;
   return (1.0 / dmin) * (((dplus * dplus + epsi2) * dmin + 2.0 * (dmin * dmin) * dplus) /
                          (dplus * dplus + 2.0 * dmin * dmin + dmin * dplus + epsi2));
+}
+
+// SLOPE_LIMITERS (src/reconstruct_p.f90:3421-3945), the limiter code of
+// UCNS3D.DAT: 1 Barth-Jespersen, 2/3/9 Michalak's polynomial, 4/8
+// Venkatakrishnan, 5 van Albada, 6 van Leer, each with sfd = (bound - mean)
+// / d2; 2/3/9 and 4/8 are blended towards 1 where the cell's range is below
+// (KAPPA_VEN MINEDGE)^3 (e3 here), 7 is plain Venkatakrishnan.
+template <typename S>
+__host__ __device__ __forceinline__ S slope_limiter(int kind, S d2, S lo, S hi, double e3) {
+  if (kind == 7) return venkat(d2, lo, hi, e3);
+  if (fabs(value(d2)) <= 0.0) return S(1.0);
+  S psi;
+  const bool blend = kind == 2 || kind == 3 || kind == 9 || kind == 4 || kind == 8;
+  if (kind == 4 || kind == 8) {
+    psi = venkat(d2, lo, hi, e3);
+  } else {
+    const S sfd = (value(d2) > 0.0 ? hi : lo) / d2;
+    if (kind == 1) psi = fmin(S(1.0), sfd);
+    else if (kind == 5) psi = (sfd * sfd + sfd) / (sfd * sfd + 1.0);
+    else if (kind == 6) psi = 2.0 * sfd / (sfd + 1.0);
+    else psi = value(sfd) < 1.5 ? -((4.0 / 27.0) * (sfd * sfd * sfd)) + sfd : S(1.0);
+  }
+  if (blend) {
+    const S du = hi - lo, du2 = du * du;
+    S sig;
+    if (value(du2) <= e3) {
+      sig = S(1.0);
+    } else if (value(du2) < 2.0 * e3) {
+      const S y = (du2 - e3) / e3;
+      sig = (2.0 * (y * y * y)) - (3.0 * (y * y)) + 1.0;
+    } else {
+      sig = S(0.0);
+    }
+    psi = sig + (1.0 - sig) * psi;
+  }
+  return psi;
 }
 
 // CHECKSOL / CHECKSOLX jump test of one face value against the cell mean

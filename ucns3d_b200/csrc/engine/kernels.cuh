@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
   for (int v = 0; v < NV; ++v) slope[v] = TOLBIG;
   for (int f = 0; f < nf; ++f)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) slope[v] = fmin(slope[v], venkat(face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2));
+    for (int v = 0; v < NV; ++v)
+      slope[v] = fmin(slope[v], slope_limiter(p.limiter, face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2));
   // limited face values and CHECKSOLX
   bool first = false;
   for (int f = 0; f < nf; ++f) {

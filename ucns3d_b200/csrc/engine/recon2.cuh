@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
             for (int d = 0; d < ID; ++d) r += m[d] * g0[d][k];
             r = r - cb[k];
             const double dd = (u0[v] + (double)r) - u0[v];
-            if (pass == 0) slope[k] = fmin(slope[k], venkat(dd, lo[v], hi[v], epsi2));
+            if (pass == 0) slope[k] = fmin(slope[k], slope_limiter(p.limiter, dd, lo[v], hi[v], epsi2));
             else o[v] = T((double)T(dd) * slope[k]);
           }
         }
