@@ -445,6 +445,45 @@ void hll(double gamma, const double* cl, const double* cr, double* flux) {
     flux[k] = f;
   }
 }
+// ROE_RIEMANN_SOLVER (riemann.f90:433-632): global frame, face normal n,
+// entropy fix of the acoustic waves (width 0.2)
+void roe(double gamma, const double* cl, const double* cr, const double* n, double* flux) {
+  const double nx = n[0], ny = n[1], nz = n[2];
+  const double rhoL = cl[0], uL = cl[1] / rhoL, vL = cl[2] / rhoL, wL = cl[3] / rhoL;
+  const double pL = (gamma - 1.0) * (cl[4] - 0.5 * rhoL * (uL * uL + vL * vL + wL * wL));
+  const double rhoR = cr[0], uR = cr[1] / rhoR, vR = cr[2] / rhoR, wR = cr[3] / rhoR;
+  const double pR = (gamma - 1.0) * (cr[4] - 0.5 * rhoR * (uR * uR + vR * vR + wR * wR));
+  const double qnL = uL * nx + vL * ny + wL * nz, qnR = uR * nx + vR * ny + wR * nz;
+  const double aL = std::sqrt(gamma * pL / rhoL), aR = std::sqrt(gamma * pR / rhoR);
+  const double HL = aL * aL / (gamma - 1.0) + 0.5 * (uL * uL + vL * vL + wL * wL);
+  const double HR = aR * aR / (gamma - 1.0) + 0.5 * (uR * uR + vR * vR + wR * wR);
+  const double RT = std::sqrt(rhoR / rhoL);
+  const double rho = RT * rhoL, u = (uL + RT * uR) / (1.0 + RT), v = (vL + RT * vR) / (1.0 + RT),
+               w = (wL + RT * wR) / (1.0 + RT), H = (HL + RT * HR) / (1.0 + RT);
+  const double a = std::sqrt((gamma - 1.0) * (H - 0.5 * (u * u + v * v + w * w)));
+  const double qn = u * nx + v * ny + w * nz;
+  const double drho = rhoR - rhoL, dp = pR - pL, dqn = qnR - qnL;
+  const double LdU[4] = {(dp - rho * a * dqn) / (2.0 * a * a), drho - dp / (a * a), (dp + rho * a * dqn) / (2.0 * a * a), rho};
+  double ws[4] = {std::fabs(qn - a), std::fabs(qn), std::fabs(qn + a), std::fabs(qn)};
+  if (ws[0] < 0.2) ws[0] = 0.5 * (ws[0] * ws[0] / 0.2 + 0.2);
+  if (ws[2] < 0.2) ws[2] = 0.5 * (ws[2] * ws[2] / 0.2 + 0.2);
+  const double du = uR - uL, dv = vR - vL, dw = wR - wL;
+  const double R[5][4] = {{1.0, 1.0, 1.0, 0.0},
+                          {u - a * nx, u, u + a * nx, du - dqn * nx},
+                          {v - a * ny, v, v + a * ny, dv - dqn * ny},
+                          {w - a * nz, w, w + a * nz, dw - dqn * nz},
+                          {H - a * qn, 0.5 * (u * u + v * v + w * w), H + a * qn, u * du + v * dv + w * dw - qn * dqn}};
+  const double fL[5] = {rhoL * qnL, rhoL * qnL * uL + pL * nx, rhoL * qnL * vL + pL * ny, rhoL * qnL * wL + pL * nz,
+                        rhoL * qnL * HL};
+  const double fR[5] = {rhoR * qnR, rhoR * qnR * uR + pR * nx, rhoR * qnR * vR + pR * ny, rhoR * qnR * wR + pR * nz,
+                        rhoR * qnR * HR};
+  for (int k = 0; k < 5; ++k) {
+    const double diss = ws[0] * LdU[0] * R[k][0] + ws[1] * LdU[1] * R[k][1] + ws[2] * LdU[2] * R[k][2] +
+                        ws[3] * LdU[3] * R[k][3];
+    flux[k] = 0.5 * (fL[k] + fR[k] - diss);
+  }
+}
+
 void riemann(const ucg_config* cfg, const double* cl, const double* cr, double* flux) {
   if (cfg->riemann == 2) rusanov(cfg->gamma, cl, cr, flux);
   else if (cfg->riemann == 9) hll(cfg->gamma, cl, cr, flux);
@@ -734,10 +773,15 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
           cr = crb;
         }
         double clr[NV], crr[NV], hf[NV], fl[NV];
-        rotf(ang, cr, crr);
-        rotf(ang, cl, clr);
-        riemann(x.cfg, clr, crr, hf);
-        rotb(ang, hf, fl);
+        if (x.cfg->riemann == 3) {  // Roe: global frame along the face normal
+          const double nrm[3] = {ang[0] * ang[3], ang[1] * ang[3], ang[2]};
+          roe(x.cfg->gamma, cl, cr, nrm, fl);
+        } else {
+          rotf(ang, cr, crr);
+          rotf(ang, cl, clr);
+          riemann(x.cfg, clr, crr, hf);
+          rotb(ang, hf, fl);
+        }
         double ws = wq_of(x, c, f, q) * g->face_area[c * F + f];
         for (int v = 0; v < NV; ++v) god[v] = god[v] + (fl[v] * ws);
       }

@@ -75,7 +75,7 @@ struct Problem {
   unsigned* health;
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
-  int riemann;   // 1 HLLC, 2 Rusanov, 9 HLL
+  int riemann;   // 1 HLLC, 2 Rusanov, 3 Roe, 9 HLL
   int limiter;   // SLOPE_LIMITERS code (7 Venkatakrishnan)
   double* dt_dev;           // device dt (ucg_step)
 };
@@ -333,6 +333,44 @@ __host__ __device__ __forceinline__ void hll(double gamma, const S* cl, const S*
   } else {
 #pragma unroll
     for (int k = 0; k < 5; ++k) flux[k] = fl[k];
+  }
+}
+
+// Roe flux with the entropy fix of the acoustic waves (ROE_RIEMANN_SOLVER,
+// src/riemann.f90:433-632), in the global frame along the face normal n.
+template <typename S>
+__host__ __device__ __forceinline__ void roe(double gamma, const S* cl, const S* cr, const double* n, S* flux) {
+  const double nx = n[0], ny = n[1], nz = n[2];
+  const S rL = cl[0], uL = cl[1] / rL, vL = cl[2] / rL, wL = cl[3] / rL;
+  const S pL = (gamma - 1.0) * (cl[4] - 0.5 * rL * (uL * uL + vL * vL + wL * wL));
+  const S rR = cr[0], uR = cr[1] / rR, vR = cr[2] / rR, wR = cr[3] / rR;
+  const S pR = (gamma - 1.0) * (cr[4] - 0.5 * rR * (uR * uR + vR * vR + wR * wR));
+  const S qnL = uL * nx + vL * ny + wL * nz, qnR = uR * nx + vR * ny + wR * nz;
+  const S aL = sqrt(gamma * pL / rL), aR = sqrt(gamma * pR / rR);
+  const S HL = aL * aL / (gamma - 1.0) + 0.5 * (uL * uL + vL * vL + wL * wL);
+  const S HR = aR * aR / (gamma - 1.0) + 0.5 * (uR * uR + vR * vR + wR * wR);
+  const S RT = sqrt(rR / rL), iRT = 1.0 / (1.0 + RT);
+  const S rho = RT * rL, u = (uL + RT * uR) * iRT, v = (vL + RT * vR) * iRT, w = (wL + RT * wR) * iRT;
+  const S H = (HL + RT * HR) * iRT;
+  const S a = sqrt((gamma - 1.0) * (H - 0.5 * (u * u + v * v + w * w)));
+  const S qn = u * nx + v * ny + w * nz;
+  const S drho = rR - rL, dp = pR - pL, dqn = qnR - qnL;
+  const S ia2 = 1.0 / (a * a);
+  const S L1 = (dp - rho * a * dqn) * (0.5 * ia2), L2 = drho - dp * ia2, L3 = (dp + rho * a * dqn) * (0.5 * ia2);
+  S ws1 = fabs(qn - a), ws2 = fabs(qn), ws3 = fabs(qn + a);
+  if (value(ws1) < 0.2) ws1 = 0.5 * (ws1 * ws1 / 0.2 + 0.2);
+  if (value(ws3) < 0.2) ws3 = 0.5 * (ws3 * ws3 / 0.2 + 0.2);
+  const S du = uR - uL, dv = vR - vL, dw = wR - wL;
+  const S R1[5] = {S(1.0), u - a * nx, v - a * ny, w - a * nz, H - a * qn};
+  const S R2[5] = {S(1.0), u, v, w, 0.5 * (u * u + v * v + w * w)};
+  const S R3[5] = {S(1.0), u + a * nx, v + a * ny, w + a * nz, H + a * qn};
+  const S R4[5] = {S(0.0), du - dqn * nx, dv - dqn * ny, dw - dqn * nz, u * du + v * dv + w * dw - qn * dqn};
+  const S fL[5] = {rL * qnL, rL * qnL * uL + pL * nx, rL * qnL * vL + pL * ny, rL * qnL * wL + pL * nz, rL * qnL * HL};
+  const S fR[5] = {rR * qnR, rR * qnR * uR + pR * nx, rR * qnR * vR + pR * ny, rR * qnR * wR + pR * nz, rR * qnR * HR};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const S diss = ws1 * L1 * R1[k] + ws2 * L2 * R2[k] + ws3 * L3 * R3[k] + ws2 * rho * R4[k];
+    flux[k] = 0.5 * (fL[k] + fR[k] - diss);
   }
 }
 

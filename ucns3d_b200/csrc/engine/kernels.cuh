@@ -178,11 +178,17 @@ __global__ void __launch_bounds__(256) k_face(Problem p, const double* __restric
     } else {
       boundary_ghost(p, p.bc[c * MF + f], r, cl, cr);
     }
-    double a[NV], b[NV], h[NV], fl[NV];
-    rot_f(r, cr, b);
-    rot_f(r, cl, a);
-    riemann_flux(p.riemann, p.gamma, a, b, h);
-    rot_b(r, h, fl);
+    double fl[NV];
+    if (p.riemann == 3) {  // Roe: global frame along the face normal
+      const double nrm[3] = {r[0] * r[3], r[1] * r[3], r[2]};
+      roe(p.gamma, cl, cr, nrm, fl);
+    } else {
+      double a[NV], b[NV], h[NV];
+      rot_f(r, cr, b);
+      rot_f(r, cl, a);
+      riemann_flux(p.riemann, p.gamma, a, b, h);
+      rot_b(r, h, fl);
+    }
     const double ws = face_weight(p, ft, q) * area;
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
