@@ -135,12 +135,13 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
 // MODE 0: write the residual; MODE 1/2/3: RK stage 1/2/3.
 // ======================================================================
 // One thread per owned face (the cell with the smaller index, or the only
-// cell of a boundary face): HLLC and viscous fluxes over the face's points,
+// cell of a boundary face): the Riemann flux RK (iRiemann: 1 HLLC, 2
+// Rusanov, 3 Roe, 9 HLL) and viscous fluxes over the face's points,
 // weighted by w_q * area.  The neighbour's face gets the negated sums: HLLC
 // and the viscous flux are antisymmetric under swapping the two states and
 // flipping the normal, so each interior face is evaluated once instead of
 // twice as in the reference's per-cell loop.
-template <typename T, bool NS>
+template <typename T, bool NS, int RK>
 __global__ void __launch_bounds__(256) k_face(Problem p, const double* __restrict__ Uc) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
@@ -179,14 +180,14 @@ __global__ void __launch_bounds__(256) k_face(Problem p, const double* __restric
       boundary_ghost(p, p.bc[c * MF + f], r, cl, cr);
     }
     double fl[NV];
-    if (p.riemann == 3) {  // Roe: global frame along the face normal
+    if constexpr (RK == 3) {  // Roe: global frame along the face normal
       const double nrm[3] = {r[0] * r[3], r[1] * r[3], r[2]};
       roe(p.gamma, cl, cr, nrm, fl);
     } else {
       double a[NV], b[NV], h[NV];
       rot_f(r, cr, b);
       rot_f(r, cl, a);
-      riemann_flux(p.riemann, p.gamma, a, b, h);
+      riemann_flux(RK, p.gamma, a, b, h);
       rot_b(r, h, fl);
     }
     const double ws = face_weight(p, ft, q) * area;
