@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
 #define UCG_WV_IS_F 5
 #endif
 #ifndef UCG_WV_FACE_F
-#define UCG_WV_FACE_F 3
+#define UCG_WV_FACE_F 5
 #endif
 #ifndef UCG_WV_FALL_F
 #define UCG_WV_FALL_F 1
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
 #define UCG_WV_IS_D 2
 #endif
 #ifndef UCG_WV_FACE_D
-#define UCG_WV_FACE_D 2
+#define UCG_WV_FACE_D 3
 #endif
 #ifndef UCG_WV_FALL_D
 #define UCG_WV_FALL_D 1
