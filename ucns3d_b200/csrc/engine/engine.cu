@@ -170,12 +170,13 @@ int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
 template <typename T, bool NS>
 int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
                   double dt) {
-  const unsigned fb = (unsigned)((e->nown + 255) / 256);
+  constexpr int FB = UCG_FACE_BLOCK;
+  const unsigned fb = (unsigned)((e->nown + FB - 1) / FB);
   switch (e->cfg.riemann) {  // the Riemann solver is a template argument of the face kernel
-    case 2: k_face<T, NS, 2><<<fb, 256, 0, e->stream>>>(p, Uc); break;
-    case 3: k_face<T, NS, 3><<<fb, 256, 0, e->stream>>>(p, Uc); break;
-    case 9: k_face<T, NS, 9><<<fb, 256, 0, e->stream>>>(p, Uc); break;
-    default: k_face<T, NS, 1><<<fb, 256, 0, e->stream>>>(p, Uc); break;
+    case 2: k_face<T, NS, 2><<<fb, FB, 0, e->stream>>>(p, Uc); break;
+    case 3: k_face<T, NS, 3><<<fb, FB, 0, e->stream>>>(p, Uc); break;
+    case 9: k_face<T, NS, 9><<<fb, FB, 0, e->stream>>>(p, Uc); break;
+    default: k_face<T, NS, 1><<<fb, FB, 0, e->stream>>>(p, Uc); break;
   }
   unsigned blocks = (unsigned)((e->n + 255) / 256);
   switch (mode) {
