@@ -192,6 +192,18 @@ def recon_bytes_per_cell(cfg):
     return b
 
 
+L2_BYTES = 126 * 2 ** 20
+
+
+def scheme_label(case, wenwrt):
+    """e.g. 'WENO5+HLLC SSP-RK3, Euler' from the case's metadata."""
+    m = case.meta
+    name = {"WENO": f"WENO{m.get('order', '')}", "CWENO": f"CWENO{m.get('order', '')}",
+            "MUSCL": "MUSCL"}.get(m.get("scheme"), str(m.get("scheme")))
+    s = f"{name}+HLLC SSP-RK3, {m.get('equations', '')}"
+    return s + (" (characteristic variables)" if wenwrt == 2 else "")
+
+
 def make_case(args, precision):
     from ucns3d_b200 import cases
     fn = cases.CASES[args.case]
@@ -405,6 +417,7 @@ def main():
     # roofline of the dominant kernel (k_lsq), achieved from its CUDA-event
     # duration on the engine stream; the whole reconstruction beside it
     bpc = lsq_bytes_per_cell(cfg32)
+    table_bytes = bpc * ncells
     lsq_ms = r32["kern"]["lsq"]
     achieved = bpc * ncells / (lsq_ms / 1000.0) / 1e9
     rbpc = recon_bytes_per_cell(cfg32)
@@ -416,8 +429,10 @@ def main():
         "dtype": "mixed: f32 tables/reconstruction, f64 flux/accumulate/update",
         "data": "synthetic (seeded mesh and analytic initial condition)",
         "config": {"workload": args.case, "cells": ncells, "n": args.n,
-                   "scheme": "WENO5+HLLC SSP-RK3" + (" (characteristic variables)" if args.wenwrt == 2 else ""),
-                   "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (tables)"},
+                   "scheme": scheme_label(c32, args.wenwrt),
+                   "parallelism": f"replicas x{ws}",
+                   "l2": ("inputs larger than L2 (tables)" if table_bytes > L2_BYTES
+                          else "tables smaller than L2: not an HBM-roofline case")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "nominal_peak": NOMINAL_HBM_GBS, "frac_nominal": achieved / NOMINAL_HBM_GBS,
                      "traffic": traffic, "traffic_unit": "bytes per launch",

@@ -770,33 +770,51 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
 // Viscous gradients for WENO/CWENO + Navier-Stokes: LSQ on (T,u,v,w) with
 // stencil 1 (gradients.f90:502-706), then face gradients (SOLUTIONTRIAV2).
 // ======================================================================
+// One lane per cell: each stencil member's primitive state is formed once
+// and its differences (T, u, v, w) are accumulated for VP variables per pass
+// (all four when the FP64 accumulators fit), reading the interleaved table
+// rows of stencil 1 with coalesced loads.  Same products and order per
+// (row, variable) as one thread per variable.
 template <int P, typename T>
-__global__ void k_visc_lsq(Problem p, const double* __restrict__ U) {
+__global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n * 4) return;
-  const int64_t c = i >> 2;
-  const int var = (int)(i & 3);
+  constexpr int VP = ID * 4 <= 80 ? 4 : 2;  // variables per pass
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
   const int IM = p.imax, W = IM + 1;
   double pm[NV];
   cons2prim(p.gamma, U + c * NV, pm);
-  const double s0 = var == 0 ? pm[4] / (pm[0] * p.r_gas) : pm[var];
+  const double s0[4] = {pm[4] / (pm[0] * p.r_gas), pm[1], pm[2], pm[3]};
   const int64_t grp = c >> 5;
   const int lane = (int)(c & 31);
   const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
   const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
-  double acc[ID];
+#pragma unroll 1
+  for (int v0 = 0; v0 < 4; v0 += VP) {
+    double acc[ID][VP];
 #pragma unroll
-  for (int d = 0; d < ID; ++d) acc[d] = 0.0;
-  for (int k = 0; k < IM; ++k) {
-    double py[NV];
-    cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
-    double ds = (var == 0 ? py[4] / (py[0] * p.r_gas) : py[var]) - s0;
+    for (int d = 0; d < ID; ++d)
 #pragma unroll
-    for (int d = 0; d < ID; ++d) acc[d] += (double)M[(k * ID + d) * 32] * ds;
+      for (int j = 0; j < VP; ++j) acc[d][j] = 0.0;
+    for (int k = 0; k < IM; ++k) {
+      double py[NV];
+      cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
+      const double sy[4] = {py[4] / (py[0] * p.r_gas), py[1], py[2], py[3]};
+      double ds[VP];
+#pragma unroll
+      for (int j = 0; j < VP; ++j) ds[j] = sy[v0 + j] - s0[v0 + j];
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        const double m = (double)M[(k * ID + d) * 32];
+#pragma unroll
+        for (int j = 0; j < VP; ++j) acc[d][j] += m * ds[j];
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < ID; ++d)
+#pragma unroll
+      for (int j = 0; j < VP; ++j) p.gv[(c * ID + d) * 4 + v0 + j] = acc[d][j];
   }
-#pragma unroll
-  for (int d = 0; d < ID; ++d) p.gv[(c * ID + d) * 4 + var] = acc[d];
 }
 
 template <int P, typename T>
@@ -873,7 +891,7 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   }
   *launches += 2;
   if (ns) {
-    k_visc_lsq<P, T><<<(unsigned)((p.n * 4 + 127) / 128), 128, 0, st>>>(p, U);
+    k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
     const int64_t nf = p.n * MF * QS;
     k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, st>>>(p);
     *launches += 2;
