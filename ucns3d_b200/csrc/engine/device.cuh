@@ -64,6 +64,7 @@ struct Problem {
   int i2off;
   // scratch
   void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the stencils
+  double* qbuf;             // characteristic WENO: G_l^T S G_l per stencil, 15 values, interleaved
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
   double* gv;               // [n][ideg][4]  viscous LSQ coefficients

@@ -125,6 +125,7 @@ Problem make_problem(ucg_engine* e) {
     p.soff[k] = e->layout.soff[k];
   }
   p.gbuf = e->gbuf.p;
+  p.qbuf = (double*)e->qbuf.p;
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.gv = (double*)e->gv.p;
@@ -319,6 +320,8 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   const int64_t ngrp = (n + 31) / 32;
   if (!(c.scheme == 2 && c.iorder == 1))
     rc = rc ? rc : alloc(e, e->gbuf, (size_t)ngrp * 32 * c.admis_max * c.ideg * NV * T);
+  if (c.wenwrt == 2)  // characteristic WENO: G^T S G of every stencil (15 values)
+    rc = rc ? rc : alloc(e, e->qbuf, (size_t)ngrp * 32 * c.admis_max * 15 * 8);
   if (c.governing == 1) {
     rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
     rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
@@ -347,7 +350,8 @@ void ucg_destroy(ucg_engine* e) {
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
-                   &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf};
+                   &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
+                   &e->qbuf};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);

@@ -295,6 +295,40 @@ __device__ __forceinline__ void quad_form(const T* __restrict__ P, const T (&g)[
   }
 }
 
+// A[u][w] += sum_d g[d][u] * sum_{e>=d} P_de g[e][w] over d, e < nd (P the
+// packed triangle as in quad_form); sym(A) = g^T S g for every pair of
+// columns, A[u][u] the quadratic form of column u.
+template <int NMAX, int VG, typename T>
+__device__ __forceinline__ void sym_form(const T* __restrict__ P, const T (&g)[NMAX][VG], int nd, T (&A)[VG][VG]) {
+  constexpr int VEC = Vec<T>::N;
+  int rs = 0;
+#pragma unroll
+  for (int d = 0; d < NMAX; ++d) {
+    if (d < nd) {
+      T t[VG];
+#pragma unroll
+      for (int k = 0; k < VG; ++k) t[k] = T(0);
+#pragma unroll
+      for (int q = 0; q < (NMAX - d + VEC - 1) / VEC; ++q)
+        if (d + q * VEC < nd) {
+          T s[VEC];
+          ldv(P + (int64_t)(rs + q) * 32 * VEC, s);
+#pragma unroll
+          for (int i = 0; i < VEC; ++i)
+            if (d + q * VEC + i < NMAX)
+#pragma unroll
+              for (int k = 0; k < VG; ++k) t[k] += s[i] * g[d + q * VEC + i][k];
+        }
+      rs += (nd - d + VEC - 1) / VEC;
+#pragma unroll
+      for (int u = 0; u < VG; ++u)
+#pragma unroll
+        for (int w = 0; w < VG; ++w) A[u][w] += g[d][u] * t[w];
+      asm volatile("" ::: "memory");
+    }
+  }
+}
+
 // k_wpost: one lane per cell, no block barriers.  Indicators and weights of
 // CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), the combined
 // polynomial, its face values and CHECKSOL; flagged cells (and every cell of
@@ -519,7 +553,9 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
     // face frame; stencil polynomials projected on the left eigenvectors
     // (global-frame conserved variables, as the reference projects them);
     // indicators and weights per characteristic variable; the face's
-    // polynomial back-projected.  With M_ll = ER diag(w_ll) EL the combined
+    // polynomial back-projected.  The indicator of the projection W = G EL^T
+    // is EL_k^T (G^T S G) EL_k, so G^T S G is formed once per stencil and
+    // each face only applies its eigenvectors.  With M_ll = ER diag(w_ll) EL the combined
     // conserved polynomial is sum_ll M_ll G_ll (rows d >= 1) and its mean
     // sum_ll M_ll u0, formed in FP64.
     const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
@@ -545,6 +581,60 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
 #pragma unroll
             for (int u = 0; u < NV; ++u) g3[d][u] = g3[d][u] + T(lk) * G(l2, d, u);
     };
+    // Q_l = G_l^T S G_l (symmetric 5x5, upper triangle row by row) once per
+    // cell: the face-independent part of the characteristic indicators
+    double* Qc = p.qbuf + grp * (int64_t)(A * 15) * 32 + lane;
+#pragma unroll 1
+    for (int ll = 0; ll < adm; ++ll) {
+      const bool low = cw && ll > 0;
+      T g3[L2][NV];
+      lower_sum(g3);
+      auto store = [&](int u, int w, double x) {
+        Qc[(int64_t)(ll * 15 + (u * (2 * NV - u + 1)) / 2 + (w - u)) * 32] = x;
+      };
+      auto forms = [&](auto& g, const T* Pl, int nd) {
+        constexpr int ND = sizeof(g) / sizeof(g[0]);
+        constexpr int VG = sizeof(g[0]) / sizeof(T);
+        if constexpr (VG == NV) {  // all five variables at once
+#pragma unroll
+          for (int d = 0; d < ND; ++d)
+#pragma unroll
+            for (int u = 0; u < NV; ++u) g[d][u] = d < nd ? Gp(ll, d, u, g3) : T(0);
+          T a[NV][NV];
+#pragma unroll
+          for (int u = 0; u < NV; ++u)
+#pragma unroll
+            for (int w = 0; w < NV; ++w) a[u][w] = T(0);
+          sym_form<ND, NV>(Pl, g, nd, a);
+#pragma unroll
+          for (int u = 0; u < NV; ++u)
+#pragma unroll
+            for (int w = u; w < NV; ++w) store(u, w, u == w ? (double)a[u][u] : 0.5 * ((double)a[u][w] + (double)a[w][u]));
+        } else {  // pairs of variables
+#pragma unroll 1
+          for (int u = 0; u < NV; ++u)
+#pragma unroll 1
+            for (int w = u; w < NV; ++w) {
+#pragma unroll
+              for (int d = 0; d < ND; ++d) {
+                g[d][0] = d < nd ? Gp(ll, d, u, g3) : T(0);
+                g[d][1] = d < nd ? Gp(ll, d, w, g3) : T(0);
+              }
+              T a[2][2] = {{T(0), T(0)}, {T(0), T(0)}};
+              sym_form<ND, 2>(Pl, g, nd, a);
+              store(u, w, u == w ? (double)a[0][0] : 0.5 * ((double)a[0][1] + (double)a[1][0]));
+            }
+        }
+      };
+      constexpr int QV = sizeof(T) == 4 ? NV : 2;
+      if (low) {
+        T g[L2][QV];
+        forms(g, Pc + (int64_t)(p.i2off / VEC) * 32 * VEC, ID2);
+      } else {
+        T g[ID][QV];
+        forms(g, Pc, ID);
+      }
+    }
     bool flag = false;
     for (int f = 0; f < nf; ++f) {
       double r[4], ur[NV];
@@ -563,46 +653,24 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
         rot_f(r, ur, rr);
         char_eigenvectors(p.gamma, rl, rr, EL, ER, BT);
       }
-      // indicators of the projected polynomials
+      // indicators of the projected polynomials: IS_l[k] = EL_k^T Q_l EL_k
 #pragma unroll 1
       for (int ll = 0; ll < adm; ++ll) {
-        const bool low = cw && ll > 0;
+        double q[15];
+#pragma unroll
+        for (int j = 0; j < 15; ++j) q[j] = Qc[(int64_t)(ll * 15 + j) * 32];
 #pragma unroll 1
-        for (int k0 = 0; k0 < NV; k0 += VI) {
-          T is[VI];
+        for (int k = 0; k < NV; ++k) {
+          double l[NV];
 #pragma unroll
-          for (int k = 0; k < VI; ++k) is[k] = T(0);
-          T g3[L2][NV];
-          lower_sum(g3);
-          auto project = [&](auto& g, int nd) {
-            constexpr int ND = sizeof(g) / sizeof(g[0]);
+          for (int u = 0; u < NV; ++u) l[u] = EL[(k * NV + u) * BT];
+          double is = 0.0;
+          int j = 0;
 #pragma unroll
-            for (int d = 0; d < ND; ++d) {
-              T gu[NV];
+          for (int u = 0; u < NV; ++u)
 #pragma unroll
-              for (int u = 0; u < NV; ++u) gu[u] = d < nd ? Gp(ll, d, u, g3) : T(0);
-#pragma unroll
-              for (int k = 0; k < VI; ++k) {
-                T a = T(0);
-                if (k0 + k < NV)
-#pragma unroll
-                  for (int u = 0; u < NV; ++u) a += T(EL[((k0 + k) * NV + u) * BT]) * gu[u];
-                g[d][k] = a;
-              }
-            }
-          };
-          if (low) {
-            T g[L2][VI];
-            project(g, ID2);
-            quad_form<L2, VI>(Pc + (int64_t)(p.i2off / VEC) * 32 * VEC, g, ID2, is);
-          } else {
-            T g[ID][VI];
-            project(g, ID);
-            quad_form<ID, VI>(Pc, g, ID, is);
-          }
-#pragma unroll
-          for (int k = 0; k < VI; ++k)
-            if (k0 + k < NV) sw[(ll * NV + k0 + k) * BT] = (double)is[k];
+            for (int w = u; w < NV; ++w, ++j) is += (u == w ? 1.0 : 2.0) * l[u] * l[w] * q[j];
+          sw[(ll * NV + k) * BT] = is;
         }
       }
       weights();
