@@ -217,10 +217,10 @@ def test_torch_autograd_function(bump):
     e.set_state(U)
 
 
-@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex"])
+@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex", "cweno4_tet"])
 def test_weno_vjp_matches_oracle_fd(name):
-    """VJP and JVP of the WENO residual (nonlinear weights, smoothness
-    indicators, stencil least squares, HLLC at every face point) against
+    """VJP and JVP of the WENO and CWENO residuals (nonlinear weights,
+    smoothness indicators, stencil least squares, HLLC at every face point) against
     central differences of the oracle's FP64 residual, and the dot-product
     test between them, on periodic meshes whose cells are all on the WENO
     branch."""
@@ -229,6 +229,8 @@ def test_weno_vjp_matches_oracle_fd(name):
     from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
     if name == "weno3_tet":
         m = Mesh.box_tet(5, 5, 5, seed=3).prepare(SCHEME_WENO, 2)
+    elif name == "cweno4_tet":
+        m = Mesh.box_tet(5, 5, 5, seed=5).prepare(SCHEME_WENO, 3, 5)
     else:
         m = Mesh.box_hex(10, 10, 10).prepare(SCHEME_WENO, 4)
     cfg = make_config(m, governing=2)

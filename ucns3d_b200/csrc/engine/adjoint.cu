@@ -951,14 +951,19 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
 // form, cells off the MUSCL fall-back.
 int adjw_setup(ucg_engine* e) {
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 3 && c.ees == 0 && c.wenwrt == 1 && c.governing == 2 && c.precision == UCG_FP64 &&
-        c.riemann == 1))
-    return fail(e, UCG_EINVAL, "the WENO adjoint covers conserved-variable WENO (EES 0), HLLC, Euler, FP64 form");
+  if (!(c.scheme == 3 && (c.ees == 0 || (c.ees == 5 && c.wenoz == 0)) && c.wenwrt == 1 && c.governing == 2 &&
+        c.precision == UCG_FP64 && c.riemann == 1))
+    return fail(e, UCG_EINVAL,
+                "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, no WENO-Z), HLLC, Euler, FP64 form");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   if (e->adjw_ready) return UCG_OK;
   const int64_t n = e->n, ngrp = (n + 31) / 32;
   const int A = c.admis_max, IM = c.imax, W = IM + 1, ID = c.ideg;
-  const int64_t slots = 1 + (int64_t)A * IM;
+  const bool cw = c.ees == 5;
+  const int IM2 = c.imax2;
+  // slots: the cell, the central stencil's members, then the others' (CWENO:
+  // IMAX2 members each)
+  const int64_t slots = cw ? 1 + IM + (int64_t)(A - 1) * IM2 : 1 + (int64_t)A * IM;
   cudaSetDevice(e->device);
   // the stencils, back from the device (interleaved over 32-cell groups)
   std::vector<int32_t> st((size_t)ngrp * 32 * A * W);
@@ -966,7 +971,14 @@ int adjw_setup(ucg_engine* e) {
   CK(cudaStreamSynchronize(e->stream));
   auto target = [&](int64_t i, int64_t s) -> int64_t {
     if (s == 0) return i;
-    const int ll = (int)((s - 1) / IM), k = (int)((s - 1) % IM);
+    int ll, k;
+    if (!cw || s - 1 < IM) {
+      ll = (int)((s - 1) / IM);
+      k = (int)((s - 1) % IM);
+    } else {
+      ll = 1 + (int)((s - 1 - IM) / IM2);
+      k = (int)((s - 1 - IM) % IM2);
+    }
     if (ll >= e->admis_h[i]) return -1;
     return st[(size_t)(((i >> 5) * A * W + ll * W + k + 1) * 32 + (i & 31))];
   };

@@ -1,5 +1,5 @@
-// Discrete adjoint (VJP) of the WENO reconstruction (conserved variables,
-// EES 0, FP64 form): the reverse of CP_RECONSTRUCTION's nonlinear weights
+// Discrete adjoint (VJP) of the WENO and CWENO reconstruction (conserved
+// variables, EES 0 or 5 without WENO-Z, FP64 form): the reverse of CP_RECONSTRUCTION's nonlinear weights
 // and smoothness indicators (src/reconstruct_p.f90:920-1250) and of the
 // stencil least squares (LEAST_SQUARES, src/gradients.f90:253-497).
 //
@@ -25,6 +25,40 @@
 using namespace ucg;
 
 namespace {
+
+// gr += 2 S g for the packed triangle P of S (rows padded to vectors; P_dd =
+// S_dd, P_de = 2 S_de), over the first nd <= NMAX rows
+template <int NMAX>
+__device__ __forceinline__ void tri_grad(const double* __restrict__ P, const double (&g)[NMAX], int nd,
+                                         double (&gr)[NMAX]) {
+  constexpr int VEC = Vec<double>::N;
+  int rs = 0;
+#pragma unroll
+  for (int d = 0; d < NMAX; ++d) {
+    if (d < nd) {
+#pragma unroll
+      for (int q = 0; q < (NMAX - d + VEC - 1) / VEC; ++q)
+        if (d + q * VEC < nd) {
+          double sv[VEC];
+          ldv(P + (int64_t)(rs + q) * 32 * VEC, sv);
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) {
+            const int e = d + q * VEC + i;
+            if (e < NMAX && e < nd) {
+              if (e == d) {
+                gr[d] += 2.0 * sv[i] * g[d];
+              } else {
+                gr[d] += sv[i] * g[e];
+                gr[e] += sv[i] * g[d];
+              }
+            }
+          }
+        }
+      rs += (nd - d + VEC - 1) / VEC;
+      asm volatile("" ::: "memory");
+    }
+  }
+}
 
 // k_adj_wpost: one lane per cell.  Writes Gb (layout of the stencil
 // polynomials G) and the direct adjoint of the cell mean; scr holds Bb and
@@ -95,21 +129,54 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
       if (v0 + 1 < NV) BB(d, v0 + 1) = acc[d][1] - b * sadj[v0 + 1];
     }
   }
-  // ---- per variable: indicators, weights and their adjoints
+  // ---- per variable: indicators, weights and their adjoints.  CWENO (EES
+  // 5): the central polynomial is g1 = (G_0 - sum_l lk G_l) / lc1 (rows
+  // below IDEGFREE2 for the lower-order stencils), the lower-order stencils
+  // have IDEGFREE2 rows and the S2 triangle, the linear weights are lc1, lk.
   const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+  const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
+  const bool cw = p.ees == 5;
+  const int ID2 = p.ideg2;
+  constexpr int L2 = ID < 9 ? ID : 9;
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
 #pragma unroll 1
   for (int v = 0; v < NV; ++v) {
+    double g3[L2];
+#pragma unroll
+    for (int d = 0; d < L2; ++d) g3[d] = 0.0;
+    if (cw)
+      for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+          if (d < ID2) g3[d] = g3[d] + lk * G(l2, d, v);
+    // row d of stencil polynomial ll as the reconstruction uses it
+    auto poly = [&](int ll, int d) -> double {
+      if (d >= nd_of(ll)) return 0.0;
+      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d, v) - (d < L2 ? g3[d] : 0.0));
+      return G(ll, d, v);
+    };
     double is[7], wt[7], om[7], omb[7];
     double sum = 0.0;
     for (int ll = 0; ll < adm; ++ll) {
-      double g[ID][1], s1[1] = {0.0};
+      double s1[1] = {0.0};
+      if (cw && ll > 0) {
+        double g[L2][1];
 #pragma unroll
-      for (int d = 0; d < ID; ++d) g[d][0] = G(ll, d, v);
-      quad_form<ID, 1>(Pc, g, ID, s1);
+        for (int d = 0; d < L2; ++d) g[d][0] = poly(ll, d);
+        quad_form<L2, 1>(Pc2, g, ID2, s1);
+      } else {
+        double g[ID][1];
+#pragma unroll
+        for (int d = 0; d < ID; ++d) g[d][0] = poly(ll, d);
+        quad_form<ID, 1>(Pc, g, ID, s1);
+      }
       is[ll] = s1[0];
       const double e = p.weno_eps + is[ll];
       const double e2 = e * e;
-      wt[ll] = (ll == 0 ? p.lwci : 1.0) / (e2 * e2);
+      const double lam = cw ? (ll == 0 ? lc1 : lk) : (ll == 0 ? p.lwci : 1.0);
+      wt[ll] = lam / (e2 * e2);
       sum += wt[ll];
     }
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
@@ -126,7 +193,7 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
         double ob = 0.0;
 #pragma unroll
         for (int d = 0; d < ID; ++d) {
-          const double gd = G(ll, d, v);
+          const double gd = poly(ll, d);
           ob += bb[d] * gd;
           gh[d] = (ll == 0 ? 0.0 : gh[d]) + om[ll] * gd;
         }
@@ -136,41 +203,42 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
 #pragma unroll
       for (int d = 0; d < ID; ++d) GH(d, v) = gh[d];
     }
+    double corr[L2];  // CWENO: the lower-order stencils' share of the central adjoint
+#pragma unroll
+    for (int d = 0; d < L2; ++d) corr[d] = 0.0;
     for (int ll = 0; ll < adm; ++ll) {
       const double wtb = (omb[ll] - dot) / sum;
       const double isb = wtb * (-4.0 * wt[ll] / (p.weno_eps + is[ll]));
-      double g[ID], gr[ID];
+      if (cw && ll > 0) {
+        double g[L2], gr[L2];
 #pragma unroll
-      for (int d = 0; d < ID; ++d) {
-        g[d] = G(ll, d, v);
-        gr[d] = 0.0;
-      }
-      // gr = 2 S g from the packed triangle (P_dd = S_dd, P_de = 2 S_de)
-      int rs = 0;
+        for (int d = 0; d < L2; ++d) {
+          g[d] = poly(ll, d);
+          gr[d] = 0.0;
+        }
+        tri_grad<L2>(Pc2, g, ID2, gr);
 #pragma unroll
-      for (int d = 0; d < ID; ++d) {
+        for (int d = 0; d < L2; ++d)
+          if (d < ID2) Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = om[ll] * BB(d, v) + isb * gr[d] + corr[d];
+      } else {
+        double g[ID], gr[ID];
 #pragma unroll
-        for (int q = 0; q < (ID - d + VEC - 1) / VEC; ++q) {
-          double sv[VEC];
-          ldv(Pc + (int64_t)(rs + q) * 32 * VEC, sv);
+        for (int d = 0; d < ID; ++d) {
+          g[d] = poly(ll, d);
+          gr[d] = 0.0;
+        }
+        tri_grad<ID>(Pc, g, ID, gr);
 #pragma unroll
-          for (int i = 0; i < VEC; ++i) {
-            const int e = d + q * VEC + i;
-            if (e < ID) {
-              if (e == d) {
-                gr[d] += 2.0 * sv[i] * g[d];
-              } else {
-                gr[d] += sv[i] * g[e];
-                gr[e] += sv[i] * g[d];
-              }
-            }
+        for (int d = 0; d < ID; ++d) {
+          const double gb = om[ll] * BB(d, v) + isb * gr[d];  // adjoint of the polynomial used
+          if (cw) {  // ll == 0: g1 = (G_0 - sum lk G_l) / lc1
+            Gb[(int64_t)((0 * ID + d) * NV + v) * 32] = (1.0 / lc1) * gb;
+            if (d < L2) corr[d] = -lk * ((1.0 / lc1) * gb);
+          } else {
+            Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = gb;
           }
         }
-        rs += (ID - d + VEC - 1) / VEC;
-        asm volatile("" ::: "memory");
       }
-#pragma unroll
-      for (int d = 0; d < ID; ++d) Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = om[ll] * BB(d, v) + isb * gr[d];
     }
   }
   // ---- CHECKSOL (0.85) on the WENO face values: a flagged cell took the
@@ -205,7 +273,8 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
 // shaped like k_lsq: DH rows of Gb in registers per pass, the members of
 // the stencil streamed; a member's contribution is the sum of its row
 // passes (the first writes, the next add).  Contributions go to slot-major
-// buffers: slot 0 the cell, 1 + l*IMAX + k member k of stencil l.
+// buffers: slot 0 the cell, 1 + l*IMAX + k member k of stencil l (CWENO:
+// 1 + IMAX + (l-1)*IMAX2 + k for the lower-order stencils).
 template <int P>
 __global__ void __launch_bounds__(128) k_adj_lsq(Problem p, const double* __restrict__ gbar,
                                                  const double* __restrict__ selfc, double* __restrict__ contrib) {
@@ -223,26 +292,30 @@ __global__ void __launch_bounds__(128) k_adj_lsq(Problem p, const double* __rest
   double self[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) self[v] = selfc[c * NV + v];
+  const bool cw = p.ees == 5;
   for (int ll = 0; ll < adm; ++ll) {
-    for (int d0 = 0; d0 < ID; d0 += DH) {
+    const bool low = cw && ll > 0;
+    const int nk = low ? p.imax2 : IM, nd = low ? p.ideg2 : ID;
+    const int64_t slot0 = ll == 0 ? 1 : (cw ? 1 + IM + (int64_t)(ll - 1) * p.imax2 : 1 + (int64_t)ll * IM);
+    for (int d0 = 0; d0 < nd; d0 += DH) {
       double gb[DH][NV];
 #pragma unroll
       for (int j = 0; j < DH; ++j)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) gb[j][v] = d0 + j < ID ? Gb[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] : 0.0;
+        for (int v = 0; v < NV; ++v) gb[j][v] = d0 + j < nd ? Gb[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] : 0.0;
       const double* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
 #pragma unroll 2
-      for (int k = 0; k < IM; ++k) {
-        const double* Mk = M + (int64_t)k * ID * 32;
+      for (int k = 0; k < nk; ++k) {
+        const double* Mk = M + (int64_t)k * nd * 32;
         double a[NV] = {0, 0, 0, 0, 0};
 #pragma unroll
         for (int j = 0; j < DH; ++j)
-          if (d0 + j < ID) {
+          if (d0 + j < nd) {
             const double m = Mk[j * 32];
 #pragma unroll
             for (int v = 0; v < NV; ++v) a[v] += m * gb[j][v];
           }
-        double* o = contrib + ((int64_t)(1 + ll * IM + k) * n + c) * NV;
+        double* o = contrib + ((slot0 + k) * n + c) * NV;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           o[v] = d0 == 0 ? a[v] : o[v] + a[v];
@@ -300,47 +373,93 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
     return;
   }
   const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
-#pragma unroll 1
-  for (int v = 0; v < NV; ++v) {
-    double is[7], dis[7], wt[7], dwt[7];
-    double sum = 0.0, dsum = 0.0;
-    for (int ll = 0; ll < adm; ++ll) {
-      double g[ID], dg[ID];
+  const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
+  const bool cw = p.ees == 5;
+  const int ID2 = p.ideg2;
+  constexpr int L2 = ID < 9 ? ID : 9;
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
+  // IS = sum_d g_d t_d, t_d = sum_{e>=d} P_de g_e, and its tangent (product rule)
+  auto is_and_tangent = [&](const double* Pt, auto& g, auto& dg, int nd, double& a, double& da) {
+    constexpr int ND = sizeof(g) / sizeof(g[0]);
+    a = da = 0.0;
+    int rs = 0;
 #pragma unroll
-      for (int d = 0; d < ID; ++d) {
-        g[d] = G(ll, d, v);
-        dg[d] = dGv(ll, d, v);
-      }
-      // IS = sum_d P_dd g_d^2 + sum_{d<e} P_de g_d g_e and its tangent
-      double a = 0.0, da = 0.0;
-      int rs = 0;
-#pragma unroll
-      for (int d = 0; d < ID; ++d) {
+    for (int d = 0; d < ND; ++d) {
+      if (d < nd) {
         double t = 0.0, dt = 0.0;
 #pragma unroll
-        for (int q = 0; q < (ID - d + VEC - 1) / VEC; ++q) {
-          double sv[VEC];
-          ldv(Pc + (int64_t)(rs + q) * 32 * VEC, sv);
+        for (int q = 0; q < (ND - d + VEC - 1) / VEC; ++q)
+          if (d + q * VEC < nd) {
+            double sv[VEC];
+            ldv(Pt + (int64_t)(rs + q) * 32 * VEC, sv);
 #pragma unroll
-          for (int i = 0; i < VEC; ++i) {
-            const int e = d + q * VEC + i;
-            if (e < ID) {
-              t += sv[i] * g[e];
-              dt += sv[i] * dg[e];
+            for (int i = 0; i < VEC; ++i) {
+              const int e = d + q * VEC + i;
+              if (e < ND && e < nd) {
+                t += sv[i] * g[e];
+                dt += sv[i] * dg[e];
+              }
             }
           }
-        }
-        rs += (ID - d + VEC - 1) / VEC;
-        // IS = sum_d g_d t_d, t_d = sum_{e>=d} P_de g_e: product rule
+        rs += (nd - d + VEC - 1) / VEC;
         a += g[d] * t;
         da += dg[d] * t + g[d] * dt;
         asm volatile("" ::: "memory");
+      }
+    }
+  };
+#pragma unroll 1
+  for (int v = 0; v < NV; ++v) {
+    double g3[L2], dg3[L2];
+#pragma unroll
+    for (int d = 0; d < L2; ++d) g3[d] = dg3[d] = 0.0;
+    if (cw)
+      for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+          if (d < ID2) {
+            g3[d] = g3[d] + lk * G(l2, d, v);
+            dg3[d] = dg3[d] + lk * dGv(l2, d, v);
+          }
+    auto poly = [&](int ll, int d) -> double {
+      if (d >= nd_of(ll)) return 0.0;
+      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d, v) - (d < L2 ? g3[d] : 0.0));
+      return G(ll, d, v);
+    };
+    auto dpoly = [&](int ll, int d) -> double {
+      if (d >= nd_of(ll)) return 0.0;
+      if (cw && ll == 0) return (1.0 / lc1) * (dGv(0, d, v) - (d < L2 ? dg3[d] : 0.0));
+      return dGv(ll, d, v);
+    };
+    double is[7], dis[7], wt[7], dwt[7];
+    double sum = 0.0, dsum = 0.0;
+    for (int ll = 0; ll < adm; ++ll) {
+      double a, da;
+      if (cw && ll > 0) {
+        double g[L2], dg[L2];
+#pragma unroll
+        for (int d = 0; d < L2; ++d) {
+          g[d] = poly(ll, d);
+          dg[d] = dpoly(ll, d);
+        }
+        is_and_tangent(Pc2, g, dg, ID2, a, da);
+      } else {
+        double g[ID], dg[ID];
+#pragma unroll
+        for (int d = 0; d < ID; ++d) {
+          g[d] = poly(ll, d);
+          dg[d] = dpoly(ll, d);
+        }
+        is_and_tangent(Pc, g, dg, ID, a, da);
       }
       is[ll] = a;
       dis[ll] = da;
       const double e = p.weno_eps + a;
       const double e2 = e * e;
-      wt[ll] = (ll == 0 ? p.lwci : 1.0) / (e2 * e2);
+      const double lam = cw ? (ll == 0 ? lc1 : lk) : (ll == 0 ? p.lwci : 1.0);
+      wt[ll] = lam / (e2 * e2);
       dwt[ll] = -4.0 * wt[ll] * dis[ll] / e;
       sum += wt[ll];
       dsum += dwt[ll];
@@ -353,8 +472,8 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
       const double dom = (dwt[ll] - om * dsum) / sum;
 #pragma unroll
       for (int d = 0; d < ID; ++d) {
-        const double gd = G(ll, d, v);
-        td[d] = (ll == 0 ? 0.0 : td[d]) + (dom * gd + om * dGv(ll, d, v));
+        const double gd = poly(ll, d);
+        td[d] = (ll == 0 ? 0.0 : td[d]) + (dom * gd + om * dpoly(ll, d));
         gh[d] = (ll == 0 ? 0.0 : gh[d]) + om * gd;
       }
     }
