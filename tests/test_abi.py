@@ -62,6 +62,21 @@ def test_create_validates_before_device(engine_lib):
     assert lib.ucg_create(C.byref(cfg), 0, 0, C.byref(h)) == N.UCG_EINVAL
 
 
+def test_create_rejects_unsupported_codes(engine_lib):
+    """Riemann solvers 1/2/3/9, limiters 1-9 and characteristic WENO (WENO
+    only) are accepted; anything else is refused before any device work."""
+    lib = N.engine()
+    m = Mesh.box_hex(4, 4, 4).prepare(SCHEME_MUSCL, 1)
+    cfg = make_config(m)
+    h = C.c_void_p()
+    for field, value in (("riemann", 4), ("riemann", 0), ("limiter", 10), ("limiter", 0), ("wenwrt", 2),
+                         ("wenwrt", 3)):
+        bad = N.UcgConfig.from_buffer_copy(cfg)
+        setattr(bad, field, value)
+        assert lib.ucg_create(C.byref(bad), m.ncells, 0, C.byref(h)) == N.UCG_EINVAL, (field, value)
+        assert not h.value
+
+
 def test_create_without_gpu_reports_cuda_error(engine_lib):
     import torch
     if torch.cuda.is_available():
