@@ -71,7 +71,8 @@ typedef struct ucg_config {
   int32_t limiter;     /* MUSCL limiter code (SLOPE_LIMITERS): 1 Barth-Jespersen,
                           2/3/9 Michalak, 4/8 Venkatakrishnan blended, 5 van Albada,
                           6 van Leer, 7 Venkatakrishnan; the adjoint covers 7           */
-  int32_t riemann;     /* iRiemann: 1 HLLC, 2 Rusanov, 3 Roe, 9 HLL (flux_p.f90:587-660);
+  int32_t riemann;     /* iRiemann: 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL,
+                          5 t-Roe, 9 HLL (flux_p.f90:587-660);
                           the adjoint covers HLLC                                      */
   int32_t precision;   /* UCG_FP64 or UCG_MIXED                                         */
   int32_t wenoz;       /* WENO-Z weights for CWENO (reconstruct_p.f90:1021-1029)         */

@@ -40,6 +40,8 @@ def lib():
         L.orc_rk3_step.argtypes = [cfgp, geop, recp, C.c_double, f64p]
         L.orc_hllc.restype = C.c_int
         L.orc_hllc.argtypes = [C.c_double, f64p, f64p, f64p]
+        L.orc_riemann.restype = C.c_int
+        L.orc_riemann.argtypes = [C.c_int, C.c_double, f64p, f64p, f64p, f64p]
         L.orc_reduce.restype = C.c_int
         L.orc_reduce.argtypes = [geop, f64p, C.c_int, f64p]
         L.orc_force.restype = C.c_int
@@ -55,6 +57,15 @@ def hllc(gamma, cl, cr):
     cr = np.ascontiguousarray(cr, dtype=np.float64)
     out = np.zeros(5)
     lib().orc_hllc(gamma, _p(cl), _p(cr), _p(out))
+    return out
+
+
+def riemann(kind, gamma, cl, cr, n):
+    """Global-frame flux of Roe (3), rotated Roe-HLL (4) or t-Roe (5)."""
+    cl, cr, n = (np.ascontiguousarray(a, dtype=np.float64) for a in (cl, cr, n))
+    out = np.zeros(5)
+    if lib().orc_riemann(kind, gamma, _p(cl), _p(cr), _p(n), _p(out)):
+        raise ValueError(f"no global-frame Riemann solver {kind}")
     return out
 
 

@@ -484,6 +484,150 @@ void roe(double gamma, const double* cl, const double* cr, const double* n, doub
   }
 }
 
+// unit vector normal to n with the largest 2D projection (the tangent choice
+// of rROE/tROE_RIEMANN_SOLVER, riemann.f90:1000-1030 and 700-725)
+static void face_tangent(const double* n, double* l) {
+  const double tx = n[1] * n[1] + n[2] * n[2], ty = n[2] * n[2] + n[0] * n[0], tz = n[0] * n[0] + n[1] * n[1];
+  if (tx >= ty && tx >= tz) {
+    l[0] = 0.0, l[1] = -n[2], l[2] = n[1];
+  } else if (ty >= tx && ty >= tz) {
+    l[0] = -n[2], l[1] = 0.0, l[2] = n[0];
+  } else {
+    l[0] = -n[1], l[1] = n[0], l[2] = 0.0;
+  }
+  const double t = std::sqrt(l[0] * l[0] + l[1] * l[1] + l[2] * l[2]);
+  for (int d = 0; d < 3; ++d) l[d] /= t;
+}
+
+static double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// primitive state, physical flux along n, sound speed and total enthalpy
+struct RoeSide {
+  double rho, vel[3], p, a, H, f[5];
+};
+static RoeSide roe_side(double gamma, const double* c, const double* n) {
+  RoeSide s;
+  s.rho = c[0];
+  for (int d = 0; d < 3; ++d) s.vel[d] = c[1 + d] / c[0];
+  const double q2 = dot3(s.vel, s.vel);
+  s.p = (gamma - 1.0) * (c[4] - 0.5 * s.rho * q2);
+  s.a = std::sqrt(gamma * s.p / s.rho);
+  s.H = s.a * s.a / (gamma - 1.0) + 0.5 * q2;
+  const double qn = dot3(s.vel, n);
+  s.f[0] = s.rho * qn;
+  for (int d = 0; d < 3; ++d) s.f[1 + d] = s.rho * qn * s.vel[d] + s.p * n[d];
+  s.f[4] = s.rho * qn * s.H;
+  return s;
+}
+
+// Roe-averaged density, velocity, enthalpy and sound speed
+struct RoeAvg {
+  double rho, vel[3], H, a;
+};
+static RoeAvg roe_avg(double gamma, const RoeSide& L, const RoeSide& R) {
+  RoeAvg m;
+  const double RT = std::sqrt(R.rho / L.rho);
+  m.rho = RT * L.rho;
+  for (int d = 0; d < 3; ++d) m.vel[d] = (L.vel[d] + RT * R.vel[d]) / (1.0 + RT);
+  m.H = (L.H + RT * R.H) / (1.0 + RT);
+  m.a = std::sqrt((gamma - 1.0) * (m.H - 0.5 * dot3(m.vel, m.vel)));
+  return m;
+}
+
+static double entropy_fix(double ws) { return ws < 0.2 ? 0.5 * (ws * ws / 0.2 + 0.2) : ws; }
+
+// rROE_RIEMANN_SOLVER (riemann.f90:892-1234): HLL along the velocity-jump
+// direction n1, Roe along n2 (in the plane of n and n1, normal to n1), with
+// the wave speeds blended by alpha1 = n.n1, alpha2 = n.n2
+void rhll(double gamma, const double* cl, const double* cr, const double* n, double* flux) {
+  const RoeSide L = roe_side(gamma, cl, n), R = roe_side(gamma, cr, n);
+  const double dvel[3] = {R.vel[0] - L.vel[0], R.vel[1] - L.vel[1], R.vel[2] - L.vel[2]};
+  const double adq = std::sqrt(dot3(dvel, dvel));
+  double n1[3], n2[3];
+  if (adq > 1.0e-13) {
+    for (int d = 0; d < 3; ++d) n1[d] = dvel[d] / adq;
+  } else {
+    face_tangent(n, n1);
+  }
+  double alpha1 = dot3(n, n1);
+  if (alpha1 < 0.0 || (alpha1 == 0.0 && std::signbit(alpha1))) {
+    for (int d = 0; d < 3; ++d) n1[d] = -n1[d];
+    alpha1 = -alpha1;
+  }
+  const double t[3] = {n1[1] * n[2] - n1[2] * n[1], n1[2] * n[0] - n1[0] * n[2], n1[0] * n[1] - n1[1] * n[0]};
+  n2[0] = t[1] * n1[2] - t[2] * n1[1];
+  n2[1] = t[2] * n1[0] - t[0] * n1[2];
+  n2[2] = t[0] * n1[1] - t[1] * n1[0];
+  const double ln2 = std::sqrt(dot3(n2, n2));
+  if (ln2 > 0.0) {
+    for (int d = 0; d < 3; ++d) n2[d] /= ln2;
+  } else {  // n1 parallel to n (alpha2 = 0): the flux does not depend on n2
+    face_tangent(n, n2);
+  }
+  double alpha2 = dot3(n, n2);
+  if (alpha2 < 0.0 || (alpha2 == 0.0 && std::signbit(alpha2))) {
+    for (int d = 0; d < 3; ++d) n2[d] = -n2[d];
+    alpha2 = -alpha2;
+  }
+  const RoeAvg m = roe_avg(gamma, L, R);
+  const double q1 = dot3(m.vel, n1);
+  const double SLm = std::min(std::min(0.0, q1 - m.a), dot3(L.vel, n1) - L.a);
+  const double SRp = std::max(std::max(0.0, q1 + m.a), dot3(R.vel, n1) + R.a);
+  const double qn = dot3(m.vel, n2), dqn = dot3(R.vel, n2) - dot3(L.vel, n2);
+  const double drho = R.rho - L.rho, dp = R.p - L.p, a = m.a;
+  const double LdU[4] = {(dp - m.rho * a * dqn) / (2.0 * a * a), drho - dp / (a * a),
+                         (dp + m.rho * a * dqn) / (2.0 * a * a), m.rho};
+  const double eig[4] = {qn - a, qn, qn + a, qn};
+  double ws[4] = {entropy_fix(std::fabs(qn - a)), std::fabs(qn), entropy_fix(std::fabs(qn + a)), std::fabs(qn)};
+  for (int k = 0; k < 4; ++k)
+    ws[k] = alpha2 * ws[k] - (alpha1 * 2.0 * SRp * SLm + alpha2 * (SRp + SLm) * eig[k]) / (SRp - SLm);
+  const double u = m.vel[0], v = m.vel[1], w = m.vel[2];
+  const double R4[5] = {0.0, dvel[0] - dqn * n2[0], dvel[1] - dqn * n2[1], dvel[2] - dqn * n2[2],
+                        dot3(m.vel, dvel) - qn * dqn};
+  const double Rv[5][4] = {{1.0, 1.0, 1.0, R4[0]},
+                           {u - a * n2[0], u, u + a * n2[0], R4[1]},
+                           {v - a * n2[1], v, v + a * n2[1], R4[2]},
+                           {w - a * n2[2], w, w + a * n2[2], R4[3]},
+                           {m.H - a * qn, 0.5 * dot3(m.vel, m.vel), m.H + a * qn, R4[4]}};
+  for (int k = 0; k < 5; ++k) {
+    double diss = 0.0;
+    for (int j = 0; j < 4; ++j) diss += ws[j] * LdU[j] * Rv[k][j];
+    flux[k] = (SRp * L.f[k] - SLm * R.f[k]) / (SRp - SLm) - 0.5 * diss;
+  }
+}
+
+// tROE_RIEMANN_SOLVER (riemann.f90:634-890): Roe with the shear waves along
+// the face tangents l (face_tangent) and m = n x l
+void troe(double gamma, const double* cl, const double* cr, const double* n, double* flux) {
+  double l[3], mt[3];
+  face_tangent(n, l);
+  mt[0] = n[1] * l[2] - n[2] * l[1];
+  mt[1] = n[2] * l[0] - n[0] * l[2];
+  mt[2] = n[0] * l[1] - n[1] * l[0];
+  const double lm = std::sqrt(dot3(mt, mt));
+  for (int d = 0; d < 3; ++d) mt[d] /= lm;
+  const RoeSide L = roe_side(gamma, cl, n), R = roe_side(gamma, cr, n);
+  const RoeAvg m = roe_avg(gamma, L, R);
+  const double a = m.a, qn = dot3(m.vel, n), ql = dot3(m.vel, l), qm = dot3(m.vel, mt);
+  const double dvel[3] = {R.vel[0] - L.vel[0], R.vel[1] - L.vel[1], R.vel[2] - L.vel[2]};
+  const double drho = R.rho - L.rho, dp = R.p - L.p, dqn = dot3(dvel, n);
+  const double LdU[5] = {(dp - m.rho * a * dqn) / (2.0 * a * a), drho - dp / (a * a),
+                         (dp + m.rho * a * dqn) / (2.0 * a * a), m.rho * dot3(dvel, l), m.rho * dot3(dvel, mt)};
+  const double ws[5] = {entropy_fix(std::fabs(qn - a)), std::fabs(qn), entropy_fix(std::fabs(qn + a)), std::fabs(qn),
+                        std::fabs(qn)};
+  const double u = m.vel[0], v = m.vel[1], w = m.vel[2];
+  const double Rv[5][5] = {{1.0, 1.0, 1.0, 0.0, 0.0},
+                           {u - a * n[0], u, u + a * n[0], l[0], mt[0]},
+                           {v - a * n[1], v, v + a * n[1], l[1], mt[1]},
+                           {w - a * n[2], w, w + a * n[2], l[2], mt[2]},
+                           {m.H - a * qn, 0.5 * dot3(m.vel, m.vel), m.H + a * qn, ql, qm}};
+  for (int k = 0; k < 5; ++k) {
+    double diss = 0.0;
+    for (int j = 0; j < 5; ++j) diss += ws[j] * LdU[j] * Rv[k][j];
+    flux[k] = 0.5 * (L.f[k] + R.f[k] - diss);
+  }
+}
+
 void riemann(const ucg_config* cfg, const double* cl, const double* cr, double* flux) {
   if (cfg->riemann == 2) rusanov(cfg->gamma, cl, cr, flux);
   else if (cfg->riemann == 9) hll(cfg->gamma, cl, cr, flux);
@@ -773,9 +917,11 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
           cr = crb;
         }
         double clr[NV], crr[NV], hf[NV], fl[NV];
-        if (x.cfg->riemann == 3) {  // Roe: global frame along the face normal
+        if (x.cfg->riemann >= 3 && x.cfg->riemann <= 5) {  // Roe family: global frame, face normal
           const double nrm[3] = {ang[0] * ang[3], ang[1] * ang[3], ang[2]};
-          roe(x.cfg->gamma, cl, cr, nrm, fl);
+          if (x.cfg->riemann == 3) roe(x.cfg->gamma, cl, cr, nrm, fl);
+          else if (x.cfg->riemann == 4) rhll(x.cfg->gamma, cl, cr, nrm, fl);
+          else troe(x.cfg->gamma, cl, cr, nrm, fl);
         } else {
           rotf(ang, cr, crr);
           rotf(ang, cl, clr);
@@ -990,6 +1136,16 @@ int orc_force(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, 
 // HLLC flux of two conserved states in the face frame (known-answer tests).
 int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
   hllc(gamma, cl, cr, flux);
+  return UCG_OK;
+}
+
+// one global-frame flux of the Roe family (iRiemann 3 Roe, 4 rotated
+// Roe-HLL, 5 t-Roe) through a face of unit normal n
+int orc_riemann(int kind, double gamma, const double* cl, const double* cr, const double* n, double* flux) {
+  if (kind == 3) roe(gamma, cl, cr, n, flux);
+  else if (kind == 4) rhll(gamma, cl, cr, n, flux);
+  else if (kind == 5) troe(gamma, cl, cr, n, flux);
+  else return UCG_EINVAL;
   return UCG_OK;
 }
 

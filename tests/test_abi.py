@@ -63,13 +63,13 @@ def test_create_validates_before_device(engine_lib):
 
 
 def test_create_rejects_unsupported_codes(engine_lib):
-    """Riemann solvers 1/2/3/9, limiters 1-9 and characteristic WENO (WENO
+    """Riemann solvers 1-5 and 9, limiters 1-9 and characteristic WENO (WENO
     only) are accepted; anything else is refused before any device work."""
     lib = N.engine()
     m = Mesh.box_hex(4, 4, 4).prepare(SCHEME_MUSCL, 1)
     cfg = make_config(m)
     h = C.c_void_p()
-    for field, value in (("riemann", 4), ("riemann", 0), ("limiter", 10), ("limiter", 0), ("wenwrt", 2),
+    for field, value in (("riemann", 6), ("riemann", 0), ("limiter", 10), ("limiter", 0), ("wenwrt", 2),
                          ("wenwrt", 3)):
         bad = N.UcgConfig.from_buffer_copy(cfg)
         setattr(bad, field, value)

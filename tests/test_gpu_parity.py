@@ -100,10 +100,12 @@ def test_characteristic_weno_residual_matches_oracle(name):
     assert np.abs(Rg - Oracle(m, cfg1).residual(U)).max() > 1e-10 * np.abs(Rg).max()
 
 
-@pytest.mark.parametrize("riemann", [2, 3, 9])
+@pytest.mark.parametrize("riemann", [2, 3, 4, 5, 9])
 @pytest.mark.parametrize("name", ["weno3_tet", "muscl_bump", "muscl_ns_hex"])
 def test_rusanov_and_hll_match_oracle(name, riemann):
-    """iRiemann 2 (Rusanov), 3 (Roe) and 9 (HLL) on the same kernels."""
+    """iRiemann 2 (Rusanov), 3 (Roe), 4 (rotated Roe-HLL), 5 (t-Roe) and 9
+    (HLL) on the same kernels; on the bump's walls the mirrored velocity jump
+    lies along n, the degenerate direction of the rotated solver."""
     m, cfg, U = _setup(name)
     cfg.riemann = riemann
     e = Engine(m, cfg)

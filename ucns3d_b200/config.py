@@ -24,7 +24,8 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
     Navier-Stokes; ``bc_state`` is the free-stream primitive state used by
     inflow/outflow boundaries; ``wenwrt`` 1 reconstructs the conserved
     variables, 2 the characteristic variables (WENWRT of UCNS3D.DAT);
-    ``riemann`` 1 HLLC, 2 Rusanov, 9 HLL (iRiemann)."""
+    ``riemann`` 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL
+    (iRiemann)."""
     if not getattr(mesh, "prepared", False):
         raise ValueError("mesh must be prepared first")
     cfg = N.UcgConfig()

@@ -76,7 +76,7 @@ struct Problem {
   unsigned* health;
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
-  int riemann;   // 1 HLLC, 2 Rusanov, 3 Roe, 9 HLL
+  int riemann;   // 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL
   int limiter;   // SLOPE_LIMITERS code (7 Venkatakrishnan)
   double* dt_dev;           // device dt (ucg_step)
 };
@@ -371,6 +371,184 @@ __host__ __device__ __forceinline__ void roe(double gamma, const S* cl, const S*
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
     const S diss = ws1 * L1 * R1[k] + ws2 * L2 * R2[k] + ws3 * L3 * R3[k] + ws2 * rho * R4[k];
+    flux[k] = 0.5 * (fL[k] + fR[k] - diss);
+  }
+}
+
+// Rotated Roe-HLL flux (rROE_RIEMANN_SOLVER, src/riemann.f90:892-1234):
+// HLL along n1 (the velocity-difference direction, or a direction normal to
+// n when the velocity jump is below TOLSMALL), Roe along n2 normal to n1 in
+// the plane of n and n1, in the global frame.
+template <typename S>
+__host__ __device__ __forceinline__ void rhll(double gamma, const S* cl, const S* cr, const double* n, S* flux) {
+  const double nx = n[0], ny = n[1], nz = n[2];
+  const S rL = cl[0], uL = cl[1] / rL, vL = cl[2] / rL, wL = cl[3] / rL;
+  const S pL = (gamma - 1.0) * (cl[4] - 0.5 * rL * (uL * uL + vL * vL + wL * wL));
+  const S rR = cr[0], uR = cr[1] / rR, vR = cr[2] / rR, wR = cr[3] / rR;
+  const S pR = (gamma - 1.0) * (cr[4] - 0.5 * rR * (uR * uR + vR * vR + wR * wR));
+  const S aL = sqrt(gamma * pL / rL), aR = sqrt(gamma * pR / rR);
+  const S HL = aL * aL / (gamma - 1.0) + 0.5 * (uL * uL + vL * vL + wL * wL);
+  const S HR = aR * aR / (gamma - 1.0) + 0.5 * (uR * uR + vR * vR + wR * wR);
+  S qnL = uL * nx + vL * ny + wL * nz, qnR = uR * nx + vR * ny + wR * nz;
+  const S fL[5] = {rL * qnL, rL * qnL * uL + pL * nx, rL * qnL * vL + pL * ny, rL * qnL * wL + pL * nz, rL * qnL * HL};
+  const S fR[5] = {rR * qnR, rR * qnR * uR + pR * nx, rR * qnR * vR + pR * ny, rR * qnR * wR + pR * nz, rR * qnR * HR};
+  // n1: the velocity-difference direction, oriented along n
+  const S abs_dq = sqrt((uR - uL) * (uR - uL) + (vR - vL) * (vR - vL) + (wR - wL) * (wR - wL));
+  S nx1, ny1, nz1;
+  if (value(abs_dq) > TOLSMALL) {
+    nx1 = (uR - uL) / abs_dq;
+    ny1 = (vR - vL) / abs_dq;
+    nz1 = (wR - wL) / abs_dq;
+  } else {
+    const double tx = ny * ny + nz * nz, ty = nz * nz + nx * nx, tz = nx * nx + ny * ny;
+    double a1, b1, c1;
+    if (tx >= ty && tx >= tz) {
+      a1 = 0.0, b1 = -nz, c1 = ny;
+    } else if (ty >= tx && ty >= tz) {
+      a1 = -nz, b1 = 0.0, c1 = nx;
+    } else {
+      a1 = -ny, b1 = nx, c1 = 0.0;
+    }
+    const double t = sqrt(a1 * a1 + b1 * b1 + c1 * c1);
+    nx1 = S(a1 / t);
+    ny1 = S(b1 / t);
+    nz1 = S(c1 / t);
+  }
+  S alpha1 = nx * nx1 + ny * ny1 + nz * nz1;
+  {
+    const double sg = copysign(1.0, value(alpha1));
+    nx1 = sg * nx1;
+    ny1 = sg * ny1;
+    nz1 = sg * nz1;
+    alpha1 = sg * alpha1;
+  }
+  // n2 = (n1 x n) x n1, normalised and oriented along n
+  const S tx = ny1 * nz - nz1 * ny, ty = nz1 * nx - nx1 * nz, tz = nx1 * ny - ny1 * nx;
+  S nx2 = ty * nz1 - tz * ny1, ny2 = tz * nx1 - tx * nz1, nz2 = tx * ny1 - ty * nx1;
+  {
+    const S t = sqrt(nx2 * nx2 + ny2 * ny2 + nz2 * nz2);
+    if (value(t) > 0.0) {
+      nx2 = nx2 / t;
+      ny2 = ny2 / t;
+      nz2 = nz2 / t;
+    } else {  // n1 parallel to n: alpha2 = 0 and any n2 normal to n gives the same flux
+      const double ax = ny * ny + nz * nz, ay = nz * nz + nx * nx, az = nx * nx + ny * ny;
+      double a1, b1, c1;
+      if (ax >= ay && ax >= az) {
+        a1 = 0.0, b1 = -nz, c1 = ny;
+      } else if (ay >= ax && ay >= az) {
+        a1 = -nz, b1 = 0.0, c1 = nx;
+      } else {
+        a1 = -ny, b1 = nx, c1 = 0.0;
+      }
+      const double q = sqrt(a1 * a1 + b1 * b1 + c1 * c1);
+      nx2 = S(a1 / q);
+      ny2 = S(b1 / q);
+      nz2 = S(c1 / q);
+    }
+  }
+  S alpha2 = nx * nx2 + ny * ny2 + nz * nz2;
+  {
+    const double sg = copysign(1.0, value(alpha2));
+    nx2 = sg * nx2;
+    ny2 = sg * ny2;
+    nz2 = sg * nz2;
+    alpha2 = sg * alpha2;
+  }
+  const S RT = sqrt(rR / rL), iRT = 1.0 / (1.0 + RT);
+  const S rho = RT * rL, u = (uL + RT * uR) * iRT, v = (vL + RT * vR) * iRT, w = (wL + RT * wR) * iRT;
+  const S H = (HL + RT * HR) * iRT;
+  const S a = sqrt((gamma - 1.0) * (H - 0.5 * (u * u + v * v + w * w)));
+  // HLL wave-speed estimates along n1
+  S qn = u * nx1 + v * ny1 + w * nz1;
+  qnL = uL * nx1 + vL * ny1 + wL * nz1;
+  qnR = uR * nx1 + vR * ny1 + wR * nz1;
+  const S SLm = fmin(fmin(S(0.0), qn - a), qnL - aL);
+  const S SRp = fmax(fmax(S(0.0), qn + a), qnR + aR);
+  // Roe dissipation along n2
+  qn = u * nx2 + v * ny2 + w * nz2;
+  qnL = uL * nx2 + vL * ny2 + wL * nz2;
+  qnR = uR * nx2 + vR * ny2 + wR * nz2;
+  const S drho = rR - rL, dp = pR - pL, dqn = qnR - qnL;
+  const S ia2 = 1.0 / (a * a);
+  const S L1 = (dp - rho * a * dqn) * (0.5 * ia2), L2 = drho - dp * ia2, L3 = (dp + rho * a * dqn) * (0.5 * ia2);
+  const S eig1 = qn - a, eig2 = qn, eig3 = qn + a;
+  S ws1 = fabs(qn - a), ws2 = fabs(qn), ws3 = fabs(qn + a);
+  if (value(ws1) < 0.2) ws1 = 0.5 * (ws1 * ws1 / 0.2 + 0.2);
+  if (value(ws3) < 0.2) ws3 = 0.5 * (ws3 * ws3 / 0.2 + 0.2);
+  const S isd = 1.0 / (SRp - SLm);
+  ws1 = alpha2 * ws1 - (alpha1 * 2.0 * SRp * SLm + alpha2 * (SRp + SLm) * eig1) * isd;
+  ws2 = alpha2 * ws2 - (alpha1 * 2.0 * SRp * SLm + alpha2 * (SRp + SLm) * eig2) * isd;
+  ws3 = alpha2 * ws3 - (alpha1 * 2.0 * SRp * SLm + alpha2 * (SRp + SLm) * eig3) * isd;
+  const S ws4 = ws2;
+  const S du = uR - uL, dv = vR - vL, dw = wR - wL;
+  const S R1[5] = {S(1.0), u - a * nx2, v - a * ny2, w - a * nz2, H - a * qn};
+  const S R2[5] = {S(1.0), u, v, w, 0.5 * (u * u + v * v + w * w)};
+  const S R3[5] = {S(1.0), u + a * nx2, v + a * ny2, w + a * nz2, H + a * qn};
+  const S R4[5] = {S(0.0), du - dqn * nx2, dv - dqn * ny2, dw - dqn * nz2, u * du + v * dv + w * dw - qn * dqn};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const S diss = ws1 * L1 * R1[k] + ws2 * L2 * R2[k] + ws3 * L3 * R3[k] + ws4 * rho * R4[k];
+    flux[k] = (SRp * fL[k] - SLm * fR[k]) * isd - 0.5 * diss;
+  }
+}
+
+// Roe flux with the two shear waves along explicit face tangents l and m
+// (tROE_RIEMANN_SOLVER, src/riemann.f90:634-890), global frame.
+template <typename S>
+__host__ __device__ __forceinline__ void troe(double gamma, const S* cl, const S* cr, const double* n, S* flux) {
+  const double nx = n[0], ny = n[1], nz = n[2];
+  double lx, ly, lz;
+  {
+    const double tx = ny * ny + nz * nz, ty = nz * nz + nx * nx, tz = nx * nx + ny * ny;
+    if (tx >= ty && tx >= tz) {
+      lx = 0.0, ly = -nz, lz = ny;
+    } else if (ty >= tx && ty >= tz) {
+      lx = -nz, ly = 0.0, lz = nx;
+    } else {
+      lx = -ny, ly = nx, lz = 0.0;
+    }
+    const double t = sqrt(lx * lx + ly * ly + lz * lz);
+    lx /= t, ly /= t, lz /= t;
+  }
+  double mx = ny * lz - nz * ly, my = nz * lx - nx * lz, mz = nx * ly - ny * lx;
+  {
+    const double t = sqrt(mx * mx + my * my + mz * mz);
+    mx /= t, my /= t, mz /= t;
+  }
+  const S rL = cl[0], uL = cl[1] / rL, vL = cl[2] / rL, wL = cl[3] / rL;
+  const S pL = (gamma - 1.0) * (cl[4] - 0.5 * rL * (uL * uL + vL * vL + wL * wL));
+  const S rR = cr[0], uR = cr[1] / rR, vR = cr[2] / rR, wR = cr[3] / rR;
+  const S pR = (gamma - 1.0) * (cr[4] - 0.5 * rR * (uR * uR + vR * vR + wR * wR));
+  const S qnL = uL * nx + vL * ny + wL * nz, qnR = uR * nx + vR * ny + wR * nz;
+  const S aL = sqrt(gamma * pL / rL), aR = sqrt(gamma * pR / rR);
+  const S HL = aL * aL / (gamma - 1.0) + 0.5 * (uL * uL + vL * vL + wL * wL);
+  const S HR = aR * aR / (gamma - 1.0) + 0.5 * (uR * uR + vR * vR + wR * wR);
+  const S RT = sqrt(rR / rL), iRT = 1.0 / (1.0 + RT);
+  const S rho = RT * rL, u = (uL + RT * uR) * iRT, v = (vL + RT * vR) * iRT, w = (wL + RT * wR) * iRT;
+  const S H = (HL + RT * HR) * iRT;
+  const S a = sqrt((gamma - 1.0) * (H - 0.5 * (u * u + v * v + w * w)));
+  const S qn = u * nx + v * ny + w * nz, ql = u * lx + v * ly + w * lz, qm = u * mx + v * my + w * mz;
+  const S drho = rR - rL, dp = pR - pL, dqn = qnR - qnL;
+  const S dql = (uR - uL) * lx + (vR - vL) * ly + (wR - wL) * lz;
+  const S dqm = (uR - uL) * mx + (vR - vL) * my + (wR - wL) * mz;
+  const S ia2 = 1.0 / (a * a);
+  const S L1 = (dp - rho * a * dqn) * (0.5 * ia2), L2 = drho - dp * ia2, L3 = (dp + rho * a * dqn) * (0.5 * ia2);
+  const S L4 = rho * dql, L5 = rho * dqm;
+  S ws1 = fabs(qn - a), ws3 = fabs(qn + a);
+  const S ws2 = fabs(qn);
+  if (value(ws1) < 0.2) ws1 = 0.5 * (ws1 * ws1 / 0.2 + 0.2);
+  if (value(ws3) < 0.2) ws3 = 0.5 * (ws3 * ws3 / 0.2 + 0.2);
+  const S R1[5] = {S(1.0), u - a * nx, v - a * ny, w - a * nz, H - a * qn};
+  const S R2[5] = {S(1.0), u, v, w, 0.5 * (u * u + v * v + w * w)};
+  const S R3[5] = {S(1.0), u + a * nx, v + a * ny, w + a * nz, H + a * qn};
+  const S R4[5] = {S(0.0), S(lx), S(ly), S(lz), ql};
+  const S R5[5] = {S(0.0), S(mx), S(my), S(mz), qm};
+  const S fL[5] = {rL * qnL, rL * qnL * uL + pL * nx, rL * qnL * vL + pL * ny, rL * qnL * wL + pL * nz, rL * qnL * HL};
+  const S fR[5] = {rR * qnR, rR * qnR * uR + pR * nx, rR * qnR * vR + pR * ny, rR * qnR * wR + pR * nz, rR * qnR * HR};
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const S diss = ws1 * L1 * R1[k] + ws2 * L2 * R2[k] + ws3 * L3 * R3[k] + ws2 * (L4 * R4[k] + L5 * R5[k]);
     flux[k] = 0.5 * (fL[k] + fR[k] - diss);
   }
 }

@@ -176,6 +176,8 @@ int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, c
   switch (e->cfg.riemann) {  // the Riemann solver is a template argument of the face kernel
     case 2: k_face<T, NS, 2><<<fb, FB, 0, e->stream>>>(p, Uc); break;
     case 3: k_face<T, NS, 3><<<fb, FB, 0, e->stream>>>(p, Uc); break;
+    case 4: k_face<T, NS, 4><<<fb, FB, 0, e->stream>>>(p, Uc); break;
+    case 5: k_face<T, NS, 5><<<fb, FB, 0, e->stream>>>(p, Uc); break;
     case 9: k_face<T, NS, 9><<<fb, FB, 0, e->stream>>>(p, Uc); break;
     default: k_face<T, NS, 1><<<fb, FB, 0, e->stream>>>(p, Uc); break;
   }
@@ -245,9 +247,9 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   int ideg = (c.iorder + 1) * (c.iorder + 2) * (c.iorder + 3) / 6 - 1;
   if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
       c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && ((c.ideg2 != 3 && c.ideg2 != 9) || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
-      c.gamma <= 1.0 || c.limiter < 1 || c.limiter > 9 || !(c.riemann == 1 || c.riemann == 2 || c.riemann == 3 || c.riemann == 9) ||
+      c.gamma <= 1.0 || c.limiter < 1 || c.limiter > 9 || !((c.riemann >= 1 && c.riemann <= 5) || c.riemann == 9) ||
       !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3))) {
-    g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC/Rusanov/Roe/HLL, limiter 1..9, "
+    g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC/Rusanov/Roe/rotated Roe-HLL/t-Roe/HLL, limiter 1..9, "
                    "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9)";
     return UCG_EINVAL;
   }

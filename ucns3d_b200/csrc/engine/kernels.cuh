@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
 // ======================================================================
 // One thread per owned face (the cell with the smaller index, or the only
 // cell of a boundary face): the Riemann flux RK (iRiemann: 1 HLLC, 2
-// Rusanov, 3 Roe, 9 HLL) and viscous fluxes over the face's points,
+// Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL) and viscous fluxes over the
+// face's points,
 // weighted by w_q * area.  The neighbour's face gets the negated sums: HLLC
 // and the viscous flux are antisymmetric under swapping the two states and
 // flipping the normal, so each interior face is evaluated once instead of
@@ -185,9 +186,11 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
       boundary_ghost(p, p.bc[c * MF + f], r, cl, cr);
     }
     double fl[NV];
-    if constexpr (RK == 3) {  // Roe: global frame along the face normal
+    if constexpr (RK >= 3 && RK <= 5) {  // Roe family: global frame, face normal
       const double nrm[3] = {r[0] * r[3], r[1] * r[3], r[2]};
-      roe(p.gamma, cl, cr, nrm, fl);
+      if constexpr (RK == 3) roe(p.gamma, cl, cr, nrm, fl);
+      else if constexpr (RK == 4) rhll(p.gamma, cl, cr, nrm, fl);
+      else troe(p.gamma, cl, cr, nrm, fl);
     } else {
       double a[NV], b[NV], h[NV];
       rot_f(r, cr, b);
