@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--adjoint-only", action="store_true", help="only the adjoint timing (bump channel)")
     ap.add_argument("--adjoint-steps", type=int, default=200, help="RK3 steps of the adjoint run")
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint stride of the adjoint run")
+    ap.add_argument("--adjoint-weno-n", type=int, default=32,
+                    help="hexahedra per side of the vortex timed for the WENO VJP/JVP")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
     return ap.parse_args()
@@ -326,7 +328,7 @@ def main_reference(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def run_adjoint(local, steps=200, every=20):
+def run_adjoint(local, steps=200, every=20, weno_n=32):
     """Adjoint cost on the bump channel (240x80 quads half split into
     triangles, 4 layers: hexahedra + prisms, MUSCL + HLLC, FP64): device
     times of the residual, its VJP and JVP at a marched state, then a
@@ -362,10 +364,10 @@ def run_adjoint(local, steps=200, every=20):
            "run_steps": steps, "checkpoint_every": every, "primal_run_ms": primal, "adjoint_run_ms": adj,
            "adjoint_run_over_primal_run": adj / primal, "J": J,
            "dJdp": [float(x) for x in gp]}
-    # the WENO residual's VJP/JVP (FP64 form) on the vortex, 32^3 hexahedra
+    # the WENO residual's VJP/JVP (FP64 form) on the vortex, weno_n^3 hexahedra
     from ucns3d_b200 import _native as N
     from ucns3d_b200.engine import EngineError
-    cw = cases.vortex_hex_weno5(n=32, precision=N.UCG_FP64)
+    cw = cases.vortex_hex_weno5(n=weno_n, precision=N.UCG_FP64)
     ew = Engine(cw.mesh, cw.cfg, device=local)
     ew.set_state(cw.U0)
     try:
@@ -389,7 +391,7 @@ def main():
     from ucns3d_b200 import _native as N
 
     if args.adjoint_only:
-        adj = run_adjoint(local, args.adjoint_steps, args.adjoint_every)
+        adj = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
         if rank == 0:
             print(json.dumps({"adjoint": adj}), flush=True)
         if ws > 1:
@@ -461,7 +463,7 @@ def main():
                        "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
                        "after_steps": args.warmup + args.steps}
     if not args.no_adjoint:
-        out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every)
+        out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_sample(args, steps=1)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",
