@@ -60,89 +60,140 @@ __device__ __forceinline__ void tri_grad(const double* __restrict__ P, const dou
   }
 }
 
-// k_adj_wpost: one lane per cell.  Writes Gb (layout of the stencil
-// polynomials G) and the direct adjoint of the cell mean; scr holds Bb and
-// the combined polynomial of the CHECKSOL test (interleaved like G).
+// IS = g^T S g and gr = 2 S g in one pass over the packed triangle
+template <int NMAX>
+__device__ __forceinline__ double is_and_grad(const double* __restrict__ P, const double (&g)[NMAX], int nd,
+                                              double (&gr)[NMAX]) {
+#pragma unroll
+  for (int d = 0; d < NMAX; ++d) gr[d] = 0.0;
+  tri_grad<NMAX>(P, g, nd, gr);
+  double is = 0.0;
+#pragma unroll
+  for (int d = 0; d < NMAX; ++d)
+    if (d < nd) is += g[d] * gr[d];
+  return 0.5 * is;
+}
+
+// Thread layout of the WENO post-processing adjoint and tangent: one block
+// per group of 32 cells (the group of the interleaved tables), NV warps,
+// warp v takes variable v of every cell of the group (lane = cell).  The
+// weights of one variable need no other variable, so the warps only meet
+// at the CHECKSOL test (all five variables of a face value); and the five
+// warps read the same smoothness matrices at about the same time, so those
+// come from DRAM about once per pass instead of once per variable.
+constexpr int WP_THREADS = NV * 32;
+#ifndef UCG_AWP_MINB
+#define UCG_AWP_MINB 2  // blocks per SM the register budget is sized for
+#endif
+
+// CHECKSOL (0.85) of the combined polynomial sGH (all variables, shared
+// memory) at the face points of cell c; warp w tests the points whose
+// running index is w modulo NV.  True if a face value of the cell fails.
 template <int P>
-__global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __restrict__ U,
-                                                  const double* __restrict__ adjF, double* __restrict__ gbar,
-                                                  double* __restrict__ scr, double* __restrict__ selfc,
-                                                  int* __restrict__ flag) {
+__device__ __forceinline__ bool checksol_split(const Problem& p, const double* __restrict__ U, int64_t c, int nf,
+                                               const double* __restrict__ xq, const double* __restrict__ bmv,
+                                               const double (*sGH)[NV][32], int lane, int w) {
   constexpr int ID = Deg<P>::ideg;
-  constexpr int VEC = Vec<double>::N;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.n) return;
-  const int A = p.admis_max;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
-  const int FQ = MF * QS;
-  const int adm = p.admis[c], nf = p.nfaces[c];
-  const int64_t grp = c >> 5;
-  const int lane = (int)(c & 31);
-  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  auto G = [&](int ll, int d, int v) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-  double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  double* Sc = scr + grp * (int64_t)(2 * ID * NV) * 32 + lane;
-  auto BB = [&](int d, int v) -> double& { return Sc[(int64_t)(d * NV + v) * 32]; };
-  auto GH = [&](int d, int v) -> double& { return Sc[(int64_t)((ID + d) * NV + v) * 32]; };
-  const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
-  const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
-  const double* aF = adjF + c * (int64_t)FQ * NV;
-  double u0[NV], pm[NV];
+  double u0[NV], pm[NV], cb[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
   cons2prim(p.gamma, u0, pm);
-  auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
-  auto mono = [&](int f, int q, double (&m)[ID]) {
-    const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
-    monomials<P, double>(xi[0], xi[32], xi[64], m);
-  };
-  if (!p.full[c]) {
-    atomicOr(flag, 1);
-    return;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    cb[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) cb[v] += bmv[d * 32] * sGH[d][v][lane];
   }
-  // ---- the direct term and Bb = sum_x ub(x) (m(x) - mean(m))
-  double sadj[NV] = {0, 0, 0, 0, 0};
-  for (int f = 0; f < nf; ++f)
-    for (int q = 0; q < nq_of(f); ++q)
+  bool bad = false;
+  int k = 0;
+  for (int f = 0; f < nf; ++f) {
+    const int nq = face_nq(p, p.ftype[c * MF + f]);
+    for (int q = 0; q < nq; ++q, ++k) {
+      if (k % NV != w || bad) continue;
+      const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+      double m[ID], uf[NV];
+      monomials<P, double>(xi[0], xi[32], xi[64], m);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) sadj[v] += aF[(f * QS + q) * NV + v];
-#pragma unroll 1
-  for (int v0 = 0; v0 < NV; v0 += 2) {
-    double acc[ID][2];
+      for (int v = 0; v < NV; ++v) {
+        // re-read the combined polynomial from shared memory at every point:
+        // kept in registers across the points it does not fit
+        asm volatile("" ::: "memory");
+        double r = 0.0;
 #pragma unroll
-    for (int d = 0; d < ID; ++d) acc[d][0] = acc[d][1] = 0.0;
-    for (int f = 0; f < nf; ++f)
-      for (int q = 0; q < nq_of(f); ++q) {
-        double m[ID];
-        mono(f, q, m);
-        const double a0 = aF[(f * QS + q) * NV + v0], a1 = v0 + 1 < NV ? aF[(f * QS + q) * NV + v0 + 1] : 0.0;
+        for (int d = 0; d < ID; ++d) r += m[d] * sGH[d][v][lane];
+        uf[v] = u0[v] + (r - cb[v]);
+      }
+      bad = jump_bad(p.gamma, pm, uf, 0.85);
+    }
+  }
+  return bad;
+}
+
+// k_adj_wpost: writes Gb (layout of the stencil polynomials G) and the
+// direct adjoint of the cell mean (selfc); scr holds Bb (interleaved like
+// G).  Gb first receives 2 S G_l (the gradient of IS_l), read back once the
+// weights' adjoints are known.
+template <int P>
+__global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem p, const double* __restrict__ U,
+                                                             const double* __restrict__ adjF,
+                                                             double* __restrict__ gbar, double* __restrict__ scr,
+                                                             double* __restrict__ selfc, int* __restrict__ flag) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int VEC = Vec<double>::N;
+  __shared__ double sGH[ID][NV][32];
+  const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
+  const int64_t grp = blockIdx.x;
+  const int64_t c = grp * 32 + lane;
+  const bool live = c < p.n && p.full[c];
+  if (c < p.n && !p.full[c] && v == 0) atomicOr(flag, 1);
+  const int A = p.admis_max;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int FQ = MF * QS;
+  const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
+  const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
+  if (live) {
+    const int adm = p.admis[c], nf = p.nfaces[c];
+    const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+    auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+    double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
+    auto GB = [&](int ll, int d) -> double& { return Gb[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+    double* BBp = scr + grp * (int64_t)(ID * NV) * 32 + lane;
+    auto BB = [&](int d) -> double& { return BBp[(int64_t)(d * NV + v) * 32]; };
+    const double* aF = adjF + c * (int64_t)FQ * NV + v;
+    // ---- the direct term and Bb = sum_x ub(x) (m(x) - mean(m))
+    {
+      double acc[ID], sa = 0.0;
 #pragma unroll
-        for (int d = 0; d < ID; ++d) {
-          acc[d][0] += m[d] * a0;
-          acc[d][1] += m[d] * a1;
+      for (int d = 0; d < ID; ++d) acc[d] = 0.0;
+      for (int f = 0; f < nf; ++f) {
+        const int nq = face_nq(p, p.ftype[c * MF + f]);
+        for (int q = 0; q < nq; ++q) {
+          const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+          double m[ID];
+          monomials<P, double>(xi[0], xi[32], xi[64], m);
+          const double a = aF[(f * QS + q) * NV];
+          sa += a;
+#pragma unroll
+          for (int d = 0; d < ID; ++d) acc[d] += m[d] * a;
         }
       }
 #pragma unroll
-    for (int d = 0; d < ID; ++d) {
-      const double b = bmv[d * 32];
-      BB(d, v0) = acc[d][0] - b * sadj[v0];
-      if (v0 + 1 < NV) BB(d, v0 + 1) = acc[d][1] - b * sadj[v0 + 1];
+      for (int d = 0; d < ID; ++d) BB(d) = acc[d] - bmv[d * 32] * sa;
+      selfc[c * NV + v] = sa;
     }
-  }
-  // ---- per variable: indicators, weights and their adjoints.  CWENO (EES
-  // 5): the central polynomial is g1 = (G_0 - sum_l lk G_l) / lc1 (rows
-  // below IDEGFREE2 for the lower-order stencils), the lower-order stencils
-  // have IDEGFREE2 rows and the S2 triangle, the linear weights are lc1, lk.
-  const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
-  const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
-  const bool cw = p.ees == 5;
-  const int ID2 = p.ideg2;
-  constexpr int L2 = ID < 9 ? ID : 9;
-  const double lc1 = 1.0 - 1.0 / p.lwci;
-  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-  auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
-#pragma unroll 1
-  for (int v = 0; v < NV; ++v) {
+    // ---- indicators and weights.  CWENO (EES 5): the central polynomial is
+    // g1 = (G_0 - sum_l lk G_l) / lc1 (rows below IDEGFREE2 for the
+    // lower-order stencils), the lower-order stencils have IDEGFREE2 rows and
+    // the S2 triangle, the linear weights are lc1, lk.
+    const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+    const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
+    const bool cw = p.ees == 5;
+    const int ID2 = p.ideg2;
+    constexpr int L2 = ID < 9 ? ID : 9;
+    const double lc1 = 1.0 - 1.0 / p.lwci;
+    const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+    auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
     double g3[L2];
 #pragma unroll
     for (int d = 0; d < L2; ++d) g3[d] = 0.0;
@@ -150,123 +201,93 @@ __global__ void __launch_bounds__(64) k_adj_wpost(Problem p, const double* __res
       for (int l2 = 1; l2 < adm; ++l2)
 #pragma unroll
         for (int d = 0; d < L2; ++d)
-          if (d < ID2) g3[d] = g3[d] + lk * G(l2, d, v);
+          if (d < ID2) g3[d] = g3[d] + lk * G(l2, d);
     // row d of stencil polynomial ll as the reconstruction uses it
     auto poly = [&](int ll, int d) -> double {
       if (d >= nd_of(ll)) return 0.0;
-      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d, v) - (d < L2 ? g3[d] : 0.0));
-      return G(ll, d, v);
+      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d) - (d < L2 ? g3[d] : 0.0));
+      return G(ll, d);
     };
     double is[7], wt[7], om[7], omb[7];
     double sum = 0.0;
+#pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
-      double s1[1] = {0.0};
+      double s;
       if (cw && ll > 0) {
-        double g[L2][1];
+        double g[L2], gr[L2];
 #pragma unroll
-        for (int d = 0; d < L2; ++d) g[d][0] = poly(ll, d);
-        quad_form<L2, 1>(Pc2, g, ID2, s1);
+        for (int d = 0; d < L2; ++d) g[d] = poly(ll, d);
+        s = is_and_grad<L2>(Pc2, g, ID2, gr);
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+          if (d < ID2) GB(ll, d) = gr[d];
       } else {
-        double g[ID][1];
+        double g[ID], gr[ID];
 #pragma unroll
-        for (int d = 0; d < ID; ++d) g[d][0] = poly(ll, d);
-        quad_form<ID, 1>(Pc, g, ID, s1);
+        for (int d = 0; d < ID; ++d) g[d] = poly(ll, d);
+        s = is_and_grad<ID>(Pc, g, ID, gr);
+#pragma unroll
+        for (int d = 0; d < ID; ++d) GB(ll, d) = gr[d];
       }
-      is[ll] = s1[0];
-      const double e = p.weno_eps + is[ll];
+      is[ll] = s;
+      const double e = p.weno_eps + s;
       const double e2 = e * e;
       const double lam = cw ? (ll == 0 ? lc1 : lk) : (ll == 0 ? p.lwci : 1.0);
       wt[ll] = lam / (e2 * e2);
       sum += wt[ll];
     }
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
-    // combined polynomial (CHECKSOL) and the weights' adjoints
+    // ---- combined polynomial (CHECKSOL) and the weights' adjoints
     double dot = 0.0;
     {
-      double gh[ID], bb[ID];
+      double gh[ID];
 #pragma unroll
-      for (int d = 0; d < ID; ++d) {
-        gh[d] = 0.0;
-        bb[d] = BB(d, v);
-      }
+      for (int d = 0; d < ID; ++d) gh[d] = 0.0;
+#pragma unroll 1
       for (int ll = 0; ll < adm; ++ll) {
         double ob = 0.0;
 #pragma unroll
         for (int d = 0; d < ID; ++d) {
           const double gd = poly(ll, d);
-          ob += bb[d] * gd;
-          gh[d] = (ll == 0 ? 0.0 : gh[d]) + om[ll] * gd;
+          ob += BB(d) * gd;
+          gh[d] += om[ll] * gd;
         }
         omb[ll] = ob;
         dot += ob * om[ll];
       }
 #pragma unroll
-      for (int d = 0; d < ID; ++d) GH(d, v) = gh[d];
+      for (int d = 0; d < ID; ++d) sGH[d][v][lane] = gh[d];
     }
-    double corr[L2];  // CWENO: the lower-order stencils' share of the central adjoint
+    // ---- Gb_l = om_l Bb + ISb_l 2 S G_l (+ the CWENO central share)
+    double corr[L2];
 #pragma unroll
     for (int d = 0; d < L2; ++d) corr[d] = 0.0;
+#pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       const double wtb = (omb[ll] - dot) / sum;
       const double isb = wtb * (-4.0 * wt[ll] / (p.weno_eps + is[ll]));
       if (cw && ll > 0) {
-        double g[L2], gr[L2];
-#pragma unroll
-        for (int d = 0; d < L2; ++d) {
-          g[d] = poly(ll, d);
-          gr[d] = 0.0;
-        }
-        tri_grad<L2>(Pc2, g, ID2, gr);
 #pragma unroll
         for (int d = 0; d < L2; ++d)
-          if (d < ID2) Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = om[ll] * BB(d, v) + isb * gr[d] + corr[d];
+          if (d < ID2) GB(ll, d) = om[ll] * BB(d) + isb * GB(ll, d) + corr[d];
       } else {
-        double g[ID], gr[ID];
 #pragma unroll
         for (int d = 0; d < ID; ++d) {
-          g[d] = poly(ll, d);
-          gr[d] = 0.0;
-        }
-        tri_grad<ID>(Pc, g, ID, gr);
-#pragma unroll
-        for (int d = 0; d < ID; ++d) {
-          const double gb = om[ll] * BB(d, v) + isb * gr[d];  // adjoint of the polynomial used
+          const double gb = om[ll] * BB(d) + isb * GB(ll, d);  // adjoint of the polynomial used
           if (cw) {  // ll == 0: g1 = (G_0 - sum lk G_l) / lc1
-            Gb[(int64_t)((0 * ID + d) * NV + v) * 32] = (1.0 / lc1) * gb;
+            GB(0, d) = (1.0 / lc1) * gb;
             if (d < L2) corr[d] = -lk * ((1.0 / lc1) * gb);
           } else {
-            Gb[(int64_t)((ll * ID + d) * NV + v) * 32] = gb;
+            GB(ll, d) = gb;
           }
         }
       }
     }
   }
+  __syncthreads();
   // ---- CHECKSOL (0.85) on the WENO face values: a flagged cell took the
   // MUSCL fall-back in the forward, which this adjoint does not cover
-  bool bad = false;
-  double cb[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    cb[v] = 0.0;
-#pragma unroll
-    for (int d = 0; d < ID; ++d) cb[v] += bmv[d * 32] * GH(d, v);
-  }
-  for (int f = 0; f < nf && !bad; ++f)
-    for (int q = 0; q < nq_of(f); ++q) {
-      double m[ID], uf[NV];
-      mono(f, q, m);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        double r = 0.0;
-#pragma unroll
-        for (int d = 0; d < ID; ++d) r += m[d] * GH(d, v);
-        uf[v] = u0[v] + (r - cb[v]);
-      }
-      bad = bad || jump_bad(p.gamma, pm, uf, 0.85);
-    }
-  if (bad) atomicOr(flag, 1);
-#pragma unroll
-  for (int v = 0; v < NV; ++v) selfc[c * NV + v] = sadj[v];
+  if (live && checksol_split<P>(p, U, c, p.nfaces[c], xq, bmv, sGH, lane, v)) atomicOr(flag, 1);
 }
 
 // k_adj_lsq: one lane per cell, the transpose of the stencil least squares,
@@ -517,7 +538,7 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
 template <int P>
 void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
               double* contrib, int* flag, cudaStream_t st) {
-  k_adj_wpost<P><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U, adjF, gbar, scr, selfc, flag);
+  k_adj_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, adjF, gbar, scr, selfc, flag);
   k_adj_lsq<P><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, gbar, selfc, contrib);
 }
 
