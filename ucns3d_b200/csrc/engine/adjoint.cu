@@ -1064,8 +1064,7 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   CK(cudaMemsetAsync(e->adjw_flag.p, 0, sizeof(int), e->stream));
   double* tdul = (double*)e->adjw_face.p;
   double* tflux = (double*)e->adjw_contrib.p;
-  if ((rc = launch_weno_tangent(e, p, U, (const double*)e->adjw_gbar.p, (double*)e->adjw_scr.p, tdul,
-                                (int*)e->adjw_flag.p)))
+  if ((rc = launch_weno_tangent(e, p, U, (const double*)e->adjw_gbar.p, tdul, (int*)e->adjw_flag.p)))
     return rc;
   k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux);
   k_jvp_sum<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, tflux, dR);

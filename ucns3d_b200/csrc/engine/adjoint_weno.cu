@@ -239,24 +239,20 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
     // ---- combined polynomial (CHECKSOL) and the weights' adjoints
     double dot = 0.0;
-    {
-      double gh[ID];
 #pragma unroll
-      for (int d = 0; d < ID; ++d) gh[d] = 0.0;
+    for (int d = 0; d < ID; ++d) sGH[d][v][lane] = 0.0;
 #pragma unroll 1
-      for (int ll = 0; ll < adm; ++ll) {
-        double ob = 0.0;
+    for (int ll = 0; ll < adm; ++ll) {
+      double ob = 0.0;
 #pragma unroll
-        for (int d = 0; d < ID; ++d) {
-          const double gd = poly(ll, d);
-          ob += BB(d) * gd;
-          gh[d] += om[ll] * gd;
-        }
-        omb[ll] = ob;
-        dot += ob * om[ll];
+      for (int d = 0; d < ID; ++d) {
+        const double gd = poly(ll, d);
+        ob += BB(d) * gd;
+        sGH[d][v][lane] += om[ll] * gd;
+        if ((d & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
       }
-#pragma unroll
-      for (int d = 0; d < ID; ++d) sGH[d][v][lane] = gh[d];
+      omb[ll] = ob;
+      dot += ob * om[ll];
     }
     // ---- Gb_l = om_l Bb + ISb_l 2 S G_l (+ the CWENO central share)
     double corr[L2];
@@ -349,90 +345,47 @@ __global__ void __launch_bounds__(128) k_adj_lsq(Problem p, const double* __rest
   for (int v = 0; v < NV; ++v) contrib[(int64_t)c * NV + v] = self[v];
 }
 
-// k_jvp_wpost: one lane per cell, the tangent of the WENO face values
-// (minus the cell mean) from the tangent stencil polynomials dG:
+
+// k_jvp_wpost: the tangent of the WENO face values (minus the cell mean)
+// from the tangent stencil polynomials dG, thread layout of k_adj_wpost:
 //   dIS_l = d(G_l^T S G_l),  dwt_l = -4 wt_l dIS_l / (eps + IS_l),
 //   dom_l = (dwt_l - om_l sum dwt) / sum wt,
 //   du(x) - dU_c = b(x) . sum_l (dom_l G_l + om_l dG_l).
-// Same fall-back flag as k_adj_wpost.
+// Same fall-back flag as k_adj_wpost; a cell on it gets a zero tangent.
 template <int P>
-__global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __restrict__ U,
-                                                  const double* __restrict__ dG, double* __restrict__ scr,
-                                                  double* __restrict__ tdul, int* __restrict__ flag) {
+__global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem p, const double* __restrict__ U,
+                                                                        const double* __restrict__ dG,
+                                                                        double* __restrict__ tdul,
+                                                                        int* __restrict__ flag) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<double>::N;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= p.n) return;
+  __shared__ double sGH[ID][NV][32];
+  const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
+  const int64_t grp = blockIdx.x;
+  const int64_t c = grp * 32 + lane;
+  const bool live = c < p.n && p.full[c];
+  if (c < p.n && !p.full[c] && v == 0) atomicOr(flag, 1);
   const int A = p.admis_max;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
   const int FQ = MF * QS;
-  const int adm = p.admis[c], nf = p.nfaces[c];
-  const int64_t grp = c >> 5;
-  const int lane = (int)(c & 31);
-  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  const double* dGc = dG + grp * (int64_t)(A * ID * NV) * 32 + lane;
-  auto G = [&](int ll, int d, int v) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-  auto dGv = [&](int ll, int d, int v) -> double { return dGc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-  double* Sc = scr + grp * (int64_t)(2 * ID * NV) * 32 + lane;
-  auto TD = [&](int d, int v) -> double& { return Sc[(int64_t)(d * NV + v) * 32]; };
-  auto GH = [&](int d, int v) -> double& { return Sc[(int64_t)((ID + d) * NV + v) * 32]; };
   const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
   const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
-  double* out = tdul + c * (int64_t)FQ * NV;
-  for (int i = 0; i < FQ * NV; ++i) out[i] = 0.0;
-  double u0[NV], pm[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
-  cons2prim(p.gamma, u0, pm);
-  auto nq_of = [&](int f) { return f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0; };
-  auto mono = [&](int f, int q, double (&m)[ID]) {
-    const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
-    monomials<P, double>(xi[0], xi[32], xi[64], m);
-  };
-  if (!p.full[c]) {
-    atomicOr(flag, 1);
-    return;
-  }
-  const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
-  const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
-  const bool cw = p.ees == 5;
-  const int ID2 = p.ideg2;
-  constexpr int L2 = ID < 9 ? ID : 9;
-  const double lc1 = 1.0 - 1.0 / p.lwci;
-  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-  auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
-  // IS = sum_d g_d t_d, t_d = sum_{e>=d} P_de g_e, and its tangent (product rule)
-  auto is_and_tangent = [&](const double* Pt, auto& g, auto& dg, int nd, double& a, double& da) {
-    constexpr int ND = sizeof(g) / sizeof(g[0]);
-    a = da = 0.0;
-    int rs = 0;
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      if (d < nd) {
-        double t = 0.0, dt = 0.0;
-#pragma unroll
-        for (int q = 0; q < (ND - d + VEC - 1) / VEC; ++q)
-          if (d + q * VEC < nd) {
-            double sv[VEC];
-            ldv(Pt + (int64_t)(rs + q) * 32 * VEC, sv);
-#pragma unroll
-            for (int i = 0; i < VEC; ++i) {
-              const int e = d + q * VEC + i;
-              if (e < ND && e < nd) {
-                t += sv[i] * g[e];
-                dt += sv[i] * dg[e];
-              }
-            }
-          }
-        rs += (nd - d + VEC - 1) / VEC;
-        a += g[d] * t;
-        da += dg[d] * t + g[d] * dt;
-        asm volatile("" ::: "memory");
-      }
-    }
-  };
-#pragma unroll 1
-  for (int v = 0; v < NV; ++v) {
+  if (c < p.n && !live)
+    for (int i = 0; i < FQ; ++i) tdul[(c * FQ + i) * NV + v] = 0.0;
+  if (live) {
+    const int adm = p.admis[c], nf = p.nfaces[c];
+    const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+    const double* dGc = dG + grp * (int64_t)(A * ID * NV) * 32 + lane;
+    auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+    auto dGv = [&](int ll, int d) -> double { return dGc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+    const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+    const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
+    const bool cw = p.ees == 5;
+    const int ID2 = p.ideg2;
+    constexpr int L2 = ID < 9 ? ID : 9;
+    const double lc1 = 1.0 - 1.0 / p.lwci;
+    const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+    auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
     double g3[L2], dg3[L2];
 #pragma unroll
     for (int d = 0; d < L2; ++d) g3[d] = dg3[d] = 0.0;
@@ -441,39 +394,39 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
 #pragma unroll
         for (int d = 0; d < L2; ++d)
           if (d < ID2) {
-            g3[d] = g3[d] + lk * G(l2, d, v);
-            dg3[d] = dg3[d] + lk * dGv(l2, d, v);
+            g3[d] = g3[d] + lk * G(l2, d);
+            dg3[d] = dg3[d] + lk * dGv(l2, d);
           }
     auto poly = [&](int ll, int d) -> double {
       if (d >= nd_of(ll)) return 0.0;
-      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d, v) - (d < L2 ? g3[d] : 0.0));
-      return G(ll, d, v);
+      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d) - (d < L2 ? g3[d] : 0.0));
+      return G(ll, d);
     };
     auto dpoly = [&](int ll, int d) -> double {
       if (d >= nd_of(ll)) return 0.0;
-      if (cw && ll == 0) return (1.0 / lc1) * (dGv(0, d, v) - (d < L2 ? dg3[d] : 0.0));
-      return dGv(ll, d, v);
+      if (cw && ll == 0) return (1.0 / lc1) * (dGv(0, d) - (d < L2 ? dg3[d] : 0.0));
+      return dGv(ll, d);
     };
     double is[7], dis[7], wt[7], dwt[7];
     double sum = 0.0, dsum = 0.0;
+#pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
-      double a, da;
+      // IS = g^T S g and dIS = dg . (2 S g)
+      double a, da = 0.0;
       if (cw && ll > 0) {
-        double g[L2], dg[L2];
+        double g[L2], gr[L2];
 #pragma unroll
-        for (int d = 0; d < L2; ++d) {
-          g[d] = poly(ll, d);
-          dg[d] = dpoly(ll, d);
-        }
-        is_and_tangent(Pc2, g, dg, ID2, a, da);
+        for (int d = 0; d < L2; ++d) g[d] = poly(ll, d);
+        a = is_and_grad<L2>(Pc2, g, ID2, gr);
+#pragma unroll
+        for (int d = 0; d < L2; ++d) da += dpoly(ll, d) * gr[d];
       } else {
-        double g[ID], dg[ID];
+        double g[ID], gr[ID];
 #pragma unroll
-        for (int d = 0; d < ID; ++d) {
-          g[d] = poly(ll, d);
-          dg[d] = dpoly(ll, d);
-        }
-        is_and_tangent(Pc, g, dg, ID, a, da);
+        for (int d = 0; d < ID; ++d) g[d] = poly(ll, d);
+        a = is_and_grad<ID>(Pc, g, ID, gr);
+#pragma unroll
+        for (int d = 0; d < ID; ++d) da += dpoly(ll, d) * gr[d];
       }
       is[ll] = a;
       dis[ll] = da;
@@ -485,54 +438,47 @@ __global__ void __launch_bounds__(64) k_jvp_wpost(Problem p, const double* __res
       sum += wt[ll];
       dsum += dwt[ll];
     }
-    double td[ID], gh[ID];
+    // tangent and value of the combined polynomial (the value in shared
+    // memory, for CHECKSOL)
+    double td[ID];
 #pragma unroll
-    for (int d = 0; d < ID; ++d) td[d] = gh[d] = 0.0;
+    for (int d = 0; d < ID; ++d) {
+      td[d] = 0.0;
+      sGH[d][v][lane] = 0.0;
+    }
+#pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       const double om = wt[ll] / sum;
       const double dom = (dwt[ll] - om * dsum) / sum;
 #pragma unroll
       for (int d = 0; d < ID; ++d) {
         const double gd = poly(ll, d);
-        td[d] = (ll == 0 ? 0.0 : td[d]) + (dom * gd + om * dpoly(ll, d));
-        gh[d] = (ll == 0 ? 0.0 : gh[d]) + om * gd;
+        td[d] += dom * gd + om * dpoly(ll, d);
+        sGH[d][v][lane] += om * gd;
+        if ((d & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
       }
     }
+    double tb = 0.0;
 #pragma unroll
-    for (int d = 0; d < ID; ++d) {
-      TD(d, v) = td[d];
-      GH(d, v) = gh[d];
-    }
-  }
-  double cb[NV], tb[NV];
+    for (int d = 0; d < ID; ++d) tb += bmv[d * 32] * td[d];
+    for (int f = 0; f < MF; ++f) {
+      const int nq = f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0;
+      for (int q = 0; q < QS; ++q) {
+        double t = 0.0;
+        if (q < nq) {
+          const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+          double m[ID];
+          monomials<P, double>(xi[0], xi[32], xi[64], m);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    cb[v] = tb[v] = 0.0;
-#pragma unroll
-    for (int d = 0; d < ID; ++d) {
-      cb[v] += bmv[d * 32] * GH(d, v);
-      tb[v] += bmv[d * 32] * TD(d, v);
-    }
-  }
-  bool bad = false;
-  for (int f = 0; f < nf; ++f)
-    for (int q = 0; q < nq_of(f); ++q) {
-      double m[ID], uf[NV];
-      mono(f, q, m);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        double r = 0.0, t = 0.0;
-#pragma unroll
-        for (int d = 0; d < ID; ++d) {
-          r += m[d] * GH(d, v);
-          t += m[d] * TD(d, v);
+          for (int d = 0; d < ID; ++d) t += m[d] * td[d];
+          t -= tb;
         }
-        uf[v] = u0[v] + (r - cb[v]);
-        out[(f * QS + q) * NV + v] = t - tb[v];
+        tdul[(c * FQ + f * QS + q) * NV + v] = t;
       }
-      bad = bad || jump_bad(p.gamma, pm, uf, 0.85);
     }
-  if (bad) atomicOr(flag, 1);
+  }
+  __syncthreads();
+  if (live && checksol_split<P>(p, U, c, p.nfaces[c], xq, bmv, sGH, lane, v)) atomicOr(flag, 1);
 }
 
 template <int P>
@@ -543,22 +489,21 @@ void launch_t(const Problem& p, const double* U, const double* adjF, double* gba
 }
 
 template <int P>
-void launch_jvp_t(const Problem& p, const double* U, const double* dG, double* scr, double* tdul, int* flag,
-                  cudaStream_t st) {
-  k_jvp_wpost<P><<<(unsigned)((p.n + 63) / 64), 64, 0, st>>>(p, U, dG, scr, tdul, flag);
+void launch_jvp_t(const Problem& p, const double* U, const double* dG, double* tdul, int* flag, cudaStream_t st) {
+  k_jvp_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, dG, tdul, flag);
 }
 
 }  // namespace
 
 namespace ucg_host {
 
-int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dG, double* scr,
-                        double* tdul, int* flag) {
+int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dG, double* tdul,
+                        int* flag) {
   switch (e->cfg.iorder) {
-    case 1: launch_jvp_t<1>(p, U, dG, scr, tdul, flag, e->stream); break;
-    case 2: launch_jvp_t<2>(p, U, dG, scr, tdul, flag, e->stream); break;
-    case 3: launch_jvp_t<3>(p, U, dG, scr, tdul, flag, e->stream); break;
-    case 4: launch_jvp_t<4>(p, U, dG, scr, tdul, flag, e->stream); break;
+    case 1: launch_jvp_t<1>(p, U, dG, tdul, flag, e->stream); break;
+    case 2: launch_jvp_t<2>(p, U, dG, tdul, flag, e->stream); break;
+    case 3: launch_jvp_t<3>(p, U, dG, tdul, flag, e->stream); break;
+    case 4: launch_jvp_t<4>(p, U, dG, tdul, flag, e->stream); break;
     default: return fail(e, UCG_EINVAL, "iorder out of range");
   }
   e->launches++;

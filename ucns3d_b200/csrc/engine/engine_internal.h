@@ -95,7 +95,7 @@ void adjoint_release(ucg_engine* e);
 int launch_weno_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, const double* adjF, double* gbar,
                         double* scr, double* selfc, double* contrib, int* flag);
 // tangent of the WENO face values from the tangent stencil polynomials dG
-int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dG, double* scr,
-                        double* tdul, int* flag);
+int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dG, double* tdul,
+                        int* flag);
 
 }  // namespace ucg_host
