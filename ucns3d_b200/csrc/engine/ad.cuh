@@ -176,22 +176,22 @@ __host__ __device__ __forceinline__ Dual<N> fmax(const Dual<N>& a, double b) {
 __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const double* cr, const double* fb,
                                          double* clb, double* crb) {
   const double g1 = gamma - 1.0;
-  // ---- forward
-  const double rl = cl[0], ul = cl[1] / rl, vl = cl[2] / rl, wl = cl[3] / rl;
+  // ---- forward (reciprocals formed once: 9 divisions in all)
+  const double rl = cl[0], irl = 1.0 / rl, ul = cl[1] * irl, vl = cl[2] * irl, wl = cl[3] * irl;
   const double kl = ul * ul + vl * vl + wl * wl;
   const double pl = g1 * (cl[4] - 0.5 * rl * kl);
-  const double rr = cr[0], ur = cr[1] / rr, vr = cr[2] / rr, wr = cr[3] / rr;
+  const double rr = cr[0], irr = 1.0 / rr, ur = cr[1] * irr, vr = cr[2] * irr, wr = cr[3] * irr;
   const double kr = ur * ur + vr * vr + wr * wr;
   const double pr = g1 * (cr[4] - 0.5 * rr * kr);
   const double el = cl[4], er = cr[4];
-  const double ccl = ::sqrt(gamma * pl / rl), ccr = ::sqrt(gamma * pr / rr);
-  const double srl = ::sqrt(rl), srr = ::sqrt(rr), ssum = srl + srr;
+  const double ccl = ::sqrt(gamma * pl * irl), ccr = ::sqrt(gamma * pr * irr);
+  const double srl = ::sqrt(rl), srr = ::sqrt(rr), ssum = srl + srr, issum = 1.0 / ssum;
   const double du = ur - ul;
   const double T1 = ccl * ccl * srl + ccr * ccr * srr;
-  const double P = (srl * srr) / (ssum * ssum);
-  const double q = T1 / ssum + 0.5 * P * (du * du);
+  const double P = (srl * srr) * (issum * issum);
+  const double q = T1 * issum + 0.5 * P * (du * du);
   const double cc2 = ::sqrt(q);
-  const double uu2 = (ul * srl + ur * srr) / ssum;
+  const double uu2 = (ul * srl + ur * srr) * issum;
   // sl = min(min(ul - ccl, uu2 - cc2), 0): which term
   const double sl1 = ul - ccl, sl2 = uu2 - cc2;
   const double slm = sl2 < sl1 ? sl2 : sl1;
@@ -203,7 +203,8 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
   const double sr = srb == 0 ? 0.0 : srm;
   const double num = pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur);
   const double den = rl * (sl - ul) - rr * (sr - ur);
-  const double sm = num / den;
+  const double iden = 1.0 / den;
+  const double sm = num * iden;
   const bool left = copysign(1.0, sm) > 0.0;
   // ---- backward: adjoints of the intermediates
   double rlb = 0, ulb = 0, vlb = 0, wlb = 0, plb = 0, elb = 0;
@@ -215,11 +216,14 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
     const double ps = left ? pl : pr, es = left ? el : er, s = left ? sl : sr;
     const double* cs = left ? cl : cr;
     double* csb = left ? clb : crb;
+    const double irs = left ? irl : irr;
     const double Bq = rs * (s - us);            // rho (s - u)
+    const double iBq = 1.0 / Bq;
     const double D1 = s - sm;
-    const double mus = Bq / D1;                 // star density factor
-    const double A = sm - us, Bt = sm + ps / Bq;
-    const double lasts = es / rs + A * Bt;
+    const double iD1 = 1.0 / D1;
+    const double mus = Bq * iD1;                // star density factor
+    const double A = sm - us, Bt = sm + ps * iBq;
+    const double lasts = es * irs + A * Bt;
     const double fs0 = rs * us;
     double rsb = 0, usb = 0, vsb = 0, wsb = 0, psb = 0, esb = 0, sb = 0;
     // F0 = fs0 + s (mus - c0); F1 = fs0 us + ps + s (mus sm - c1);
@@ -245,17 +249,17 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
     rsb += fs0b * us;
     usb += fs0b * rs;
     // lasts = es/rs + A Bt, A = sm - us, Bt = sm + ps/Bq
-    esb += lastb / rs;
-    rsb -= lastb * es / (rs * rs);
+    esb += lastb * irs;
+    rsb -= lastb * es * (irs * irs);
     const double Ab = lastb * Bt, Btb = lastb * A;
     smb += Ab;
     usb -= Ab;
     smb += Btb;
-    psb += Btb / Bq;
-    double Bqb = -Btb * ps / (Bq * Bq);
+    psb += Btb * iBq;
+    double Bqb = -Btb * ps * (iBq * iBq);
     // mus = Bq / D1, D1 = s - sm
-    Bqb += musb / D1;
-    const double D1b = -musb * Bq / (D1 * D1);
+    Bqb += musb * iD1;
+    const double D1b = -musb * Bq * (iD1 * iD1);
     sb += D1b;
     smb -= D1b;
     // Bq = rs (s - us)
@@ -269,7 +273,7 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
     }
   }
   // sm = num / den
-  const double numb = smb / den, denb = -smb * num / (den * den);
+  const double numb = smb * iden, denb = -smb * num * (iden * iden);
   prb += numb;
   plb -= numb;
   rlb += numb * ul * (sl - ul);
@@ -302,21 +306,22 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
   }
   // uu2 = (ul srl + ur srr) / ssum
   double srlb = 0, srrb = 0, ssumb = 0;
-  const double Xb = uu2b / ssum;
-  ssumb -= uu2b * uu2 / ssum;
+  const double Xb = uu2b * issum;
+  ssumb -= uu2b * uu2 * issum;
   ulb += Xb * srl;
   srlb += Xb * ul;
   urb += Xb * srr;
   srrb += Xb * ur;
   // cc2 = sqrt(q), q = T1/ssum + 0.5 P du^2
-  const double qb = cc2b / (2.0 * cc2);
-  const double T1b = qb / ssum;
-  ssumb -= qb * T1 / (ssum * ssum);
+  const double qb = cc2b * (0.5 / cc2);
+  const double T1b = qb * issum;
+  const double is2 = issum * issum;
+  ssumb -= qb * T1 * is2;
   const double Pb = qb * 0.5 * du * du;
   const double dub = qb * P * du;
-  srlb += Pb * srr / (ssum * ssum);
-  srrb += Pb * srl / (ssum * ssum);
-  ssumb -= Pb * 2.0 * srl * srr / (ssum * ssum * ssum);
+  srlb += Pb * srr * is2;
+  srrb += Pb * srl * is2;
+  ssumb -= Pb * 2.0 * srl * srr * (is2 * issum);
   urb += dub;
   ulb -= dub;
   cclb += T1b * 2.0 * ccl * srl;
@@ -325,16 +330,16 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
   srrb += T1b * ccr * ccr;
   srlb += ssumb;
   srrb += ssumb;
-  rlb += srlb / (2.0 * srl);
-  rrb += srrb / (2.0 * srr);
+  rlb += srlb * (0.5 * srl * irl);  // 1 / (2 sqrt(rl)) = sqrt(rl) / (2 rl)
+  rrb += srrb * (0.5 * srr * irr);
   // ccl = sqrt(gamma pl / rl)
   {
-    const double zb = cclb / (2.0 * ccl);
-    plb += zb * gamma / rl;
-    rlb -= zb * gamma * pl / (rl * rl);
-    const double zr = ccrb / (2.0 * ccr);
-    prb += zr * gamma / rr;
-    rrb -= zr * gamma * pr / (rr * rr);
+    const double zb = cclb * (0.5 / ccl);
+    plb += zb * gamma * irl;
+    rlb -= zb * gamma * pl * (irl * irl);
+    const double zr = ccrb * (0.5 / ccr);
+    prb += zr * gamma * irr;
+    rrb -= zr * gamma * pr * (irr * irr);
   }
   // pl = g1 (el - 0.5 rl kl), el = cl[4]
   elb += plb * g1;
@@ -350,16 +355,16 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
   vrb += krb * 2.0 * vr;
   wrb += krb * 2.0 * wr;
   // ul = cl1 / rl, ...; rl = cl0, el = cl4
-  clb[1] += ulb / rl;
-  clb[2] += vlb / rl;
-  clb[3] += wlb / rl;
-  rlb -= (ulb * ul + vlb * vl + wlb * wl) / rl;
+  clb[1] += ulb * irl;
+  clb[2] += vlb * irl;
+  clb[3] += wlb * irl;
+  rlb -= (ulb * ul + vlb * vl + wlb * wl) * irl;
   clb[0] += rlb;
   clb[4] += elb;
-  crb[1] += urb / rr;
-  crb[2] += vrb / rr;
-  crb[3] += wrb / rr;
-  rrb -= (urb * ur + vrb * vr + wrb * wr) / rr;
+  crb[1] += urb * irr;
+  crb[2] += vrb * irr;
+  crb[3] += wrb * irr;
+  rrb -= (urb * ur + vrb * vr + wrb * wr) * irr;
   crb[0] += rrb;
   crb[4] += erb;
 }

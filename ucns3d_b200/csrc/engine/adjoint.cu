@@ -151,7 +151,7 @@ __device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* 
 // (ad::hllc_adj) in the face frame at every face point.  The rotations are
 // orthogonal (rot_b = rot_f^T), and a mirror ghost is b = S a in the face
 // frame (S flips the normal momentum).
-__global__ void __launch_bounds__(128) k_adj_face(Problem p, int64_t nplain, const double* __restrict__ U,
+__global__ void __launch_bounds__(64) k_adj_face(Problem p, int64_t nplain, const double* __restrict__ U,
                                                   const double* __restrict__ lam, double* __restrict__ adjF) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nplain) return;
@@ -875,7 +875,7 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
   const int64_t n = e->n;
   const int64_t nplain = e->nown_plain, nbnd = e->nown - nplain;
   if (nplain)
-    k_adj_face<<<blocks_for(nplain, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p);
+    k_adj_face<<<blocks_for(nplain, 64), 64, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p);
   if (nbnd)
     k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p,
                                                                       (double*)e->adj_pface.p);
@@ -1023,7 +1023,7 @@ int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   if (rc) return rc;
   const int64_t n = e->n, nplain = e->nown_plain, nbnd = e->nown - nplain;
   double* adjF = (double*)e->adjw_face.p;
-  if (nplain) k_adj_face<<<blocks_for(nplain, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF);
+  if (nplain) k_adj_face<<<blocks_for(nplain, 64), 64, 0, e->stream>>>(p, nplain, U, lam, adjF);
   if (nbnd)
     k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF,
                                                                       (double*)e->adjw_pface.p);
