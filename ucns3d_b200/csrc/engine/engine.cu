@@ -151,8 +151,14 @@ int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
   const ucg_config& c = e->cfg;
   if (c.scheme == 2 && c.iorder == 1) {
     unsigned blocks = (unsigned)((e->n + 127) / 128);
-    if (c.governing == 1) k_muscl<T, true><<<blocks, 128, 0, e->stream>>>(p, U);
-    else k_muscl<T, false><<<blocks, 128, 0, e->stream>>>(p, U);
+    const bool vk = c.limiter == 7;
+    if (c.governing == 1) {
+      if (vk) k_muscl<T, true, true><<<blocks, 128, 0, e->stream>>>(p, U);
+      else k_muscl<T, true, false><<<blocks, 128, 0, e->stream>>>(p, U);
+    } else {
+      if (vk) k_muscl<T, false, true><<<blocks, 128, 0, e->stream>>>(p, U);
+      else k_muscl<T, false, false><<<blocks, 128, 0, e->stream>>>(p, U);
+    }
     e->launches++;
     CK(cudaGetLastError());
     return UCG_OK;

@@ -13,8 +13,10 @@ namespace ucg {
 // LEAST_SQUARES (gradients.f90:253-497), MUSCL + Venkatakrishnan
 // (reconstruct_p.f90:2286, 1821, 2044, 3421), CHECKSOLX (3245), and for
 // Navier-Stokes the viscous LSQ (gradients.f90:502-706) + SOLUTIONTRIAV2.
+// VK: the limiter is Venkatakrishnan (LIMITER 7) inline; otherwise the
+// SLOPE_LIMITERS code of the configuration, chosen at run time.
 // ======================================================================
-template <typename T, bool NS>
+template <typename T, bool NS, bool VK>
 __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restrict__ U) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
@@ -96,7 +98,8 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
   for (int f = 0; f < nf; ++f)
 #pragma unroll
     for (int v = 0; v < NV; ++v)
-      slope[v] = fmin(slope[v], slope_limiter(p.limiter, face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2));
+      slope[v] = fmin(slope[v], VK ? venkat(face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2)
+                                   : slope_limiter(p.limiter, face_d(f, v), umin[v] - u0[v], umax[v] - u0[v], epsi2));
   // limited face values and CHECKSOLX
   bool first = false;
   for (int f = 0; f < nf; ++f) {
