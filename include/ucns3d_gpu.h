@@ -235,8 +235,8 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
  * Discrete adjoint (VJP) and tangent (JVP) for the FP64 form of a MUSCL
  * (scheme 2, IORDER 1) Euler configuration (the adjoint workload is the
  * bump channel).  ucg_residual_vjp and ucg_residual_jvp also cover
- * conserved-variable WENO and CWENO (scheme 3, EES 0 or 5 without WENO-Z,
- * HLLC, Euler, FP64 form): the
+ * conserved-variable WENO and CWENO (scheme 3, EES 0 or 5, CWENO with or
+ * without WENO-Z, HLLC, Euler, FP64 form): the
  * reverse/tangent of the nonlinear weights, smoothness indicators and
  * stencil least squares; a cell on the MUSCL fall-back (FULL = 0 or
  * CHECKSOL) makes them return UCG_EINVAL.  p denotes the free-stream state bc_state[5] (primitive:

@@ -217,23 +217,23 @@ def test_torch_autograd_function(bump):
     e.set_state(U)
 
 
-@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex", "cweno4_tet"])
+@pytest.mark.parametrize("name", ["weno3_tet", "weno5_hex", "cweno4_tet", "cweno4_tet_wenoz"])
 def test_weno_vjp_matches_oracle_fd(name):
-    """VJP and JVP of the WENO and CWENO residuals (nonlinear weights,
-    smoothness indicators, stencil least squares, HLLC at every face point) against
-    central differences of the oracle's FP64 residual, and the dot-product
-    test between them, on periodic meshes whose cells are all on the WENO
-    branch."""
+    """VJP and JVP of the WENO and CWENO residuals (nonlinear weights, WENO-Z
+    weights for CWENO, smoothness indicators, stencil least squares, HLLC at
+    every face point) against central differences of the oracle's FP64
+    residual, and the dot-product test between them, on periodic meshes
+    whose cells are all on the WENO branch."""
     from oracle import Oracle
     from ucns3d_b200.config import make_config
     from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
     if name == "weno3_tet":
         m = Mesh.box_tet(5, 5, 5, seed=3).prepare(SCHEME_WENO, 2)
-    elif name == "cweno4_tet":
+    elif name.startswith("cweno4_tet"):
         m = Mesh.box_tet(5, 5, 5, seed=5).prepare(SCHEME_WENO, 3, 5)
     else:
         m = Mesh.box_hex(10, 10, 10).prepare(SCHEME_WENO, 4)
-    cfg = make_config(m, governing=2)
+    cfg = make_config(m, governing=2, wenoz=int(name.endswith("wenoz")))
     U = m.initial_condition(IC_TGV, [1.4, 5.0, 1.0])
     rng = np.random.default_rng(12)
     cc = m.centres()
@@ -244,6 +244,9 @@ def test_weno_vjp_matches_oracle_fd(name):
     mu, pbar = e.residual_vjp(lam)
     assert np.all(pbar == 0.0)  # periodic: no free-stream dependence
     o = Oracle(m, cfg)
+    if name.endswith("wenoz"):  # the WENO-Z weights give another residual
+        R0 = Oracle(m, make_config(m, governing=2)).residual(U)
+        assert np.abs(o.residual(U) - R0).max() > 1e-8 * np.abs(R0).max()
     eps = 1e-6
     for trial in range(2):
         du = rng.standard_normal(U.shape) * np.abs(U).max(0) * 1e-2

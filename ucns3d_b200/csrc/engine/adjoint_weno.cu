@@ -1,5 +1,5 @@
 // Discrete adjoint (VJP) of the WENO and CWENO reconstruction (conserved
-// variables, EES 0 or 5 without WENO-Z, FP64 form): the reverse of CP_RECONSTRUCTION's nonlinear weights
+// variables, EES 0 or 5, CWENO with or without WENO-Z, FP64 form): the reverse of CP_RECONSTRUCTION's nonlinear weights
 // and smoothness indicators (src/reconstruct_p.f90:920-1250) and of the
 // stencil least squares (LEAST_SQUARES, src/gradients.f90:253-497).
 //
@@ -209,7 +209,6 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
       return G(ll, d);
     };
     double is[7], wt[7], om[7], omb[7];
-    double sum = 0.0;
 #pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       double s;
@@ -230,10 +229,26 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
         for (int d = 0; d < ID; ++d) GB(ll, d) = gr[d];
       }
       is[ll] = s;
-      const double e = p.weno_eps + s;
-      const double e2 = e * e;
+    }
+    // weights: lam / (eps + IS)^4, or WENO-Z (CWENO only)
+    // lam (1 + (tau / (eps + IS))^4) with tau = sum_l |IS_0 - IS_l| / (adm - 1)
+    const bool wz = cw && p.wenoz;
+    double tau = 0.0, sum = 0.0;
+    if (wz) {
+      for (int ll = 0; ll < adm; ++ll) tau += fabs(is[0] - is[ll]);
+      tau = tau / (adm - 1);
+    }
+    for (int ll = 0; ll < adm; ++ll) {
+      const double e = p.weno_eps + is[ll];
       const double lam = cw ? (ll == 0 ? lc1 : lk) : (ll == 0 ? p.lwci : 1.0);
-      wt[ll] = lam / (e2 * e2);
+      if (wz) {
+        double q = tau / e;
+        q = q * q;
+        wt[ll] = lam * (1.0 + q * q);
+      } else {
+        const double e2 = e * e;
+        wt[ll] = lam / (e2 * e2);
+      }
       sum += wt[ll];
     }
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
@@ -258,10 +273,29 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
     double corr[L2];
 #pragma unroll
     for (int d = 0; d < L2; ++d) corr[d] = 0.0;
+    // WENO-Z: wt_l = lam_l (1 + q_l^4), q_l = tau / (eps + IS_l):
+    // d wt_l / d tau = 4 (wt_l - lam_l) / tau, d wt_l / d IS_l = -4 (wt_l - lam_l) / (eps + IS_l);
+    // tau's adjoint goes back to the IS through sign(IS_0 - IS_l) / (adm - 1)
+    double taub = 0.0;
+    if (wz && tau > 0.0)
+      for (int ll = 0; ll < adm; ++ll) {
+        const double lam = ll == 0 ? lc1 : lk;
+        taub += (omb[ll] - dot) / sum * 4.0 * (wt[ll] - lam) / tau;
+      }
+    double tsg = 0.0;  // sum_l sign(IS_0 - IS_l)
+    if (wz)
+      for (int ll = 1; ll < adm; ++ll) tsg += is[0] > is[ll] ? 1.0 : (is[0] < is[ll] ? -1.0 : 0.0);
 #pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       const double wtb = (omb[ll] - dot) / sum;
-      const double isb = wtb * (-4.0 * wt[ll] / (p.weno_eps + is[ll]));
+      double isb;
+      if (wz) {
+        const double lam = ll == 0 ? lc1 : lk;
+        const double sg = ll == 0 ? tsg : (is[0] > is[ll] ? -1.0 : (is[0] < is[ll] ? 1.0 : 0.0));
+        isb = wtb * (-4.0 * (wt[ll] - lam) / (p.weno_eps + is[ll])) + taub * sg / (adm - 1);
+      } else {
+        isb = wtb * (-4.0 * wt[ll] / (p.weno_eps + is[ll]));
+      }
       if (cw && ll > 0) {
 #pragma unroll
         for (int d = 0; d < L2; ++d)
@@ -408,7 +442,6 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem 
       return dGv(ll, d);
     };
     double is[7], dis[7], wt[7], dwt[7];
-    double sum = 0.0, dsum = 0.0;
 #pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       // IS = g^T S g and dIS = dg . (2 S g)
@@ -430,11 +463,32 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem 
       }
       is[ll] = a;
       dis[ll] = da;
-      const double e = p.weno_eps + a;
-      const double e2 = e * e;
+    }
+    // weights and their tangents (WENO-Z: wt = lam (1 + (tau / e)^4),
+    // dwt = 4 (wt - lam) (dtau / tau - dIS / e))
+    const bool wz = cw && p.wenoz;
+    double tau = 0.0, dtau = 0.0, sum = 0.0, dsum = 0.0;
+    if (wz) {
+      for (int ll = 1; ll < adm; ++ll) {
+        tau += fabs(is[0] - is[ll]);
+        dtau += (is[0] > is[ll] ? 1.0 : (is[0] < is[ll] ? -1.0 : 0.0)) * (dis[0] - dis[ll]);
+      }
+      tau = tau / (adm - 1);
+      dtau = dtau / (adm - 1);
+    }
+    for (int ll = 0; ll < adm; ++ll) {
+      const double e = p.weno_eps + is[ll];
       const double lam = cw ? (ll == 0 ? lc1 : lk) : (ll == 0 ? p.lwci : 1.0);
-      wt[ll] = lam / (e2 * e2);
-      dwt[ll] = -4.0 * wt[ll] * dis[ll] / e;
+      if (wz) {
+        double q = tau / e;
+        q = q * q;
+        wt[ll] = lam * (1.0 + q * q);
+        dwt[ll] = 4.0 * (wt[ll] - lam) * ((tau > 0.0 ? dtau / tau : 0.0) - dis[ll] / e);
+      } else {
+        const double e2 = e * e;
+        wt[ll] = lam / (e2 * e2);
+        dwt[ll] = -4.0 * wt[ll] * dis[ll] / e;
+      }
       sum += wt[ll];
       dsum += dwt[ll];
     }
