@@ -264,18 +264,45 @@ def test_weno_vjp_matches_oracle_fd(name):
     e.close()
 
 
-def test_weno_vjp_rejects_the_muscl_fall_back():
-    """Cells next to the channel walls are not FULL (they take the MUSCL
-    fall-back), which the WENO adjoint does not cover."""
+@pytest.mark.parametrize("order,ees", [(2, 0), (3, 5)])
+def test_weno_adjoint_with_muscl_fall_back(order, ees):
+    """WENO3 and CWENO4 on the bump channel (slip walls, inflow/outflow):
+    the cells next to the boundaries are not FULL and take the MUSCL
+    fall-back (the central stencil polynomial limited by Venkatakrishnan
+    with FIND_BOUNDS over the face neighbours), others may fail CHECKSOL.
+    VJP and JVP in the state and the free-stream state against central
+    differences of the oracle's FP64 residual, and the dot-product test."""
+    from oracle import Oracle
     from ucns3d_b200.config import make_config
     from ucns3d_b200.mesh import SCHEME_WENO, Mesh
-    m = Mesh.bump_channel(16, 8, 8, seed=2).prepare(SCHEME_WENO, 2)
-    cfg = make_config(m, governing=2, bc_state=(1.0, 0.8, 0.0, 0.0, 1.0))
+    m = Mesh.bump_channel(16, 8, 8, seed=2).prepare(SCHEME_WENO, order, ees)
+    g = m.geometry_struct()
+    full = np.ctypeslib.as_array(g.full, shape=(m.ncells,))
+    assert 0 < full.sum() < m.ncells  # both branches present
+    bc = np.array([1.0, 0.8, 0.0, 0.0, 1.0])
+    cfg = make_config(m, governing=2, bc_state=tuple(bc))
+    rng = np.random.default_rng(17)
+    cc = m.centres()
+    U = np.tile([1.0, 0.8, 0.0, 0.0, 1.0 / 0.4 + 0.32], (m.ncells, 1))
+    U = U * (1.0 + 0.03 * np.sin(3.1 * cc[:, :1] + 1.7 * cc[:, 1:2] + 9.0 * cc[:, 2:3] + rng.uniform(0, 6.3, (1, 5))))
     e = Engine(m, cfg)
-    e.set_state(np.tile([1.0, 0.8, 0.0, 0.0, 1.0 / 0.4 + 0.32], (m.ncells, 1)))
-    with pytest.raises(EngineError) as ei:
-        e.residual_vjp(np.ones((m.ncells, 5)))
-    assert ei.value.code == N.UCG_EINVAL
+    e.set_state(U)
+    lam = rng.standard_normal(U.shape)
+    mu, pbar = e.residual_vjp(lam)
+    eps = 1e-6
+    for trial in range(2):
+        du, dp = _directions(U, 30 + trial)
+        fdv = (Oracle(m, _cfg_with_bc(cfg, bc + eps * dp)).residual(U + eps * du) -
+               Oracle(m, _cfg_with_bc(cfg, bc - eps * dp)).residual(U - eps * du)) / (2 * eps)
+        fd = float(np.sum(lam * fdv))
+        ad = float(np.sum(mu * du) + np.sum(pbar * dp))
+        assert abs(ad - fd) <= 1e-6 * abs(fd), (trial, ad, fd)
+        jvp = e.residual_jvp(du, dp)
+        err = (np.abs(jvp - fdv) / (np.abs(fdv).max(0) + 1e-300)).max()
+        print(f"order {order} ees {ees}: WENO JVP vs oracle differences {err:.2e}")
+        assert err < 1e-6
+        a = float(np.sum(lam * jvp))
+        assert abs(a - ad) <= 1e-12 * np.abs(lam * jvp).sum(), (a, ad)
     e.close()
 
 

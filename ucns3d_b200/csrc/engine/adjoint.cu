@@ -777,7 +777,7 @@ void adjoint_release(ucg_engine* e) {
                                &e->adj_mu,     &e->adj_pface,   &e->adj_tflux, &e->adj_tdul,     &e->adj_tU,
                                &e->adj_fcell,  &e->adj_traj,    &e->adj_bar,   &e->adj_tmp,      &e->adj_fwd,
                                &e->adjw_face,  &e->adjw_gbar,   &e->adjw_scr,  &e->adjw_self,    &e->adjw_contrib,
-                               &e->adjw_rptr,  &e->adjw_rsrc,   &e->adjw_flag, &e->adjw_lam,     &e->adjw_mu,
+                               &e->adjw_rptr,  &e->adjw_rsrc,   &e->adjw_lam,     &e->adjw_mu,
                                &e->adjw_pface, &e->adjw_tmp};
   for (auto* b : all) {
     if (b->p) e->bytes -= (int64_t)b->bytes;
@@ -963,7 +963,9 @@ int adjw_setup(ucg_engine* e) {
   const int IM2 = c.imax2;
   // slots: the cell, the central stencil's members, then the others' (CWENO:
   // IMAX2 members each)
-  const int64_t slots = cw ? 1 + IM + (int64_t)(A - 1) * IM2 : 1 + (int64_t)A * IM;
+  // and one per face: the neighbour that set a bound of the MUSCL fall-back
+  const int64_t fslot = cw ? 1 + IM + (int64_t)(A - 1) * IM2 : 1 + (int64_t)A * IM;
+  const int64_t slots = fslot + MF;
   cudaSetDevice(e->device);
   // the stencils, back from the device (interleaved over 32-cell groups)
   std::vector<int32_t> st((size_t)ngrp * 32 * A * W);
@@ -971,6 +973,7 @@ int adjw_setup(ucg_engine* e) {
   CK(cudaStreamSynchronize(e->stream));
   auto target = [&](int64_t i, int64_t s) -> int64_t {
     if (s == 0) return i;
+    if (s >= fslot) return e->neigh_h[(size_t)i * MF + (s - fslot)];
     int ll, k;
     if (!cw || s - 1 < IM) {
       ll = (int)((s - 1) / IM);
@@ -1003,7 +1006,6 @@ int adjw_setup(ucg_engine* e) {
   rc = rc ? rc : get(e->adjw_contrib, (size_t)n * slots * NV * 8);
   rc = rc ? rc : get(e->adjw_rptr, (size_t)(n + 1) * 8);
   rc = rc ? rc : get(e->adjw_rsrc, (size_t)std::max<int64_t>(1, cnt[n]) * 8);
-  rc = rc ? rc : get(e->adjw_flag, 64);
   rc = rc ? rc : get(e->adjw_lam, (size_t)n * NV * 8);
   rc = rc ? rc : get(e->adjw_mu, (size_t)n * NV * 8 + 64 * 8);
   rc = rc ? rc : get(e->adjw_pface, (size_t)std::max<int64_t>(1, e->nown - e->nown_plain) * NV * 8);
@@ -1028,9 +1030,8 @@ int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const doub
     k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF,
                                                                       (double*)e->adjw_pface.p);
   e->launches += (nplain > 0) + (nbnd > 0);
-  CK(cudaMemsetAsync(e->adjw_flag.p, 0, sizeof(int), e->stream));
   if ((rc = launch_weno_adjoint(e, p, U, adjF, (double*)e->adjw_gbar.p, (double*)e->adjw_scr.p,
-                                (double*)e->adjw_self.p, (double*)e->adjw_contrib.p, (int*)e->adjw_flag.p)))
+                                (double*)e->adjw_self.p, (double*)e->adjw_contrib.p)))
     return rc;
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adjw_rptr.p,
                                                           (const int64_t*)e->adjw_rsrc.p,
@@ -1046,10 +1047,6 @@ int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const doub
     CK(cudaMemsetAsync(psum, 0, NV * sizeof(double), e->stream));
   }
   CK(cudaGetLastError());
-  int flag = 0;
-  CK(cudaMemcpyAsync(&flag, e->adjw_flag.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
-  if (flag) return fail(e, UCG_EINVAL, "a cell is on the MUSCL fall-back (FULL = 0 or CHECKSOL), which the WENO adjoint does not cover");
   return UCG_OK;
 }
 
@@ -1061,19 +1058,13 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   pt.gbuf = e->adjw_gbar.p;  // dG = least squares of dU
   CK(launch_lsq_f64(e->cfg.iorder, pt, dU, e->stream));
   e->launches++;
-  CK(cudaMemsetAsync(e->adjw_flag.p, 0, sizeof(int), e->stream));
   double* tdul = (double*)e->adjw_face.p;
   double* tflux = (double*)e->adjw_contrib.p;
-  if ((rc = launch_weno_tangent(e, p, U, (const double*)e->adjw_gbar.p, tdul, (int*)e->adjw_flag.p)))
-    return rc;
+  if ((rc = launch_weno_tangent(e, p, U, dU, (const double*)e->adjw_gbar.p, tdul))) return rc;
   k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux);
   k_jvp_sum<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, tflux, dR);
   e->launches += 2;
   CK(cudaGetLastError());
-  int flag = 0;
-  CK(cudaMemcpyAsync(&flag, e->adjw_flag.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
-  if (flag) return fail(e, UCG_EINVAL, "a cell is on the MUSCL fall-back (FULL = 0 or CHECKSOL), which the WENO tangent does not cover");
   return UCG_OK;
 }
 

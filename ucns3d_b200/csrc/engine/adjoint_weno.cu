@@ -15,10 +15,13 @@
 //   ISb_l   = -4 wtb_l wt_l / (eps + IS_l)
 //   Gb_l    = om_l Bb + ISb_l 2 S G_l
 //   U_c    += sum_x ub(x);  U_st(l,k) += M_l[k]^T Gb_l;  U_c -= sum_k M_l[k]^T Gb_l
-// A cell whose CHECKSOL test (or FULL = 0) put it on the MUSCL fall-back is
-// not covered: the kernel raises a flag and the VJP returns UCG_EINVAL.
+// A cell whose CHECKSOL test (or FULL = 0) put it on the MUSCL fall-back
+// takes the reverse (and tangent) of that branch instead: the central
+// polynomial G_0 limited by Venkatakrishnan with FIND_BOUNDS over the face
+// neighbours, and CHECKSOLX.
 #include <cuda_runtime.h>
 
+#include "ad.cuh"
 #include "engine_internal.h"
 #include "recon2.cuh"
 
@@ -130,85 +133,149 @@ __device__ __forceinline__ bool checksol_split(const Problem& p, const double* _
   return bad;
 }
 
-// k_adj_wpost: writes Gb (layout of the stencil polynomials G) and the
-// direct adjoint of the cell mean (selfc); scr holds Bb (interleaved like
-// G).  Gb first receives 2 S G_l (the gradient of IS_l), read back once the
-// weights' adjoints are known.
+// CHECKSOLX (0.95) of the MUSCL fall-back face values u0 + dd(x) slope of
+// cell c, dd(x) = (u0 + m(x).g0 - mean) - u0 with the central polynomial g0
+// (sG, all variables) and the limiter value (sS); warp w tests the points
+// whose running index is w modulo NV.  True if a face value of the cell fails.
+template <int P>
+__device__ __forceinline__ bool checksolx_split(const Problem& p, const double* __restrict__ U, int64_t c, int nf,
+                                                const double* __restrict__ xq, const double* __restrict__ bmv,
+                                                const double (*sG)[NV][32], const double (*sS)[32], int lane, int w) {
+  constexpr int ID = Deg<P>::ideg;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  double u0[NV], pm[NV], cb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u0[v] = U[c * NV + v];
+  cons2prim(p.gamma, u0, pm);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    cb[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) cb[v] += bmv[d * 32] * sG[d][v][lane];
+  }
+  bool bad = false;
+  int k = 0;
+  for (int f = 0; f < nf; ++f) {
+    const int nq = face_nq(p, p.ftype[c * MF + f]);
+    for (int q = 0; q < nq; ++q, ++k) {
+      if (k % NV != w || bad) continue;
+      const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+      double m[ID], uf[NV];
+      monomials<P, double>(xi[0], xi[32], xi[64], m);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        asm volatile("" ::: "memory");  // re-read the polynomial from shared memory at every point
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) r += m[d] * sG[d][v][lane];
+        r = r - cb[v];
+        const double dd = (u0[v] + r) - u0[v];
+        uf[v] = u0[v] + dd * sS[v][lane];
+      }
+      bad = jump_bad(p.gamma, pm, uf, 0.95);
+    }
+  }
+  return bad;
+}
+
+// k_adj_wpost: writes Gb (layout of the stencil polynomials G), the direct
+// adjoint of the cell mean (selfc) and the face slots of the MUSCL
+// fall-back's bounds; scr holds Bb (interleaved like G).  Gb first receives
+// 2 S G_l (the gradient of IS_l), read back once the weights' adjoints are
+// known.  The branch of every cell is decided as in the forward: FULL = 0
+// or a failed CHECKSOL (0.85) takes the MUSCL fall-back (the central
+// stencil polynomial G_0, FIND_BOUNDS over the face neighbours and the
+// Venkatakrishnan limiter, src/reconstruct_p.f90:3126-3406), whose reverse
+// is
+//   out(x) = dd(x) slope,  slope = min_x phi(dd(x), lo, hi):
+//   Gb_0 = slope Bb + sb dphi/ddd(x*) (m(x*) - mean),  sb = sum_x ub(x) dd(x),
+//   lo/hi's adjoints sb dphi/dlo, sb dphi/dhi to the face neighbour that set
+//   the bound (face slot) and minus that to the cell;
+// a fall-back that CHECKSOLX (0.95) reduced to first order has no
+// dependence on the polynomials or the bounds.
 template <int P>
 __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem p, const double* __restrict__ U,
-                                                             const double* __restrict__ adjF,
-                                                             double* __restrict__ gbar, double* __restrict__ scr,
-                                                             double* __restrict__ selfc, int* __restrict__ flag) {
+                                                                        const double* __restrict__ adjF,
+                                                                        double* __restrict__ gbar,
+                                                                        double* __restrict__ scr,
+                                                                        double* __restrict__ selfc,
+                                                                        double* __restrict__ contrib) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<double>::N;
-  __shared__ double sGH[ID][NV][32];
+  __shared__ double sGH[ID][NV][32];  // WENO combined polynomial, then the fall-back's G_0
+  __shared__ double sSlope[NV][32];
+  __shared__ int sFall[32];  // bit 0: MUSCL fall-back, bit 1: reduced to first order
   const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
   const int64_t grp = blockIdx.x;
   const int64_t c = grp * 32 + lane;
-  const bool live = c < p.n && p.full[c];
-  if (c < p.n && !p.full[c] && v == 0) atomicOr(flag, 1);
-  const int A = p.admis_max;
+  const bool cell = c < p.n;
+  const bool full = cell && p.full[c];
+  if (v == 0) sFall[lane] = cell && !full ? 1 : 0;
+  const int A = p.admis_max, IM = p.imax;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
   const int FQ = MF * QS;
+  const bool cw = p.ees == 5;
+  const int64_t fslot = (cw ? 1 + IM + (int64_t)(A - 1) * p.imax2 : 1 + (int64_t)A * IM);
   const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
   const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
-  if (live) {
-    const int adm = p.admis[c], nf = p.nfaces[c];
-    const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-    auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-    double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
-    auto GB = [&](int ll, int d) -> double& { return Gb[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-    double* BBp = scr + grp * (int64_t)(ID * NV) * 32 + lane;
-    auto BB = [&](int d) -> double& { return BBp[(int64_t)(d * NV + v) * 32]; };
-    const double* aF = adjF + c * (int64_t)FQ * NV + v;
-    // ---- the direct term and Bb = sum_x ub(x) (m(x) - mean(m))
-    {
-      double acc[ID], sa = 0.0;
+  const int adm = cell ? p.admis[c] : 0, nf = cell ? p.nfaces[c] : 0;
+  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  double* Gb = gbar + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto GB = [&](int ll, int d) -> double& { return Gb[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  double* BBp = scr + grp * (int64_t)(ID * NV) * 32 + lane;
+  auto BB = [&](int d) -> double& { return BBp[(int64_t)(d * NV + v) * 32]; };
+  const double* aF = adjF + c * (int64_t)FQ * NV + v;
+  const int ID2 = p.ideg2;
+  constexpr int L2 = ID < 9 ? ID : 9;
+  auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
+  // ---- the direct term and Bb = sum_x ub(x) (m(x) - mean(m))
+  if (cell) {
+    double acc[ID], sa = 0.0;
 #pragma unroll
-      for (int d = 0; d < ID; ++d) acc[d] = 0.0;
-      for (int f = 0; f < nf; ++f) {
-        const int nq = face_nq(p, p.ftype[c * MF + f]);
-        for (int q = 0; q < nq; ++q) {
-          const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
-          double m[ID];
-          monomials<P, double>(xi[0], xi[32], xi[64], m);
-          const double a = aF[(f * QS + q) * NV];
-          sa += a;
+    for (int d = 0; d < ID; ++d) acc[d] = 0.0;
+    for (int f = 0; f < nf; ++f) {
+      const int nq = face_nq(p, p.ftype[c * MF + f]);
+      for (int q = 0; q < nq; ++q) {
+        const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+        double m[ID];
+        monomials<P, double>(xi[0], xi[32], xi[64], m);
+        const double a = aF[(f * QS + q) * NV];
+        sa += a;
 #pragma unroll
-          for (int d = 0; d < ID; ++d) acc[d] += m[d] * a;
-        }
+        for (int d = 0; d < ID; ++d) acc[d] += m[d] * a;
       }
-#pragma unroll
-      for (int d = 0; d < ID; ++d) BB(d) = acc[d] - bmv[d * 32] * sa;
-      selfc[c * NV + v] = sa;
     }
-    // ---- indicators and weights.  CWENO (EES 5): the central polynomial is
-    // g1 = (G_0 - sum_l lk G_l) / lc1 (rows below IDEGFREE2 for the
-    // lower-order stencils), the lower-order stencils have IDEGFREE2 rows and
-    // the S2 triangle, the linear weights are lc1, lk.
-    const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
-    const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
-    const bool cw = p.ees == 5;
-    const int ID2 = p.ideg2;
-    constexpr int L2 = ID < 9 ? ID : 9;
-    const double lc1 = 1.0 - 1.0 / p.lwci;
-    const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-    auto nd_of = [&](int ll) { return cw && ll > 0 ? ID2 : ID; };
-    double g3[L2];
 #pragma unroll
-    for (int d = 0; d < L2; ++d) g3[d] = 0.0;
-    if (cw)
-      for (int l2 = 1; l2 < adm; ++l2)
+    for (int d = 0; d < ID; ++d) BB(d) = acc[d] - bmv[d * 32] * sa;
+    selfc[c * NV + v] = sa;
+  }
+  // ---- WENO branch: indicators and weights.  CWENO (EES 5): the central
+  // polynomial is g1 = (G_0 - sum_l lk G_l) / lc1 (rows below IDEGFREE2 for
+  // the lower-order stencils), the lower-order stencils have IDEGFREE2 rows
+  // and the S2 triangle, the linear weights are lc1, lk.
+  const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
+  const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  double g3[L2];
 #pragma unroll
-        for (int d = 0; d < L2; ++d)
-          if (d < ID2) g3[d] = g3[d] + lk * G(l2, d);
-    // row d of stencil polynomial ll as the reconstruction uses it
-    auto poly = [&](int ll, int d) -> double {
-      if (d >= nd_of(ll)) return 0.0;
-      if (cw && ll == 0) return (1.0 / lc1) * (G(0, d) - (d < L2 ? g3[d] : 0.0));
-      return G(ll, d);
-    };
-    double is[7], wt[7], om[7], omb[7];
+  for (int d = 0; d < L2; ++d) g3[d] = 0.0;
+  if (cw && full)
+    for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+      for (int d = 0; d < L2; ++d)
+        if (d < ID2) g3[d] = g3[d] + lk * G(l2, d);
+  // row d of stencil polynomial ll as the reconstruction uses it
+  auto poly = [&](int ll, int d) -> double {
+    if (d >= nd_of(ll)) return 0.0;
+    if (cw && ll == 0) return (1.0 / lc1) * (G(0, d) - (d < L2 ? g3[d] : 0.0));
+    return G(ll, d);
+  };
+  const bool wz = cw && p.wenoz;
+  double is[7], wt[7], om[7], omb[7];
+  double tau = 0.0, sum = 0.0, dot = 0.0;
+  if (full) {
 #pragma unroll 1
     for (int ll = 0; ll < adm; ++ll) {
       double s;
@@ -232,8 +299,6 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
     }
     // weights: lam / (eps + IS)^4, or WENO-Z (CWENO only)
     // lam (1 + (tau / (eps + IS))^4) with tau = sum_l |IS_0 - IS_l| / (adm - 1)
-    const bool wz = cw && p.wenoz;
-    double tau = 0.0, sum = 0.0;
     if (wz) {
       for (int ll = 0; ll < adm; ++ll) tau += fabs(is[0] - is[ll]);
       tau = tau / (adm - 1);
@@ -252,8 +317,7 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
       sum += wt[ll];
     }
     for (int ll = 0; ll < adm; ++ll) om[ll] = wt[ll] / sum;
-    // ---- combined polynomial (CHECKSOL) and the weights' adjoints
-    double dot = 0.0;
+    // combined polynomial (CHECKSOL, in shared memory) and the weights' adjoints
 #pragma unroll
     for (int d = 0; d < ID; ++d) sGH[d][v][lane] = 0.0;
 #pragma unroll 1
@@ -269,6 +333,13 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
       omb[ll] = ob;
       dot += ob * om[ll];
     }
+  }
+  __syncthreads();
+  // ---- CHECKSOL (0.85) on the WENO face values
+  if (full && checksol_split<P>(p, U, c, nf, xq, bmv, sGH, lane, v)) atomicOr(&sFall[lane], 1);
+  __syncthreads();
+  const bool fall = cell && (sFall[lane] & 1);
+  if (full && !fall) {
     // ---- Gb_l = om_l Bb + ISb_l 2 S G_l (+ the CWENO central share)
     double corr[L2];
 #pragma unroll
@@ -314,10 +385,88 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_adj_wpost(Problem 
       }
     }
   }
+  // ---- MUSCL fall-back: the forward again (bounds, limiter and its
+  // limiting point), G_0 and the limiter value shared for CHECKSOLX
+  double lo = 0.0, hi = 0.0, slope = TOLBIG, ddx = 0.0, sb = 0.0, epsi2 = 0.0;
+  int flo = -1, fhi = -1, xs = -1;
+  if (fall) {
+    const double u0v = U[c * NV + v];
+    lo = hi = u0v;
+    for (int f = 0; f < nf; ++f) {
+      const int64_t nb = p.neigh[c * MF + f];
+      if (nb < 0) continue;
+      const double un = U[nb * NV + v];
+      if (un < lo) lo = un, flo = f;
+      if (un > hi) hi = un, fhi = f;
+    }
+    lo -= u0v;
+    hi -= u0v;
+    const double e3 = p.kappa_ven * p.minedge[c];
+    epsi2 = e3 * e3 * e3;
+    double g0[ID], cb = 0.0;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      g0[d] = G(0, d);
+      cb += bmv[d * 32] * g0[d];
+    }
+    for (int f = 0; f < nf; ++f) {
+      const int nq = face_nq(p, p.ftype[c * MF + f]);
+      for (int q = 0; q < nq; ++q) {
+        const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+        double m[ID];
+        monomials<P, double>(xi[0], xi[32], xi[64], m);
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) r += m[d] * g0[d];
+        r = r - cb;
+        const double dd = (u0v + r) - u0v;
+        const double phi = venkat(dd, lo, hi, epsi2);
+        if (phi < slope) slope = phi, xs = f * QS + q, ddx = dd;
+        sb += aF[(f * QS + q) * NV] * dd;
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < ID; ++d) sGH[d][v][lane] = g0[d];
+    sSlope[v][lane] = slope;
+  }
   __syncthreads();
-  // ---- CHECKSOL (0.85) on the WENO face values: a flagged cell took the
-  // MUSCL fall-back in the forward, which this adjoint does not cover
-  if (live && checksol_split<P>(p, U, c, p.nfaces[c], xq, bmv, sGH, lane, v)) atomicOr(flag, 1);
+  if (fall && checksolx_split<P>(p, U, c, nf, xq, bmv, sGH, sSlope, lane, v)) atomicOr(&sFall[lane], 2);
+  __syncthreads();
+  double fb[MF];
+#pragma unroll
+  for (int f = 0; f < MF; ++f) fb[f] = 0.0;
+  if (fall) {
+    const bool first = sFall[lane] & 2;
+    if (!first && xs >= 0) {
+      ad::Dual<3> dd(ddx), dlo(lo), dhi(hi);
+      dd.d[0] = 1.0;
+      dlo.d[1] = 1.0;
+      dhi.d[2] = 1.0;
+      const ad::Dual<3> ph = venkat(dd, dlo, dhi, epsi2);
+      const double ddb = sb * ph.d[0], lob = sb * ph.d[1], hib = sb * ph.d[2];
+      const double* xi = xq + (int64_t)xs * 3 * 32;
+      double m[ID];
+      monomials<P, double>(xi[0], xi[32], xi[64], m);
+#pragma unroll
+      for (int d = 0; d < ID; ++d) GB(0, d) = slope * BB(d) + ddb * (m[d] - bmv[d * 32]);
+      // lo = U_nb - u0 (or 0 when the cell itself is the minimum)
+      double selfb = 0.0;
+#pragma unroll
+      for (int f = 0; f < MF; ++f) {
+        if (f == flo) fb[f] += lob, selfb -= lob;
+        if (f == fhi) fb[f] += hib, selfb -= hib;
+      }
+      selfc[c * NV + v] += selfb;
+    } else {
+#pragma unroll
+      for (int d = 0; d < ID; ++d) GB(0, d) = 0.0;
+    }
+    for (int ll = 1; ll < adm; ++ll)
+      for (int d = 0; d < nd_of(ll); ++d) GB(ll, d) = 0.0;
+  }
+  if (cell)
+#pragma unroll
+    for (int f = 0; f < MF; ++f) contrib[((fslot + f) * p.n + c) * NV + v] = fb[f];
 }
 
 // k_adj_lsq: one lane per cell, the transpose of the stencil least squares,
@@ -385,33 +534,39 @@ __global__ void __launch_bounds__(128) k_adj_lsq(Problem p, const double* __rest
 //   dIS_l = d(G_l^T S G_l),  dwt_l = -4 wt_l dIS_l / (eps + IS_l),
 //   dom_l = (dwt_l - om_l sum dwt) / sum wt,
 //   du(x) - dU_c = b(x) . sum_l (dom_l G_l + om_l dG_l).
-// Same fall-back flag as k_adj_wpost; a cell on it gets a zero tangent.
+// Cells on the MUSCL fall-back (decided as in k_adj_wpost): with
+// out(x) = dd(x) slope, dout(x) = ddt(x) slope + dd(x) dslope,
+//   dslope = dphi/ddd ddt(x*) + dphi/dlo dlo + dphi/dhi dhi,
+// dlo = dU_nb - dU_c for the neighbour that set the bound; zero where
+// CHECKSOLX reduced the cell to first order.
 template <int P>
 __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem p, const double* __restrict__ U,
+                                                                        const double* __restrict__ dU,
                                                                         const double* __restrict__ dG,
-                                                                        double* __restrict__ tdul,
-                                                                        int* __restrict__ flag) {
+                                                                        double* __restrict__ tdul) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<double>::N;
-  __shared__ double sGH[ID][NV][32];
+  __shared__ double sGH[ID][NV][32];  // WENO combined polynomial, then the fall-back's G_0
+  __shared__ double sSlope[NV][32];
+  __shared__ int sFall[32];  // bit 0: MUSCL fall-back, bit 1: reduced to first order
   const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
   const int64_t grp = blockIdx.x;
   const int64_t c = grp * 32 + lane;
-  const bool live = c < p.n && p.full[c];
-  if (c < p.n && !p.full[c] && v == 0) atomicOr(flag, 1);
+  const bool cell = c < p.n;
+  const bool live = cell && p.full[c];
+  if (v == 0) sFall[lane] = cell && !live ? 1 : 0;
   const int A = p.admis_max;
   const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
   const int FQ = MF * QS;
   const double* xq = (const double*)p.qpts + grp * (int64_t)FQ * 3 * 32 + lane;
   const double* bmv = (const double*)p.bmean + grp * (int64_t)ID * 32 + lane;
-  if (c < p.n && !live)
-    for (int i = 0; i < FQ; ++i) tdul[(c * FQ + i) * NV + v] = 0.0;
+  const int nf = cell ? p.nfaces[c] : 0;
+  const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  const double* dGc = dG + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+  auto dGv = [&](int ll, int d) -> double { return dGc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
   if (live) {
-    const int adm = p.admis[c], nf = p.nfaces[c];
-    const double* Gc = (const double*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
-    const double* dGc = dG + grp * (int64_t)(A * ID * NV) * 32 + lane;
-    auto G = [&](int ll, int d) -> double { return Gc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
-    auto dGv = [&](int ll, int d) -> double { return dGc[(int64_t)((ll * ID + d) * NV + v) * 32]; };
+    const int adm = p.admis[c];
     const double* Pc = (const double*)p.ind + grp * p.istride * 32 + lane * VEC;
     const double* Pc2 = Pc + (int64_t)(p.i2off / VEC) * 32 * VEC;
     const bool cw = p.ees == 5;
@@ -532,32 +687,126 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem 
     }
   }
   __syncthreads();
-  if (live && checksol_split<P>(p, U, c, p.nfaces[c], xq, bmv, sGH, lane, v)) atomicOr(flag, 1);
+  if (live && checksol_split<P>(p, U, c, nf, xq, bmv, sGH, lane, v)) atomicOr(&sFall[lane], 1);
+  __syncthreads();
+  // ---- MUSCL fall-back: the forward again, G_0 and the limiter value
+  // shared for CHECKSOLX
+  const bool fall = cell && (sFall[lane] & 1);
+  double lo = 0.0, hi = 0.0, slope = TOLBIG, ddx = 0.0, epsi2 = 0.0, cb = 0.0, dcb = 0.0;
+  int flo = -1, fhi = -1, xs = -1;
+  const double u0v = cell ? U[c * NV + v] : 0.0;
+  if (fall) {
+    lo = hi = u0v;
+    for (int f = 0; f < nf; ++f) {
+      const int64_t nb = p.neigh[c * MF + f];
+      if (nb < 0) continue;
+      const double un = U[nb * NV + v];
+      if (un < lo) lo = un, flo = f;
+      if (un > hi) hi = un, fhi = f;
+    }
+    lo -= u0v;
+    hi -= u0v;
+    const double e3 = p.kappa_ven * p.minedge[c];
+    epsi2 = e3 * e3 * e3;
+    double g0[ID];
+#pragma unroll
+    for (int d = 0; d < ID; ++d) {
+      g0[d] = G(0, d);
+      cb += bmv[d * 32] * g0[d];
+    }
+    for (int f = 0; f < nf; ++f) {
+      const int nq = face_nq(p, p.ftype[c * MF + f]);
+      for (int q = 0; q < nq; ++q) {
+        const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+        double m[ID];
+        monomials<P, double>(xi[0], xi[32], xi[64], m);
+        double r = 0.0;
+#pragma unroll
+        for (int d = 0; d < ID; ++d) r += m[d] * g0[d];
+        r = r - cb;
+        const double dd = (u0v + r) - u0v;
+        const double phi = venkat(dd, lo, hi, epsi2);
+        if (phi < slope) slope = phi, xs = f * QS + q, ddx = dd;
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < ID; ++d) sGH[d][v][lane] = g0[d];
+    sSlope[v][lane] = slope;
+  }
+  __syncthreads();
+  if (fall && checksolx_split<P>(p, U, c, nf, xq, bmv, sGH, sSlope, lane, v)) atomicOr(&sFall[lane], 2);
+  __syncthreads();
+  if (fall) {
+    const bool first = (sFall[lane] & 2) || xs < 0;
+    double dslope = 0.0;
+    if (!first) {
+#pragma unroll
+      for (int d = 0; d < ID; ++d) dcb += bmv[d * 32] * dGv(0, d);
+      const double* xi = xq + (int64_t)xs * 3 * 32;
+      double m[ID];
+      monomials<P, double>(xi[0], xi[32], xi[64], m);
+      double ddt = 0.0;
+#pragma unroll
+      for (int d = 0; d < ID; ++d) ddt += m[d] * dGv(0, d);
+      ddt -= dcb;
+      ad::Dual<3> dd(ddx), dlo(lo), dhi(hi);
+      dd.d[0] = 1.0;
+      dlo.d[1] = 1.0;
+      dhi.d[2] = 1.0;
+      const ad::Dual<3> ph = venkat(dd, dlo, dhi, epsi2);
+      const double du0 = dU[c * NV + v];
+      const double tlo = flo >= 0 ? dU[(int64_t)p.neigh[c * MF + flo] * NV + v] - du0 : 0.0;
+      const double thi = fhi >= 0 ? dU[(int64_t)p.neigh[c * MF + fhi] * NV + v] - du0 : 0.0;
+      dslope = ph.d[0] * ddt + ph.d[1] * tlo + ph.d[2] * thi;
+    }
+    for (int f = 0; f < MF; ++f) {
+      const int nq = f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0;
+      for (int q = 0; q < QS; ++q) {
+        double t = 0.0;
+        if (q < nq && !first) {
+          const double* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+          double m[ID];
+          monomials<P, double>(xi[0], xi[32], xi[64], m);
+          double r = 0.0, rt = 0.0;
+#pragma unroll
+          for (int d = 0; d < ID; ++d) {
+            r += m[d] * sGH[d][v][lane];
+            rt += m[d] * dGv(0, d);
+            if ((d & 7) == 7) asm volatile("" ::: "memory");  // bound the loads in flight
+          }
+          const double dd = (u0v + (r - cb)) - u0v;
+          t = (rt - dcb) * slope + dd * dslope;
+        }
+        tdul[(c * FQ + f * QS + q) * NV + v] = t;
+      }
+    }
+  }
 }
 
 template <int P>
 void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
-              double* contrib, int* flag, cudaStream_t st) {
-  k_adj_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, adjF, gbar, scr, selfc, flag);
+              double* contrib, cudaStream_t st) {
+  k_adj_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, adjF, gbar, scr, selfc, contrib);
   k_adj_lsq<P><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, gbar, selfc, contrib);
 }
 
 template <int P>
-void launch_jvp_t(const Problem& p, const double* U, const double* dG, double* tdul, int* flag, cudaStream_t st) {
-  k_jvp_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, dG, tdul, flag);
+void launch_jvp_t(const Problem& p, const double* U, const double* dU, const double* dG, double* tdul,
+                  cudaStream_t st) {
+  k_jvp_wpost<P><<<(unsigned)((p.n + 31) / 32), WP_THREADS, 0, st>>>(p, U, dU, dG, tdul);
 }
 
 }  // namespace
 
 namespace ucg_host {
 
-int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dG, double* tdul,
-                        int* flag) {
+int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dU, const double* dG,
+                        double* tdul) {
   switch (e->cfg.iorder) {
-    case 1: launch_jvp_t<1>(p, U, dG, tdul, flag, e->stream); break;
-    case 2: launch_jvp_t<2>(p, U, dG, tdul, flag, e->stream); break;
-    case 3: launch_jvp_t<3>(p, U, dG, tdul, flag, e->stream); break;
-    case 4: launch_jvp_t<4>(p, U, dG, tdul, flag, e->stream); break;
+    case 1: launch_jvp_t<1>(p, U, dU, dG, tdul, e->stream); break;
+    case 2: launch_jvp_t<2>(p, U, dU, dG, tdul, e->stream); break;
+    case 3: launch_jvp_t<3>(p, U, dU, dG, tdul, e->stream); break;
+    case 4: launch_jvp_t<4>(p, U, dU, dG, tdul, e->stream); break;
     default: return fail(e, UCG_EINVAL, "iorder out of range");
   }
   e->launches++;
@@ -567,12 +816,12 @@ int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const 
 
 
 int launch_weno_adjoint(ucg_engine* e, const Problem& p, const double* U, const double* adjF, double* gbar,
-                        double* scr, double* selfc, double* contrib, int* flag) {
+                        double* scr, double* selfc, double* contrib) {
   switch (e->cfg.iorder) {
-    case 1: launch_t<1>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
-    case 2: launch_t<2>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
-    case 3: launch_t<3>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
-    case 4: launch_t<4>(p, U, adjF, gbar, scr, selfc, contrib, flag, e->stream); break;
+    case 1: launch_t<1>(p, U, adjF, gbar, scr, selfc, contrib, e->stream); break;
+    case 2: launch_t<2>(p, U, adjF, gbar, scr, selfc, contrib, e->stream); break;
+    case 3: launch_t<3>(p, U, adjF, gbar, scr, selfc, contrib, e->stream); break;
+    case 4: launch_t<4>(p, U, adjF, gbar, scr, selfc, contrib, e->stream); break;
     default: return fail(e, UCG_EINVAL, "iorder out of range");
   }
   e->launches += 2;

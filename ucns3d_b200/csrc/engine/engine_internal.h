@@ -67,7 +67,7 @@ struct ucg_engine {
       adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd;
   // discrete adjoint of the WENO reconstruction (adjoint_weno.cu)
   bool adjw_ready = false;
-  DevBuf adjw_face, adjw_gbar, adjw_scr, adjw_self, adjw_contrib, adjw_rptr, adjw_rsrc, adjw_flag, adjw_lam, adjw_mu,
+  DevBuf adjw_face, adjw_gbar, adjw_scr, adjw_self, adjw_contrib, adjw_rptr, adjw_rsrc, adjw_lam, adjw_mu,
       adjw_pface, adjw_tmp;
 };
 
@@ -93,9 +93,9 @@ int rk3(ucg_engine* e, double dt, bool dt_dev);
 void adjoint_release(ucg_engine* e);
 // reverse of the WENO post-processing and least squares (adjoint_weno.cu)
 int launch_weno_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, const double* adjF, double* gbar,
-                        double* scr, double* selfc, double* contrib, int* flag);
+                        double* scr, double* selfc, double* contrib);
 // tangent of the WENO face values from the tangent stencil polynomials dG
-int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dG, double* tdul,
-                        int* flag);
+int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dU, const double* dG,
+                        double* tdul);
 
 }  // namespace ucg_host
