@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint stride of the adjoint run")
     ap.add_argument("--adjoint-weno-n", type=int, default=32,
                     help="hexahedra per side of the vortex timed for the WENO VJP/JVP")
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="RK3 steps of the vortex accuracy run (FP64 and mixed against the analytic solution); 0 skips")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
     return ap.parse_args()
@@ -269,6 +271,43 @@ def run_gpu(args, case, ws, local, timed_e2e=True):
     return dict(ms=ms, kern=kern, state=state, clocks=clocks, launches=launches, e2e=e2e, device_bytes=nbytes_dev)
 
 
+def run_accuracy(case, local, steps):
+    """Isentropic vortex: `steps` RK3 steps at one fixed dt (CFL from the
+    initial state) in the FP64 and the mixed form on the same mesh; density
+    error of each against the analytic solution (the initial vortex advected
+    by the free stream for steps * dt) and of mixed against FP64."""
+    import numpy as np
+    from ucns3d_b200 import _native as N
+    from ucns3d_b200.cases import vortex_params
+    from ucns3d_b200.engine import Engine
+    from ucns3d_b200.mesh import IC_VORTEX
+
+    rho = {}
+    dt = None
+    for prec in (N.UCG_FP64, N.UCG_MIXED):
+        cfg = N.UcgConfig.from_buffer_copy(case.cfg)
+        cfg.precision = prec
+        eng = Engine(case.mesh, cfg, device=local)
+        eng.set_state(case.U0)
+        if dt is None:
+            dt = eng.calculate_cfl(case.cfl)
+        for _ in range(steps):
+            eng.runge_kutta3(dt)
+        eng.check_health()
+        rho[prec] = eng.get_state()[:, 0].copy()
+        eng.close()
+    exact = case.mesh.initial_condition(IC_VORTEX, vortex_params(case.meta["L"], t=steps * dt))[:, 0]
+
+    def err(a, b):
+        return {"rel_l2": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2))),
+                "rel_linf": float(np.abs(a - b).max() / np.abs(b).max())}
+
+    return {"steps": steps, "dt": dt, "t": steps * dt,
+            "density_mixed_vs_fp64": err(rho[N.UCG_MIXED], rho[N.UCG_FP64]),
+            "density_fp64_vs_analytic": err(rho[N.UCG_FP64], exact),
+            "density_mixed_vs_analytic": err(rho[N.UCG_MIXED], exact)}
+
+
 def cpu_sample(args, steps=1):
     """The oracle (CPU restatement) on a bounded sample of the workload: the
     same scheme on a smaller mesh, all host threads."""
@@ -462,6 +501,8 @@ def main():
                        "mixed_speedup": value / v64,
                        "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
                        "after_steps": args.warmup + args.steps}
+    if args.case == "vortex_hex_weno5" and args.accuracy_steps > 0:
+        out["accuracy"] = run_accuracy(c32, local, args.accuracy_steps)
     if not args.no_adjoint:
         out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -267,6 +267,33 @@ def test_mixed_weno5_vortex_density_error():
     assert l2 < 1e-6
 
 
+def test_mixed_weno5_vortex_100_steps_against_fp64_and_analytic():
+    """Isentropic vortex, WENO5, 100 RK3 steps at one fixed dt: the mixed
+    form's density stays within 1e-6 relative L2 of the FP64 form, and its
+    error against the analytic solution (the vortex advected by the free
+    stream) is the FP64 form's error to within 1 %."""
+    from ucns3d_b200.cases import vortex_params
+    c64 = cases.vortex_hex_weno5(n=16)
+    c32 = cases.vortex_hex_weno5(n=16, precision=N.UCG_MIXED)
+    a, b = Engine(c64.mesh, c64.cfg), Engine(c32.mesh, c32.cfg)
+    a.set_state(c64.U0)
+    b.set_state(c32.U0)
+    dt = a.calculate_cfl(0.5)
+    for _ in range(100):
+        a.runge_kutta3(dt)
+        b.runge_kutta3(dt)
+    ra, rb = a.get_state()[:, 0], b.get_state()[:, 0]
+    ex = c64.mesh.initial_condition(IC_VORTEX, vortex_params(c64.meta["L"], t=100 * dt))[:, 0]
+
+    def rel_l2(x, y):
+        return np.sqrt(np.mean((x - y) ** 2)) / np.sqrt(np.mean(y ** 2))
+
+    l2, ea, eb = rel_l2(rb, ra), rel_l2(ra, ex), rel_l2(rb, ex)
+    print(f"100 steps: mixed vs fp64 {l2:.3e}, fp64 vs analytic {ea:.3e}, mixed vs analytic {eb:.3e}")
+    assert l2 < 1e-6
+    assert abs(eb - ea) <= 0.01 * ea
+
+
 def test_nonphysical_state_is_reported_not_trapped():
     m, cfg, U = _setup("muscl_ns_hex")
     e = Engine(m, cfg)
