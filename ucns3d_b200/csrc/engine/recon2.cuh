@@ -878,10 +878,12 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
         for (int j = 0; j < VP; ++j) acc[d][j] += m * ds[j];
       }
     }
+    // 16-byte stores of variable pairs (VP is even; rows are 32-byte aligned)
 #pragma unroll
     for (int d = 0; d < ID; ++d)
 #pragma unroll
-      for (int j = 0; j < VP; ++j) p.gv[(c * ID + d) * 4 + v0 + j] = acc[d][j];
+      for (int j = 0; j < VP; j += 2)
+        *(double2*)(p.gv + (c * ID + d) * 4 + v0 + j) = make_double2(acc[d][j], acc[d][j + 1]);
   }
 }
 
@@ -898,7 +900,7 @@ __global__ void k_visc_face(Problem p) {
   double dx[ID], dy[ID], dz[ID];
   dmonomials<P>((double)xi[0], (double)xi[32], (double)xi[64], dx, dy, dz);
   const double* J = p.jinv + c * 9;
-  double* o = p.ulv + ((c * MF + f) * QS + q) * 12;
+  double out[12];
 #pragma unroll
   for (int var = 0; var < 4; ++var) {
     double gl[3] = {0.0, 0.0, 0.0};
@@ -910,8 +912,13 @@ __global__ void k_visc_face(Problem p) {
       gl[2] += g * dz[d];
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) o[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
+    for (int k = 0; k < 3; ++k) out[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
   }
+  // the point's 96 bytes as six 16-byte stores (half as many store
+  // instructions, each touching one sector per lane)
+  double2* o = (double2*)(p.ulv + ((c * MF + f) * QS + q) * 12);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) o[k] = make_double2(out[2 * k], out[2 * k + 1]);
 }
 
 // Characteristic-variable post-processing (k_wpost<P, T, true>), 64 threads
