@@ -205,8 +205,18 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
     if (NS && nb >= 0) {
-      const double* gl = p.ulv + ((c * MF + f) * QS + q) * 12;
-      const double* gr = p.ulv + ((nb * MF + nf) * QS + qq) * 12;
+      // both sides' face-point gradients as six 16-byte loads each
+      const double2* gl2 = (const double2*)(p.ulv + ((c * MF + f) * QS + q) * 12);
+      const double2* gr2 = (const double2*)(p.ulv + ((nb * MF + nf) * QS + qq) * 12);
+      double gl[12], gr[12];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double2 a2 = gl2[k], b2 = gr2[k];
+        gl[2 * k] = a2.x;
+        gl[2 * k + 1] = a2.y;
+        gr[2 * k] = b2.x;
+        gr[2 * k + 1] = b2.y;
+      }
       double fv[NV];
       viscous_flux(p, r, p.dih[c * MF + f], cl, cr, gl, gr, fv);
 #pragma unroll
