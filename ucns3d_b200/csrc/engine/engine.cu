@@ -129,6 +129,7 @@ Problem make_problem(ucg_engine* e) {
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.gv = (double*)e->gv.p;
+  p.prim = (double*)e->prim.p;
   p.rhs = (double*)e->rhs.p;
   p.own = (const int32_t*)e->own.p;
   p.nown = e->nown;
@@ -333,6 +334,7 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (c.governing == 1) {
     rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
     rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
+    rc = rc ? rc : alloc(e, e->prim, (size_t)n * 4 * 8);
   }
   rc = rc ? rc : alloc(e, e->health, 64);
   rc = rc ? rc : alloc(e, e->dt, 64);
@@ -357,7 +359,7 @@ void ucg_destroy(ucg_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
-                   &e->ind, &e->dul, &e->ulv, &e->gv, &e->rhs, &e->Un, &e->Ua, &e->Ub,
+                   &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
                    &e->qbuf};
   for (DevBuf* b : all) release(*b);

@@ -843,6 +843,20 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
 // (all four when the FP64 accumulators fit), reading the interleaved table
 // rows of stencil 1 with coalesced loads.  Same products and order per
 // (row, variable) as one thread per variable.
+// T = p / (rho R), u, v, w of every cell, formed once per stage: the viscous
+// least squares then gathers 32-byte records (two 16-byte loads, no
+// division) instead of forming them from the conserved state per member.
+template <int P, typename T>
+__global__ void k_visc_prim(Problem p, const double* __restrict__ U) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  double pm[NV];
+  cons2prim(p.gamma, U + c * NV, pm);
+  double2* o = (double2*)(p.prim + c * 4);
+  o[0] = make_double2(pm[4] / (pm[0] * p.r_gas), pm[1]);
+  o[1] = make_double2(pm[2], pm[3]);
+}
+
 template <int P, typename T>
 __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
@@ -865,9 +879,9 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
 #pragma unroll
       for (int j = 0; j < VP; ++j) acc[d][j] = 0.0;
     for (int k = 0; k < IM; ++k) {
-      double py[NV];
-      cons2prim(p.gamma, U + (int64_t)st[(k + 1) * 32] * NV, py);
-      const double sy[4] = {py[4] / (py[0] * p.r_gas), py[1], py[2], py[3]};
+      const double2* q = (const double2*)(p.prim + (int64_t)st[(k + 1) * 32] * 4);
+      const double2 qa = q[0], qb = q[1];
+      const double sy[4] = {qa.x, qa.y, qb.x, qb.y};
       double ds[VP];
 #pragma unroll
       for (int j = 0; j < VP; ++j) ds[j] = sy[v0 + j] - s0[v0 + j];
@@ -966,10 +980,11 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   }
   *launches += 2;
   if (ns) {
+    k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
     k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
     const int64_t nf = p.n * MF * QS;
     k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, st>>>(p);
-    *launches += 2;
+    *launches += 3;
   }
   return cudaGetLastError();
 }
