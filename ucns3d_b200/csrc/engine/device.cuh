@@ -69,6 +69,7 @@ struct Problem {
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
   double* gv;               // [n][ideg][4]  viscous LSQ coefficients
   double* prim;             // [n][4] T, u, v, w of each cell (viscous LSQ, formed once per stage)
+  double* upad;             // [n][6] conserved state in 48-byte records (k_lsq gathers, formed once per stage)
   double* rhs;              // [n][NV] residual output (residual-only mode)
   const int32_t* own;       // owned faces, code cell*8 + face
   int64_t nown;

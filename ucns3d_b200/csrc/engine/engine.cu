@@ -130,6 +130,7 @@ Problem make_problem(ucg_engine* e) {
   p.ulv = (double*)e->ulv.p;
   p.gv = (double*)e->gv.p;
   p.prim = (double*)e->prim.p;
+  p.upad = (double*)e->upad.p;
   p.rhs = (double*)e->rhs.p;
   p.own = (const int32_t*)e->own.p;
   p.nown = e->nown;
@@ -327,8 +328,10 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (c.governing == 1) rc = rc ? rc : alloc(e, e->vflux, (size_t)n * MF * NV * 8);
   rc = rc ? rc : alloc(e, e->dul, (size_t)n * MF * e->QS * NV * T);
   const int64_t ngrp = (n + 31) / 32;
-  if (!(c.scheme == 2 && c.iorder == 1))
+  if (!(c.scheme == 2 && c.iorder == 1)) {
     rc = rc ? rc : alloc(e, e->gbuf, (size_t)ngrp * 32 * c.admis_max * c.ideg * NV * T);
+    if (c.iorder == 3) rc = rc ? rc : alloc(e, e->upad, (size_t)n * 6 * 8);  // k_lsq<3, T, true>
+  }
   if (c.wenwrt == 2)  // characteristic WENO: G^T S G of every stencil (15 values)
     rc = rc ? rc : alloc(e, e->qbuf, (size_t)ngrp * 32 * c.admis_max * 15 * 8);
   if (c.governing == 1) {
@@ -359,7 +362,7 @@ void ucg_destroy(ucg_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   DevBuf* all[] = {&e->nfaces, &e->ftype, &e->neigh, &e->nface, &e->bc, &e->qperm, &e->rot, &e->area, &e->dih,
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
-                   &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->rhs, &e->Un, &e->Ua, &e->Ub,
+                   &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
                    &e->qbuf};
   for (DevBuf* b : all) release(*b);
