@@ -50,10 +50,12 @@ def parse():
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint stride of the adjoint run")
     ap.add_argument("--adjoint-weno-n", type=int, default=32,
                     help="hexahedra per side of the vortex timed for the WENO VJP/JVP")
-    ap.add_argument("--accuracy-steps", type=int, default=100,
-                    help="RK3 steps of the vortex accuracy run (FP64 and mixed against the analytic solution); 0 skips")
+    ap.add_argument("--accuracy-steps", type=int, default=None,
+                    help="RK3 steps of the accuracy run (mixed against FP64; the vortex also against the analytic "
+                         "solution): default 100 for the vortex, the workload's own step count otherwise; 0 skips")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--cpu-n", type=int, default=24, help="mesh size of the CPU baseline sample")
+    ap.add_argument("--cpu-n", type=int, default=0,
+                    help="mesh size of the CPU baseline and reference arm (0: the benchmarked --n)")
     return ap.parse_args()
 
 
@@ -157,12 +159,14 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes per cell of one k_lsq launch (mixed form, WENO5 on hexahedra),
-# dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the
-# 32^3 case divided by its 32,768 cells (profiles/k_lsq_mixed_vortex_n32.md);
-# the traffic grows in proportion to the cells (no re-reads), so a launch on
-# n^3 cells moves this times n^3.
-LSQ_DRAM_BYTES_PER_CELL_MIXED_WENO5_HEX = 106_700
+# DRAM traffic of one k_lsq launch per cell, dram__bytes_read.sum +
+# dram__bytes_write.sum of a one-kernel ncu capture divided by the cells of
+# the captured mesh, keyed by (workload, precision).  Only measured entries
+# are listed; other workloads report traffic null.  The k_lsq traffic grows
+# in proportion to the cells (no re-reads between cells), so a launch on a
+# larger mesh of the same workload moves this times its cells.
+#   vortex_hex_weno5, mixed: 32^3 capture, 1.00x the algorithmic bytes
+LSQ_DRAM_BYTES_PER_CELL = {("vortex_hex_weno5", 1): 106_700}
 
 
 def lsq_bytes_per_cell(cfg):
@@ -272,10 +276,11 @@ def run_gpu(args, case, ws, local, timed_e2e=True):
 
 
 def run_accuracy(case, local, steps):
-    """Isentropic vortex: `steps` RK3 steps at one fixed dt (CFL from the
-    initial state) in the FP64 and the mixed form on the same mesh; density
-    error of each against the analytic solution (the initial vortex advected
-    by the free stream for steps * dt) and of mixed against FP64."""
+    """`steps` RK3 steps at one fixed dt (CFL from the initial state) in the
+    FP64 and the mixed form on the same mesh: the density of mixed against
+    FP64 (relative L2 and Linf) and, for the isentropic vortex, of each
+    against the analytic solution (the initial vortex advected by the free
+    stream for steps * dt)."""
     import numpy as np
     from ucns3d_b200 import _native as N
     from ucns3d_b200.cases import vortex_params
@@ -296,72 +301,104 @@ def run_accuracy(case, local, steps):
         eng.check_health()
         rho[prec] = eng.get_state()[:, 0].copy()
         eng.close()
-    exact = case.mesh.initial_condition(IC_VORTEX, vortex_params(case.meta["L"], t=steps * dt))[:, 0]
 
     def err(a, b):
         return {"rel_l2": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2))),
                 "rel_linf": float(np.abs(a - b).max() / np.abs(b).max())}
 
-    return {"steps": steps, "dt": dt, "t": steps * dt,
-            "density_mixed_vs_fp64": err(rho[N.UCG_MIXED], rho[N.UCG_FP64]),
-            "density_fp64_vs_analytic": err(rho[N.UCG_FP64], exact),
-            "density_mixed_vs_analytic": err(rho[N.UCG_MIXED], exact)}
+    out = {"steps": steps, "dt": dt, "t": steps * dt,
+           "density_mixed_vs_fp64": err(rho[N.UCG_MIXED], rho[N.UCG_FP64])}
+    if case.name == "vortex_hex_weno5":
+        exact = case.mesh.initial_condition(IC_VORTEX, vortex_params(case.meta["L"], t=steps * dt))[:, 0]
+        out["density_fp64_vs_analytic"] = err(rho[N.UCG_FP64], exact)
+        out["density_mixed_vs_analytic"] = err(rho[N.UCG_MIXED], exact)
+    return out
 
 
-def cpu_sample(args, steps=1):
-    """The oracle (CPU restatement) on a bounded sample of the workload: the
-    same scheme on a smaller mesh, all host threads."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import Oracle
+def cpu_case(args):
+    """The workload prepared for the oracle (FP64 tables), at the bench's own
+    size unless --cpu-n asks for another."""
     from ucns3d_b200 import _native as N
     from ucns3d_b200 import cases
     fn = cases.CASES[args.case]
     kw = {"precision": N.UCG_FP64}
     if args.case in ("tgv_hex_muscl", "tgv_tet_weno3", "vortex_hex_weno5", "mixed_cweno4"):
-        kw["n"] = args.cpu_n
-    c = fn(**kw)
-    o = Oracle(c.mesh, c.cfg)
-    U = c.U0.copy()
-    dt = o.compute_dt(U, c.cfl)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        U = o.rk3_step(U, dt)
-    t = time.perf_counter() - t0
-    cores = os.cpu_count()
+        kw["n"] = args.cpu_n or args.n
+    if args.case == "vortex_hex_weno5" and args.wenwrt != 1:
+        kw["wenwrt"] = args.wenwrt
+    return fn(**kw)
+
+
+def cpu_stages(case, cfg, stages):
+    """The oracle (FP64 CPU restatement, OpenMP over all host threads) for
+    `stages` consecutive SSP-RK3 stages of the workload on its full mesh;
+    seconds of the stage calls alone (set-up excluded)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    o = Oracle(case.mesh, cfg)
+    Un = case.U0.copy()
+    U = Un.copy()
+    dt = o.compute_dt(Un, case.cfl)
+    t = 0.0
+    for k in range(stages):
+        stage = k % 3 + 1
+        if stage == 1:
+            Un[:] = U
+        t0 = time.perf_counter()
+        o.rk3_stage(Un, U, dt, stage)
+        t += time.perf_counter() - t0
+    return t
+
+
+def host_cores():
     thr = os.environ.get("OMP_NUM_THREADS")
-    if thr:
-        cores = int(thr)
-    return dict(value=c.mesh.ncells * 3 * steps / t, cores=cores, seconds=t, ncells=c.mesh.ncells,
-                sample=f"{args.case} with n={args.cpu_n} ({c.mesh.ncells} cells), {steps} RK3 step(s), "
+    return int(thr) if thr else os.cpu_count()
+
+
+def cpu_sample(args, case=None, stages=3):
+    """cpu_baseline: the oracle on one SSP-RK3 step (3 stages) of the same
+    workload and mesh, all host threads."""
+    from ucns3d_b200 import _native as N
+    if case is None:
+        case = cpu_case(args)
+    cfg = N.UcgConfig.from_buffer_copy(case.cfg)
+    cfg.precision = N.UCG_FP64
+    t = cpu_stages(case, cfg, stages)
+    n = case.mesh.ncells
+    return dict(value=n * stages / t, cores=host_cores(), seconds=t, ncells=n,
+                sample=f"{args.case}, {n} cells (the benchmarked mesh), {stages} SSP-RK3 stage(s), "
                        f"oracle FP64 CPU restatement, OpenMP")
 
 
 def main_reference(args, ws, rank, local):
     """The reference arm: the CPU restatement of the reference path (the
-    Fortran reference cannot be built on this image) on the host cores,
-    each step one RK3 step of a bounded sample of the workload."""
+    Fortran reference cannot be built on this image) on the host cores, on
+    the benchmarked workload and mesh; each step is one SSP-RK3 stage of
+    that mesh (a full RK3 step takes three), one stage of warm-up."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
+    from ucns3d_b200 import _native as N
     orc.build()
-    for _ in range(max(args.warmup, 0)):
-        cpu_sample(args, steps=1)
-    t = 0.0
-    cells = 0
-    info = None
-    for _ in range(args.steps):
-        info = cpu_sample(args, steps=1)
-        t += info["seconds"]
-        cells += info["ncells"] * 3
-    value = cells / t
+    case = cpu_case(args)
+    cfg = N.UcgConfig.from_buffer_copy(case.cfg)
+    cfg.precision = N.UCG_FP64
+    cpu_stages(case, cfg, 1)
+    t = cpu_stages(case, cfg, args.steps)
+    n = case.mesh.ncells
+    value = n * args.steps / t
+    sample = (f"{args.case}, {n} cells (the benchmarked mesh), {args.steps} SSP-RK3 stages timed after 1 "
+              f"warm-up stage, oracle FP64 CPU restatement, OpenMP")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.case, "n": args.cpu_n, "note": "bounded CPU sample of the workload"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": "port",
-                         "sample": info["sample"]},
+        "config": {"workload": args.case, "cells": n, "n": args.cpu_n or args.n,
+                   "scheme": scheme_label(case, args.wenwrt),
+                   "step": "one SSP-RK3 stage of the full mesh (the metric counts cell-stages); "
+                           "1 warm-up stage whatever --warmup says"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -462,8 +499,8 @@ def main():
     lsq_ms = r32["kern"]["lsq"]
     achieved = bpc * ncells / (lsq_ms / 1000.0) / 1e9
     rbpc = recon_bytes_per_cell(cfg32)
-    traffic = (LSQ_DRAM_BYTES_PER_CELL_MIXED_WENO5_HEX * ncells
-               if args.case == "vortex_hex_weno5" else None)
+    per_cell = LSQ_DRAM_BYTES_PER_CELL.get((args.case, int(cfg32.precision)))
+    traffic = per_cell * ncells if per_cell is not None and args.wenwrt == 1 else None
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -501,12 +538,14 @@ def main():
                        "mixed_speedup": value / v64,
                        "density_rel_l2_mixed_vs_fp64": l2, "density_rel_linf_mixed_vs_fp64": linf,
                        "after_steps": args.warmup + args.steps}
-    if args.case == "vortex_hex_weno5" and args.accuracy_steps > 0:
-        out["accuracy"] = run_accuracy(c32, local, args.accuracy_steps)
+    acc_steps = args.accuracy_steps if args.accuracy_steps is not None else (
+        100 if args.case == "vortex_hex_weno5" else c32.steps)
+    if acc_steps > 0:
+        out["accuracy"] = run_accuracy(c32, local, acc_steps)
     if not args.no_adjoint:
         out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cb = cpu_sample(args, steps=1)
+        cb = cpu_sample(args, case=c32 if not args.cpu_n else None)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",
                                "sample": cb["sample"]}
     if rank == 0:

@@ -96,6 +96,11 @@ typedef struct ucg_config {
   double quad_w[UCG_MAX_QP];  /* face weights, summing to 1 (QUADRATUREQUAD3D)          */
   double tri_w[UCG_MAX_QP];   /* face weights, summing to 1 (QUADRATURETRIANG)          */
   double bc_state[UCG_NV];    /* free-stream primitive state rho,u,v,w,p for the BCs    */
+  int32_t boundtype;   /* BOUNDTYPE (parameters.f90:253): 0 inflow faces take the free
+                          stream and outflow faces their own state (supersonic);
+                          1 the characteristic subsonic treatment where |u| < c
+                          (BOUNDARYS, flow_operations.f90:2883-3012).  The far field
+                          (code 6, :3230) does not depend on it                       */
 } ucg_config;
 
 /* Per-cell geometry (IELEM(N,I) and the small parts of ILOCAL_RECON3(I),
@@ -107,7 +112,10 @@ typedef struct ucg_geometry {
   const int32_t* face_type;   /* [n][F]   types_faces: 5 quadrilateral, 6 triangle      */
   const int32_t* neigh;       /* [n][F]   INEIGH, -1 on a physical boundary face        */
   const int32_t* neigh_face;  /* [n][F]   INEIGHN                                      */
-  const int32_t* bc;          /* [n][F]   boundary code (0 interior or periodic)        */
+  const int32_t* bc;          /* [n][F]   boundary code on faces with neigh = -1:
+                                 1 inflow, 2 outflow, 3 symmetry, 4 wall (inviscid
+                                 slip, Euler only), 6 far field (BOUNDARYS,
+                                 flow_operations.f90:2860-3375); 0 elsewhere         */
   const int32_t* qperm;       /* [n][F][Q] quadrature point of the neighbour's face that
                                  coincides with this face's point q                     */
   const double* face_angle;   /* [n][F][2] FACEANGLEX, FACEANGLEY                       */
@@ -222,11 +230,15 @@ int ucg_last_error(const ucg_engine* e, char* buf, int32_t len);
  * UCG_EINVAL.  Every call writes all the scratch it later reads, so nothing
  * needs clearing, but all calls in the process share the array: calls that
  * overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  Indices read from `geo` and `rec` on the device are
- * bounds-checked, not followed: a cell with an index out of range gets a NaN
- * row in rhs (and so may its face neighbours).  Returns UCG_OK, UCG_EINVAL
+ * serialised by the caller.  The first call in each CUDA context (the
+ * device's primary context, or a context the caller made current) looks up
+ * the array's device address in that context (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Indices, face types and
+ * boundary codes read from `geo` and `rec` on the device are checked, not
+ * followed: a cell with an index out of range, a face type other than 5/6,
+ * a boundary code other than 1, 2, 3, 4, 6, or (Navier-Stokes) any physical
+ * boundary face gets a NaN row in rhs (and so may its face neighbours)
+ * rather than a plausible-looking residual.  Returns UCG_OK, UCG_EINVAL
  * (unsupported configuration, NULL argument or too many cells) or
  * UCG_ECUDA.                                                              */
 int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, const ucg_recon* rec,

@@ -38,8 +38,12 @@ def lib():
         L.orc_compute_dt.argtypes = [cfgp, geop, f64p, C.c_double, f64p]
         L.orc_rk3_step.restype = C.c_int
         L.orc_rk3_step.argtypes = [cfgp, geop, recp, C.c_double, f64p]
+        L.orc_rk3_stage.restype = C.c_int
+        L.orc_rk3_stage.argtypes = [cfgp, geop, recp, C.c_double, C.c_int, f64p, f64p]
         L.orc_hllc.restype = C.c_int
         L.orc_hllc.argtypes = [C.c_double, f64p, f64p, f64p]
+        L.orc_boundary.restype = C.c_int
+        L.orc_boundary.argtypes = [cfgp, C.c_int, f64p, f64p, f64p]
         L.orc_riemann.restype = C.c_int
         L.orc_riemann.argtypes = [C.c_int, C.c_double, f64p, f64p, f64p, f64p]
         L.orc_reduce.restype = C.c_int
@@ -57,6 +61,16 @@ def hllc(gamma, cl, cr):
     cr = np.ascontiguousarray(cr, dtype=np.float64)
     out = np.zeros(5)
     lib().orc_hllc(gamma, _p(cl), _p(cr), _p(out))
+    return out
+
+
+def boundary(cfg, code, angles, cl):
+    """Ghost state of BOUNDARYS for one face (code, ANGLE1/ANGLE2, left state)."""
+    angles = np.ascontiguousarray(angles, dtype=np.float64)
+    cl = np.ascontiguousarray(cl, dtype=np.float64)
+    out = np.zeros(5)
+    if lib().orc_boundary(C.byref(cfg), code, _p(angles), _p(cl), _p(out)):
+        raise ValueError(f"no boundary code {code}")
     return out
 
 
@@ -113,6 +127,14 @@ class Oracle:
         if rc:
             raise RuntimeError(f"orc_rk3_step failed: {rc}")
         return U
+
+    def rk3_stage(self, Un: np.ndarray, U: np.ndarray, dt: float, stage: int) -> None:
+        """Stage `stage` (1..3) of one RK3 step, in place on U (U = Un before stage 1)."""
+        Un = np.ascontiguousarray(Un, dtype=np.float64)
+        assert U.flags.c_contiguous and U.dtype == np.float64
+        rc = lib().orc_rk3_stage(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), dt, stage, _p(Un), _p(U))
+        if rc:
+            raise RuntimeError(f"orc_rk3_stage failed: {rc}")
 
     def force(self, U: np.ndarray) -> float:
         """Wall pressure force in x (COMPUTEFORCE, inviscid part)."""

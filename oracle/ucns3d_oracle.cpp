@@ -26,7 +26,8 @@
 //                                                    src/flux_p.f90:478, riemann.f90:221, 1236, 28,
 //                                                    grid_t.f90:4217
 //   CALCULATE_FLUXESHI_DIFFUSIVE + SUTHERLAND        src/flux_p.f90:1520, flow_operations.f90:2609
-//   BOUNDARYS (inflow/outflow/symmetry/wall)         src/flow_operations.f90:2860-3230
+//   BOUNDARYS (inflow/outflow/symmetry/wall/far field, BOUNDTYPE 0|1)
+//                                                    src/flow_operations.f90:2860-3375
 //   RUNGE_KUTTA3, CALCULATE_CFL                      src/time_p.f90:885-1027, 27-191
 #include <algorithm>
 #include <cmath>
@@ -634,9 +635,10 @@ void riemann(const ucg_config* cfg, const double* cl, const double* cr, double* 
   else hllc(cfg->gamma, cl, cr, flux);
 }
 
-// ghost state of a physical boundary face (BOUNDARYS, boundtype 1 = subsonic
-// treatment, src/flow_operations.f90:2860-3230).  cfg->bc_state holds the
-// free-stream primitive state (rho, u, v, w, p) that INFLOW/OUTFLOW return.
+// ghost state of a physical boundary face (BOUNDARYS,
+// src/flow_operations.f90:2860-3375).  cfg->bc_state holds the free-stream
+// primitive state (rho, u, v, w, p) that INFLOW/OUTFLOW return
+// (flow_operations.f90:1161, 1526: RRES, uvel, vvel, wvel, PRES).
 void prim2cons(double gm, const double* p, double* u) {
   double skin = 0.5 * ((p[1] * p[1]) + (p[2] * p[2]) + (p[3] * p[3]));
   double ie = p[4] / ((gm - 1.0) * p[0]);
@@ -646,52 +648,99 @@ void prim2cons(double gm, const double* p, double* u) {
   u[3] = p[3] * p[0];
   u[4] = (p[0] * ie) + (p[0] * skin);
 }
+// subsonic inflow state of CASE(1) (:2911-2928) and of the CASE(6) inflow
+void subsonic_inflow(double gm, const double* s1, const double* s2, double sps, double nx, double ny, double nz,
+                     double* cr) {
+  double s3[NV];
+  s3[4] = 0.5 * ((s1[4]) + (s2[4]) - (s2[0] * sps * ((nx * (s1[1] - s2[1])) + (ny * (s1[2] - s2[2])) + (nz * (s1[3] - s2[3])))));
+  s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
+  s3[1] = s1[1] - (nx * (s1[4] - s3[4])) / (sps * s2[0]);
+  s3[2] = s1[2] - (ny * (s1[4] - s3[4])) / (sps * s2[0]);
+  s3[3] = s1[3] - (nz * (s1[4] - s3[4])) / (sps * s2[0]);
+  prim2cons(gm, s3, cr);
+}
+// subsonic outflow state of CASE(2) (:2997-3010) and of the CASE(6) outflow
+void subsonic_outflow(double gm, const double* s1, const double* s2, double sps, double nx, double ny, double nz,
+                      double* cr) {
+  double s3[NV];
+  s3[4] = s1[4];
+  s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
+  s3[1] = s2[1] + (nx * (s2[4] - s3[4])) / (sps * s2[0]);
+  s3[2] = s2[2] + (ny * (s2[4] - s3[4])) / (sps * s2[0]);
+  s3[3] = s2[3] + (nz * (s2[4] - s3[4])) / (sps * s2[0]);
+  prim2cons(gm, s3, cr);
+}
 void boundary_state(const Ctx& x, int code, const double* ang, const double* cl, double* cr) {
   const ucg_config* cfg = x.cfg;
   const double gm = cfg->gamma;
   double nx = ang[0] * ang[3], ny = ang[1] * ang[3], nz = ang[2];
-  if (code == 3 || code == 4) {  // symmetry; inviscid wall (ITESTCASE 3)
-    double rl[NV], rr[NV];
-    rotf(ang, cl, rl);
-    rr[0] = rl[0];
-    rr[1] = -rl[1];
-    rr[2] = rl[2];
-    rr[3] = rl[3];
-    rr[4] = rl[4];
-    rotb(ang, rr, cr);
-    return;
-  }
-  double s1[NV], s2[NV], s3[NV];
+  double s1[NV], s2[NV];
   for (int k = 0; k < NV; ++k) s1[k] = cfg->bc_state[k];
-  cons2prim(x, cl, s2);
-  double sps = std::sqrt((gm * s2[4]) / (s2[0]));
-  double vel = std::sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
-  bool super = vel / (sps + TOLSMALL) > 1.0;
-  if (code == 1) {  // inflow
-    if (super) {
-      prim2cons(gm, s1, cr);
+  switch (code) {
+    case 1: {  // INFLOW (:2883)
+      if (cfg->boundtype == 0) {  // supersonic: the free stream
+        prim2cons(gm, s1, cr);
+        return;
+      }
+      cons2prim(x, cl, s2);
+      double sps = std::sqrt((gm * s2[4]) / (s2[0]));
+      double vel = std::sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+      if (vel / (sps + TOLSMALL) > 1.0) prim2cons(gm, s1, cr);
+      else subsonic_inflow(gm, s1, s2, sps, nx, ny, nz, cr);
       return;
     }
-    s3[4] = 0.5 * ((s1[4]) + (s2[4]) - (s2[0] * sps * ((nx * (s1[1] - s2[1])) + (ny * (s1[2] - s2[2])) + (nz * (s1[3] - s2[3])))));
-    s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
-    s3[1] = s1[1] - (nx * (s1[4] - s3[4])) / (sps * s2[0]);
-    s3[2] = s1[2] - (ny * (s1[4] - s3[4])) / (sps * s2[0]);
-    s3[3] = s1[3] - (nz * (s1[4] - s3[4])) / (sps * s2[0]);
-  } else if (code == 2) {  // outflow
-    if (super) {
-      for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+    case 2: {  // OUTFLOW (:2972)
+      if (cfg->boundtype == 0) {  // supersonic: the cell's own state
+        for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+        return;
+      }
+      cons2prim(x, cl, s2);
+      double sps = std::sqrt((gm * s2[4]) / (s2[0]));
+      double vel = std::sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+      if (vel / (sps + TOLSMALL) > 1.0) {
+        for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+      } else {
+        subsonic_outflow(gm, s1, s2, sps, nx, ny, nz, cr);
+      }
       return;
     }
-    s3[4] = s1[4];
-    s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
-    s3[1] = s2[1] + (nx * (s2[4] - s3[4])) / (sps * s2[0]);
-    s3[2] = s2[2] + (ny * (s2[4] - s3[4])) / (sps * s2[0]);
-    s3[3] = s2[3] + (nz * (s2[4] - s3[4])) / (sps * s2[0]);
-  } else {  // any other code: free stream
-    prim2cons(gm, s1, cr);
-    return;
+    case 3:    // SYMMETRY (:3102)
+    case 4: {  // WALL, ITESTCASE 3 (:3140): the face-frame normal momentum mirrored
+      double rl[NV], rr[NV];
+      rotf(ang, cl, rl);
+      rr[0] = rl[0];
+      rr[1] = -rl[1];
+      rr[2] = rl[2];
+      rr[3] = rl[3];
+      rr[4] = rl[4];
+      rotb(ang, rr, cr);
+      return;
+    }
+    case 6: {  // FARFIELD (:3230): direction from vnb = the rotated conserved
+               // normal momentum, supersonic when |vnb| >= the sound speed
+      double rl[NV];
+      rotf(ang, cl, rl);
+      const double vnb = rl[1];
+      cons2prim(x, cl, s2);
+      double sps = std::sqrt((gm * s2[4]) / (s2[0]));
+      if (vnb <= 0.0) {
+        if (std::fabs(vnb) >= sps) prim2cons(gm, s1, cr);
+        else subsonic_inflow(gm, s1, s2, sps, nx, ny, nz, cr);
+      } else {
+        if (std::fabs(vnb) >= sps) {
+          for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+        } else {
+          subsonic_outflow(gm, s1, s2, sps, nx, ny, nz, cr);
+        }
+      }
+      return;
+    }
+    default: {  // no other code reaches the residual (the engine rejects them)
+      const double nan = std::nan("");
+      for (int k = 0; k < NV; ++k) cr[k] = nan;
+      return;
+    }
   }
-  prim2cons(gm, s3, cr);
 }
 
 // COMPUTE_EIGENVECTORS (flow_operations.f90:3934-3995): left (EL) and right
@@ -1101,6 +1150,29 @@ int orc_rk3_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* 
   return UCG_OK;
 }
 
+// One stage of RUNGE_KUTTA3 (src/time_p.f90:885-1027): stage 1 U = Un -
+// dt R(Un)/V (U holds Un on entry), stage 2 U = 3/4 Un + 1/4 U - 1/4 dt R(U)/V,
+// stage 3 U = 1/3 Un + 2/3 U - 2/3 dt R(U)/V, in place on U.
+int orc_rk3_stage(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt, int stage,
+                  const double* Un, double* U) {
+  if (!check_ctx(cfg, g, r) || !U || !Un || stage < 1 || stage > 3) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const int64_t n = g->ncells;
+  std::vector<double> rhs(n * NV), UL, ULV;
+  residual(x, U, rhs.data(), UL, ULV);
+  const double a[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, b[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0}, k[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  const int s = stage - 1;
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    double oov = 1.0 / g->volume[c];
+    for (int v = 0; v < NV; ++v) {
+      const double u = U[c * NV + v], rr = dt * (rhs[c * NV + v] * oov);
+      U[c * NV + v] = s == 0 ? Un[c * NV + v] - rr : (a[s] * Un[c * NV + v]) + (b[s] * u) - (k[s] * rr);
+    }
+  }
+  return UCG_OK;
+}
+
 // Wall force in x (COMPUTEFORCE, src/io.f90:18752-18915, inviscid part):
 // over faces with boundary code 4, SSP = sum_q p(ULEFT_q) * w_q - PRES, then
 // FORCEX += SSP * SURF * NX with NX = cos(angle1) * sin(angle2).
@@ -1137,6 +1209,16 @@ int orc_force(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, 
 int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
   hllc(gamma, cl, cr, flux);
   return UCG_OK;
+}
+
+// one ghost state of BOUNDARYS for boundary code `code` on a face of angles
+// (ANGLE1, ANGLE2); gamma, boundtype and the free stream come from cfg
+int orc_boundary(const ucg_config* cfg, int code, const double* angles, const double* cl, double* cr) {
+  Ctx x{};
+  x.cfg = cfg;
+  const double ang[4] = {std::cos(angles[0]), std::sin(angles[0]), std::cos(angles[1]), std::sin(angles[1])};
+  boundary_state(x, code, ang, cl, cr);
+  return (code == 1 || code == 2 || code == 3 || code == 4 || code == 6) ? UCG_OK : UCG_EINVAL;
 }
 
 // one global-frame flux of the Roe family (iRiemann 3 Roe, 4 rotated

@@ -32,6 +32,16 @@ SMALL = {
 }
 
 
+# far-field boundaries (code 6) on the two x sides of a box and, for the
+# tetrahedra, the two y sides; and the bump channel under BOUNDTYPE 0
+# (inflow faces take the free stream, outflow faces their own state)
+SMALL["muscl_farfield_hex"] = (lambda: Mesh.box_hex(10, 6, 6, L=(3.0, 1.0, 1.0), periodic=(0, 1, 1),
+                                                   bc=(6, 6, 0, 0, 0, 0)), SCHEME_MUSCL, 1, 0, EULER)
+SMALL["weno3_farfield_tet"] = (lambda: Mesh.box_tet(6, 6, 4, L=(3.0, 2.0, 1.0), periodic=(0, 0, 1),
+                                                    bc=(6, 6, 6, 6, 0, 0), seed=8), SCHEME_WENO, 2, 0, EULER)
+SMALL["muscl_bump_bt0"] = (lambda: Mesh.bump_channel(24, 10, 2, seed=2), SCHEME_MUSCL, 1, 0, EULER)
+FARFIELD = ("muscl_farfield_hex", "weno3_farfield_tet")
+
 # characteristic-variable WENO (WENWRT 2) on the WENO cases, and on a
 # channel with inflow/outflow/slip walls (boundary ghosts in the eigenvectors)
 SMALL["weno3_channel"] = (lambda: Mesh.bump_channel(16, 8, 8, seed=2), SCHEME_WENO, 2, 0, EULER)
@@ -44,8 +54,18 @@ def _setup(name, precision=N.UCG_FP64, wenwrt=1):
     p0 = 71.43
     bc = (1.0, 0.675 * np.sqrt(1.4), 0.0, 0.0, 1.0)
     cfg = make_config(m, governing=gov, precision=precision, reynolds=1600.0, pres=p0 if gov == NAVIER_STOKES else 1.0,
-                      prandtl=0.71, bc_state=bc, wenwrt=wenwrt)
-    if name in ("muscl_bump", "weno3_channel"):
+                      prandtl=0.71, bc_state=bc, wenwrt=wenwrt, boundtype=0 if name.endswith("_bt0") else 1)
+    if name in FARFIELD:
+        # a stream along x whose density and speed vary across the box: the
+        # far-field faces see inflow and outflow, subsonic and supersonic
+        # (in the reference's test on the normal momentum |rho u_n| >= c)
+        c = m.centres()
+        rho = 1.0 + 0.5 * np.sin(2 * np.pi * c[:, 1] / 2.0 + 0.3)
+        ux = np.sqrt(1.4) * (0.55 + 0.45 * np.cos(2 * np.pi * c[:, 1] / 2.0)) + 0.1 * np.sin(2 * np.pi * c[:, 0] / 3.0)
+        uy = 0.3 * np.sin(2 * np.pi * c[:, 0] / 3.0)
+        p = 1.0 + 0.1 * np.cos(2 * np.pi * c[:, 2])
+        U = np.stack([rho, rho * ux, rho * uy, 0.0 * rho, p / 0.4 + 0.5 * rho * (ux * ux + uy * uy)], axis=1)
+    elif name in ("muscl_bump", "weno3_channel", "muscl_bump_bt0"):
         U = m.initial_condition(1, [1.4, *bc])
         # a smooth disturbance so that every branch sees non-trivial data
         c = m.centres()

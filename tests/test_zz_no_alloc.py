@@ -1,5 +1,5 @@
 """The allocation-free entry point ucg_residual_muscl_static, through the C
-ABI, against the engine's ucg_residual on the same inputs.
+ABI, against the engine's ucg_residual and the oracle on the same inputs.
 
 Callers of ucg_residual_muscl_static cannot allocate device memory; the test
 itself is not such a caller, so it uses torch to place the inputs and
@@ -59,22 +59,45 @@ def _device_structs(mesh, dev):
     return gd, rd, keep
 
 
-@pytest.mark.parametrize("which", ["tgv_ns", "bump_euler"])
-def test_static_scratch_residual_matches_engine(which):
-    import torch
+def _static_fn():
     lib = N.engine()
     fn = lib.ucg_residual_muscl_static
     fn.restype = C.c_int
     fn.argtypes = [C.POINTER(N.UcgConfig), C.POINTER(N.UcgGeometry), C.POINTER(N.UcgRecon),
                    C.c_void_p, C.c_void_p, C.c_void_p]
-    c = cases.tgv_hex_muscl(n=16) if which == "tgv_ns" else cases.bump_muscl(nx=60, ny=20, nlayers=2)
+    return fn
+
+
+def _state(which, c):
     U = c.U0.copy()
+    cc = c.mesh.centres()
     if which == "bump_euler":
-        cc = c.mesh.centres()
         U[:, 0] *= 1.0 + 0.05 * np.sin(2 * np.pi * cc[:, 0] / 3.0) * np.sin(np.pi * cc[:, 1])
+    elif which == "bump_shock_tube":
+        # a density and pressure jump of 8x and 10x across x = 1.5: the limited
+        # face values next to it move the cell's density by more than 95 %,
+        # so CHECKSOLX sends those cells back to first order
+        hi = cc[:, 0] < 1.5
+        prim = np.where(hi[:, None], [1.0, 0.3, 0.0, 0.0, 1.0], [0.125, 0.3, 0.0, 0.0, 0.1])
+        U = np.stack([prim[:, 0], prim[:, 0] * prim[:, 1], prim[:, 0] * prim[:, 2], prim[:, 0] * prim[:, 3],
+                      prim[:, 4] / 0.4 + 0.5 * prim[:, 0] * (prim[:, 1:4] ** 2).sum(1)], axis=1)
+    return U
+
+
+@pytest.mark.parametrize("which", ["tgv_ns", "bump_euler", "bump_shock_tube"])
+def test_static_scratch_residual_matches_engine_and_oracle(which):
+    """Two calls in a row through the C ABI, each against the engine's
+    ucg_residual and the oracle's residual on the same inputs."""
+    import torch
+    from oracle import Oracle
+    fn = _static_fn()
+    c = cases.tgv_hex_muscl(n=16) if which == "tgv_ns" else cases.bump_muscl(nx=60, ny=20, nlayers=2)
+    U = _state(which, c)
     e = Engine(c.mesh, c.cfg)
     e.set_state(U)
     ref = e.call_flux_subroutines_3d()
+    e.close()
+    orc = Oracle(c.mesh, c.cfg).residual(U)
     dev = torch.device("cuda:0")
     gd, rd, keep = _device_structs(c.mesh, dev)
     scale = _flux_scale(c.mesh, U)
@@ -86,7 +109,54 @@ def test_static_scratch_residual_matches_engine(which):
         torch.cuda.synchronize()
         got = rhs.cpu().numpy()
         err = (np.abs(got - ref) / scale).max()
+        err_o = (np.abs(got - orc) / scale).max()
         assert err < 1e-12, (call, err)
+        assert err_o < 1e-12, (call, err_o)
+
+
+def test_static_scratch_unsupported_faces_give_nan():
+    """Faces the allocation-free path does not treat come back as NaN rows,
+    not as a plausible residual: every boundary cell of a Navier-Stokes
+    channel (the viscous wall treatment is not in this path), and a cell
+    whose boundary code is not one of 1, 2, 3, 4, 6.  Other rows stay
+    finite and equal to the engine's."""
+    import torch
+    from ucns3d_b200.config import NAVIER_STOKES, make_config
+    fn = _static_fn()
+    c = cases.bump_muscl(nx=30, ny=10, nlayers=2)
+    dev = torch.device("cuda:0")
+    g = c.mesh.geometry()
+    nf = g["nfaces"]
+    phys = ((g["neigh"] < 0) & (np.arange(F)[None, :] < nf[:, None])).any(1)
+    # Navier-Stokes with walls, inflow and outflow
+    cfg_ns = make_config(c.mesh, governing=NAVIER_STOKES, reynolds=1000.0, pres=1.0, prandtl=0.72,
+                         bc_state=tuple(c.cfg.bc_state))
+    gd, rd, keep = _device_structs(c.mesh, dev)
+    u = torch.from_numpy(c.U0).to(dev)
+    rhs = torch.zeros_like(u)
+    assert fn(C.byref(cfg_ns), C.byref(gd), C.byref(rd), C.c_void_p(u.data_ptr()), C.c_void_p(rhs.data_ptr()),
+              None) == N.UCG_OK
+    torch.cuda.synchronize()
+    got = rhs.cpu().numpy()
+    assert np.array_equal(np.isnan(got).any(1), phys)
+    assert np.isfinite(got[~phys]).all()
+    # Euler, one boundary face given code 5 (not a BOUNDARYS case here)
+    cell, face = [(i, f) for i in range(len(nf)) for f in range(nf[i]) if g["neigh"][i, f] < 0][3]
+    keep["bc"].view(-1)[cell * F + face] = 5
+    rhs = torch.zeros_like(u)
+    assert fn(C.byref(c.cfg), C.byref(gd), C.byref(rd), C.c_void_p(u.data_ptr()), C.c_void_p(rhs.data_ptr()),
+              None) == N.UCG_OK
+    torch.cuda.synchronize()
+    got = rhs.cpu().numpy()
+    bad_rows = np.nonzero(np.isnan(got).any(1))[0].tolist()
+    assert bad_rows == [cell]
+    e = Engine(c.mesh, c.cfg)
+    e.set_state(c.U0)
+    ref = e.call_flux_subroutines_3d()
+    e.close()
+    ok = np.ones(len(nf), bool)
+    ok[cell] = False
+    assert (np.abs(got[ok] - ref[ok]) / _flux_scale(c.mesh, c.U0)[ok]).max() < 1e-12
 
 
 def test_static_scratch_rejects_oversize_and_wrong_scheme():

@@ -80,6 +80,7 @@ struct Problem {
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
   int riemann;   // 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL
   int limiter;   // SLOPE_LIMITERS code (7 Venkatakrishnan)
+  int boundtype; // BOUNDTYPE: 0 supersonic inflow/outflow, 1 characteristic treatment
   double* dt_dev;           // device dt (ucg_step)
 };
 
@@ -687,10 +688,43 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long l
 
 namespace ucg {
 
-// Ghost state of a physical boundary face (BOUNDARYS, src/flow_operations.f90:2860-3230)
+// Ghost state of a physical boundary face (BOUNDARYS, src/flow_operations.f90:2860-3375)
 // and the viscous face flux (CALCULATE_FLUXESHI_DIFFUSIVE, src/flux_p.f90:1614-1779).
 // `bcs` is the free-stream state (primitive) of the inflow/outflow/far-field
-// conditions, normally Problem::bc_state.
+// conditions, normally Problem::bc_state.  Codes:
+//   1 inflow  (:2883): BOUNDTYPE 0 the free stream; BOUNDTYPE 1 the free stream
+//             when |u|/c > 1 at the cell, else the subsonic characteristic state
+//   2 outflow (:2972): BOUNDTYPE 0 the cell's own state; BOUNDTYPE 1 that state
+//             when |u|/c > 1, else the state at the free-stream pressure
+//   3 symmetry, 4 inviscid wall (:3102, :3140): normal momentum mirrored
+//   6 far field (:3230): inflow or outflow by the sign of the face-frame normal
+//             momentum rho*u_n of the cell, supersonic when |rho*u_n| >= c (the
+//             reference compares that momentum, not the velocity, with the sound
+//             speed), then the inflow or outflow states above
+// Subsonic states share the formulas of cases 1 and 2 (bc_sub_in, bc_sub_out).
+template <typename S>
+__host__ __device__ __forceinline__ void bc_sub_in(double gm, const S* s1, const S* s2, S sps, double nx, double ny,
+                                                   double nz, S* cr) {
+  S s3[NV];
+  s3[4] = 0.5 * (s1[4] + s2[4] - s2[0] * sps * (nx * (s1[1] - s2[1]) + ny * (s1[2] - s2[2]) + nz * (s1[3] - s2[3])));
+  s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
+  s3[1] = s1[1] - nx * (s1[4] - s3[4]) / (sps * s2[0]);
+  s3[2] = s1[2] - ny * (s1[4] - s3[4]) / (sps * s2[0]);
+  s3[3] = s1[3] - nz * (s1[4] - s3[4]) / (sps * s2[0]);
+  prim2cons(gm, s3, cr);
+}
+template <typename S>
+__host__ __device__ __forceinline__ void bc_sub_out(double gm, const S* s1, const S* s2, S sps, double nx, double ny,
+                                                    double nz, S* cr) {
+  S s3[NV];
+  s3[4] = s1[4];
+  s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
+  s3[1] = s2[1] + nx * (s2[4] - s3[4]) / (sps * s2[0]);
+  s3[2] = s2[2] + ny * (s2[4] - s3[4]) / (sps * s2[0]);
+  s3[3] = s2[3] + nz * (s2[4] - s3[4]) / (sps * s2[0]);
+  prim2cons(gm, s3, cr);
+}
+
 template <typename S>
 __host__ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const S* cl, const S* bcs,
                                                S* cr) {
@@ -707,39 +741,40 @@ __host__ __device__ __forceinline__ void boundary_ghost(const Problem& p, int co
     rot_b(r, b, cr);
     return;
   }
-  S s1[NV], s2[NV], s3[NV];
+  S s1[NV], s2[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) s1[k] = bcs[k];
-  cons2prim(gm, cl, s2);
-  S sps = sqrt(gm * s2[4] / s2[0]);
-  S vel = sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
-  bool super = value(vel / (sps + TOLSMALL)) > 1.0;
-  if (code == 1) {  // inflow (BOUNDARYS case 1, subsonic characteristic treatment)
-    if (super) {
+  if (p.boundtype == 0 && (code == 1 || code == 2)) {  // BOUNDTYPE 0: supersonic treatment
+    if (code == 1) {
       prim2cons(gm, s1, cr);
-      return;
-    }
-    s3[4] = 0.5 * (s1[4] + s2[4] - s2[0] * sps * (nx * (s1[1] - s2[1]) + ny * (s1[2] - s2[2]) + nz * (s1[3] - s2[3])));
-    s3[0] = s1[0] + (s3[4] - s1[4]) / (sps * sps);
-    s3[1] = s1[1] - nx * (s1[4] - s3[4]) / (sps * s2[0]);
-    s3[2] = s1[2] - ny * (s1[4] - s3[4]) / (sps * s2[0]);
-    s3[3] = s1[3] - nz * (s1[4] - s3[4]) / (sps * s2[0]);
-  } else if (code == 2) {  // outflow (case 2)
-    if (super) {
+    } else {
 #pragma unroll
       for (int k = 0; k < NV; ++k) cr[k] = cl[k];
-      return;
     }
-    s3[4] = s1[4];
-    s3[0] = s2[0] + (s3[4] - s2[4]) / (sps * sps);
-    s3[1] = s2[1] + nx * (s2[4] - s3[4]) / (sps * s2[0]);
-    s3[2] = s2[2] + ny * (s2[4] - s3[4]) / (sps * s2[0]);
-    s3[3] = s2[3] + nz * (s2[4] - s3[4]) / (sps * s2[0]);
-  } else {
-    prim2cons(gm, s1, cr);
     return;
   }
-  prim2cons(gm, s3, cr);
+  cons2prim(gm, cl, s2);
+  S sps = sqrt(gm * s2[4] / s2[0]);
+  bool in, super;
+  if (code == 6) {
+    S a[NV];
+    rot_f(r, cl, a);
+    in = value(a[1]) <= 0.0;
+    super = fabs(value(a[1])) >= value(sps);
+  } else {
+    S vel = sqrt(s2[1] * s2[1] + s2[2] * s2[2] + s2[3] * s2[3]);
+    in = code == 1;
+    super = value(vel / (sps + TOLSMALL)) > 1.0;
+  }
+  if (in) {
+    if (super) prim2cons(gm, s1, cr);
+    else bc_sub_in(gm, s1, s2, sps, nx, ny, nz, cr);
+  } else if (super) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) cr[k] = cl[k];
+  } else {
+    bc_sub_out(gm, s1, s2, sps, nx, ny, nz, cr);
+  }
 }
 
 __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const double* r, const double* cl,

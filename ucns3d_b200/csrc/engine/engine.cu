@@ -142,6 +142,7 @@ Problem make_problem(ucg_engine* e) {
   p.wenwrt = c.wenwrt;
   p.riemann = c.riemann;
   p.limiter = c.limiter;
+  p.boundtype = c.boundtype;
   return p;
 }
 
@@ -256,9 +257,9 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
       c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && ((c.ideg2 != 3 && c.ideg2 != 9) || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
       c.gamma <= 1.0 || c.limiter < 1 || c.limiter > 9 || !((c.riemann >= 1 && c.riemann <= 5) || c.riemann == 9) ||
-      !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3))) {
+      !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3)) || (c.boundtype != 0 && c.boundtype != 1)) {
     g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC/Rusanov/Roe/rotated Roe-HLL/t-Roe/HLL, limiter 1..9, "
-                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9)";
+                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9, boundtype 0|1)";
     return UCG_EINVAL;
   }
   if (c.scheme == 2 && c.admis_max != 1) {

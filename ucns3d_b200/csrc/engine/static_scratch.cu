@@ -8,6 +8,7 @@
 // computation needs, the face values (and, for Navier-Stokes, the face
 // gradients) of every cell, lives in a fixed file-scope device array below,
 // which every GPU that loads this library holds until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -26,25 +27,72 @@ constexpr int kNSPerCell = MF * NV + MF * 12;   // + face gradients of T,u,v,w
 
 static __device__ __align__(256) double g_scratch[kScratchDoubles];
 
-// Device address of g_scratch, looked up once per device.  In host code the
-// name g_scratch is only a host-side stand-in, never a device address.
-std::mutex g_mu;
-double* g_addr[128] = {nullptr};
+// Device address of g_scratch, looked up once per CUDA context.  In host
+// code the name g_scratch is only a host-side stand-in, never a device
+// address, and a __device__ variable's address belongs to a context, not to
+// a device ordinal: a caller may make its own context current
+// (cuCtxCreate/cuCtxSetCurrent), and a cudaDeviceReset replaces the primary
+// context.  The cache is therefore keyed by the context's unique id
+// (cuCtxGetId, reached through the runtime's driver entry points, so the
+// library does not link libcuda itself).
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
 
-int scratch_on_current_device(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return UCG_ECUDA;
+struct ScratchAddr {
+  unsigned long long ctx_id;
+  double* addr;
+};
+
+std::mutex g_mu;
+ScratchAddr g_addr[64];
+int g_naddr = 0, g_next = 0;
+PfnCtxGetCurrent g_get_current = nullptr;
+PfnCtxGetId g_get_id = nullptr;
+bool g_resolved = false;
+
+bool current_context_id(unsigned long long* id) {
+  CUcontext ctx = nullptr;
+  if (g_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return g_get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+int scratch_in_current_context(double** out) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
-    void* ptr = nullptr;
-    cudaError_t st = cudaGetSymbolAddress(&ptr, g_scratch);
-    if (st != cudaSuccess || !ptr) {
-      cudaGetLastError();
-      return UCG_ECUDA;
-    }
-    g_addr[dev] = (double*)ptr;
+  if (!g_resolved) {
+    g_resolved = true;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", (void**)&g_get_current, 12000, cudaEnableDefault, &q1) !=
+            cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess)
+      g_get_current = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", (void**)&g_get_id, 12000, cudaEnableDefault, &q2) !=
+            cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess)
+      g_get_id = nullptr;
+    cudaGetLastError();
   }
-  *out = g_addr[dev];
+  if (!g_get_current || !g_get_id) return UCG_ECUDA;
+  unsigned long long id = 0;
+  const bool have_ctx = current_context_id(&id);
+  if (have_ctx)
+    for (int i = 0; i < g_naddr; ++i)
+      if (g_addr[i].ctx_id == id) {
+        *out = g_addr[i].addr;
+        return UCG_OK;
+      }
+  // first call in this context (which this lookup creates if the thread had
+  // none): the symbol's address in the current context
+  void* ptr = nullptr;
+  cudaError_t st = cudaGetSymbolAddress(&ptr, g_scratch);
+  if (st != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    return UCG_ECUDA;
+  }
+  if (!have_ctx && !current_context_id(&id)) return UCG_ECUDA;
+  ScratchAddr& slot = g_naddr < 64 ? g_addr[g_naddr++] : g_addr[g_next++ % 64];
+  slot.ctx_id = id;
+  slot.addr = (double*)ptr;
+  *out = (double*)ptr;
   return UCG_OK;
 }
 
@@ -169,8 +217,16 @@ __global__ void k_static_flux(Problem p, ucg_geometry g, const double* __restric
   const int nf = c < g.ncells && f < MF ? g.neigh_face[c * MF + f] : 0;
   const bool in = c < g.ncells, badn = in && (nfc < 1 || nfc > MF);
   const bool ok = in && !badn && f < nfc;
-  if ((badn && f == 0) || (ok && (nb >= g.ncells || (nb >= 0 && (nf < 0 || nf >= MF))))) {
-    // count or index out of range in caller memory: NaN instead of following it
+  const int ft = ok ? g.face_type[c * MF + f] : 5;
+  const int code = ok && nb < 0 ? g.bc[c * MF + f] : 0;
+  // a physical face this path does not treat: Navier-Stokes walls and
+  // boundaries (the reference's CALCULATE_BOUNDED_VISCOUS) and codes other
+  // than inflow 1, outflow 2, symmetry 3, wall 4 and far field 6
+  const bool unsupported = ok && nb < 0 && (NS || !(code == 1 || code == 2 || code == 3 || code == 4 || code == 6));
+  if ((badn && f == 0) || (ok && (nb >= g.ncells || (nb >= 0 && (nf < 0 || nf >= MF)))) ||
+      (ok && ft != 5 && ft != 6) || unsupported) {
+    // count, index or code out of range in caller memory, or a face this
+    // path does not treat: NaN instead of a plausible-looking residual
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = __longlong_as_double(0x7ff8000000000000LL);
   } else if (ok) {
@@ -182,7 +238,7 @@ __global__ void k_static_flux(Problem p, ucg_geometry g, const double* __restric
     if (nb >= 0) {
       cr = scratch + nb * per + nf * NV;
     } else {
-      boundary_ghost(p, g.bc[c * MF + f], rt, cl, crb);
+      boundary_ghost(p, code, rt, cl, crb);
       cr = crb;
     }
     double a[NV], b[NV], h[NV], fl[NV];
@@ -190,7 +246,7 @@ __global__ void k_static_flux(Problem p, ucg_geometry g, const double* __restric
     rot_f(rt, cl, a);
     hllc(p.gamma, a, b, h);
     rot_b(rt, h, fl);
-    const double ws = p.quad_w[0] * g.face_area[c * MF + f];
+    const double ws = (ft == 5 ? p.quad_w[0] : p.tri_w[0]) * g.face_area[c * MF + f];
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = fl[v] * ws;
     if (NS && nb >= 0) {
@@ -223,14 +279,15 @@ extern "C" int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geomet
                                          const double* u, double* rhs, void* stream) {
   if (!cfg || !geo || !rec || !u || !rhs) return UCG_EINVAL;
   if (cfg->scheme != 2 || cfg->iorder != 1 || cfg->ideg != 3 || cfg->admis_max != 1 || cfg->nq_quad != 1 ||
-      cfg->nq_tri != 1 || cfg->limiter != 7 || cfg->riemann != 1 || (cfg->governing != 1 && cfg->governing != 2))
+      cfg->nq_tri != 1 || cfg->limiter != 7 || cfg->riemann != 1 || (cfg->governing != 1 && cfg->governing != 2) ||
+      (cfg->boundtype != 0 && cfg->boundtype != 1))
     return UCG_EINVAL;
   const int64_t n = geo->ncells;
   if (n <= 0 || rec->first != 0 || rec->count != n || !rec->stencil || !rec->invmat) return UCG_EINVAL;
   const bool ns = cfg->governing == 1;
   if ((long long)n * (ns ? kNSPerCell : kEulerPerCell) > kScratchDoubles) return UCG_EINVAL;  // beyond the fixed scratch
   double* scratch = nullptr;
-  int rc = scratch_on_current_device(&scratch);
+  int rc = scratch_in_current_context(&scratch);
   if (rc) return rc;
   Problem p{};
   p.n = n;
@@ -246,6 +303,7 @@ extern "C" int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geomet
   p.quad_w[0] = cfg->quad_w[0];
   p.tri_w[0] = cfg->tri_w[0];
   for (int v = 0; v < NV; ++v) p.bc_state[v] = cfg->bc_state[v];
+  p.boundtype = cfg->boundtype;
   cudaStream_t s = (cudaStream_t)stream;
   const unsigned b1 = (unsigned)((n + 127) / 128), b2 = (unsigned)((n * 8 + 255) / 256);
   if (ns) {
