@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=None,
                     help="RK3 steps of the accuracy run (mixed against FP64; the vortex also against the analytic "
                          "solution): default 100 for the vortex, the workload's own step count otherwise; 0 skips")
+    ap.add_argument("--shuffle", action="store_true",
+                    help="hand the mesh over in a seeded random cell numbering (as from a partitioner) and time "
+                         "it with the engine's renumbering on (the line's value) and off (shuffle.reorder_off)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-n", type=int, default=0,
                     help="mesh size of the CPU baseline and reference arm (0: the benchmarked --n)")
@@ -220,7 +223,14 @@ def make_case(args, precision):
         kw["n"] = args.n
     if args.case == "vortex_hex_weno5" and args.wenwrt != 1:
         kw["wenwrt"] = args.wenwrt
-    return fn(**kw)
+    c = fn(**kw)
+    if args.shuffle:
+        import numpy as np
+        from ucns3d_b200.mesh import RenumberedMesh
+        order = np.random.default_rng(2024).permutation(c.mesh.ncells)
+        c = cases.Case(c.name, RenumberedMesh(c.mesh, order), c.cfg, np.ascontiguousarray(c.U0[order]), c.cfl,
+                       c.steps, dict(c.meta, shuffled=True))
+    return c
 
 
 def run_gpu(args, case, ws, local, timed_e2e=True):
@@ -488,6 +498,19 @@ def main():
         c64 = Case(c32.name, c32.mesh, cfg64, c32.U0, c32.cfl, c32.steps, c32.meta)
         r64 = run_gpu(args, c64, ws, local, timed_e2e=False)
         del c64
+    shuffle = None
+    if args.shuffle:
+        # the same shuffled numbering with the engine's renumbering off
+        from ucns3d_b200.cases import Case
+        cfg0 = N.UcgConfig.from_buffer_copy(c32.cfg)
+        cfg0.reorder = 0
+        r0 = run_gpu(args, Case(c32.name, c32.mesh, cfg0, c32.U0, c32.cfl, c32.steps, c32.meta), ws, local,
+                     timed_e2e=False)
+        ms0 = max_over_ranks(r0["ms"], ws, local)
+        shuffle = {"numbering": "seeded random permutation of the cells",
+                   "reorder_on": {"ms_per_step": None, "kernel_ms": r32["kern"]},
+                   "reorder_off": {"value": ws * ncells * 3 * args.steps / (ms0 / 1000.0),
+                                   "ms_per_step": ms0 / args.steps, "kernel_ms": r0["kern"]}}
     ms = max_over_ranks(r32["ms"], ws, local)
     value = ws * ncells * 3 * args.steps / (ms / 1000.0)
     e2e_s = max_over_ranks(r32["e2e"]["seconds"], ws, local)
@@ -526,6 +549,10 @@ def main():
         "clocks": r32["clocks"],
         "device_bytes": r32["device_bytes"],
     }
+    if shuffle is not None:
+        shuffle["reorder_on"]["ms_per_step"] = ms / args.steps
+        out["shuffle"] = shuffle
+        out["config"]["numbering"] = "shuffled (engine renumbering on)"
     if r64 is not None:
         ms64 = max_over_ranks(r64["ms"], ws, local)
         v64 = ws * ncells * 3 * args.steps / (ms64 / 1000.0)

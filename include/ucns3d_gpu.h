@@ -101,6 +101,16 @@ typedef struct ucg_config {
                           1 the characteristic subsonic treatment where |u| < c
                           (BOUNDARYS, flow_operations.f90:2883-3012).  The far field
                           (code 6, :3230) does not depend on it                       */
+  int32_t reorder;     /* 0 keep the caller's cell order on the device; 1 renumber the
+                          cells internally by reverse Cuthill-McKee on the face-
+                          neighbour graph at ucg_upload_geometry, so that the stencil
+                          and face gathers of a mesh in partitioner or file order
+                          touch nearby memory.  Every [n][5] array of the ABI stays
+                          in the caller's order (permuted on the device), and each
+                          face flux is still evaluated by the face side of the lower
+                          caller index, so the results are bitwise those of
+                          reorder 0 except for domain sums (ucg_reduce, ucg_force),
+                          whose order of addition changes                         */
 } ucg_config;
 
 /* Per-cell geometry (IELEM(N,I) and the small parts of ILOCAL_RECON3(I),

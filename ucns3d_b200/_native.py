@@ -47,7 +47,7 @@ class UcgConfig(C.Structure):
         ("lamx", C.c_double),
         ("quad_w", C.c_double * UCG_MAX_QP), ("tri_w", C.c_double * UCG_MAX_QP),
         ("bc_state", C.c_double * UCG_NV),
-        ("boundtype", C.c_int32),
+        ("boundtype", C.c_int32), ("reorder", C.c_int32),
     ]
 
 

@@ -19,7 +19,7 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
                 ufreestream: float = 1.0, pres: float = 1.0, char_length: float = 1.0,
                 lwci: float = 1000.0, wenoz: int = 0, limiter: int = 7,
                 bc_state=(1.0, 0.0, 0.0, 0.0, 1.0), lamx: float = 1.0, wenwrt: int = 1,
-                riemann: int = 1, boundtype: int = 1) -> N.UcgConfig:
+                riemann: int = 1, boundtype: int = 1, reorder: int = 1) -> N.UcgConfig:
     """A ucg_config for a prepared mesh.  ``reynolds`` sets VISC for
     Navier-Stokes; ``bc_state`` is the free-stream primitive state used by
     inflow/outflow/far-field boundaries; ``boundtype`` is BOUNDTYPE (0 supersonic
@@ -54,6 +54,7 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
     cfg.kappa_ven = 10.0
     cfg.lamx = lamx
     cfg.boundtype = boundtype
+    cfg.reorder = reorder
     for k in range(5):
         cfg.bc_state[k] = bc_state[k]
     return cfg

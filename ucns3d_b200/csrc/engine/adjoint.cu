@@ -1068,11 +1068,14 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   return UCG_OK;
 }
 
+// host <-> device; [n][5] per-cell arrays go through the caller's cell order
 int copy_in(ucg_engine* e, double* dst, const double* src, size_t count) {
+  if (count == (size_t)e->n * NV) return cells_in(e, dst, src);
   CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyHostToDevice, e->stream));
   return UCG_OK;
 }
 int copy_out(ucg_engine* e, double* dst, const double* src, size_t count) {
+  if (count == (size_t)e->n * NV) return cells_out(e, dst, src);
   CK(cudaMemcpyAsync(dst, src, count * 8, cudaMemcpyDeviceToHost, e->stream));
   return UCG_OK;
 }

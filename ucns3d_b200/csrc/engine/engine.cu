@@ -225,6 +225,103 @@ int rk3(ucg_engine* e, double dt, bool dt_dev) {
   return UCG_OK;
 }
 
+// Reverse Cuthill-McKee order of the face-neighbour graph: each connected
+// component is numbered breadth first from a pseudo-peripheral cell (the
+// far end of two breadth-first sweeps started at a cell of least degree),
+// neighbours in order of increasing degree, then the whole order is
+// reversed.  Ties are broken by the caller's index, so the order is
+// deterministic.  n2o[c] = the caller's cell at position c.
+void rcm_order(int64_t n, const int32_t* nfaces, const int32_t* neigh, std::vector<int32_t>& n2o) {
+  std::vector<int32_t> deg(n, 0);
+  auto nbr = [&](int64_t c, int f) -> int64_t {
+    const int64_t y = neigh[c * MF + f];
+    return (f < nfaces[c] && y >= 0 && y != c) ? y : -1;
+  };
+  for (int64_t c = 0; c < n; ++c)
+    for (int f = 0; f < MF; ++f) deg[c] += nbr(c, f) >= 0;
+  std::vector<int32_t> mark(n, -1), order, queue;
+  order.reserve(n);
+  queue.reserve(n);
+  int32_t stamp = 0;
+  // breadth-first sweep from `s` over the unnumbered cells; returns the last
+  // level's cell of least degree; appends the visit order to `out` if given
+  auto sweep = [&](int64_t s, std::vector<int32_t>* out) -> int64_t {
+    const int32_t tag = stamp++;
+    queue.clear();
+    queue.push_back((int32_t)s);
+    mark[s] = tag;
+    size_t head = 0, level_start = 0;
+    while (head < queue.size()) {
+      const size_t level_end = queue.size();
+      level_start = head;
+      for (; head < level_end; ++head) {
+        const int64_t u = queue[head];
+        int32_t nb[MF];
+        int k = 0;
+        for (int f = 0; f < MF; ++f) {
+          const int64_t y = nbr(u, f);
+          if (y >= 0 && mark[y] != tag && mark[y] != -2) {
+            mark[y] = tag;
+            nb[k++] = (int32_t)y;
+          }
+        }
+        std::sort(nb, nb + k, [&](int32_t a, int32_t b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+        for (int j = 0; j < k; ++j) queue.push_back(nb[j]);
+      }
+    }
+    if (out) out->insert(out->end(), queue.begin(), queue.end());
+    int64_t best = queue[level_start];
+    for (size_t i = level_start; i < queue.size(); ++i)
+      if (deg[queue[i]] < deg[best] || (deg[queue[i]] == deg[best] && queue[i] < best)) best = queue[i];
+    return best;
+  };
+  std::vector<int32_t> comp;
+  for (int64_t s0 = 0; s0 < n; ++s0) {
+    if (mark[s0] == -2) continue;
+    // least-degree cell of this component (found by a first sweep)
+    comp.clear();
+    sweep(s0, &comp);
+    int64_t start = comp[0];
+    for (int32_t c : comp)
+      if (deg[c] < deg[start] || (deg[c] == deg[start] && c < start)) start = c;
+    start = sweep(start, nullptr);
+    start = sweep(start, nullptr);
+    comp.clear();
+    sweep(start, &comp);
+    for (int32_t c : comp) mark[c] = -2;  // numbered
+    order.insert(order.end(), comp.begin(), comp.end());
+  }
+  n2o.assign(order.rbegin(), order.rend());
+}
+
+int cells_in(ucg_engine* e, double* dev_dst, const double* host_src) {
+  const size_t bytes = (size_t)e->n * NV * 8;
+  if (e->n2o.empty()) {
+    CK(cudaMemcpyAsync(dev_dst, host_src, bytes, cudaMemcpyHostToDevice, e->stream));
+    return UCG_OK;
+  }
+  CK(cudaMemcpyAsync(e->permbuf.p, host_src, bytes, cudaMemcpyHostToDevice, e->stream));
+  k_perm_rows<true><<<(unsigned)((e->n * NV + 255) / 256), 256, 0, e->stream>>>(
+      (const int32_t*)e->d_n2o.p, (const double*)e->permbuf.p, dev_dst, e->n);
+  e->launches++;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int cells_out(ucg_engine* e, double* host_dst, const double* dev_src) {
+  const size_t bytes = (size_t)e->n * NV * 8;
+  if (e->n2o.empty()) {
+    CK(cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, e->stream));
+    return UCG_OK;
+  }
+  k_perm_rows<false><<<(unsigned)((e->n * NV + 255) / 256), 256, 0, e->stream>>>(
+      (const int32_t*)e->d_n2o.p, dev_src, (double*)e->permbuf.p, e->n);
+  e->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host_dst, e->permbuf.p, bytes, cudaMemcpyDeviceToHost, e->stream));
+  return UCG_OK;
+}
+
 int cfl_device(ucg_engine* e, double cfl) {
   Problem p = make_problem(e);
   k_dt_init<<<1, 1, 0, e->stream>>>((double*)e->dt.p);
@@ -257,9 +354,10 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (!okscheme || c.ideg != ideg || c.imax < ideg || c.admis_max < 1 || c.admis_max > 7 || c.nq_quad < 1 ||
       c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && ((c.ideg2 != 3 && c.ideg2 != 9) || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
       c.gamma <= 1.0 || c.limiter < 1 || c.limiter > 9 || !((c.riemann >= 1 && c.riemann <= 5) || c.riemann == 9) ||
-      !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3)) || (c.boundtype != 0 && c.boundtype != 1)) {
+      !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3)) || (c.boundtype != 0 && c.boundtype != 1) ||
+      (c.reorder != 0 && c.reorder != 1)) {
     g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC/Rusanov/Roe/rotated Roe-HLL/t-Roe/HLL, limiter 1..9, "
-                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9, boundtype 0|1)";
+                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9, boundtype 0|1, reorder 0|1)";
     return UCG_EINVAL;
   }
   if (c.scheme == 2 && c.admis_max != 1) {
@@ -365,7 +463,7 @@ void ucg_destroy(ucg_engine* e) {
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
-                   &e->qbuf};
+                   &e->qbuf, &e->d_n2o, &e->permbuf};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -383,69 +481,94 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   const int64_t n = e->n;
   const int QS = e->QS, ideg = e->cfg.ideg;
   const bool ns = e->cfg.governing == 1;
-  std::vector<int8_t> nfaces(n), ftype(n * MF), nface(n * MF), bc(n * MF), admis(n), full(n);
-  std::vector<int32_t> neigh(n * MF);
-  std::vector<uint8_t> qperm((size_t)n * MF * QS);
-  std::vector<double> rot((size_t)n * MF * 4), area(n * MF), dih(n * MF), vol(n), minedge(n), jinv(n * 9);
+  if (n >= (int64_t(1) << 28)) return fail(e, UCG_EINVAL, "too many cells (face codes are 32-bit)");
+  // validate in the caller's order first (the renumbering follows the
+  // neighbour lists, which must be in range)
   for (int64_t c = 0; c < n; ++c) {
     int nf = g->nfaces[c];
     if (nf < 4 || nf > MF) return fail(e, UCG_EINVAL, "cell " + std::to_string(c) + " has " + std::to_string(nf) + " faces");
     if (!(g->volume[c] > 0.0)) return fail(e, UCG_EINVAL, "non-positive cell volume at cell " + std::to_string(c));
     int adm = g->admis[c];
     if (adm < 1 || adm > e->cfg.admis_max) return fail(e, UCG_EINVAL, "ADMIS out of range at cell " + std::to_string(c));
-    nfaces[c] = (int8_t)nf;
-    admis[c] = (int8_t)adm;
-    full[c] = (int8_t)(g->full[c] ? 1 : 0);
-    vol[c] = g->volume[c];
-    minedge[c] = g->minedge[c];
-    for (int k = 0; k < 9; ++k) jinv[c * 9 + k] = g->invccjac[c * 9 + k];
-    for (int f = 0; f < MF; ++f) {
+    for (int f = 0; f < nf; ++f) {
       int64_t i = c * MF + f;
-      ftype[i] = (int8_t)g->face_type[i];
-      neigh[i] = f < nf ? g->neigh[i] : -1;
-      nface[i] = (int8_t)(f < nf ? g->neigh_face[i] : -1);
-      bc[i] = (int8_t)(f < nf ? g->bc[i] : 0);
-      area[i] = g->face_area[i];
-      dih[i] = g->dih[i];
-      double a1 = g->face_angle[i * 2], a2 = g->face_angle[i * 2 + 1];
+      int ft = g->face_type[i];
+      if (ft != 5 && ft != 6) return fail(e, UCG_EINVAL, "face type must be 5 or 6");
+      int64_t nb = g->neigh[i];
+      if (nb >= n || nb < -1) return fail(e, UCG_EINVAL, "neighbour index out of range at cell " + std::to_string(c));
+      if (nb >= 0 && (g->neigh_face[i] < 0 || g->neigh_face[i] >= MF))
+        return fail(e, UCG_EINVAL, "neighbour face out of range at cell " + std::to_string(c));
+      if (nb < 0) {
+        int code = g->bc[i];
+        if (ns) return fail(e, UCG_EINVAL, "Navier-Stokes with physical boundary faces is not supported");
+        if (code != 1 && code != 2 && code != 3 && code != 4 && code != 6)
+          return fail(e, UCG_EINVAL, "unsupported boundary code " + std::to_string(code));
+      }
+      int nq = ft == 5 ? e->cfg.nq_quad : e->cfg.nq_tri;
+      for (int q = 0; q < nq; ++q) {
+        int qq = g->qperm[i * UCG_MAX_QP + q];
+        if (qq < 0 || qq >= nq) return fail(e, UCG_EINVAL, "qperm out of range at cell " + std::to_string(c));
+      }
+    }
+  }
+  // device order: n2o[c] = the caller's cell stored at device cell c
+  e->n2o.clear();
+  e->o2n.clear();
+  if (e->cfg.reorder == 1) {
+    rcm_order(n, g->nfaces, g->neigh, e->n2o);
+    e->o2n.assign(n, -1);
+    for (int64_t c = 0; c < n; ++c) e->o2n[e->n2o[c]] = (int32_t)c;
+  }
+  const bool perm = !e->n2o.empty();
+  auto src = [&](int64_t c) -> int64_t { return perm ? e->n2o[c] : c; };
+  auto dst = [&](int64_t o) -> int64_t { return perm ? e->o2n[o] : o; };
+  std::vector<int8_t> nfaces(n), ftype(n * MF), nface(n * MF), bc(n * MF), admis(n), full(n);
+  std::vector<int32_t> neigh(n * MF);
+  std::vector<uint8_t> qperm((size_t)n * MF * QS);
+  std::vector<double> rot((size_t)n * MF * 4), area(n * MF), dih(n * MF), vol(n), minedge(n), jinv(n * 9);
+  for (int64_t c = 0; c < n; ++c) {
+    const int64_t o = src(c);
+    const int nf = g->nfaces[o];
+    nfaces[c] = (int8_t)nf;
+    admis[c] = (int8_t)g->admis[o];
+    full[c] = (int8_t)(g->full[o] ? 1 : 0);
+    vol[c] = g->volume[o];
+    minedge[c] = g->minedge[o];
+    for (int k = 0; k < 9; ++k) jinv[c * 9 + k] = g->invccjac[o * 9 + k];
+    for (int f = 0; f < MF; ++f) {
+      const int64_t i = c * MF + f, io = o * MF + f;
+      ftype[i] = (int8_t)g->face_type[io];
+      const int64_t nb = f < nf ? g->neigh[io] : -1;
+      neigh[i] = (int32_t)(nb >= 0 ? dst(nb) : -1);
+      nface[i] = (int8_t)(f < nf ? g->neigh_face[io] : -1);
+      bc[i] = (int8_t)(f < nf ? g->bc[io] : 0);
+      area[i] = g->face_area[io];
+      dih[i] = g->dih[io];
+      double a1 = g->face_angle[io * 2], a2 = g->face_angle[io * 2 + 1];
       rot[i * 4 + 0] = cos(a1);
       rot[i * 4 + 1] = sin(a1);
       rot[i * 4 + 2] = cos(a2);
       rot[i * 4 + 3] = sin(a2);
       if (f < nf) {
-        int ft = g->face_type[i];
-        if (ft != 5 && ft != 6) return fail(e, UCG_EINVAL, "face type must be 5 or 6");
-        int64_t nb = g->neigh[i];
-        if (nb >= n || nb < -1) return fail(e, UCG_EINVAL, "neighbour index out of range at cell " + std::to_string(c));
-        if (nb >= 0 && (g->neigh_face[i] < 0 || g->neigh_face[i] >= MF))
-          return fail(e, UCG_EINVAL, "neighbour face out of range at cell " + std::to_string(c));
-        if (nb < 0) {
-          int code = g->bc[i];
-          if (ns) return fail(e, UCG_EINVAL, "Navier-Stokes with physical boundary faces is not supported");
-          if (code != 1 && code != 2 && code != 3 && code != 4 && code != 6)
-            return fail(e, UCG_EINVAL, "unsupported boundary code " + std::to_string(code));
-        }
-        int nq = ft == 5 ? e->cfg.nq_quad : e->cfg.nq_tri;
-        for (int q = 0; q < QS; ++q) {
-          int qq = q < nq ? g->qperm[i * UCG_MAX_QP + q] : 0;
-          if (qq < 0 || qq >= nq) return fail(e, UCG_EINVAL, "qperm out of range at cell " + std::to_string(c));
-          qperm[(size_t)i * QS + q] = (uint8_t)qq;
-        }
+        int nq = ftype[i] == 5 ? e->cfg.nq_quad : e->cfg.nq_tri;
+        for (int q = 0; q < QS; ++q) qperm[(size_t)i * QS + q] = (uint8_t)(q < nq ? g->qperm[io * UCG_MAX_QP + q] : 0);
       }
     }
   }
-  if (n >= (int64_t(1) << 28)) return fail(e, UCG_EINVAL, "too many cells (face codes are 32-bit)");
   // owned faces, grouped: interior faces, then mirror boundaries (symmetry,
-  // slip wall), then the other boundaries (each group in cell order), so
-  // that kernels branching on the face kind see uniform warps
+  // slip wall), then the other boundaries (each group in device cell order),
+  // so that kernels branching on the face kind see uniform warps.  An
+  // interior face belongs to the side of the lower caller index, so the
+  // renumbering leaves every face flux bit for bit as it was.
   std::vector<int32_t> own, own_mir, own_bnd;
   own.reserve(n * 3);
   for (int64_t c = 0; c < n; ++c)
     for (int f = 0; f < nfaces[c]; ++f) {
-      int64_t nb = neigh[c * MF + f];
+      const int64_t nb = neigh[c * MF + f];
       const int32_t code = (int32_t)(c * 8 + f);
       if (nb >= 0) {
-        if (c < nb || (c == nb && f < nface[c * MF + f])) own.push_back(code);
+        const int64_t oc = src(c), onb = src(nb);
+        if (oc < onb || (oc == onb && f < nface[c * MF + f])) own.push_back(code);
       } else if (bc[c * MF + f] == 3 || bc[c * MF + f] == 4) {
         own_mir.push_back(code);
       } else {
@@ -472,18 +595,23 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   rc = rc ? rc : upload(e, e->jinv, jinv);
   rc = rc ? rc : upload(e, e->admis, admis);
   rc = rc ? rc : upload(e, e->full, full);
+  if (perm) {
+    rc = rc ? rc : upload(e, e->d_n2o, e->n2o);
+    rc = rc ? rc : alloc(e, e->permbuf, (size_t)n * NV * 8);
+  }
   if (rc) return rc;
   // reference-frame quadrature points and basis means, in table precision
   // interleaved over 32-cell groups: element j of cell c at ((c/32)*len + j)*32 + c%32
   const int64_t ngrp = (n + 31) / 32, lq = (int64_t)MF * QS * 3;
   std::vector<double> qp((size_t)ngrp * 32 * lq, 0.0), bm((size_t)ngrp * 32 * ideg, 0.0);
   for (int64_t c = 0; c < n; ++c) {
+    const int64_t o = src(c);
     const int64_t gq = (c >> 5) * lq, gb = (c >> 5) * ideg, ln = c & 31;
     for (int f = 0; f < MF; ++f)
       for (int q = 0; q < QS; ++q)
         for (int k = 0; k < 3; ++k)
-          qp[(size_t)((gq + (f * QS + q) * 3 + k) * 32 + ln)] = g->qpoints[((c * MF + f) * UCG_MAX_QP + q) * 3 + k];
-    for (int d = 0; d < ideg; ++d) bm[(size_t)((gb + d) * 32 + ln)] = g->basis_mean[(size_t)c * ideg + d];
+          qp[(size_t)((gq + (f * QS + q) * 3 + k) * 32 + ln)] = g->qpoints[((o * MF + f) * UCG_MAX_QP + q) * 3 + k];
+    for (int d = 0; d < ideg; ++d) bm[(size_t)((gb + d) * 32 + ln)] = g->basis_mean[(size_t)o * ideg + d];
   }
   if (e->mixed) {
     std::vector<float> qf(qp.begin(), qp.end()), bf(bm.begin(), bm.end());
@@ -500,6 +628,7 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   for (int64_t c = 0; c < n; ++c)  // no neighbour past the cell's last face
     for (int f = nfaces[c]; f < MF; ++f) e->neigh_h[(size_t)c * MF + f] = -1;
   e->adj_ready = false;
+  e->adjw_ready = false;
   e->have_geometry = true;
   return UCG_OK;
 }
@@ -530,16 +659,35 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
         if (y >= n || y < -1) return fail(e, UCG_EINVAL, "stencil index out of range at cell " + std::to_string(cell));
         // rows 1..nk of the admissible stencils are read by the kernels
         const int nk = cw && ll > 0 ? c.imax2 : c.imax;
-        if (y < 0 && ll < e->admis_h[cell] && k >= 1 && k <= nk)
+        if (y < 0 && ll < e->admis_h[e->o2n.empty() ? cell : e->o2n[cell]] && k >= 1 && k <= nk)
           return fail(e, UCG_EINVAL, "unused slot (-1) inside admissible stencil " + std::to_string(ll) + " of cell " +
                                          std::to_string(cell));
       }
     if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
   }
+  // stencil indices in device numbering, and which device cell takes each
+  // row of this upload (renumbered engines only)
+  const bool perm = !e->o2n.empty();
+  std::vector<int32_t> sten_dev;
+  const int32_t* sten = r->stencil;
+  DevBuf rowbuf;
+  const int32_t* d_rowmap = nullptr;
+  if (perm) {
+    sten_dev.resize((size_t)count * A * W);
+    for (size_t j = 0; j < sten_dev.size(); ++j) sten_dev[j] = r->stencil[j] >= 0 ? e->o2n[r->stencil[j]] : -1;
+    sten = sten_dev.data();
+    std::vector<int32_t> rowmap(n, -1);
+    for (int64_t i = 0; i < count; ++i) rowmap[e->o2n[first + i]] = (int32_t)i;
+    CK(cudaMalloc(&rowbuf.p, (size_t)n * 4));
+    CK(cudaMemcpyAsync(rowbuf.p, rowmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    d_rowmap = (const int32_t*)rowbuf.p;
+  }
+  auto dcell = [&](int64_t o) -> int64_t { return perm ? e->o2n[o] : o; };
   if (c.scheme == 2 && c.iorder == 1) {  // first stencil kept on the host for the adjoint's reverse map
     e->sten1_h.resize((size_t)n * W, -1);
     for (int64_t i = 0; i < count; ++i)
-      for (int k = 0; k < W; ++k) e->sten1_h[(size_t)(first + i) * W + k] = r->stencil[(i * A) * W + k];
+      for (int k = 0; k < W; ++k) e->sten1_h[(size_t)dcell(first + i) * W + k] = sten[(i * A) * W + k];
     e->adj_ready = false;
   }
   const Layout& Ly = e->layout;
@@ -549,16 +697,23 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   rc = rc ? rc : alloc(e, e->sten, (size_t)ngrp * 32 * A * W * 4);
   rc = rc ? rc : alloc(e, e->invmat, (size_t)ngrp * 32 * Ly.tstride * T);
   if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)ngrp * 32 * Ly.istride * T);
-  if (rc) return rc;
+  if (rc) {
+    release(rowbuf);
+    return rc;
+  }
   {
     // stencils: staged per cell, interleaved on the device
     rc = alloc(e, e->staging, (size_t)count * A * W * 4);
-    if (rc) return rc;
-    CK(cudaMemcpyAsync(e->staging.p, r->stencil, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
-    int64_t total = count * A * W;
+    if (rc) {
+      release(rowbuf);
+      return rc;
+    }
+    CK(cudaMemcpyAsync(e->staging.p, sten, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
+    int64_t total = (perm ? n : count) * A * W;
     unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
     k_expand_il<int32_t, int32_t, 1><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
-                                                                nullptr, first, count, (int64_t)A * W, 0, count);
+                                                                nullptr, first, count, (int64_t)A * W, 0, count,
+                                                                d_rowmap, n);
     e->launches++;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e->stream));
@@ -624,22 +779,23 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
       rc = alloc(e, e->staging, bytes);
       if (rc) {
         if (tidbuf.p) cudaFree(tidbuf.p);
+        release(rowbuf);
         return rc;
       }
       CK(cudaMemcpyAsync(e->staging.p, host.data(), bytes, cudaMemcpyHostToDevice, e->stream));
-      int64_t total = count * pt.len;
+      int64_t total = (perm ? n : count) * pt.len;
       unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
       const double* sp = (const double*)e->staging.p;
       if (e->mixed) {
         if (pt.which == 0)
-          k_expand_il<float, double, 1><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+          k_expand_il<float, double, 1><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
         else
-          k_expand_il<float, double, 4><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+          k_expand_il<float, double, 4><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
       } else {
         if (pt.which == 0)
-          k_expand_il<double, double, 1><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+          k_expand_il<double, double, 1><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
         else
-          k_expand_il<double, double, 2><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1);
+          k_expand_il<double, double, 2><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
       }
       e->launches++;
       CK(cudaGetLastError());
@@ -647,6 +803,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     }
   }
   if (tidbuf.p) cudaFree(tidbuf.p);
+  release(rowbuf);
   e->bytes -= (int64_t)e->staging.bytes;
   release(e->staging);
   CK(cudaStreamSynchronize(e->stream));
@@ -664,7 +821,8 @@ int ucg_set_state(ucg_engine* e, const double* u, int64_t n) {
   if (!e || !u) return fail(e, UCG_EINVAL, "null argument");
   if (n != e->n) return fail(e, UCG_EINVAL, "state size mismatch");
   cudaSetDevice(e->device);
-  CK(cudaMemcpyAsync(e->Un.p, u, n * NV * 8, cudaMemcpyHostToDevice, e->stream));
+  int rc = cells_in(e, (double*)e->Un.p, u);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   e->have_state = true;
   return UCG_OK;
@@ -675,7 +833,8 @@ int ucg_get_state(ucg_engine* e, double* u, int64_t n) {
   if (n != e->n) return fail(e, UCG_EINVAL, "state size mismatch");
   if (!e->have_state) return fail(e, UCG_ESTATE, "no state set");
   cudaSetDevice(e->device);
-  CK(cudaMemcpyAsync(u, e->Un.p, n * NV * 8, cudaMemcpyDeviceToHost, e->stream));
+  int rc = cells_out(e, u, (const double*)e->Un.p);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   return UCG_OK;
 }
@@ -701,7 +860,7 @@ int ucg_residual(ucg_engine* e, double* rhs) {
   rc = launch_flux(e, p, 0, (const double*)e->Un.p, (const double*)e->Un.p, nullptr, 0.0);
   if (rc) return rc;
   if (rhs) {
-    CK(cudaMemcpyAsync(rhs, e->rhs.p, e->n * NV * 8, cudaMemcpyDeviceToHost, e->stream));
+    if ((rc = cells_out(e, rhs, (const double*)e->rhs.p))) return rc;
     CK(cudaStreamSynchronize(e->stream));
   }
   return UCG_OK;

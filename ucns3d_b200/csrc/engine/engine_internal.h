@@ -61,6 +61,10 @@ struct ucg_engine {
   std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
   std::vector<int32_t> neigh_h;     // [n][6] face neighbours (host copy, adjoint set-up)
   std::vector<int32_t> sten1_h;     // [n][IMAX+1] first stencil (host copy, MUSCL IORDER 1 only)
+  // cell renumbering (cfg.reorder): device cell c holds the caller's cell
+  // n2o[c]; o2n is the inverse.  Empty when the caller's order is kept.
+  std::vector<int32_t> n2o, o2n;
+  DevBuf d_n2o, permbuf;            // n2o on the device; [n][5] staging of permuted transfers
   // discrete adjoint / tangent (adjoint.cu)
   bool adj_ready = false;
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
@@ -89,6 +93,11 @@ int launch_recon(ucg_engine* e, const ucg::Problem& p, const double* U);
 int launch_flux(ucg_engine* e, const ucg::Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
                 double dt);
 int rk3(ucg_engine* e, double dt, bool dt_dev);
+// [n][5] FP64 arrays between the caller's cell order on the host and the
+// device order (a plain copy when the engine keeps the caller's order);
+// both leave the copy queued on the handle's stream
+int cells_in(ucg_engine* e, double* dev_dst, const double* host_src);
+int cells_out(ucg_engine* e, double* host_dst, const double* dev_src);
 // frees the adjoint buffers (adjoint.cu)
 void adjoint_release(ucg_engine* e);
 // reverse of the WENO post-processing and least squares (adjoint_weno.cu)

@@ -379,20 +379,24 @@ __global__ void k_reduce_final(const double* partial, int64_t np, double* out) {
 // [first, first+count) or whose table set is outside [tlo, thi) are left
 // untouched.
 template <typename D, typename S, int VEC>
+// With `rowmap` (renumbered cells), device cell c takes source row
+// rowmap[c] (-1: not in this upload) and every group of `n` cells is
+// visited; otherwise cells [first, first + count) take rows 0.. in order.
 __global__ void __launch_bounds__(256) k_expand_il(D* __restrict__ dst, const S* __restrict__ src,
                                                    const int32_t* __restrict__ tid, int64_t first, int64_t count,
-                                                   int64_t len, int64_t tlo, int64_t thi) {
+                                                   int64_t len, int64_t tlo, int64_t thi,
+                                                   const int32_t* __restrict__ rowmap = nullptr, int64_t n = 0) {
   __shared__ S tile[32][65];
   __shared__ int64_t trow[32];
-  const int64_t g0 = first >> 5, g1 = (first + count - 1) >> 5;
+  const int64_t g0 = rowmap ? 0 : first >> 5, g1 = rowmap ? (n - 1) >> 5 : (first + count - 1) >> 5;
   const int64_t ntile = (len + 63) / 64, nblk = (g1 - g0 + 1) * ntile;
   for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
     const int64_t g = g0 + b / ntile, j0 = (b % ntile) * 64;
     if (threadIdx.x < 32) {
       const int64_t c = g * 32 + threadIdx.x;
       int64_t t = -1;
-      if (c >= first && c < first + count) {
-        const int64_t cl = c - first;
+      const int64_t cl = rowmap ? (c < n ? rowmap[c] : -1) : (c >= first && c < first + count ? c - first : -1);
+      if (cl >= 0) {
         t = tid ? tid[cl] : cl;
         if (t < tlo || t >= thi) t = -1;
       }
@@ -412,6 +416,18 @@ __global__ void __launch_bounds__(256) k_expand_il(D* __restrict__ dst, const S*
     }
     __syncthreads();
   }
+}
+
+// [n][5] rows between orders: GATHER dst[c] = src[map[c]], else the
+// scatter dst[map[c]] = src[c] (map = the device-to-caller cell map).
+template <bool GATHER>
+__global__ void k_perm_rows(const int32_t* __restrict__ map, const double* __restrict__ src, double* __restrict__ dst,
+                            int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * NV) return;
+  const int64_t c = i / NV, v = i - c * NV, o = map[c];
+  if (GATHER) dst[i] = src[o * NV + v];
+  else dst[o * NV + v] = src[i];
 }
 
 }  // namespace ucg

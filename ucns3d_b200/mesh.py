@@ -175,3 +175,90 @@ class Mesh:
         _check(N.prep().ucp_initial_condition(self._h, kind, N.ptr(p, C.c_double), len(p),
                                               N.ptr(out, C.c_double)), "ucp_initial_condition")
         return out
+
+
+class RenumberedMesh:
+    """A prepared mesh seen through another cell numbering: caller cell i is
+    the base mesh's cell ``order[i]``.  Neighbour and stencil indices are
+    renumbered, per-cell rows moved; the shared matrix sets (``table_id``)
+    are kept.  It stands in for a mesh that arrives in partitioner or file
+    order, as UCNS3D's cells do after METIS and the grid reader
+    (src/main.f90:103-137), and offers the interface the engine, the oracle
+    and the benchmarks use."""
+
+    def __init__(self, base: Mesh, order: np.ndarray):
+        if not getattr(base, "prepared", False):
+            raise ValueError("mesh must be prepared first")
+        n = base.ncells
+        order = np.asarray(order, dtype=np.int64)
+        if order.shape != (n,) or not np.array_equal(np.sort(order), np.arange(n)):
+            raise ValueError("order must be a permutation of the cells")
+        self.base, self.order = base, order
+        self.inverse = np.empty(n, dtype=np.int64)
+        self.inverse[order] = np.arange(n)
+        self.prepared = True
+        self.sizes = base.sizes
+        self.scheme, self.iorder, self.ees = base.scheme, base.iorder, base.ees
+        remap = lambda a: np.where(a >= 0, self.inverse[np.maximum(a, 0)], -1).astype(np.int32)  # noqa: E731
+        g = base.geometry()
+        self._g = {k: (np.ascontiguousarray(v[order]) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
+        self._g["neigh"] = remap(self._g["neigh"])
+        r = base.recon()
+        self._r = dict(r)
+        self._r["stencil"] = np.ascontiguousarray(remap(r["stencil"][order]))
+        if r["table_id"] is not None:
+            self._r["table_id"] = np.ascontiguousarray(r["table_id"][order])
+        else:  # per-cell matrix sets: move them with their cells
+            for k in ("invmat", "invmat2", "indicator", "indicator2"):
+                if r.get(k) is not None:
+                    self._r[k] = np.ascontiguousarray(r[k][order])
+
+    @property
+    def ncells(self) -> int:
+        return len(self.order)
+
+    @property
+    def ntables(self) -> int:
+        return self._r["ntables"]
+
+    def fill_config(self, cfg: N.UcgConfig) -> N.UcgConfig:
+        return self.base.fill_config(cfg)
+
+    def geometry_struct(self) -> N.UcgGeometry:
+        g, s = self._g, N.UcgGeometry()
+        s.ncells = self.ncells
+        for k in ("nfaces", "face_type", "neigh", "neigh_face", "bc", "qperm", "admis", "full"):
+            setattr(s, k, N.ptr(g[k], C.c_int32))
+        for k in ("face_angle", "face_area", "dih", "qpoints", "volume", "minedge", "invccjac", "basis_mean"):
+            setattr(s, k, N.ptr(g[k], C.c_double))
+        return s
+
+    def recon_struct(self) -> N.UcgRecon:
+        r, s = self._r, N.UcgRecon()
+        s.first, s.count = 0, self.ncells
+        s.stencil = N.ptr(r["stencil"], C.c_int32)
+        s.ntables = r["ntables"]
+        if r["table_id"] is not None:
+            s.table_id = N.ptr(r["table_id"], C.c_int32)
+        for k in ("invmat", "invmat2", "indicator", "indicator2"):
+            if r.get(k) is not None:
+                setattr(s, k, N.ptr(r[k], C.c_double))
+        return s
+
+    def geometry(self) -> dict:
+        return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self._g.items()}
+
+    def recon(self) -> dict:
+        return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self._r.items()}
+
+    def centres(self) -> np.ndarray:
+        return self.base.centres()[self.order]
+
+    def initial_condition(self, kind: int, params) -> np.ndarray:
+        return self.base.initial_condition(kind, params)[self.order]
+
+    def to_base(self, a: np.ndarray) -> np.ndarray:
+        """Per-cell rows of this numbering in the base mesh's numbering."""
+        out = np.empty_like(a)
+        out[self.order] = a
+        return out
