@@ -281,8 +281,11 @@ def run_gpu(args, case, ws, local, timed_e2e=True):
         t1 = time.perf_counter()
         e2e = dict(seconds=t1 - t0, bytes_in=nin.nbytes, bytes_out=nout.nbytes)
     nbytes_dev = eng.device_bytes
+    co = eng.cell_order()
+    order = {"renumbered": co["renumbered"], "gather_cost_caller": co["cost_caller"], "gather_cost_rcm": co["cost_rcm"]}
     eng.close()
-    return dict(ms=ms, kern=kern, state=state, clocks=clocks, launches=launches, e2e=e2e, device_bytes=nbytes_dev)
+    return dict(ms=ms, kern=kern, state=state, clocks=clocks, launches=launches, e2e=e2e, device_bytes=nbytes_dev,
+                order=order)
 
 
 def run_accuracy(case, local, steps):
@@ -548,6 +551,7 @@ def main():
         "gpu_launches": r32["launches"],
         "clocks": r32["clocks"],
         "device_bytes": r32["device_bytes"],
+        "cell_order": r32["order"],
     }
     if shuffle is not None:
         shuffle["reorder_on"]["ms_per_step"] = ms / args.steps

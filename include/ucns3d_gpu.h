@@ -105,7 +105,9 @@ typedef struct ucg_config {
                           cells internally by reverse Cuthill-McKee on the face-
                           neighbour graph at ucg_upload_geometry, so that the stencil
                           and face gathers of a mesh in partitioner or file order
-                          touch nearby memory.  Every [n][5] array of the ABI stays
+                          touch nearby memory; kept only where it gathers from
+                          fewer cache lines (ucg_cell_order).  Every [n][5] array
+                          of the ABI stays
                           in the caller's order (permuted on the device), and each
                           face flux is still evaluated by the face side of the lower
                           caller index, so the results are bitwise those of
@@ -212,6 +214,16 @@ int ucg_synchronize(ucg_engine* e);
  * alone (part of ms[0]; all of it for MUSCL IORDER 1).  For profiling; it
  * leaves the state unchanged.                                              */
 int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms);
+
+/* The cell numbering chosen at ucg_upload_geometry.  With cfg.reorder 1 the
+ * engine computes reverse Cuthill-McKee and keeps it only if the face
+ * neighbours of each 32-cell warp then span fewer 128-byte lines of the
+ * state (by 5 %) than in the caller's order; *renumbered = 1 if it did.
+ * n2o (optional, [n]) receives the caller's cell at each device position,
+ * cost (optional, [2]) the mean lines per warp and face slot of the caller's
+ * order and of reverse Cuthill-McKee (0 when reorder is 0).  No counterpart
+ * in the reference, which takes the order of its grid reader and METIS. */
+int ucg_cell_order(const ucg_engine* e, int32_t* renumbered, int32_t* n2o, double* cost);
 
 /* The cudaStream_t of the handle, as an opaque pointer. */
 void* ucg_get_stream(ucg_engine* e);

@@ -69,23 +69,51 @@ def _run(m, cfg, U, steps):
     return out
 
 
+def _shuffled(name, reorder, **kw):
+    m, cfg, U = _setup(name, reorder, **kw)
+    order = np.random.default_rng(11).permutation(m.ncells)
+    return m, RenumberedMesh(m, order), cfg, U, order
+
+
+def _order(m, cfg):
+    e = Engine(m, cfg)
+    out = e.cell_order()
+    e.close()
+    return out
+
+
 @pytest.mark.parametrize("name", list(MESHES))
 def test_reorder_is_bitwise_transparent(name):
-    m, cfg0, U = _setup(name, 0)
+    """On a shuffled numbering the engine renumbers (reverse Cuthill-McKee
+    gathers from fewer cache lines); results equal reorder 0 bit for bit."""
+    m, ms, cfg0, U, order = _shuffled(name, 0)
     cfg1 = N.UcgConfig.from_buffer_copy(cfg0)
     cfg1.reorder = 1
-    R0, S0 = _run(m, cfg0, U, 3)
-    R1, S1 = _run(m, cfg1, U, 3)
+    o = _order(ms, cfg1)
+    print(f"{name}: gather cost shuffled {o['cost_caller']:.2f}, reverse Cuthill-McKee {o['cost_rcm']:.2f}")
+    assert o["renumbered"]
+    assert sorted(o["n2o"].tolist()) == list(range(m.ncells))
+    R0, S0 = _run(ms, cfg0, U[order], 3)
+    R1, S1 = _run(ms, cfg1, U[order], 3)
     assert np.array_equal(R0, R1)
     assert np.array_equal(S0, S1)
 
 
+def test_structured_order_is_kept():
+    """A box numbered row by row already gathers from fewer lines than
+    reverse Cuthill-McKee would: the engine keeps it."""
+    m, cfg, U = _setup("weno5_hex", 1)
+    o = _order(m, cfg)
+    assert not o["renumbered"] and o["cost_caller"] < o["cost_rcm"]
+    assert np.array_equal(o["n2o"], np.arange(m.ncells))
+
+
 @pytest.mark.parametrize("precision", [N.UCG_FP64, N.UCG_MIXED])
 def test_reorder_characteristic_weno_bitwise(precision):
-    m, cfg0, U = _setup("weno3_tet", 0, precision=precision, wenwrt=2)
+    m, ms, cfg0, U, order = _shuffled("weno3_tet", 0, precision=precision, wenwrt=2)
     cfg1 = N.UcgConfig.from_buffer_copy(cfg0)
     cfg1.reorder = 1
-    assert np.array_equal(_run(m, cfg0, U, 1)[1], _run(m, cfg1, U, 1)[1])
+    assert np.array_equal(_run(ms, cfg0, U[order], 1)[1], _run(ms, cfg1, U[order], 1)[1])
 
 
 @pytest.mark.parametrize("name", ["weno3_tet", "cweno4_ns_mixed", "muscl_bump"])
@@ -108,12 +136,15 @@ def test_shuffled_numbering_gives_the_same_residual(name):
 
 
 def test_reorder_adjoint_matches_caller_order():
-    """VJP and JVP of the MUSCL bump channel with the engine renumbered
-    internally, against the same with the caller's order kept (1e-13: the
-    reverse map sums a cell's contributions in device order)."""
-    m, cfg1, U = _setup("muscl_bump", 1)
+    """VJP and JVP of the MUSCL bump channel (shuffled numbering) with the
+    engine renumbered internally, against the same with the caller's order
+    kept (1e-13: the reverse map sums a cell's contributions in device
+    order)."""
+    _, m, cfg1, U, order = _shuffled("muscl_bump", 1)
+    U = U[order]
     cfg0 = N.UcgConfig.from_buffer_copy(cfg1)
     cfg0.reorder = 0
+    assert _order(m, cfg1)["renumbered"]
     rng = np.random.default_rng(3)
     lam, du = rng.standard_normal(U.shape), 1e-2 * rng.standard_normal(U.shape)
     out = []

@@ -294,6 +294,35 @@ void rcm_order(int64_t n, const int32_t* nfaces, const int32_t* neigh, std::vect
   n2o.assign(order.rbegin(), order.rend());
 }
 
+// Gather cost of a cell order: over every group of 32 consecutive device
+// cells (one warp of the lane-per-cell kernels) and face slot, the number of
+// distinct 128-byte lines of the [n][5] FP64 state that the face neighbours
+// of the group occupy, averaged.  n2o empty = the caller's order.
+double gather_cost(int64_t n, const int32_t* nfaces, const int32_t* neigh, const std::vector<int32_t>& n2o) {
+  std::vector<int32_t> o2n;
+  if (!n2o.empty()) {
+    o2n.assign(n, 0);
+    for (int64_t c = 0; c < n; ++c) o2n[n2o[c]] = (int32_t)c;
+  }
+  double lines = 0.0;
+  int64_t slots = 0;
+  int64_t ids[32];
+  for (int64_t g = 0; g < n; g += 32)
+    for (int f = 0; f < MF; ++f) {
+      int k = 0;
+      for (int64_t c = g; c < g + 32 && c < n; ++c) {
+        const int64_t o = n2o.empty() ? c : n2o[c];
+        const int64_t y = f < nfaces[o] ? neigh[o * MF + f] : -1;
+        if (y >= 0) ids[k++] = (n2o.empty() ? y : o2n[y]) * (NV * 8) / 128;
+      }
+      if (!k) continue;
+      std::sort(ids, ids + k);
+      lines += (double)(std::unique(ids, ids + k) - ids);
+      ++slots;
+    }
+  return slots ? lines / (double)slots : 0.0;
+}
+
 int cells_in(ucg_engine* e, double* dev_dst, const double* host_src) {
   const size_t bytes = (size_t)e->n * NV * 8;
   if (e->n2o.empty()) {
@@ -515,9 +544,18 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   e->n2o.clear();
   e->o2n.clear();
   if (e->cfg.reorder == 1) {
-    rcm_order(n, g->nfaces, g->neigh, e->n2o);
-    e->o2n.assign(n, -1);
-    for (int64_t c = 0; c < n; ++c) e->o2n[e->n2o[c]] = (int32_t)c;
+    // reverse Cuthill-McKee, kept only where it gathers from fewer cache
+    // lines than the caller's order (a structured or already local order,
+    // such as a box numbered row by row, is better left as it is)
+    std::vector<int32_t> rcm, none;
+    rcm_order(n, g->nfaces, g->neigh, rcm);
+    e->cost_caller = gather_cost(n, g->nfaces, g->neigh, none);
+    e->cost_rcm = gather_cost(n, g->nfaces, g->neigh, rcm);
+    if (e->cost_rcm < 0.95 * e->cost_caller) {
+      e->n2o = std::move(rcm);
+      e->o2n.assign(n, -1);
+      for (int64_t c = 0; c < n; ++c) e->o2n[e->n2o[c]] = (int32_t)c;
+    }
   }
   const bool perm = !e->n2o.empty();
   auto src = [&](int64_t c) -> int64_t { return perm ? e->n2o[c] : c; };
@@ -968,6 +1006,19 @@ int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
   if (rc) return rc;
   for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
   CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int ucg_cell_order(const ucg_engine* e, int32_t* renumbered, int32_t* n2o, double* cost) {
+  if (!e) return UCG_EINVAL;
+  if (!e->have_geometry) return UCG_ESTATE;
+  if (renumbered) *renumbered = e->n2o.empty() ? 0 : 1;
+  if (n2o)
+    for (int64_t c = 0; c < e->n; ++c) n2o[c] = e->n2o.empty() ? (int32_t)c : e->n2o[c];
+  if (cost) {
+    cost[0] = e->cost_caller;
+    cost[1] = e->cost_rcm;
+  }
   return UCG_OK;
 }
 

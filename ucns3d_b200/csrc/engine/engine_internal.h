@@ -65,6 +65,7 @@ struct ucg_engine {
   // n2o[c]; o2n is the inverse.  Empty when the caller's order is kept.
   std::vector<int32_t> n2o, o2n;
   DevBuf d_n2o, permbuf;            // n2o on the device; [n][5] staging of permuted transfers
+  double cost_caller = 0.0, cost_rcm = 0.0;  // gather cost of both orders (reorder 1)
   // discrete adjoint / tangent (adjoint.cu)
   bool adj_ready = false;
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,

@@ -184,6 +184,17 @@ class Engine:
     def synchronize(self):
         self._check(self.lib.ucg_synchronize(self._h))
 
+    def cell_order(self) -> dict:
+        """The device numbering chosen at upload: whether the engine
+        renumbered the cells, the caller's cell at each device position, and
+        the gather costs (cache lines per warp and face slot) of the caller's
+        order and of reverse Cuthill-McKee."""
+        ren = C.c_int32()
+        n2o = np.empty(self.n, dtype=np.int32)
+        cost = np.zeros(2)
+        self._check(self.lib.ucg_cell_order(self._h, C.byref(ren), N.ptr(n2o, C.c_int32), N.ptr(cost, C.c_double)))
+        return dict(renumbered=bool(ren.value), n2o=n2o, cost_caller=float(cost[0]), cost_rcm=float(cost[1]))
+
     @property
     def stream_ptr(self) -> int:
         return int(self.lib.ucg_get_stream(self._h) or 0)
