@@ -66,7 +66,8 @@ struct Problem {
   void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the stencils
   double* qbuf;             // characteristic WENO: G_l^T S G_l per stencil, 15 values, interleaved
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
-  double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w
+  double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w (MUSCL IORDER 1)
+  double* fgrad;            // [nown][QS][4][3] face-point average of both sides' gradients of T,u,v,w (WENO)
   double* gv;               // [n][ideg][4]  viscous LSQ coefficients
   double* prim;             // [n][4] T, u, v, w of each cell (viscous LSQ, formed once per stage)
   double* upad;             // [n][6] conserved state in 48-byte records (k_lsq gathers, formed once per stage)

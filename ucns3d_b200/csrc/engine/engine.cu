@@ -128,6 +128,7 @@ Problem make_problem(ucg_engine* e) {
   p.qbuf = (double*)e->qbuf.p;
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
+  p.fgrad = (double*)e->fgrad.p;
   p.gv = (double*)e->gv.p;
   p.prim = (double*)e->prim.p;
   p.upad = (double*)e->upad.p;
@@ -463,9 +464,12 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (c.wenwrt == 2)  // characteristic WENO: G^T S G of every stencil (15 values)
     rc = rc ? rc : alloc(e, e->qbuf, (size_t)ngrp * 32 * c.admis_max * 15 * 8);
   if (c.governing == 1) {
-    rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
-    rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
-    rc = rc ? rc : alloc(e, e->prim, (size_t)n * 4 * 8);
+    if (c.scheme == 2 && c.iorder == 1) {
+      rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
+    } else {
+      rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
+      rc = rc ? rc : alloc(e, e->prim, (size_t)n * 4 * 8);
+    }
   }
   rc = rc ? rc : alloc(e, e->health, 64);
   rc = rc ? rc : alloc(e, e->dt, 64);
@@ -492,7 +496,7 @@ void ucg_destroy(ucg_engine* e) {
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
-                   &e->qbuf, &e->d_n2o, &e->permbuf};
+                   &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -619,6 +623,8 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   int rc = UCG_OK;
   rc = rc ? rc : upload(e, e->own, own);
   e->nown = (int64_t)own.size();
+  if (ns && !(e->cfg.scheme == 2 && e->cfg.iorder == 1))  // face-point gradients, one record per owned face point
+    rc = rc ? rc : alloc(e, e->fgrad, (size_t)e->nown * QS * 12 * 8);
   rc = rc ? rc : upload(e, e->nfaces, nfaces);
   rc = rc ? rc : upload(e, e->ftype, ftype);
   rc = rc ? rc : upload(e, e->neigh, neigh);

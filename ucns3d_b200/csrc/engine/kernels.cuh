@@ -205,9 +205,13 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
     if (NS && nb >= 0) {
-      // both sides' face-point gradients as six 16-byte loads each
-      const double2* gl2 = (const double2*)(p.ulv + ((c * MF + f) * QS + q) * 12);
-      const double2* gr2 = (const double2*)(p.ulv + ((nb * MF + nf) * QS + qq) * 12);
+      // both sides' face-point gradients as six 16-byte loads each; the WENO
+      // path stores their average once per face point (both pointers at it:
+      // (g + g) / 2 is g exactly)
+      const double2* gl2 = (const double2*)(p.fgrad ? p.fgrad + (i * QS + q) * 12
+                                                    : p.ulv + ((c * MF + f) * QS + q) * 12);
+      const double2* gr2 = (const double2*)(p.fgrad ? p.fgrad + (i * QS + q) * 12
+                                                    : p.ulv + ((nb * MF + nf) * QS + qq) * 12);
       double gl[12], gr[12];
 #pragma unroll
       for (int k = 0; k < 6; ++k) {

@@ -37,7 +37,14 @@ __global__ void k_pad_state(Problem p, const double* __restrict__ U) {
 
 // PAD: stencil members gathered from p.upad (the engine's stage), else from U
 // (also used on tangent states by the discrete adjoint).
-template <int P, typename T, bool PAD = false>
+// VIS (mixed form, Navier-Stokes, IORDER 2-3): the viscous least squares of
+// COMPUTE_GRADIENTS_INNER_MEAN_LSQ_VISCOUS (gradients.f90:502-706) in the
+// same pass over the central stencil: each member's (T, u, v, w) record
+// (p.prim) is gathered beside its state and its differences multiply the
+// same pseudo-inverse rows, accumulated in FP32 like the conserved
+// differences; the coefficients go to p.gv in FP64.  The central rows are
+// then read once per stage instead of twice.
+template <int P, typename T, bool PAD = false, bool VIS = false>
 __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int DH = LsqRows<P, T>::value;
@@ -51,6 +58,15 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
   double u0[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u0[v] = live ? U[c * NV + v] : 0.0;
+  double s0[4] = {0.0, 0.0, 0.0, 0.0};
+  if (VIS && live) {
+    const double2* q = (const double2*)(p.prim + c * 4);
+    const double2 a = q[0], b = q[1];
+    s0[0] = a.x;
+    s0[1] = a.y;
+    s0[2] = b.x;
+    s0[3] = b.y;
+  }
   const T* Mi = (const T*)p.invmat + grp * p.tstride * 32 + lane;
   const int32_t* Si = p.sten + grp * (int64_t)(A * W) * 32 + lane;
   T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
@@ -59,16 +75,32 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
     const int nk = low ? p.imax2 : p.imax, nd = low ? p.ideg2 : ID;
     const bool act = ll < adm;
     for (int d0 = 0; d0 < nd; d0 += DH) {
+      static_assert(!VIS || DH == Deg<P>::ideg, "the fused viscous least squares needs all rows in one pass");
       T acc[DH][NV];
+      T vac[VIS ? DH : 1][4];
+      const bool vis = VIS && ll == 0;
 #pragma unroll
       for (int j = 0; j < DH; ++j)
 #pragma unroll
         for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
+#pragma unroll
+      for (int j = 0; j < (VIS ? DH : 1); ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) vac[j][v] = T(0);
       if (act) {
         const T* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
         const int32_t* S = Si + (ll * W + 1) * 32;
 #pragma unroll 2
         for (int k = 0; k < nk; ++k) {
+          T ds[4];
+          if (VIS && vis) {
+            const double2* q = (const double2*)(p.prim + (int64_t)S[k * 32] * 4);
+            const double2 a = q[0], b = q[1];
+            ds[0] = T(a.x - s0[0]);
+            ds[1] = T(a.y - s0[1]);
+            ds[2] = T(b.x - s0[2]);
+            ds[3] = T(b.y - s0[3]);
+          }
           T du[NV];
           if (PAD) {
             const double2* q = (const double2*)(p.upad + (int64_t)S[k * 32] * 6);
@@ -88,6 +120,9 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
               T m = Mk[j * 32];
 #pragma unroll
               for (int v = 0; v < NV; ++v) acc[j][v] += m * du[v];
+              if (VIS && vis)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) vac[j][v] += m * ds[v];
             }
         }
       }
@@ -97,6 +132,13 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
           if (d0 + j < nd)
 #pragma unroll
             for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] = acc[j][v];
+      if (VIS && vis && live)
+#pragma unroll
+        for (int j = 0; j < DH; ++j) {
+          double2* o = (double2*)(p.gv + (c * ID + j) * 4);
+          o[0] = make_double2((double)vac[j][0], (double)vac[j][1]);
+          o[1] = make_double2((double)vac[j][2], (double)vac[j][3]);
+        }
     }
   }
 }
@@ -925,20 +967,19 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
   }
 }
 
+// Face-point gradients of T, u, v, w for the viscous flux, one thread per
+// (owned interior face, point): SOLUTIONTRIAV2 (reconstruct_p.f90:2358) on
+// both sides of the face at the paired points, and their average, the only
+// form CALCULATE_FLUXESHI_DIFFUSIVE uses (flux_p.f90:1614-1779), written
+// once per face point to p.fgrad [nown][QS][12] (half the bytes of one
+// record per cell face and point, read back once instead of twice).
 template <int P, typename T>
-__global__ void k_visc_face(Problem p) {
+__device__ __forceinline__ void visc_point_grad(const Problem& p, int64_t c, int f, int q, int QS, double* out) {
   constexpr int ID = Deg<P>::ideg;
-  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.n * MF * QS) return;
-  const int64_t c = i / (MF * QS);
-  const int r = (int)(i - c * MF * QS), f = r / QS, q = r - f * QS;
-  if (f >= p.nfaces[c] || q >= face_nq(p, p.ftype[c * MF + f])) return;
   const T* xi = (const T*)p.qpts + ((c >> 5) * MF * QS * 3 + (f * QS + q) * 3) * 32 + (c & 31);
   double dx[ID], dy[ID], dz[ID];
   dmonomials<P>((double)xi[0], (double)xi[32], (double)xi[64], dx, dy, dz);
   const double* J = p.jinv + c * 9;
-  double out[12];
 #pragma unroll
   for (int var = 0; var < 4; ++var) {
     double gl[3] = {0.0, 0.0, 0.0};
@@ -952,11 +993,29 @@ __global__ void k_visc_face(Problem p) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) out[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
   }
-  // the point's 96 bytes as six 16-byte stores (half as many store
-  // instructions, each touching one sector per lane)
-  double2* o = (double2*)(p.ulv + ((c * MF + f) * QS + q) * 12);
+}
+
+template <int P, typename T>
+__global__ void k_visc_facegrad(Problem p) {
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = t / QS;
+  const int q = (int)(t - i * QS);
+  if (i >= p.nown) return;
+  const int32_t code = p.own[i];
+  const int64_t c = code >> 3;
+  const int f = code & 7;
+  const int64_t nb = p.neigh[c * MF + f];
+  if (nb < 0 || q >= face_nq(p, p.ftype[c * MF + f])) return;
+  const int nf = p.nface[c * MF + f];
+  const int qq = p.qperm[(c * MF + f) * QS + q];
+  double gl[12], gr[12];
+  visc_point_grad<P, T>(p, c, f, q, QS, gl);
+  visc_point_grad<P, T>(p, nb, nf, qq, QS, gr);
+  double2* o = (double2*)(p.fgrad + (i * QS + q) * 12);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) o[k] = make_double2(out[2 * k], out[2 * k + 1]);
+  for (int k = 0; k < 6; ++k)
+    o[k] = make_double2((gl[2 * k] + gr[2 * k]) / 2.0, (gl[2 * k + 1] + gr[2 * k + 1]) / 2.0);
 }
 
 // Characteristic-variable post-processing (k_wpost<P, T, true>), 64 threads
@@ -987,6 +1046,10 @@ template <int P, typename T>
 cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st, int64_t* launches,
                           cudaEvent_t mark) {
   const unsigned b = (unsigned)((p.n + 127) / 128);
+  // the viscous least squares rides on the central-stencil pass of k_lsq
+  // where all its rows fit in one register pass (FP32, IORDER 2-3)
+  constexpr bool can_fuse = sizeof(T) == 4 && (P == 2 || P == 3);
+  const bool fuse_vis = can_fuse && ns && !p.lsq_bulk;
   if (p.lsq_bulk) {  // opt-in: tables staged through shared memory (UCG_LSQ_BULK=1)
     constexpr int NSTG = 4;
     constexpr size_t smem = lsq_tma_smem<P, T, NSTG>();
@@ -998,10 +1061,30 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     // registers: it breaks the load schedule) and made IORDER 2 slower by a
     // third, so those keep five 8-byte loads
     k_pad_state<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
-    k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
     ++*launches;
+    if constexpr (can_fuse) {
+      if (fuse_vis) {
+        k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+        k_lsq<P, T, (P == 3), true><<<b, 128, 0, st>>>(p, U);
+        ++*launches;
+      } else {
+        k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
+      }
+    } else {
+      k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
+    }
   } else {
-    k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
+    if constexpr (can_fuse) {
+      if (fuse_vis) {
+        k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+        k_lsq<P, T, false, true><<<b, 128, 0, st>>>(p, U);
+        ++*launches;
+      } else {
+        k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
+      }
+    } else {
+      k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
+    }
   }
   if (mark) cudaEventRecord(mark, st);
   if (p.wenwrt == 2) {
@@ -1012,11 +1095,14 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   }
   *launches += 2;
   if (ns) {
-    k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
-    k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
-    const int64_t nf = p.n * MF * QS;
-    k_visc_face<P, T><<<(unsigned)((nf + 127) / 128), 128, 0, st>>>(p);
-    *launches += 3;
+    if (!fuse_vis) {
+      k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+      k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
+      *launches += 2;
+    }
+    const int64_t nfp = p.nown * QS;
+    k_visc_facegrad<P, T><<<(unsigned)((nfp + 127) / 128), 128, 0, st>>>(p);
+    *launches += 1;
   }
   return cudaGetLastError();
 }
