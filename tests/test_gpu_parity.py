@@ -343,24 +343,3 @@ def test_call_order_is_checked():
     e.set_state(U)
     e.runge_kutta3(1e-3)
     e.check_health()
-
-
-@pytest.mark.parametrize("name", ["cweno4_ns_mixed", "weno3_ns_hex"])
-def test_fused_viscous_least_squares_matches_separate(name, monkeypatch):
-    """Mixed form, Navier-Stokes: the viscous least squares inside k_lsq
-    (default) against the separate k_visc_lsq (UCG_VISC_FUSE=0 at engine
-    creation).  Both accumulate the same products, in FP32 and FP64
-    respectively, so they agree to FP32 rounding of the viscous
-    coefficients: 1e-6 of the per-cell flux scale."""
-    m, cfg, U = _setup(name, precision=N.UCG_MIXED)
-    out = []
-    for fuse in ("1", "0"):
-        monkeypatch.setenv("UCG_VISC_FUSE", fuse)
-        e = Engine(m, cfg)
-        e.set_state(U)
-        out.append(e.residual())
-        e.check_health()
-        e.close()
-    err = (np.abs(out[0] - out[1]) / _flux_scale(None, m, U)).max()
-    print(f"{name}: fused vs separate viscous least squares {err:.3e}")
-    assert err < 1e-6

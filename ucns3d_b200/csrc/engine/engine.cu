@@ -140,7 +140,6 @@ Problem make_problem(ucg_engine* e) {
   p.health = (unsigned*)e->health.p;
   p.dt_dev = nullptr;
   p.lsq_bulk = e->lsq_bulk ? 1 : 0;
-  p.visc_fuse = e->visc_fuse ? 1 : 0;
   p.wenwrt = c.wenwrt;
   p.riemann = c.riemann;
   p.limiter = c.limiter;
@@ -416,8 +415,6 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   {
     const char* bulk = std::getenv("UCG_LSQ_BULK");
     e->lsq_bulk = bulk && bulk[0] == '1';
-    const char* fuse = std::getenv("UCG_VISC_FUSE");
-    e->visc_fuse = !(fuse && fuse[0] == '0');
   }
   {
     // slices and smoothness blocks padded to 16 bytes (bulk-copy granularity)

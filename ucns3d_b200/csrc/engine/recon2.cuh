@@ -47,10 +47,7 @@ __global__ void k_pad_state(Problem p, const double* __restrict__ U) {
 template <int P, typename T, bool PAD = false, bool VIS = false>
 __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
-  // the fused viscous form holds 4 more accumulators per row: half the rows
-  // per pass keeps it near the plain kernel's registers (two passes over the
-  // central stencil's members; every table row is still read once)
-  constexpr int DH = VIS ? (LsqRows<P, T>::value + 1) / 2 : LsqRows<P, T>::value;
+  constexpr int DH = LsqRows<P, T>::value;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int A = p.admis_max, W = p.imax + 1;
   const bool cw = p.ees == 5;
@@ -78,6 +75,7 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
     const int nk = low ? p.imax2 : p.imax, nd = low ? p.ideg2 : ID;
     const bool act = ll < adm;
     for (int d0 = 0; d0 < nd; d0 += DH) {
+      static_assert(!VIS || DH == Deg<P>::ideg, "the fused viscous least squares needs all rows in one pass");
       T acc[DH][NV];
       T vac[VIS ? DH : 1][4];
       const bool vis = VIS && ll == 0;
@@ -136,12 +134,11 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
             for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] = acc[j][v];
       if (VIS && vis && live)
 #pragma unroll
-        for (int j = 0; j < DH; ++j)
-          if (d0 + j < nd) {
-            double2* o = (double2*)(p.gv + (c * ID + d0 + j) * 4);
-            o[0] = make_double2((double)vac[j][0], (double)vac[j][1]);
-            o[1] = make_double2((double)vac[j][2], (double)vac[j][3]);
-          }
+        for (int j = 0; j < DH; ++j) {
+          double2* o = (double2*)(p.gv + (c * ID + j) * 4);
+          o[0] = make_double2((double)vac[j][0], (double)vac[j][1]);
+          o[1] = make_double2((double)vac[j][2], (double)vac[j][3]);
+        }
     }
   }
 }
@@ -1052,7 +1049,7 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   // the viscous least squares rides on the central-stencil pass of k_lsq
   // where all its rows fit in one register pass (FP32, IORDER 2-3)
   constexpr bool can_fuse = sizeof(T) == 4 && (P == 2 || P == 3);
-  const bool fuse_vis = can_fuse && ns && !p.lsq_bulk && p.visc_fuse;
+  const bool fuse_vis = can_fuse && ns && !p.lsq_bulk;
   if (p.lsq_bulk) {  // opt-in: tables staged through shared memory (UCG_LSQ_BULK=1)
     constexpr int NSTG = 4;
     constexpr size_t smem = lsq_tma_smem<P, T, NSTG>();
