@@ -37,14 +37,7 @@ __global__ void k_pad_state(Problem p, const double* __restrict__ U) {
 
 // PAD: stencil members gathered from p.upad (the engine's stage), else from U
 // (also used on tangent states by the discrete adjoint).
-// VIS (mixed form, Navier-Stokes, IORDER 2-3): the viscous least squares of
-// COMPUTE_GRADIENTS_INNER_MEAN_LSQ_VISCOUS (gradients.f90:502-706) in the
-// same pass over the central stencil: each member's (T, u, v, w) record
-// (p.prim) is gathered beside its state and its differences multiply the
-// same pseudo-inverse rows, accumulated in FP32 like the conserved
-// differences; the coefficients go to p.gv in FP64.  The central rows are
-// then read once per stage instead of twice.
-template <int P, typename T, bool PAD = false, bool VIS = false>
+template <int P, typename T, bool PAD = false>
 __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int DH = LsqRows<P, T>::value;
@@ -58,15 +51,6 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
   double u0[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u0[v] = live ? U[c * NV + v] : 0.0;
-  double s0[4] = {0.0, 0.0, 0.0, 0.0};
-  if (VIS && live) {
-    const double2* q = (const double2*)(p.prim + c * 4);
-    const double2 a = q[0], b = q[1];
-    s0[0] = a.x;
-    s0[1] = a.y;
-    s0[2] = b.x;
-    s0[3] = b.y;
-  }
   const T* Mi = (const T*)p.invmat + grp * p.tstride * 32 + lane;
   const int32_t* Si = p.sten + grp * (int64_t)(A * W) * 32 + lane;
   T* Gi = (T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
@@ -75,32 +59,16 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
     const int nk = low ? p.imax2 : p.imax, nd = low ? p.ideg2 : ID;
     const bool act = ll < adm;
     for (int d0 = 0; d0 < nd; d0 += DH) {
-      static_assert(!VIS || DH == Deg<P>::ideg, "the fused viscous least squares needs all rows in one pass");
       T acc[DH][NV];
-      T vac[VIS ? DH : 1][4];
-      const bool vis = VIS && ll == 0;
 #pragma unroll
       for (int j = 0; j < DH; ++j)
 #pragma unroll
         for (int v = 0; v < NV; ++v) acc[j][v] = T(0);
-#pragma unroll
-      for (int j = 0; j < (VIS ? DH : 1); ++j)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) vac[j][v] = T(0);
       if (act) {
         const T* M = Mi + (int64_t)(p.soff[ll] + d0) * 32;
         const int32_t* S = Si + (ll * W + 1) * 32;
 #pragma unroll 2
         for (int k = 0; k < nk; ++k) {
-          T ds[4];
-          if (VIS && vis) {
-            const double2* q = (const double2*)(p.prim + (int64_t)S[k * 32] * 4);
-            const double2 a = q[0], b = q[1];
-            ds[0] = T(a.x - s0[0]);
-            ds[1] = T(a.y - s0[1]);
-            ds[2] = T(b.x - s0[2]);
-            ds[3] = T(b.y - s0[3]);
-          }
           T du[NV];
           if (PAD) {
             const double2* q = (const double2*)(p.upad + (int64_t)S[k * 32] * 6);
@@ -120,9 +88,6 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
               T m = Mk[j * 32];
 #pragma unroll
               for (int v = 0; v < NV; ++v) acc[j][v] += m * du[v];
-              if (VIS && vis)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) vac[j][v] += m * ds[v];
             }
         }
       }
@@ -132,13 +97,6 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
           if (d0 + j < nd)
 #pragma unroll
             for (int v = 0; v < NV; ++v) Gi[(int64_t)((ll * ID + d0 + j) * NV + v) * 32] = acc[j][v];
-      if (VIS && vis && live)
-#pragma unroll
-        for (int j = 0; j < DH; ++j) {
-          double2* o = (double2*)(p.gv + (c * ID + j) * 4);
-          o[0] = make_double2((double)vac[j][0], (double)vac[j][1]);
-          o[1] = make_double2((double)vac[j][2], (double)vac[j][3]);
-        }
     }
   }
 }
@@ -1046,10 +1004,6 @@ template <int P, typename T>
 cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st, int64_t* launches,
                           cudaEvent_t mark) {
   const unsigned b = (unsigned)((p.n + 127) / 128);
-  // the viscous least squares rides on the central-stencil pass of k_lsq
-  // where all its rows fit in one register pass (FP32, IORDER 2-3)
-  constexpr bool can_fuse = sizeof(T) == 4 && (P == 2 || P == 3);
-  const bool fuse_vis = can_fuse && ns && !p.lsq_bulk;
   if (p.lsq_bulk) {  // opt-in: tables staged through shared memory (UCG_LSQ_BULK=1)
     constexpr int NSTG = 4;
     constexpr size_t smem = lsq_tma_smem<P, T, NSTG>();
@@ -1061,30 +1015,10 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     // registers: it breaks the load schedule) and made IORDER 2 slower by a
     // third, so those keep five 8-byte loads
     k_pad_state<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+    k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
     ++*launches;
-    if constexpr (can_fuse) {
-      if (fuse_vis) {
-        k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
-        k_lsq<P, T, (P == 3), true><<<b, 128, 0, st>>>(p, U);
-        ++*launches;
-      } else {
-        k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
-      }
-    } else {
-      k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
-    }
   } else {
-    if constexpr (can_fuse) {
-      if (fuse_vis) {
-        k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
-        k_lsq<P, T, false, true><<<b, 128, 0, st>>>(p, U);
-        ++*launches;
-      } else {
-        k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
-      }
-    } else {
-      k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
-    }
+    k_lsq<P, T><<<b, 128, 0, st>>>(p, U);
   }
   if (mark) cudaEventRecord(mark, st);
   if (p.wenwrt == 2) {
@@ -1095,11 +1029,9 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   }
   *launches += 2;
   if (ns) {
-    if (!fuse_vis) {
-      k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
-      k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
-      *launches += 2;
-    }
+    k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+    k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
+    *launches += 2;
     const int64_t nfp = p.nown * QS;
     k_visc_facegrad<P, T><<<(unsigned)((nfp + 127) / 128), 128, 0, st>>>(p);
     *launches += 1;
