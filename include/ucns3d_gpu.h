@@ -302,6 +302,19 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
                     double* dJdp);
 int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
                     double* dJ);
+/* The same runs with the scalar output chosen: UCG_OBJ_FORCE_X the wall
+ * force above (MUSCL), UCG_OBJ_KE the domain kinetic energy
+ * J = sum_c V_c |rho u|^2 / (2 rho) (the TGV sum of time_p.f90:4145-4198
+ * without its normalisation), which also covers the conserved-variable WENO
+ * and CWENO residuals: the reverse sweeps then run the WENO VJP (nonlinear
+ * weights, smoothness indicators, least squares, MUSCL fall-back) at every
+ * recomputed stage state.  ucg_adjoint_run/ucg_tangent_run are these with
+ * UCG_OBJ_FORCE_X.                                                        */
+enum { UCG_OBJ_FORCE_X = 1, UCG_OBJ_KE = 2 };
+int ucg_adjoint_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, int32_t every, double* J,
+                        double* dJdU0, double* dJdp);
+int ucg_tangent_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, const double* dU0,
+                        const double* dp, double* J, double* dJ);
 /* Average device times over `reps` evaluations at the current state (CUDA
  * events on the handle's stream), into ms[3]: ms[0] residual (reconstruction
  * + fluxes), ms[1] residual VJP, ms[2] residual JVP (MUSCL or WENO).       */

@@ -314,3 +314,96 @@ def test_adjoint_rejects_other_configurations():
         e.force()
     assert ei.value.code == N.UCG_EINVAL
     e.close()
+
+
+def _weno_run_case(name):
+    """Small WENO/CWENO cases for the adjoint runs: periodic tetrahedra
+    (every cell on the WENO branch) and the WENO3 bump channel (MUSCL
+    fall-back next to the walls, inflow/outflow ghosts), with a generic
+    perturbed state."""
+    from ucns3d_b200.config import make_config
+    from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
+    rng = np.random.default_rng(21)
+    if name == "bump_weno3":
+        m = Mesh.bump_channel(16, 8, 4, seed=2).prepare(SCHEME_WENO, 2)
+        bc = (1.0, 0.8, 0.0, 0.0, 1.0)
+        cfg = make_config(m, governing=2, bc_state=bc)
+        U = np.tile([1.0, 0.8, 0.0, 0.0, 1.0 / 0.4 + 0.32], (m.ncells, 1))
+    else:
+        m = Mesh.box_tet(4, 4, 4, seed=3).prepare(SCHEME_WENO, *((2, 0) if name == "weno3_tet" else (3, 5)))
+        cfg = make_config(m, governing=2)
+        U = m.initial_condition(IC_TGV, [1.4, 5.0, 1.0])
+    cc = m.centres()
+    U = U * (1.0 + 0.02 * np.sin(1.3 * cc[:, :1] + 0.7 * cc[:, 1:2] + 2.1 * cc[:, 2:3] + rng.uniform(0, 6.3, (1, 5))))
+    return m, cfg, U
+
+
+WENO_RUN_STEPS, WENO_RUN_EVERY = 12, 5
+
+
+@pytest.mark.parametrize("name", ["weno3_tet", "cweno4_tet", "bump_weno3"])
+def test_weno_adjoint_run_kinetic_energy(name):
+    """Adjoint through 12 SSP-RK3 steps of the WENO/CWENO residual with
+    checkpoints every 5 (J = domain kinetic energy): against central
+    differences of J after the same steps of the oracle (state and, on the
+    channel, free-stream state; 1e-5), against the tangent run (1e-10) and
+    independent of the checkpoint stride (bitwise)."""
+    from oracle import Oracle
+    m, cfg, U = _weno_run_case(name)
+    e = Engine(m, cfg)
+    e.set_state(U)
+    dt = 0.5 * e.calculate_cfl(0.5)
+    e.set_state(U)
+    J, g, gp = e.adjoint_run(WENO_RUN_STEPS, dt, every=WENO_RUN_EVERY, objective=N.UCG_OBJ_KE)
+    bc = np.array([cfg.bc_state[k] for k in range(5)])
+
+    def J_oracle(U0, bcs):
+        o = Oracle(m, _cfg_with_bc(cfg, bcs))
+        W = U0.copy()
+        for _ in range(WENO_RUN_STEPS):
+            W = o.rk3_step(W, dt)
+        return o.reduce(W, N.UCG_REDUCE_KE)
+
+    assert abs(J_oracle(U, bc) - J) <= 1e-12 * abs(J)
+    eps = 1e-6
+    du, dp = _directions(U, 41)
+    fd_u = (J_oracle(U + eps * du, bc) - J_oracle(U - eps * du, bc)) / (2 * eps)
+    ad_u = float(np.sum(g * du))
+    print(f"{name}: adjoint run dJ/dU0.du {ad_u:.10e}, oracle differences {fd_u:.10e}")
+    assert abs(ad_u - fd_u) <= 1e-5 * abs(fd_u), (ad_u, fd_u)
+    if name == "bump_weno3":
+        fd_p = (J_oracle(U, bc + eps * dp) - J_oracle(U, bc - eps * dp)) / (2 * eps)
+        ad_p = float(np.sum(gp * dp))
+        print(f"{name}: dJ/dp.dp {ad_p:.10e}, oracle differences {fd_p:.10e}")
+        assert abs(ad_p - fd_p) <= 1e-5 * abs(fd_p), (ad_p, fd_p)
+    else:
+        assert np.all(gp == 0.0)
+    e.set_state(U)
+    J1, dJ = e.tangent_run(WENO_RUN_STEPS, dt, du, dp, objective=N.UCG_OBJ_KE)
+    assert J1 == J
+    ad = float(np.sum(g * du) + np.sum(gp * dp))
+    assert abs(ad - dJ) <= 1e-10 * abs(dJ), (ad, dJ)
+    e.set_state(U)
+    J2, g2, gp2 = e.adjoint_run(WENO_RUN_STEPS, dt, every=1, objective=N.UCG_OBJ_KE)
+    assert J2 == J and np.array_equal(g2, g) and np.array_equal(gp2, gp)
+    with pytest.raises(EngineError) as ei:
+        e.adjoint_run(2, dt, objective=N.UCG_OBJ_FORCE_X)
+    assert ei.value.code == N.UCG_EINVAL
+    e.close()
+
+
+def test_muscl_adjoint_run_kinetic_energy(short_bump):
+    """The kinetic-energy objective on the MUSCL channel: adjoint run
+    against the tangent run (1e-10), with a free-stream gradient that is not
+    vacuous (the inflow state changes the kinetic energy of the cells next
+    to it from the first step)."""
+    e, U, dt = short_bump["engine"], short_bump["U"], short_bump["dt"]
+    du, dp = _directions(U, 43)
+    e.set_state(U)
+    J1, dJ = e.tangent_run(NSTEPS, dt, du, dp, objective=N.UCG_OBJ_KE)
+    e.set_state(U)
+    J2, g, gp = e.adjoint_run(NSTEPS, dt, every=EVERY, objective=N.UCG_OBJ_KE)
+    assert J1 == J2
+    ad = float(np.sum(g * du) + np.sum(gp * dp))
+    assert abs(ad - dJ) <= 1e-10 * abs(dJ), (ad, dJ)
+    assert np.abs(gp).max() > 1e-8

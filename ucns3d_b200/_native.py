@@ -18,6 +18,7 @@ UCG_MAX_QP = 16
 
 UCG_OK, UCG_EINVAL, UCG_ECUDA, UCG_ENONPHYS, UCG_ESTATE, UCG_ENOMEM, UCG_ETIMEOUT = range(7)
 UCG_FP64, UCG_MIXED = 0, 1
+UCG_OBJ_FORCE_X, UCG_OBJ_KE = 1, 2
 UCG_REDUCE_KE, UCG_REDUCE_MASS, UCG_REDUCE_ENERGY, UCG_REDUCE_ENSTROPHY = 1, 2, 3, 4
 
 ERROR_NAMES = {
@@ -134,7 +135,7 @@ ENGINE_SYMBOLS = [
     "ucg_step", "ucg_last_dt", "ucg_reduce", "ucg_check_health", "ucg_synchronize",
     "ucg_time_kernels", "ucg_get_stream", "ucg_launch_count", "ucg_device_bytes", "ucg_last_error",
     "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
-    "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order",
+    "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
 ]
 
 
@@ -196,6 +197,10 @@ def engine() -> C.CDLL:
         lib.ucg_adjoint_run.argtypes = [vp, C.c_int32, C.c_double, C.c_int32, _f64p, _f64p, _f64p]
         lib.ucg_time_adjoint.restype = C.c_int
         lib.ucg_time_adjoint.argtypes = [vp, C.c_int32, _f64p]
+        lib.ucg_adjoint_run_obj.restype = C.c_int
+        lib.ucg_adjoint_run_obj.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_int32, _f64p, _f64p, _f64p]
+        lib.ucg_tangent_run_obj.restype = C.c_int
+        lib.ucg_tangent_run_obj.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
         lib.ucg_cell_order.restype = C.c_int
         lib.ucg_cell_order.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _f64p]
         lib.ucg_tangent_run.restype = C.c_int

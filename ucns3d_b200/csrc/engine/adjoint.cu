@@ -1068,6 +1068,91 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   return UCG_OK;
 }
 
+// ------------------------------------------------ the kinetic-energy objective
+// J = sum_c V_c |m_c|^2 / (2 rho_c), the TGV kinetic-energy sum of
+// TIME_MARCHING (src/time_p.f90:4145-4198) without its normalisation.
+// Per cell: V * KE, or with a tangent dU its derivative V * dKE/dU . dU.
+__global__ void k_ke_cell(Problem p, const double* __restrict__ U, const double* __restrict__ dU,
+                          double* __restrict__ out) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const double* u = U + c * NV;
+  const double ir = 1.0 / u[0], mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  if (!dU) {
+    out[c] = p.vol[c] * (0.5 * mm * ir);
+    return;
+  }
+  const double* d = dU + c * NV;
+  out[c] = p.vol[c] * ((-0.5 * mm * ir * ir) * d[0] + (u[1] * d[1] + u[2] * d[2] + u[3] * d[3]) * ir);
+}
+// g = dJ/dU of the kinetic energy
+__global__ void k_ke_grad(Problem p, const double* __restrict__ U, double* __restrict__ g) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const double* u = U + c * NV;
+  const double ir = 1.0 / u[0], mm = u[1] * u[1] + u[2] * u[2] + u[3] * u[3], v = p.vol[c];
+  g[c * NV + 0] = v * (-0.5 * mm * ir * ir);
+  g[c * NV + 1] = v * (u[1] * ir);
+  g[c * NV + 2] = v * (u[2] * ir);
+  g[c * NV + 3] = v * (u[3] * ir);
+  g[c * NV + 4] = 0.0;
+}
+
+// The scheme-specific pieces of the adjoint and tangent runs: the residual
+// VJP/JVP (MUSCL or WENO) with their buffers, and the objective J (wall
+// force, MUSCL only; kinetic energy, either).
+struct RunOps {
+  bool weno;
+  int obj;
+  double* lam;   // scratch vectors the VJP reads and writes
+  double* mu;
+  double* cell;  // [n] per-cell objective values
+};
+
+int run_setup(ucg_engine* e, int obj, RunOps& o) {
+  o.weno = e->cfg.scheme == 3;
+  o.obj = obj;
+  if (obj != UCG_OBJ_FORCE_X && obj != UCG_OBJ_KE) return fail(e, UCG_EINVAL, "unknown objective");
+  if (o.weno && obj == UCG_OBJ_FORCE_X)
+    return fail(e, UCG_EINVAL, "the wall-force objective covers MUSCL (IORDER 1); WENO runs take the kinetic energy");
+  int rc = o.weno ? adjw_setup(e) : adj_setup(e);
+  if (rc) return rc;
+  const int64_t n = e->n;
+  // four state-sized vectors and a few scalars (bar_vec, bar_scal), and the
+  // per-cell objective values
+  rc = alloc(e, e->adj_bar, (size_t)4 * n * NV * 8 + 64 * 8);
+  rc = rc ? rc : alloc(e, e->adj_fcell, (size_t)n * 8);
+  if (rc) return rc;
+  o.lam = o.weno ? (double*)e->adjw_lam.p : (double*)e->adj_lam.p;
+  o.mu = o.weno ? (double*)e->adjw_mu.p : (double*)e->adj_mu.p;
+  o.cell = (double*)e->adj_fcell.p;
+  return UCG_OK;
+}
+int run_vjp(ucg_engine* e, const RunOps& o, const Problem& p, const double* U, const double* lam, double* mu,
+            double* psum) {
+  return o.weno ? weno_vjp_device(e, p, U, lam, mu, psum) : vjp_device(e, p, U, lam, mu, psum);
+}
+int run_jvp(ucg_engine* e, const RunOps& o, const Problem& p, const double* U, const double* dU, const Dp5& dp,
+            double* dR) {
+  return o.weno ? weno_jvp_device(e, p, U, dU, dp, dR) : jvp_device(e, p, U, dU, dp, dR);
+}
+// J (dU null) or dJ/dU . dU at U into out[0]
+int run_obj(ucg_engine* e, const RunOps& o, const Problem& p, const double* U, const double* dU, double* out) {
+  if (o.obj == UCG_OBJ_FORCE_X) return force_device(e, p, U, dU, out);
+  k_ke_cell<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, U, dU, o.cell);
+  k_sum1<<<1, 1024, 0, e->stream>>>(o.cell, e->n, out);
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+int run_obj_vjp(ucg_engine* e, const RunOps& o, const Problem& p, const double* U, double* g) {
+  if (o.obj == UCG_OBJ_FORCE_X) return force_vjp_device(e, p, U, g);
+  k_ke_grad<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, U, g);
+  e->launches++;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
 // host <-> device; [n][5] per-cell arrays go through the caller's cell order
 int copy_in(ucg_engine* e, double* dst, const double* src, size_t count) {
   if (count == (size_t)e->n * NV) return cells_in(e, dst, src);
@@ -1216,10 +1301,11 @@ int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms) {
   return UCG_OK;
 }
 
-int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, double* J, double* dJdU0,
-                    double* dJdp) {
+int ucg_adjoint_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, int32_t every, double* J,
+                        double* dJdU0, double* dJdp) {
   if (!e || nsteps < 0 || every < 1 || !(dt > 0.0)) return fail(e, UCG_EINVAL, "bad argument");
-  int rc = adj_setup(e);
+  RunOps o{};
+  int rc = run_setup(e, objective, o);
   if (rc) return rc;
   cudaSetDevice(e->device);
   const int64_t n = e->n;
@@ -1242,15 +1328,15 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
   double* sc = bar_scal(e);  // sc[0] J, sc[8..12] pbar accumulator, sc[16..20] partial
   double* pacc = sc + 8;
   double* part = sc + 16;
-  if ((rc = force_device(e, p, Un, nullptr, sc))) return rc;
+  if ((rc = run_obj(e, o, p, Un, nullptr, sc))) return rc;
   // terminal adjoint: dJ/dU^N
   double* ub = bar_vec(e, 0);   // adjoint of the current step's output
   double* u0b = bar_vec(e, 1);  // adjoint of its input
   double* u1b = bar_vec(e, 2);
   double* u2b = bar_vec(e, 3);
-  double* mu = (double*)e->adj_mu.p;
-  double* lam = (double*)e->adj_lam.p;
-  if ((rc = force_vjp_device(e, p, Un, ub))) return rc;
+  double* mu = o.mu;
+  double* lam = o.lam;
+  if ((rc = run_obj_vjp(e, o, p, Un, ub))) return rc;
   CK(cudaMemsetAsync(pacc, 0, NV * 8, e->stream));
   const unsigned bm = blocks_for((int64_t)m, 256), bv = blocks_for((int64_t)m, 256);
   for (int seg = nseg - 1; seg >= 0; --seg) {
@@ -1269,7 +1355,7 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
       const double* U2 = U0 + 2 * m;
       // U3 = 1/3 U0 + 2/3 U2 - 2/3 dt R(U2)/V
       k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, ub, lam);
-      if ((rc = vjp_device(e, p, U2, lam, mu, part))) return rc;
+      if ((rc = run_vjp(e, o, p, U2, lam, mu, part))) return rc;
       k_pacc<<<1, 32, 0, e->stream>>>(-(2.0 / 3.0) * dt, part, pacc);
       CK(cudaMemcpyAsync(u2b, ub, mb, cudaMemcpyDeviceToDevice, e->stream));
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -(2.0 / 3.0) * dt, mu, 2.0 / 3.0, u2b);
@@ -1277,14 +1363,14 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.0, ub, 1.0 / 3.0, u0b);
       // U2 = 3/4 U0 + 1/4 U1 - 1/4 dt R(U1)/V
       k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, u2b, lam);
-      if ((rc = vjp_device(e, p, U1, lam, mu, part))) return rc;
+      if ((rc = run_vjp(e, o, p, U1, lam, mu, part))) return rc;
       k_pacc<<<1, 32, 0, e->stream>>>(-0.25 * dt, part, pacc);
       CK(cudaMemcpyAsync(u1b, u2b, mb, cudaMemcpyDeviceToDevice, e->stream));
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -0.25 * dt, mu, 0.25, u1b);
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.75, u2b, 1.0, u0b);
       // U1 = U0 - dt R(U0)/V
       k_over_vol<<<bv, 256, 0, e->stream>>>(p, 1.0, u1b, lam);
-      if ((rc = vjp_device(e, p, U0, lam, mu, part))) return rc;
+      if ((rc = run_vjp(e, o, p, U0, lam, mu, part))) return rc;
       k_pacc<<<1, 32, 0, e->stream>>>(-dt, part, pacc);
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0, u1b, 1.0, u0b);
       k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, -dt, mu, 1.0, u0b);
@@ -1302,10 +1388,16 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
   return UCG_OK;
 }
 
-int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
-                    double* dJ) {
+int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, double* J, double* dJdU0,
+                    double* dJdp) {
+  return ucg_adjoint_run_obj(e, UCG_OBJ_FORCE_X, nsteps, dt, every, J, dJdU0, dJdp);
+}
+
+int ucg_tangent_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, const double* dU0,
+                        const double* dp, double* J, double* dJ) {
   if (!e || nsteps < 0 || !dU0 || !(dt > 0.0)) return fail(e, UCG_EINVAL, "bad argument");
-  int rc = adj_setup(e);
+  RunOps o{};
+  int rc = run_setup(e, objective, o);
   if (rc) return rc;
   cudaSetDevice(e->device);
   const int64_t n = e->n;
@@ -1322,20 +1414,22 @@ int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0,
   double* sc = bar_scal(e);
   const unsigned bm = blocks_for((int64_t)m, 256);
   if ((rc = copy_in(e, t0, dU0, m))) return rc;
+  // each JVP leaves the face values of its state in the reconstruction
+  // buffers, which the stage's flux and update then use
   for (int s = 0; s < nsteps; ++s) {
     // stage 1 at U0 = Un
-    if ((rc = jvp_device(e, p, Un, t0, d, dR))) return rc;
+    if ((rc = run_jvp(e, o, p, Un, t0, d, dR))) return rc;
     if ((rc = launch_flux(e, p, 1, Un, Un, (double*)e->Ua.p, dt))) return rc;
     k_over_vol<<<bm, 256, 0, e->stream>>>(p, -dt, dR, t1);
     k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0, t0, 1.0, t1);
     // stage 2 at U1 = Ua
-    if ((rc = jvp_device(e, p, (const double*)e->Ua.p, t1, d, dR))) return rc;
+    if ((rc = run_jvp(e, o, p, (const double*)e->Ua.p, t1, d, dR))) return rc;
     if ((rc = launch_flux(e, p, 2, (const double*)e->Ua.p, Un, (double*)e->Ub.p, dt))) return rc;
     k_over_vol<<<bm, 256, 0, e->stream>>>(p, -0.25 * dt, dR, t2);
     k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.75, t0, 1.0, t2);
     k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 0.25, t1, 1.0, t2);
     // stage 3 at U2 = Ub
-    if ((rc = jvp_device(e, p, (const double*)e->Ub.p, t2, d, dR))) return rc;
+    if ((rc = run_jvp(e, o, p, (const double*)e->Ub.p, t2, d, dR))) return rc;
     if ((rc = launch_flux(e, p, 3, (const double*)e->Ub.p, Un, Un, dt))) return rc;
     k_over_vol<<<bm, 256, 0, e->stream>>>(p, -(2.0 / 3.0) * dt, dR, t1);
     k_axpby<<<bm, 256, 0, e->stream>>>((int64_t)m, 1.0 / 3.0, t0, 1.0, t1);
@@ -1343,13 +1437,18 @@ int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0,
     CK(cudaMemcpyAsync(t0, t1, mb, cudaMemcpyDeviceToDevice, e->stream));
     e->launches += 9;
   }
-  if ((rc = force_device(e, p, Un, nullptr, sc))) return rc;
-  if ((rc = force_device(e, p, Un, t0, sc + 1))) return rc;
+  if ((rc = run_obj(e, o, p, Un, nullptr, sc))) return rc;
+  if ((rc = run_obj(e, o, p, Un, t0, sc + 1))) return rc;
   CK(cudaGetLastError());
   if (J && (rc = copy_out(e, J, sc, 1))) return rc;
   if (dJ && (rc = copy_out(e, dJ, sc + 1, 1))) return rc;
   CK(cudaStreamSynchronize(e->stream));
   return UCG_OK;
+}
+
+int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
+                    double* dJ) {
+  return ucg_tangent_run_obj(e, UCG_OBJ_FORCE_X, nsteps, dt, dU0, dp, J, dJ);
 }
 
 }  // extern "C"

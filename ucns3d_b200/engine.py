@@ -147,22 +147,25 @@ class Engine:
                                               N.ptr(out, C.c_double)))
         return out
 
-    def adjoint_run(self, nsteps: int, dt: float, every: int = 20):
+    def adjoint_run(self, nsteps: int, dt: float, every: int = 20, objective: int = N.UCG_OBJ_FORCE_X):
         """J after nsteps RK3 steps of fixed dt, dJ/dU0 (n, 5) and dJ/dp (5,);
-        the state becomes the final state."""
+        the state becomes the final state.  ``objective``: UCG_OBJ_FORCE_X
+        (wall force, MUSCL) or UCG_OBJ_KE (domain kinetic energy, MUSCL or
+        WENO/CWENO)."""
         J, g, gp = C.c_double(), np.empty((self.n, 5)), np.empty(5)
-        self._check(self.lib.ucg_adjoint_run(self._h, nsteps, dt, every, C.byref(J), N.ptr(g, C.c_double),
-                                             N.ptr(gp, C.c_double)))
+        self._check(self.lib.ucg_adjoint_run_obj(self._h, objective, nsteps, dt, every, C.byref(J),
+                                                 N.ptr(g, C.c_double), N.ptr(gp, C.c_double)))
         return J.value, g, gp
 
-    def tangent_run(self, nsteps: int, dt: float, dU0: np.ndarray, dp: np.ndarray | None = None):
+    def tangent_run(self, nsteps: int, dt: float, dU0: np.ndarray, dp: np.ndarray | None = None,
+                    objective: int = N.UCG_OBJ_FORCE_X):
         """J and its directional derivative along (dU0, dp) after nsteps
         RK3 steps of fixed dt; the state becomes the final state."""
         dU0 = np.ascontiguousarray(dU0, dtype=np.float64)
         dp = None if dp is None else np.ascontiguousarray(dp, dtype=np.float64)
         J, dJ = C.c_double(), C.c_double()
-        self._check(self.lib.ucg_tangent_run(self._h, nsteps, dt, N.ptr(dU0, C.c_double), N.ptr(dp, C.c_double),
-                                             C.byref(J), C.byref(dJ)))
+        self._check(self.lib.ucg_tangent_run_obj(self._h, objective, nsteps, dt, N.ptr(dU0, C.c_double),
+                                                 N.ptr(dp, C.c_double), C.byref(J), C.byref(dJ)))
         return J.value, dJ.value
 
     def time_adjoint(self, reps: int = 5) -> dict:
