@@ -215,6 +215,16 @@ int ucg_synchronize(ucg_engine* e);
  * leaves the state unchanged.                                              */
 int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms);
 
+/* Bounded device waits.  The opt-in least squares through the shared-memory
+ * bulk-copy ring (UCG_LSQ_BULK=1 in the environment at ucg_create) waits on
+ * each copy for at most `polls` polls (about 300 ns each; the default, about
+ * 20 ms, is restored by polls < 0).  A wait that gives up makes its warp
+ * finish the copies it has in flight (each with the default bound) and
+ * return, and the next ucg_check_health reports UCG_ETIMEOUT; the handle
+ * stays usable.  polls = 0 makes every such wait give up at once, which
+ * exercises that path without a fault.  No counterpart in the reference. */
+int ucg_set_wait_limit(ucg_engine* e, int64_t polls);
+
 /* The cell numbering chosen at ucg_upload_geometry.  With cfg.reorder 1 the
  * engine computes reverse Cuthill-McKee and keeps it only if the face
  * neighbours of each 32-cell warp then span fewer 128-byte lines of the

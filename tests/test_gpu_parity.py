@@ -220,6 +220,31 @@ def test_bulk_copy_lsq_is_bitwise_equal(name, precision, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
+def test_bulk_copy_wait_timeout_is_reported_and_recoverable(monkeypatch):
+    """The bounded waits of the opt-in bulk-copy least squares: with a wait
+    limit of 0 polls every stage wait gives up, the warps drain their copies
+    in flight and return, ucg_check_health reports UCG_ETIMEOUT, and with the
+    default limit restored the same handle gives the normal residual bit for
+    bit."""
+    m, cfg, U = _setup("weno5_hex", N.UCG_MIXED)
+    monkeypatch.setenv("UCG_LSQ_BULK", "1")
+    e = Engine(m, cfg)
+    e.set_state(U)
+    ref = e.residual()
+    e.check_health()
+    assert e.lib.ucg_set_wait_limit(e._h, 0) == N.UCG_OK
+    e.residual()
+    with pytest.raises(EngineError) as ei:
+        e.check_health()
+    assert ei.value.code == N.UCG_ETIMEOUT
+    assert e.lib.ucg_set_wait_limit(e._h, -1) == N.UCG_OK
+    e.set_state(U)
+    again = e.residual()
+    e.check_health()
+    assert np.array_equal(again, ref)
+    e.close()
+
+
 def test_bitwise_deterministic():
     m, cfg, U = _setup("weno3_tet")
     out = []

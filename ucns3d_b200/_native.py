@@ -136,6 +136,7 @@ ENGINE_SYMBOLS = [
     "ucg_time_kernels", "ucg_get_stream", "ucg_launch_count", "ucg_device_bytes", "ucg_last_error",
     "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
+    "ucg_set_wait_limit",
 ]
 
 
@@ -201,6 +202,8 @@ def engine() -> C.CDLL:
         lib.ucg_adjoint_run_obj.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_int32, _f64p, _f64p, _f64p]
         lib.ucg_tangent_run_obj.restype = C.c_int
         lib.ucg_tangent_run_obj.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
+        lib.ucg_set_wait_limit.restype = C.c_int
+        lib.ucg_set_wait_limit.argtypes = [vp, C.c_int64]
         lib.ucg_cell_order.restype = C.c_int
         lib.ucg_cell_order.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _f64p]
         lib.ucg_tangent_run.restype = C.c_int

@@ -78,6 +78,7 @@ struct Problem {
   double* vflux;            // [n][MF][NV] viscous face sums
   unsigned* health;
   int lsq_bulk;  // stencil least squares through the shared-memory bulk-copy ring (k_lsq_tma)
+  long lsq_wait; // polls of a k_lsq_tma stage wait before it gives up (< 0: the default)
   int wenwrt;    // 1 conserved-variable WENO, 2 characteristic-variable WENO
   int riemann;   // 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL
   int limiter;   // SLOPE_LIMITERS code (7 Venkatakrishnan)

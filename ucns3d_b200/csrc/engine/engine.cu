@@ -140,6 +140,7 @@ Problem make_problem(ucg_engine* e) {
   p.health = (unsigned*)e->health.p;
   p.dt_dev = nullptr;
   p.lsq_bulk = e->lsq_bulk ? 1 : 0;
+  p.lsq_wait = e->lsq_wait;
   p.wenwrt = c.wenwrt;
   p.riemann = c.riemann;
   p.limiter = c.limiter;
@@ -1012,6 +1013,12 @@ int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
   if (rc) return rc;
   for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
   CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int ucg_set_wait_limit(ucg_engine* e, int64_t polls) {
+  if (!e) return UCG_EINVAL;
+  e->lsq_wait = polls < 0 ? -1 : (long)polls;
   return UCG_OK;
 }
 

@@ -57,6 +57,7 @@ struct ucg_engine {
   int64_t nown_plain = 0;  // owned faces [0, nown_plain): interior and mirror; the rest other boundaries
   cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs
   bool lsq_bulk = false;       // UCG_LSQ_BULK=1 at ucg_create: k_lsq_tma instead of k_lsq
+  long lsq_wait = -1;          // polls of a k_lsq_tma stage wait (ucg_set_wait_limit; < 0 the default)
   std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
   std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
   std::vector<int32_t> neigh_h;     // [n][6] face neighbours (host copy, adjoint set-up)

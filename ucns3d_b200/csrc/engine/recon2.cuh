@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(128) k_lsq(Problem p, const double* __restrict
 // flight while the warp multiplies the current one; the gathered neighbour
 // state of the next member is loaded one member ahead.  Same products and
 // accumulation order as k_lsq, so G is the same bit for bit.  A wait that
-// gives up sets HEALTH_TIMEOUT, drains the copies in flight (bounded) and
+// gives up (after Problem::lsq_wait polls) sets HEALTH_TIMEOUT, drains the
+// copies in flight (each wait bounded by LSQ_WAIT, whatever lsq_wait is) and
 // leaves the group.  Opt-in (Problem::lsq_bulk): on B200 it takes 7.2 ms
 // against k_lsq's 5.8 ms for the mixed WENO5 64^3 stage, at 3, 4 or 6
 // stages alike, because k_lsq is bound by the per-member gather of the
@@ -183,6 +184,7 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
   for (; issued < NSTG && ill < admw; ++issued) copy_next(issued);
   int t = 0;  // members consumed
   bool ok = true;
+  const long wait = p.lsq_wait < 0 ? LSQ_WAIT : p.lsq_wait;
   for (int ll = 0; ll < admw && ok; ++ll) {
     const int nk = n_k(ll), nd = n_d(ll);
     const bool act = ll < adm;
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
           for (int v = 0; v < NV; ++v) un[v] = uy[v];
         }
         const int slot = t % NSTG;
-        if (!__all_sync(0xffffffffu, mbar_wait(&bar[slot], (unsigned)(t / NSTG) & 1u, LSQ_WAIT))) {
+        if (!__all_sync(0xffffffffu, mbar_wait(&bar[slot], (unsigned)(t / NSTG) & 1u, wait))) {
           ok = false;
           break;
         }
