@@ -368,3 +368,22 @@ def test_call_order_is_checked():
     e.set_state(U)
     e.runge_kutta3(1e-3)
     e.check_health()
+
+
+@pytest.mark.parametrize("name", ["weno5_hex", "cweno4_tet", "weno3_channel", "cweno4_ns_mixed"])
+@pytest.mark.parametrize("precision", [N.UCG_FP64, N.UCG_MIXED])
+def test_indicator_kernel_is_bitwise_equal(name, precision, monkeypatch):
+    """The smoothness indicators formed by k_wis (one warp per stencil of a
+    32-cell group, the default) and inside k_wpost (UCG_WENO_IS=0 at engine
+    creation) are the same quadratic forms in the same order: residuals
+    equal bit for bit."""
+    m, cfg, U = _setup(name, precision)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("UCG_WENO_IS", flag)
+        e = Engine(m, cfg)
+        e.set_state(U)
+        out.append(e.residual())
+        e.check_health()
+        e.close()
+    assert np.array_equal(out[0], out[1])

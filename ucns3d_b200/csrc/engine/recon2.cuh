@@ -355,6 +355,77 @@ __device__ __forceinline__ void sym_form(const T* __restrict__ P, const T (&g)[N
   }
 }
 
+// Smoothness indicators IS[ll][v] = g^T S g of every stencil polynomial,
+// one block per 32-cell group with one warp per stencil: lane i of warp ll
+// takes stencil ll of cell i of the group.  The warps of a block read the
+// same packed triangles (the cells' INDICATOR, prestore.f90:1529-1673) at
+// about the same time, so each triangle comes from DRAM once and is reused
+// from L1/L2 by the other stencils, instead of once per stencil as when one
+// lane runs all the stencils of its cell.  Output: p.isb, FP64, interleaved
+// over 32-cell groups ((group * A + ll) * NV + v) * 32 + lane; cells that
+// take the MUSCL fall-back outright (not FULL) are skipped.
+template <int P, typename T>
+__global__ void __launch_bounds__(224) k_wis(Problem p) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int VEC = Vec<T>::N;
+  constexpr int L2 = ID < 9 ? ID : 9;
+  constexpr int VI = WVars<T>::is;
+  const int lane = threadIdx.x & 31, ll = threadIdx.x >> 5;
+  const int64_t grp = blockIdx.x, c = grp * 32 + lane;
+  if (c >= p.n || !p.full[c]) return;
+  const int adm = p.admis[c];
+  if (ll >= adm) return;
+  const int A = p.admis_max, ID2 = p.ideg2;
+  const bool cw = p.ees == 5, low = cw && ll > 0;
+  const T* Gc = (const T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + lane;
+  auto G = [&](int l, int d, int v) -> T { return Gc[(int64_t)((l * ID + d) * NV + v) * 32]; };
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
+  double* out = p.isb + (grp * A + ll) * (int64_t)NV * 32 + lane;
+  for (int v0 = 0; v0 < NV; v0 += VI) {
+    T is[VI];
+#pragma unroll
+    for (int k = 0; k < VI; ++k) is[k] = T(0);
+    if (low) {
+      T g[L2][VI];
+#pragma unroll
+      for (int d = 0; d < L2; ++d)
+#pragma unroll
+        for (int k = 0; k < VI; ++k) g[d][k] = (v0 + k < NV && d < ID2) ? G(ll, d, v0 + k) : T(0);
+      quad_form<L2, VI>(Pc + (int64_t)(p.i2off / VEC) * 32 * VEC, g, ID2, is);
+    } else {
+      T g[ID][VI];
+#pragma unroll
+      for (int d = 0; d < ID; ++d)
+#pragma unroll
+        for (int k = 0; k < VI; ++k) g[d][k] = (v0 + k < NV) ? G(ll, d, v0 + k) : T(0);
+      if (ll == 0 && cw) {  // the CWENO central polynomial with the lower-order stencils removed
+        T g3[L2][VI];
+#pragma unroll
+        for (int d = 0; d < L2; ++d)
+#pragma unroll
+          for (int k = 0; k < VI; ++k) g3[d][k] = T(0);
+        for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+          for (int d = 0; d < L2; ++d)
+#pragma unroll
+            for (int k = 0; k < VI; ++k)
+              if (v0 + k < NV && d < ID2) g3[d][k] = g3[d][k] + T(lk) * G(l2, d, v0 + k);
+#pragma unroll
+        for (int d = 0; d < ID; ++d)
+#pragma unroll
+          for (int k = 0; k < VI; ++k)
+            if (v0 + k < NV) g[d][k] = T(1.0 / lc1) * (g[d][k] - (d < L2 ? g3[d][k] : T(0)));
+      }
+      quad_form<ID, VI>(Pc, g, ID, is);
+    }
+#pragma unroll
+    for (int k = 0; k < VI; ++k)
+      if (v0 + k < NV) out[(int64_t)(v0 + k) * 32] = (double)is[k];
+  }
+}
+
 // k_wpost: one lane per cell, no block barriers.  Indicators and weights of
 // CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), the combined
 // polynomial, its face values and CHECKSOL; flagged cells (and every cell of
@@ -363,7 +434,8 @@ __device__ __forceinline__ void sym_form(const T* __restrict__ P, const T (&g)[N
 // face value minus cell mean, 0 in unused slots.  A face value is
 // sum_d m_d(x) g_d - sum_d mean(m_d) g_d: the second sum is formed once per
 // polynomial instead of subtracting the basis means at every face point.
-template <int P, typename T, bool CH = false>
+// ISB: the indicators come from k_wis (p.isb) instead of being formed here.
+template <int P, typename T, bool CH = false, bool ISB = false>
 __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<T>::N;
@@ -479,7 +551,13 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
     }
   };
   bool fall = !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
-  if (!CH && !fall) {
+  if (!CH && !fall && ISB) {
+    // ---- smoothness indicators from k_wis
+    const double* is = p.isb + grp * (int64_t)A * NV * 32 + lane;
+    for (int ll = 0; ll < adm; ++ll)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sw[(ll * NV + v) * BT] = is[(int64_t)(ll * NV + v) * 32];
+  } else if (!CH && !ISB && !fall) {
     // ---- smoothness indicators g^T S g per stencil and variable
     const T* Pc = (const T*)p.ind + grp * p.istride * 32 + lane * VEC;
     for (int ll = 0; ll < adm; ++ll) {
@@ -503,6 +581,8 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
           if (v0 + k < NV) sw[(ll * NV + v0 + k) * BT] = (double)is[k];
       }
     }
+  }
+  if (!CH && !fall) {
     weights();
     // ---- combined polynomial, face values, CHECKSOL (threshold 0.85)
     bool flag = false;
@@ -1027,7 +1107,13 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     const cudaError_t e = launch_wpost_char<P, T>(p, U, st);
     if (e != cudaSuccess) return e;
   } else {
-    k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+    if (p.isb && p.scheme == 3) {
+      k_wis<P, T><<<(unsigned)((p.n + 31) / 32), 32 * p.admis_max, 0, st>>>(p);
+      k_wpost<P, T, false, true><<<b, 128, 0, st>>>(p, U);
+      ++*launches;
+    } else {
+      k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+    }
   }
   *launches += 2;
   if (ns) {
