@@ -463,7 +463,7 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
     rc = rc ? rc : alloc(e, e->gbuf, (size_t)ngrp * 32 * c.admis_max * c.ideg * NV * T);
     if (c.iorder == 3) rc = rc ? rc : alloc(e, e->upad, (size_t)n * 6 * 8);  // k_lsq<3, T, true>
   }
-  if (c.scheme == 3 && c.wenwrt == 1) {  // smoothness indicators of every stencil (k_wis)
+  if (c.scheme == 3 && c.wenwrt == 1 && c.iorder == 4) {  // smoothness indicators of every stencil (k_wis)
     const char* wis = std::getenv("UCG_WENO_IS");
     if (!(wis && wis[0] == '0')) rc = rc ? rc : alloc(e, e->isb, (size_t)ngrp * 32 * c.admis_max * NV * 8);
   }

@@ -1107,13 +1107,21 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     const cudaError_t e = launch_wpost_char<P, T>(p, U, st);
     if (e != cudaSuccess) return e;
   } else {
-    if (p.isb && p.scheme == 3) {
-      k_wis<P, T><<<(unsigned)((p.n + 31) / 32), 32 * p.admis_max, 0, st>>>(p);
-      k_wpost<P, T, false, true><<<b, 128, 0, st>>>(p, U);
-      ++*launches;
-    } else {
-      k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
+    // indicators in their own kernel at IORDER 4, where the cell's packed
+    // triangle (595 entries) no longer stays in L1 between the stencils of
+    // one lane (64^3 WENO5: FP64 stage 17.2 -> 15.5 ms, mixed 7.80 -> 7.67 ms);
+    // at IORDER 2-3 the triangle is small and the extra kernel costs more
+    // than it saves (2.1 M-cell CWENO4: 17.3 -> 19.6 ms)
+    bool done = false;
+    if constexpr (P == 4) {
+      if (p.isb && p.scheme == 3) {
+        k_wis<P, T><<<(unsigned)((p.n + 31) / 32), 32 * p.admis_max, 0, st>>>(p);
+        k_wpost<P, T, false, true><<<b, 128, 0, st>>>(p, U);
+        ++*launches;
+        done = true;
+      }
     }
+    if (!done) k_wpost<P, T><<<b, 128, 0, st>>>(p, U);
   }
   *launches += 2;
   if (ns) {
