@@ -26,6 +26,7 @@
 //                                                    src/flux_p.f90:478, riemann.f90:221, 1236, 28,
 //                                                    grid_t.f90:4217
 //   CALCULATE_FLUXESHI_DIFFUSIVE + SUTHERLAND        src/flux_p.f90:1520, flow_operations.f90:2609
+//   CALCULATE_BOUNDED_VISCOUS (walls, boundaries)    src/dg_functions.f90:1179
 //   BOUNDARYS (inflow/outflow/symmetry/wall/far field, BOUNDTYPE 0|1)
 //                                                    src/flow_operations.f90:2860-3375
 //   RUNGE_KUTTA3, CALCULATE_CFL                      src/time_p.f90:885-1027, 27-191
@@ -704,8 +705,17 @@ void boundary_state(const Ctx& x, int code, const double* ang, const double* cl,
       }
       return;
     }
-    case 3:    // SYMMETRY (:3102)
-    case 4: {  // WALL, ITESTCASE 3 (:3140): the face-frame normal momentum mirrored
+    case 4:  // WALL (:3140)
+      if (cfg->governing == 1) {  // ITESTCASE 4 (:3172-3186): no slip, the whole momentum mirrored
+        cr[0] = cl[0];
+        cr[1] = -cl[1];
+        cr[2] = -cl[2];
+        cr[3] = -cl[3];
+        cr[4] = cl[4];
+        return;
+      }
+      [[fallthrough]];
+    case 3: {  // SYMMETRY (:3102), and the ITESTCASE 3 wall: the face-frame normal momentum mirrored
       double rl[NV], rr[NV];
       rotf(ang, cl, rl);
       rr[0] = rl[0];
@@ -993,11 +1003,27 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
         int64_t nb = g->neigh[c * F + f];
         int nf = g->neigh_face[c * F + f];
         for (int q = 0; q < nq_of(x, c, f); ++q) {
-          int qq = g->qperm[(c * F + f) * Q + q];
           const double* cl = &UL[(((size_t)c * F + f) * Q + q) * NV];
-          const double* cr = &UL[(((size_t)nb * F + nf) * Q + qq) * NV];
           const double* gl = &ULV[(((size_t)c * F + f) * Q + q) * 12];
-          const double* gr = &ULV[(((size_t)nb * F + nf) * Q + qq) * 12];
+          const double* cr;
+          const double* gr;
+          double crb[NV];
+          double damp = cfg->lamx, vdamp = 4.0 / 3.0;
+          if (nb >= 0) {
+            int qq = g->qperm[(c * F + f) * Q + q];
+            cr = &UL[(((size_t)nb * F + nf) * Q + qq) * NV];
+            gr = &ULV[(((size_t)nb * F + nf) * Q + qq) * 12];
+          } else {
+            // CALCULATE_BOUNDED_VISCOUS (dg_functions.f90:1179-1300): the
+            // ghost state of BOUNDARYS and the cell's own gradients on the
+            // ghost side; codes 1-4 drop the jump term (flux_p.f90:1872-1874)
+            const double ang[4] = {std::cos(a1), std::sin(a1), std::cos(a2), std::sin(a2)};
+            const int code = g->bc[c * F + f];
+            boundary_state(x, code, ang, cl, crb);
+            cr = crb;
+            gr = gl;
+            if (code > 0 && code < 5) damp = 0.0;
+          }
           double lv[NV], rv[NV];
           cons2prim(x, cl, lv);
           cons2prim(x, cr, rv);
@@ -1010,7 +1036,6 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
             lg[0][k] = gl[1 * 3 + k]; lg[1][k] = gl[2 * 3 + k]; lg[2][k] = gl[3 * 3 + k]; lg[3][k] = gl[0 * 3 + k];
             rg[0][k] = gr[1 * 3 + k]; rg[1][k] = gr[2 * 3 + k]; rg[2][k] = gr[3 * 3 + k]; rg[3][k] = gr[0 * 3 + k];
           }
-          double damp = cfg->lamx, vdamp = 4.0 / 3.0;
           double dih = std::fabs(g->dih[c * F + f]);
           double jump[4] = {rv[1] - lv[1], rv[2] - lv[2], rv[3] - lv[3],
                             (rv[4] / (rv[0] * cfg->r_gas)) - (lv[4] / (lv[0] * cfg->r_gas))};
@@ -1060,11 +1085,6 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
 bool check_ctx(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r) {
   if (!cfg || !g || !r) return false;
   if (r->first != 0 || r->count != g->ncells) return false;
-  if (cfg->governing == 1) {
-    for (int64_t c = 0; c < g->ncells; ++c)
-      for (int f = 0; f < g->nfaces[c]; ++f)
-        if (g->neigh[c * F + f] < 0) return false;  // viscous walls are not restated
-  }
   return true;
 }
 

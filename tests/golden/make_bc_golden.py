@@ -68,7 +68,7 @@ def sub_out(s1, s2, sps, n):
     return s3
 
 
-def boundarys(code, boundtype, g, free, a1, a2, left):
+def boundarys(code, boundtype, g, free, a1, a2, left, navier_stokes=False):
     """Ghost state RIGHTV of BOUNDARYS for the conserved LEFTV `left`."""
     n = np.array([np.cos(a1) * np.sin(a2), np.sin(a1) * np.sin(a2), np.cos(a2)])
     inflow = to_cons(g, free)
@@ -83,6 +83,8 @@ def boundarys(code, boundtype, g, free, a1, a2, left):
         if boundtype == 0 or vel / (sps + TOLSMALL) > 1.0:
             return left.copy()
         return to_cons(g, sub_out(free, s2, sps, n))
+    if code == 4 and navier_stokes:  # ITESTCASE 4: no slip
+        return np.array([left[0], -left[1], -left[2], -left[3], left[4]])
     if code in (3, 4):
         rot = rotation(a1, a2) @ left
         rot[1] = -rot[1]
@@ -119,10 +121,12 @@ def main():
     cases = []
     for code in (1, 2, 3, 4, 6):
         for bt in (0, 1):
-            for w, a1, a2 in states:
-                left = to_cons(g, w)
-                cases.append({"code": code, "boundtype": bt, "angles": [float(a1), float(a2)],
-                              "left": left.tolist(), "ghost": boundarys(code, bt, g, free, a1, a2, left).tolist()})
+            for ns in ((False, True) if code == 4 else (False,)):
+                for w, a1, a2 in states:
+                    left = to_cons(g, w)
+                    cases.append({"code": code, "boundtype": bt, "governing": 1 if ns else 2,
+                                  "angles": [float(a1), float(a2)], "left": left.tolist(),
+                                  "ghost": boundarys(code, bt, g, free, a1, a2, left, ns).tolist()})
     out = {"gamma": g, "free_stream": free.tolist(), "cases": cases}
     with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "bc_kat.json"), "w") as fh:
         json.dump(out, fh, indent=0)

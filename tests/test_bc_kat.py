@@ -2,7 +2,8 @@
 the oracle and of the engine's device function against known-answer vectors
 from an independent numpy restatement of the Fortran
 (tests/golden/make_bc_golden.py -> bc_kat.json): codes 1 inflow, 2 outflow,
-3 symmetry, 4 inviscid wall and 6 far field, BOUNDTYPE 0 and 1, subsonic and
+3 symmetry, 4 wall (inviscid for Euler, no slip for Navier-Stokes) and 6
+far field, BOUNDTYPE 0 and 1, subsonic and
 supersonic states into and out of the domain.  The engine's function is
 compiled with nvcc as host code (tests/bc_host_check.cu); no GPU needed.
 Tolerance: 1e-13 of the largest component of the state (the restatements
@@ -23,10 +24,11 @@ ROOT = os.path.dirname(HERE)
 KAT = json.load(open(os.path.join(HERE, "golden", "bc_kat.json")))
 
 
-def _cfg(boundtype):
+def _cfg(boundtype, governing=2):
     cfg = N.UcgConfig()
     cfg.gamma = KAT["gamma"]
     cfg.boundtype = boundtype
+    cfg.governing = governing
     for k in range(5):
         cfg.bc_state[k] = KAT["free_stream"][k]
     return cfg
@@ -39,6 +41,7 @@ def _err(got, want):
 def test_kat_covers_every_branch():
     codes = {(c["code"], c["boundtype"]) for c in KAT["cases"]}
     assert codes == {(c, b) for c in (1, 2, 3, 4, 6) for b in (0, 1)}
+    assert {c["governing"] for c in KAT["cases"] if c["code"] == 4} == {1, 2}
     # the far field meets all four of its branches (inflow/outflow x subsonic/supersonic)
     g = KAT["gamma"]
     seen = set()
@@ -57,7 +60,7 @@ def test_kat_covers_every_branch():
 def test_oracle_boundary_states_match_kat():
     worst = 0.0
     for c in KAT["cases"]:
-        got = orc.boundary(_cfg(c["boundtype"]), c["code"], c["angles"], c["left"])
+        got = orc.boundary(_cfg(c["boundtype"], c["governing"]), c["code"], c["angles"], c["left"])
         worst = max(worst, _err(got, c["ghost"]))
     assert worst < 1e-13, worst
 
@@ -76,7 +79,8 @@ def test_engine_boundary_ghost_matches_kat(tmp_path):
                            "-I", os.path.join(ROOT, "include"), os.path.join(HERE, "bc_host_check.cu"), "-o", exe])
     lines = [" ".join(repr(float(x)) for x in [KAT["gamma"], *KAT["free_stream"]])]
     for c in KAT["cases"]:
-        lines.append(" ".join([str(c["code"]), str(c["boundtype"])] + [repr(float(x)) for x in c["angles"] + c["left"]]))
+        lines.append(" ".join([str(c["code"]), str(c["boundtype"]), str(c["governing"])] +
+                              [repr(float(x)) for x in c["angles"] + c["left"]]))
     out = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True, check=True).stdout
     got = np.array([[float(x) for x in ln.split()] for ln in out.strip().splitlines()])
     assert got.shape == (len(KAT["cases"]), 5)

@@ -41,12 +41,19 @@ SMALL["weno3_farfield_tet"] = (lambda: Mesh.box_tet(6, 6, 4, L=(3.0, 2.0, 1.0), 
                                                     bc=(6, 6, 6, 6, 0, 0), seed=8), SCHEME_WENO, 2, 0, EULER)
 SMALL["muscl_bump_bt0"] = (lambda: Mesh.bump_channel(24, 10, 2, seed=2), SCHEME_MUSCL, 1, 0, EULER)
 FARFIELD = ("muscl_farfield_hex", "weno3_farfield_tet")
+# Navier-Stokes on the bump channel: no-slip walls, inflow, outflow and
+# symmetry faces (the bounded viscous fluxes of CALCULATE_BOUNDED_VISCOUS)
+SMALL["muscl_ns_bump"] = (lambda: Mesh.bump_channel(24, 10, 2, seed=2), SCHEME_MUSCL, 1, 0, NAVIER_STOKES)
+SMALL["weno3_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 4, seed=2), SCHEME_WENO, 2, 0, NAVIER_STOKES)
+SMALL["cweno4_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 4, seed=2), SCHEME_WENO, 3, 5, NAVIER_STOKES)
+BUMPLIKE = ("muscl_bump", "weno3_channel", "muscl_bump_bt0", "weno5_channel", "muscl_ns_bump", "weno3_ns_bump",
+            "cweno4_ns_bump")
 
 # characteristic-variable WENO (WENWRT 2) on the WENO cases, and on a
 # channel with inflow/outflow/slip walls (boundary ghosts in the eigenvectors)
 SMALL["weno3_channel"] = (lambda: Mesh.bump_channel(16, 8, 8, seed=2), SCHEME_WENO, 2, 0, EULER)
 SMALL["weno5_channel"] = (lambda: Mesh.bump_channel(24, 12, 12, seed=2), SCHEME_WENO, 4, 0, EULER)
-CHAR = ["weno3_tet", "weno5_hex", "cweno4_tet", "cweno4_ns_mixed", "weno3_channel"]
+CHAR = ["weno3_tet", "weno5_hex", "cweno4_tet", "cweno4_ns_mixed", "weno3_channel", "weno3_ns_bump"]
 
 
 def _setup(name, precision=N.UCG_FP64, wenwrt=1):
@@ -54,7 +61,8 @@ def _setup(name, precision=N.UCG_FP64, wenwrt=1):
     m = mk().prepare(scheme, iorder, ees)
     p0 = 71.43
     bc = (1.0, 0.675 * np.sqrt(1.4), 0.0, 0.0, 1.0)
-    cfg = make_config(m, governing=gov, precision=precision, reynolds=1600.0, pres=p0 if gov == NAVIER_STOKES else 1.0,
+    cfg = make_config(m, governing=gov, precision=precision, reynolds=1600.0,
+                      pres=p0 if gov == NAVIER_STOKES and name not in BUMPLIKE else 1.0,
                       prandtl=0.71, bc_state=bc, wenwrt=wenwrt, boundtype=0 if name.endswith("_bt0") else 1)
     if name in FARFIELD:
         # a stream along x whose density and speed vary across the box: the
@@ -66,7 +74,7 @@ def _setup(name, precision=N.UCG_FP64, wenwrt=1):
         uy = 0.3 * np.sin(2 * np.pi * c[:, 0] / 3.0)
         p = 1.0 + 0.1 * np.cos(2 * np.pi * c[:, 2])
         U = np.stack([rho, rho * ux, rho * uy, 0.0 * rho, p / 0.4 + 0.5 * rho * (ux * ux + uy * uy)], axis=1)
-    elif name in ("muscl_bump", "weno3_channel", "muscl_bump_bt0", "weno5_channel"):
+    elif name in BUMPLIKE:
         U = m.initial_condition(1, [1.4, *bc])
         # a smooth disturbance so that every branch sees non-trivial data
         c = m.centres()
@@ -171,7 +179,8 @@ def test_characteristic_weno_mixed_close_to_fp64(name):
     assert err < 2e-5
 
 
-@pytest.mark.parametrize("name", ["muscl_ns_hex", "weno3_tet", "weno5_hex", "cweno4_tet", "muscl_bump"])
+@pytest.mark.parametrize("name", ["muscl_ns_hex", "weno3_tet", "weno5_hex", "cweno4_tet", "muscl_bump", "muscl_ns_bump",
+                                  "weno3_ns_bump"])
 def test_rk3_steps_match_oracle(name):
     m, cfg, U = _setup(name)
     o = Oracle(m, cfg)

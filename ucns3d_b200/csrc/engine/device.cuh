@@ -699,7 +699,9 @@ namespace ucg {
 //             when |u|/c > 1 at the cell, else the subsonic characteristic state
 //   2 outflow (:2972): BOUNDTYPE 0 the cell's own state; BOUNDTYPE 1 that state
 //             when |u|/c > 1, else the state at the free-stream pressure
-//   3 symmetry, 4 inviscid wall (:3102, :3140): normal momentum mirrored
+//   3 symmetry, 4 wall (:3102, :3140): normal momentum mirrored; a wall of a
+//             Navier-Stokes run (ITESTCASE 4, :3172-3186) mirrors the whole
+//             momentum (no slip)
 //   6 far field (:3230): inflow or outflow by the sign of the face-frame normal
 //             momentum rho*u_n of the cell, supersonic when |rho*u_n| >= c (the
 //             reference compares that momentum, not the velocity, with the sound
@@ -733,6 +735,14 @@ __host__ __device__ __forceinline__ void boundary_ghost(const Problem& p, int co
                                                S* cr) {
   const double gm = p.gamma;
   const double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
+  if (code == 4 && p.governing == 1) {  // Navier-Stokes wall: no slip
+    cr[0] = cl[0];
+    cr[1] = -cl[1];
+    cr[2] = -cl[2];
+    cr[3] = -cl[3];
+    cr[4] = cl[4];
+    return;
+  }
   if (code == 3 || code == 4) {  // symmetry / inviscid wall: mirror the normal momentum
     S a[NV], b[NV];
     rot_f(r, cl, a);
@@ -785,8 +795,11 @@ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const
   boundary_ghost<double>(p, code, r, cl, p.bc_state, cr);
 }
 
+// `damp` multiplies the jump term: LAMX on interior and far-field faces, 0
+// on faces with boundary codes 1-4 (flux_p.f90:1872-1874).
 __device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, double dih, const double* cl,
-                                             const double* cr, const double* gl, const double* gr, double* fv) {
+                                             const double* cr, const double* gl, const double* gr, double* fv,
+                                             double damp) {
   double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
   double nn[3] = {nx, ny, nz};
   double lv[NV], rv[NV];
@@ -805,7 +818,7 @@ __device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, 
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      gg[a][k] = (gl[src[a] * 3 + k] + gr[src[a] * 3 + k]) / 2.0 + p.lamx * (vd * nn[k] * jump[a]);
+      gg[a][k] = (gl[src[a] * 3 + k] + gr[src[a] * 3 + k]) / 2.0 + damp * (vd * nn[k] * jump[a]);
   double lam2 = 0.5 * (laml + lamr), mu2 = 0.5 * (mul + mur);
   double ux = gg[0][0], uy = gg[0][1], uz = gg[0][2];
   double vx = gg[1][0], vy = gg[1][1], vz = gg[1][2];

@@ -539,7 +539,6 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
         return fail(e, UCG_EINVAL, "neighbour face out of range at cell " + std::to_string(c));
       if (nb < 0) {
         int code = g->bc[i];
-        if (ns) return fail(e, UCG_EINVAL, "Navier-Stokes with physical boundary faces is not supported");
         if (code != 1 && code != 2 && code != 3 && code != 4 && code != 6)
           return fail(e, UCG_EINVAL, "unsupported boundary code " + std::to_string(code));
       }

@@ -204,14 +204,19 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
     const double ws = face_weight(p, ft, q) * area;
 #pragma unroll
     for (int v = 0; v < NV; ++v) god[v] = god[v] + fl[v] * ws;
-    if (NS && nb >= 0) {
+    if (NS) {
       // both sides' face-point gradients as six 16-byte loads each; the WENO
       // path stores their average once per face point (both pointers at it:
-      // (g + g) / 2 is g exactly)
+      // (g + g) / 2 is g exactly).  On a physical boundary face the ghost
+      // side takes the cell's own gradient (CALCULATE_BOUNDED_VISCOUS,
+      // dg_functions.f90:1179-1300) and faces with codes 1-4 drop the jump
+      // term (flux_p.f90:1872-1874).
       const double2* gl2 = (const double2*)(p.fgrad ? p.fgrad + (i * QS + q) * 12
                                                     : p.ulv + ((c * MF + f) * QS + q) * 12);
       const double2* gr2 = (const double2*)(p.fgrad ? p.fgrad + (i * QS + q) * 12
-                                                    : p.ulv + ((nb * MF + nf) * QS + qq) * 12);
+                                                    : nb >= 0 ? p.ulv + ((nb * MF + nf) * QS + qq) * 12
+                                                              : p.ulv + ((c * MF + f) * QS + q) * 12);
+      const int code = nb >= 0 ? 0 : p.bc[c * MF + f];
       double gl[12], gr[12];
 #pragma unroll
       for (int k = 0; k < 6; ++k) {
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
         gr[2 * k + 1] = b2.y;
       }
       double fv[NV];
-      viscous_flux(p, r, p.dih[c * MF + f], cl, cr, gl, gr, fv);
+      viscous_flux(p, r, p.dih[c * MF + f], cl, cr, gl, gr, fv, code >= 1 && code <= 4 ? 0.0 : p.lamx);
 #pragma unroll
       for (int v = 0; v < NV; ++v) gvis[v] = gvis[v] + fv[v] * ws;
     }

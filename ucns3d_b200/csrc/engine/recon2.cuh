@@ -1008,7 +1008,7 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
 }
 
 // Face-point gradients of T, u, v, w for the viscous flux, one thread per
-// (owned interior face, point): SOLUTIONTRIAV2 (reconstruct_p.f90:2358) on
+// (owned face, point): SOLUTIONTRIAV2 (reconstruct_p.f90:2358) on
 // both sides of the face at the paired points, and their average, the only
 // form CALCULATE_FLUXESHI_DIFFUSIVE uses (flux_p.f90:1614-1779), written
 // once per face point to p.fgrad [nown][QS][12] (half the bytes of one
@@ -1046,12 +1046,15 @@ __global__ void k_visc_facegrad(Problem p) {
   const int64_t c = code >> 3;
   const int f = code & 7;
   const int64_t nb = p.neigh[c * MF + f];
-  if (nb < 0 || q >= face_nq(p, p.ftype[c * MF + f])) return;
-  const int nf = p.nface[c * MF + f];
-  const int qq = p.qperm[(c * MF + f) * QS + q];
+  if (q >= face_nq(p, p.ftype[c * MF + f])) return;
   double gl[12], gr[12];
   visc_point_grad<P, T>(p, c, f, q, QS, gl);
-  visc_point_grad<P, T>(p, nb, nf, qq, QS, gr);
+  if (nb >= 0) {
+    visc_point_grad<P, T>(p, nb, p.nface[c * MF + f], p.qperm[(c * MF + f) * QS + q], QS, gr);
+  } else {  // physical boundary: the ghost side takes the cell's own gradient
+#pragma unroll
+    for (int k = 0; k < 12; ++k) gr[k] = gl[k];
+  }
   double2* o = (double2*)(p.fgrad + (i * QS + q) * 12);
 #pragma unroll
   for (int k = 0; k < 6; ++k)

@@ -252,7 +252,7 @@ __global__ void k_static_flux(Problem p, ucg_geometry g, const double* __restric
     if (NS && nb >= 0) {
       double fv[NV];
       viscous_flux(p, rt, g.dih[c * MF + f], cl, cr, scratch + c * per + MF * NV + f * 12,
-                   scratch + nb * per + MF * NV + nf * 12, fv);
+                   scratch + nb * per + MF * NV + nf * 12, fv, p.lamx);
 #pragma unroll
       for (int v = 0; v < NV; ++v) gvis[v] = fv[v] * ws;
     }
@@ -304,6 +304,7 @@ extern "C" int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geomet
   p.tri_w[0] = cfg->tri_w[0];
   for (int v = 0; v < NV; ++v) p.bc_state[v] = cfg->bc_state[v];
   p.boundtype = cfg->boundtype;
+  p.governing = cfg->governing;
   cudaStream_t s = (cudaStream_t)stream;
   const unsigned b1 = (unsigned)((n + 127) / 128), b2 = (unsigned)((n * 8 + 255) / 256);
   if (ns) {
