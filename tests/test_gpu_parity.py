@@ -44,8 +44,8 @@ FARFIELD = ("muscl_farfield_hex", "weno3_farfield_tet")
 # Navier-Stokes on the bump channel: no-slip walls, inflow, outflow and
 # symmetry faces (the bounded viscous fluxes of CALCULATE_BOUNDED_VISCOUS)
 SMALL["muscl_ns_bump"] = (lambda: Mesh.bump_channel(24, 10, 2, seed=2), SCHEME_MUSCL, 1, 0, NAVIER_STOKES)
-SMALL["weno3_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 4, seed=2), SCHEME_WENO, 2, 0, NAVIER_STOKES)
-SMALL["cweno4_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 4, seed=2), SCHEME_WENO, 3, 5, NAVIER_STOKES)
+SMALL["weno3_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 8, seed=2), SCHEME_WENO, 2, 0, NAVIER_STOKES)
+SMALL["cweno4_ns_bump"] = (lambda: Mesh.bump_channel(16, 8, 8, seed=2), SCHEME_WENO, 3, 5, NAVIER_STOKES)
 BUMPLIKE = ("muscl_bump", "weno3_channel", "muscl_bump_bt0", "weno5_channel", "muscl_ns_bump", "weno3_ns_bump",
             "cweno4_ns_bump")
 
