@@ -280,11 +280,18 @@ __global__ void __launch_bounds__(128) k_lsq_tma(Problem p, const double* __rest
 #ifndef UCG_WV_FALL_D
 #define UCG_WV_FALL_D 1
 #endif
+#ifndef UCG_WV_CHAR_F
+#define UCG_WV_CHAR_F 5
+#endif
+#ifndef UCG_WV_CHAR_D
+#define UCG_WV_CHAR_D 3
+#endif
 template <typename T>
 struct WVars {
   static constexpr int is = sizeof(T) == 4 ? UCG_WV_IS_F : UCG_WV_IS_D;
   static constexpr int face = sizeof(T) == 4 ? UCG_WV_FACE_F : UCG_WV_FACE_D;
   static constexpr int fall = sizeof(T) == 4 ? UCG_WV_FALL_F : UCG_WV_FALL_D;
+  static constexpr int chr = sizeof(T) == 4 ? UCG_WV_CHAR_F : UCG_WV_CHAR_D;
 };
 
 // is[k] += sum_d g[d][k] * sum_{e>=d} P_de g[e][k] over d, e < nd <= NMAX.
@@ -441,6 +448,13 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
   constexpr int VEC = Vec<T>::N;
   constexpr int L2 = ID < 9 ? ID : 9;  // CWENO lower order: IDEGFREE2 3 or 9 (grid_p.f90:6145-6160)
   constexpr int VI = WVars<T>::is, VH = WVars<T>::face, VF = WVars<T>::fall;
+  // variables per pass of the characteristic face polynomial (its 5x5 FP64
+  // combination matrices beside the polynomial).  Every pass reads all the
+  // stencil polynomials again for each face, so fewer variables per pass
+  // remove the spills (FP32: 978 bytes at 5, 16 at 2, none at 1) but cost
+  // more: 64^3 WENO5 reconstruction 17.2 ms at 5, 21.1 at 3, 25.3 at 2,
+  // 36.8 at 1 (FP32); FP64 52.6 ms at 3, 61.6 at 2, 78.5 at 1.
+  constexpr int VC = WVars<T>::chr;
   constexpr int BT = CH ? 64 : 128;    // threads per block
   __shared__ double s_w[7 * NV * BT];  // per thread, [ll][v]: indicators, then weights
   __shared__ double s_e[CH ? 50 * BT : 1];  // per thread: left then right eigenvectors (characteristic form)
@@ -780,14 +794,14 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
         }
       }
       weights();
-      // the face's polynomial in conserved variables, VH at a time
+      // the face's polynomial in conserved variables, VC at a time
       const int nq = face_nq(p, p.ftype[c * MF + f]);
 #pragma unroll 1
-      for (int v0 = 0; v0 < NV; v0 += VH) {
-        T gh[ID][VH];
-        double f0[VH];
+      for (int v0 = 0; v0 < NV; v0 += VC) {
+        T gh[ID][VC];
+        double f0[VC];
 #pragma unroll
-        for (int k = 0; k < VH; ++k) {
+        for (int k = 0; k < VC; ++k) {
           f0[k] = 0.0;
 #pragma unroll
           for (int d = 0; d < ID; ++d) gh[d][k] = T(0);
@@ -797,9 +811,9 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
           const int nd = cw && ll > 0 ? ID2 : ID;
           T g3[L2][NV];
           if (ll == 0) lower_sum(g3);
-          double M[VH][NV];
+          double M[VC][NV];
 #pragma unroll
-          for (int k = 0; k < VH; ++k)
+          for (int k = 0; k < VC; ++k)
 #pragma unroll
             for (int u = 0; u < NV; ++u) {
               double a = 0.0;
@@ -810,7 +824,7 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
               M[k][u] = a;
             }
 #pragma unroll
-          for (int k = 0; k < VH; ++k)
+          for (int k = 0; k < VC; ++k)
 #pragma unroll
             for (int u = 0; u < NV; ++u) f0[k] += M[k][u] * u0[u];
 #pragma unroll
@@ -820,25 +834,25 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
 #pragma unroll
               for (int u = 0; u < NV; ++u) gu[u] = Gp(ll, d, u, g3);
 #pragma unroll
-              for (int k = 0; k < VH; ++k)
+              for (int k = 0; k < VC; ++k)
 #pragma unroll
                 for (int u = 0; u < NV; ++u) gh[d][k] += T(M[k][u]) * gu[u];
             }
         }
-        T cb[VH];
+        T cb[VC];
         mean_term(gh, cb);
         for (int q = 0; q < QS; ++q) {
           T* o = out + (f * QS + q) * NV;
           if (q >= nq) {
 #pragma unroll
-            for (int k = 0; k < VH; ++k)
+            for (int k = 0; k < VC; ++k)
               if (v0 + k < NV) o[v0 + k] = T(0);
             continue;
           }
           T m[ID];
           mono(f, q, m);
 #pragma unroll
-          for (int k = 0; k < VH; ++k) {
+          for (int k = 0; k < VC; ++k) {
             T rsum = T(0);
 #pragma unroll
             for (int d = 0; d < ID; ++d) rsum += m[d] * gh[d][k];
