@@ -291,12 +291,13 @@ def test_reductions_match_oracle():
         assert abs(a - b) <= 1e-13 * abs(b)
 
 
-@pytest.mark.parametrize("name", ["weno5_hex", "weno3_tet", "muscl_ns_hex", "cweno4_tet"])
+@pytest.mark.parametrize("name", ["weno5_hex", "weno3_tet", "muscl_ns_hex", "cweno4_tet", "cweno4_ns_mixed",
+                                  "weno3_ns_hex", "weno3_ns_bump"])
 def test_mixed_precision_close_to_fp64(name):
     m, cfg64, U = _setup(name, N.UCG_FP64)
     _, cfg32, _ = _setup(name, N.UCG_MIXED)
-    cfg32 = make_config(m, governing=cfg64.governing, precision=N.UCG_MIXED, reynolds=1600.0, pres=cfg64.pres,
-                        prandtl=0.71)
+    cfg32 = N.UcgConfig.from_buffer_copy(cfg64)
+    cfg32.precision = N.UCG_MIXED
     a, b = Engine(m, cfg64), Engine(m, cfg32)
     a.set_state(U)
     b.set_state(U)

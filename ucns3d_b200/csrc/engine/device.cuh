@@ -69,7 +69,7 @@ struct Problem {
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w (MUSCL IORDER 1)
   double* fgrad;            // [nown][QS][4][3] face-point average of both sides' gradients of T,u,v,w (WENO)
-  double* gv;               // [n][ideg][4]  viscous LSQ coefficients
+  void* gv;                 // [n][ideg][4]  viscous LSQ coefficients, in the table precision
   double* prim;             // [n][4] T, u, v, w of each cell (viscous LSQ, formed once per stage)
   double* upad;             // [n][6] conserved state in 48-byte records (k_lsq gathers, formed once per stage)
   double* rhs;              // [n][NV] residual output (residual-only mode)
@@ -143,11 +143,11 @@ __device__ __forceinline__ void monomials(R x, R y, R z, R* m) {
       for (int b = 0; b <= n - c; ++b) m[d++] = px[n - c - b] * py[b] * pz[c];
 }
 
-// first derivatives d/dx, d/dy, d/dz of the monomials (DFX/DFY/DFZ)
-template <int P>
-__device__ __forceinline__ void dmonomials(double x, double y, double z, double* dx, double* dy, double* dz) {
-  double px[P + 1], py[P + 1], pz[P + 1];
-  px[0] = py[0] = pz[0] = 1.0;
+// first derivatives d/dx, d/dy, d/dz of the monomials (DFX/DFY/DFZ), in R
+template <int P, typename R = double>
+__device__ __forceinline__ void dmonomials(R x, R y, R z, R* dx, R* dy, R* dz) {
+  R px[P + 1], py[P + 1], pz[P + 1];
+  px[0] = py[0] = pz[0] = R(1);
 #pragma unroll
   for (int k = 1; k <= P; ++k) {
     px[k] = px[k - 1] * x;
@@ -162,9 +162,9 @@ __device__ __forceinline__ void dmonomials(double x, double y, double z, double*
 #pragma unroll
       for (int b = 0; b <= n - c; ++b) {
         int a = n - c - b;
-        dx[d] = a ? a * px[a - 1] * py[b] * pz[c] : 0.0;
-        dy[d] = b ? b * px[a] * py[b - 1] * pz[c] : 0.0;
-        dz[d] = c ? c * px[a] * py[b] * pz[c - 1] : 0.0;
+        dx[d] = a ? R(a) * px[a - 1] * py[b] * pz[c] : R(0);
+        dy[d] = b ? R(b) * px[a] * py[b - 1] * pz[c] : R(0);
+        dz[d] = c ? R(c) * px[a] * py[b] * pz[c - 1] : R(0);
         ++d;
       }
 }

@@ -130,7 +130,7 @@ Problem make_problem(ucg_engine* e) {
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.fgrad = (double*)e->fgrad.p;
-  p.gv = (double*)e->gv.p;
+  p.gv = e->gv.p;
   p.prim = (double*)e->prim.p;
   p.upad = (double*)e->upad.p;
   p.rhs = (double*)e->rhs.p;
@@ -473,7 +473,7 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
     if (c.scheme == 2 && c.iorder == 1) {
       rc = rc ? rc : alloc(e, e->ulv, (size_t)n * MF * e->QS * 12 * 8);
     } else {
-      rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * 8);
+      rc = rc ? rc : alloc(e, e->gv, (size_t)n * c.ideg * 4 * T);
       rc = rc ? rc : alloc(e, e->prim, (size_t)n * 4 * 8);
     }
   }

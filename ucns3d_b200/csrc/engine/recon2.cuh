@@ -977,10 +977,14 @@ __global__ void k_visc_prim(Problem p, const double* __restrict__ U) {
   o[1] = make_double2(pm[2], pm[3]);
 }
 
+// Accumulated in the table precision T: FP64 in the FP64 form; in the mixed
+// form FP32 on the differences of (T, u, v, w) from the cell's own, like
+// the stencil least squares of the conserved variables (all four variables
+// in one pass there).
 template <int P, typename T>
 __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
-  constexpr int VP = ID * 4 <= 80 ? 4 : 2;  // variables per pass
+  constexpr int VP = sizeof(T) == 4 || ID * 4 <= 80 ? 4 : 2;  // variables per pass
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
   const int IM = p.imax, W = IM + 1;
@@ -991,33 +995,40 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
   const int lane = (int)(c & 31);
   const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
   const T* M = (const T*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  T* gv = (T*)p.gv;
 #pragma unroll 1
   for (int v0 = 0; v0 < 4; v0 += VP) {
-    double acc[ID][VP];
+    T acc[ID][VP];
 #pragma unroll
     for (int d = 0; d < ID; ++d)
 #pragma unroll
-      for (int j = 0; j < VP; ++j) acc[d][j] = 0.0;
+      for (int j = 0; j < VP; ++j) acc[d][j] = T(0);
     for (int k = 0; k < IM; ++k) {
       const double2* q = (const double2*)(p.prim + (int64_t)st[(k + 1) * 32] * 4);
       const double2 qa = q[0], qb = q[1];
       const double sy[4] = {qa.x, qa.y, qb.x, qb.y};
-      double ds[VP];
+      T ds[VP];
 #pragma unroll
-      for (int j = 0; j < VP; ++j) ds[j] = sy[v0 + j] - s0[v0 + j];
+      for (int j = 0; j < VP; ++j) ds[j] = T(sy[v0 + j] - s0[v0 + j]);
 #pragma unroll
       for (int d = 0; d < ID; ++d) {
-        const double m = (double)M[(k * ID + d) * 32];
+        const T m = M[(k * ID + d) * 32];
 #pragma unroll
         for (int j = 0; j < VP; ++j) acc[d][j] += m * ds[j];
       }
     }
-    // 16-byte stores of variable pairs (VP is even; rows are 32-byte aligned)
+    // 16-byte stores: a row's four FP32 values, or FP64 pairs (VP even;
+    // rows are 16- and 32-byte aligned)
 #pragma unroll
-    for (int d = 0; d < ID; ++d)
+    for (int d = 0; d < ID; ++d) {
+      if constexpr (sizeof(T) == 4) {
+        *(float4*)(gv + (c * ID + d) * 4) = make_float4(acc[d][0], acc[d][1], acc[d][2], acc[d][3]);
+      } else {
 #pragma unroll
-      for (int j = 0; j < VP; j += 2)
-        *(double2*)(p.gv + (c * ID + d) * 4 + v0 + j) = make_double2(acc[d][j], acc[d][j + 1]);
+        for (int j = 0; j < VP; j += 2)
+          *(double2*)(gv + (c * ID + d) * 4 + v0 + j) = make_double2(acc[d][j], acc[d][j + 1]);
+      }
+    }
   }
 }
 
@@ -1027,25 +1038,29 @@ __global__ void __launch_bounds__(128) k_visc_lsq(Problem p, const double* __res
 // form CALCULATE_FLUXESHI_DIFFUSIVE uses (flux_p.f90:1614-1779), written
 // once per face point to p.fgrad [nown][QS][12] (half the bytes of one
 // record per cell face and point, read back once instead of twice).
+// evaluated in T (FP32 in the mixed form, from the FP32 coefficients and
+// reference-frame points)
 template <int P, typename T>
-__device__ __forceinline__ void visc_point_grad(const Problem& p, int64_t c, int f, int q, int QS, double* out) {
+__device__ __forceinline__ void visc_point_grad(const Problem& p, int64_t c, int f, int q, int QS, T* out) {
   constexpr int ID = Deg<P>::ideg;
   const T* xi = (const T*)p.qpts + ((c >> 5) * MF * QS * 3 + (f * QS + q) * 3) * 32 + (c & 31);
-  double dx[ID], dy[ID], dz[ID];
-  dmonomials<P>((double)xi[0], (double)xi[32], (double)xi[64], dx, dy, dz);
+  T dx[ID], dy[ID], dz[ID];
+  dmonomials<P, T>(xi[0], xi[32], xi[64], dx, dy, dz);
   const double* J = p.jinv + c * 9;
+  const T* gv = (const T*)p.gv + c * ID * 4;
 #pragma unroll
   for (int var = 0; var < 4; ++var) {
-    double gl[3] = {0.0, 0.0, 0.0};
+    T gl[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int d = 0; d < ID; ++d) {
-      double g = p.gv[(c * ID + d) * 4 + var];
+      const T g = gv[d * 4 + var];
       gl[0] += g * dx[d];
       gl[1] += g * dy[d];
       gl[2] += g * dz[d];
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) out[var * 3 + k] = J[0 * 3 + k] * gl[0] + J[1 * 3 + k] * gl[1] + J[2 * 3 + k] * gl[2];
+    for (int k = 0; k < 3; ++k)
+      out[var * 3 + k] = T(J[0 * 3 + k]) * gl[0] + T(J[1 * 3 + k]) * gl[1] + T(J[2 * 3 + k]) * gl[2];
   }
 }
 
@@ -1061,7 +1076,7 @@ __global__ void k_visc_facegrad(Problem p) {
   const int f = code & 7;
   const int64_t nb = p.neigh[c * MF + f];
   if (q >= face_nq(p, p.ftype[c * MF + f])) return;
-  double gl[12], gr[12];
+  T gl[12], gr[12];
   visc_point_grad<P, T>(p, c, f, q, QS, gl);
   if (nb >= 0) {
     visc_point_grad<P, T>(p, nb, p.nface[c * MF + f], p.qperm[(c * MF + f) * QS + q], QS, gr);
@@ -1072,7 +1087,7 @@ __global__ void k_visc_facegrad(Problem p) {
   double2* o = (double2*)(p.fgrad + (i * QS + q) * 12);
 #pragma unroll
   for (int k = 0; k < 6; ++k)
-    o[k] = make_double2((gl[2 * k] + gr[2 * k]) / 2.0, (gl[2 * k + 1] + gr[2 * k + 1]) / 2.0);
+    o[k] = make_double2((double)((gl[2 * k] + gr[2 * k]) / T(2)), (double)((gl[2 * k + 1] + gr[2 * k + 1]) / T(2)));
 }
 
 // Characteristic-variable post-processing (k_wpost<P, T, true>), 64 threads
