@@ -54,6 +54,18 @@ ucp_mesh* ucp_bump_channel(int32_t nx, int32_t ny, int32_t nlayers, double bump,
  * with quadrilateral top and bottom so that every face is conforming.     */
 ucp_mesh* ucp_mixed_box(int32_t n, double L, uint64_t seed);
 
+/* UCNS3D's ASCII grid files <prefix>GRID.vrt, GRID.cel, GRID.bnd (the
+ * reader of OPEN_ARBITRARY / FIND_SHAPE / READ_BOUND, src/io.f90:4157-4304,
+ * src/grid_p.f90:1652-1743, src/bc_p.f90:36-130): hexahedra, tetrahedra,
+ * pyramids and prisms in the 8-node encoding with repeated nodes, boundary
+ * faces with their codes.  Periodic faces (codes 5, 50) are refused.  The
+ * mesh is then prepared like any other; every boundary face must appear in
+ * GRID.bnd.  ucp_write_grid writes a prepared, non-periodic mesh in the same
+ * format (coordinates with 17 significant digits, so a read-back prepares
+ * to the same tables).                                                    */
+ucp_mesh* ucp_read_grid(const char* prefix);
+int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix);
+
 typedef struct ucp_scheme {
   int32_t scheme;     /* 2 MUSCL, 3 WENO                                     */
   int32_t iorder;     /* 1..4                                                */

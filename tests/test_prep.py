@@ -135,3 +135,63 @@ def test_renumbered_mesh_oracle_residual_is_permuted():
     Rb = Oracle(m, cfg).residual(U)
     Rs = Oracle(ms, cfg).residual(U[order])
     assert np.array_equal(ms.to_base(Rs), Rb)
+
+
+@pytest.mark.parametrize("kind", ["bump", "tet_box"])
+def test_grid_files_round_trip(kind, tmp_path):
+    """UCNS3D's GRID.vrt/cel/bnd: a mesh written and read back prepares to
+    the same geometry, boundary codes and reconstruction tables, bit for bit
+    (coordinates are written with 17 significant digits)."""
+    if kind == "bump":
+        m = Mesh.bump_channel(16, 8, 4, seed=3).prepare(SCHEME_WENO, 2)
+    else:
+        m = Mesh.box_tet(4, 4, 4, periodic=(0, 0, 0), bc=(1, 2, 3, 3, 4, 6), seed=7).prepare(SCHEME_WENO, 2)
+    prefix = str(tmp_path) + "/"
+    m.write_grid(prefix)
+    r = Mesh.read_grid(prefix).prepare(SCHEME_WENO, 2)
+    ga, gb = m.geometry(), r.geometry()
+    for k in ("nfaces", "face_type", "neigh", "neigh_face", "bc", "qperm", "face_angle", "face_area", "dih",
+              "qpoints", "volume", "minedge", "invccjac", "basis_mean", "admis", "full"):
+        assert np.array_equal(ga[k], gb[k]), k
+    ra, rb = m.recon(), r.recon()
+    assert np.array_equal(ra["stencil"], rb["stencil"])
+    ia = ra["invmat"][ra["table_id"]] if ra["table_id"] is not None else ra["invmat"]
+    ib = rb["invmat"][rb["table_id"]] if rb["table_id"] is not None else rb["invmat"]
+    assert np.array_equal(ia, ib)
+    lines = open(prefix + "GRID.bnd").read().split("\n")
+    assert len([x for x in lines if x]) == int(((ga["neigh"] < 0) & (np.arange(6)[None, :] < ga["nfaces"][:, None])).sum())
+
+
+def test_grid_reader_shapes_and_errors(tmp_path):
+    """The 8-node encoding of the four cell shapes, told apart by repeated
+    nodes as FIND_SHAPE does: a pyramid on a hexahedron's top with a
+    tetrahedron and a prism beside it is read with the right face counts;
+    a boundary face missing from GRID.bnd, and periodic codes, are refused."""
+    d = str(tmp_path) + "/"
+    # unit cube 1-8, apex 9 above it, 10 beside, 11-12 for a prism
+    pts = {1: (0, 0, 0), 2: (1, 0, 0), 3: (1, 1, 0), 4: (0, 1, 0), 5: (0, 0, 1), 6: (1, 0, 1), 7: (1, 1, 1),
+           8: (0, 1, 1), 9: (0.5, 0.5, 1.6), 10: (0.5, -0.8, 0.5)}
+    with open(d + "GRID.vrt", "w") as f:
+        for k, p in pts.items():
+            f.write(f"{k} {p[0]} {p[1]} {p[2]}\n")
+    with open(d + "GRID.cel", "w") as f:
+        f.write("1 1 2 3 4 5 6 7 8\n")        # hexahedron
+        f.write("2 5 6 7 8 9 9 9 9\n")        # pyramid on its top
+        f.write("3 1 2 6 6 10 10 10 10\n")    # tetrahedron on the face 1-2-6
+    # a boundary file that misses most boundary faces: read, refused at prepare
+    with open(d + "GRID.bnd", "w") as f:
+        f.write("1 1 4 3 2 4\n")
+    m = Mesh.read_grid(d)
+    assert m.ncells == 3
+    with pytest.raises(RuntimeError, match="GRID.bnd"):
+        m.prepare(SCHEME_MUSCL, 1)
+    with open(d + "GRID.bnd", "w") as f:
+        f.write("1 1 4 3 2 5\n")
+    with pytest.raises(RuntimeError, match="periodic"):
+        Mesh.read_grid(d)
+    with open(d + "GRID.bnd", "w") as f:
+        f.write("1 1 4 3 2 4\n")
+    with open(d + "GRID.cel", "a") as f:
+        f.write("4 1 2 3 4 5 5 6 6\n")        # no shape of FIND_SHAPE
+    with pytest.raises(RuntimeError, match="none of"):
+        Mesh.read_grid(d)

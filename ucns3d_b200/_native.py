@@ -105,6 +105,10 @@ def prep() -> C.CDLL:
                                          C.c_double, C.c_uint64]
         lib.ucp_mixed_box.restype = vp
         lib.ucp_mixed_box.argtypes = [C.c_int32, C.c_double, C.c_uint64]
+        lib.ucp_read_grid.restype = vp
+        lib.ucp_read_grid.argtypes = [C.c_char_p]
+        lib.ucp_write_grid.restype = C.c_int32
+        lib.ucp_write_grid.argtypes = [vp, C.c_char_p]
         lib.ucp_prepare.restype = C.c_int32
         lib.ucp_prepare.argtypes = [vp, C.POINTER(UcpScheme)]
         lib.ucp_ncells.restype = C.c_int64

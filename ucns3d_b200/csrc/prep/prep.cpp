@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <random>
 #include <string>
@@ -336,6 +337,10 @@ struct ucp_mesh {
   std::vector<int32_t> stencil, table_id;
   int64_t ntab = 0;
   std::vector<double> invmat, invmat2, indicator, indicator2;
+  // boundary codes of a mesh read from GRID files, by the sorted global
+  // node ids of the face (the last entry -1 for a triangle)
+  bool has_bnd = false;
+  std::map<std::array<int64_t, 4>, int32_t> bnd_code;
 };
 
 namespace {
@@ -418,6 +423,15 @@ int bc_of_boundary_face(const ucp_mesh& m, V3 fc, V3 n) {
   int side = ax * 2 + (a[ax] > 0 ? 1 : 0);
   (void)fc;
   return m.box_bc[side];
+}
+
+// sorted global node ids of face f of cell c (-1 fills a triangle's 4th slot)
+std::array<int64_t, 4> face_key(const ucp_mesh& m, int64_t c, int f) {
+  std::array<int64_t, 4> k = {-1, -1, -1, -1};
+  const int nv = m.face_type[c * 6 + f] == 5 ? 4 : 3;
+  for (int i = 0; i < nv; ++i) k[i] = m.gnode[c * 8 + m.fnode[c * 24 + f * 4 + i]];
+  std::sort(k.begin(), k.begin() + nv);
+  return k;
 }
 
 bool build_connectivity(ucp_mesh& m) {
@@ -600,6 +614,18 @@ bool build_geometry(ucp_mesh& m) {
     }
     m.minedge[c] = 3.0 * m.volume[c] / ssum;
   }
+  // codes of a mesh read from GRID files: from GRID.bnd, by face nodes
+  if (m.has_bnd)
+    for (int64_t c = 0; c < nc; ++c)
+      for (int f = 0; f < m.nfaces[c]; ++f) {
+        if (m.neigh[c * 6 + f] >= 0) continue;
+        const auto it = m.bnd_code.find(face_key(m, c, f));
+        if (it == m.bnd_code.end()) {
+          set_err("boundary face of cell " + std::to_string(c + 1) + " has no entry in GRID.bnd");
+          return false;
+        }
+        m.bc[c * 6 + f] = it->second;
+      }
   // quadrature point pairing across faces
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < nc; ++c) {
@@ -1268,6 +1294,186 @@ ucp_mesh* ucp_mixed_box(int32_t n, double L, uint64_t seed) {
         }
       }
   return m;
+}
+
+// ------------------------------------------------------------ GRID files
+// UCNS3D's ASCII grid (OPEN_ARBITRARY, io.f90:4157-4304; FIND_SHAPE,
+// grid_p.f90:1652-1743; READ_BOUND, bc_p.f90:36-130): GRID.vrt "id x y z",
+// GRID.cel "id n1 .. n8" with the shape told by repeated nodes (hexahedron:
+// all distinct; tetrahedron n3 = n4, n5 = n6 = n7 = n8; pyramid n5 = .. = n8;
+// prism n3 = n4, n7 = n8), GRID.bnd "id n1 n2 n3 n4 code" (a triangle has
+// n3 = n4).  Ids are 1-based.
+ucp_mesh* ucp_read_grid(const char* prefix) {
+  const std::string pre = prefix ? prefix : "";
+  FILE* fv = std::fopen((pre + "GRID.vrt").c_str(), "r");
+  FILE* fc = std::fopen((pre + "GRID.cel").c_str(), "r");
+  FILE* fb = std::fopen((pre + "GRID.bnd").c_str(), "r");
+  auto close_all = [&]() {
+    if (fv) std::fclose(fv);
+    if (fc) std::fclose(fc);
+    if (fb) std::fclose(fb);
+  };
+  if (!fv || !fc || !fb) {
+    close_all();
+    set_err("cannot open " + pre + "GRID.vrt, GRID.cel or GRID.bnd");
+    return nullptr;
+  }
+  std::vector<V3> node;
+  long long id;
+  double x, y, z;
+  while (std::fscanf(fv, "%lld %lf %lf %lf", &id, &x, &y, &z) == 4) {
+    if (id < 1) {
+      close_all();
+      set_err("GRID.vrt: node ids start at 1");
+      return nullptr;
+    }
+    if ((size_t)id > node.size()) node.resize(id, {std::nan(""), 0, 0});
+    node[id - 1] = {x, y, z};
+  }
+  std::vector<std::array<long long, 8>> cells;
+  std::array<long long, 8> n8;
+  while (std::fscanf(fc, "%lld %lld %lld %lld %lld %lld %lld %lld %lld", &id, &n8[0], &n8[1], &n8[2], &n8[3], &n8[4],
+                     &n8[5], &n8[6], &n8[7]) == 9)
+    cells.push_back(n8);
+  ucp_mesh* m = new_mesh((int64_t)cells.size());
+  bool ok = !cells.empty();
+  if (!ok) set_err("GRID.cel holds no cells");
+  for (int64_t c = 0; ok && c < (int64_t)cells.size(); ++c) {
+    const auto& a = cells[c];
+    int type;
+    int slot[8];
+    int nv;
+    if (a[4] != a[5] && a[5] != a[6] && a[6] != a[7] && a[2] != a[3]) {
+      type = 1, nv = 8;
+      for (int k = 0; k < 8; ++k) slot[k] = k;
+    } else if (a[2] == a[3] && a[4] == a[5] && a[5] == a[6] && a[6] == a[7]) {
+      type = 2, nv = 4;
+      slot[0] = 0, slot[1] = 1, slot[2] = 2, slot[3] = 4;
+    } else if (a[2] != a[3] && a[4] == a[5] && a[5] == a[6] && a[6] == a[7]) {
+      type = 3, nv = 5;
+      for (int k = 0; k < 5; ++k) slot[k] = k;
+    } else if (a[2] == a[3] && a[4] != a[5] && a[6] == a[7]) {
+      type = 4, nv = 6;
+      slot[0] = 0, slot[1] = 1, slot[2] = 2, slot[3] = 4, slot[4] = 5, slot[5] = 6;
+    } else {
+      set_err("GRID.cel: cell " + std::to_string(c + 1) + " is none of hexahedron, tetrahedron, pyramid, prism");
+      ok = false;
+      break;
+    }
+    int64_t ids[8];
+    V3 pts[8];
+    for (int k = 0; k < nv; ++k) {
+      const long long g = a[slot[k]];
+      if (g < 1 || (size_t)g > node.size() || std::isnan(node[g - 1].x)) {
+        set_err("GRID.cel: cell " + std::to_string(c + 1) + " names a node missing from GRID.vrt");
+        ok = false;
+        break;
+      }
+      ids[k] = g - 1;
+      pts[k] = node[g - 1];
+    }
+    if (ok) set_cell(m, c, type, ids, pts);
+  }
+  long long b[4];
+  int code;
+  while (ok && std::fscanf(fb, "%lld %lld %lld %lld %lld %d", &id, &b[0], &b[1], &b[2], &b[3], &code) == 6) {
+    if (code == 5 || code == 50) {
+      set_err("GRID.bnd: periodic faces (codes 5, 50) are not supported by this reader");
+      ok = false;
+      break;
+    }
+    std::array<int64_t, 4> k = {b[0] - 1, b[1] - 1, b[2] - 1, b[2] == b[3] ? -1 : b[3] - 1};
+    const int nv = b[2] == b[3] ? 3 : 4;
+    std::sort(k.begin(), k.begin() + nv);
+    m->bnd_code[k] = code;
+  }
+  close_all();
+  if (!ok) {
+    delete m;
+    return nullptr;
+  }
+  m->has_bnd = true;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (const V3& p : node)
+    if (!std::isnan(p.x)) {
+      lo[0] = std::min(lo[0], p.x), hi[0] = std::max(hi[0], p.x);
+      lo[1] = std::min(lo[1], p.y), hi[1] = std::max(hi[1], p.y);
+      lo[2] = std::min(lo[2], p.z), hi[2] = std::max(hi[2], p.z);
+    }
+  for (int k = 0; k < 3; ++k) {
+    m->box_lo[k] = lo[k];
+    m->box_hi[k] = hi[k];
+  }
+  return m;
+}
+
+int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix) {
+  if (!m || !m->prepared) {
+    set_err("write_grid needs a prepared mesh (its boundary faces and codes)");
+    return UCG_ESTATE;
+  }
+  if (m->per[0] || m->per[1] || m->per[2]) {
+    set_err("write_grid: periodic meshes are not written (their faces would need codes 5/50 and pairing)");
+    return UCG_EINVAL;
+  }
+  const std::string pre = prefix ? prefix : "";
+  FILE* fv = std::fopen((pre + "GRID.vrt").c_str(), "w");
+  FILE* fc = std::fopen((pre + "GRID.cel").c_str(), "w");
+  FILE* fb = std::fopen((pre + "GRID.bnd").c_str(), "w");
+  if (!fv || !fc || !fb) {
+    if (fv) std::fclose(fv);
+    if (fc) std::fclose(fc);
+    if (fb) std::fclose(fb);
+    set_err("cannot create " + pre + "GRID.vrt, GRID.cel or GRID.bnd");
+    return UCG_EINVAL;
+  }
+  // nodes by global id (each node's position as its first cell sees it)
+  int64_t nn = 0;
+  for (int64_t c = 0; c < m->nc; ++c)
+    for (int k = 0; k < topo(m->type[c]).nv; ++k) nn = std::max(nn, m->gnode[c * 8 + k] + 1);
+  std::vector<V3> pos(nn);
+  std::vector<char> seen(nn, 0);
+  for (int64_t c = 0; c < m->nc; ++c)
+    for (int k = 0; k < topo(m->type[c]).nv; ++k) {
+      const int64_t g = m->gnode[c * 8 + k];
+      if (!seen[g]) {
+        seen[g] = 1;
+        pos[g] = vtx(*m, c, k);
+      }
+    }
+  for (int64_t g = 0; g < nn; ++g)
+    if (seen[g]) std::fprintf(fv, "%lld %.17g %.17g %.17g\n", (long long)(g + 1), pos[g].x, pos[g].y, pos[g].z);
+  for (int64_t c = 0; c < m->nc; ++c) {
+    const int64_t* gn = &m->gnode[c * 8];
+    long long s[8];
+    switch (m->type[c]) {
+      case 1: for (int k = 0; k < 8; ++k) s[k] = gn[k]; break;
+      case 2: s[0] = gn[0], s[1] = gn[1], s[2] = s[3] = gn[2], s[4] = s[5] = s[6] = s[7] = gn[3]; break;
+      case 3: for (int k = 0; k < 5; ++k) s[k] = gn[k]; s[5] = s[6] = s[7] = gn[4]; break;
+      default: s[0] = gn[0], s[1] = gn[1], s[2] = s[3] = gn[2], s[4] = gn[3], s[5] = gn[4], s[6] = s[7] = gn[5];
+    }
+    std::fprintf(fc, "%lld %lld %lld %lld %lld %lld %lld %lld %lld\n", (long long)(c + 1), s[0] + 1, s[1] + 1, s[2] + 1,
+                 s[3] + 1, s[4] + 1, s[5] + 1, s[6] + 1, s[7] + 1);
+  }
+  long long ib = 0;
+  for (int64_t c = 0; c < m->nc; ++c)
+    for (int f = 0; f < m->nfaces[c]; ++f) {
+      if (m->neigh[c * 6 + f] >= 0) continue;
+      const int nv = m->face_type[c * 6 + f] == 5 ? 4 : 3;
+      long long g[4];
+      for (int k = 0; k < nv; ++k) g[k] = m->gnode[c * 8 + m->fnode[c * 24 + f * 4 + k]] + 1;
+      if (nv == 3) g[3] = g[2];
+      std::fprintf(fb, "%lld %lld %lld %lld %lld %d\n", ++ib, g[0], g[1], g[2], g[3], m->bc[c * 6 + f]);
+    }
+  const bool bad = std::ferror(fv) || std::ferror(fc) || std::ferror(fb);
+  std::fclose(fv);
+  std::fclose(fc);
+  std::fclose(fb);
+  if (bad) {
+    set_err("write error in the GRID files");
+    return UCG_EINVAL;
+  }
+  return UCG_OK;
 }
 
 int32_t ucp_prepare(ucp_mesh* m, const ucp_scheme* s) {

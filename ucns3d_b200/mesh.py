@@ -75,6 +75,18 @@ class Mesh:
         return cls(h, "bump_channel", dict(nx=nx, ny=ny, nlayers=nlayers, bump=bump, seed=seed))
 
     @classmethod
+    def read_grid(cls, prefix: str):
+        """A mesh from UCNS3D's ASCII grid files <prefix>GRID.vrt, GRID.cel
+        and GRID.bnd (non-periodic)."""
+        h = N.prep().ucp_read_grid(prefix.encode())
+        return cls(h, "grid", dict(prefix=prefix))
+
+    def write_grid(self, prefix: str):
+        """Write this prepared, non-periodic mesh as <prefix>GRID.vrt,
+        GRID.cel and GRID.bnd."""
+        _check(N.prep().ucp_write_grid(self._h, prefix.encode()), "ucp_write_grid")
+
+    @classmethod
     def mixed_box(cls, n, L=2 * np.pi, seed=1234):
         h = N.prep().ucp_mixed_box(n, L, int(seed))
         return cls(h, "mixed_box", dict(n=n, L=L, seed=seed))
