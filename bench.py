@@ -203,6 +203,15 @@ def recon_bytes_per_cell(cfg):
     return b
 
 
+def recon_kernels(cfg, wenwrt):
+    """The kernels of one reconstruction (the launch sequence of launch_weno)."""
+    if cfg.scheme == 2 and cfg.iorder == 1:
+        return "k_muscl"
+    if cfg.scheme == 3 and cfg.iorder == 4 and wenwrt == 1:
+        return "k_lsq + k_wis + k_wface + k_wpost fall-back"
+    return "k_lsq + k_wpost"
+
+
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -587,7 +596,7 @@ def main():
                      "traffic": traffic, "traffic_unit": "bytes per launch",
                      "kernel": "k_lsq (stencil least squares)",
                      "bytes_per_cell": bpc, "kernel_ms": lsq_ms,
-                     "reconstruction": {"kernels": "k_lsq + k_wpost", "bytes_per_cell": rbpc,
+                     "reconstruction": {"kernels": recon_kernels(cfg32, args.wenwrt), "bytes_per_cell": rbpc,
                                         "ms": r32["kern"]["recon"],
                                         "frac": rbpc * ncells / (r32["kern"]["recon"] / 1000.0) / 1e9 / peak}},
         "kernel_ms": r32["kern"],

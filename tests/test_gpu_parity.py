@@ -390,6 +390,7 @@ def test_indicator_kernel_is_bitwise_equal(name, precision, monkeypatch):
     same order: residuals equal bit for bit (the channel adds cells on the
     MUSCL fall-back, which k_wis skips)."""
     m, cfg, U = _setup(name, precision)
+    monkeypatch.setenv("UCG_WENO_FACE", "0")
     out = []
     for flag in ("1", "0"):
         monkeypatch.setenv("UCG_WENO_IS", flag)
@@ -399,3 +400,34 @@ def test_indicator_kernel_is_bitwise_equal(name, precision, monkeypatch):
         e.check_health()
         e.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("name", ["weno5_hex", "weno5_channel", "weno5_shock"])
+@pytest.mark.parametrize("precision", [N.UCG_FP64, N.UCG_MIXED])
+def test_variable_warp_face_values_match_lane_per_cell(name, precision, monkeypatch):
+    """WENO5: the weights, combined polynomial and face values formed one
+    warp per conserved variable (k_wface, then the MUSCL fall-back of the
+    cells it flags) against one lane per cell (k_wpost, UCG_WENO_FACE=0).
+    Both take the same operations in the same order; only the compiler's
+    multiply-add contraction may differ, so the residuals agree to the
+    rounding of the reconstruction's type: 1e-12 of the flux scale in FP64,
+    2e-6 in the mixed form.  The shock case (a Sod-like jump across the
+    box) sends the cells beside the jump to the fall-back through CHECKSOL."""
+    m, cfg, U = _setup("weno5_hex" if name == "weno5_shock" else name, precision)
+    if name == "weno5_shock":
+        x = m.centres()[:, 0]
+        left = x < 0.5 * (x.min() + x.max())
+        rho, pr = np.where(left, 1.0, 0.125), np.where(left, 1.0, 0.1)
+        U = np.zeros_like(U)
+        U[:, 0], U[:, 4] = rho, pr / 0.4
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("UCG_WENO_FACE", flag)
+        e = Engine(m, cfg)
+        e.set_state(U)
+        out.append(e.residual())
+        e.check_health()
+        e.close()
+    err = (np.abs(out[0] - out[1]) / _flux_scale(None, m, U)).max()
+    print(f"{name}: k_wface vs k_wpost rel err {err:.3e}, bitwise {np.array_equal(out[0], out[1])}")
+    assert err < (1e-12 if precision == N.UCG_FP64 else 2e-6)

@@ -66,6 +66,7 @@ struct Problem {
   void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the stencils
   double* qbuf;             // characteristic WENO: G_l^T S G_l per stencil, 15 values, interleaved
   double* isb;              // conserved WENO: smoothness indicators [A][NV] per cell, interleaved (k_wis)
+  int8_t* wflag;            // WENO5: cells k_wface leaves to the MUSCL fall-back [n]
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w (MUSCL IORDER 1)
   double* fgrad;            // [nown][QS][4][3] face-point average of both sides' gradients of T,u,v,w (WENO)

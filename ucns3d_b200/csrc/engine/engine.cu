@@ -127,6 +127,7 @@ Problem make_problem(ucg_engine* e) {
   p.gbuf = e->gbuf.p;
   p.qbuf = (double*)e->qbuf.p;
   p.isb = (double*)e->isb.p;
+  p.wflag = (int8_t*)e->wflag.p;
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.fgrad = (double*)e->fgrad.p;
@@ -466,6 +467,9 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
   if (c.scheme == 3 && c.wenwrt == 1 && c.iorder == 4) {  // smoothness indicators of every stencil (k_wis)
     const char* wis = std::getenv("UCG_WENO_IS");
     if (!(wis && wis[0] == '0')) rc = rc ? rc : alloc(e, e->isb, (size_t)ngrp * 32 * c.admis_max * NV * 8);
+    // face values one warp per variable (k_wface), unless UCG_WENO_FACE=0
+    const char* wf = std::getenv("UCG_WENO_FACE");
+    if (!(wis && wis[0] == '0') && !(wf && wf[0] == '0')) rc = rc ? rc : alloc(e, e->wflag, (size_t)n);
   }
   if (c.wenwrt == 2)  // characteristic WENO: G^T S G of every stencil (15 values)
     rc = rc ? rc : alloc(e, e->qbuf, (size_t)ngrp * 32 * c.admis_max * 15 * 8);
@@ -502,7 +506,7 @@ void ucg_destroy(ucg_engine* e) {
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
-                   &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb};
+                   &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb, &e->wflag};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);

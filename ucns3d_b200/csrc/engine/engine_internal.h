@@ -52,7 +52,7 @@ struct ucg_engine {
   // tables
   DevBuf sten, invmat, ind;
   // scratch and state
-  DevBuf gbuf, isb, dul, ulv, fgrad, gv, prim, upad, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux, qbuf;
+  DevBuf gbuf, isb, wflag, dul, ulv, fgrad, gv, prim, upad, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux, qbuf;
   int64_t nown = 0;
   int64_t nown_plain = 0;  // owned faces [0, nown_plain): interior and mirror; the rest other boundaries
   cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs

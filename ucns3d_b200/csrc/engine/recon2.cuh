@@ -433,6 +433,167 @@ __global__ void __launch_bounds__(224) k_wis(Problem p) {
   }
 }
 
+// k_wface (conserved-variable WENO, IORDER 4, indicators from k_wis): the
+// nonlinear weights, the combined polynomial and its face values, one block
+// per 32-cell group with one warp per conserved variable (lane i: cell i of
+// the group).  A thread holds one variable's combined polynomial (ID
+// coefficients) instead of all five, so the block runs at several times
+// k_wpost's occupancy.  The group's face points are staged in shared memory
+// once (the five warps evaluate at the same points); the values of one face
+// go through shared memory, [cell][point][variable] with an odd row stride
+// (no bank conflicts), from where the block tests CHECKSOL (0.85) and stores
+// them as one contiguous run per cell.  Cells that fail CHECKSOL, or are not FULL, are marked in
+// p.wflag for k_wpost<..., FB> (the MUSCL fall-back).  Weights, combination
+// and face values take k_wpost's operations in k_wpost's order.
+template <int P, typename T>
+__global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __restrict__ U) {
+  constexpr int ID = Deg<P>::ideg;
+  constexpr int L2 = ID < 9 ? ID : 9;
+  constexpr int MA = 7;  // stencils per cell at most
+  extern __shared__ __align__(16) unsigned char wf_smem[];
+  __shared__ int s_flag[32];
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int FQ = MF * QS;
+  const int RS = (QS * NV) | 1;  // row stride of a cell in s_o
+  T* s_x = (T*)wf_smem;          // [FQ * 3][32]: the group's face points, as in p.qpts
+  T* s_o = s_x + FQ * 3 * 32;    // [32][RS]: the values of one face
+  const int tid = threadIdx.x, lane = tid & 31, v = tid >> 5;
+  const int64_t grp = blockIdx.x, c = grp * 32 + lane;
+  {
+    const T* xg = (const T*)p.qpts + grp * (int64_t)FQ * 3 * 32;
+    for (int i = tid; i < FQ * 3 * 32; i += 32 * NV) s_x[i] = __ldcs(xg + i);
+  }
+  const bool cell = c < p.n;
+  const bool live = cell && p.full[c];
+  const int A = p.admis_max;
+  const int adm = live ? p.admis[c] : 0;
+  const bool cw = p.ees == 5;
+  const int ID2 = p.ideg2;
+  const double lc1 = 1.0 - 1.0 / p.lwci;
+  const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
+  if (tid < 32) s_flag[tid] = live ? 0 : 1;
+  // ---- weights of variable v (WENOWEIGHTS, FP64)
+  double w[MA];
+  {
+    const double* is = p.isb + grp * (int64_t)A * NV * 32 + lane + v * 32;
+    const double lam0 = cw ? lc1 : p.lwci, lamk = cw ? lk : 1.0;
+    double tau = 0.0, sum = 0.0;
+    if (cw && p.wenoz) {
+#pragma unroll
+      for (int l = 0; l < MA; ++l)
+        if (l < adm) tau += fabs(is[0] - is[(int64_t)l * NV * 32]);
+      tau = tau / (adm - 1);
+    }
+#pragma unroll
+    for (int l = 0; l < MA; ++l) {
+      w[l] = 0.0;
+      if (l < adm) {
+        const double e = p.weno_eps + is[(int64_t)l * NV * 32];
+        const double lam = l == 0 ? lam0 : lamk;
+        double wt;
+        if (cw && p.wenoz) {
+          double q = tau / e;
+          q = q * q;
+          wt = lam * (1.0 + q * q);
+        } else {
+          const double e2 = e * e;
+          wt = lam / (e2 * e2);
+        }
+        w[l] = wt;
+        sum += wt;
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < MA; ++l) w[l] = w[l] / sum;
+  }
+  // ---- combined polynomial of variable v (CWENO: the central stencil with
+  // the lower-order ones removed, reconstruct_p.f90:956-965)
+  const T* Gc = (const T*)p.gbuf + grp * (int64_t)(A * ID * NV) * 32 + v * 32 + lane;
+  auto G = [&](int l, int d) -> T { return Gc[(int64_t)((l * ID + d) * NV) * 32]; };
+  T gh[ID];
+#pragma unroll
+  for (int d = 0; d < ID; ++d) gh[d] = live ? G(0, d) : T(0);
+  if (live && cw) {
+    T g3[L2];
+#pragma unroll
+    for (int d = 0; d < L2; ++d) g3[d] = T(0);
+    for (int l2 = 1; l2 < adm; ++l2)
+#pragma unroll
+      for (int d = 0; d < L2; ++d)
+        if (d < ID2) g3[d] = g3[d] + T(lk) * G(l2, d);
+#pragma unroll
+    for (int d = 0; d < ID; ++d) gh[d] = T(1.0 / lc1) * (gh[d] - (d < L2 ? g3[d] : T(0)));
+  }
+  if (live) {
+    const T w0 = T(w[0]);
+#pragma unroll
+    for (int d = 0; d < ID; ++d) gh[d] = w0 * gh[d];
+    // every stencil row of the table is in the buffer (l < A), so the loads
+    // need no guard on adm and can all be in flight; rows past adm add 0 * 0
+#pragma unroll
+    for (int l = 1; l < MA; ++l)
+      if (l < A) {
+        const bool on = l < adm;
+        const T wl = on ? T(w[l]) : T(0);
+#pragma unroll
+        for (int d = 0; d < ID; ++d)
+          if (!cw || d < ID2) {
+            const T gv = G(l, d);
+            gh[d] += wl * (on ? gv : T(0));
+          }
+      }
+  }
+  T cb = T(0);
+  {
+    const T* bmv = (const T*)p.bmean + grp * (int64_t)ID * 32 + lane;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) cb += bmv[d * 32] * gh[d];
+  }
+  // ---- face values, CHECKSOL and the stores, face by face
+  __syncthreads();  // s_x
+  const T* xq = s_x + lane;
+  const int nf = cell ? p.nfaces[c] : 0;
+  double u0[NV], pm[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) u0[k] = cell ? U[c * NV + k] : 1.0;
+  cons2prim(p.gamma, u0, pm);
+  bool flag = false;
+  T* out = (T*)p.dul + grp * 32 * (int64_t)FQ * NV;
+  const int ncl = p.n - grp * 32 < 32 ? (int)(p.n - grp * 32) : 32;  // cells of this group
+  for (int f = 0; f < MF; ++f) {
+    T* so = s_o;
+    if (f) __syncthreads();  // the stores of face f - 1 have read s_o
+    const int nq = live && f < nf ? face_nq(p, p.ftype[c * MF + f]) : 0;
+    for (int q = 0; q < QS; ++q) {
+      T r = T(0);
+      if (q < nq) {
+        const T* xi = xq + (int64_t)(f * QS + q) * 3 * 32;
+        T m[ID];
+        monomials<P, T>(xi[0], xi[32], xi[64], m);
+#pragma unroll
+        for (int d = 0; d < ID; ++d) r += m[d] * gh[d];
+        r = r - cb;
+      }
+      so[lane * RS + q * NV + v] = r;
+    }
+    __syncthreads();
+    // CHECKSOL: warp v takes the points v, v + NV, ... of its lane's cell
+    for (int q = v; q < nq; q += NV) {
+      double uf[NV];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) uf[k] = u0[k] + (double)so[lane * RS + q * NV + k];
+      flag = flag || jump_bad(p.gamma, pm, uf, 0.85);
+    }
+    // the group's values of face f: one run of QS * NV per cell, warp v
+    // storing the cells v, v + NV, ...
+    for (int cl = v; cl < ncl; cl += NV)
+      for (int r = lane; r < QS * NV; r += 32) out[(int64_t)cl * FQ * NV + f * QS * NV + r] = so[cl * RS + r];
+  }
+  if (flag) atomicOr(&s_flag[lane], 1);
+  __syncthreads();
+  if (tid < ncl) p.wflag[grp * 32 + tid] = (int8_t)s_flag[tid];
+}
+
 // k_wpost: one lane per cell, no block barriers.  Indicators and weights of
 // CP_RECONSTRUCTION (src/reconstruct_p.f90:920-1250), the combined
 // polynomial, its face values and CHECKSOL; flagged cells (and every cell of
@@ -442,7 +603,9 @@ __global__ void __launch_bounds__(224) k_wis(Problem p) {
 // sum_d m_d(x) g_d - sum_d mean(m_d) g_d: the second sum is formed once per
 // polynomial instead of subtracting the basis means at every face point.
 // ISB: the indicators come from k_wis (p.isb) instead of being formed here.
-template <int P, typename T, bool CH = false, bool ISB = false>
+// FB: only the cells that k_wface marked in p.wflag, straight to the MUSCL
+// fall-back (the others return at once).
+template <int P, typename T, bool CH = false, bool ISB = false, bool FB = false>
 __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<T>::N;
@@ -564,7 +727,8 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
       for (int ll = 0; ll < adm; ++ll) sw[(ll * NV + v) * BT] = sw[(ll * NV + v) * BT] / sum;
     }
   };
-  bool fall = !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
+  if (FB && !p.wflag[c]) return;
+  bool fall = FB || !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
   if (!CH && !fall && ISB) {
     // ---- smoothness indicators from k_wis
     const double* is = p.isb + grp * (int64_t)A * NV * 32 + lane;
@@ -1146,7 +1310,19 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     // than it saves (2.1 M-cell CWENO4: 17.3 -> 19.6 ms)
     bool done = false;
     if constexpr (P == 4) {
-      if (p.isb && p.scheme == 3) {
+      if (p.wflag && p.isb && p.scheme == 3) {
+        const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+        const size_t smem = ((size_t)MF * QS * 3 + ((QS * NV) | 1)) * 32 * sizeof(T);
+        cudaFuncSetAttribute(k_wface<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_wis<P, T><<<(unsigned)((p.n + 31) / 32), 32 * p.admis_max, 0, st>>>(p);
+        k_wface<P, T><<<(unsigned)((p.n + 31) / 32), 32 * NV, smem, st>>>(p, U);
+        k_wpost<P, T, false, false, true><<<b, 128, 0, st>>>(p, U);
+        *launches += 2;
+        done = true;
+      }
+    }
+    if constexpr (P == 4) {
+      if (!done && p.isb && p.scheme == 3) {
         k_wis<P, T><<<(unsigned)((p.n + 31) / 32), 32 * p.admis_max, 0, st>>>(p);
         k_wpost<P, T, false, true><<<b, 128, 0, st>>>(p, U);
         ++*launches;
