@@ -113,6 +113,20 @@ typedef struct ucg_config {
                           caller index, so the results are bitwise those of
                           reorder 0 except for domain sums (ucg_reduce, ucg_force),
                           whose order of addition changes                         */
+  int32_t mood;        /* 1: MOOD a posteriori limiting in every RK3 stage (MOOD = 1
+                          when MOOD.DAT exists, parameters.f90:126-140;
+                          RUNGE_KUTTA3_MOOD, time_p.f90:582-880; mood.f90).  WENO /
+                          CWENO (scheme 3) and Euler only: the reference's MOOD
+                          recomputes only the convective fluxes.  With MOOD the
+                          CHECKSOL fall-back of a reconstruction runs only on the
+                          cells the last MOOD pass recomputed (RECALC, initially 0,
+                          memory.f90:1002-1010; reconstruct_p.f90:2310); the other
+                          reduced cells keep their WENO values, then CHECKSOLX.  The
+                          flags persist in the handle across stages and steps     */
+  int32_t mood_mode;   /* MOOD_MODE: 1 relaxed (bounds widened by max(var1,
+                          var2 * range)), 0 original                               */
+  double mood_var[4];  /* MOOD_VAR1, MOOD_VAR2 (first cascade, to MUSCL), MOOD_VAR3,
+                          MOOD_VAR4 (second cascade, to first order)               */
 } ucg_config;
 
 /* Per-cell geometry (IELEM(N,I) and the small parts of ILOCAL_RECON3(I),
@@ -125,9 +139,11 @@ typedef struct ucg_geometry {
   const int32_t* neigh;       /* [n][F]   INEIGH, -1 on a physical boundary face        */
   const int32_t* neigh_face;  /* [n][F]   INEIGHN                                      */
   const int32_t* bc;          /* [n][F]   boundary code on faces with neigh = -1:
-                                 1 inflow, 2 outflow, 3 symmetry, 4 wall (inviscid
-                                 slip, Euler only), 6 far field (BOUNDARYS,
-                                 flow_operations.f90:2860-3375); 0 elsewhere         */
+                                 1 inflow, 2 outflow, 3 symmetry, 4 wall (slip for
+                                 Euler, no slip for Navier-Stokes,
+                                 flow_operations.f90:3172-3186), 6 far field
+                                 (BOUNDARYS, flow_operations.f90:2860-3375); 0
+                                 elsewhere                                           */
   const int32_t* qperm;       /* [n][F][Q] quadrature point of the neighbour's face that
                                  coincides with this face's point q                     */
   const double* face_angle;   /* [n][F][2] FACEANGLEX, FACEANGLEY                       */
@@ -234,6 +250,15 @@ int ucg_set_wait_limit(ucg_engine* e, int64_t polls);
  * order and of reverse Cuthill-McKee (0 when reorder is 0).  No counterpart
  * in the reference, which takes the order of its grid reader and METIS. */
 int ucg_cell_order(const ucg_engine* e, int32_t* renumbered, int32_t* n2o, double* cost);
+
+/* MOOD state after the last RK3 stage (cfg.mood 1), in the caller's cell
+ * order: order[c] = IELEM(N,I)%MOOD_O, 1 where the second cascade
+ * recomputed the cell at first order, 2 where only the first cascade
+ * recomputed it (MUSCL), IORDER + 1 elsewhere (time_p.f90:660-680,
+ * mood.f90:375-384); recalc[c] = RECALC, the cells whose reconstruction
+ * may fall back to MUSCL in the next stage.  Either may be NULL.  Waits for
+ * the handle's stream.  UCG_EINVAL without MOOD. */
+int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
 
 /* The cudaStream_t of the handle, as an opaque pointer. */
 void* ucg_get_stream(ucg_engine* e);

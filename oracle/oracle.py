@@ -40,6 +40,9 @@ def lib():
         L.orc_rk3_step.argtypes = [cfgp, geop, recp, C.c_double, f64p]
         L.orc_rk3_stage.restype = C.c_int
         L.orc_rk3_stage.argtypes = [cfgp, geop, recp, C.c_double, C.c_int, f64p, f64p]
+        L.orc_rk3_step_mood.restype = C.c_int
+        L.orc_rk3_step_mood.argtypes = [cfgp, geop, recp, C.c_double, f64p, C.POINTER(C.c_int8),
+                                        C.POINTER(C.c_int32)]
         L.orc_hllc.restype = C.c_int
         L.orc_hllc.argtypes = [C.c_double, f64p, f64p, f64p]
         L.orc_boundary.restype = C.c_int
@@ -127,6 +130,20 @@ class Oracle:
         if rc:
             raise RuntimeError(f"orc_rk3_step failed: {rc}")
         return U
+
+    def rk3_step_mood(self, U: np.ndarray, dt: float, recalc: np.ndarray) -> tuple:
+        """One RUNGE_KUTTA3_MOOD step (cfg.mood 1): the new state and MOOD_O per
+        cell; recalc (int8 [n], RECALC, zero before the first step) is
+        updated in place."""
+        U = np.array(U, dtype=np.float64, copy=True, order="C")
+        assert recalc.dtype == np.int8 and recalc.flags.c_contiguous and recalc.size == self.n
+        order = np.zeros(self.n, dtype=np.int32)
+        rc = lib().orc_rk3_step_mood(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), dt, _p(U),
+                                     recalc.ctypes.data_as(C.POINTER(C.c_int8)),
+                                     order.ctypes.data_as(C.POINTER(C.c_int32)))
+        if rc:
+            raise RuntimeError(f"orc_rk3_step_mood failed: {rc}")
+        return U, order
 
     def rk3_stage(self, Un: np.ndarray, U: np.ndarray, dt: float, stage: int) -> None:
         """Stage `stage` (1..3) of one RK3 step, in place on U (U = Un before stage 1)."""

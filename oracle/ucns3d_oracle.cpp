@@ -201,7 +201,14 @@ bool jump_check(const Ctx& x, int64_t c, const double* u0, const double* ul, dou
 // Navier-Stokes, face gradients ulv [F][Q][4][3] of (T, u, v, w)
 void char_faces(const Ctx& x, int64_t c, const double* U, const double* G, double* ul);
 
-void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, double* ulv) {
+// MOOD (recalc != nullptr, RUNGE_KUTTA3_MOOD): every cell gets its WENO
+// values; a reduced cell (CHECKSOL or not FULL) takes the MUSCL fall-back only
+// if recalc[c] (RECALC of the last MOOD pass: MUSCL, reconstruct_p.f90:2306-
+// 2315, with RECALC from FIX_LIST, mood.f90:440-518), then CHECKSOLX as
+// always.  reduced (optional): the cell's REDUCE; G0 (optional, [ideg][5]):
+// the central stencil polynomial.
+void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, double* ulv,
+                      const int8_t* recalc = nullptr, int8_t* reduced = nullptr, double* G0 = nullptr) {
   const ucg_config* cfg = x.cfg;
   const ucg_geometry* g = x.g;
   const ucg_recon* r = x.r;
@@ -320,8 +327,13 @@ void reconstruct_cell(const Ctx& x, int64_t c, const double* U, double* ul, doub
     if (!g->full[c]) reduce = true;
     else reduce = jump_check(x, c, u0, ul, 0.85);
   }
-  // MUSCL (all cells for scheme 2; flagged cells for WENO)
-  if (cfg->scheme == 2 || reduce || !g->full[c]) muscl_cell(x, c, U, G.data(), ul);
+  if (!g->full[c]) reduce = true;
+  if (reduced) *reduced = reduce ? 1 : 0;
+  if (G0)
+    for (int i = 0; i < ideg * NV; ++i) G0[i] = G[i];
+  // MUSCL (all cells for scheme 2; flagged cells for WENO; under MOOD only
+  // the flagged cells of the last RECALC)
+  if (recalc ? (reduce && recalc[c]) : (cfg->scheme == 2 || reduce)) muscl_cell(x, c, U, G.data(), ul);
   // CHECKSOLX: first order where the face values jump too far
   if (jump_check(x, c, u0, ul, 0.95)) {
     for (int f = 0; f < F; ++f)
@@ -946,16 +958,13 @@ void sutherland(const ucg_config* cfg, double rho, double p, double* mu, double*
 }
 
 // CALL_FLUX_SUBROUTINES_3D: rhs [n][5]
-void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& UL, std::vector<double>& ULV) {
-  const int64_t n = x.n;
+// RHS(I) of one cell from the face values UL (and ULV for Navier-Stokes):
+// CALCULATE_FLUXESHI_CONVECTIVE, flux_p.f90:478-1030, and the diffusive
+// fluxes of CALCULATE_FLUXESHI_DIFFUSIVE, flux_p.f90:1520-2107
+void cell_rhs(const Ctx& x, int64_t c, const std::vector<double>& UL, const std::vector<double>& ULV, double* out) {
   const bool ns = x.cfg->governing == 1;
-  UL.assign((size_t)n * F * Q * NV, 0.0);
-  if (ns) ULV.assign((size_t)n * F * Q * 12, 0.0);
-#pragma omp parallel for schedule(dynamic, 64)
-  for (int64_t c = 0; c < n; ++c) reconstruct_cell(x, c, U, &UL[(size_t)c * F * Q * NV], ns ? &ULV[(size_t)c * F * Q * 12] : nullptr);
   const ucg_geometry* g = x.g;
-#pragma omp parallel for schedule(dynamic, 64)
-  for (int64_t c = 0; c < n; ++c) {
+  {
     double R[NV] = {0, 0, 0, 0, 0};
     // convective
     for (int f = 0; f < g->nfaces[c]; ++f) {
@@ -1078,8 +1087,131 @@ void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& U
         for (int v = 0; v < NV; ++v) R[v] = R[v] - god[v];
       }
     }
-    for (int v = 0; v < NV; ++v) rhs[c * NV + v] = R[v];
+    for (int v = 0; v < NV; ++v) out[v] = R[v];
   }
+}
+
+void residual(const Ctx& x, const double* U, double* rhs, std::vector<double>& UL, std::vector<double>& ULV) {
+  const int64_t n = x.n;
+  const bool ns = x.cfg->governing == 1;
+  UL.assign((size_t)n * F * Q * NV, 0.0);
+  if (ns) ULV.assign((size_t)n * F * Q * 12, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) reconstruct_cell(x, c, U, &UL[(size_t)c * F * Q * NV], ns ? &ULV[(size_t)c * F * Q * 12] : nullptr);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) cell_rhs(x, c, UL, ULV, &rhs[c * NV]);
+}
+
+// PAD_NAD (mood.f90:35-330): PAD if the candidate Uk's density or pressure is
+// not positive (or NaN); else NAD if its density or total energy (variables 1
+// and 5) leaves [min, max] of the stage input Uc over the cell and its face
+// neighbours through interior and periodic faces, widened in the relaxed
+// mode (MOOD_MODE > 0) by NAD_DELTA = max(d1, d2 * (max - min)).
+void pad_nad(const Ctx& x, const double* Uc, const double* Uk, double d1, double d2, std::vector<int8_t>& mood) {
+  const ucg_geometry* g = x.g;
+  mood.assign(x.n, 0);
+  for (int64_t c = 0; c < x.n; ++c) {
+    double pr[NV];
+    cons2prim(x, &Uk[c * NV], pr);
+    bool pad = !(pr[0] > 0.0) || !(pr[4] > 0.0);
+    bool nad = false;
+    if (!pad) {
+      double umin[NV], umax[NV];
+      for (int v = 0; v < NV; ++v) umin[v] = umax[v] = Uc[c * NV + v];
+      for (int f = 0; f < g->nfaces[c]; ++f) {
+        const int64_t nb = g->neigh[c * F + f];
+        if (nb < 0) continue;
+        for (int v = 0; v < NV; ++v) {
+          umin[v] = std::min(umin[v], Uc[nb * NV + v]);
+          umax[v] = std::max(umax[v], Uc[nb * NV + v]);
+        }
+      }
+      for (int v : {0, NV - 1}) {
+        const double u = Uk[c * NV + v];
+        if (x.cfg->mood_mode > 0) {
+          const double delta = std::max(d1, d2 * (umax[v] - umin[v]));
+          if (u < umin[v] - delta || u > umax[v] + delta) nad = true;
+        } else {
+          if (u < umin[v] || u > umax[v]) nad = true;
+        }
+      }
+    }
+    mood[c] = (pad || nad) ? 1 : 0;
+  }
+}
+
+// FIX_LIST (mood.f90:440-518): the flagged cells and their face neighbours
+void fix_list(const Ctx& x, const std::vector<int8_t>& mood, std::vector<int8_t>& recalc) {
+  const ucg_geometry* g = x.g;
+  recalc.assign(x.n, 0);
+  for (int64_t c = 0; c < x.n; ++c) {
+    bool s = mood[c] != 0;
+    for (int f = 0; f < g->nfaces[c]; ++f) {
+      const int64_t nb = g->neigh[c * F + f];
+      if (nb >= 0 && mood[nb]) s = true;
+    }
+    recalc[c] = s ? 1 : 0;
+  }
+}
+
+// One stage of RUNGE_KUTTA3_MOOD (time_p.f90:582-880), Euler: stage s (1-3)
+// from the stage input Uc and the step base Un into Uo, RECALC in/out.
+// The candidate from the reconstruction under the last RECALC; then
+// MOOD_OPERATOR_2 (MOOD_VAR1/2): PAD_NAD, FIX_LIST, MUSCL (no CHECKSOLX) on
+// the selected reduced cells, their residual and stage redone; then
+// MOOD_OPERATOR_1 (MOOD_VAR3/4): PAD_NAD, FIX_LIST, the flagged cells' face
+// values their stage-input mean (CASCADE 2 of
+// CALCULATE_FLUXESHI_CONVECTIVE_MOOD, flux_p.f90:2722-2733), the selected
+// cells' residual and stage redone.  order: MOOD_O.
+void mood_stage(const Ctx& x, int s, double dt, const double* Uc, const double* Un, double* Uo,
+                std::vector<int8_t>& recalc, int32_t* order) {
+  const int64_t n = x.n;
+  const ucg_geometry* g = x.g;
+  const int ideg = x.cfg->ideg;
+  std::vector<double> UL((size_t)n * F * Q * NV, 0.0), ULV, G0((size_t)n * ideg * NV), R((size_t)n * NV),
+      Uk((size_t)n * NV);
+  std::vector<int8_t> red(n);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c)
+    reconstruct_cell(x, c, Uc, &UL[(size_t)c * F * Q * NV], nullptr, recalc.data(), &red[c], &G0[(size_t)c * ideg * NV]);
+  const double a[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0}, b[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0}, k[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  const int si = s - 1;
+  auto stage = [&](int64_t c, double* out) {
+    double rr[NV];
+    cell_rhs(x, c, UL, ULV, rr);
+    const double oov = 1.0 / g->volume[c];
+    for (int v = 0; v < NV; ++v) {
+      const double d = dt * (rr[v] * oov);
+      out[v] = si == 0 ? Un[c * NV + v] - d : (a[si] * Un[c * NV + v]) + (b[si] * Uc[c * NV + v]) - (k[si] * d);
+    }
+  };
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) stage(c, &Uk[c * NV]);
+  // first cascade
+  std::vector<int8_t> m1, s1, m2, s2;
+  pad_nad(x, Uc, Uk.data(), x.cfg->mood_var[0], x.cfg->mood_var[1], m1);
+  fix_list(x, m1, s1);
+  for (int64_t c = 0; c < n; ++c)
+    if (s1[c] && red[c]) muscl_cell(x, c, Uc, &G0[(size_t)c * ideg * NV], &UL[(size_t)c * F * Q * NV]);
+  std::vector<double> Uk2(Uk);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c)
+    if (s1[c]) stage(c, &Uk2[c * NV]);
+  // second cascade
+  pad_nad(x, Uc, Uk2.data(), x.cfg->mood_var[2], x.cfg->mood_var[3], m2);
+  fix_list(x, m2, s2);
+  for (int64_t c = 0; c < n; ++c)
+    if (m2[c])
+      for (int i = 0; i < F * Q; ++i)
+        for (int v = 0; v < NV; ++v) UL[((size_t)c * F * Q + i) * NV + v] = Uc[c * NV + v];
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c) {
+    if (s2[c]) stage(c, &Uo[c * NV]);
+    else
+      for (int v = 0; v < NV; ++v) Uo[c * NV + v] = Uk2[c * NV + v];
+    if (order) order[c] = s2[c] ? 1 : s1[c] ? 2 : x.cfg->iorder + 1;
+  }
+  recalc = s2;
 }
 
 bool check_ctx(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r) {
@@ -1190,6 +1322,24 @@ int orc_rk3_stage(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon*
       U[c * NV + v] = s == 0 ? Un[c * NV + v] - rr : (a[s] * Un[c * NV + v]) + (b[s] * u) - (k[s] * rr);
     }
   }
+  return UCG_OK;
+}
+
+// RUNGE_KUTTA3_MOOD (time_p.f90:582-880) in place on U [n][5], Euler with
+// WENO; recalc [n] is RECALC, carried between calls (zero before the first
+// step, memory.f90:1002-1005); order (optional, [n]) MOOD_O after the step.
+int orc_rk3_step_mood(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt, double* U,
+                      int8_t* recalc, int32_t* order) {
+  if (!check_ctx(cfg, g, r) || !U || !recalc || !cfg->mood || cfg->governing != 2 || cfg->scheme != 3)
+    return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const int64_t n = g->ncells;
+  std::vector<int8_t> rc(recalc, recalc + n);
+  std::vector<double> Un(U, U + n * NV), Ua(n * NV), Ub(n * NV);
+  mood_stage(x, 1, dt, Un.data(), Un.data(), Ua.data(), rc, nullptr);
+  mood_stage(x, 2, dt, Ua.data(), Un.data(), Ub.data(), rc, nullptr);
+  mood_stage(x, 3, dt, Ub.data(), Un.data(), U, rc, order);
+  for (int64_t c = 0; c < n; ++c) recalc[c] = rc[c];
   return UCG_OK;
 }
 

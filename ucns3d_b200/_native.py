@@ -49,6 +49,7 @@ class UcgConfig(C.Structure):
         ("quad_w", C.c_double * UCG_MAX_QP), ("tri_w", C.c_double * UCG_MAX_QP),
         ("bc_state", C.c_double * UCG_NV),
         ("boundtype", C.c_int32), ("reorder", C.c_int32),
+        ("mood", C.c_int32), ("mood_mode", C.c_int32), ("mood_var", C.c_double * 4),
     ]
 
 
@@ -210,6 +211,8 @@ def engine() -> C.CDLL:
         lib.ucg_set_wait_limit.argtypes = [vp, C.c_int64]
         lib.ucg_cell_order.restype = C.c_int
         lib.ucg_cell_order.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _f64p]
+        lib.ucg_mood_state.restype = C.c_int
+        lib.ucg_mood_state.argtypes = [vp, _i32p, _i32p]
         lib.ucg_tangent_run.restype = C.c_int
         lib.ucg_tangent_run.argtypes = [vp, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
         _engine = lib

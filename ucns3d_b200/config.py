@@ -19,7 +19,8 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
                 ufreestream: float = 1.0, pres: float = 1.0, char_length: float = 1.0,
                 lwci: float = 1000.0, wenoz: int = 0, limiter: int = 7,
                 bc_state=(1.0, 0.0, 0.0, 0.0, 1.0), lamx: float = 1.0, wenwrt: int = 1,
-                riemann: int = 1, boundtype: int = 1, reorder: int = 1) -> N.UcgConfig:
+                riemann: int = 1, boundtype: int = 1, reorder: int = 1, mood: int = 0, mood_mode: int = 1,
+                mood_var=(1e-4, 1e-3, 1e-4, 1e-3)) -> N.UcgConfig:
     """A ucg_config for a prepared mesh.  ``reynolds`` sets VISC for
     Navier-Stokes; ``bc_state`` is the free-stream primitive state used by
     inflow/outflow/far-field boundaries; ``boundtype`` is BOUNDTYPE (0 supersonic
@@ -27,7 +28,9 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
     ``wenwrt`` 1 reconstructs the conserved
     variables, 2 the characteristic variables (WENWRT of UCNS3D.DAT);
     ``riemann`` 1 HLLC, 2 Rusanov, 3 Roe, 4 rotated Roe-HLL, 5 t-Roe, 9 HLL
-    (iRiemann)."""
+    (iRiemann); ``mood`` 1 turns on MOOD in the RK3 stages with MOOD_MODE
+    ``mood_mode`` (1 relaxed, 0 original) and MOOD_VAR1-4 ``mood_var`` (the
+    lines of MOOD.DAT)."""
     if not getattr(mesh, "prepared", False):
         raise ValueError("mesh must be prepared first")
     cfg = N.UcgConfig()
@@ -55,6 +58,10 @@ def make_config(mesh, governing: int = EULER, precision: int = N.UCG_FP64, gamma
     cfg.lamx = lamx
     cfg.boundtype = boundtype
     cfg.reorder = reorder
+    cfg.mood = mood
+    cfg.mood_mode = mood_mode
+    for k in range(4):
+        cfg.mood_var[k] = mood_var[k]
     for k in range(5):
         cfg.bc_state[k] = bc_state[k]
     return cfg

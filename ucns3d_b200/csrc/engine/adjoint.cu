@@ -952,9 +952,9 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
 int adjw_setup(ucg_engine* e) {
   const ucg_config& c = e->cfg;
   if (!(c.scheme == 3 && (c.ees == 0 || c.ees == 5) && c.wenwrt == 1 && c.governing == 2 &&
-        c.precision == UCG_FP64 && c.riemann == 1))
+        c.precision == UCG_FP64 && c.riemann == 1 && !c.mood))
     return fail(e, UCG_EINVAL,
-                "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, CWENO with or without WENO-Z), HLLC, Euler, FP64 form");
+                "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, CWENO with or without WENO-Z), HLLC, Euler, FP64 form, without MOOD");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   if (e->adjw_ready) return UCG_OK;
   const int64_t n = e->n, ngrp = (n + 31) / 32;

@@ -66,7 +66,16 @@ struct Problem {
   void* gbuf;               // stencil polynomials G[ll][d][v], interleaved like the stencils
   double* qbuf;             // characteristic WENO: G_l^T S G_l per stencil, 15 values, interleaved
   double* isb;              // conserved WENO: smoothness indicators [A][NV] per cell, interleaved (k_wis)
-  int8_t* wflag;            // WENO5: cells k_wface leaves to the MUSCL fall-back [n]
+  bool wface;               // IORDER 4 conserved WENO through k_wis + k_wface
+  int8_t* wflag;            // cells whose reconstruction was reduced (CHECKSOL or not FULL) [n];
+                            // k_wface writes it for k_wpost's fall-back pass, k_wpost under MOOD
+  // MOOD (RUNGE_KUTTA3_MOOD): all nullptr without it
+  int8_t* mprev;            // RECALC of the last MOOD pass: the fall-back cells of the next reconstruction
+  int8_t* mood;             // MOOD flag of the current cascade (PAD_NAD)
+  int8_t* msel;             // cells whose residual the current cascade recomputes (FIX_LIST); also
+                            // selects the faces k_face recomputes (nullptr: every face)
+  int8_t* mmus;             // first cascade: msel and reduced, MUSCL recomputed
+  int8_t* mord;             // MOOD_O per cell
   void* dul;                // [n][MF][MQ][NV]  face value minus cell mean (T)
   double* ulv;              // [n][MF][MQ][4][3] face gradients of T,u,v,w (MUSCL IORDER 1)
   double* fgrad;            // [nown][QS][4][3] face-point average of both sides' gradients of T,u,v,w (WENO)

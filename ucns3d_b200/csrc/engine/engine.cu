@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -128,6 +129,12 @@ Problem make_problem(ucg_engine* e) {
   p.qbuf = (double*)e->qbuf.p;
   p.isb = (double*)e->isb.p;
   p.wflag = (int8_t*)e->wflag.p;
+  p.wface = e->wface;
+  p.mprev = e->cfg.mood ? (int8_t*)e->mprev.p : nullptr;
+  p.mood = (int8_t*)e->mflag.p;
+  p.msel = nullptr;
+  p.mmus = nullptr;
+  p.mord = (int8_t*)e->mord.p;
   p.dul = e->dul.p;
   p.ulv = (double*)e->ulv.p;
   p.fgrad = (double*)e->fgrad.p;
@@ -182,8 +189,7 @@ int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
 }
 
 template <typename T, bool NS>
-int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
-                  double dt) {
+void launch_faces_t(ucg_engine* e, const Problem& p, const double* Uc) {
   constexpr int FB = UCG_FACE_BLOCK;
   const unsigned fb = (unsigned)((e->nown + FB - 1) / FB);
   switch (e->cfg.riemann) {  // the Riemann solver is a template argument of the face kernel
@@ -194,22 +200,91 @@ int launch_flux_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, c
     case 9: k_face<T, NS, 9><<<fb, FB, 0, e->stream>>>(p, Uc); break;
     default: k_face<T, NS, 1><<<fb, FB, 0, e->stream>>>(p, Uc); break;
   }
-  unsigned blocks = (unsigned)((e->n + 255) / 256);
-  switch (mode) {
-    case 0: k_update<NS, 0><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    case 1: k_update<NS, 1><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    case 2: k_update<NS, 2><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-    default: k_update<NS, 3><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
-  }
-  e->launches += 2;
+  e->launches += 1;
+}
+
+int launch_faces(ucg_engine* e, const Problem& p, const double* Uc) {
+  const bool ns = e->cfg.governing == 1;
+  if (e->mixed) ns ? launch_faces_t<float, true>(e, p, Uc) : launch_faces_t<float, false>(e, p, Uc);
+  else ns ? launch_faces_t<double, true>(e, p, Uc) : launch_faces_t<double, false>(e, p, Uc);
   CK(cudaGetLastError());
   return UCG_OK;
 }
 
-int launch_flux(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo, double dt) {
-  bool ns = e->cfg.governing == 1;
-  if (e->mixed) return ns ? launch_flux_t<float, true>(e, p, mode, Uc, Un, Uo, dt) : launch_flux_t<float, false>(e, p, mode, Uc, Un, Uo, dt);
-  return ns ? launch_flux_t<double, true>(e, p, mode, Uc, Un, Uo, dt) : launch_flux_t<double, false>(e, p, mode, Uc, Un, Uo, dt);
+template <bool NS, bool CHK>
+void launch_update_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
+                     double dt) {
+  unsigned blocks = (unsigned)((e->n + 255) / 256);
+  switch (mode) {
+    case 0: k_update<NS, 0, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 1: k_update<NS, 1, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    case 2: k_update<NS, 2, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+    default: k_update<NS, 3, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
+  }
+  e->launches += 1;
+}
+
+// face fluxes, then the residual (mode 0) or RK stage `mode`; check = false
+// leaves the new state's physical test to the caller (MOOD's candidate)
+int launch_flux(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo, double dt,
+                bool check) {
+  int rc = launch_faces(e, p, Uc);
+  if (rc) return rc;
+  const bool ns = e->cfg.governing == 1;
+  if (ns) check ? launch_update_t<true, true>(e, p, mode, Uc, Un, Uo, dt) : launch_update_t<true, false>(e, p, mode, Uc, Un, Uo, dt);
+  else check ? launch_update_t<false, true>(e, p, mode, Uc, Un, Uo, dt) : launch_update_t<false, false>(e, p, mode, Uc, Un, Uo, dt);
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+// One RK stage under MOOD (RUNGE_KUTTA3_MOOD, time_p.f90:582-880): the
+// candidate into Um from the stage input Uc (step base Un), then the two
+// cascades of MOOD_OPERATOR_2 / MOOD_OPERATOR_1 (mood.f90:337-437): PAD_NAD,
+// FIX_LIST, the selected cells' faces recomputed (first cascade after the
+// MUSCL of the selected reduced cells, second with the flagged cells at
+// first order) and their stage redone; the result into Uo.  The second
+// cascade's selection stays in mprev (RECALC) for the next reconstruction.
+int mood_stage(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo, double dt) {
+  double* Um = (double*)e->Um.p;
+  int8_t* sel1 = (int8_t*)e->msel.p;
+  const ucg_config& c = e->cfg;
+  const unsigned blocks = (unsigned)((e->n + 255) / 256);
+  int rc;
+  if ((rc = launch_recon(e, p, Uc))) return rc;
+  if ((rc = launch_flux(e, p, mode, Uc, Un, Um, dt, false))) return rc;
+  // first cascade (MOOD_VAR1/2): MUSCL where the reconstruction was reduced
+  k_mood_detect<<<blocks, 256, 0, e->stream>>>(p, Uc, Um, c.mood_var[0], c.mood_var[1], c.mood_mode);
+  k_mood_fix<<<blocks, 256, 0, e->stream>>>(p, sel1, (int8_t*)e->mmus.p);
+  e->launches += 2;
+  Problem p1 = p;
+  p1.mmus = (int8_t*)e->mmus.p;
+  if ((rc = launch_recon(e, p1, Uc))) return rc;
+  Problem p2 = p;
+  p2.msel = sel1;
+  if ((rc = launch_faces(e, p2, Uc))) return rc;
+  switch (mode) {
+    case 1: k_mood_update<1, false><<<blocks, 256, 0, e->stream>>>(p2, Uc, Un, Um, Um, nullptr, dt); break;
+    case 2: k_mood_update<2, false><<<blocks, 256, 0, e->stream>>>(p2, Uc, Un, Um, Um, nullptr, dt); break;
+    default: k_mood_update<3, false><<<blocks, 256, 0, e->stream>>>(p2, Uc, Un, Um, Um, nullptr, dt); break;
+  }
+  // second cascade (MOOD_VAR3/4): first order on the flagged cells
+  k_mood_detect<<<blocks, 256, 0, e->stream>>>(p, Uc, Um, c.mood_var[2], c.mood_var[3], c.mood_mode);
+  k_mood_fix<<<blocks, 256, 0, e->stream>>>(p, (int8_t*)e->mprev.p, nullptr);
+  const int64_t nd = e->n * MF * e->QS * NV;
+  if (e->mixed) k_mood_first<float><<<(unsigned)((nd + 255) / 256), 256, 0, e->stream>>>(p);
+  else k_mood_first<double><<<(unsigned)((nd + 255) / 256), 256, 0, e->stream>>>(p);
+  e->launches += 4;
+  Problem p3 = p;
+  p3.msel = (int8_t*)e->mprev.p;
+  if ((rc = launch_faces(e, p3, Uc))) return rc;
+  switch (mode) {
+    case 1: k_mood_update<1, true><<<blocks, 256, 0, e->stream>>>(p3, Uc, Un, Um, Uo, sel1, dt); break;
+    case 2: k_mood_update<2, true><<<blocks, 256, 0, e->stream>>>(p3, Uc, Un, Um, Uo, sel1, dt); break;
+    default: k_mood_update<3, true><<<blocks, 256, 0, e->stream>>>(p3, Uc, Un, Um, Uo, sel1, dt); break;
+  }
+  e->launches += 1;
+  CK(cudaGetLastError());
+  return UCG_OK;
 }
 
 // one RUNGE_KUTTA3 step; dt from the host value or, if dt_dev, from device memory
@@ -220,6 +295,11 @@ int rk3(ucg_engine* e, double dt, bool dt_dev) {
   double* Ua = (double*)e->Ua.p;
   double* Ub = (double*)e->Ub.p;
   int rc;
+  if (e->cfg.mood) {
+    if ((rc = mood_stage(e, p, 1, Un, Un, Ua, dt))) return rc;
+    if ((rc = mood_stage(e, p, 2, Ua, Un, Ub, dt))) return rc;
+    return mood_stage(e, p, 3, Ub, Un, Un, dt);
+  }
   if ((rc = launch_recon(e, p, Un))) return rc;
   if ((rc = launch_flux(e, p, 1, Un, Un, Ua, dt))) return rc;
   if ((rc = launch_recon(e, p, Ua))) return rc;
@@ -388,9 +468,13 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
       c.nq_quad > UCG_MAX_QP || c.nq_tri < 1 || c.nq_tri > UCG_MAX_QP || (c.ees == 5 && ((c.ideg2 != 3 && c.ideg2 != 9) || c.imax2 < c.ideg2 || c.ideg2 > c.ideg || c.imax2 > c.imax)) ||
       c.gamma <= 1.0 || c.limiter < 1 || c.limiter > 9 || !((c.riemann >= 1 && c.riemann <= 5) || c.riemann == 9) ||
       !(c.wenwrt == 1 || (c.wenwrt == 2 && c.scheme == 3)) || (c.boundtype != 0 && c.boundtype != 1) ||
-      (c.reorder != 0 && c.reorder != 1)) {
+      (c.reorder != 0 && c.reorder != 1) || (c.mood != 0 && c.mood != 1) ||
+      (c.mood && (c.scheme != 3 || c.governing != 2 || (c.mood_mode != 0 && c.mood_mode != 1) ||
+                  !(c.mood_var[0] >= 0.0 && c.mood_var[1] >= 0.0 && c.mood_var[2] >= 0.0 && c.mood_var[3] >= 0.0 &&
+                    std::isfinite(c.mood_var[0] + c.mood_var[1] + c.mood_var[2] + c.mood_var[3]))))) {
     g_create_err = "unsupported or inconsistent configuration (scheme 2|3, iorder 1..4, ees 0|5, HLLC/Rusanov/Roe/rotated Roe-HLL/t-Roe/HLL, limiter 1..9, "
-                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9, boundtype 0|1, reorder 0|1)";
+                   "conserved or (WENO only) characteristic-variable WENO, CWENO lower-order degree 3 or 9, boundtype 0|1, reorder 0|1, "
+                   "MOOD 0|1 with WENO, Euler, mode 0|1 and finite non-negative MOOD_VAR1-4)";
     return UCG_EINVAL;
   }
   if (c.scheme == 2 && c.admis_max != 1) {
@@ -469,7 +553,19 @@ int ucg_create(const ucg_config* cfg, int64_t ncells, int device, ucg_engine** o
     if (!(wis && wis[0] == '0')) rc = rc ? rc : alloc(e, e->isb, (size_t)ngrp * 32 * c.admis_max * NV * 8);
     // face values one warp per variable (k_wface), unless UCG_WENO_FACE=0
     const char* wf = std::getenv("UCG_WENO_FACE");
-    if (!(wis && wis[0] == '0') && !(wf && wf[0] == '0')) rc = rc ? rc : alloc(e, e->wflag, (size_t)n);
+    e->wface = !(wis && wis[0] == '0') && !(wf && wf[0] == '0');
+    if (e->wface) rc = rc ? rc : alloc(e, e->wflag, (size_t)n);
+  }
+  if (c.mood) {  // RECALC (zero at the start, memory.f90:1002-1005), flags, MOOD_O, candidate
+    rc = rc ? rc : alloc(e, e->wflag, (size_t)n);
+    rc = rc ? rc : alloc(e, e->mprev, (size_t)n);
+    rc = rc ? rc : alloc(e, e->mflag, (size_t)n);
+    rc = rc ? rc : alloc(e, e->msel, (size_t)n);
+    rc = rc ? rc : alloc(e, e->mmus, (size_t)n);
+    rc = rc ? rc : alloc(e, e->mord, (size_t)n);
+    rc = rc ? rc : alloc(e, e->Um, n * NV * 8);
+    if (!rc && cudaMemset(e->mprev.p, 0, (size_t)n) != cudaSuccess) rc = fail(e, UCG_ECUDA, "cudaMemset failed");
+    if (!rc && cudaMemset(e->mord.p, c.iorder + 1, (size_t)n) != cudaSuccess) rc = fail(e, UCG_ECUDA, "cudaMemset failed");
   }
   if (c.wenwrt == 2)  // characteristic WENO: G^T S G of every stencil (15 values)
     rc = rc ? rc : alloc(e, e->qbuf, (size_t)ngrp * 32 * c.admis_max * 15 * 8);
@@ -506,7 +602,8 @@ void ucg_destroy(ucg_engine* e) {
                    &e->vol, &e->minedge, &e->jinv, &e->admis, &e->full, &e->qpts, &e->bmean, &e->sten, &e->invmat,
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
-                   &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb, &e->wflag};
+                   &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb, &e->wflag, &e->mprev, &e->mflag,
+                   &e->msel, &e->mmus, &e->mord, &e->Um};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -1021,6 +1118,22 @@ int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms) {
   if (rc) return rc;
   for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
   CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc) {
+  if (!e) return UCG_EINVAL;
+  if (!e->cfg.mood) return fail(e, UCG_EINVAL, "MOOD is off (cfg.mood 0)");
+  const int64_t n = e->n;
+  std::vector<int8_t> a((size_t)n), b((size_t)n);
+  CK(cudaStreamSynchronize(e->stream));
+  CK(cudaMemcpy(a.data(), e->mord.p, (size_t)n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(b.data(), e->mprev.p, (size_t)n, cudaMemcpyDeviceToHost));
+  for (int64_t c = 0; c < n; ++c) {
+    const int64_t o = e->n2o.empty() ? c : e->n2o[c];  // caller's cell at device position c
+    if (order) order[o] = a[c];
+    if (recalc) recalc[o] = b[c];
+  }
   return UCG_OK;
 }
 

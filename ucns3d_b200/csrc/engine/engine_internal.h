@@ -53,10 +53,13 @@ struct ucg_engine {
   DevBuf sten, invmat, ind;
   // scratch and state
   DevBuf gbuf, isb, wflag, dul, ulv, fgrad, gv, prim, upad, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux, qbuf;
+  // MOOD (cfg.mood): RECALC, the cascade's flags and selections, MOOD_O, the candidate state
+  DevBuf mprev, mflag, msel, mmus, mord, Um;
   int64_t nown = 0;
   int64_t nown_plain = 0;  // owned faces [0, nown_plain): interior and mirror; the rest other boundaries
   cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs
   bool lsq_bulk = false;       // UCG_LSQ_BULK=1 at ucg_create: k_lsq_tma instead of k_lsq
+  bool wface = false;          // IORDER 4 conserved WENO: face values one warp per variable (k_wface)
   long lsq_wait = -1;          // polls of a k_lsq_tma stage wait (ucg_set_wait_limit; < 0 the default)
   std::vector<uint8_t> recon_done;  // per cell, for ucg_upload_recon chunks
   std::vector<int8_t> admis_h;      // ADMIS per cell, for the stencil checks of ucg_upload_recon
@@ -93,7 +96,9 @@ ucg::Problem make_problem(ucg_engine* e);
 bool ready(ucg_engine* e);
 int launch_recon(ucg_engine* e, const ucg::Problem& p, const double* U);
 int launch_flux(ucg_engine* e, const ucg::Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
-                double dt);
+                double dt, bool check = true);
+// the face fluxes alone (k_face; with p.msel only the faces of the selected cells)
+int launch_faces(ucg_engine* e, const ucg::Problem& p, const double* Uc);
 int rk3(ucg_engine* e, double dt, bool dt_dev);
 // [n][5] FP64 arrays between the caller's cell order on the host and the
 // device order (a plain copy when the engine keeps the caller's order);

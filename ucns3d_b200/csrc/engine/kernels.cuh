@@ -161,9 +161,10 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
   double u0[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) u0[v] = Uc[c * NV + v];
+  const int64_t nb = p.neigh[c * MF + f];
+  if (p.msel && !(p.msel[c] || (nb >= 0 && p.msel[nb]))) return;  // MOOD: faces of the recomputed cells
   const int ft = p.ftype[c * MF + f];
   const int nq = face_nq(p, ft);
-  const int64_t nb = p.neigh[c * MF + f];
   const int nf = p.nface[c * MF + f];
   double r[4];
 #pragma unroll
@@ -256,7 +257,9 @@ __global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double
 // viscous ones subtracted, as CALCULATE_FLUXESHI_CONVECTIVE/_DIFFUSIVE add
 // them to RHS) and the RUNGE_KUTTA3 stage update (time_p.f90:885-1027).
 // MODE 0: write the residual; MODE 1/2/3: RK stage 1/2/3.
-template <bool NS, int MODE>
+// CHK: test the new state (HEALTH_NONPHYS); MOOD's candidate states are
+// tested after the cascades instead
+template <bool NS, int MODE, bool CHK = true>
 __global__ void __launch_bounds__(256) k_update(Problem p, const double* __restrict__ Uc, const double* Un,
                                                 double* Uout, double dt_host) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -285,11 +288,133 @@ __global__ void __launch_bounds__(256) k_update(Problem p, const double* __restr
     else if (MODE == 2) out[v] = (3.0 / 4.0) * Un[c * NV + v] + (1.0 / 4.0) * Uc[c * NV + v] - (1.0 / 4.0) * rr;
     else out[v] = (1.0 / 3.0) * Un[c * NV + v] + (2.0 / 3.0) * Uc[c * NV + v] - (2.0 / 3.0) * rr;
   }
-  double pr[NV];
-  cons2prim(p.gamma, out, pr);
-  if (!(pr[0] > 0.0) || !(pr[4] > 0.0) || !isfinite(out[4])) atomicOr(p.health, HEALTH_NONPHYS);
+  if (CHK) {
+    double pr[NV];
+    cons2prim(p.gamma, out, pr);
+    if (!(pr[0] > 0.0) || !(pr[4] > 0.0) || !isfinite(out[4])) atomicOr(p.health, HEALTH_NONPHYS);
+  }
 #pragma unroll
   for (int v = 0; v < NV; ++v) Uout[c * NV + v] = out[v];
+}
+
+// ======================================================================
+// MOOD (RUNGE_KUTTA3_MOOD, time_p.f90:582-880; mood.f90), Euler only.
+// After a stage's candidate Uk: per cascade, PAD_NAD flags the cells whose
+// candidate is not admissible, FIX_LIST adds their face neighbours, the
+// faces of the selected cells are recomputed (first cascade: MUSCL on the
+// selected reduced cells; second: the flagged cells at first order, their
+// stage-input mean on every face) and the selected cells' stage is redone.
+// ======================================================================
+
+// PAD_NAD (mood.f90:35-330): PAD if the candidate's density or pressure is
+// not positive (or NaN); else NAD if its density or energy leaves the
+// bounds of the stage-input state over the cell and its face neighbours
+// (interior and periodic faces), widened by max(d1, d2 * (max - min)) in
+// the relaxed mode.  p.mood[c] = PAD or NAD.
+__global__ void k_mood_detect(Problem p, const double* __restrict__ Uc, const double* __restrict__ Uk, double d1,
+                              double d2, int relaxed) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  double u[NV], pr[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) u[v] = Uk[c * NV + v];
+  cons2prim(p.gamma, u, pr);
+  bool bad = !(pr[0] > 0.0) || !(pr[4] > 0.0);
+  if (!bad) {
+    constexpr int VS[2] = {0, NV - 1};  // density and energy
+    double lo[2], hi[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) lo[k] = hi[k] = Uc[c * NV + VS[k]];
+    const int nf = p.nfaces[c];
+    for (int f = 0; f < nf; ++f) {
+      const int64_t nb = p.neigh[c * MF + f];
+      if (nb < 0) continue;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double un = Uc[nb * NV + VS[k]];
+        lo[k] = fmin(lo[k], un);
+        hi[k] = fmax(hi[k], un);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const double x = u[VS[k]];
+      if (relaxed) {
+        const double dl = fmax(d1, d2 * (hi[k] - lo[k]));
+        bad = bad || x < lo[k] - dl || x > hi[k] + dl;
+      } else {
+        bad = bad || x < lo[k] || x > hi[k];
+      }
+    }
+  }
+  p.mood[c] = bad ? 1 : 0;
+}
+
+// FIX_LIST (mood.f90:440-518): sel[c] = the cell or a face neighbour
+// (interior and periodic faces) is flagged; mus (first cascade) = sel and
+// the cell's reconstruction was reduced (MUSCL, mood.f90:353 with
+// reconstruct_p.f90:2306-2315)
+__global__ void k_mood_fix(Problem p, int8_t* __restrict__ sel, int8_t* __restrict__ mus) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  bool s = p.mood[c] != 0;
+  const int nf = p.nfaces[c];
+  for (int f = 0; f < nf; ++f) {
+    const int64_t nb = p.neigh[c * MF + f];
+    if (nb >= 0 && p.mood[nb]) s = true;
+  }
+  sel[c] = s ? 1 : 0;
+  if (mus) mus[c] = (s && p.wflag[c]) ? 1 : 0;
+}
+
+// second cascade: the flagged cells' face values become their stage-input
+// mean (CALCULATE_FLUXESHI_CONVECTIVE_MOOD with CASCADE 2, flux_p.f90:2722-2733)
+template <typename T>
+__global__ void k_mood_first(Problem p) {
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int64_t W = (int64_t)MF * QS * NV;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n * W) return;
+  if (p.mood[i / W]) ((T*)p.dul)[i] = T(0);
+}
+
+// the stage redone on the selected cells (p.msel) from the recomputed face
+// fluxes, the other cells keep the candidate Uk; FIN (second cascade): into
+// Uo, MOOD_O and the HEALTH_NONPHYS test of every cell
+template <int MODE, bool FIN>
+__global__ void __launch_bounds__(256) k_mood_update(Problem p, const double* __restrict__ Uc, const double* Un,
+                                                     const double* Uk, double* Uo, const int8_t* __restrict__ sel1,
+                                                     double dt_host) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  double out[NV];
+  if (p.msel[c]) {
+    const int nf = p.nfaces[c];
+    double R[NV] = {0, 0, 0, 0, 0};
+    for (int f = 0; f < nf; ++f)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) R[v] = R[v] + p.fflux[(c * MF + f) * NV + v];
+    const double dt = p.dt_dev ? *p.dt_dev : dt_host;
+    const double oov = 1.0 / p.vol[c];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double rr = dt * (R[v] * oov);
+      if (MODE == 1) out[v] = Un[c * NV + v] - rr;
+      else if (MODE == 2) out[v] = (3.0 / 4.0) * Un[c * NV + v] + (1.0 / 4.0) * Uc[c * NV + v] - (1.0 / 4.0) * rr;
+      else out[v] = (1.0 / 3.0) * Un[c * NV + v] + (2.0 / 3.0) * Uc[c * NV + v] - (2.0 / 3.0) * rr;
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = Uk[c * NV + v];
+  }
+  if (FIN) {
+    double pr[NV];
+    cons2prim(p.gamma, out, pr);
+    if (!(pr[0] > 0.0) || !(pr[4] > 0.0) || !isfinite(out[4])) atomicOr(p.health, HEALTH_NONPHYS);
+    p.mord[c] = (int8_t)(p.msel[c] ? 1 : sel1[c] ? 2 : p.iorder + 1);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Uo[c * NV + v] = out[v];
 }
 
 // ======================================================================

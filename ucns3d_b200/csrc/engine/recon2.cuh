@@ -370,7 +370,8 @@ __device__ __forceinline__ void sym_form(const T* __restrict__ P, const T (&g)[N
 // from L1/L2 by the other stencils, instead of once per stencil as when one
 // lane runs all the stencils of its cell.  Output: p.isb, FP64, interleaved
 // over 32-cell groups ((group * A + ll) * NV + v) * 32 + lane; cells that
-// take the MUSCL fall-back outright (not FULL) are skipped.
+// take the MUSCL fall-back outright (not FULL) are skipped, except under
+// MOOD, where every cell is reconstructed.
 template <int P, typename T>
 __global__ void __launch_bounds__(224) k_wis(Problem p) {
   constexpr int ID = Deg<P>::ideg;
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(224) k_wis(Problem p) {
   constexpr int VI = WVars<T>::is;
   const int lane = threadIdx.x & 31, ll = threadIdx.x >> 5;
   const int64_t grp = blockIdx.x, c = grp * 32 + lane;
-  if (c >= p.n || !p.full[c]) return;
+  if (c >= p.n || (!p.mprev && !p.full[c])) return;
   const int adm = p.admis[c];
   if (ll >= adm) return;
   const int A = p.admis_max, ID2 = p.ideg2;
@@ -442,9 +443,11 @@ __global__ void __launch_bounds__(224) k_wis(Problem p) {
 // once (the five warps evaluate at the same points); the values of one face
 // go through shared memory, [cell][point][variable] with an odd row stride
 // (no bank conflicts), from where the block tests CHECKSOL (0.85) and stores
-// them as one contiguous run per cell.  Cells that fail CHECKSOL, or are not FULL, are marked in
-// p.wflag for k_wpost<..., FB> (the MUSCL fall-back).  Weights, combination
-// and face values take k_wpost's operations in k_wpost's order.
+// them as one contiguous run per cell.  Cells that fail CHECKSOL, or are not
+// FULL, are marked in p.wflag for k_wpost<..., FB> (the MUSCL fall-back).
+// Weights, combination and face values take k_wpost's operations in
+// k_wpost's order.  Under MOOD the cells that are not FULL are reconstructed
+// too (over their admissible stencils) and marked.
 template <int P, typename T>
 __global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
@@ -464,14 +467,15 @@ __global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __re
     for (int i = tid; i < FQ * 3 * 32; i += 32 * NV) s_x[i] = __ldcs(xg + i);
   }
   const bool cell = c < p.n;
-  const bool live = cell && p.full[c];
+  const bool full = cell && p.full[c];
+  const bool live = cell && (full || p.mprev);
   const int A = p.admis_max;
   const int adm = live ? p.admis[c] : 0;
   const bool cw = p.ees == 5;
   const int ID2 = p.ideg2;
   const double lc1 = 1.0 - 1.0 / p.lwci;
   const double lk = adm > 1 ? (1.0 - lc1) / (adm - 1) : 0.0;
-  if (tid < 32) s_flag[tid] = live ? 0 : 1;
+  if (tid < 32) s_flag[tid] = full ? 0 : 1;
   // ---- weights of variable v (WENOWEIGHTS, FP64)
   double w[MA];
   {
@@ -604,8 +608,14 @@ __global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __re
 // polynomial instead of subtracting the basis means at every face point.
 // ISB: the indicators come from k_wis (p.isb) instead of being formed here.
 // FB: only the cells that k_wface marked in p.wflag, straight to the MUSCL
-// fall-back (the others return at once).
-template <int P, typename T, bool CH = false, bool ISB = false, bool FB = false>
+// fall-back (the others return at once).  MU (with FB): the first MOOD
+// cascade, MUSCL on the cells of p.mmus without CHECKSOLX (MUSCL of
+// MOOD_OPERATOR_2, mood.f90:353).
+// Under MOOD (p.mprev) every cell is reconstructed; a reduced cell (CHECKSOL,
+// or not FULL) takes the MUSCL fall-back only if the last MOOD pass
+// recomputed it (RECALC, reconstruct_p.f90:2306-2315), else it keeps its
+// WENO values and only CHECKSOLX; the reduced flags go to p.wflag.
+template <int P, typename T, bool CH = false, bool ISB = false, bool FB = false, bool MU = false>
 __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<T>::N;
@@ -727,8 +737,9 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
       for (int ll = 0; ll < adm; ++ll) sw[(ll * NV + v) * BT] = sw[(ll * NV + v) * BT] / sum;
     }
   };
-  if (FB && !p.wflag[c]) return;
-  bool fall = FB || !weno || !p.full[c];  // CHECKSOL: FULL = 0 -> REDUCE
+  const bool md = p.mprev != nullptr;
+  if (FB && !(MU ? p.mmus[c] : p.wflag[c])) return;
+  bool fall = FB || !weno || (!md && !p.full[c]);  // CHECKSOL: FULL = 0 -> REDUCE
   if (!CH && !fall && ISB) {
     // ---- smoothness indicators from k_wis
     const double* is = p.isb + grp * (int64_t)A * NV * 32 + lane;
@@ -1041,67 +1052,80 @@ __global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double
   }
   // CHECKSOLX (threshold 0.95) cannot fire where the 0.85 test passed on the
   // same face values
-  if (!fall) return;
+  bool mus = fall, chkx = fall;
+  if (md && !FB && weno) {  // MOOD: the fall-back only where RECALC
+    const bool reduce = fall || !p.full[c];
+    p.wflag[c] = reduce ? 1 : 0;
+    mus = reduce && p.mprev[c];
+    chkx = reduce;
+  } else if (md && FB && !MU) {
+    mus = p.mprev[c];
+  }
+  if (MU) chkx = false;
+  if (!mus && !chkx) return;
 
-  // ---- MUSCL with the central stencil polynomial (FIND_BOUNDS + Venkatakrishnan)
-  double lo[NV], hi[NV];
+  if (mus) {
+    // ---- MUSCL with the central stencil polynomial (FIND_BOUNDS + Venkatakrishnan)
+    double lo[NV], hi[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) lo[v] = hi[v] = u0[v];
-  for (int f = 0; f < nf; ++f) {
-    const int64_t nb = p.neigh[c * MF + f];
-    if (nb < 0) continue;
+    for (int v = 0; v < NV; ++v) lo[v] = hi[v] = u0[v];
+    for (int f = 0; f < nf; ++f) {
+      const int64_t nb = p.neigh[c * MF + f];
+      if (nb < 0) continue;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double un = U[nb * NV + v];
+        lo[v] = fmin(lo[v], un);
+        hi[v] = fmax(hi[v], un);
+      }
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      const double un = U[nb * NV + v];
-      lo[v] = fmin(lo[v], un);
-      hi[v] = fmax(hi[v], un);
+      lo[v] -= u0[v];
+      hi[v] -= u0[v];
     }
-  }
+    const double e3 = p.kappa_ven * p.minedge[c];
+    const double epsi2 = e3 * e3 * e3;
+    for (int v0 = 0; v0 < NV; v0 += VF) {
+      T g0[ID][VF];
+      load_poly(0, v0, g0, ID);
+      T cb[VF];
+      mean_term(g0, cb);
+      double slope[VF];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    lo[v] -= u0[v];
-    hi[v] -= u0[v];
-  }
-  const double e3 = p.kappa_ven * p.minedge[c];
-  const double epsi2 = e3 * e3 * e3;
-  for (int v0 = 0; v0 < NV; v0 += VF) {
-    T g0[ID][VF];
-    load_poly(0, v0, g0, ID);
-    T cb[VF];
-    mean_term(g0, cb);
-    double slope[VF];
+      for (int k = 0; k < VF; ++k) slope[k] = TOLBIG;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int f = 0; f < MF; ++f) {
+          const int nq = nq_of(f);
+          for (int q = 0; q < QS; ++q) {
+            T* o = out + (f * QS + q) * NV;
+            if (q >= nq) {
+              if (pass == 1)
 #pragma unroll
-    for (int k = 0; k < VF; ++k) slope[k] = TOLBIG;
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int f = 0; f < MF; ++f) {
-        const int nq = nq_of(f);
-        for (int q = 0; q < QS; ++q) {
-          T* o = out + (f * QS + q) * NV;
-          if (q >= nq) {
-            if (pass == 1)
+                for (int k = 0; k < VF; ++k)
+                  if (v0 + k < NV) o[v0 + k] = T(0);
+              continue;
+            }
+            T m[ID];
+            mono(f, q, m);
 #pragma unroll
-              for (int k = 0; k < VF; ++k)
-                if (v0 + k < NV) o[v0 + k] = T(0);
-            continue;
-          }
-          T m[ID];
-          mono(f, q, m);
+            for (int k = 0; k < VF; ++k) {
+              const int v = v0 + k;
+              if (v >= NV) continue;
+              T r = T(0);
 #pragma unroll
-          for (int k = 0; k < VF; ++k) {
-            const int v = v0 + k;
-            if (v >= NV) continue;
-            T r = T(0);
-#pragma unroll
-            for (int d = 0; d < ID; ++d) r += m[d] * g0[d][k];
-            r = r - cb[k];
-            const double dd = (u0[v] + (double)r) - u0[v];
-            if (pass == 0) slope[k] = fmin(slope[k], slope_limiter(p.limiter, dd, lo[v], hi[v], epsi2));
-            else o[v] = T((double)T(dd) * slope[k]);
+              for (int d = 0; d < ID; ++d) r += m[d] * g0[d][k];
+              r = r - cb[k];
+              const double dd = (u0[v] + (double)r) - u0[v];
+              if (pass == 0) slope[k] = fmin(slope[k], slope_limiter(p.limiter, dd, lo[v], hi[v], epsi2));
+              else o[v] = T((double)T(dd) * slope[k]);
+            }
           }
         }
       }
     }
   }
+  if (!chkx) return;
   // ---- CHECKSOLX: first order where a face value jumps by 95 %
   bool bad = false;
   for (int f = 0; f < nf; ++f) {
@@ -1282,6 +1306,11 @@ template <int P, typename T>
 cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st, int64_t* launches,
                           cudaEvent_t mark) {
   const unsigned b = (unsigned)((p.n + 127) / 128);
+  if (p.mmus) {  // the first MOOD cascade: MUSCL of the selected cells from this stage's G
+    k_wpost<P, T, false, false, true, true><<<b, 128, 0, st>>>(p, U);
+    ++*launches;
+    return cudaGetLastError();
+  }
   if (p.lsq_bulk) {  // opt-in: tables staged through shared memory (UCG_LSQ_BULK=1)
     constexpr int NSTG = 4;
     constexpr size_t smem = lsq_tma_smem<P, T, NSTG>();
@@ -1310,7 +1339,7 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     // than it saves (2.1 M-cell CWENO4: 17.3 -> 19.6 ms)
     bool done = false;
     if constexpr (P == 4) {
-      if (p.wflag && p.isb && p.scheme == 3) {
+      if (p.wface && p.isb && p.scheme == 3) {
         const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
         const size_t smem = ((size_t)MF * QS * 3 + ((QS * NV) | 1)) * 32 * sizeof(T);
         cudaFuncSetAttribute(k_wface<P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

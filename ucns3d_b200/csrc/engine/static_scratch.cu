@@ -280,7 +280,7 @@ extern "C" int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geomet
   if (!cfg || !geo || !rec || !u || !rhs) return UCG_EINVAL;
   if (cfg->scheme != 2 || cfg->iorder != 1 || cfg->ideg != 3 || cfg->admis_max != 1 || cfg->nq_quad != 1 ||
       cfg->nq_tri != 1 || cfg->limiter != 7 || cfg->riemann != 1 || (cfg->governing != 1 && cfg->governing != 2) ||
-      (cfg->boundtype != 0 && cfg->boundtype != 1))
+      (cfg->boundtype != 0 && cfg->boundtype != 1) || cfg->mood != 0)
     return UCG_EINVAL;
   const int64_t n = geo->ncells;
   if (n <= 0 || rec->first != 0 || rec->count != n || !rec->stencil || !rec->invmat) return UCG_EINVAL;

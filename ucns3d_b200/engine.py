@@ -198,6 +198,16 @@ class Engine:
         self._check(self.lib.ucg_cell_order(self._h, C.byref(ren), N.ptr(n2o, C.c_int32), N.ptr(cost, C.c_double)))
         return dict(renumbered=bool(ren.value), n2o=n2o, cost_caller=float(cost[0]), cost_rcm=float(cost[1]))
 
+    def mood_state(self) -> dict:
+        """MOOD after the last RK3 stage (cfg.mood 1): MOOD_O per cell (1
+        first order, 2 MUSCL, IORDER + 1 the target scheme) and RECALC (the
+        cells whose next reconstruction may fall back to MUSCL), in the
+        caller's cell order."""
+        order = np.empty(self.n, dtype=np.int32)
+        recalc = np.empty(self.n, dtype=np.int32)
+        self._check(self.lib.ucg_mood_state(self._h, N.ptr(order, C.c_int32), N.ptr(recalc, C.c_int32)))
+        return dict(order=order, recalc=recalc)
+
     @property
     def stream_ptr(self) -> int:
         return int(self.lib.ucg_get_stream(self._h) or 0)
