@@ -57,6 +57,9 @@ def parse():
                     help="hand the mesh over in a seeded random cell numbering (as from a partitioner) and time "
                          "it with the engine's renumbering on (the line's value) and off (shuffle.reorder_off)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--setup", action="store_true",
+                    help="also time the reconstruction-table set-up: host (ucp_prepare + upload) against the "
+                         "device (ucg_build_recon) on meshes with one matrix set per cell")
     ap.add_argument("--cpu-n", type=int, default=0,
                     help="mesh size of the CPU baseline and reference arm (0: the benchmarked --n)")
     return ap.parse_args()
@@ -524,6 +527,51 @@ def run_adjoint(local, steps=200, every=20, weno_n=32):
     return out
 
 
+def run_setup(local):
+    """Start-up time of the reconstruction tables on meshes whose cells all
+    have their own matrix sets (jittered tetrahedra): the host set-up
+    library's tables (the difference between ucp_prepare and
+    ucp_prepare_geometry, all host threads) plus their upload
+    (ucg_upload_recon), against ucg_build_recon on the device; wall-clock
+    seconds of each synchronous call, and whether the residuals agree bit
+    for bit."""
+    import os
+    import numpy as np
+    from ucns3d_b200.config import make_config, EULER
+    from ucns3d_b200.engine import Engine
+    from ucns3d_b200.mesh import IC_TGV, SCHEME_WENO, Mesh
+    out = []
+    for name, mk, io in (("tets 16^3x6, WENO5", lambda: Mesh.box_tet(16, 16, 16, seed=7), 4),
+                         ("tets 24^3x6, WENO3", lambda: Mesh.box_tet(24, 24, 24, seed=7), 2)):
+        mg, mh = mk(), mk()
+        t0 = time.perf_counter()
+        mg.prepare(SCHEME_WENO, io, tables=False)
+        t1 = time.perf_counter()
+        mh.prepare(SCHEME_WENO, io)
+        t2 = time.perf_counter()
+        cfg = make_config(mh, governing=EULER)
+        U = mh.initial_condition(IC_TGV, [1.4, 5.0, 1.0])
+        eh, ed = Engine(mh, cfg, device=local, upload=False), Engine(mg, cfg, device=local, upload=False)
+        eh.upload_geometry(mh.geometry_struct())
+        ed.upload_geometry(mg.geometry_struct())
+        t3 = time.perf_counter()
+        eh.upload_recon(mh.recon_struct())
+        t4 = time.perf_counter()
+        ed.build_recon(mg.shapes_struct(), mg.recon_struct())
+        t5 = time.perf_counter()
+        res = []
+        for e in (eh, ed):
+            e.set_state(U)
+            res.append(e.call_flux_subroutines_3d())
+            e.close()
+        host_tables = (t2 - t1) - (t1 - t0)
+        out.append({"workload": name, "cells": mh.ncells, "matrix_sets": mh.ntables, "host_threads": os.cpu_count(),
+                    "host_tables_s": host_tables, "upload_s": t4 - t3, "host_total_s": host_tables + (t4 - t3),
+                    "device_build_s": t5 - t4, "speedup": (host_tables + (t4 - t3)) / (t5 - t4),
+                    "residual_bitwise_equal": bool(np.array_equal(res[0], res[1]))})
+    return out
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
@@ -629,6 +677,8 @@ def main():
         out["accuracy"] = run_accuracy(c32, local, acc_steps)
     if not args.no_adjoint:
         out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
+    if args.setup:
+        out["setup"] = run_setup(local)
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_sample(args, case=c32 if not args.cpu_n else None)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",

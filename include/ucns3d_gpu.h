@@ -153,7 +153,8 @@ typedef struct ucg_geometry {
   const double* volume;       /* [n]      TOTVOLUME                                     */
   const double* minedge;      /* [n]      MINEDGE                                       */
   const double* invccjac;     /* [n][3][3] INVCCJAC                                     */
-  const double* basis_mean;   /* [n][ideg] INTEG_BASIS / VOLUME(1,1): basis cell means  */
+  const double* basis_mean;   /* [n][ideg] INTEG_BASIS / VOLUME(1,1): basis cell means
+                                 (NULL if ucg_build_recon forms them)                 */
   const int32_t* admis;       /* [n]      ADMIS                                         */
   const int32_t* full;        /* [n]      FULL                                          */
 } ucg_geometry;
@@ -178,6 +179,30 @@ typedef struct ucg_recon {
   const double* indicator2;   /* [ntab][ideg2][ideg2] INDICATORC (CWENO) or NULL       */
 } ucg_recon;
 
+/* Cell shapes for building the tables of ucg_recon on the device
+ * (ucg_build_recon), in the caller's cell order.  Vertices are the cell's
+ * nodes as seen from the cell (a periodic mesh gives each cell its own
+ * unwrapped copy); the reference frame of cell c maps x to
+ * INVCCJAC(c) (x - frame_origin(c)) and has Jacobian determinant
+ * frame_det(c) (VEXT(1,:) and the determinant of the cell's mapping,
+ * src/prestore.f90:167-260).                                                */
+typedef struct ucg_shapes {
+  int64_t ncells;
+  const int32_t* shape;        /* [n]       ISHAPE: 1 hexahedron, 2 tetrahedron,
+                                  3 pyramid, 4 prism                            */
+  const double* vertices;      /* [n][8][3] nodes (hexahedron: hexaVOLUME order,
+                                  src/grid_t.f90:662-669; prism: bottom 0-2, top
+                                  3-5; pyramid: base 0-3, apex 4)             */
+  const double* centre;        /* [n][3]    cell centres                        */
+  const double* volume;        /* [n]       TOTVOLUME                           */
+  const double* frame;         /* [n][3][3] INVCCJAC (as ucg_geometry.invccjac) */
+  const double* frame_origin;  /* [n][3]                                        */
+  const double* frame_det;     /* [n]                                           */
+  double period[3];            /* box length of each periodic direction, 0 where
+                                  the mesh is not periodic (stencil members are
+                                  moved to the cell's periodic image)           */
+} ucg_shapes;
+
 typedef struct ucg_engine ucg_engine;
 
 /* Create an engine on CUDA device `device` for meshes of `ncells` cells. */
@@ -189,6 +214,24 @@ void ucg_destroy(ucg_engine* e);
  * ucg_upload_recon before ucg_upload_geometry returns UCG_ESTATE. */
 int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g);
 int ucg_upload_recon(ucg_engine* e, const ucg_recon* r);
+/* The reconstruction tables built on the device instead of uploaded:
+ * the basis means of every cell, and per matrix set (r->table_id, as from
+ * ucp_prepare_geometry, or one set per cell when NULL) the pseudo-inverses
+ * of every stencil of the set's first cell (PRESTORE_RECONSTRUCTION3,
+ * src/prestore.f90:167-818: moments of the stencil cells in the cell's
+ * frame, the normal matrix, its inverse by Householder QR, QRDECOMPOSITION +
+ * INVERT of src/matrix.f90:93-150) and its smoothness matrices
+ * (INDICATORMATRIX, src/prestore.f90:1529-1673).  The quadrature, the
+ * operations and their order are those of the host set-up library
+ * (ucp_prepare), without fused multiply-adds on either side, so the tables
+ * are ucp_prepare's bit for bit.  r: all cells (first 0, count n), stencil
+ * and table_id / ntables as in ucg_recon; the matrix pointers are ignored.
+ * Replaces ucg_upload_recon and the basis_mean of ucg_upload_geometry
+ * (which may then be NULL).  Synchronous.  Device memory beyond the
+ * handle's own while it runs: the shapes (about 300 bytes per cell) and a
+ * staging buffer of at most 512 MiB.  UCG_EINVAL also when a normal matrix
+ * is singular. */
+int ucg_build_recon(ucg_engine* e, const ucg_shapes* s, const ucg_recon* r);
 
 /* Conserved state U_C(I)%VAL(1,1:5), [n][5]. */
 int ucg_set_state(ucg_engine* e, const double* u, int64_t n);

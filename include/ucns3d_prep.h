@@ -75,6 +75,13 @@ typedef struct ucp_scheme {
 
 /* Connectivity, geometry, stencils and tables for the given scheme.        */
 int32_t ucp_prepare(ucp_mesh* m, const ucp_scheme* s);
+/* The same without the tables (basis means, pseudo-inverses, smoothness
+ * matrices): ucp_geometry then gives basis_mean NULL and ucp_recon only
+ * the stencils; the engine builds the tables with ucg_build_recon from
+ * ucp_shapes.                                                              */
+int32_t ucp_prepare_geometry(ucp_mesh* m, const ucp_scheme* s);
+/* Pointers into the mesh for ucg_build_recon (valid until ucp_free).       */
+int32_t ucp_shapes(const ucp_mesh* m, ucg_shapes* out);
 
 int64_t ucp_ncells(const ucp_mesh* m);
 /* Sizes and face weights to copy into ucg_config.                          */

@@ -73,6 +73,15 @@ class UcgRecon(C.Structure):
     ]
 
 
+class UcgShapes(C.Structure):
+    _fields_ = [
+        ("ncells", C.c_int64),
+        ("shape", _i32p), ("vertices", _f64p), ("centre", _f64p), ("volume", _f64p),
+        ("frame", _f64p), ("frame_origin", _f64p), ("frame_det", _f64p),
+        ("period", C.c_double * 3),
+    ]
+
+
 class UcpScheme(C.Structure):
     _fields_ = [("scheme", C.c_int32), ("iorder", C.c_int32), ("ees", C.c_int32),
                 ("nthreads", C.c_int32)]
@@ -112,6 +121,10 @@ def prep() -> C.CDLL:
         lib.ucp_write_grid.argtypes = [vp, C.c_char_p]
         lib.ucp_prepare.restype = C.c_int32
         lib.ucp_prepare.argtypes = [vp, C.POINTER(UcpScheme)]
+        lib.ucp_prepare_geometry.restype = C.c_int32
+        lib.ucp_prepare_geometry.argtypes = [vp, C.POINTER(UcpScheme)]
+        lib.ucp_shapes.restype = C.c_int32
+        lib.ucp_shapes.argtypes = [vp, C.POINTER(UcgShapes)]
         lib.ucp_ncells.restype = C.c_int64
         lib.ucp_ncells.argtypes = [vp]
         lib.ucp_ntables.restype = C.c_int64
@@ -141,7 +154,7 @@ ENGINE_SYMBOLS = [
     "ucg_time_kernels", "ucg_get_stream", "ucg_launch_count", "ucg_device_bytes", "ucg_last_error",
     "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
-    "ucg_set_wait_limit",
+    "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon",
 ]
 
 
@@ -213,6 +226,8 @@ def engine() -> C.CDLL:
         lib.ucg_cell_order.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _f64p]
         lib.ucg_mood_state.restype = C.c_int
         lib.ucg_mood_state.argtypes = [vp, _i32p, _i32p]
+        lib.ucg_build_recon.restype = C.c_int
+        lib.ucg_build_recon.argtypes = [vp, C.POINTER(UcgShapes), C.POINTER(UcgRecon)]
         lib.ucg_tangent_run.restype = C.c_int
         lib.ucg_tangent_run.argtypes = [vp, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
         _engine = lib

@@ -37,12 +37,15 @@ def _stale(out, srcs):
 def build_prep(force=False):
     src = os.path.join(PKG, "csrc", "prep", "prep.cpp")
     out = os.path.join(LIB, "libucns3d_prep.so")
-    deps = [src, os.path.join(INC, "ucns3d_prep.h"), os.path.join(INC, "ucns3d_gpu.h")]
+    deps = [src, os.path.join(INC, "ucns3d_prep.h"), os.path.join(INC, "ucns3d_gpu.h"),
+            os.path.join(PKG, "csrc", "common", "rules.h")]
     if force or _stale(out, deps):
         os.makedirs(LIB, exist_ok=True)
-        # the system g++ (the environment's CXX wrapper has no OpenMP runtime)
-        _run(["g++", "-O3", "-march=x86-64-v2", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-I", INC, src,
-              "-o", out])
+        # the system g++ (the environment's CXX wrapper has no OpenMP runtime);
+        # no contracted multiply-adds, like the device set-up (setup.cu), so
+        # both give the same tables bit for bit
+        _run(["g++", "-O3", "-march=x86-64-v2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-std=c++17",
+              "-I", INC, src, "-o", out])
     return out
 
 
@@ -50,8 +53,11 @@ def build_prep(force=False):
 # the reconstruction kernels are split by precision and order because the
 # IORDER 4 instantiations dominate the compile time
 ENGINE_TUS = ("recon_char_p4.cu", "recon_f64_p4.cu", "recon_f32_p4.cu", "recon_char.cu", "recon_f64.cu", "recon_f32.cu",
-              "adjoint_weno.cu", "adjoint.cu", "engine.cu", "static_scratch.cu")
-ENGINE_HDRS = ("kernels.cuh", "recon2.cuh", "device.cuh", "ad.cuh", "engine_internal.h")
+              "adjoint_weno.cu", "adjoint.cu", "engine.cu", "static_scratch.cu", "setup.cu")
+ENGINE_HDRS = ("kernels.cuh", "recon2.cuh", "device.cuh", "ad.cuh", "engine_internal.h", "expand.cuh", "../common/rules.h")
+# per-unit flags: the device set-up evaluates the host set-up's operations
+# one by one (no fused multiply-adds), so its tables match bit for bit
+ENGINE_TU_FLAGS = {"setup.cu": ["-fmad=false"]}
 
 
 def build_engine(force=False, extra=()):
@@ -67,7 +73,7 @@ def build_engine(force=False, extra=()):
         for tu in ENGINE_TUS:
             obj = os.path.join(objdir, tu.replace(".cu", ".o"))
             cmd = [NVCC, *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INC, *extra,
-                   "-c", os.path.join(d, tu), "-o", obj]
+                   *ENGINE_TU_FLAGS.get(tu, []), "-c", os.path.join(d, tu), "-o", obj]
             print(" ".join(cmd), flush=True)
             procs.append((subprocess.Popen(cmd), cmd))
             objs.append(obj)

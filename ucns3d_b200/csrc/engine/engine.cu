@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -614,7 +615,7 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   if (!e || !g) return fail(e, UCG_EINVAL, "null argument");
   if (g->ncells != e->n) return fail(e, UCG_EINVAL, "geometry has " + std::to_string(g->ncells) + " cells, engine " + std::to_string(e->n));
   if (!g->nfaces || !g->face_type || !g->neigh || !g->neigh_face || !g->bc || !g->qperm || !g->face_angle ||
-      !g->face_area || !g->dih || !g->qpoints || !g->volume || !g->minedge || !g->invccjac || !g->basis_mean ||
+      !g->face_area || !g->dih || !g->qpoints || !g->volume || !g->minedge || !g->invccjac ||
       !g->admis || !g->full)
     return fail(e, UCG_EINVAL, "a geometry array is NULL");
   cudaSetDevice(e->device);
@@ -761,7 +762,8 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
       for (int q = 0; q < QS; ++q)
         for (int k = 0; k < 3; ++k)
           qp[(size_t)((gq + (f * QS + q) * 3 + k) * 32 + ln)] = g->qpoints[((o * MF + f) * UCG_MAX_QP + q) * 3 + k];
-    for (int d = 0; d < ideg; ++d) bm[(size_t)((gb + d) * 32 + ln)] = g->basis_mean[(size_t)o * ideg + d];
+    if (g->basis_mean)  // else formed by ucg_build_recon
+      for (int d = 0; d < ideg; ++d) bm[(size_t)((gb + d) * 32 + ln)] = g->basis_mean[(size_t)o * ideg + d];
   }
   if (e->mixed) {
     std::vector<float> qf(qp.begin(), qp.end()), bf(bm.begin(), bm.end());
@@ -783,29 +785,25 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   return UCG_OK;
 }
 
-int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
-  if (!e || !r) return fail(e, UCG_EINVAL, "null argument");
+}  // extern "C"
+
+// The stencils of cells [first, first + count) (caller order): checked,
+// mapped to device numbering, interleaved on the device; the table buffers
+// allocated.  rowbuf/d_rowmap (renumbered engines): the device cell that
+// takes each row of this upload, for the table expansion; the caller
+// releases rowbuf.
+int ucg_host::upload_stencils(ucg_engine* e, int64_t first, int64_t count, const int32_t* stencil, DevBuf& rowbuf,
+                              const int32_t** d_rowmap) {
   const ucg_config& c = e->cfg;
-  if (r->first < 0 || r->count <= 0 || r->first + r->count > e->n) return fail(e, UCG_EINVAL, "cell range out of bounds");
-  if (!r->stencil || !r->invmat) return fail(e, UCG_EINVAL, "stencil and invmat are required");
-  const bool weno = c.scheme == 3, cw = c.ees == 5;
-  if (weno && !r->indicator) return fail(e, UCG_EINVAL, "WENO needs the INDICATOR matrices");
-  if (cw && (!r->invmat2 || !r->indicator2)) return fail(e, UCG_EINVAL, "CWENO needs invmat2 and INDICATORC");
-  if (!e->have_geometry) return fail(e, UCG_ESTATE, "upload the geometry before the reconstruction tables");
-  cudaSetDevice(e->device);
-  const int64_t n = e->n, first = r->first, count = r->count;
+  const int64_t n = e->n;
   const int A = c.admis_max, W = c.imax + 1;
-  const int64_t ntab = r->table_id ? r->ntables : count;
-  if (r->table_id) {
-    if (ntab <= 0) return fail(e, UCG_EINVAL, "ntables must be positive with table_id");
-    for (int64_t i = 0; i < count; ++i)
-      if (r->table_id[i] < 0 || r->table_id[i] >= ntab) return fail(e, UCG_EINVAL, "table_id out of range");
-  }
+  const bool cw = c.ees == 5, weno = c.scheme == 3;
+  *d_rowmap = nullptr;
   for (int64_t i = 0; i < count; ++i) {
     int64_t cell = first + i;
     for (int ll = 0; ll < A; ++ll)
       for (int k = 0; k < W; ++k) {
-        int32_t y = r->stencil[(i * A + ll) * W + k];
+        int32_t y = stencil[(i * A + ll) * W + k];
         if (y >= n || y < -1) return fail(e, UCG_EINVAL, "stencil index out of range at cell " + std::to_string(cell));
         // rows 1..nk of the admissible stencils are read by the kernels
         const int nk = cw && ll > 0 ? c.imax2 : c.imax;
@@ -813,25 +811,23 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
           return fail(e, UCG_EINVAL, "unused slot (-1) inside admissible stencil " + std::to_string(ll) + " of cell " +
                                          std::to_string(cell));
       }
-    if (r->stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
+    if (stencil[i * A * W] != cell) return fail(e, UCG_EINVAL, "stencil slot 0 must be the cell itself");
   }
   // stencil indices in device numbering, and which device cell takes each
   // row of this upload (renumbered engines only)
   const bool perm = !e->o2n.empty();
   std::vector<int32_t> sten_dev;
-  const int32_t* sten = r->stencil;
-  DevBuf rowbuf;
-  const int32_t* d_rowmap = nullptr;
+  const int32_t* sten = stencil;
   if (perm) {
     sten_dev.resize((size_t)count * A * W);
-    for (size_t j = 0; j < sten_dev.size(); ++j) sten_dev[j] = r->stencil[j] >= 0 ? e->o2n[r->stencil[j]] : -1;
+    for (size_t j = 0; j < sten_dev.size(); ++j) sten_dev[j] = stencil[j] >= 0 ? e->o2n[stencil[j]] : -1;
     sten = sten_dev.data();
     std::vector<int32_t> rowmap(n, -1);
     for (int64_t i = 0; i < count; ++i) rowmap[e->o2n[first + i]] = (int32_t)i;
     CK(cudaMalloc(&rowbuf.p, (size_t)n * 4));
     CK(cudaMemcpyAsync(rowbuf.p, rowmap.data(), (size_t)n * 4, cudaMemcpyHostToDevice, e->stream));
     CK(cudaStreamSynchronize(e->stream));
-    d_rowmap = (const int32_t*)rowbuf.p;
+    *d_rowmap = (const int32_t*)rowbuf.p;
   }
   auto dcell = [&](int64_t o) -> int64_t { return perm ? e->o2n[o] : o; };
   if (c.scheme == 2 && c.iorder == 1) {  // first stencil kept on the host for the adjoint's reverse map
@@ -847,26 +843,114 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   rc = rc ? rc : alloc(e, e->sten, (size_t)ngrp * 32 * A * W * 4);
   rc = rc ? rc : alloc(e, e->invmat, (size_t)ngrp * 32 * Ly.tstride * T);
   if (weno) rc = rc ? rc : alloc(e, e->ind, (size_t)ngrp * 32 * Ly.istride * T);
+  if (rc) return rc;
+  // stencils: staged per cell, interleaved on the device
+  rc = alloc(e, e->staging, (size_t)count * A * W * 4);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(e->staging.p, sten, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
+  int64_t total = (perm ? n : count) * A * W;
+  unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
+  k_expand_il<int32_t, int32_t, 1><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
+                                                              nullptr, first, count, (int64_t)A * W, 0, count,
+                                                              *d_rowmap, n);
+  e->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+// The matrix sets of tables [0, ntab) into the engine's interleaved tables
+// for cells [first, first + count): `fill(which, t0, t1, staging)` writes
+// the FP64 blocks of tables [t0, t1) into the device staging buffer, the
+// pseudo-inverses (which 0, Layout::tstride each: stencil ll's rows at
+// soff[ll]) or the packed smoothness matrices (which 1, Layout::istride
+// each); they are expanded per cell (d_tid: cell -> table, NULL = the
+// cell's own row), pseudo-inverses element by element, smoothness matrices
+// by 16-byte vectors, in 512 MiB chunks.
+int ucg_host::expand_tables(ucg_engine* e, int64_t first, int64_t count, int64_t ntab, const int32_t* d_tid,
+                            const int32_t* d_rowmap, const std::function<int(int, int64_t, int64_t, double*)>& fill) {
+  const Layout& Ly = e->layout;
+  const int64_t n = e->n;
+  const bool perm = !e->o2n.empty();
+  struct Part {
+    int64_t len;
+    DevBuf* dst;
+    int which;
+  } parts[2] = {{Ly.tstride, &e->invmat, 0}, {e->cfg.scheme == 3 ? Ly.istride : 0, &e->ind, 1}};
+  const size_t stage_bytes = (size_t)512 << 20;
+  for (auto& pt : parts) {
+    if (pt.len == 0) continue;
+    int64_t per = (int64_t)(stage_bytes / (pt.len * 8));
+    if (per < 1) per = 1;
+    for (int64_t t0 = 0; t0 < ntab; t0 += per) {
+      int64_t t1 = t0 + per < ntab ? t0 + per : ntab;
+      size_t bytes = (size_t)(t1 - t0) * pt.len * 8;
+      int rc = alloc(e, e->staging, bytes);
+      if (rc) return rc;
+      rc = fill(pt.which, t0, t1, (double*)e->staging.p);
+      if (rc) return rc;
+      int64_t total = (perm ? n : count) * pt.len;
+      unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
+      const double* sp = (const double*)e->staging.p;
+      if (e->mixed) {
+        if (pt.which == 0)
+          k_expand_il<float, double, 1><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
+        else
+          k_expand_il<float, double, 4><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
+      } else {
+        if (pt.which == 0)
+          k_expand_il<double, double, 1><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
+        else
+          k_expand_il<double, double, 2><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
+      }
+      e->launches++;
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(e->stream));
+    }
+  }
+  e->bytes -= (int64_t)e->staging.bytes;
+  release(e->staging);
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+// cells [first, first + count) have their tables
+void ucg_host::mark_recon(ucg_engine* e, int64_t first, int64_t count) {
+  int64_t newly = 0;
+  for (int64_t i = 0; i < count; ++i)
+    if (!e->recon_done[first + i]) {
+      e->recon_done[first + i] = 1;
+      ++newly;
+    }
+  e->recon_cells += newly;
+}
+
+extern "C" {
+
+int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
+  if (!e || !r) return fail(e, UCG_EINVAL, "null argument");
+  const ucg_config& c = e->cfg;
+  if (r->first < 0 || r->count <= 0 || r->first + r->count > e->n) return fail(e, UCG_EINVAL, "cell range out of bounds");
+  if (!r->stencil || !r->invmat) return fail(e, UCG_EINVAL, "stencil and invmat are required");
+  const bool weno = c.scheme == 3, cw = c.ees == 5;
+  if (weno && !r->indicator) return fail(e, UCG_EINVAL, "WENO needs the INDICATOR matrices");
+  if (cw && (!r->invmat2 || !r->indicator2)) return fail(e, UCG_EINVAL, "CWENO needs invmat2 and INDICATORC");
+  if (!e->have_geometry) return fail(e, UCG_ESTATE, "upload the geometry before the reconstruction tables");
+  cudaSetDevice(e->device);
+  const int64_t first = r->first, count = r->count;
+  const int A = c.admis_max;
+  const int64_t ntab = r->table_id ? r->ntables : count;
+  if (r->table_id) {
+    if (ntab <= 0) return fail(e, UCG_EINVAL, "ntables must be positive with table_id");
+    for (int64_t i = 0; i < count; ++i)
+      if (r->table_id[i] < 0 || r->table_id[i] >= ntab) return fail(e, UCG_EINVAL, "table_id out of range");
+  }
+  DevBuf rowbuf;
+  const int32_t* d_rowmap = nullptr;
+  int rc = upload_stencils(e, first, count, r->stencil, rowbuf, &d_rowmap);
   if (rc) {
     release(rowbuf);
     return rc;
-  }
-  {
-    // stencils: staged per cell, interleaved on the device
-    rc = alloc(e, e->staging, (size_t)count * A * W * 4);
-    if (rc) {
-      release(rowbuf);
-      return rc;
-    }
-    CK(cudaMemcpyAsync(e->staging.p, sten, (size_t)count * A * W * 4, cudaMemcpyHostToDevice, e->stream));
-    int64_t total = (perm ? n : count) * A * W;
-    unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
-    k_expand_il<int32_t, int32_t, 1><<<blocks, 256, 0, e->stream>>>((int32_t*)e->sten.p, (const int32_t*)e->staging.p,
-                                                                nullptr, first, count, (int64_t)A * W, 0, count,
-                                                                d_rowmap, n);
-    e->launches++;
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(e->stream));
   }
   DevBuf tidbuf;
   int32_t* d_tid = nullptr;
@@ -877,6 +961,7 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
   }
   // pack matrix sets into the engine's per-cell block layout on the host
   // (FP64, padding zeroed), stage them in chunks, expand per cell on the GPU
+  const Layout& Ly = e->layout;
   const int ideg = c.ideg, imax = c.imax, ideg2 = c.ideg2, imax2 = c.imax2;
   const int vec = e->mixed ? 4 : 2;  // elements per 16-byte vector on the device
   auto pack_mat = [&](int64_t t, double* dst) {
@@ -904,66 +989,22 @@ int ucg_upload_recon(ucg_engine* e, const ucg_recon* r) {
     pack_tri(r->indicator + t * ideg * ideg, ideg, dst);
     if (cw) pack_tri(r->indicator2 + t * ideg2 * ideg2, ideg2, dst + Ly.i2off);
   };
-  struct Part {
-    int64_t len;
-    DevBuf* dst;
-    int which;
-  } parts[2] = {{Ly.tstride, &e->invmat, 0}, {weno ? Ly.istride : 0, &e->ind, 1}};
-  // pseudo-inverses interleaved element by element, smoothness matrices by
-  // 16-byte vectors
-  const size_t stage_bytes = (size_t)512 << 20;
   std::vector<double> host;
-  for (auto& pt : parts) {
-    if (pt.len == 0) continue;
-    int64_t per = (int64_t)(stage_bytes / (pt.len * 8));
-    if (per < 1) per = 1;
-    for (int64_t t0 = 0; t0 < ntab; t0 += per) {
-      int64_t t1 = t0 + per < ntab ? t0 + per : ntab;
-      size_t bytes = (size_t)(t1 - t0) * pt.len * 8;
-      host.resize((size_t)(t1 - t0) * pt.len);
-      for (int64_t t = t0; t < t1; ++t) {
-        double* d = host.data() + (t - t0) * pt.len;
-        if (pt.which == 0) pack_mat(t, d);
-        else pack_ind(t, d);
-      }
-      rc = alloc(e, e->staging, bytes);
-      if (rc) {
-        if (tidbuf.p) cudaFree(tidbuf.p);
-        release(rowbuf);
-        return rc;
-      }
-      CK(cudaMemcpyAsync(e->staging.p, host.data(), bytes, cudaMemcpyHostToDevice, e->stream));
-      int64_t total = (perm ? n : count) * pt.len;
-      unsigned blocks = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 64);
-      const double* sp = (const double*)e->staging.p;
-      if (e->mixed) {
-        if (pt.which == 0)
-          k_expand_il<float, double, 1><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
-        else
-          k_expand_il<float, double, 4><<<blocks, 256, 0, e->stream>>>((float*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
-      } else {
-        if (pt.which == 0)
-          k_expand_il<double, double, 1><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
-        else
-          k_expand_il<double, double, 2><<<blocks, 256, 0, e->stream>>>((double*)pt.dst->p, sp, d_tid, first, count, pt.len, t0, t1, d_rowmap, n);
-      }
-      e->launches++;
-      CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(e->stream));
+  rc = expand_tables(e, first, count, ntab, d_tid, d_rowmap, [&](int which, int64_t t0, int64_t t1, double* dev) {
+    const int64_t len = which == 0 ? Ly.tstride : Ly.istride;
+    host.resize((size_t)(t1 - t0) * len);
+    for (int64_t t = t0; t < t1; ++t) {
+      double* d = host.data() + (t - t0) * len;
+      if (which == 0) pack_mat(t, d);
+      else pack_ind(t, d);
     }
-  }
+    CK(cudaMemcpyAsync(dev, host.data(), host.size() * 8, cudaMemcpyHostToDevice, e->stream));
+    return (int)UCG_OK;
+  });
   if (tidbuf.p) cudaFree(tidbuf.p);
   release(rowbuf);
-  e->bytes -= (int64_t)e->staging.bytes;
-  release(e->staging);
-  CK(cudaStreamSynchronize(e->stream));
-  int64_t newly = 0;
-  for (int64_t i = 0; i < count; ++i)
-    if (!e->recon_done[first + i]) {
-      e->recon_done[first + i] = 1;
-      ++newly;
-    }
-  e->recon_cells += newly;
+  if (rc) return rc;
+  mark_recon(e, first, count);
   return UCG_OK;
 }
 

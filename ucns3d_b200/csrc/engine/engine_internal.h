@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -105,6 +106,14 @@ int rk3(ucg_engine* e, double dt, bool dt_dev);
 // both leave the copy queued on the handle's stream
 int cells_in(ucg_engine* e, double* dev_dst, const double* host_src);
 int cells_out(ucg_engine* e, double* host_dst, const double* dev_src);
+// reconstruction tables (engine.cu): stencil upload, staged expansion of
+// per-table FP64 blocks, bookkeeping; the device set-up (setup.cu) fills
+// the staging buffer itself
+int upload_stencils(ucg_engine* e, int64_t first, int64_t count, const int32_t* stencil, DevBuf& rowbuf,
+                    const int32_t** d_rowmap);
+int expand_tables(ucg_engine* e, int64_t first, int64_t count, int64_t ntab, const int32_t* d_tid,
+                  const int32_t* d_rowmap, const std::function<int(int, int64_t, int64_t, double*)>& fill);
+void mark_recon(ucg_engine* e, int64_t first, int64_t count);
 // frees the adjoint buffers (adjoint.cu)
 void adjoint_release(ucg_engine* e);
 // reverse of the WENO post-processing and least squares (adjoint_weno.cu)

@@ -19,6 +19,7 @@
 //   admissible stencils, FULL        STENCILS           src/grid_p.f90:6452-6554
 //   initial condition averages       INITIALISE         src/init_p.f90:14, profile.f90:253
 #include "ucns3d_prep.h"
+#include "../common/rules.h"
 
 #include <algorithm>
 #include <array>
@@ -49,103 +50,12 @@ inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
 inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
 
-// ---------------------------------------------------------------- topology
-// Shapes use UCNS3D's ISHAPE codes: 1 hexahedron, 2 tetrahedron,
-// 3 pyramid, 4 prism.  Node numbering of the hexahedron is that of
-// hexaVOLUME (src/grid_t.f90:662-669); prisms have nodes 0-2 at the bottom
-// and 3-5 above them; pyramids have the base 0-3 and apex 4.
-struct Topo {
-  int nv, nf;
-  int fnv[6];
-  int fv[6][4];
-  int ntet;
-  int tet[6][4];
-};
-
-const Topo& topo(int type) {
-  static const Topo hex = {8, 6, {4, 4, 4, 4, 4, 4},
-                           {{0, 3, 2, 1}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {0, 4, 7, 3}},
-                           6,
-                           // DECOMPOSE3 case(1), 0-based
-                           {{0, 5, 7, 4}, {0, 1, 7, 5}, {1, 6, 7, 5}, {0, 7, 2, 3}, {0, 7, 1, 2}, {1, 7, 6, 2}}};
-  static const Topo tet = {4, 4, {3, 3, 3, 3, 0, 0},
-                           {{1, 2, 3, 0}, {0, 3, 2, 0}, {0, 1, 3, 0}, {0, 2, 1, 0}, {0}, {0}},
-                           1,
-                           {{0, 1, 2, 3}}};
-  static const Topo pyr = {5, 5, {4, 3, 3, 3, 3, 0},
-                           {{0, 3, 2, 1}, {0, 1, 4, 0}, {1, 2, 4, 0}, {2, 3, 4, 0}, {3, 0, 4, 0}, {0}},
-                           2,
-                           {{0, 1, 2, 4}, {0, 2, 3, 4}}};
-  static const Topo pri = {6, 5, {3, 3, 4, 4, 4, 0},
-                           {{0, 2, 1, 0}, {3, 4, 5, 0}, {0, 1, 4, 3}, {1, 2, 5, 4}, {2, 0, 3, 5}, {0}},
-                           3,
-                           {{0, 1, 2, 5}, {0, 1, 5, 4}, {0, 4, 5, 3}}};
-  switch (type) {
-    case 1: return hex;
-    case 2: return tet;
-    case 3: return pyr;
-    default: return pri;
-  }
-}
-
-// ------------------------------------------------------------ quadrature
-// Gauss-Legendre nodes/weights on [-1,1] by Newton iteration.
-void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
-  x.assign(n, 0.0);
-  w.assign(n, 0.0);
-  for (int i = 0; i < n; ++i) {
-    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5));
-    for (int it = 0; it < 100; ++it) {
-      double p0 = 1.0, p1 = z;
-      for (int k = 2; k <= n; ++k) {
-        double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
-        p0 = p1;
-        p1 = p2;
-      }
-      if (n == 1) { p1 = z; p0 = 1.0; }
-      double dp = n * (z * p1 - p0) / (z * z - 1.0);
-      double dz = p1 / dp;
-      z -= dz;
-      if (std::fabs(dz) < 1e-16) break;
-    }
-    double p0 = 1.0, p1 = z;
-    for (int k = 2; k <= n; ++k) {
-      double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
-      p0 = p1;
-      p1 = p2;
-    }
-    if (n == 1) { p0 = 1.0; p1 = z; }
-    double dp = n * (z * p1 - p0) / (z * z - 1.0);
-    x[i] = -z;
-    w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
-  }
-  if (n == 1) { x[0] = 0.0; w[0] = 2.0; }
-}
-
-// Collapsed (conical product) rule on the unit tetrahedron; points in
-// barycentric-free form (xi, eta, zeta), weights summing to 1.  Exact for
-// polynomials of degree <= 2n-3.
-struct TetRule {
-  std::vector<std::array<double, 3>> p;
-  std::vector<double> w;
-};
-TetRule tet_rule(int n) {
-  std::vector<double> gx, gw;
-  gauss_legendre(n, gx, gw);
-  TetRule r;
-  double sum = 0.0;
-  for (int a = 0; a < n; ++a)
-    for (int b = 0; b < n; ++b)
-      for (int c = 0; c < n; ++c) {
-        double u = 0.5 * (gx[a] + 1.0), v = 0.5 * (gx[b] + 1.0), t = 0.5 * (gx[c] + 1.0);
-        double wt = 0.125 * gw[a] * gw[b] * gw[c] * (1.0 - u) * (1.0 - u) * (1.0 - v);
-        r.p.push_back({u, (1.0 - u) * v, (1.0 - u) * (1.0 - v) * t});
-        r.w.push_back(wt);
-        sum += wt;
-      }
-  for (auto& x : r.w) x /= sum;
-  return r;
-}
+// topology, volume quadrature, monomial order: ../common/rules.h
+using ucrules::Topo;
+using ucrules::topo;
+using ucrules::gauss_legendre;
+using ucrules::TetRule;
+using ucrules::tet_rule;
 
 // Face rules.  Quadrilaterals: tensor Gauss-Legendre with n = IGQRULES per
 // direction, weights w_i w_j / 4 (QUADRATUREQUAD3D).  Triangles: the
@@ -206,19 +116,9 @@ FaceRule tri_rule(int ig) {
   return r;
 }
 
-// ------------------------------------------------------------ monomials
-// Basis ordering of BASIS_REC (src/basis.f90:24-100): degree by degree; in
-// a degree, powers of z ascending, then powers of y ascending.
-struct Mono {
-  int e[3];
-};
-std::vector<Mono> monomials(int order) {
-  std::vector<Mono> m;
-  for (int n = 1; n <= order; ++n)
-    for (int c = 0; c <= n; ++c)
-      for (int b = 0; b <= n - c; ++b) m.push_back({{n - c - b, b, c}});
-  return m;
-}
+using ucrules::Mono;
+using ucrules::monomials;
+
 inline double ipow(double x, int e) {
   double r = 1.0;
   for (int i = 0; i < e; ++i) r *= x;
@@ -325,6 +225,8 @@ struct ucp_mesh {
   int box_bc[6] = {0, 0, 0, 0, 0, 0};
   double box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
   bool prepared = false;
+  bool tables = false;          // basis means and matrix sets built (ucp_prepare)
+  std::vector<int32_t> shape32; // ISHAPE per cell as int32 (ucp_shapes)
   SchemeSizes sz;
   // derived geometry
   std::vector<double> centre;   // [nc][3]
@@ -868,28 +770,14 @@ inline uint64_t mix64(uint64_t h, uint64_t v) {
   return h;
 }
 
-bool build_tables(ucp_mesh& m) {
+// Matrix sets shared by cells whose stencils look the same: keys from the
+// stencil members' shapes and vertex positions relative to the cell
+// (quantised at 1e-9 of the cell size); table_id[c] numbers the sets in
+// the order of the first cell that uses each, rep[t] = that cell.
+void assign_tables(ucp_mesh& m, std::vector<int64_t>& rep) {
   SchemeSizes& s = m.sz;
   const int64_t nc = m.nc;
   const int W = s.imax + 1;
-  const int ideg = s.ideg;
-  std::vector<Mono> mono = monomials(s.iorder);
-  TetRule Rm = tet_rule(std::max(2, (s.iorder + 4) / 2));
-  TetRule Ri = tet_rule(std::max(2, (2 * s.iorder + 2) / 2 + 1));
-  m.basis_mean.assign(nc * ideg, 0.0);
-  // frames + cell means
-  std::vector<Frame> frames(nc);
-#pragma omp parallel for schedule(static)
-  for (int64_t c = 0; c < nc; ++c) {
-    Frame& F = frames[c];
-    std::memcpy(F.J, &m.invccjac[c * 9], sizeof(F.J));
-    F.a = {m.jac_a[c * 3], m.jac_a[c * 3 + 1], m.jac_a[c * 3 + 2]};
-    F.absdet = std::fabs(m.jac_det[c]);
-    std::vector<double> mom(ideg);
-    cell_moments(m, c, {0, 0, 0}, F, mono, Rm, mom.data());
-    double vloc = m.volume[c] / F.absdet;  // VOLUME(1,1)
-    for (int d = 0; d < ideg; ++d) m.basis_mean[c * ideg + d] = mom[d] / vloc;
-  }
   // geometry keys: cells whose stencils look the same share tables
   std::vector<std::array<uint64_t, 2>> key(nc);
 #pragma omp parallel for schedule(static)
@@ -925,7 +813,7 @@ bool build_tables(ucp_mesh& m) {
   std::iota(idx.begin(), idx.end(), 0);
   std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return key[a] < key[b] || (key[a] == key[b] && a < b); });
   m.table_id.assign(nc, -1);
-  std::vector<int64_t> rep;
+  rep.clear();
   for (int64_t i = 0; i < nc; ++i) {
     if (i == 0 || key[idx[i]] != key[idx[i - 1]]) rep.push_back(idx[i]);
     m.table_id[idx[i]] = (int32_t)(rep.size() - 1);
@@ -946,8 +834,34 @@ bool build_tables(ucp_mesh& m) {
     for (int64_t c = 0; c < nc; ++c) m.table_id[c] = remap[m.table_id[c]];
     rep.swap(rep2);
   }
-  const int64_t ntab = (int64_t)rep.size();
-  m.ntab = ntab;
+  m.ntab = (int64_t)rep.size();
+}
+
+bool build_tables(ucp_mesh& m) {
+  SchemeSizes& s = m.sz;
+  const int64_t nc = m.nc;
+  const int W = s.imax + 1;
+  const int ideg = s.ideg;
+  std::vector<Mono> mono = monomials(s.iorder);
+  TetRule Rm = tet_rule(std::max(2, (s.iorder + 4) / 2));
+  TetRule Ri = tet_rule(std::max(2, (2 * s.iorder + 2) / 2 + 1));
+  m.basis_mean.assign(nc * ideg, 0.0);
+  // frames + cell means
+  std::vector<Frame> frames(nc);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    Frame& F = frames[c];
+    std::memcpy(F.J, &m.invccjac[c * 9], sizeof(F.J));
+    F.a = {m.jac_a[c * 3], m.jac_a[c * 3 + 1], m.jac_a[c * 3 + 2]};
+    F.absdet = std::fabs(m.jac_det[c]);
+    std::vector<double> mom(ideg);
+    cell_moments(m, c, {0, 0, 0}, F, mono, Rm, mom.data());
+    double vloc = m.volume[c] / F.absdet;  // VOLUME(1,1)
+    for (int d = 0; d < ideg; ++d) m.basis_mean[c * ideg + d] = mom[d] / vloc;
+  }
+  std::vector<int64_t> rep;
+  assign_tables(m, rep);
+  const int64_t ntab = m.ntab;
   const int A = s.admis_max;
   m.invmat.assign(ntab * A * s.imax * ideg, 0.0);
   if (s.ees == 5) m.invmat2.assign(ntab * A * s.imax2 * s.ideg2, 0.0);
@@ -1476,7 +1390,7 @@ int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix) {
   return UCG_OK;
 }
 
-int32_t ucp_prepare(ucp_mesh* m, const ucp_scheme* s) {
+static int32_t prepare(ucp_mesh* m, const ucp_scheme* s, bool tables) {
   if (!m || !s) {
     set_err("null argument");
     return UCG_EINVAL;
@@ -1496,8 +1410,43 @@ int32_t ucp_prepare(ucp_mesh* m, const ucp_scheme* s) {
   if (!build_connectivity(*m)) return UCG_EINVAL;
   if (!build_geometry(*m)) return UCG_EINVAL;
   if (!build_stencils(*m)) return UCG_EINVAL;
-  if (!build_tables(*m)) return UCG_EINVAL;
+  m->tables = false;
+  m->basis_mean.clear();
+  m->invmat.clear();
+  m->invmat2.clear();
+  m->indicator.clear();
+  m->indicator2.clear();
+  m->table_id.clear();
+  m->ntab = 0;
+  if (tables) {
+    if (!build_tables(*m)) return UCG_EINVAL;
+  } else {
+    std::vector<int64_t> rep;
+    assign_tables(*m, rep);
+  }
+  m->tables = tables;
+  m->shape32.assign(m->type.begin(), m->type.end());
   m->prepared = true;
+  return UCG_OK;
+}
+
+int32_t ucp_prepare(ucp_mesh* m, const ucp_scheme* s) { return prepare(m, s, true); }
+int32_t ucp_prepare_geometry(ucp_mesh* m, const ucp_scheme* s) { return prepare(m, s, false); }
+
+int32_t ucp_shapes(const ucp_mesh* m, ucg_shapes* out) {
+  if (!m || !out || !m->prepared) {
+    set_err("mesh not prepared");
+    return UCG_ESTATE;
+  }
+  out->ncells = m->nc;
+  out->shape = m->shape32.data();
+  out->vertices = m->vx.data();
+  out->centre = m->centre.data();
+  out->volume = m->volume.data();
+  out->frame = m->invccjac.data();
+  out->frame_origin = m->jac_a.data();
+  out->frame_det = m->jac_det.data();
+  for (int k = 0; k < 3; ++k) out->period[k] = m->per[k] ? m->L[k] : 0.0;
   return UCG_OK;
 }
 
@@ -1546,7 +1495,7 @@ int32_t ucp_geometry(const ucp_mesh* m, ucg_geometry* g) {
   g->volume = m->volume.data();
   g->minedge = m->minedge.data();
   g->invccjac = m->invccjac.data();
-  g->basis_mean = m->basis_mean.data();
+  g->basis_mean = m->tables ? m->basis_mean.data() : nullptr;
   g->admis = m->admis.data();
   g->full = m->full.data();
   return UCG_OK;
@@ -1562,7 +1511,7 @@ int32_t ucp_recon(const ucp_mesh* m, ucg_recon* r) {
   r->stencil = m->stencil.data();
   r->ntables = m->ntab;
   r->table_id = m->table_id.data();
-  r->invmat = m->invmat.data();
+  r->invmat = m->tables ? m->invmat.data() : nullptr;
   r->invmat2 = m->invmat2.empty() ? nullptr : m->invmat2.data();
   r->indicator = m->indicator.empty() ? nullptr : m->indicator.data();
   r->indicator2 = m->indicator2.empty() ? nullptr : m->indicator2.data();

@@ -27,7 +27,11 @@ class EngineError(RuntimeError):
 
 
 class Engine:
-    def __init__(self, mesh, cfg: N.UcgConfig, device: int = 0, upload: bool = True):
+    def __init__(self, mesh, cfg: N.UcgConfig, device: int = 0, upload: bool = True, tables: str = "host"):
+        """``tables``: "host" uploads the set-up library's reconstruction
+        tables (ucg_upload_recon), "device" builds them on the GPU from the
+        cell shapes (ucg_build_recon; the mesh may be prepared without
+        tables)."""
         self.lib = N.engine()
         self.mesh = mesh
         self.cfg = cfg
@@ -39,7 +43,10 @@ class Engine:
         self._h = h
         if upload:
             self.upload_geometry(mesh.geometry_struct())
-            self.upload_recon(mesh.recon_struct())
+            if tables == "device":
+                self.build_recon(mesh.shapes_struct(), mesh.recon_struct())
+            else:
+                self.upload_recon(mesh.recon_struct())
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -65,6 +72,10 @@ class Engine:
 
     def upload_recon(self, r: N.UcgRecon):
         self._check(self.lib.ucg_upload_recon(self._h, C.byref(r)))
+
+    def build_recon(self, s: N.UcgShapes, r: N.UcgRecon):
+        """The reconstruction tables built on the device (ucg_build_recon)."""
+        self._check(self.lib.ucg_build_recon(self._h, C.byref(s), C.byref(r)))
 
     # ------------------------------------------------------------- state
     def set_state(self, U: np.ndarray):

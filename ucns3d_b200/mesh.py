@@ -96,10 +96,17 @@ class Mesh:
     def ncells(self) -> int:
         return int(N.prep().ucp_ncells(self._h))
 
-    def prepare(self, scheme: int, iorder: int, ees: int = 0, nthreads: int = 0) -> "Mesh":
+    def prepare(self, scheme: int, iorder: int, ees: int = 0, nthreads: int = 0, tables: bool = True) -> "Mesh":
+        """Connectivity, geometry, stencils and (``tables``) the
+        reconstruction tables; without them the engine builds the tables on
+        the device (``Engine(..., tables="device")``)."""
         s = N.UcpScheme(scheme, iorder, ees, nthreads)
-        _check(N.prep().ucp_prepare(self._h, C.byref(s)), "ucp_prepare")
+        if tables:
+            _check(N.prep().ucp_prepare(self._h, C.byref(s)), "ucp_prepare")
+        else:
+            _check(N.prep().ucp_prepare_geometry(self._h, C.byref(s)), "ucp_prepare_geometry")
         self.prepared = True
+        self.tables = tables
         self.scheme, self.iorder, self.ees = scheme, iorder, ees
         cfg = N.UcgConfig()
         _check(N.prep().ucp_fill_config(self._h, C.byref(cfg)), "ucp_fill_config")
@@ -122,6 +129,12 @@ class Mesh:
         _check(N.prep().ucp_recon(self._h, C.byref(r)), "ucp_recon")
         return r
 
+    def shapes_struct(self) -> N.UcgShapes:
+        """Cell shapes, frames and periods for ucg_build_recon."""
+        s = N.UcgShapes()
+        _check(N.prep().ucp_shapes(self._h, C.byref(s)), "ucp_shapes")
+        return s
+
     @property
     def ntables(self) -> int:
         return int(N.prep().ucp_ntables(self._h))
@@ -135,6 +148,8 @@ class Mesh:
         ideg = self.sizes["ideg"]
 
         def arr(p, shape, dt):
+            if not p:
+                return None
             count = int(np.prod(shape))
             ct = C.c_int32 if dt == np.int32 else C.c_double
             buf = (ct * count).from_address(C.cast(p, C.c_void_p).value)
@@ -151,6 +166,23 @@ class Mesh:
             invccjac=arr(g.invccjac, (n, 3, 3), np.float64), basis_mean=arr(g.basis_mean, (n, ideg), np.float64),
             admis=arr(g.admis, (n,), np.int32), full=arr(g.full, (n,), np.int32),
         )
+
+    def shapes(self) -> dict:
+        """Copies of the cell shapes of ucp_shapes (for tests and
+        renumbered views)."""
+        sh = self.shapes_struct()
+        n = sh.ncells
+
+        def arr(p, shape, dt):
+            count = int(np.prod(shape))
+            ct = C.c_int32 if dt == np.int32 else C.c_double
+            buf = (ct * count).from_address(C.cast(p, C.c_void_p).value)
+            return np.frombuffer(buf, dtype=dt).reshape(shape).copy()
+
+        return dict(shape=arr(sh.shape, (n,), np.int32), vertices=arr(sh.vertices, (n, 8, 3), np.float64),
+                    centre=arr(sh.centre, (n, 3), np.float64), volume=arr(sh.volume, (n,), np.float64),
+                    frame=arr(sh.frame, (n, 3, 3), np.float64), frame_origin=arr(sh.frame_origin, (n, 3), np.float64),
+                    frame_det=arr(sh.frame_det, (n,), np.float64), period=list(sh.period))
 
     def recon(self) -> dict:
         """Copies of the reconstruction tables (for tests)."""
@@ -215,6 +247,8 @@ class RenumberedMesh:
         g = base.geometry()
         self._g = {k: (np.ascontiguousarray(v[order]) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
         self._g["neigh"] = remap(self._g["neigh"])
+        self._s = {k: (np.ascontiguousarray(v[order]) if isinstance(v, np.ndarray) else v)
+                   for k, v in base.shapes().items()}
         r = base.recon()
         self._r = dict(r)
         self._r["stencil"] = np.ascontiguousarray(remap(r["stencil"][order]))
@@ -242,7 +276,8 @@ class RenumberedMesh:
         for k in ("nfaces", "face_type", "neigh", "neigh_face", "bc", "qperm", "admis", "full"):
             setattr(s, k, N.ptr(g[k], C.c_int32))
         for k in ("face_angle", "face_area", "dih", "qpoints", "volume", "minedge", "invccjac", "basis_mean"):
-            setattr(s, k, N.ptr(g[k], C.c_double))
+            if g[k] is not None:  # basis_mean: absent when the engine builds the tables
+                setattr(s, k, N.ptr(g[k], C.c_double))
         return s
 
     def recon_struct(self) -> N.UcgRecon:
@@ -255,6 +290,16 @@ class RenumberedMesh:
         for k in ("invmat", "invmat2", "indicator", "indicator2"):
             if r.get(k) is not None:
                 setattr(s, k, N.ptr(r[k], C.c_double))
+        return s
+
+    def shapes_struct(self) -> N.UcgShapes:
+        sh, s = self._s, N.UcgShapes()
+        s.ncells = self.ncells
+        s.shape = N.ptr(sh["shape"], C.c_int32)
+        for k in ("vertices", "centre", "volume", "frame", "frame_origin", "frame_det"):
+            setattr(s, k, N.ptr(sh[k], C.c_double))
+        for k in range(3):
+            s.period[k] = sh["period"][k]
         return s
 
     def geometry(self) -> dict:
