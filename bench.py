@@ -57,6 +57,8 @@ def parse():
                     help="hand the mesh over in a seeded random cell numbering (as from a partitioner) and time "
                          "it with the engine's renumbering on (the line's value) and off (shuffle.reorder_off)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--implicit", action="store_true",
+                    help="also time implicit steps (ucg_implicit_step) against explicit RK3 on the bump channel")
     ap.add_argument("--setup", action="store_true",
                     help="also time the reconstruction-table set-up: host (ucp_prepare + upload) against the "
                          "device (ucg_build_recon) on meshes with one matrix set per cell")
@@ -527,6 +529,41 @@ def run_adjoint(local, steps=200, every=20, weno_n=32):
     return out
 
 
+def run_implicit(local):
+    """The bump channel (MUSCL + HLLC, Euler, 240 x 80 x 4 layers) from the
+    free stream toward its steady state: implicit steps at CFL 50
+    (IMPLICIT_TIMEs, 10 relaxation sweeps) against explicit RK3 steps at CFL
+    0.9, each timed with CUDA events on the engine stream; the residual norm
+    relative to the free stream's after each run."""
+    import numpy as np
+    import torch
+    from ucns3d_b200 import cases
+    from ucns3d_b200.engine import Engine
+    c = cases.bump_muscl()
+    out = {"workload": "bump_muscl 240x80x4", "cells": c.mesh.ncells}
+    for kind, steps in (("implicit", 200), ("explicit_rk3", 2000)):
+        e = Engine(c.mesh, c.cfg, device=local)
+        e.set_state(c.U0)
+        r0 = float(np.linalg.norm(e.call_flux_subroutines_3d()))
+        stream = torch.cuda.ExternalStream(e.stream_ptr, device=f"cuda:{local}")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e.synchronize()
+        ev0.record(stream)
+        if kind == "implicit":
+            e.implicit_step(50.0, steps, 10)
+        else:
+            e.time_marching(steps, 0.9)
+        ev1.record(stream)
+        ev1.synchronize()
+        e.check_health()
+        r1 = float(np.linalg.norm(e.call_flux_subroutines_3d()))
+        ms = ev0.elapsed_time(ev1)
+        out[kind] = {"steps": steps, "cfl": 50.0 if kind == "implicit" else 0.9, "ms": ms, "ms_per_step": ms / steps,
+                     "residual_ratio": r1 / r0}
+        e.close()
+    return out
+
+
 def run_setup(local):
     """Start-up time of the reconstruction tables on meshes whose cells all
     have their own matrix sets (jittered tetrahedra): the host set-up
@@ -679,6 +716,8 @@ def main():
         out["adjoint"] = run_adjoint(local, args.adjoint_steps, args.adjoint_every, args.adjoint_weno_n)
     if args.setup:
         out["setup"] = run_setup(local)
+    if args.implicit:
+        out["implicit"] = run_implicit(local)
     if rank == 0 and ws == 1 and not args.no_cpu:
         cb = cpu_sample(args, case=c32 if not args.cpu_n else None)
         out["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": "port",

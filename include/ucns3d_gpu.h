@@ -294,6 +294,35 @@ int ucg_set_wait_limit(ucg_engine* e, int64_t polls);
  * in the reference, which takes the order of its grid reader and METIS. */
 int ucg_cell_order(const ucg_engine* e, int32_t* renumbered, int32_t* n2o, double* cost);
 
+/* `nsteps` implicit pseudo-time steps toward a steady state (RUNGEKUTTA =
+ * 10: IMPLICIT_TIMEs, src/time_p.f90:2783-2905, RELAX = 1): each step forms
+ * RHS, the local time steps DTL of CALCULATE_CFLL at CFL `cfl`
+ * (src/time_p.f90:193-333), the first-order Jacobian of CALCULATE_JACOBIAN
+ * (src/implicit_fluxes.f90:12-594: diagonal sum_f vpp_f area_f / 2 + V/DTL,
+ * per face (J(U_R) n / 2 - vpp / 2) area with COMPUTE_JACOBIANSE), relaxes
+ * du = D^-1 (-RHS - sum_f O_f du_f) `nsweeps` times from du = 0 (RELAXATION
+ * takes 10) and adds du to the state.  Every sweep reads the previous
+ * sweep's corrections (the reference's in-place OpenMP loop depends on the
+ * thread schedule); the steady state is the same.  Euler and Navier-Stokes,
+ * any reconstruction.  A non-finite correction raises UCG_ENONPHYS at the
+ * next ucg_check_health.  Queued on the handle's stream. */
+int ucg_implicit_step(ucg_engine* e, double cfl, int32_t nsteps, int32_t nsweeps);
+
+/* One physical time step dt of the dual-time scheme (RUNGEKUTTA = 11:
+ * DUAL_TIME, src/time_p.f90:3035-3243): BDF2 in physical time, implicit
+ * inner iterations in pseudo time (local steps at `cfl`, `nsweeps` sweeps,
+ * the diagonal V (1/DTL + 1.5/dt) + ...): the first without the time term
+ * (ISCOUN 1), the others with -V (1.5 U - 2 U^n + 0.5 U^{n-1}) / dt added
+ * to the right-hand side, each adding its correction to the state, until
+ * the correction norm sum |du| V / TOTALVOLUME, relative to its largest
+ * value in this step, is at most inner_tol (RESLIMIT) or max_inner
+ * iterations (UPPERLIMIT) are done; *inner_iters (optional) receives their
+ * number.  Then U^{n-1} <- U^n <- U.  The history (U^n, U^{n-1}) starts as
+ * the state of the first call after ucg_set_state (IT = RESTART).
+ * Synchronous (one 8-byte read per inner iteration). */
+int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t max_inner, double inner_tol, int32_t nsweeps,
+                       int32_t* inner_iters);
+
 /* MOOD state after the last RK3 stage (cfg.mood 1), in the caller's cell
  * order: order[c] = IELEM(N,I)%MOOD_O, 1 where the second cascade
  * recomputed the cell at first order, 2 where only the first cascade

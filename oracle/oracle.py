@@ -40,6 +40,11 @@ def lib():
         L.orc_rk3_step.argtypes = [cfgp, geop, recp, C.c_double, f64p]
         L.orc_rk3_stage.restype = C.c_int
         L.orc_rk3_stage.argtypes = [cfgp, geop, recp, C.c_double, C.c_int, f64p, f64p]
+        L.orc_implicit_step.restype = C.c_int
+        L.orc_implicit_step.argtypes = [cfgp, geop, recp, C.c_double, C.c_int, C.c_int, f64p]
+        L.orc_dual_time_step.restype = C.c_int
+        L.orc_dual_time_step.argtypes = [cfgp, geop, recp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                         f64p, f64p, f64p, C.POINTER(C.c_int)]
         L.orc_rk3_step_mood.restype = C.c_int
         L.orc_rk3_step_mood.argtypes = [cfgp, geop, recp, C.c_double, f64p, C.POINTER(C.c_int8),
                                         C.POINTER(C.c_int32)]
@@ -130,6 +135,29 @@ class Oracle:
         if rc:
             raise RuntimeError(f"orc_rk3_step failed: {rc}")
         return U
+
+    def implicit_step(self, U: np.ndarray, cfl: float, nsteps: int = 1, nsweeps: int = 10) -> np.ndarray:
+        """`nsteps` IMPLICIT_TIMEs steps (local time steps at `cfl`, `nsweeps`
+        relaxation sweeps)."""
+        U = np.array(U, dtype=np.float64, copy=True, order="C")
+        rc = lib().orc_implicit_step(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), cfl, nsteps, nsweeps,
+                                     _p(U))
+        if rc:
+            raise RuntimeError(f"orc_implicit_step failed: {rc}")
+        return U
+
+    def dual_time_step(self, U: np.ndarray, hist: tuple, dt: float, cfl: float, maxit: int = 20,
+                       tol: float = 1e-3, nsweeps: int = 10) -> tuple:
+        """One DUAL_TIME physical step: (U, (U^n, U^{n-1}), inner iterations);
+        hist is None before the first step."""
+        U = np.array(U, dtype=np.float64, copy=True, order="C")
+        U2, U3 = (U.copy(), U.copy()) if hist is None else (np.array(hist[0], copy=True), np.array(hist[1], copy=True))
+        it = C.c_int()
+        rc = lib().orc_dual_time_step(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), dt, cfl, maxit, tol,
+                                      nsweeps, _p(U), _p(U2), _p(U3), C.byref(it))
+        if rc:
+            raise RuntimeError(f"orc_dual_time_step failed: {rc}")
+        return U, (U2, U3), it.value
 
     def rk3_step_mood(self, U: np.ndarray, dt: float, recalc: np.ndarray) -> tuple:
         """One RUNGE_KUTTA3_MOOD step (cfg.mood 1): the new state and MOOD_O per

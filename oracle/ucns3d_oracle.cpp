@@ -1325,6 +1325,192 @@ int orc_rk3_stage(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon*
   return UCG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// One implicit correction du of U: RHS, DTL, the Jacobian and `nsweeps`
+// sweeps from du = 0.  Dual time (dt > 0): the diagonal V (1/DTL + 1.5/dt)
+// + ..., and with U2 (U^n) and U3 (U^{n-1}) given (ISCOUN 2) the right-hand
+// side -(RHS + V (1.5 U - 2 U^n + 0.5 U^{n-1}) / dt).
+void implicit_du(const Ctx& x, const double* U, double ccfl, int nsweeps, double dt, const double* U2,
+                 const double* U3, std::vector<double>& du) {
+  const ucg_config* cfg = x.cfg;
+  const ucg_geometry* g = x.g;
+  const int64_t n = x.n;
+  const bool ns = cfg->governing == 1;
+  const double gm = cfg->gamma;
+  std::vector<double> rhs(n * NV), UL, ULV, dtl(n), dinv(n), off((size_t)n * F * 25), dn(n * NV);
+  du.assign(n * NV, 0.0);
+  {
+    residual(x, U, rhs.data(), UL, ULV);
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < n; ++c) {
+      double p[NV];
+      cons2prim(x, &U[c * NV], p);
+      const double agrt = std::sqrt(p[4] * gm / p[0]);
+      const double veln = std::max(std::max(std::fabs(p[1]), std::fabs(p[2])), std::fabs(p[3])) + agrt;
+      const double me = g->minedge[c];
+      if (ns) {
+        double mu, lam;
+        sutherland(cfg, p[0], p[4], &mu, &lam);
+        dtl[c] = ccfl * (1.0 / ((std::fabs(veln) / me) + (0.5 * (lam + mu) / (me * me))));
+      } else {
+        dtl[c] = ccfl * (me / std::fabs(veln));
+      }
+      // Jacobian
+      const double* cl = &U[c * NV];
+      double lv[NV];
+      cons2prim(x, cl, lv);
+      double diag = 0.0;
+      for (int f = 0; f < g->nfaces[c]; ++f) {
+        const double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+        const double ang[4] = {std::cos(a1), std::sin(a1), std::cos(a2), std::sin(a2)};
+        const double nx = ang[0] * ang[3], ny = ang[1] * ang[3], nz = ang[2];
+        const double area = g->face_area[c * F + f];
+        const int64_t nb = g->neigh[c * F + f];
+        double cr[NV], rv[NV], clr[NV], crr[NV];
+        if (nb >= 0)
+          for (int v = 0; v < NV; ++v) cr[v] = U[nb * NV + v];
+        else
+          boundary_state(x, g->bc[c * F + f], ang, cl, cr);
+        rotf(ang, cr, crr);
+        rotf(ang, cl, clr);
+        cons2prim(x, cr, rv);
+        const double as1 = std::sqrt(lv[4] * gm / lv[0]) + std::fabs(clr[1] / clr[0]);
+        const double as2 = std::sqrt(rv[4] * gm / rv[0]) + std::fabs(crr[1] / crr[0]);
+        double vpp = std::max(as1, as2);
+        if (ns) {
+          double mul, laml, mur, lamr;
+          sutherland(cfg, lv[0], lv[4], &mul, &laml);
+          sutherland(cfg, rv[0], rv[4], &mur, &lamr);
+          double vis = (mul + mur) * 0.5;
+          const double rh = 0.5 * (cl[0] + cr[0]), dih = g->dih[c * F + f];
+          vis = std::max((4.0 / (3.0 * rh)) * vis * area / dih, (gm / rh) * vis * area / (dih * cfg->prandtl));
+          vpp = vpp + vis;
+        }
+        diag = diag + (0.5 * (vpp * 1.0)) * area;
+        // COMPUTE_JACOBIANSE of the right state
+        const double A2 = gm - 1.0, A3 = gm - 2.0, oors = 1.0 / cr[0];
+        const double us = cr[1] * oors, vs = cr[2] * oors, ws = cr[3] * oors, es = cr[4] * oors;
+        const double phi = 0.5 * A2 * ((us * us) + (vs * vs) + (ws * ws));
+        const double A1 = gm * es - phi, vvs = nx * us + ny * vs + nz * ws;
+        const double J[25] = {0.0, nx, ny, nz, 0.0,
+                              nx * phi - us * vvs, vvs - A3 * nx * us, ny * us - A2 * nx * vs, nz * us - A2 * nx * ws, A2 * nx,
+                              ny * phi - vs * vvs, nx * vs - A2 * ny * us, vvs - A3 * ny * vs, nz * vs - A2 * ny * ws, A2 * ny,
+                              nz * phi - ws * vvs, nx * ws - A2 * nz * us, ny * ws - A2 * nz * vs, vvs - A3 * nz * ws, A2 * nz,
+                              vvs * (phi - A1), nx * A1 - A2 * us * vvs, ny * A1 - A3 * vs * vvs, nz * A1 - A2 * ws * vvs,
+                              gm * vvs};
+        for (int i = 0; i < NV; ++i)
+          for (int j = 0; j < NV; ++j)
+            off[((size_t)c * F + f) * 25 + i * NV + j] = ((0.5 * J[i * NV + j]) - ((0.5 * vpp) * (i == j ? 1.0 : 0.0))) * area;
+      }
+      if (dt > 0.0) diag = g->volume[c] * ((1.0 / dtl[c]) + (1.5 / dt)) + diag;
+      else diag = diag + (g->volume[c] / dtl[c]);
+      dinv[c] = 1.0 / diag;
+    }
+    for (int sw = 0; sw < nsweeps; ++sw) {
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < n; ++c) {
+        double b[NV];
+        const double* d0 = &du[c * NV];
+        for (int v = 0; v < NV; ++v) {
+          const int64_t i = c * NV + v;
+          b[v] = U2 ? -(rhs[i] + ((((1.5 * U[i]) - (2.0 * U2[i]) + (0.5 * U3[i])) / dt) * g->volume[c])) : -rhs[i];
+        }
+        for (int f = 0; f < g->nfaces[c]; ++f) {
+          const int64_t nb = g->neigh[c * F + f];
+          double d1[NV];
+          if (nb >= 0) {
+            for (int v = 0; v < NV; ++v) d1[v] = du[nb * NV + v];
+          } else {
+            const int code = g->bc[c * F + f];
+            if (code == 1) {
+              for (int v = 0; v < NV; ++v) d1[v] = 0.0;
+            } else if (code == 3 || code == 4) {
+              const double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+              const double ang[4] = {std::cos(a1), std::sin(a1), std::cos(a2), std::sin(a2)};
+              boundary_state(x, code, ang, d0, d1);
+            } else {
+              for (int v = 0; v < NV; ++v) d1[v] = d0[v];
+            }
+          }
+          const double* o = &off[((size_t)c * F + f) * 25];
+          for (int i = 0; i < NV; ++i) {
+            double t = 0.0;
+            for (int j = 0; j < NV; ++j) t = t + o[i * NV + j] * d1[j];
+            b[i] = b[i] - t;
+          }
+        }
+        for (int v = 0; v < NV; ++v) dn[c * NV + v] = dinv[c] * b[v];
+      }
+      du.swap(dn);
+    }
+  }
+}
+}  // namespace
+
+extern "C" {
+
+// IMPLICIT_TIMEs (time_p.f90:2783-2905, RUNGEKUTTA = 10, ISCOUN = 1) in
+// place on U, `nsteps` times: RHS, the local time steps of CALCULATE_CFLL
+// (time_p.f90:193-333), the first-order Jacobian of CALCULATE_JACOBIAN
+// (implicit_fluxes.f90:12-594) with COMPUTE_JACOBIANSE
+// (flow_operations.f90:4004-4049; its entry (5,3) takes gamma - 2), then
+// RELAXATION (implicit_time.f90:1-778, RELAX = 1): `nsweeps` sweeps of
+// du = D^-1 (-RHS - sum_f O_f du_f) from du = 0, each reading the previous
+// sweep's du (the reference updates in place, in an order set by its
+// OpenMP schedule); du_f on physical faces: 0 on inflow, the cell's du on
+// outflow and far field, BOUNDARYS of du on symmetry and walls.
+int orc_implicit_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double cfl, int nsteps,
+                      int nsweeps, double* U) {
+  if (!check_ctx(cfg, g, r) || !U || !(cfl > 0.0) || nsteps < 0 || nsweeps < 1) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  std::vector<double> du;
+  for (int step = 0; step < nsteps; ++step) {
+    implicit_du(x, U, cfl / 3.0, nsweeps, 0.0, nullptr, nullptr, du);
+    for (int64_t c = 0; c < g->ncells * NV; ++c) U[c] = U[c] + du[c];
+  }
+  return UCG_OK;
+}
+
+// DUAL_TIME (time_p.f90:3035-3243, RUNGEKUTTA = 11): one physical step dt
+// in place on U with U^n in U2 and U^{n-1} in U3 (both U before the first
+// step, IT = RESTART), rotated on return; inner implicit iterations, the
+// first without the time term (ISCOUN 1), until sum_c |du_c| V_c /
+// TOTALVOLUME over its largest value in the step is <= tol or maxit are
+// done (*iters).
+int orc_dual_time_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt, double cfl,
+                       int maxit, double tol, int nsweeps, double* U, double* U2, double* U3, int* iters) {
+  if (!check_ctx(cfg, g, r) || !U || !U2 || !U3 || !(dt > 0.0) || !(cfl > 0.0) || maxit < 1 || nsweeps < 1)
+    return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const int64_t n = g->ncells;
+  double tot = 0.0;
+  for (int64_t c = 0; c < n; ++c) tot += g->volume[c];
+  std::vector<double> du;
+  double firsti = 0.0;
+  int jj;
+  for (jj = 1; jj <= maxit; ++jj) {
+    implicit_du(x, U, cfl / 3.0, nsweeps, dt, jj == 1 ? nullptr : U2, U3, du);
+    double res = 0.0;
+    for (int64_t c = 0; c < n; ++c) {
+      const double* d = &du[c * NV];
+      res += std::sqrt((d[0] * d[0]) + (d[1] * d[1]) + (d[2] * d[2]) + (d[3] * d[3]) + (d[4] * d[4])) * g->volume[c];
+    }
+    for (int64_t i = 0; i < n * NV; ++i) U[i] = U[i] + du[i];
+    res = res / tot;
+    if (res > firsti) firsti = res;
+    res = res / firsti;
+    if (res <= tol) break;
+  }
+  if (iters) *iters = jj > maxit ? maxit : jj;
+  for (int64_t i = 0; i < n * NV; ++i) {
+    U3[i] = U2[i];
+    U2[i] = U[i];
+  }
+  return UCG_OK;
+}
+
 // RUNGE_KUTTA3_MOOD (time_p.f90:582-880) in place on U [n][5], Euler with
 // WENO; recalc [n] is RECALC, carried between calls (zero before the first
 // step, memory.f90:1002-1005); order (optional, [n]) MOOD_O after the step.

@@ -154,7 +154,8 @@ ENGINE_SYMBOLS = [
     "ucg_time_kernels", "ucg_get_stream", "ucg_launch_count", "ucg_device_bytes", "ucg_last_error",
     "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
-    "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon",
+    "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon", "ucg_implicit_step",
+    "ucg_dual_time_step",
 ]
 
 
@@ -226,6 +227,11 @@ def engine() -> C.CDLL:
         lib.ucg_cell_order.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _f64p]
         lib.ucg_mood_state.restype = C.c_int
         lib.ucg_mood_state.argtypes = [vp, _i32p, _i32p]
+        lib.ucg_implicit_step.restype = C.c_int
+        lib.ucg_implicit_step.argtypes = [vp, C.c_double, C.c_int32, C.c_int32]
+        lib.ucg_dual_time_step.restype = C.c_int
+        lib.ucg_dual_time_step.argtypes = [vp, C.c_double, C.c_double, C.c_int32, C.c_double, C.c_int32,
+                                           C.POINTER(C.c_int32)]
         lib.ucg_build_recon.restype = C.c_int
         lib.ucg_build_recon.argtypes = [vp, C.POINTER(UcgShapes), C.POINTER(UcgRecon)]
         lib.ucg_tangent_run.restype = C.c_int

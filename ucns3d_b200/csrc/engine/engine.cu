@@ -604,7 +604,8 @@ void ucg_destroy(ucg_engine* e) {
                    &e->ind, &e->dul, &e->ulv, &e->gv, &e->prim, &e->upad, &e->rhs, &e->Un, &e->Ua, &e->Ub,
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
                    &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb, &e->wflag, &e->mprev, &e->mflag,
-                   &e->msel, &e->mmus, &e->mord, &e->Um};
+                   &e->msel, &e->mmus, &e->mord, &e->Um, &e->imp_dtl, &e->imp_dinv, &e->imp_off, &e->imp_du,
+                   &e->dual_hist, &e->dual_part};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -776,6 +777,8 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   e->admis_h = std::move(admis);
+  e->totvol = 0.0;
+  for (int64_t c = 0; c < n; ++c) e->totvol += g->volume[c];
   e->neigh_h = neigh;
   for (int64_t c = 0; c < n; ++c)  // no neighbour past the cell's last face
     for (int f = nfaces[c]; f < MF; ++f) e->neigh_h[(size_t)c * MF + f] = -1;
@@ -1016,6 +1019,7 @@ int ucg_set_state(ucg_engine* e, const double* u, int64_t n) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(e->stream));
   e->have_state = true;
+  e->dual_ready = false;  // a new state starts a new dual-time history
   return UCG_OK;
 }
 

@@ -56,6 +56,12 @@ struct ucg_engine {
   DevBuf gbuf, isb, wflag, dul, ulv, fgrad, gv, prim, upad, rhs, Un, Ua, Ub, health, dt, partial, red, staging, own, fflux, vflux, qbuf;
   // MOOD (cfg.mood): RECALC, the cascade's flags and selections, MOOD_O, the candidate state
   DevBuf mprev, mflag, msel, mmus, mord, Um;
+  // implicit steps (ucg_implicit_step): local time steps, inverse diagonals, face blocks, corrections
+  DevBuf imp_dtl, imp_dinv, imp_off, imp_du;
+  // dual time (ucg_dual_time_step): U^n and U^{n-1}, the norm's block sums
+  DevBuf dual_hist, dual_part;
+  bool dual_ready = false;  // the history holds the state of a step (reset by ucg_set_state)
+  double totvol = 0.0;      // TOTALVOLUME
   int64_t nown = 0;
   int64_t nown_plain = 0;  // owned faces [0, nown_plain): interior and mirror; the rest other boundaries
   cudaEvent_t mark = nullptr;  // recorded after k_lsq while ucg_time_kernels runs

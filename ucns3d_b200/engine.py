@@ -209,6 +209,19 @@ class Engine:
         self._check(self.lib.ucg_cell_order(self._h, C.byref(ren), N.ptr(n2o, C.c_int32), N.ptr(cost, C.c_double)))
         return dict(renumbered=bool(ren.value), n2o=n2o, cost_caller=float(cost[0]), cost_rcm=float(cost[1]))
 
+    def implicit_step(self, cfl: float, nsteps: int = 1, nsweeps: int = 10):
+        """`nsteps` implicit pseudo-time steps toward the steady state
+        (IMPLICIT_TIMEs with `nsweeps` relaxation sweeps)."""
+        self._check(self.lib.ucg_implicit_step(self._h, cfl, nsteps, nsweeps))
+
+    def dual_time_step(self, dt: float, cfl: float, max_inner: int = 20, inner_tol: float = 1e-3,
+                       nsweeps: int = 10) -> int:
+        """One DUAL_TIME physical step dt (BDF2, implicit inner iterations
+        at pseudo CFL `cfl`); returns the inner iterations taken."""
+        it = C.c_int32()
+        self._check(self.lib.ucg_dual_time_step(self._h, dt, cfl, max_inner, inner_tol, nsweeps, C.byref(it)))
+        return int(it.value)
+
     def mood_state(self) -> dict:
         """MOOD after the last RK3 stage (cfg.mood 1): MOOD_O per cell (1
         first order, 2 MUSCL, IORDER + 1 the target scheme) and RECALC (the
