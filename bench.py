@@ -491,6 +491,19 @@ def run_adjoint(local, steps=200, every=20, weno_n=32):
            "dJdp_note": "inflow changes reach the bump only after about 500 steps at this size, so dJ/dp is "
                         "physically near zero over the 200-step window; see short_channel",
            "short_channel": short}
+    # the Navier-Stokes residual's VJP/JVP on the same channel (Re 200,
+    # no-slip walls on BC 4), at the free stream marched 50 steps
+    from ucns3d_b200.config import NAVIER_STOKES, make_config
+    cfg_ns = make_config(c.mesh, governing=NAVIER_STOKES, reynolds=200.0, pres=1.0,
+                         bc_state=tuple(c.cfg.bc_state[k] for k in range(5)))
+    en = Engine(c.mesh, cfg_ns, device=local)
+    en.set_state(c.U0)
+    en.time_marching(50, c.cfl)
+    tn = en.time_adjoint(reps=10)
+    en.close()
+    out["ns"] = {"workload": "bump_muscl_ns Re 200", "cells": c.mesh.ncells, "dtype": "f64",
+                 "residual_ms": tn["residual"], "vjp_ms": tn["vjp"], "jvp_ms": tn["jvp"],
+                 "vjp_over_residual": tn["vjp"] / tn["residual"]}
     # the WENO residual's VJP/JVP (FP64 form) on the vortex, weno_n^3 hexahedra
     from ucns3d_b200 import _native as N
     from ucns3d_b200.engine import EngineError

@@ -374,8 +374,10 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
                               const double* u, double* rhs, void* stream);
 /* ---------------------------------------------------------------- adjoint
  * Discrete adjoint (VJP) and tangent (JVP) for the FP64 form of a MUSCL
- * (scheme 2, IORDER 1) Euler configuration (the adjoint workload is the
- * bump channel).  ucg_residual_vjp and ucg_residual_jvp also cover
+ * (scheme 2, IORDER 1, Venkatakrishnan, HLLC) Euler or Navier-Stokes
+ * configuration (the adjoint workload is the bump channel; Navier-Stokes
+ * adds the reverse of the viscous fluxes, of the viscous least squares and
+ * of the no-slip wall ghost).  ucg_residual_vjp and ucg_residual_jvp also cover
  * conserved-variable WENO and CWENO (scheme 3, EES 0 or 5, CWENO with or
  * without WENO-Z, HLLC, Euler, FP64 form): the
  * reverse/tangent of the nonlinear weights, smoothness indicators and

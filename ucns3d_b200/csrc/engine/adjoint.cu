@@ -50,9 +50,10 @@ namespace {
 int adj_check(ucg_engine* e) {
   if (!e) return UCG_EINVAL;
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 2 && c.iorder == 1 && c.governing == 2 && c.precision == UCG_FP64 && c.riemann == 1 &&
-        c.limiter == 7))
-    return fail(e, UCG_EINVAL, "the adjoint covers MUSCL (scheme 2, IORDER 1, Venkatakrishnan), HLLC, Euler, FP64 form");
+  if (!(c.scheme == 2 && c.iorder == 1 && (c.governing == 2 || c.governing == 1) && c.precision == UCG_FP64 &&
+        c.riemann == 1 && c.limiter == 7 && !c.mood))
+    return fail(e, UCG_EINVAL,
+                "the adjoint covers MUSCL (scheme 2, IORDER 1, Venkatakrishnan), HLLC, Euler or Navier-Stokes, FP64 form");
   if (e->QS != 1) return fail(e, UCG_EINVAL, "the adjoint needs one face point per face (IORDER 1)");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   return UCG_OK;
@@ -150,7 +151,8 @@ __device__ __forceinline__ void adj_face_inputs(const Problem& p, const double* 
 // Interior and mirror faces, owned faces [0, nplain): reverse sweep of HLLC
 // (ad::hllc_adj) in the face frame at every face point.  The rotations are
 // orthogonal (rot_b = rot_f^T), and a mirror ghost is b = S a in the face
-// frame (S flips the normal momentum).
+// frame (S flips the normal momentum; a Navier-Stokes wall, no slip, flips
+// the whole momentum).
 __global__ void __launch_bounds__(64) k_adj_face(Problem p, int64_t nplain, const double* __restrict__ U,
                                                   const double* __restrict__ lam, double* __restrict__ adjF) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -162,17 +164,19 @@ __global__ void __launch_bounds__(64) k_adj_face(Problem p, int64_t nplain, cons
     adj_face_inputs(p, U, lam, F, q, r, ul, ur, g, qq);
     double a[NV], b[NV], hb[NV], ab[NV] = {0, 0, 0, 0, 0}, bb[NV] = {0, 0, 0, 0, 0}, o[NV];
     rot_f(r, ul, a);
+    const bool noslip = F.nb < 0 && p.governing == 1 && p.bc[F.c * MF + F.f] == 4;
+    auto flip = [&](int v) { return noslip ? (v >= 1 && v <= 3) : v == 1; };
     if (F.nb >= 0) {
       rot_f(r, ur, b);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) b[v] = v == 1 ? -a[v] : a[v];
+      for (int v = 0; v < NV; ++v) b[v] = flip(v) ? -a[v] : a[v];
     }
     rot_f(r, g, hb);
     ad::hllc_adj(p.gamma, a, b, hb, ab, bb);
     if (F.nb < 0)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) ab[v] += v == 1 ? -bb[v] : bb[v];
+      for (int v = 0; v < NV; ++v) ab[v] += flip(v) ? -bb[v] : bb[v];
     rot_b(r, ab, o);
 #pragma unroll
     for (int k = 0; k < NV; ++k) adjF[((F.c * MF + F.f) * F.QS + q) * NV + k] = o[k];
@@ -226,6 +230,93 @@ __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain,
     else sp += s;
   }
   if (k >= NV) pown[(i - nplain) * NV + (k - NV)] = sp;
+}
+
+// Viscous face fluxes (Navier-Stokes): the adjoint of their inputs, one
+// thread per owned face and input direction k (one point per face):
+// k < 5 the cell's face value, 5..9 the neighbour's face value (on a
+// boundary face of the second group the free-stream state of the ghost),
+// 10..21 the cell's gradient of (T, u, v, w), 22..33 the neighbour's.  The
+// flux leaves R_c and enters R_nb, so the weights are ws (lam_nb - lam_c),
+// -ws lam_c on a boundary face, whose ghost side takes the cell's own
+// gradient (CALCULATE_BOUNDED_VISCOUS) and its ghost state from
+// boundary_ghost.  Each column is one Dual<1> pass of viscous_flux.  Adds
+// to adjF and pown (written before by the face kernels, one thread per
+// element) and writes gadj[c][f] (the adjoint of cell c's gradient through
+// face f).
+constexpr int VIS_DIRS = 34;
+__global__ void __launch_bounds__(128) k_adj_visc(Problem p, int64_t nplain, const double* __restrict__ U,
+                                                  const double* __restrict__ lam, double* __restrict__ adjF,
+                                                  double* __restrict__ pown, double* __restrict__ gadj) {
+  using D = Dual<1>;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = t / VIS_DIRS;
+  const int k = (int)(t % VIS_DIRS);
+  if (i >= p.nown) return;
+  const FaceRef F = face_ref(p, i);
+  const bool bnd = F.nb < 0;
+  if (bnd && (k >= 22 || (k >= 5 && k < 10 && i < nplain))) return;
+  const int64_t c = F.c, nb = F.nb;
+  const int f = F.f, nf = F.nf, QS = F.QS;
+  const int code = bnd ? p.bc[c * MF + f] : 0;
+  double r[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) r[j] = p.rot[(c * MF + f) * 4 + j];
+  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
+  const double* dul = (const double*)p.dul;
+  const int qq = bnd ? 0 : p.qperm[(c * MF + f) * QS];
+  D L[NV], R[NV], gl[12], gr[12];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    L[v] = D(U[c * NV + v] + dul[(c * MF + f) * QS * NV + v]);
+    L[v].d[0] = k == v ? 1.0 : 0.0;
+  }
+  if (!bnd) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      R[v] = D(U[nb * NV + v] + dul[((nb * MF + nf) * QS + qq) * NV + v]);
+      R[v].d[0] = k == 5 + v ? 1.0 : 0.0;
+    }
+  } else {
+    D bcs[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      bcs[v] = D(p.bc_state[v]);
+      bcs[v].d[0] = k == 5 + v ? 1.0 : 0.0;
+    }
+    boundary_ghost(p, code, r, L, bcs, R);
+  }
+  const double* g0 = p.ulv + (c * MF + f) * QS * 12;
+  const double* g1 = bnd ? g0 : p.ulv + ((nb * MF + nf) * QS + qq) * 12;
+#pragma unroll
+  for (int j = 0; j < 12; ++j) {
+    gl[j] = D(g0[j]);
+    gl[j].d[0] = k == 10 + j ? 1.0 : 0.0;
+    if (bnd) {
+      gr[j] = gl[j];
+    } else {
+      gr[j] = D(g1[j]);
+      gr[j].d[0] = k == 22 + j ? 1.0 : 0.0;
+    }
+  }
+  D fv[NV];
+  viscous_flux(p, r, p.dih[c * MF + f], L, R, gl, gr, fv, code >= 1 && code <= 4 ? 0.0 : p.lamx);
+  double s = 0.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double w = bnd ? -ws * lam[c * NV + v] : ws * (lam[nb * NV + v] - lam[c * NV + v]);
+    s += w * fv[v].d[0];
+  }
+  if (k < 5) {
+    adjF[(c * MF + f) * QS * NV + k] += s;
+  } else if (k < 10) {
+    if (!bnd) adjF[((nb * MF + nf) * QS + qq) * NV + (k - 5)] += s;
+    else pown[(i - nplain) * NV + (k - 5)] += s;
+  } else if (k < 22) {
+    gadj[(c * MF + f) * 12 + (k - 10)] = s;
+  } else {
+    gadj[(nb * MF + nf) * 12 + (k - 22)] = s;
+  }
 }
 
 // deterministic column sums of a [m][5] array in two passes: k_colsum5_part
@@ -468,8 +559,30 @@ __global__ void __launch_bounds__(128) k_adj_fwd(Problem p, const double* __rest
 // (only the faces of fmask).  Each slot that the reverse map reads is
 // written exactly once.  Face values u_f = u0 + dd_f * slope (or u0 when
 // CHECKSOLX chose first order).
+// (T, u, v, w) of a conserved state and its 4x5 Jacobian (the variables of
+// the viscous least squares, gradients.f90:502-706)
+__device__ __forceinline__ void visc_vars_jac(const Problem& p, const double* u, double (&J)[4][NV]) {
+  Dual<NV> q[NV], pr[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    q[v] = Dual<NV>(u[v]);
+    q[v].d[v] = 1.0;
+  }
+  cons2prim(p.gamma, q, pr);
+  const Dual<NV> s[4] = {pr[4] / (pr[0] * p.r_gas), pr[1], pr[2], pr[3]};
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) J[a][v] = s[a].d[v];
+}
+
+// gadj (Navier-Stokes, else null): the adjoint of each cell's gradient of
+// (T, u, v, w) through each of its faces (k_adj_visc); reversed through the
+// frame (AINVJT), the viscous least squares on stencil 1 and (T, u, v, w)(U)
+// into the same slots as the MUSCL reconstruction's.
 __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, FwdStore fwd, const double* __restrict__ adjF,
-                                                   double* __restrict__ contrib) {
+                                                   double* __restrict__ contrib, const double* __restrict__ U,
+                                                   const double* __restrict__ gadj) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t n = p.n;
   if (c >= n) return;
@@ -480,13 +593,65 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, FwdStore fwd, cons
   for (int f = 0; f < nf; ++f)
 #pragma unroll
     for (int v = 0; v < NV; ++v) self[v] += adjF[(c * MF + f) * NV + v];
+  // viscous gradients: gr[a][k] = sum_d J[d][k] gvv[d][a], gvv[d][a] =
+  // sum_k M_dk (s_a(U_k) - s_a(U_c)); vslot(k, v) adds to stencil slot 1 + k
+  const int64_t vgrp = c >> 5;
+  const int vlane = (int)(c & 31);
+  const double* Mv = (const double*)p.invmat + (vgrp * p.tstride + p.soff[0]) * 32 + vlane;
+  const int32_t* stv = p.sten + vgrp * (int64_t)p.admis_max * (IM + 1) * 32 + vlane;
+  double gvvb[3][4] = {}, sc[4] = {0, 0, 0, 0};
+  if (gadj) {
+    double gb[12] = {};
+    for (int f = 0; f < nf; ++f)
+#pragma unroll
+      for (int j = 0; j < 12; ++j) gb[j] += gadj[(c * MF + f) * 12 + j];
+    const double* Jc = p.jinv + c * 9;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        gvvb[d][a] = Jc[d * 3 + 0] * gb[a * 3 + 0] + Jc[d * 3 + 1] * gb[a * 3 + 1] + Jc[d * 3 + 2] * gb[a * 3 + 2];
+  }
+  // the viscous contribution to stencil slot 1 + k (member state adjoint)
+  auto vslot = [&](int k, double (&out)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = 0.0;
+    if (!gadj) return;
+    const double m0 = Mv[(k * 3 + 0) * 32], m1 = Mv[(k * 3 + 1) * 32], m2 = Mv[(k * 3 + 2) * 32];
+    double sb[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      sb[a] = m0 * gvvb[0][a] + m1 * gvvb[1][a] + m2 * gvvb[2][a];
+      sc[a] -= sb[a];
+    }
+    const int64_t y = stv[(k + 1) * 32];
+    double J[4][NV];
+    visc_vars_jac(p, U + y * NV, J);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = J[0][v] * sb[0] + J[1][v] * sb[1] + J[2][v] * sb[2] + J[3][v] * sb[3];
+  };
+  // the cell's own viscous term (after every vslot)
+  auto vself = [&](double (&out)[NV]) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = 0.0;
+    if (!gadj) return;
+    double J[4][NV];
+    visc_vars_jac(p, U + c * NV, J);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v] = J[0][v] * sc[0] + J[1][v] * sc[1] + J[2][v] * sc[2] + J[3][v] * sc[3];
+  };
   auto put = [&](int slot, int v, double x) { contrib[((int64_t)slot * n + c) * NV + v] = x; };
   if (m.first) {
+    for (int k = 0; k < IM; ++k) {
+      double vk[NV];
+      vslot(k, vk);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) put(0, v, self[v]);
-    for (int k = 0; k < IM; ++k)
+      for (int v = 0; v < NV; ++v) put(1 + k, v, vk[v]);
+    }
+    double vs[NV];
+    vself(vs);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) put(1 + k, v, 0.0);
+    for (int v = 0; v < NV; ++v) put(0, v, self[v] + vs[v]);
     for (int f = 0; f < MF; ++f)
       if (m.fmask >> f & 1)
 #pragma unroll
@@ -536,10 +701,12 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, FwdStore fwd, cons
   const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
   for (int k = 0; k < IM; ++k) {
     const double m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
+    double vk[NV];
+    vslot(k, vk);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const double ck = m0 * gbar[0][v] + m1 * gbar[1][v] + m2 * gbar[2][v];
-      put(1 + k, v, ck + bounds(1 + k, v));
+      put(1 + k, v, ck + bounds(1 + k, v) + vk[v]);
       self[v] -= ck;
     }
   }
@@ -547,8 +714,10 @@ __global__ void __launch_bounds__(128) k_adj_muscl(Problem p, FwdStore fwd, cons
     if (m.fmask >> f & 1)
 #pragma unroll
       for (int v = 0; v < NV; ++v) put(1 + IM + f, v, bounds(1 + IM + f, v));
+  double vs[NV];
+  vself(vs);
 #pragma unroll
-  for (int v = 0; v < NV; ++v) put(0, v, self[v] - (lob[v] + hib[v]) + bounds(0, v));
+  for (int v = 0; v < NV; ++v) put(0, v, self[v] - (lob[v] + hib[v]) + bounds(0, v) + vs[v]);
 }
 
 // mu[j] = sum over the slots that point at cell j (reverse map, fixed order)
@@ -571,9 +740,12 @@ struct Dp5 {
   double v[NV];
 };
 
-// tangent of the face values: tdul[c][f] = d(u_f - u0) along dU
+// tangent of the face values: tdul[c][f] = d(u_f - u0) along dU; tgr
+// (Navier-Stokes, else null): the tangent of the cell's gradient of
+// (T, u, v, w), [n][12] in the layout of ulv
 __global__ void __launch_bounds__(128) k_jvp_muscl(Problem p, const double* __restrict__ U,
-                                                   const double* __restrict__ dU, double* __restrict__ tdul) {
+                                                   const double* __restrict__ dU, double* __restrict__ tdul,
+                                                   double* __restrict__ tgr) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
   using D = Dual<1>;
@@ -589,23 +761,56 @@ __global__ void __launch_bounds__(128) k_jvp_muscl(Problem p, const double* __re
   const int lane = (int)(c & 31);
   const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
   const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
-  D g[3][NV];
+  D g[3][NV], gvv[3][4];
 #pragma unroll
-  for (int d = 0; d < 3; ++d)
+  for (int d = 0; d < 3; ++d) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) g[d][v] = D(0.0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) gvv[d][a] = D(0.0);
+  }
+  D s0[4];
+  if (tgr) {
+    D pm0[NV];
+    cons2prim(p.gamma, u0, pm0);
+    s0[0] = pm0[4] / (pm0[0] * p.r_gas);
+    s0[1] = pm0[1];
+    s0[2] = pm0[2];
+    s0[3] = pm0[3];
+  }
   for (int k = 0; k < IM; ++k) {
     const int64_t y = st[(k + 1) * 32];
     const double m0 = M[(k * 3 + 0) * 32], m1 = M[(k * 3 + 1) * 32], m2 = M[(k * 3 + 2) * 32];
+    D uy[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      D uy(U[y * NV + v]);
-      uy.d[0] = dU[y * NV + v];
-      const D du = uy - u0[v];
+      uy[v] = D(U[y * NV + v]);
+      uy[v].d[0] = dU[y * NV + v];
+      const D du = uy[v] - u0[v];
       g[0][v] = g[0][v] + m0 * du;
       g[1][v] = g[1][v] + m1 * du;
       g[2][v] = g[2][v] + m2 * du;
     }
+    if (tgr) {
+      D py[NV];
+      cons2prim(p.gamma, uy, py);
+      const D ds[4] = {py[4] / (py[0] * p.r_gas) - s0[0], py[1] - s0[1], py[2] - s0[2], py[3] - s0[3]};
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        gvv[0][a] = gvv[0][a] + m0 * ds[a];
+        gvv[1][a] = gvv[1][a] + m1 * ds[a];
+        gvv[2][a] = gvv[2][a] + m2 * ds[a];
+      }
+    }
+  }
+  if (tgr) {
+    const double* Jc = p.jinv + c * 9;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int kk = 0; kk < 3; ++kk)
+        tgr[c * 12 + a * 3 + kk] =
+            (Jc[0 * 3 + kk] * gvv[0][a] + Jc[1 * 3 + kk] * gvv[1][a] + Jc[2 * 3 + kk] * gvv[2][a]).d[0];
   }
   D mn[NV], mx[NV];
 #pragma unroll
@@ -656,10 +861,12 @@ __global__ void __launch_bounds__(128) k_jvp_muscl(Problem p, const double* __re
     for (int v = 0; v < NV; ++v) tdul[(c * MF + f) * NV + v] = first ? 0.0 : (face_d(f, v) * slope[v]).d[0];
 }
 
-// tangent of the face fluxes (owner and negated neighbour copy)
+// tangent of the face fluxes (owner and negated neighbour copy); with tgr
+// (Navier-Stokes) the viscous flux's tangent subtracted, as the residual
+// subtracts the viscous fluxes
 __global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __restrict__ U,
                                                   const double* __restrict__ dU, const double* __restrict__ tdul,
-                                                  Dp5 dp, double* __restrict__ tflux) {
+                                                  Dp5 dp, double* __restrict__ tflux, const double* __restrict__ tgr) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   using D = Dual<1>;
@@ -702,6 +909,25 @@ __global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __res
     rot_b(r, h, fl);
 #pragma unroll
     for (int v = 0; v < NV; ++v) tf[v] = tf[v] + fl[v].d[0] * ws;
+    if (tgr) {
+      const int qq = nb >= 0 ? p.qperm[(c * MF + f) * QS + q] : 0;
+      const double* g0 = p.ulv + ((c * MF + f) * QS + q) * 12;
+      const double* g1 = nb >= 0 ? p.ulv + ((nb * MF + nf) * QS + qq) * 12 : g0;
+      const double* t0 = tgr + c * 12;
+      const double* t1 = nb >= 0 ? tgr + nb * 12 : t0;
+      D gl[12], gr[12], fv[NV];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        gl[j] = D(g0[j]);
+        gl[j].d[0] = t0[j];
+        gr[j] = D(g1[j]);
+        gr[j].d[0] = t1[j];
+      }
+      const int code = nb >= 0 ? 0 : p.bc[c * MF + f];
+      viscous_flux(p, r, p.dih[c * MF + f], L, R, gl, gr, fv, code >= 1 && code <= 4 ? 0.0 : p.lamx);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) tf[v] = tf[v] - fv[v].d[0] * ws;
+    }
   }
 #pragma unroll
   for (int v = 0; v < NV; ++v) tflux[(c * MF + f) * NV + v] = tf[v];
@@ -778,7 +1004,7 @@ void adjoint_release(ucg_engine* e) {
                                &e->adj_fcell,  &e->adj_traj,    &e->adj_bar,   &e->adj_tmp,      &e->adj_fwd,
                                &e->adjw_face,  &e->adjw_gbar,   &e->adjw_scr,  &e->adjw_self,    &e->adjw_contrib,
                                &e->adjw_rptr,  &e->adjw_rsrc,   &e->adjw_lam,     &e->adjw_mu,
-                               &e->adjw_pface, &e->adjw_tmp};
+                               &e->adjw_pface, &e->adjw_tmp,    &e->adj_gadj,  &e->adj_tgr};
   for (auto* b : all) {
     if (b->p) e->bytes -= (int64_t)b->bytes;
     release(*b);
@@ -842,6 +1068,10 @@ int adj_setup(ucg_engine* e) {
   rc = rc ? rc : get(e->adj_bar, (size_t)4 * n * NV * 8 + 64 * 8);
   rc = rc ? rc : get(e->adj_tmp, (size_t)2 * n * NV * 8);
   rc = rc ? rc : get(e->adj_fwd, (size_t)n * (FWD_D * 8 + FWD_B));
+  if (e->cfg.governing == 1) {  // viscous: gradient adjoints per face, gradient tangents per cell
+    rc = rc ? rc : get(e->adj_gadj, (size_t)n * MF * 12 * 8);
+    rc = rc ? rc : get(e->adj_tgr, (size_t)n * 12 * 8);
+  }
   if (rc) return rc;
   CK(cudaMemcpyAsync(e->adj_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
   if (cnt[n]) CK(cudaMemcpyAsync(e->adj_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
@@ -870,7 +1100,9 @@ int adj_forward(ucg_engine* e, const Problem& p, const double* U) {
 }
 
 int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* lam, double* mu, double* psum) {
-  int rc = adj_forward(e, p, U);
+  const bool ns = e->cfg.governing == 1;
+  int rc = ns ? launch_recon(e, p, U) : UCG_OK;  // Navier-Stokes: the cells' gradients (ulv)
+  rc = rc ? rc : adj_forward(e, p, U);
   if (rc) return rc;
   const int64_t n = e->n;
   const int64_t nplain = e->nown_plain, nbnd = e->nown - nplain;
@@ -879,8 +1111,14 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
   if (nbnd)
     k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, (double*)e->adj_face.p,
                                                                       (double*)e->adj_pface.p);
+  if (ns) {
+    k_adj_visc<<<blocks_for(e->nown * VIS_DIRS, 128), 128, 0, e->stream>>>(
+        p, nplain, U, lam, (double*)e->adj_face.p, (double*)e->adj_pface.p, (double*)e->adj_gadj.p);
+    e->launches++;
+  }
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
-                                                         (double*)e->adj_contrib.p);
+                                                         (double*)e->adj_contrib.p, U,
+                                                         ns ? (const double*)e->adj_gadj.p : nullptr);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, mu);
@@ -904,9 +1142,10 @@ int jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* d
   int rc = launch_recon(e, p, U);
   if (rc) return rc;
   const int64_t n = e->n;
-  k_jvp_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p);
+  double* tgr = e->cfg.governing == 1 ? (double*)e->adj_tgr.p : nullptr;
+  k_jvp_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p, tgr);
   k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p, dp,
-                                                              (double*)e->adj_tflux.p);
+                                                              (double*)e->adj_tflux.p, tgr);
   k_jvp_sum<<<blocks_for(n, 256), 256, 0, e->stream>>>(p, (const double*)e->adj_tflux.p, dR);
   e->launches += 3;
   CK(cudaGetLastError());
@@ -918,7 +1157,7 @@ int force_device(ucg_engine* e, const Problem& p, const double* U, const double*
   int rc = launch_recon(e, p, U);
   if (rc) return rc;
   if (dU) {
-    k_jvp_muscl<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p);
+    k_jvp_muscl<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p, nullptr);
     e->launches++;
   }
   k_force_cell<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p,
@@ -937,7 +1176,7 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
   k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p,
                                                           (double*)e->adj_face.p, 1.0);
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
-                                                         (double*)e->adj_contrib.p);
+                                                         (double*)e->adj_contrib.p, U, nullptr);
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adj_rptr.p,
                                                           (const int64_t*)e->adj_rsrc.p,
                                                           (const double*)e->adj_contrib.p, g);
@@ -1061,7 +1300,7 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   double* tdul = (double*)e->adjw_face.p;
   double* tflux = (double*)e->adjw_contrib.p;
   if ((rc = launch_weno_tangent(e, p, U, dU, (const double*)e->adjw_gbar.p, tdul))) return rc;
-  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux);
+  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux, nullptr);
   k_jvp_sum<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, tflux, dR);
   e->launches += 2;
   CK(cudaGetLastError());

@@ -638,12 +638,13 @@ __device__ __forceinline__ double face_weight(const Problem& p, int ft, int q) {
 __device__ __forceinline__ int face_nq(const Problem& p, int ft) { return ft == 5 ? p.nq_quad : p.nq_tri; }
 
 // Sutherland's law (SUTHERLAND, src/flow_operations.f90:2609-2640);
-// (t1/t0)^1.5 written as r*sqrt(r).
-__device__ __forceinline__ void sutherland(const Problem& p, double rho, double pr, double* mu, double* lam) {
+// (t1/t0)^1.5 written as r*sqrt(r).  S: double or a dual number.
+template <typename S>
+__device__ __forceinline__ void sutherland(const Problem& p, S rho, S pr, S* mu, S* lam) {
   const double suther = 0.412158681;
-  double t1 = pr / (rho * p.r_gas);
+  S t1 = pr / (rho * p.r_gas);
   double t0 = p.pres / (p.rres * p.r_gas);
-  double r = t1 / t0;
+  S r = t1 / t0;
   *mu = p.visc * (r * sqrt(r)) * ((t0 + suther * t0) / (t1 + suther * t0));
   *lam = (*mu) * p.r_gas * p.gamma / (p.prandtl * (p.gamma - 1.0));
 }
@@ -806,44 +807,45 @@ __device__ __forceinline__ void boundary_ghost(const Problem& p, int code, const
 }
 
 // `damp` multiplies the jump term: LAMX on interior and far-field faces, 0
-// on faces with boundary codes 1-4 (flux_p.f90:1872-1874).
-__device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, double dih, const double* cl,
-                                             const double* cr, const double* gl, const double* gr, double* fv,
-                                             double damp) {
+// on faces with boundary codes 1-4 (flux_p.f90:1872-1874).  S: double or a
+// dual number (the discrete adjoint and tangent).
+template <typename S>
+__device__ __forceinline__ void viscous_flux(const Problem& p, const double* r, double dih, const S* cl, const S* cr,
+                                             const S* gl, const S* gr, S* fv, double damp) {
   double nx = r[0] * r[3], ny = r[1] * r[3], nz = r[2];
   double nn[3] = {nx, ny, nz};
-  double lv[NV], rv[NV];
+  S lv[NV], rv[NV];
   cons2prim(p.gamma, cl, lv);
   cons2prim(p.gamma, cr, rv);
-  double mul, mur, laml, lamr;
+  S mul, mur, laml, lamr;
   sutherland(p, lv[0], lv[4], &mul, &laml);
   sutherland(p, rv[0], rv[4], &mur, &lamr);
   // gradient rows u, v, w, T; stored components are T, u, v, w
   const int src[4] = {1, 2, 3, 0};
-  double jump[4] = {rv[1] - lv[1], rv[2] - lv[2], rv[3] - lv[3],
-                    rv[4] / (rv[0] * p.r_gas) - lv[4] / (lv[0] * p.r_gas)};
+  S jump[4] = {rv[1] - lv[1], rv[2] - lv[2], rv[3] - lv[3],
+               rv[4] / (rv[0] * p.r_gas) - lv[4] / (lv[0] * p.r_gas)};
   const double vd = (4.0 / 3.0) / fabs(dih);
-  double gg[4][3];
+  S gg[4][3];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       gg[a][k] = (gl[src[a] * 3 + k] + gr[src[a] * 3 + k]) / 2.0 + damp * (vd * nn[k] * jump[a]);
-  double lam2 = 0.5 * (laml + lamr), mu2 = 0.5 * (mul + mur);
-  double ux = gg[0][0], uy = gg[0][1], uz = gg[0][2];
-  double vx = gg[1][0], vy = gg[1][1], vz = gg[1][2];
-  double wx = gg[2][0], wy = gg[2][1], wz = gg[2][2];
-  double txx = mu2 * ((4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz);
-  double tyy = mu2 * ((4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz);
-  double tzz = mu2 * ((4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy);
-  double txy = mu2 * (uy + vx), txz = mu2 * (wx + uz), tyz = mu2 * (vz + wy);
-  double rho12 = 0.5 * (cl[0] + cr[0]);
-  double u12 = 0.5 * (cl[1] + cr[1]) / rho12, v12 = 0.5 * (cl[2] + cr[2]) / rho12, w12 = 0.5 * (cl[3] + cr[3]) / rho12;
-  double qx = lam2 * gg[3][0], qy = lam2 * gg[3][1], qz = lam2 * gg[3][2];  // -Q
-  double fx4 = qx + u12 * txx + v12 * txy + w12 * txz;
-  double fy4 = qy + u12 * txy + v12 * tyy + w12 * tyz;
-  double fz4 = qz + u12 * txz + v12 * tyz + w12 * tzz;
-  fv[0] = 0.0;
+  S lam2 = 0.5 * (laml + lamr), mu2 = 0.5 * (mul + mur);
+  S ux = gg[0][0], uy = gg[0][1], uz = gg[0][2];
+  S vx = gg[1][0], vy = gg[1][1], vz = gg[1][2];
+  S wx = gg[2][0], wy = gg[2][1], wz = gg[2][2];
+  S txx = mu2 * ((4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz);
+  S tyy = mu2 * ((4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz);
+  S tzz = mu2 * ((4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy);
+  S txy = mu2 * (uy + vx), txz = mu2 * (wx + uz), tyz = mu2 * (vz + wy);
+  S rho12 = 0.5 * (cl[0] + cr[0]);
+  S u12 = 0.5 * (cl[1] + cr[1]) / rho12, v12 = 0.5 * (cl[2] + cr[2]) / rho12, w12 = 0.5 * (cl[3] + cr[3]) / rho12;
+  S qx = lam2 * gg[3][0], qy = lam2 * gg[3][1], qz = lam2 * gg[3][2];  // -Q
+  S fx4 = qx + u12 * txx + v12 * txy + w12 * txz;
+  S fy4 = qy + u12 * txy + v12 * tyy + w12 * tyz;
+  S fz4 = qz + u12 * txz + v12 * tyz + w12 * tzz;
+  fv[0] = S(0.0);
   fv[1] = nx * txx + ny * txy + nz * txz;
   fv[2] = nx * txy + ny * tyy + nz * tyz;
   fv[3] = nx * txz + ny * tyz + nz * tzz;

@@ -80,7 +80,7 @@ struct ucg_engine {
   // discrete adjoint / tangent (adjoint.cu)
   bool adj_ready = false;
   DevBuf adj_face, adj_contrib, adj_rptr, adj_rsrc, adj_lam, adj_mu, adj_pface, adj_tflux, adj_tdul, adj_tU,
-      adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd;
+      adj_fcell, adj_traj, adj_bar, adj_tmp, adj_fwd, adj_gadj, adj_tgr;
   // discrete adjoint of the WENO reconstruction (adjoint_weno.cu)
   bool adjw_ready = false;
   DevBuf adjw_face, adjw_gbar, adjw_scr, adjw_self, adjw_contrib, adjw_rptr, adjw_rsrc, adjw_lam, adjw_mu,
