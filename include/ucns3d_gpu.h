@@ -270,8 +270,8 @@ int ucg_synchronize(ucg_engine* e);
  * evaluations of the current state, measured with CUDA events on the
  * handle's stream, into ms[4]: ms[0] reconstruction, ms[1] face fluxes,
  * ms[2] time step (CALCULATE_CFL), ms[3] the stencil least-squares kernel
- * alone (part of ms[0]; all of it for MUSCL IORDER 1).  For profiling; it
- * leaves the state unchanged.                                              */
+ * alone (part of ms[0]; all of it for MUSCL IORDER 1), after one untimed
+ * evaluation.  For profiling; it leaves the state unchanged.               */
 int ucg_time_kernels(ucg_engine* e, int32_t reps, double* ms);
 
 /* Bounded device waits.  The opt-in least squares through the shared-memory
@@ -425,8 +425,9 @@ int ucg_adjoint_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double
 int ucg_tangent_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, const double* dU0,
                         const double* dp, double* J, double* dJ);
 /* Average device times over `reps` evaluations at the current state (CUDA
- * events on the handle's stream), into ms[3]: ms[0] residual (reconstruction
- * + fluxes), ms[1] residual VJP, ms[2] residual JVP (MUSCL or WENO).       */
+ * events on the handle's stream), after one untimed evaluation, into ms[3]:
+ * ms[0] residual (reconstruction + fluxes), ms[1] residual VJP, ms[2]
+ * residual JVP (MUSCL or WENO).                                            */
 int ucg_time_adjoint(ucg_engine* e, int32_t reps, double* ms);
 
 /* Message of the last failure of ucg_create (no handle exists then). */
