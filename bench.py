@@ -1,5 +1,6 @@
 """Benchmark: cell-RK-stage updates per second of the explicit residual
-engine on one B200 (or N independent replicas under torchrun).
+engine on one B200 (or N independent replicas under torchrun; with
+--partition, one mesh split over the N ranks).
 
 Default workload: the isentropic vortex on a periodic 64^3 hexahedral box
 (262,144 cells), Euler, 5th-order WENO + HLLC, SSP-RK3 - the mixed-precision
@@ -62,13 +63,17 @@ def parse():
     ap.add_argument("--setup", action="store_true",
                     help="also time the reconstruction-table set-up: host (ucp_prepare + upload) against the "
                          "device (ucg_build_recon) on meshes with one matrix set per cell")
+    ap.add_argument("--partition", action="store_true",
+                    help="split the mesh over the ranks (recursive coordinate bisection, a halo of cell states "
+                         "moved over NCCL in every RK stage: strong scaling) instead of one replica per rank")
     ap.add_argument("--cpu-n", type=int, default=0,
                     help="mesh size of the CPU baseline and reference arm (0: the benchmarked --n)")
     return ap.parse_args()
 
 
 def dist_init():
-    """One process per GPU under torchrun; replicas only (no data exchange)."""
+    """One process per GPU under torchrun: replicas (no data exchange), or
+    the partitions of one mesh with --partition."""
     import torch
     import torch.distributed as dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -622,11 +627,89 @@ def run_setup(local):
     return out
 
 
+def main_partition(args, ws, rank, local):
+    """The workload split over the ranks (ucns3d_b200.partition): every rank
+    builds the same mesh and plan, steps its partition with halo transfers in
+    each stage and CFL time steps reduced over the ranks; value = the whole
+    mesh's cell-stages per second, timed on the device as the slowest rank."""
+    import numpy as np
+    import torch
+    from ucns3d_b200 import _native as N
+    from ucns3d_b200.partition import HaloEngine, PartitionPlan, rcb
+
+    case = make_case(args, N.UCG_MIXED)
+    ncells = case.mesh.ncells
+    plan = PartitionPlan(case.mesh, rcb(case.mesh.centres(), ws))
+    h = HaloEngine(plan, rank, case.cfg, device=local)
+    h.set_state(case.U0)
+    for _ in range(args.warmup):
+        h.rk3_step(h.compute_dt(case.cfl))
+    h.engine.synchronize()
+    h.engine.check_health()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize(local)
+    sampler.start()
+    l0 = h.engine.launch_count
+    ev0.record(h.stream)
+    for _ in range(args.steps):
+        h.rk3_step(h.compute_dt(case.cfl))
+    ev1.record(h.stream)
+    ev1.synchronize()
+    torch.cuda.synchronize(local)
+    launches = h.engine.launch_count - l0
+    clocks = sampler.stop()
+    barrier(ws)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), ws, local)
+    h.engine.check_health()
+    # end to end: the rank's rows from pinned host memory, one step, its
+    # owned rows back, every step
+    U = plan.local(rank, case.U0)
+    hin = torch.from_numpy(U).pin_memory()
+    hout = torch.empty((int(plan.owned[rank].sum()), 5), dtype=torch.float64).pin_memory()
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h.engine.set_state(hin.numpy())
+        h.rk3_step(h.compute_dt(case.cfl))
+        hout.numpy()[:] = h.owned_state()
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0, ws, local)
+    local_cells = len(plan.cells[rank])
+    owned = int(plan.owned[rank].sum())
+    halo_rows = max_over_ranks(float(len(h.lists.recv)), ws, local)
+    h.close()
+    if rank == 0:
+        value = ncells * 3 * args.steps / (ms / 1000.0)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "mixed: f32 tables/reconstruction, f64 flux/accumulate/update",
+            "data": "synthetic (seeded mesh and analytic initial condition)",
+            "config": {"workload": args.case, "cells": ncells, "n": args.n, "scheme": scheme_label(case, 1),
+                       "parallelism": f"partitions x{ws} (recursive coordinate bisection; cell-state halo "
+                                      f"over NCCL each stage)",
+                       "rank0_cells": {"owned": owned, "local": local_cells},
+                       "max_halo_rows": int(halo_rows)},
+            "e2e": {"value": ncells * 3 * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": int(hin.numpy().nbytes), "d2h_bytes_per_step": int(hout.numpy().nbytes)},
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
     if args.impl == "reference":
         main_reference(args, ws, rank, local)
+        return
+    if args.partition:
+        main_partition(args, ws, rank, local)
         return
     import numpy as np
     from ucns3d_b200 import _native as N

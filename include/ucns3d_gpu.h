@@ -332,6 +332,36 @@ int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t max_inner, 
  * the handle's stream.  UCG_EINVAL without MOOD. */
 int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
 
+/* ---------------------------------------------------------------- partitions
+ * One engine per rank of a partitioned mesh.  The rank's mesh is its owned
+ * cells plus a halo: their face neighbours, every stencil member of both,
+ * and the neighbours' face neighbours, numbered in increasing global index
+ * (so each face keeps its owning side), with the tables of the whole mesh
+ * sliced to it.  The residual of an owned cell is then that of the whole
+ * mesh once the halo holds the current states.  UCNS3D exchanges cell means
+ * (EXCHANGE_HIGHER, src/communications.f90:1085-1246) and partition-face
+ * quadrature values (EXHBOUNDHIGHER, :1745-1956) in each stage; here the
+ * deeper halo is reconstructed locally and only cell states travel.
+ *
+ * ucg_rk3_stage: RK3 stage `stage` (1, 2, 3) of step size dt, the same
+ *   launches as the corresponding third of ucg_rk3_step (which equals the
+ *   three stages in order).  UCG_EINVAL with MOOD.
+ * ucg_halo_set: the rows this rank sends (owned cells, repeated per peer,
+ *   in the order the peers expect) and receives (halo cells, each once), as
+ *   the caller's cell indices.
+ * ucg_halo_pack / ucg_halo_unpack: gather the send rows of the input state
+ *   of `stage` (1: U^n, 2: U^(1), 3: U^(2)) into a DEVICE buffer
+ *   [nsend][5], or scatter a DEVICE buffer [nrecv][5] into the receive rows,
+ *   asynchronously on the handle's stream; the caller orders its transfer
+ *   (NCCL or a device copy) on that stream.  The step of a rank is:
+ *   unpack(1) <- peers' pack(1); stage 1; the same for stages 2 and 3.
+ * No counterpart entry points in the reference (its exchange is MPI inside
+ * the time loop, src/time_p.f90:885-1027).                                 */
+int ucg_rk3_stage(ucg_engine* e, int32_t stage, double dt);
+int ucg_halo_set(ucg_engine* e, const int32_t* send_cells, int64_t nsend, const int32_t* recv_cells, int64_t nrecv);
+int ucg_halo_pack(ucg_engine* e, int32_t stage, double* send_buf);
+int ucg_halo_unpack(ucg_engine* e, int32_t stage, const double* recv_buf);
+
 /* The cudaStream_t of the handle, as an opaque pointer. */
 void* ucg_get_stream(ucg_engine* e);
 /* Kernel launches issued by the handle since creation. */

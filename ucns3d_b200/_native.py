@@ -155,7 +155,7 @@ ENGINE_SYMBOLS = [
     "ucg_create_error", "ucg_force", "ucg_force_vjp", "ucg_residual_vjp", "ucg_residual_jvp", "ucg_adjoint_run",
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
     "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon", "ucg_implicit_step",
-    "ucg_dual_time_step",
+    "ucg_dual_time_step", "ucg_rk3_stage", "ucg_halo_set", "ucg_halo_pack", "ucg_halo_unpack",
 ]
 
 
@@ -234,6 +234,15 @@ def engine() -> C.CDLL:
                                            C.POINTER(C.c_int32)]
         lib.ucg_build_recon.restype = C.c_int
         lib.ucg_build_recon.argtypes = [vp, C.POINTER(UcgShapes), C.POINTER(UcgRecon)]
+        lib.ucg_rk3_stage.restype = C.c_int
+        lib.ucg_rk3_stage.argtypes = [vp, C.c_int32, C.c_double]
+        lib.ucg_halo_set.restype = C.c_int
+        lib.ucg_halo_set.argtypes = [vp, _i32p, C.c_int64, _i32p, C.c_int64]
+        # device buffers, passed as addresses
+        lib.ucg_halo_pack.restype = C.c_int
+        lib.ucg_halo_pack.argtypes = [vp, C.c_int32, vp]
+        lib.ucg_halo_unpack.restype = C.c_int
+        lib.ucg_halo_unpack.argtypes = [vp, C.c_int32, vp]
         lib.ucg_tangent_run.restype = C.c_int
         lib.ucg_tangent_run.argtypes = [vp, C.c_int32, C.c_double, _f64p, _f64p, _f64p, _f64p]
         _engine = lib

@@ -53,7 +53,8 @@ def build_prep(force=False):
 # the reconstruction kernels are split by precision and order because the
 # IORDER 4 instantiations dominate the compile time
 ENGINE_TUS = ("recon_char_p4.cu", "recon_f64_p4.cu", "recon_f32_p4.cu", "recon_char.cu", "recon_f64.cu", "recon_f32.cu",
-              "adjoint_weno.cu", "adjoint.cu", "engine.cu", "static_scratch.cu", "setup.cu", "implicit.cu")
+              "adjoint_weno.cu", "adjoint.cu", "engine.cu", "static_scratch.cu", "setup.cu", "implicit.cu",
+              "halo.cu")
 ENGINE_HDRS = ("kernels.cuh", "recon2.cuh", "device.cuh", "ad.cuh", "engine_internal.h", "expand.cuh", "../common/rules.h")
 # per-unit flags: the device set-up evaluates the host set-up's operations
 # one by one (no fused multiply-adds), so its tables match bit for bit

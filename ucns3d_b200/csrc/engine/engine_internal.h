@@ -76,6 +76,9 @@ struct ucg_engine {
   // n2o[c]; o2n is the inverse.  Empty when the caller's order is kept.
   std::vector<int32_t> n2o, o2n;
   DevBuf d_n2o, permbuf;            // n2o on the device; [n][5] staging of permuted transfers
+  // halo lists of a partition (ucg_halo_set), in the engine's order
+  DevBuf halo_send, halo_recv;
+  int64_t halo_nsend = 0, halo_nrecv = 0;
   double cost_caller = 0.0, cost_rcm = 0.0;  // gather cost of both orders (reorder 1)
   // discrete adjoint / tangent (adjoint.cu)
   bool adj_ready = false;

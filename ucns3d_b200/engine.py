@@ -107,6 +107,28 @@ class Engine:
     def runge_kutta3(self, dt: float):
         self._check(self.lib.ucg_rk3_step(self._h, dt))
 
+    def rk3_stage(self, stage: int, dt: float):
+        """One of the three stages of `runge_kutta3` (1, 2, 3, in order)."""
+        self._check(self.lib.ucg_rk3_stage(self._h, stage, dt))
+
+    # ------------------------------------------------------- partitions
+    def halo_set(self, send_cells: np.ndarray, recv_cells: np.ndarray):
+        """Rows this rank sends (its owned cells, per peer in the peer's
+        order) and receives (halo cells), as cell indices of this mesh."""
+        s = np.ascontiguousarray(send_cells, dtype=np.int32)
+        r = np.ascontiguousarray(recv_cells, dtype=np.int32)
+        self._check(self.lib.ucg_halo_set(self._h, N.ptr(s, C.c_int32), len(s), N.ptr(r, C.c_int32), len(r)))
+
+    def halo_pack(self, stage: int, send_ptr: int):
+        """Gather the send rows of stage `stage`'s input state into the device
+        buffer at `send_ptr` ([nsend][5] FP64), on the engine's stream."""
+        self._check(self.lib.ucg_halo_pack(self._h, stage, C.c_void_p(send_ptr)))
+
+    def halo_unpack(self, stage: int, recv_ptr: int):
+        """Scatter the device buffer at `recv_ptr` ([nrecv][5] FP64) into the
+        receive rows of stage `stage`'s input state, on the engine's stream."""
+        self._check(self.lib.ucg_halo_unpack(self._h, stage, C.c_void_p(recv_ptr)))
+
     def time_marching(self, nsteps: int, cfl: float):
         """nsteps of CALCULATE_CFL + RUNGE_KUTTA3 with dt kept on the device."""
         self._check(self.lib.ucg_step(self._h, cfl, nsteps))
