@@ -355,8 +355,17 @@ int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
  *   asynchronously on the handle's stream; the caller orders its transfer
  *   (NCCL or a device copy) on that stream.  The step of a rank is:
  *   unpack(1) <- peers' pack(1); stage 1; the same for stages 2 and 3.
+ * ucg_set_cell_roles (before ucg_upload_geometry; NULL clears): per cell
+ *   (caller order) 0 owned: stepped; 1 ring 1 (a face neighbour of an owned
+ *   cell): reconstructed, not stepped; 2 the rest of the halo: only read.
+ *   The reconstruction then covers roles 0-1, the face fluxes the faces of
+ *   owned cells, the residual and the update the owned cells; rows of roles
+ *   1-2 of ucg_residual and of the stepped state are unspecified until the
+ *   next unpack.  Without roles every cell is reconstructed and stepped.
+ *   The adjoint, implicit steps and MOOD refuse an engine with roles.
  * No counterpart entry points in the reference (its exchange is MPI inside
  * the time loop, src/time_p.f90:885-1027).                                 */
+int ucg_set_cell_roles(ucg_engine* e, const int8_t* roles);
 int ucg_rk3_stage(ucg_engine* e, int32_t stage, double dt);
 int ucg_halo_set(ucg_engine* e, const int32_t* send_cells, int64_t nsend, const int32_t* recv_cells, int64_t nrecv);
 int ucg_halo_pack(ucg_engine* e, int32_t stage, double* send_buf);

@@ -91,14 +91,62 @@ def test_stage_refuses_mood():
         e.close()
 
 
+def test_cell_roles_are_checked():
+    from test_partition import _case as case
+    m, cfg, U = case("muscl_bump")
+    plan = PartitionPlan(m, rcb(m.centres(), 2))
+    from ucns3d_b200.partition import PartitionMesh
+    pm = PartitionMesh(plan, 0)
+    roles = plan.roles(0)
+    for bad in (np.where(roles == 0, 3, roles), np.full_like(roles, 2)):
+        with pytest.raises(EngineError) as ei:
+            Engine(pm, cfg, roles=bad)
+        assert ei.value.code == N.UCG_EINVAL
+    e = Engine(pm, cfg)  # geometry uploaded: too late for roles
+    try:
+        r = np.ascontiguousarray(roles)
+        import ctypes as C
+        assert e.lib.ucg_set_cell_roles(e._h, r.ctypes.data_as(C.POINTER(C.c_int8))) == N.UCG_ESTATE
+    finally:
+        e.close()
+    e = Engine(pm, cfg, roles=roles)  # the adjoint covers whole meshes
+    try:
+        e.set_state(plan.local(0, U))
+        with pytest.raises(EngineError) as ei:
+            e.force()
+        assert ei.value.code == N.UCG_EINVAL
+    finally:
+        e.close()
+
+
+@pytest.mark.parametrize("restrict", [True, False])
+@pytest.mark.parametrize("name", ["weno5_hex", "cweno4_ns_mixed", "muscl_ns_bump"])
+def test_owned_residual_rows_equal_whole_mesh(name, restrict):
+    m, cfg, U = _case(name)
+    plan = PartitionPlan(m, rcb(m.centres(), 3))
+    whole = Engine(m, cfg)
+    cluster = LocalCluster(plan, cfg, restrict=restrict)
+    try:
+        whole.set_state(U)
+        R = whole.residual()
+        cluster.set_state(U)
+        cluster.exchange(1)
+        got = plan.assemble([h.engine.residual()[plan.owned[h.rank]] for h in cluster.ranks])
+        assert np.array_equal(got, R)
+    finally:
+        cluster.close()
+        whole.close()
+
+
+@pytest.mark.parametrize("restrict", [True, False])
 @pytest.mark.parametrize("precision", [N.UCG_FP64, N.UCG_MIXED])
 @pytest.mark.parametrize("nparts", [2, 3])
 @pytest.mark.parametrize("name", ["weno5_hex", "weno3_tet", "cweno4_tet", "cweno4_ns_mixed", "muscl_ns_bump"])
-def test_partitioned_steps_equal_whole_mesh(name, nparts, precision):
+def test_partitioned_steps_equal_whole_mesh(name, nparts, precision, restrict):
     m, cfg, U = _case(name, precision)
     plan = PartitionPlan(m, rcb(m.centres(), nparts))
     whole = Engine(m, cfg)
-    cluster = LocalCluster(plan, cfg)
+    cluster = LocalCluster(plan, cfg, restrict=restrict)
     try:
         whole.set_state(U)
         cluster.set_state(U)

@@ -56,6 +56,7 @@ int adj_check(ucg_engine* e) {
                 "the adjoint covers MUSCL (scheme 2, IORDER 1, Venkatakrishnan), HLLC, Euler or Navier-Stokes, FP64 form");
   if (e->QS != 1) return fail(e, UCG_EINVAL, "the adjoint needs one face point per face (IORDER 1)");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (!e->roles.empty()) return fail(e, UCG_EINVAL, "the adjoint covers whole meshes (no partition roles)");
   return UCG_OK;
 }
 
@@ -1364,6 +1365,7 @@ int adjw_setup(ucg_engine* e) {
     return fail(e, UCG_EINVAL,
                 "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, CWENO with or without WENO-Z), HLLC, Euler, FP64 form, without MOOD");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (!e->roles.empty()) return fail(e, UCG_EINVAL, "the adjoint covers whole meshes (no partition roles)");
   if (e->adjw_ready) return UCG_OK;
   const int64_t n = e->n, ngrp = (n + 31) / 32;
   const int A = c.admis_max, IM = c.imax, W = IM + 1, ID = c.ideg;

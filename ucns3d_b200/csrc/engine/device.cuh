@@ -21,7 +21,8 @@ enum : unsigned { HEALTH_NONPHYS = 1u };  // HEALTH_TIMEOUT = 2 below
 // Problem description passed by value to every kernel.  Arrays are device
 // pointers; "[c]" means one entry per cell, cell index fastest where noted.
 struct Problem {
-  int64_t n;
+  int64_t n;     // cells the kernels of a launch cover
+  int64_t nall;  // cells of the engine (more than n for a partition's reconstruction: ucg_set_cell_roles)
   int iorder, ideg, imax, admis_max, ideg2, imax2, ees, scheme, governing, wenoz;
   int nq_quad, nq_tri;
   double gamma, prandtl, visc, r_gas, pres, rres, lwci, weno_eps, kappa_ven, lamx;

@@ -74,6 +74,7 @@ Problem make_problem(ucg_engine* e) {
   std::memset(&p, 0, sizeof(p));
   const ucg_config& c = e->cfg;
   p.n = e->n;
+  p.nall = e->n;
   p.iorder = c.iorder;
   p.ideg = c.ideg;
   p.imax = c.imax;
@@ -165,7 +166,7 @@ template <typename T>
 int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
   const ucg_config& c = e->cfg;
   if (c.scheme == 2 && c.iorder == 1) {
-    unsigned blocks = (unsigned)((e->n + 127) / 128);
+    unsigned blocks = (unsigned)((p.n + 127) / 128);
     const bool vk = c.limiter == 7;
     if (c.governing == 1) {
       if (vk) k_muscl<T, true, true><<<blocks, 128, 0, e->stream>>>(p, U);
@@ -185,8 +186,13 @@ int launch_recon_t(ucg_engine* e, const Problem& p, const double* U) {
   return UCG_OK;
 }
 
+// the reconstruction covers cells [0, n_recon) (all of them unless a
+// partition's roles leave its outer halo out); the per-cell records that
+// stencils gather (k_pad_state, k_visc_prim) still cover every cell
 int launch_recon(ucg_engine* e, const Problem& p, const double* U) {
-  return e->mixed ? launch_recon_t<float>(e, p, U) : launch_recon_t<double>(e, p, U);
+  Problem pr = p;
+  pr.n = e->n_recon;
+  return e->mixed ? launch_recon_t<float>(e, pr, U) : launch_recon_t<double>(e, pr, U);
 }
 
 template <typename T, bool NS>
@@ -212,10 +218,14 @@ int launch_faces(ucg_engine* e, const Problem& p, const double* Uc) {
   return UCG_OK;
 }
 
+// the residual and the update cover cells [0, n_update) (all of them unless
+// a partition's roles step only its owned cells)
 template <bool NS, bool CHK>
-void launch_update_t(ucg_engine* e, const Problem& p, int mode, const double* Uc, const double* Un, double* Uo,
+void launch_update_t(ucg_engine* e, const Problem& p0, int mode, const double* Uc, const double* Un, double* Uo,
                      double dt) {
-  unsigned blocks = (unsigned)((e->n + 255) / 256);
+  Problem p = p0;
+  p.n = e->n_update;
+  unsigned blocks = (unsigned)((p.n + 255) / 256);
   switch (mode) {
     case 0: k_update<NS, 0, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
     case 1: k_update<NS, 1, CHK><<<blocks, 256, 0, e->stream>>>(p, Uc, Un, Uo, dt); break;
@@ -655,7 +665,20 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   // device order: n2o[c] = the caller's cell stored at device cell c
   e->n2o.clear();
   e->o2n.clear();
-  if (e->cfg.reorder == 1) {
+  e->n_recon = e->n_update = n;
+  if (!e->roles.empty()) {
+    // a partition: stepped cells, then the other reconstructed cells, then
+    // the rest, each in the caller's order
+    e->n2o.reserve(n);
+    for (int r = 0; r < 3; ++r) {
+      for (int64_t o = 0; o < n; ++o)
+        if (e->roles[o] == r) e->n2o.push_back((int32_t)o);
+      if (r == 0) e->n_update = (int64_t)e->n2o.size();
+      if (r == 1) e->n_recon = (int64_t)e->n2o.size();
+    }
+    e->o2n.assign(n, -1);
+    for (int64_t c = 0; c < n; ++c) e->o2n[e->n2o[c]] = (int32_t)c;
+  } else if (e->cfg.reorder == 1) {
     // reverse Cuthill-McKee, kept only where it gathers from fewer cache
     // lines than the caller's order (a structured or already local order,
     // such as a box numbered row by row, is better left as it is)
@@ -709,13 +732,16 @@ int ucg_upload_geometry(ucg_engine* e, const ucg_geometry* g) {
   // slip wall), then the other boundaries (each group in device cell order),
   // so that kernels branching on the face kind see uniform warps.  An
   // interior face belongs to the side of the lower caller index, so the
-  // renumbering leaves every face flux bit for bit as it was.
+  // renumbering leaves every face flux bit for bit as it was.  With
+  // partition roles only the faces of stepped cells are kept (both their
+  // sides are then reconstructed).
   std::vector<int32_t> own, own_mir, own_bnd;
   own.reserve(n * 3);
   for (int64_t c = 0; c < n; ++c)
     for (int f = 0; f < nfaces[c]; ++f) {
       const int64_t nb = neigh[c * MF + f];
       const int32_t code = (int32_t)(c * 8 + f);
+      if (c >= e->n_update && (nb < 0 || nb >= e->n_update)) continue;
       if (nb >= 0) {
         const int64_t oc = src(c), onb = src(nb);
         if (oc < onb || (oc == onb && f < nface[c * MF + f])) own.push_back(code);

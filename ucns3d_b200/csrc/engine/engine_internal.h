@@ -76,6 +76,11 @@ struct ucg_engine {
   // n2o[c]; o2n is the inverse.  Empty when the caller's order is kept.
   std::vector<int32_t> n2o, o2n;
   DevBuf d_n2o, permbuf;            // n2o on the device; [n][5] staging of permuted transfers
+  // partition roles (ucg_set_cell_roles, caller order; empty: every cell
+  // is stepped): the device order holds the stepped cells [0, n_update),
+  // then the other reconstructed cells [n_update, n_recon), then the rest
+  std::vector<int8_t> roles;
+  int64_t n_recon = 0, n_update = 0;
   // halo lists of a partition (ucg_halo_set), in the engine's order
   DevBuf halo_send, halo_recv;
   int64_t halo_nsend = 0, halo_nrecv = 0;

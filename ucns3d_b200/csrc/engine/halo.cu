@@ -62,6 +62,24 @@ int map_cells(ucg_engine* e, const int32_t* cells, int64_t count, std::vector<in
 
 extern "C" {
 
+int ucg_set_cell_roles(ucg_engine* e, const int8_t* roles) {
+  if (!e) return UCG_EINVAL;
+  if (e->have_geometry) return fail(e, UCG_ESTATE, "the roles go before the geometry upload");
+  if (!roles) {
+    e->roles.clear();
+    return UCG_OK;
+  }
+  if (e->cfg.mood) return fail(e, UCG_EINVAL, "partition roles and MOOD do not combine");
+  int64_t stepped = 0;
+  for (int64_t c = 0; c < e->n; ++c) {
+    if (roles[c] < 0 || roles[c] > 2) return fail(e, UCG_EINVAL, "a role is 0, 1 or 2");
+    stepped += roles[c] == 0;
+  }
+  if (!stepped) return fail(e, UCG_EINVAL, "no cell has role 0");
+  e->roles.assign(roles, roles + e->n);
+  return UCG_OK;
+}
+
 int ucg_rk3_stage(ucg_engine* e, int32_t stage, double dt) {
   if (!e || stage < 1 || stage > 3 || !(dt > 0)) return fail(e, UCG_EINVAL, "bad argument");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");

@@ -288,6 +288,7 @@ extern "C" int ucg_implicit_step(ucg_engine* e, double cfl, int32_t nsteps, int3
   if (!(cfl > 0.0) || !std::isfinite(cfl) || nsteps < 0 || nsweeps < 1)
     return fail(e, UCG_EINVAL, "cfl > 0, nsteps >= 0 and nsweeps >= 1 are needed");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (!e->roles.empty()) return fail(e, UCG_EINVAL, "implicit steps cover whole meshes (no partition roles)");
   cudaSetDevice(e->device);
   int rc = implicit_buffers(e);
   if (rc) return rc;
@@ -319,6 +320,7 @@ extern "C" int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t 
       !(inner_tol >= 0.0))
     return fail(e, UCG_EINVAL, "dt > 0, cfl > 0, max_inner >= 1, nsweeps >= 1 and inner_tol >= 0 are needed");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (!e->roles.empty()) return fail(e, UCG_EINVAL, "implicit steps cover whole meshes (no partition roles)");
   cudaSetDevice(e->device);
   const int64_t n = e->n;
   int rc = implicit_buffers(e);

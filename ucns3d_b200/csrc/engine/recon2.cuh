@@ -1306,6 +1306,10 @@ template <int P, typename T>
 cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cudaStream_t st, int64_t* launches,
                           cudaEvent_t mark) {
   const unsigned b = (unsigned)((p.n + 127) / 128);
+  // the per-cell records that the stencils gather cover every cell, also
+  // those past the reconstructed prefix of a partition (p.n < p.nall)
+  Problem pa = p;
+  pa.n = p.nall > p.n ? p.nall : p.n;
   if (p.mmus) {  // the first MOOD cascade: MUSCL of the selected cells from this stage's G
     k_wpost<P, T, false, false, true, true><<<b, 128, 0, st>>>(p, U);
     ++*launches;
@@ -1321,7 +1325,7 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
     // B200 the vector gather doubled k_lsq's time at IORDER 4 (255
     // registers: it breaks the load schedule) and made IORDER 2 slower by a
     // third, so those keep five 8-byte loads
-    k_pad_state<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+    k_pad_state<P, T><<<(unsigned)((pa.n + 255) / 256), 256, 0, st>>>(pa, U);
     k_lsq<P, T, (P == 3)><<<b, 128, 0, st>>>(p, U);
     ++*launches;
   } else {
@@ -1362,7 +1366,7 @@ cudaError_t launch_weno_t(const Problem& p, const double* U, bool ns, int QS, cu
   }
   *launches += 2;
   if (ns) {
-    k_visc_prim<P, T><<<(unsigned)((p.n + 255) / 256), 256, 0, st>>>(p, U);
+    k_visc_prim<P, T><<<(unsigned)((pa.n + 255) / 256), 256, 0, st>>>(pa, U);
     k_visc_lsq<P, T><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U);
     *launches += 2;
     const int64_t nfp = p.nown * QS;

@@ -27,11 +27,14 @@ class EngineError(RuntimeError):
 
 
 class Engine:
-    def __init__(self, mesh, cfg: N.UcgConfig, device: int = 0, upload: bool = True, tables: str = "host"):
+    def __init__(self, mesh, cfg: N.UcgConfig, device: int = 0, upload: bool = True, tables: str = "host",
+                 roles=None):
         """``tables``: "host" uploads the set-up library's reconstruction
         tables (ucg_upload_recon), "device" builds them on the GPU from the
         cell shapes (ucg_build_recon; the mesh may be prepared without
-        tables)."""
+        tables).  ``roles`` (int8 per cell, a partition's: 0 owned, 1 ring 1,
+        2 the rest of the halo; ucg_set_cell_roles) limits the work to what
+        the owned cells need."""
         self.lib = N.engine()
         self.mesh = mesh
         self.cfg = cfg
@@ -41,6 +44,12 @@ class Engine:
         if rc:
             raise EngineError(rc, self.lib.ucg_create_error().decode())
         self._h = h
+        if roles is not None:
+            self._roles = np.ascontiguousarray(roles, dtype=np.int8)
+            if self._roles.shape != (self.n,):
+                self.close()
+                raise ValueError("one role per cell")
+            self._check(self.lib.ucg_set_cell_roles(h, self._roles.ctypes.data_as(C.POINTER(C.c_int8))))
         if upload:
             self.upload_geometry(mesh.geometry_struct())
             if tables == "device":

@@ -43,7 +43,10 @@ class Mesh:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            N.prep().ucp_free(h)
+            try:
+                N.prep().ucp_free(h)
+            except TypeError:  # interpreter shutdown: the module is already torn down
+                pass
             self._h = None
 
     # -------------------------------------------------------- constructors

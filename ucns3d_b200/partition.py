@@ -129,6 +129,14 @@ class PartitionPlan:
         """Ranks that rank `rank` exchanges with, increasing."""
         return sorted(set(self.recv[rank]) | set(self.send[rank]))
 
+    def roles(self, rank: int) -> np.ndarray:
+        """Per local cell of rank `rank`: 0 owned, 1 ring 1, 2 the rest of the
+        halo (ucg_set_cell_roles)."""
+        r = np.full(len(self.cells[rank]), 2, dtype=np.int8)
+        r[self.core[rank]] = 1
+        r[self.owned[rank]] = 0
+        return r
+
     def local(self, rank: int, a: np.ndarray) -> np.ndarray:
         """Rows of a whole-mesh per-cell array that rank `rank` holds."""
         return np.ascontiguousarray(a[self.cells[rank]])
@@ -277,16 +285,18 @@ def transfer(lists: HaloLists, sendbuf, recvbuf, group=None):
 
 
 class HaloEngine:
-    """One rank's engine on its partition.  `comm` moves the halo rows: a
-    `torch.distributed` process group (None: the default group) for one rank
-    per process, or a `LocalCluster` that owns this engine."""
+    """One rank's engine on its partition.  `comm` is the `torch.distributed`
+    process group of the transfers (None: the default group).  `restrict`
+    (default) gives the engine the cells' roles, so that it reconstructs
+    owned + ring 1 only and steps the owned cells; without it the whole
+    local mesh is reconstructed and stepped (the same owned results)."""
 
-    def __init__(self, plan: PartitionPlan, rank: int, cfg, device: int = 0, comm=None):
+    def __init__(self, plan: PartitionPlan, rank: int, cfg, device: int = 0, comm=None, restrict: bool = True):
         import torch
         from .engine import Engine
         self.plan, self.rank, self.device = plan, rank, device
         self.mesh = PartitionMesh(plan, rank)
-        self.engine = Engine(self.mesh, cfg, device=device)
+        self.engine = Engine(self.mesh, cfg, device=device, roles=plan.roles(rank) if restrict else None)
         self.lists = HaloLists(plan, rank)
         self.peers = self.lists.peers
         self.engine.halo_set(self.lists.send, self.lists.recv)
@@ -358,9 +368,9 @@ class LocalCluster:
     unpacks and runs the stage on every rank.  Every kernel is ordered by the
     host, so none waits for another rank's."""
 
-    def __init__(self, plan: PartitionPlan, cfg, device: int = 0):
+    def __init__(self, plan: PartitionPlan, cfg, device: int = 0, restrict: bool = True):
         self.plan = plan
-        self.ranks = [HaloEngine(plan, k, cfg, device=device) for k in range(plan.nparts)]
+        self.ranks = [HaloEngine(plan, k, cfg, device=device, restrict=restrict) for k in range(plan.nparts)]
 
     def close(self):
         for h in self.ranks:
