@@ -509,6 +509,17 @@ def run_adjoint(local, steps=200, every=20, weno_n=32):
     out["ns"] = {"workload": "bump_muscl_ns Re 200", "cells": c.mesh.ncells, "dtype": "f64",
                  "residual_ms": tn["residual"], "vjp_ms": tn["vjp"], "jvp_ms": tn["jvp"],
                  "vjp_over_residual": tn["vjp"] / tn["residual"]}
+    # the CWENO4 Navier-Stokes residual's VJP/JVP on the mixed-element box
+    # (the 2.1 M-cell workload's scheme at n = 24)
+    from ucns3d_b200 import _native as N
+    cm = cases.mixed_cweno4(n=24, precision=N.UCG_FP64)
+    em = Engine(cm.mesh, cm.cfg, device=local)
+    em.set_state(cm.U0)
+    tm = em.time_adjoint(reps=5)
+    em.close()
+    out["weno_ns"] = {"workload": "mixed_cweno4 n=24", "cells": cm.mesh.ncells, "dtype": "f64",
+                      "residual_ms": tm["residual"], "vjp_ms": tm["vjp"], "jvp_ms": tm["jvp"],
+                      "vjp_over_residual": tm["vjp"] / tm["residual"]}
     # the WENO residual's VJP/JVP (FP64 form) on the vortex, weno_n^3 hexahedra
     from ucns3d_b200 import _native as N
     from ucns3d_b200.engine import EngineError

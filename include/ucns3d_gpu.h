@@ -418,11 +418,13 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
  * adds the reverse of the viscous fluxes, of the viscous least squares and
  * of the no-slip wall ghost).  ucg_residual_vjp and ucg_residual_jvp also cover
  * conserved-variable WENO and CWENO (scheme 3, EES 0 or 5, CWENO with or
- * without WENO-Z, HLLC, Euler, FP64 form): the
+ * without WENO-Z, HLLC, Euler or Navier-Stokes, FP64 form): the
  * reverse/tangent of the nonlinear weights, smoothness indicators and
  * stencil least squares, and of the MUSCL fall-back of the cells that
  * FULL = 0 or CHECKSOL send there (central polynomial, FIND_BOUNDS,
- * Venkatakrishnan, CHECKSOLX).  p denotes the free-stream state bc_state[5] (primitive:
+ * Venkatakrishnan, CHECKSOLX), and with Navier-Stokes of the viscous
+ * fluxes at every face point, the face-point gradients and the viscous
+ * least squares.  p denotes the free-stream state bc_state[5] (primitive:
  * rho, u, v, w, pressure) used by the inflow, outflow and far-field ghost
  * states.  Host arrays; [n][5] as everywhere.  Other configurations return
  * UCG_EINVAL.

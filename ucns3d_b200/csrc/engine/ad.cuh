@@ -369,5 +369,41 @@ __host__ __device__ inline void hllc_adj(double gamma, const double* cl, const d
   crb[4] += erb;
 }
 
+// Transpose of cons2prim's Jacobian at a state whose primitive form is
+// `prim`: cb = (d prim / d cons)^T pb, with rho = c0, u = c1/c0 (v, w
+// alike), p = (gamma - 1)(c4 - |c1..3|^2 / (2 c0)).
+__device__ __forceinline__ void cons2prim_rev(double gamma, const double* prim, const double* pb, double* cb) {
+  const double oo = 1.0 / prim[0], q = pb[4] * (gamma - 1.0);
+  cb[0] = pb[0] - (pb[1] * prim[1] + pb[2] * prim[2] + pb[3] * prim[3]) * oo +
+          0.5 * q * (prim[1] * prim[1] + prim[2] * prim[2] + prim[3] * prim[3]);
+  cb[1] = pb[1] * oo - q * prim[1];
+  cb[2] = pb[2] * oo - q * prim[2];
+  cb[3] = pb[3] * oo - q * prim[3];
+  cb[4] = q;
+}
+
+// The variables of the viscous least squares (T, u, v, w) of a conserved
+// state u (gradients.f90:502-706), reversed: out = (d(T, u, v, w)/du)^T sb.
+__device__ __forceinline__ void visc_vars_rev(const Problem& p, const double* u, const double* sb, double* out) {
+  double pr[NV];
+  cons2prim(p.gamma, u, pr);
+  const double T = pr[4] / (pr[0] * p.r_gas);
+  const double pb[NV] = {-sb[0] * T / pr[0], sb[1], sb[2], sb[3], sb[0] / (pr[0] * p.r_gas)};
+  cons2prim_rev(p.gamma, pr, pb, out);
+}
+
+// The tangent of variable `var` of (T, u, v, w) at the conserved state u
+// along du (the forward counterpart of visc_vars_rev).
+__device__ __forceinline__ double visc_var_tan(const Problem& p, const double* u, const double* du, int var) {
+  double pr[NV];
+  cons2prim(p.gamma, u, pr);
+  const double oo = 1.0 / pr[0];
+  if (var > 0) return (du[var] - pr[var] * du[0]) * oo;
+  const double dp = (p.gamma - 1.0) * (du[4] - (pr[1] * du[1] + pr[2] * du[2] + pr[3] * du[3]) +
+                                       0.5 * (pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]) * du[0]);
+  const double T = pr[4] / (pr[0] * p.r_gas);
+  return dp / (pr[0] * p.r_gas) - T * du[0] * oo;
+}
+
 }  // namespace ad
 }  // namespace ucg

@@ -1,6 +1,8 @@
 // Discrete adjoint (VJP) and tangent (JVP) of the engine's MUSCL residual,
 // of the wall pressure force and of SSP-RK3 steps, for the FP64 form of a
-// MUSCL (scheme 2, IORDER 1) Euler configuration.
+// MUSCL (scheme 2, IORDER 1) Euler or Navier-Stokes configuration; the
+// host side of the WENO/CWENO residual's (adjoint_weno.cu), whose viscous
+// fluxes are reversed here too (k_adj_visc over the face points).
 //
 // Residual R(U) = net outward flux (CALL_FLUX_SUBROUTINES_3D,
 // src/time_p.f90:2253-2497); force J(U) = sum over wall faces (BC code 4) of
@@ -29,6 +31,8 @@
 //                      order, so results are deterministic (no atomics).
 //   4. k_colsum5_part, k_colsum5: pbar, summed over the other boundary faces
 //                      in a fixed order.
+// Navier-Stokes adds k_adj_visc (the viscous flux reversed at each face
+// point, after step 1) and the reverse of the viscous gradients in step 2.
 // JVP: the same reconstruction and fluxes on Dual<1> numbers.
 #include <cuda_runtime.h>
 
@@ -42,7 +46,9 @@
 
 using namespace ucg;
 using namespace ucg_host;
+using ad::cons2prim_rev;
 using ad::Dual;
+using ad::visc_vars_rev;
 
 namespace {
 
@@ -234,19 +240,6 @@ __global__ void __launch_bounds__(128) k_adj_face_bnd(Problem p, int64_t nplain,
 }
 
 // Viscous face fluxes (Navier-Stokes): the adjoint of their inputs, one
-// Transpose of cons2prim's Jacobian at a state whose primitive form is
-// `prim`: cb = (d prim / d cons)^T pb, with rho = c0, u = c1/c0 (v, w
-// alike), p = (gamma - 1)(c4 - |c1..3|^2 / (2 c0)).
-__device__ __forceinline__ void cons2prim_rev(double gamma, const double* prim, const double* pb, double* cb) {
-  const double oo = 1.0 / prim[0], q = pb[4] * (gamma - 1.0);
-  cb[0] = pb[0] - (pb[1] * prim[1] + pb[2] * prim[2] + pb[3] * prim[3]) * oo +
-          0.5 * q * (prim[1] * prim[1] + prim[2] * prim[2] + prim[3] * prim[3]);
-  cb[1] = pb[1] * oo - q * prim[1];
-  cb[2] = pb[2] * oo - q * prim[2];
-  cb[3] = pb[3] * oo - q * prim[3];
-  cb[4] = q;
-}
-
 // Reverse of viscous_flux (CALCULATE_FLUXESHI_DIFFUSIVE, flux_p.f90:1520-2107,
 // with SUTHERLAND) for one face point: given fb = the adjoint of the face's
 // viscous flux, the adjoints of its inputs, the two face states cl, cr and
@@ -354,17 +347,23 @@ __device__ __forceinline__ void viscous_flux_rev(const Problem& p, const double*
   crb[3] += 0.5 * w12b / rho12;
 }
 
-// thread per owned face (one point per face): the flux leaves R_c and
-// enters R_nb, so its adjoint is fb = ws (lam_nb - lam_c), -ws lam_c on a
-// boundary face, whose ghost side takes the cell's own gradient
+// thread per owned face, over its points: the flux leaves R_c and enters
+// R_nb, so its adjoint is fb = w_q area (lam_nb - lam_c), -w_q area lam_c
+// on a boundary face, whose ghost side takes the cell's own gradient
 // (CALCULATE_BOUNDED_VISCOUS) and its ghost state from boundary_ghost; the
 // ghost's Jacobians in the face state and (second face group) in the
-// free-stream state are dual-number columns.  Adds to adjF and pown
-// (written before by the face kernels, one thread per element) and writes
-// gadj[c][f] (the adjoint of cell c's gradient through face f).
+// free-stream state are dual-number columns.  The face-point gradient is,
+// with fg == null (MUSCL), the mean of the two cells' gradients (slot 0 of
+// ulv, written by k_adj_fwd) and, with fg (WENO: the averaged face-point
+// gradients of k_visc_facegrad, [nown][QS][12]), fg at the point.  Adds to
+// adjF and pown (written before by the face kernels, one thread per
+// element) and writes gadj[c][f][q] (the adjoint of cell c's own gradient
+// at its point q of face f: half the mean's on an interior face, all of it
+// on a boundary face, where both sides are the cell's).
 __global__ void __launch_bounds__(128, 4) k_adj_visc(Problem p, int64_t nplain, const double* __restrict__ U,
-                                                  const double* __restrict__ lam, double* __restrict__ adjF,
-                                                  double* __restrict__ pown, double* __restrict__ gadj) {
+                                                     const double* __restrict__ lam, double* __restrict__ adjF,
+                                                     double* __restrict__ pown, double* __restrict__ gadj,
+                                                     const double* __restrict__ fg) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   const FaceRef F = face_ref(p, i);
@@ -375,66 +374,76 @@ __global__ void __launch_bounds__(128, 4) k_adj_visc(Problem p, int64_t nplain, 
   double r[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) r[j] = p.rot[(c * MF + f) * 4 + j];
-  const double ws = face_weight(p, p.ftype[c * MF + f], 0) * p.area[c * MF + f];
   const double* dul = (const double*)p.dul;
-  const int qq = bnd ? 0 : p.qperm[(c * MF + f) * QS];
-  double L[NV], R[NV], fb[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    L[v] = U[c * NV + v] + dul[(c * MF + f) * QS * NV + v];
-    fb[v] = bnd ? -ws * lam[c * NV + v] : ws * (lam[nb * NV + v] - lam[c * NV + v]);
-  }
-  if (!bnd) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) R[v] = U[nb * NV + v] + dul[((nb * MF + nf) * QS + qq) * NV + v];
-  } else {
-    boundary_ghost(p, code, r, L, R);
-  }
-  // each cell's viscous gradient is the same at all its face points: slot 0
-  // (written by k_adj_fwd)
-  const double* g0 = p.ulv + c * (int64_t)MF * QS * 12;
-  const double* g1 = bnd ? g0 : p.ulv + nb * (int64_t)MF * QS * 12;
-  double gm[12];
-#pragma unroll
-  for (int j = 0; j < 12; ++j) gm[j] = (g0[j] + g1[j]) / 2.0;
-  double Lb[NV], Rb[NV], gb[12];
-  viscous_flux_rev(p, r, p.dih[c * MF + f], L, R, gm, code >= 1 && code <= 4 ? 0.0 : p.lamx, fb, Lb, Rb, gb);
-  if (!bnd) {
+  const double damp = code >= 1 && code <= 4 ? 0.0 : p.lamx;
+  double pb[NV] = {0, 0, 0, 0, 0};  // adjoint of the free-stream state, summed over the points
+  for (int q = 0; q < F.nq; ++q) {
+    const double ws = face_weight(p, p.ftype[c * MF + f], q) * p.area[c * MF + f];
+    const int qq = bnd ? 0 : p.qperm[(c * MF + f) * QS + q];
+    const int64_t sl = (c * MF + f) * QS + q, sr = bnd ? sl : (nb * MF + nf) * QS + qq;
+    double L[NV], R[NV], fb[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      adjF[(c * MF + f) * QS * NV + v] += Lb[v];
-      adjF[((nb * MF + nf) * QS + qq) * NV + v] += Rb[v];
+      L[v] = U[c * NV + v] + dul[sl * NV + v];
+      fb[v] = bnd ? -ws * lam[c * NV + v] : ws * (lam[nb * NV + v] - lam[c * NV + v]);
+    }
+    if (!bnd) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) R[v] = U[nb * NV + v] + dul[sr * NV + v];
+    } else {
+      boundary_ghost(p, code, r, L, R);
+    }
+    double gm[12];
+    if (fg) {
+#pragma unroll
+      for (int j = 0; j < 12; ++j) gm[j] = fg[(i * QS + q) * 12 + j];
+    } else {  // each cell's gradient is the same at all its face points: slot 0
+      const double* g0 = p.ulv + c * (int64_t)MF * QS * 12;
+      const double* g1 = bnd ? g0 : p.ulv + nb * (int64_t)MF * QS * 12;
+#pragma unroll
+      for (int j = 0; j < 12; ++j) gm[j] = (g0[j] + g1[j]) / 2.0;
+    }
+    double Lb[NV], Rb[NV], gb[12];
+    viscous_flux_rev(p, r, p.dih[c * MF + f], L, R, gm, damp, fb, Lb, Rb, gb);
+    if (!bnd) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        adjF[sl * NV + v] += Lb[v];
+        adjF[sr * NV + v] += Rb[v];
+      }
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        gadj[sl * 12 + j] = gb[j];
+        gadj[sr * 12 + j] = gb[j];
+      }
+      continue;
     }
 #pragma unroll
-    for (int j = 0; j < 12; ++j) {
-      gadj[(c * MF + f) * 12 + j] = gb[j];
-      gadj[(nb * MF + nf) * 12 + j] = gb[j];
-    }
-    return;
-  }
-  // ghost R = G(L, bcs), one dual-number column per input (the face state,
-  // then for the second face group the free-stream state); the ghost side's
-  // gradient is the cell's own
-#pragma unroll
-  for (int j = 0; j < 12; ++j) gadj[(c * MF + f) * 12 + j] = 2.0 * gb[j];
-  const int ncol = i < nplain ? NV : 2 * NV;
+    for (int j = 0; j < 12; ++j) gadj[sl * 12 + j] = 2.0 * gb[j];
+    // ghost R = G(L, bcs), one dual-number column per input (the face state,
+    // then for the second face group the free-stream state)
+    const int ncol = i < nplain ? NV : 2 * NV;
 #pragma unroll 1
-  for (int k = 0; k < ncol; ++k) {
-    Dual<1> Ld[NV], bd[NV], Rd[NV];
+    for (int k = 0; k < ncol; ++k) {
+      Dual<1> Ld[NV], bd[NV], Rd[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      Ld[v] = Dual<1>(L[v]);
-      Ld[v].d[0] = k == v ? 1.0 : 0.0;
-      bd[v] = Dual<1>(p.bc_state[v]);
-      bd[v].d[0] = k == NV + v ? 1.0 : 0.0;
+      for (int v = 0; v < NV; ++v) {
+        Ld[v] = Dual<1>(L[v]);
+        Ld[v].d[0] = k == v ? 1.0 : 0.0;
+        bd[v] = Dual<1>(p.bc_state[v]);
+        bd[v].d[0] = k == NV + v ? 1.0 : 0.0;
+      }
+      boundary_ghost(p, code, r, Ld, bd, Rd);
+      double s = 0.0;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s += Rb[v] * Rd[v].d[0];
+      if (k < NV) adjF[sl * NV + k] += Lb[k] + s;
+      else pb[k - NV] += s;
     }
-    boundary_ghost(p, code, r, Ld, bd, Rd);
-    double s = 0.0;
-#pragma unroll
-    for (int v = 0; v < NV; ++v) s += Rb[v] * Rd[v].d[0];
-    if (k < NV) adjF[(c * MF + f) * QS * NV + k] += Lb[k] + s;
-    else pown[(i - nplain) * NV + (k - NV)] += s;
   }
+  if (bnd && i >= nplain)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) pown[(i - nplain) * NV + v] += pb[v];
 }
 
 // deterministic column sums of a [m][5] array in two passes: k_colsum5_part
@@ -461,7 +470,7 @@ __global__ void __launch_bounds__(256) k_colsum5_part(const double* __restrict__
 
 // ------------------------------------------------------------ MUSCL reverse
 // Forward quantities of the MUSCL reconstruction of cell c (k_muscl,
-// IORDER 1, Euler), kept for the reverse sweep.
+// IORDER 1), kept for the reverse sweep.
 struct MusclFwd {
   double u0[NV];
   double g[3][NV];
@@ -727,16 +736,6 @@ __global__ void __launch_bounds__(128) k_adj_fwd(Problem p, const double* __rest
 // (only the faces of fmask).  Each slot that the reverse map reads is
 // written exactly once.  Face values u_f = u0 + dd_f * slope (or u0 when
 // CHECKSOLX chose first order).
-// The variables of the viscous least squares (T, u, v, w) of a conserved
-// state u (gradients.f90:502-706), reversed: out = (d(T, u, v, w)/du)^T sb.
-__device__ __forceinline__ void visc_vars_rev(const Problem& p, const double* u, const double* sb, double* out) {
-  double pr[NV];
-  cons2prim(p.gamma, u, pr);
-  const double T = pr[4] / (pr[0] * p.r_gas);
-  const double pb[NV] = {-sb[0] * T / pr[0], sb[1], sb[2], sb[3], sb[0] / (pr[0] * p.r_gas)};
-  cons2prim_rev(p.gamma, pr, pb, out);
-}
-
 // gadj (Navier-Stokes, else null): the adjoint of each cell's gradient of
 // (T, u, v, w) through each of its faces (k_adj_visc); reversed through the
 // frame (AINVJT), the viscous least squares on stencil 1 and (T, u, v, w)(U)
@@ -1031,7 +1030,8 @@ __global__ void __launch_bounds__(128) k_jvp_muscl(Problem p, const double* __re
 // subtracts the viscous fluxes
 __global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __restrict__ U,
                                                   const double* __restrict__ dU, const double* __restrict__ tdul,
-                                                  Dp5 dp, double* __restrict__ tflux, const double* __restrict__ tgr) {
+                                                  Dp5 dp, double* __restrict__ tflux, const double* __restrict__ tgr,
+                                                  const double* __restrict__ tfg) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   using D = Dual<1>;
@@ -1089,6 +1089,17 @@ __global__ void __launch_bounds__(128) k_jvp_face(Problem p, const double* __res
       }
       const int code = nb >= 0 ? 0 : p.bc[c * MF + f];
       viscous_flux(p, r, p.dih[c * MF + f], L, R, gl, gr, fv, code >= 1 && code <= 4 ? 0.0 : p.lamx);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) tf[v] = tf[v] - fv[v].d[0] * ws;
+    } else if (tfg) {  // WENO: both sides take the averaged face-point gradient and its tangent
+      D g[12], fv[NV];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        g[j] = D(p.fgrad[(i * QS + q) * 12 + j]);
+        g[j].d[0] = tfg[(i * QS + q) * 12 + j];
+      }
+      const int code = nb >= 0 ? 0 : p.bc[c * MF + f];
+      viscous_flux(p, r, p.dih[c * MF + f], L, R, g, g, fv, code >= 1 && code <= 4 ? 0.0 : p.lamx);
 #pragma unroll
       for (int v = 0; v < NV; ++v) tf[v] = tf[v] - fv[v].d[0] * ws;
     }
@@ -1168,7 +1179,8 @@ void adjoint_release(ucg_engine* e) {
                                &e->adj_fcell,  &e->adj_traj,    &e->adj_bar,   &e->adj_tmp,      &e->adj_fwd,
                                &e->adjw_face,  &e->adjw_gbar,   &e->adjw_scr,  &e->adjw_self,    &e->adjw_contrib,
                                &e->adjw_rptr,  &e->adjw_rsrc,   &e->adjw_lam,     &e->adjw_mu,
-                               &e->adjw_pface, &e->adjw_tmp,    &e->adj_gadj,  &e->adj_tgr};
+                               &e->adjw_pface, &e->adjw_tmp,    &e->adj_gadj,  &e->adj_tgr,
+                               &e->adjw_gpt,   &e->adjw_gvb,    &e->adjw_tfg};
   for (auto* b : all) {
     if (b->p) e->bytes -= (int64_t)b->bytes;
     release(*b);
@@ -1276,7 +1288,7 @@ int vjp_device(ucg_engine* e, const Problem& p, const double* U, const double* l
                                                                       (double*)e->adj_pface.p);
   if (ns) {
     k_adj_visc<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(
-        p, nplain, U, lam, (double*)e->adj_face.p, (double*)e->adj_pface.p, (double*)e->adj_gadj.p);
+        p, nplain, U, lam, (double*)e->adj_face.p, (double*)e->adj_pface.p, (double*)e->adj_gadj.p, nullptr);
     e->launches++;
   }
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
@@ -1315,7 +1327,7 @@ int jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* d
   double* tgr = e->cfg.governing == 1 ? (double*)e->adj_tgr.p : nullptr;
   k_jvp_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p, tgr, !recon);
   k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p, dp,
-                                                              (double*)e->adj_tflux.p, tgr);
+                                                              (double*)e->adj_tflux.p, tgr, nullptr);
   k_jvp_sum<<<blocks_for(n, 256), 256, 0, e->stream>>>(p, (const double*)e->adj_tflux.p, dR);
   e->launches += 3;
   CK(cudaGetLastError());
@@ -1356,14 +1368,14 @@ int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g
 }
 
 // ---------------------------------------------------------------- WENO
-// The VJP of the WENO residual: conserved-variable WENO (EES 0), Euler, FP64
-// form, cells off the MUSCL fall-back.
+// The VJP of the WENO residual: conserved-variable WENO and CWENO, Euler or
+// Navier-Stokes, FP64 form (the reverse map of its per-slot contributions).
 int adjw_setup(ucg_engine* e) {
   const ucg_config& c = e->cfg;
-  if (!(c.scheme == 3 && (c.ees == 0 || c.ees == 5) && c.wenwrt == 1 && c.governing == 2 &&
+  if (!(c.scheme == 3 && (c.ees == 0 || c.ees == 5) && c.wenwrt == 1 && (c.governing == 2 || c.governing == 1) &&
         c.precision == UCG_FP64 && c.riemann == 1 && !c.mood))
     return fail(e, UCG_EINVAL,
-                "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, CWENO with or without WENO-Z), HLLC, Euler, FP64 form, without MOOD");
+                "the WENO adjoint covers conserved-variable WENO and CWENO (EES 0 or 5, CWENO with or without WENO-Z), HLLC, Euler or Navier-Stokes, FP64 form, without MOOD");
   if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
   if (!e->roles.empty()) return fail(e, UCG_EINVAL, "the adjoint covers whole meshes (no partition roles)");
   if (e->adjw_ready) return UCG_OK;
@@ -1420,6 +1432,11 @@ int adjw_setup(ucg_engine* e) {
   rc = rc ? rc : get(e->adjw_mu, (size_t)n * NV * 8 + 64 * 8);
   rc = rc ? rc : get(e->adjw_pface, (size_t)std::max<int64_t>(1, e->nown - e->nown_plain) * NV * 8);
   rc = rc ? rc : get(e->adjw_tmp, (size_t)(std::max<int64_t>(1, e->nown - e->nown_plain) / 1024 + 2) * NV * 8);
+  if (c.governing == 1) {  // viscous terms: point-gradient adjoints, coefficient adjoints or tangents
+    rc = rc ? rc : get(e->adjw_gpt, (size_t)n * MF * e->QS * 12 * 8);
+    rc = rc ? rc : get(e->adjw_gvb, (size_t)n * ID * 4 * 8);
+    rc = rc ? rc : get(e->adjw_tfg, (size_t)std::max<int64_t>(1, e->nown) * e->QS * 12 * 8);
+  }
   if (rc) return rc;
   CK(cudaMemcpyAsync(e->adjw_rptr.p, cnt.data(), (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
   if (cnt[n]) CK(cudaMemcpyAsync(e->adjw_rsrc.p, src.data(), cnt[n] * 8, cudaMemcpyHostToDevice, e->stream));
@@ -1440,8 +1457,17 @@ int weno_vjp_device(ucg_engine* e, const Problem& p, const double* U, const doub
     k_adj_face_bnd<<<blocks_for(nbnd * 10, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF,
                                                                       (double*)e->adjw_pface.p);
   e->launches += (nplain > 0) + (nbnd > 0);
+  const bool ns = e->cfg.governing == 1;
+  if (ns) {  // the viscous fluxes at every face point, from the stored face-point gradients
+    k_adj_visc<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, nplain, U, lam, adjF, (double*)e->adjw_pface.p,
+                                                               (double*)e->adjw_gpt.p, p.fgrad);
+    e->launches++;
+  }
   if ((rc = launch_weno_adjoint(e, p, U, adjF, (double*)e->adjw_gbar.p, (double*)e->adjw_scr.p,
                                 (double*)e->adjw_self.p, (double*)e->adjw_contrib.p)))
+    return rc;
+  if (ns && (rc = launch_weno_visc_adjoint(e, p, U, (const double*)e->adjw_gpt.p, (double*)e->adjw_gvb.p,
+                                           (double*)e->adjw_contrib.p)))
     return rc;
   k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adjw_rptr.p,
                                                           (const int64_t*)e->adjw_rsrc.p,
@@ -1471,7 +1497,12 @@ int weno_jvp_device(ucg_engine* e, const Problem& p, const double* U, const doub
   double* tdul = (double*)e->adjw_face.p;
   double* tflux = (double*)e->adjw_contrib.p;
   if ((rc = launch_weno_tangent(e, p, U, dU, (const double*)e->adjw_gbar.p, tdul))) return rc;
-  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux, nullptr);
+  double* tfg = nullptr;
+  if (e->cfg.governing == 1) {
+    tfg = (double*)e->adjw_tfg.p;
+    if ((rc = launch_weno_visc_tangent(e, p, U, dU, (double*)e->adjw_gvb.p, tfg))) return rc;
+  }
+  k_jvp_face<<<blocks_for(e->nown, 128), 128, 0, e->stream>>>(p, U, dU, tdul, dp, tflux, nullptr, tfg);
   k_jvp_sum<<<blocks_for(e->n, 256), 256, 0, e->stream>>>(p, tflux, dR);
   e->launches += 2;
   CK(cudaGetLastError());

@@ -783,6 +783,140 @@ __global__ void __launch_bounds__(WP_THREADS, UCG_AWP_MINB) k_jvp_wpost(Problem 
   }
 }
 
+// ------------------------------------------------------------ viscous terms
+// Navier-Stokes: the forward pass forms, per cell, the coefficients of the
+// viscous least squares on (T, u, v, w) over the central stencil,
+//   gv[c][d][a] = sum_k M_0[k][d] (S_a(U_st(k)) - S_a(U_c))   (k_visc_lsq),
+// per face point the gradient of each side, J_c^T sum_d gv[c][d][a] dm_d(xi)
+// (SOLUTIONTRIAV2, k_visc_facegrad), and the viscous flux from their mean.
+// gpt[c][f][q][12] holds the adjoint of cell c's own gradient at its point
+// q of face f (k_adj_visc); these kernels take it back to U.
+
+// thread per (cell, variable a): gvb[c][d][a] = sum over the cell's face
+// points of (J_c gpt_a) . dm_d(xi)
+template <int P>
+__global__ void __launch_bounds__(128) k_adj_visc_coef(Problem p, const double* __restrict__ gpt,
+                                                       double* __restrict__ gvb) {
+  constexpr int ID = Deg<P>::ideg;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = t >> 2;
+  const int a = (int)(t & 3);
+  if (c >= p.n) return;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const double* J = p.jinv + c * 9;
+  double acc[ID];
+#pragma unroll
+  for (int d = 0; d < ID; ++d) acc[d] = 0.0;
+  const int nf = p.nfaces[c];
+  for (int f = 0; f < nf; ++f) {
+    const int nq = face_nq(p, p.ftype[c * MF + f]);
+    for (int q = 0; q < nq; ++q) {
+      const double* g = gpt + (((c * MF + f) * QS + q) * 12 + a * 3);
+      // the gradient's component k is sum_j J[j][k] (d/dxi_j of the polynomial)
+      const double t0 = J[0] * g[0] + J[1] * g[1] + J[2] * g[2];
+      const double t1 = J[3] * g[0] + J[4] * g[1] + J[5] * g[2];
+      const double t2 = J[6] * g[0] + J[7] * g[1] + J[8] * g[2];
+      const double* xi = (const double*)p.qpts + ((c >> 5) * MF * QS * 3 + (f * QS + q) * 3) * 32 + (c & 31);
+      double dx[ID], dy[ID], dz[ID];
+      dmonomials<P, double>(xi[0], xi[32], xi[64], dx, dy, dz);
+#pragma unroll
+      for (int d = 0; d < ID; ++d) acc[d] += t0 * dx[d] + t1 * dy[d] + t2 * dz[d];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < ID; ++d) gvb[(c * ID + d) * 4 + a] = acc[d];
+}
+
+// thread per cell: the transpose of the viscous least squares into the
+// slots of k_adj_lsq (slot 0 the cell, 1 + k member k of the central
+// stencil), added to what k_adj_lsq wrote there: one writer per slot
+template <int P>
+__global__ void __launch_bounds__(128) k_adj_visc_lsq(Problem p, const double* __restrict__ U,
+                                                      const double* __restrict__ gvb, double* __restrict__ contrib) {
+  constexpr int ID = Deg<P>::ideg;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = p.n;
+  if (c >= n) return;
+  const int IM = p.imax, W = IM + 1;
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  const double* gb = gvb + c * ID * 4;
+  double sc[4] = {0, 0, 0, 0};
+  for (int k = 0; k < IM; ++k) {
+    double a[4] = {0, 0, 0, 0};
+#pragma unroll 4
+    for (int d = 0; d < ID; ++d) {
+      const double m = M[(k * ID + d) * 32];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) a[j] += m * gb[d * 4 + j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sc[j] -= a[j];
+    double out[NV];
+    ad::visc_vars_rev(p, U + (int64_t)st[(k + 1) * 32] * NV, a, out);
+    double* o = contrib + ((1 + k) * n + c) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o[v] += out[v];
+  }
+  double out[NV];
+  ad::visc_vars_rev(p, U + c * NV, sc, out);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) contrib[c * NV + v] += out[v];
+}
+
+// thread per (cell, variable a): the tangent of the coefficients,
+// dgv[c][d][a] = sum_k M_0[k][d] (dS_a(st(k)) - dS_a(c)), in k_visc_lsq's
+// layout [n][ID][4]
+template <int P>
+__global__ void __launch_bounds__(128) k_jvp_visc_coef(Problem p, const double* __restrict__ U,
+                                                       const double* __restrict__ dU, double* __restrict__ dgv) {
+  constexpr int ID = Deg<P>::ideg;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = t >> 2;
+  const int a = (int)(t & 3);
+  if (c >= p.n) return;
+  const int IM = p.imax, W = IM + 1;
+  const int64_t grp = c >> 5;
+  const int lane = (int)(c & 31);
+  const int32_t* st = p.sten + grp * (int64_t)p.admis_max * W * 32 + lane;
+  const double* M = (const double*)p.invmat + (grp * p.tstride + p.soff[0]) * 32 + lane;
+  const double sc = ad::visc_var_tan(p, U + c * NV, dU + c * NV, a);
+  double acc[ID];
+#pragma unroll
+  for (int d = 0; d < ID; ++d) acc[d] = 0.0;
+  for (int k = 0; k < IM; ++k) {
+    const int64_t y = st[(k + 1) * 32];
+    const double ds = ad::visc_var_tan(p, U + y * NV, dU + y * NV, a) - sc;
+#pragma unroll
+    for (int d = 0; d < ID; ++d) acc[d] += M[(k * ID + d) * 32] * ds;
+  }
+#pragma unroll
+  for (int d = 0; d < ID; ++d) dgv[(c * ID + d) * 4 + a] = acc[d];
+}
+
+template <int P>
+void launch_visc_t(const Problem& p, const double* U, const double* gpt, double* gvb, double* contrib,
+                   cudaStream_t st) {
+  k_adj_visc_coef<P><<<(unsigned)((p.n * 4 + 127) / 128), 128, 0, st>>>(p, gpt, gvb);
+  k_adj_visc_lsq<P><<<(unsigned)((p.n + 127) / 128), 128, 0, st>>>(p, U, gvb, contrib);
+}
+
+// the tangent of the face-point gradients: the coefficients' tangent, then
+// k_visc_facegrad itself (linear in the coefficients) on it
+template <int P>
+void launch_visc_jvp_t(const Problem& p, const double* U, const double* dU, double* dgv, double* tfg,
+                       cudaStream_t st) {
+  k_jvp_visc_coef<P><<<(unsigned)((p.n * 4 + 127) / 128), 128, 0, st>>>(p, U, dU, dgv);
+  Problem pt = p;
+  pt.gv = dgv;
+  pt.fgrad = tfg;
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+  const int64_t nfp = p.nown * QS;
+  k_visc_facegrad<P, double><<<(unsigned)((nfp + 127) / 128), 128, 0, st>>>(pt);
+}
+
 template <int P>
 void launch_t(const Problem& p, const double* U, const double* adjF, double* gbar, double* scr, double* selfc,
               double* contrib, cudaStream_t st) {
@@ -814,6 +948,34 @@ int launch_weno_tangent(ucg_engine* e, const Problem& p, const double* U, const 
   return UCG_OK;
 }
 
+
+int launch_weno_visc_adjoint(ucg_engine* e, const Problem& p, const double* U, const double* gpt, double* gvb,
+                             double* contrib) {
+  switch (e->cfg.iorder) {
+    case 1: launch_visc_t<1>(p, U, gpt, gvb, contrib, e->stream); break;
+    case 2: launch_visc_t<2>(p, U, gpt, gvb, contrib, e->stream); break;
+    case 3: launch_visc_t<3>(p, U, gpt, gvb, contrib, e->stream); break;
+    case 4: launch_visc_t<4>(p, U, gpt, gvb, contrib, e->stream); break;
+    default: return fail(e, UCG_EINVAL, "iorder out of range");
+  }
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
+
+int launch_weno_visc_tangent(ucg_engine* e, const Problem& p, const double* U, const double* dU, double* dgv,
+                             double* tfg) {
+  switch (e->cfg.iorder) {
+    case 1: launch_visc_jvp_t<1>(p, U, dU, dgv, tfg, e->stream); break;
+    case 2: launch_visc_jvp_t<2>(p, U, dU, dgv, tfg, e->stream); break;
+    case 3: launch_visc_jvp_t<3>(p, U, dU, dgv, tfg, e->stream); break;
+    case 4: launch_visc_jvp_t<4>(p, U, dU, dgv, tfg, e->stream); break;
+    default: return fail(e, UCG_EINVAL, "iorder out of range");
+  }
+  e->launches += 2;
+  CK(cudaGetLastError());
+  return UCG_OK;
+}
 
 int launch_weno_adjoint(ucg_engine* e, const Problem& p, const double* U, const double* adjF, double* gbar,
                         double* scr, double* selfc, double* contrib) {

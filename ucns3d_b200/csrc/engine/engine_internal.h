@@ -92,7 +92,7 @@ struct ucg_engine {
   // discrete adjoint of the WENO reconstruction (adjoint_weno.cu)
   bool adjw_ready = false;
   DevBuf adjw_face, adjw_gbar, adjw_scr, adjw_self, adjw_contrib, adjw_rptr, adjw_rsrc, adjw_lam, adjw_mu,
-      adjw_pface, adjw_tmp;
+      adjw_pface, adjw_tmp, adjw_gpt, adjw_gvb, adjw_tfg;
 };
 
 namespace ucg_host {
@@ -136,5 +136,12 @@ int launch_weno_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, c
 // tangent of the WENO face values from the tangent stencil polynomials dG
 int launch_weno_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dU, const double* dG,
                         double* tdul);
+// Navier-Stokes WENO: the face-point gradient adjoints gpt back through the
+// viscous coefficients and least squares into the slots of contrib; the
+// tangent of the face-point gradients (tfg, k_visc_facegrad's layout)
+int launch_weno_visc_adjoint(ucg_engine* e, const ucg::Problem& p, const double* U, const double* gpt, double* gvb,
+                             double* contrib);
+int launch_weno_visc_tangent(ucg_engine* e, const ucg::Problem& p, const double* U, const double* dU, double* dgv,
+                             double* tfg);
 
 }  // namespace ucg_host
