@@ -615,8 +615,14 @@ __global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __re
 // or not FULL) takes the MUSCL fall-back only if the last MOOD pass
 // recomputed it (RECALC, reconstruct_p.f90:2306-2315), else it keeps its
 // WENO values and only CHECKSOLX; the reduced flags go to p.wflag.
+// Three blocks of 128 per SM where that measured faster than the two that
+// the kernel's registers otherwise allow: IORDER 2 (WENO3 tets, 82,944
+// cells: 1.109 -> 1.083 ms per step mixed, 1.585 -> 1.540 FP64) and IORDER 3
+// in FP32 (2.1 M-cell CWENO4 Navier-Stokes: 52.7 -> 51.2 ms; in FP64 the
+// bound made the 647 k-cell step 31.8 -> 33.8 ms, so FP64 keeps two).
 template <int P, typename T, bool CH = false, bool ISB = false, bool FB = false, bool MU = false>
-__global__ void __launch_bounds__(CH ? 64 : 128) k_wpost(Problem p, const double* __restrict__ U) {
+__global__ void __launch_bounds__(CH ? 64 : 128, !CH && (P == 2 || (P == 3 && sizeof(T) == 4)) ? 3 : 1)
+    k_wpost(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int VEC = Vec<T>::N;
   constexpr int L2 = ID < 9 ? ID : 9;  // CWENO lower order: IDEGFREE2 3 or 9 (grid_p.f90:6145-6160)
@@ -1236,19 +1242,45 @@ __device__ __forceinline__ void visc_point_grad(const Problem& p, int64_t c, int
   dmonomials<P, T>(xi[0], xi[32], xi[64], dx, dy, dz);
   const double* J = p.jinv + c * 9;
   const T* gv = (const T*)p.gv + c * ID * 4;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: a coefficient row's four variables in one 16-byte load (the
+    // scalar loads kept k_visc_facegrad at 80 % of L1 throughput; 2.1 M-cell
+    // CWENO4: 52.7 -> 51.8 ms per step); each variable's sum still runs over
+    // the rows in order, so the values are the same bit for bit
+    T gl[4][3];
 #pragma unroll
-  for (int var = 0; var < 4; ++var) {
-    T gl[3] = {T(0), T(0), T(0)};
+    for (int var = 0; var < 4; ++var) gl[var][0] = gl[var][1] = gl[var][2] = T(0);
 #pragma unroll
     for (int d = 0; d < ID; ++d) {
-      const T g = gv[d * 4 + var];
-      gl[0] += g * dx[d];
-      gl[1] += g * dy[d];
-      gl[2] += g * dz[d];
+      const float4 a = *(const float4*)(gv + d * 4);
+      const T g[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int var = 0; var < 4; ++var) {
+        gl[var][0] += g[var] * dx[d];
+        gl[var][1] += g[var] * dy[d];
+        gl[var][2] += g[var] * dz[d];
+      }
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
-      out[var * 3 + k] = T(J[0 * 3 + k]) * gl[0] + T(J[1 * 3 + k]) * gl[1] + T(J[2 * 3 + k]) * gl[2];
+    for (int var = 0; var < 4; ++var)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        out[var * 3 + k] = T(J[0 * 3 + k]) * gl[var][0] + T(J[1 * 3 + k]) * gl[var][1] + T(J[2 * 3 + k]) * gl[var][2];
+  } else {
+#pragma unroll
+    for (int var = 0; var < 4; ++var) {
+      T gl[3] = {T(0), T(0), T(0)};
+#pragma unroll
+      for (int d = 0; d < ID; ++d) {
+        const T g = gv[d * 4 + var];
+        gl[0] += g * dx[d];
+        gl[1] += g * dy[d];
+        gl[2] += g * dz[d];
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        out[var * 3 + k] = T(J[0 * 3 + k]) * gl[0] + T(J[1 * 3 + k]) * gl[1] + T(J[2 * 3 + k]) * gl[2];
+    }
   }
 }
 
