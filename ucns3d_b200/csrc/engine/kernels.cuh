@@ -152,8 +152,12 @@ __global__ void __launch_bounds__(128) k_muscl(Problem p, const double* __restri
 #ifndef UCG_FACE_BLOCK
 #define UCG_FACE_BLOCK 64
 #endif
+// Navier-Stokes: six blocks per SM (168 registers instead of 202): 64^3
+// MUSCL TGV step 1.278 -> 1.224 ms mixed, 1.334 -> 1.290 ms FP64, 2.1 M-cell
+// CWENO4 57.3 -> 56.2 ms; eight (128 registers) gained less.  Euler keeps
+// the compiler's choice (eight blocks changed the 64^3 WENO5 step by 0.5 %).
 template <typename T, bool NS, int RK>
-__global__ void __launch_bounds__(UCG_FACE_BLOCK) k_face(Problem p, const double* __restrict__ Uc) {
+__global__ void __launch_bounds__(UCG_FACE_BLOCK, NS ? 6 : 1) k_face(Problem p, const double* __restrict__ Uc) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nown) return;
   const int32_t code = p.own[i];
