@@ -37,12 +37,13 @@ __global__ void k_pad_state(Problem p, const double* __restrict__ U) {
 
 // PAD: stencil members gathered from p.upad (the engine's stage), else from U
 // (also used on tangent states by the discrete adjoint).
-// IORDER 3 in FP32: four blocks per SM (128 registers instead of 160): the
-// gather of the directional stencils' members is latency-bound, and more
-// warps in flight made the 2.1 M-cell CWENO4 step 6 % faster (61.1 -> 57.3
-// ms on one box); the same values bit for bit
+// FP32 at IORDER 3: four blocks per SM (128 registers instead of 160), at
+// IORDER 2 five (instead of four at 126): the gather of the stencil members
+// is latency-bound, and more warps in flight made the 2.1 M-cell CWENO4
+// step 6 % faster (61.1 -> 57.3 ms on one box) and the 82,944-tet WENO3
+// step 3 % (1.094 -> 1.063 ms); the same values bit for bit
 template <int P, typename T, bool PAD = false>
-__global__ void __launch_bounds__(128, (P == 3 && sizeof(T) == 4) ? 4 : 1)
+__global__ void __launch_bounds__(128, sizeof(T) != 4 ? 1 : P == 3 ? 4 : P == 2 ? 5 : 1)
     k_lsq(Problem p, const double* __restrict__ U) {
   constexpr int ID = Deg<P>::ideg;
   constexpr int DH = LsqRows<P, T>::value;
