@@ -41,7 +41,8 @@ __global__ void k_pad_state(Problem p, const double* __restrict__ U) {
 // IORDER 2 five (instead of four at 126): the gather of the stencil members
 // is latency-bound, and more warps in flight made the 2.1 M-cell CWENO4
 // step 6 % faster (61.1 -> 57.3 ms on one box) and the 82,944-tet WENO3
-// step 3 % (1.094 -> 1.063 ms); the same values bit for bit
+// step 3 % (1.094 -> 1.063 ms); the same values bit for bit.  Five blocks
+// at IORDER 3 (102 registers) made the CWENO4 step slower (56.0 -> 58.0 ms).
 template <int P, typename T, bool PAD = false>
 __global__ void __launch_bounds__(128, sizeof(T) != 4 ? 1 : P == 3 ? 4 : P == 2 ? 5 : 1)
     k_lsq(Problem p, const double* __restrict__ U) {
@@ -625,7 +626,8 @@ __global__ void __launch_bounds__(32 * NV) k_wface(Problem p, const double* __re
 // the kernel's registers otherwise allow: IORDER 2 (WENO3 tets, 82,944
 // cells: 1.109 -> 1.083 ms per step mixed, 1.585 -> 1.540 FP64) and IORDER 3
 // in FP32 (2.1 M-cell CWENO4 Navier-Stokes: 52.7 -> 51.2 ms; in FP64 the
-// bound made the 647 k-cell step 31.8 -> 33.8 ms, so FP64 keeps two).
+// bound made the 647 k-cell step 31.8 -> 33.8 ms, so FP64 keeps two; four
+// blocks in FP32 made it 56.0 -> 57.6 ms on another box).
 template <int P, typename T, bool CH = false, bool ISB = false, bool FB = false, bool MU = false>
 __global__ void __launch_bounds__(CH ? 64 : 128, !CH && (P == 2 || (P == 3 && sizeof(T) == 4)) ? 3 : 1)
     k_wpost(Problem p, const double* __restrict__ U) {
