@@ -150,3 +150,11 @@ def test_two_gloo_ranks_step_like_whole_mesh(name, tmp_path):
     assert np.array_equal(got, U)
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"dt{r}.npy"), np.array(dts))
+
+
+def test_plan_refuses_an_empty_part():
+    m, cfg, U = _case("muscl_bump")
+    part = rcb(m.centres(), 2)
+    part[part == 1] = 2  # parts 0 and 2: part 1 owns nothing
+    with pytest.raises(ValueError):
+        PartitionPlan(m, part)

@@ -97,6 +97,8 @@ class PartitionPlan:
             raise ValueError("part must give a non-negative part index per cell")
         self.base, self.part = mesh, part
         self.nparts = int(part.max()) + 1
+        if np.bincount(part, minlength=self.nparts).min() == 0:
+            raise ValueError("every part from 0 to max(part) must own at least one cell")
         g, r = mesh.geometry(), mesh.recon()
         neigh, nfaces, sten = g["neigh"], g["nfaces"], r["stencil"]
         self.cells, self.owned, self.core = [], [], []
