@@ -301,6 +301,11 @@ class HaloEngine:
         self.engine = Engine(self.mesh, cfg, device=device, roles=plan.roles(rank) if restrict else None)
         self.lists = HaloLists(plan, rank)
         self.peers = self.lists.peers
+        if plan.nparts > 1 and not self.peers:
+            # the grouped point-to-point call of every stage (NCCL) must
+            # include every rank, so a rank without halo rows would hang it
+            self.engine.close()
+            raise ValueError(f"rank {rank} shares no halo with another part (a disconnected piece of the mesh)")
         self.engine.halo_set(self.lists.send, self.lists.recv)
         dev = torch.device("cuda", device)
         self.sendbuf = torch.empty((len(self.lists.send), 5), dtype=torch.float64, device=dev)
