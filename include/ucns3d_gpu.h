@@ -361,7 +361,9 @@ int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
  *   The reconstruction then covers roles 0-1, the face fluxes the faces of
  *   owned cells, the residual and the update the owned cells; rows of roles
  *   1-2 of ucg_residual and of the stepped state are unspecified until the
- *   next unpack.  Without roles every cell is reconstructed and stepped.
+ *   next unpack, and the domain sums of ucg_reduce run over every local cell
+ *   (sum the owned rows on the host instead).  Without roles every cell is
+ *   reconstructed and stepped.
  *   The adjoint, implicit steps and MOOD refuse an engine with roles.
  * No counterpart entry points in the reference (its exchange is MPI inside
  * the time loop, src/time_p.f90:885-1027).                                 */
