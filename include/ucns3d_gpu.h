@@ -346,9 +346,9 @@ int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
  * ucg_rk3_stage: RK3 stage `stage` (1, 2, 3) of step size dt, the same
  *   launches as the corresponding third of ucg_rk3_step (which equals the
  *   three stages in order).  UCG_EINVAL with MOOD.
- * ucg_halo_set: the rows this rank sends (owned cells, repeated per peer,
- *   in the order the peers expect) and receives (halo cells, each once), as
- *   the caller's cell indices.
+ * ucg_halo_set (after ucg_upload_geometry): the rows this rank sends (owned
+ *   cells, repeated per peer, in the order the peers expect) and receives
+ *   (halo cells, each once), as the caller's cell indices.
  * ucg_halo_pack / ucg_halo_unpack: gather the send rows of the input state
  *   of `stage` (1: U^n, 2: U^(1), 3: U^(2)) into a DEVICE buffer
  *   [nsend][5], or scatter a DEVICE buffer [nrecv][5] into the receive rows,

@@ -62,6 +62,13 @@ def test_halo_pack_and_unpack_rows():
 
 def test_halo_and_stage_arguments_are_checked():
     m, cfg, U = _case("muscl_bump")
+    e = Engine(m, cfg, upload=False)  # the lists map through the cell order fixed at the geometry upload
+    try:
+        with pytest.raises(EngineError) as ei:
+            e.halo_set(np.array([0]), np.array([1]))
+        assert ei.value.code == N.UCG_ESTATE
+    finally:
+        e.close()
     e = Engine(m, cfg)
     try:
         e.set_state(U)

@@ -101,6 +101,8 @@ int ucg_rk3_stage(ucg_engine* e, int32_t stage, double dt) {
 int ucg_halo_set(ucg_engine* e, const int32_t* send_cells, int64_t nsend, const int32_t* recv_cells, int64_t nrecv) {
   if (!e || nsend < 0 || nrecv < 0 || (nsend && !send_cells) || (nrecv && !recv_cells))
     return fail(e, UCG_EINVAL, "bad argument");
+  if (!e->have_geometry)  // the engine's cell order, which the lists are mapped to, is fixed there
+    return fail(e, UCG_ESTATE, "set the halo lists after ucg_upload_geometry");
   std::vector<int32_t> s, r;
   int rc = map_cells(e, send_cells, nsend, s, "send");
   rc = rc ? rc : map_cells(e, recv_cells, nrecv, r, "receive");
