@@ -656,7 +656,7 @@ namespace ucg {
 
 // ------------------------------------------------ async bulk copy helpers
 // 1-D bulk copies global -> shared completed on an mbarrier (sm_90+ PTX),
-// without cluster multicast.  Waits are bounded: a wait that gives up
+// each CTA copying for itself alone.  Waits are bounded: a wait that gives up
 // returns false and the caller records UCG_ETIMEOUT in the health word.
 enum : unsigned { HEALTH_TIMEOUT = 2u };
 
