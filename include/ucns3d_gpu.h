@@ -332,6 +332,20 @@ int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t max_inner, 
  * the handle's stream.  UCG_EINVAL without MOOD. */
 int ucg_mood_state(ucg_engine* e, int32_t* order, int32_t* recalc);
 
+/* Explicit dual time: one physical step dt of BDF2 (DUAL_TIME_EX,
+ * src/time_p.f90:3244-3436, RUNGEKUTTA = 12) by explicit pseudo-time
+ * iterations (RELAXATION_EX, :3844-3888): local steps DTL at `cfl`
+ * (CALCULATE_CFLL, with CFL/3 as everywhere) from the state at the start of
+ * the step, then per iteration du = -(V/dt (1.5 U - 2 U^n + 0.5 U^{n-1}) +
+ * RHS(U)) dtau with dtau = (DTL/V) / (1 + 1.5 DTL/dt), U += du, until the
+ * volume-weighted norm of du relative to its largest value in the step is
+ * at most inner_tol (RESLIMIT) or max_inner (UPPERLIMIT) iterations are
+ * done (*inner_iters, may be NULL).  Afterwards U^{n-1} <- U^n <- U and the
+ * state becomes 2 U^n - U^{n-1}, the next step's first iterate.  The history
+ * is shared with ucg_dual_time_step and restarts at ucg_set_state. */
+int ucg_dual_time_step_explicit(ucg_engine* e, double dt, double cfl, int32_t max_inner, double inner_tol,
+                                int32_t* inner_iters);
+
 /* ---------------------------------------------------------------- partitions
  * One engine per rank of a partitioned mesh.  The rank's mesh is its owned
  * cells plus a halo: their face neighbours, every stencil member of both,

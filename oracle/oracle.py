@@ -45,6 +45,9 @@ def lib():
         L.orc_dual_time_step.restype = C.c_int
         L.orc_dual_time_step.argtypes = [cfgp, geop, recp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                          f64p, f64p, f64p, C.POINTER(C.c_int)]
+        L.orc_dual_time_step_explicit.restype = C.c_int
+        L.orc_dual_time_step_explicit.argtypes = [cfgp, geop, recp, C.c_double, C.c_double, C.c_int, C.c_double,
+                                                  f64p, f64p, f64p, C.POINTER(C.c_int)]
         L.orc_rk3_step_mood.restype = C.c_int
         L.orc_rk3_step_mood.argtypes = [cfgp, geop, recp, C.c_double, f64p, C.POINTER(C.c_int8),
                                         C.POINTER(C.c_int32)]
@@ -157,6 +160,20 @@ class Oracle:
                                       nsweeps, _p(U), _p(U2), _p(U3), C.byref(it))
         if rc:
             raise RuntimeError(f"orc_dual_time_step failed: {rc}")
+        return U, (U2, U3), it.value
+
+    def dual_time_step_explicit(self, U: np.ndarray, hist: tuple, dt: float, cfl: float, maxit: int = 50,
+                                tol: float = 1e-3) -> tuple:
+        """One DUAL_TIME_EX physical step (explicit pseudo-time iterations):
+        (U, (U^n, U^{n-1}), inner iterations); hist is None before the first
+        step.  The returned U is the next step's first iterate 2 U^n - U^{n-1}."""
+        U = np.array(U, dtype=np.float64, copy=True, order="C")
+        U2, U3 = (U.copy(), U.copy()) if hist is None else (np.array(hist[0], copy=True), np.array(hist[1], copy=True))
+        it = C.c_int()
+        rc = lib().orc_dual_time_step_explicit(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), dt, cfl,
+                                               maxit, tol, _p(U), _p(U2), _p(U3), C.byref(it))
+        if rc:
+            raise RuntimeError(f"orc_dual_time_step_explicit failed: {rc}")
         return U, (U2, U3), it.value
 
     def rk3_step_mood(self, U: np.ndarray, dt: float, recalc: np.ndarray) -> tuple:

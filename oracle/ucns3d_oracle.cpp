@@ -1328,35 +1328,49 @@ int orc_rk3_stage(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon*
 }  // extern "C"
 
 namespace {
-// One implicit correction du of U: RHS, DTL, the Jacobian and `nsweeps`
-// sweeps from du = 0.  Dual time (dt > 0): the diagonal V (1/DTL + 1.5/dt)
-// + ..., and with U2 (U^n) and U3 (U^{n-1}) given (ISCOUN 2) the right-hand
-// side -(RHS + V (1.5 U - 2 U^n + 0.5 U^{n-1}) / dt).
-void implicit_du(const Ctx& x, const double* U, double ccfl, int nsweeps, double dt, const double* U2,
-                 const double* U3, std::vector<double>& du) {
+// CALCULATE_CFLL (time_p.f90:193-333): the local time step of every cell
+void local_dt(const Ctx& x, const double* U, double ccfl, std::vector<double>& dtl) {
   const ucg_config* cfg = x.cfg;
   const ucg_geometry* g = x.g;
   const int64_t n = x.n;
   const bool ns = cfg->governing == 1;
   const double gm = cfg->gamma;
-  std::vector<double> rhs(n * NV), UL, ULV, dtl(n), dinv(n), off((size_t)n * F * 25), dn(n * NV);
+  dtl.assign(n, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) {
+    double p[NV];
+    cons2prim(x, &U[c * NV], p);
+    const double agrt = std::sqrt(p[4] * gm / p[0]);
+    const double veln = std::max(std::max(std::fabs(p[1]), std::fabs(p[2])), std::fabs(p[3])) + agrt;
+    const double me = g->minedge[c];
+    if (ns) {
+      double mu, lam;
+      sutherland(cfg, p[0], p[4], &mu, &lam);
+      dtl[c] = ccfl * (1.0 / ((std::fabs(veln) / me) + (0.5 * (lam + mu) / (me * me))));
+    } else {
+      dtl[c] = ccfl * (me / std::fabs(veln));
+    }
+  }
+}
+
+// One implicit correction du of U: RHS, the Jacobian and `nsweeps` sweeps
+// from du = 0, with the local time steps dtl.  Dual time (dt > 0): the
+// diagonal V (1/DTL + 1.5/dt) + ..., and with U2 (U^n) and U3 (U^{n-1})
+// given (ISCOUN 2) the right-hand side -(RHS + V (1.5 U - 2 U^n + 0.5
+// U^{n-1}) / dt).
+void implicit_du(const Ctx& x, const double* U, const std::vector<double>& dtl, int nsweeps, double dt,
+                 const double* U2, const double* U3, std::vector<double>& du) {
+  const ucg_config* cfg = x.cfg;
+  const ucg_geometry* g = x.g;
+  const int64_t n = x.n;
+  const bool ns = cfg->governing == 1;
+  const double gm = cfg->gamma;
+  std::vector<double> rhs(n * NV), UL, ULV, dinv(n), off((size_t)n * F * 25), dn(n * NV);
   du.assign(n * NV, 0.0);
   {
     residual(x, U, rhs.data(), UL, ULV);
 #pragma omp parallel for schedule(static)
     for (int64_t c = 0; c < n; ++c) {
-      double p[NV];
-      cons2prim(x, &U[c * NV], p);
-      const double agrt = std::sqrt(p[4] * gm / p[0]);
-      const double veln = std::max(std::max(std::fabs(p[1]), std::fabs(p[2])), std::fabs(p[3])) + agrt;
-      const double me = g->minedge[c];
-      if (ns) {
-        double mu, lam;
-        sutherland(cfg, p[0], p[4], &mu, &lam);
-        dtl[c] = ccfl * (1.0 / ((std::fabs(veln) / me) + (0.5 * (lam + mu) / (me * me))));
-      } else {
-        dtl[c] = ccfl * (me / std::fabs(veln));
-      }
       // Jacobian
       const double* cl = &U[c * NV];
       double lv[NV];
@@ -1465,9 +1479,10 @@ int orc_implicit_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_re
                       int nsweeps, double* U) {
   if (!check_ctx(cfg, g, r) || !U || !(cfl > 0.0) || nsteps < 0 || nsweeps < 1) return UCG_EINVAL;
   Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
-  std::vector<double> du;
+  std::vector<double> du, dtl;
   for (int step = 0; step < nsteps; ++step) {
-    implicit_du(x, U, cfl / 3.0, nsweeps, 0.0, nullptr, nullptr, du);
+    local_dt(x, U, cfl / 3.0, dtl);  // CALCULATE_CFLL before each IMPLICIT_TIMEs call
+    implicit_du(x, U, dtl, nsweeps, 0.0, nullptr, nullptr, du);
     for (int64_t c = 0; c < g->ncells * NV; ++c) U[c] = U[c] + du[c];
   }
   return UCG_OK;
@@ -1475,10 +1490,11 @@ int orc_implicit_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_re
 
 // DUAL_TIME (time_p.f90:3035-3243, RUNGEKUTTA = 11): one physical step dt
 // in place on U with U^n in U2 and U^{n-1} in U3 (both U before the first
-// step, IT = RESTART), rotated on return; inner implicit iterations, the
-// first without the time term (ISCOUN 1), until sum_c |du_c| V_c /
-// TOTALVOLUME over its largest value in the step is <= tol or maxit are
-// done (*iters).
+// step, IT = RESTART), rotated on return; the local time steps once, from
+// the state at the start of the step (CALCULATE_CFLL in the time loop,
+// :4104); inner implicit iterations, the first without the time term
+// (ISCOUN 1), until sum_c |du_c| V_c / TOTALVOLUME over its largest value
+// in the step is <= tol or maxit are done (*iters).
 int orc_dual_time_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt, double cfl,
                        int maxit, double tol, int nsweeps, double* U, double* U2, double* U3, int* iters) {
   if (!check_ctx(cfg, g, r) || !U || !U2 || !U3 || !(dt > 0.0) || !(cfl > 0.0) || maxit < 1 || nsweeps < 1)
@@ -1487,11 +1503,12 @@ int orc_dual_time_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_r
   const int64_t n = g->ncells;
   double tot = 0.0;
   for (int64_t c = 0; c < n; ++c) tot += g->volume[c];
-  std::vector<double> du;
+  std::vector<double> du, dtl;
+  local_dt(x, U, cfl / 3.0, dtl);
   double firsti = 0.0;
   int jj;
   for (jj = 1; jj <= maxit; ++jj) {
-    implicit_du(x, U, cfl / 3.0, nsweeps, dt, jj == 1 ? nullptr : U2, U3, du);
+    implicit_du(x, U, dtl, nsweeps, dt, jj == 1 ? nullptr : U2, U3, du);
     double res = 0.0;
     for (int64_t c = 0; c < n; ++c) {
       const double* d = &du[c * NV];
@@ -1507,6 +1524,55 @@ int orc_dual_time_step(const ucg_config* cfg, const ucg_geometry* g, const ucg_r
   for (int64_t i = 0; i < n * NV; ++i) {
     U3[i] = U2[i];
     U2[i] = U[i];
+  }
+  return UCG_OK;
+}
+
+// DUAL_TIME_EX (time_p.f90:3244-3436, RUNGEKUTTA = 12) with RELAXATION_EX
+// (:3844-3888): one physical step dt in place on U (U^n in U2, U^{n-1} in
+// U3, both U before the first step), the local time steps once from the
+// state at the start of the step; explicit pseudo-time iterations
+//   du = -(V/dt (1.5 U - 2 U^n + 0.5 U^{n-1}) + RHS(U)) dtau,
+//   dtau = (DTL / V) / (1 + 1.5 DTL/dt),  U += du,
+// until sum_c |du_c| V_c / TOTALVOLUME over its largest value in the step is
+// <= tol or maxit are done (*iters); then U^{n-1} <- U^n <- U and U <- 2 U^n
+// - U^{n-1}, the next step's first iterate.
+int orc_dual_time_step_explicit(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, double dt,
+                                double cfl, int maxit, double tol, double* U, double* U2, double* U3, int* iters) {
+  if (!check_ctx(cfg, g, r) || !U || !U2 || !U3 || !(dt > 0.0) || !(cfl > 0.0) || maxit < 1) return UCG_EINVAL;
+  Ctx x{cfg, g, r, g->ncells, monos(cfg->iorder)};
+  const int64_t n = g->ncells;
+  double tot = 0.0;
+  for (int64_t c = 0; c < n; ++c) tot += g->volume[c];
+  std::vector<double> dtl, rhs(n * NV), du(n * NV), UL, ULV;
+  local_dt(x, U, cfl / 3.0, dtl);
+  double firsti = 0.0;
+  int jj;
+  for (jj = 1; jj <= maxit; ++jj) {
+    residual(x, U, rhs.data(), UL, ULV);
+    double res = 0.0;
+    for (int64_t c = 0; c < n; ++c) {
+      const double dt1 = g->volume[c] / dt;
+      const double dtau = (dtl[c] / g->volume[c]) * (1.0 / (1.0 + (1.5 * (dtl[c] / dt))));
+      double* d = &du[c * NV];
+      for (int v = 0; v < NV; ++v) {
+        const int64_t i = c * NV + v;
+        const double imp = (dt1 * (((1.5 * U[i]) - (2.0 * U2[i])) + (0.5 * U3[i]))) + rhs[i];
+        d[v] = (-imp) * dtau;
+      }
+      res += std::sqrt((d[0] * d[0]) + (d[1] * d[1]) + (d[2] * d[2]) + (d[3] * d[3]) + (d[4] * d[4])) * g->volume[c];
+    }
+    for (int64_t i = 0; i < n * NV; ++i) U[i] = U[i] + du[i];
+    res = res / tot;
+    if (res > firsti) firsti = res;
+    res = res / firsti;
+    if (res <= tol) break;
+  }
+  if (iters) *iters = jj > maxit ? maxit : jj;
+  for (int64_t i = 0; i < n * NV; ++i) {
+    U3[i] = U2[i];
+    U2[i] = U[i];
+    U[i] = (2.0 * U2[i]) - U3[i];
   }
   return UCG_OK;
 }

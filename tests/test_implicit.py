@@ -162,3 +162,46 @@ def test_engine_dual_time_matches_oracle(name):
     err = np.abs(Ug - U).max() / np.abs(U).max()
     print(f"{name}: dual time state rel err {err:.3e}, inner iterations {it_o}")
     assert err < 1e-10
+
+
+def test_oracle_explicit_dual_time_follows_the_explicit_solution():
+    """DUAL_TIME_EX with dt twice the explicit CFL step: the explicit
+    pseudo-time iterations converge (fewer than the limit), the state after
+    three physical steps is within 2 % of six explicit RK3 steps of dt/2, and
+    the returned state is the extrapolated first iterate 2 U^n - U^{n-1}."""
+    m, cfg, U0 = _vortex()
+    o = Oracle(m, cfg)
+    dt = 2.0 * o.compute_dt(U0, 0.5)
+    U, hist = U0.copy(), None
+    for _ in range(3):
+        U, hist, it = o.dual_time_step_explicit(U, hist, dt, 1.5, 200, 1e-3)
+        assert it < 200
+    assert np.array_equal(U, 2.0 * hist[0] - hist[1])
+    Ue = U0.copy()
+    for _ in range(6):
+        Ue = o.rk3_step(Ue, dt / 2.0)
+    assert np.abs(hist[0] - Ue).max() / np.abs(Ue).max() < 0.02
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["vortex_weno5", "muscl_ns_bump"])
+def test_engine_explicit_dual_time_matches_oracle(name):
+    """Three DUAL_TIME_EX steps: the engine's state (the extrapolated next
+    iterate) within 1e-10 of the oracle's and the same number of inner
+    iterations in each step."""
+    from ucns3d_b200.engine import Engine
+    m, cfg, U0 = _vortex() if name == "vortex_weno5" else _bump(NAVIER_STOKES)
+    o = Oracle(m, cfg)
+    dt = 2.0 * o.compute_dt(U0, 0.5)
+    e = Engine(m, cfg)
+    e.set_state(U0)
+    U, hist = U0.copy(), None
+    for s in range(3):
+        U, hist, it_o = o.dual_time_step_explicit(U, hist, dt, 1.5, 200, 1e-3)
+        it_g = e.dual_time_step_explicit(dt, 1.5, 200, 1e-3)
+        assert it_g == it_o, (s, it_g, it_o)
+    e.check_health()
+    Ug = e.get_state()
+    err = np.abs(Ug - U).max() / np.abs(U).max()
+    print(f"{name}: explicit dual time state rel err {err:.3e}, inner iterations {it_o}")
+    assert err < 1e-10

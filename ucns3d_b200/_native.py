@@ -156,7 +156,7 @@ ENGINE_SYMBOLS = [
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
     "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon", "ucg_implicit_step",
     "ucg_dual_time_step", "ucg_rk3_stage", "ucg_halo_set", "ucg_halo_pack", "ucg_halo_unpack",
-    "ucg_set_cell_roles",
+    "ucg_set_cell_roles", "ucg_dual_time_step_explicit",
 ]
 
 
@@ -235,6 +235,9 @@ def engine() -> C.CDLL:
                                            C.POINTER(C.c_int32)]
         lib.ucg_build_recon.restype = C.c_int
         lib.ucg_build_recon.argtypes = [vp, C.POINTER(UcgShapes), C.POINTER(UcgRecon)]
+        lib.ucg_dual_time_step_explicit.restype = C.c_int
+        lib.ucg_dual_time_step_explicit.argtypes = [vp, C.c_double, C.c_double, C.c_int32, C.c_double,
+                                                    C.POINTER(C.c_int32)]
         lib.ucg_set_cell_roles.restype = C.c_int
         lib.ucg_set_cell_roles.argtypes = [vp, C.POINTER(C.c_int8)]
         lib.ucg_rk3_stage.restype = C.c_int

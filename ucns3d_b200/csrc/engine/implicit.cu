@@ -244,10 +244,10 @@ __global__ void k_imp_norm_sum(const double* __restrict__ part, int64_t nb, doub
   *out = t;
 }
 
-// RHS, local time steps, Jacobian and the sweeps from du = 0; the
-// correction in du[*cur]
+// RHS, local time steps (with local_steps; else those in imp_dtl),
+// Jacobian and the sweeps from du = 0; the correction in du[*cur]
 int implicit_correction(ucg_engine* e, const Problem& p, double* U, double ccfl, int32_t nsweeps, double dt,
-                        const double* U2, const double* U3, int* cur) {
+                        const double* U2, const double* U3, int* cur, bool local_steps = true) {
   const int64_t n = e->n;
   const unsigned blocks = (unsigned)((n + 127) / 128);
   double* dtl = (double*)e->imp_dtl.p;
@@ -257,7 +257,7 @@ int implicit_correction(ucg_engine* e, const Problem& p, double* U, double ccfl,
   int rc;
   if ((rc = launch_recon(e, p, U))) return rc;
   if ((rc = launch_flux(e, p, 0, U, U, nullptr, 0.0))) return rc;
-  k_imp_dtl<<<blocks, 128, 0, e->stream>>>(p, U, ccfl, dtl);
+  if (local_steps) k_imp_dtl<<<blocks, 128, 0, e->stream>>>(p, U, ccfl, dtl);
   k_imp_jac<<<blocks, 128, 0, e->stream>>>(p, U, dtl, dt, dinv, off);
   CK(cudaMemsetAsync(du[0], 0, (size_t)n * NV * 8, e->stream));
   int k = 0;
@@ -307,7 +307,9 @@ extern "C" int ucg_implicit_step(ucg_engine* e, double cfl, int32_t nsteps, int3
 
 // DUAL_TIME (src/time_p.f90:3035-3243, RUNGEKUTTA = 11): one physical step
 // dt of BDF2 by inner implicit iterations in pseudo time (local steps at
-// `cfl`): the first without the time term in the right-hand side (ISCOUN
+// `cfl`, formed once from the state at the start of the step, as
+// CALCULATE_CFLL runs in the time loop before DUAL_TIME, :4104): the first
+// without the time term in the right-hand side (ISCOUN
 // 1), the others with it, each adding its correction, until the
 // volume-weighted correction norm, relative to its largest value in this
 // step, is at most inner_tol or max_inner iterations are done; then
@@ -339,11 +341,14 @@ extern "C" int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t 
     e->dual_ready = true;
   }
   const unsigned blocks = (unsigned)((n + 127) / 128);
+  k_imp_dtl<<<blocks, 128, 0, e->stream>>>(p, U, cfl / 3.0, (double*)e->imp_dtl.p);
+  e->launches++;
   double firsti = 0.0;
   int32_t jj = 0;
   for (jj = 1; jj <= max_inner; ++jj) {
     int cur;
-    if ((rc = implicit_correction(e, p, U, cfl / 3.0, nsweeps, dt, jj == 1 ? nullptr : U2, U3, &cur))) return rc;
+    if ((rc = implicit_correction(e, p, U, cfl / 3.0, nsweeps, dt, jj == 1 ? nullptr : U2, U3, &cur, false)))
+      return rc;
     const double* du = (const double*)e->imp_du.p + cur * n * NV;
     k_imp_norm_part<<<(unsigned)nblk, 256, 0, e->stream>>>(p, du, part);
     k_imp_norm_sum<<<1, 1, 0, e->stream>>>(part, nblk, part + nblk);
@@ -360,5 +365,103 @@ extern "C" int ucg_dual_time_step(ucg_engine* e, double dt, double cfl, int32_t 
   if (inner_iters) *inner_iters = jj > max_inner ? max_inner : jj;
   CK(cudaMemcpyAsync(U3, U2, (size_t)n * NV * 8, cudaMemcpyDeviceToDevice, e->stream));
   CK(cudaMemcpyAsync(U2, U, (size_t)n * NV * 8, cudaMemcpyDeviceToDevice, e->stream));
+  return UCG_OK;
+}
+
+namespace {
+
+// RELAXATION_EX (src/time_p.f90:3844-3888): per cell the explicit
+// pseudo-time correction du = -(V/dt (1.5 U - 2 U^n + 0.5 U^{n-1}) + RHS)
+// dtau, dtau = (DTL/V) / (1 + 1.5 DTL/dt), in the reference's order of
+// operations
+__global__ void k_dtex_du(Problem p, const double* __restrict__ U, const double* __restrict__ U2,
+                          const double* __restrict__ U3, const double* __restrict__ dtl, double dt,
+                          double* __restrict__ du) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= p.n) return;
+  const double v = p.vol[c], dt1 = v / dt;
+  const double dtau = (dtl[c] / v) * (1.0 / (1.0 + (1.5 * (dtl[c] / dt))));
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const int64_t i = c * NV + k;
+    const double imp = (dt1 * (((1.5 * U[i]) - (2.0 * U2[i])) + (0.5 * U3[i]))) + p.rhs[i];
+    du[i] = (-imp) * dtau;
+  }
+}
+
+// U^{n-1} <- U^n, U^n <- U, U <- 2 U^n - U^{n-1} (DUAL_TIME_EX, :3422-3430)
+__global__ void k_dtex_rotate(int64_t m, double* __restrict__ U, double* __restrict__ U2, double* __restrict__ U3) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double u = U[i], u2 = U2[i];
+  U3[i] = u2;
+  U2[i] = u;
+  U[i] = (2.0 * u) - u2;
+}
+
+}  // namespace
+
+// DUAL_TIME_EX (src/time_p.f90:3244-3436, RUNGEKUTTA = 12): one physical
+// step dt of BDF2 by explicit pseudo-time iterations (RELAXATION_EX; local
+// steps at `cfl` formed once from the state at the start of the step), each
+// adding its correction, until the volume-weighted correction norm,
+// relative to its largest value in this step, is at most inner_tol or
+// max_inner iterations are done; then U^{n-1} <- U^n <- U and the state
+// becomes 2 U^n - U^{n-1}, the next step's first iterate.  The history is
+// the one of ucg_dual_time_step (it starts from the state at the first call
+// after ucg_set_state, IT = RESTART).
+extern "C" int ucg_dual_time_step_explicit(ucg_engine* e, double dt, double cfl, int32_t max_inner, double inner_tol,
+                                           int32_t* inner_iters) {
+  if (!e) return UCG_EINVAL;
+  if (!(dt > 0.0) || !std::isfinite(dt) || !(cfl > 0.0) || !std::isfinite(cfl) || max_inner < 1 ||
+      !(inner_tol >= 0.0))
+    return fail(e, UCG_EINVAL, "dt > 0, cfl > 0, max_inner >= 1 and inner_tol >= 0 are needed");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (!e->roles.empty()) return fail(e, UCG_EINVAL, "dual time steps cover whole meshes (no partition roles)");
+  cudaSetDevice(e->device);
+  const int64_t n = e->n;
+  int rc = implicit_buffers(e);
+  rc = rc ? rc : alloc(e, e->dual_hist, (size_t)n * NV * 8 * 2);
+  const int64_t nblk = (n + 255) / 256;
+  rc = rc ? rc : alloc(e, e->dual_part, (size_t)(nblk + 1) * 8);
+  if (rc) return rc;
+  Problem p = make_problem(e);
+  double* U = (double*)e->Un.p;
+  double* U2 = (double*)e->dual_hist.p;
+  double* U3 = U2 + n * NV;
+  double* part = (double*)e->dual_part.p;
+  double* dtl = (double*)e->imp_dtl.p;
+  double* du = (double*)e->imp_du.p;
+  if (!e->dual_ready) {
+    CK(cudaMemcpyAsync(U2, U, (size_t)n * NV * 8, cudaMemcpyDeviceToDevice, e->stream));
+    CK(cudaMemcpyAsync(U3, U, (size_t)n * NV * 8, cudaMemcpyDeviceToDevice, e->stream));
+    e->dual_ready = true;
+  }
+  const unsigned blocks = (unsigned)((n + 127) / 128);
+  k_imp_dtl<<<blocks, 128, 0, e->stream>>>(p, U, cfl / 3.0, dtl);
+  e->launches++;
+  double firsti = 0.0;
+  int32_t jj = 0;
+  for (jj = 1; jj <= max_inner; ++jj) {
+    if ((rc = launch_recon(e, p, U))) return rc;
+    if ((rc = launch_flux(e, p, 0, U, U, nullptr, 0.0))) return rc;
+    k_dtex_du<<<blocks, 128, 0, e->stream>>>(p, U, U2, U3, dtl, dt, du);
+    k_imp_norm_part<<<(unsigned)nblk, 256, 0, e->stream>>>(p, du, part);
+    k_imp_norm_sum<<<1, 1, 0, e->stream>>>(part, nblk, part + nblk);
+    k_imp_add<<<blocks, 128, 0, e->stream>>>(p, U, du);
+    e->launches += 4;
+    double res = 0.0;
+    CK(cudaMemcpyAsync(&res, part + nblk, 8, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    res = res / e->totvol;
+    if (res > firsti) firsti = res;
+    res = res / firsti;
+    if (res <= inner_tol) break;
+  }
+  if (inner_iters) *inner_iters = jj > max_inner ? max_inner : jj;
+  const int64_t m = n * NV;
+  k_dtex_rotate<<<(unsigned)((m + 255) / 256), 256, 0, e->stream>>>(m, U, U2, U3);
+  e->launches++;
+  CK(cudaGetLastError());
   return UCG_OK;
 }

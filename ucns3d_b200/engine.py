@@ -253,6 +253,14 @@ class Engine:
         self._check(self.lib.ucg_dual_time_step(self._h, dt, cfl, max_inner, inner_tol, nsweeps, C.byref(it)))
         return int(it.value)
 
+    def dual_time_step_explicit(self, dt: float, cfl: float, max_inner: int = 50, inner_tol: float = 1e-3) -> int:
+        """One DUAL_TIME_EX physical step dt (BDF2, explicit pseudo-time
+        iterations at pseudo CFL `cfl`); returns the inner iterations taken.
+        The state afterwards is the next step's first iterate 2 U^n - U^{n-1}."""
+        it = C.c_int32()
+        self._check(self.lib.ucg_dual_time_step_explicit(self._h, dt, cfl, max_inner, inner_tol, C.byref(it)))
+        return int(it.value)
+
     def mood_state(self) -> dict:
         """MOOD after the last RK3 stage (cfg.mood 1): MOOD_O per cell (1
         first order, 2 MUSCL, IORDER + 1 the target scheme) and RECALC (the
