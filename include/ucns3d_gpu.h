@@ -440,7 +440,8 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
  * FULL = 0 or CHECKSOL send there (central polynomial, FIND_BOUNDS,
  * Venkatakrishnan, CHECKSOLX), and with Navier-Stokes of the viscous
  * fluxes at every face point, the face-point gradients and the viscous
- * least squares.  p denotes the free-stream state bc_state[5] (primitive:
+ * least squares; the wall force and the runs below cover the same WENO and
+ * CWENO configurations.  p denotes the free-stream state bc_state[5] (primitive:
  * rho, u, v, w, pressure) used by the inflow, outflow and far-field ghost
  * states.  Host arrays; [n][5] as everywhere.  Other configurations return
  * UCG_EINVAL.
@@ -469,13 +470,13 @@ int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, dou
 int ucg_tangent_run(ucg_engine* e, int32_t nsteps, double dt, const double* dU0, const double* dp, double* J,
                     double* dJ);
 /* The same runs with the scalar output chosen: UCG_OBJ_FORCE_X the wall
- * force above (MUSCL), UCG_OBJ_KE the domain kinetic energy
+ * force above, UCG_OBJ_KE the domain kinetic energy
  * J = sum_c V_c |rho u|^2 / (2 rho) (the TGV sum of time_p.f90:4145-4198
- * without its normalisation), which also covers the conserved-variable WENO
- * and CWENO residuals: the reverse sweeps then run the WENO VJP (nonlinear
- * weights, smoothness indicators, least squares, MUSCL fall-back) at every
- * recomputed stage state.  ucg_adjoint_run/ucg_tangent_run are these with
- * UCG_OBJ_FORCE_X.                                                        */
+ * without its normalisation).  With the conserved-variable WENO and CWENO
+ * residuals the reverse sweeps run the WENO VJP (nonlinear weights,
+ * smoothness indicators, least squares, MUSCL fall-back) at every
+ * recomputed stage state, and the wall force sums its quadrature points.
+ * ucg_adjoint_run/ucg_tangent_run are these with UCG_OBJ_FORCE_X.         */
 enum { UCG_OBJ_FORCE_X = 1, UCG_OBJ_KE = 2 };
 int ucg_adjoint_run_obj(ucg_engine* e, int32_t objective, int32_t nsteps, double dt, int32_t every, double* J,
                         double* dJdU0, double* dJdp);

@@ -1124,44 +1124,54 @@ __global__ void k_jvp_sum(Problem p, const double* __restrict__ tflux, double* _
 }
 
 // ------------------------------------------------------------ wall force
-// per cell: sum over its wall faces of (sum_q w_q p_q - PRES) * area * n_x;
-// with dU != null the tangent of the same sum, with adjF != null the
-// adjoint of the face values (jbar * area * n_x * w_q * dp/du), else 0.
+// per cell: sum over its wall faces of (sum_q w_q p_q - PRES) * area * n_x
+// (the face points of [n][F][QS] face values: one for MUSCL IORDER 1, the
+// quadrature points for WENO/CWENO); with dU != null the tangent of the
+// same sum, with adjF != null the adjoint of the face values (jbar * area *
+// n_x * w_q * dp/du), else 0.
 __global__ void k_force_cell(Problem p, const double* __restrict__ U, const double* __restrict__ dU,
                              const double* __restrict__ tdul, double* __restrict__ fcell, double* __restrict__ adjF,
                              double jbar) {
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= p.n) return;
   const int nf = p.nfaces[c];
+  const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
   const double* dul = (const double*)p.dul;
   double sum = 0.0;
   for (int f = 0; f < nf; ++f) {
     const bool wall = p.neigh[c * MF + f] < 0 && p.bc[c * MF + f] == 4;
+    const int ft = p.ftype[c * MF + f], nq = face_nq(p, ft);
     if (adjF)
+      for (int q = 0; q < QS; ++q)
 #pragma unroll
-      for (int v = 0; v < NV; ++v) adjF[(c * MF + f) * NV + v] = 0.0;
+        for (int v = 0; v < NV; ++v) adjF[((c * MF + f) * QS + q) * NV + v] = 0.0;
     if (!wall) continue;
     const double nx = p.rot[(c * MF + f) * 4 + 0] * p.rot[(c * MF + f) * 4 + 3];
     const double area = p.area[c * MF + f];
-    const double w = face_weight(p, p.ftype[c * MF + f], 0);
-    Dual<NV> u[NV], pr[NV];
+    double ssp = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      const int64_t s = (c * MF + f) * QS + q;
+      const double w = face_weight(p, ft, q);
+      Dual<NV> u[NV], pr[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      u[v] = Dual<NV>(U[c * NV + v] + dul[(c * MF + f) * NV + v]);
-      u[v].d[v] = 1.0;
+      for (int v = 0; v < NV; ++v) {
+        u[v] = Dual<NV>(U[c * NV + v] + dul[s * NV + v]);
+        u[v].d[v] = 1.0;
+      }
+      cons2prim(p.gamma, u, pr);
+      if (dU) {
+        double t = 0.0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) t += pr[4].d[v] * (dU[c * NV + v] + tdul[s * NV + v]);
+        sum += w * t * area * nx;
+      } else {
+        ssp = ssp + (pr[4].v * w);
+      }
+      if (adjF)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) adjF[s * NV + v] = jbar * area * nx * w * pr[4].d[v];
     }
-    cons2prim(p.gamma, u, pr);
-    if (dU) {
-      double t = 0.0;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) t += pr[4].d[v] * (dU[c * NV + v] + tdul[(c * MF + f) * NV + v]);
-      sum += w * t * area * nx;
-    } else {
-      sum += ((pr[4].v * w) - p.pres) * area * nx;
-    }
-    if (adjF)
-#pragma unroll
-      for (int v = 0; v < NV; ++v) adjF[(c * MF + f) * NV + v] = jbar * area * nx * w * pr[4].d[v];
+    if (!dU) sum += (ssp - p.pres) * area * nx;
   }
   fcell[c] = sum;
 }
@@ -1338,12 +1348,19 @@ int jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* d
 int force_device(ucg_engine* e, const Problem& p, const double* U, const double* dU, double* out) {
   int rc = launch_recon(e, p, U);
   if (rc) return rc;
-  if (dU) {
-    k_jvp_muscl<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (double*)e->adj_tdul.p, nullptr, false);
+  const bool weno = e->cfg.scheme == 3;
+  double* tdul = weno ? (double*)e->adjw_face.p : (double*)e->adj_tdul.p;
+  if (dU && weno) {  // the tangent face values: dG = least squares of dU, then the WENO tangent
+    Problem pt = p;
+    pt.gbuf = e->adjw_gbar.p;
+    CK(launch_lsq_f64(e->cfg.iorder, pt, dU, e->stream));
+    e->launches++;
+    if ((rc = launch_weno_tangent(e, p, U, dU, (const double*)e->adjw_gbar.p, tdul))) return rc;
+  } else if (dU) {
+    k_jvp_muscl<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, tdul, nullptr, false);
     e->launches++;
   }
-  k_force_cell<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, (const double*)e->adj_tdul.p,
-                                                              (double*)e->adj_fcell.p, nullptr, 0.0);
+  k_force_cell<<<blocks_for(e->n, 128), 128, 0, e->stream>>>(p, U, dU, tdul, (double*)e->adj_fcell.p, nullptr, 0.0);
   k_sum1<<<1, 1024, 0, e->stream>>>((const double*)e->adj_fcell.p, e->n, out);
   e->launches += 2;
   CK(cudaGetLastError());
@@ -1352,9 +1369,25 @@ int force_device(ucg_engine* e, const Problem& p, const double* U, const double*
 
 // dJ/dU at state U into g (device)
 int force_vjp_device(ucg_engine* e, const Problem& p, const double* U, double* g) {
+  const int64_t n = e->n;
+  if (e->cfg.scheme == 3) {  // WENO: the face-value seed through the reconstruction's reverse
+    int rc = launch_recon(e, p, U);
+    if (rc) return rc;
+    double* adjF = (double*)e->adjw_face.p;
+    k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p, adjF, 1.0);
+    e->launches++;
+    if ((rc = launch_weno_adjoint(e, p, U, adjF, (double*)e->adjw_gbar.p, (double*)e->adjw_scr.p,
+                                  (double*)e->adjw_self.p, (double*)e->adjw_contrib.p)))
+      return rc;
+    k_adj_gather<<<blocks_for(n, 128), 128, 0, e->stream>>>(n, (const int64_t*)e->adjw_rptr.p,
+                                                            (const int64_t*)e->adjw_rsrc.p,
+                                                            (const double*)e->adjw_contrib.p, g);
+    e->launches++;
+    CK(cudaGetLastError());
+    return UCG_OK;
+  }
   int rc = adj_forward(e, p, U);
   if (rc) return rc;
-  const int64_t n = e->n;
   k_force_cell<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, U, nullptr, nullptr, (double*)e->adj_fcell.p,
                                                           (double*)e->adj_face.p, 1.0);
   k_adj_muscl<<<blocks_for(n, 128), 128, 0, e->stream>>>(p, fwd_store(e), (const double*)e->adj_face.p,
@@ -1554,8 +1587,6 @@ int run_setup(ucg_engine* e, int obj, RunOps& o) {
   o.weno = e->cfg.scheme == 3;
   o.obj = obj;
   if (obj != UCG_OBJ_FORCE_X && obj != UCG_OBJ_KE) return fail(e, UCG_EINVAL, "unknown objective");
-  if (o.weno && obj == UCG_OBJ_FORCE_X)
-    return fail(e, UCG_EINVAL, "the wall-force objective covers MUSCL (IORDER 1); WENO runs take the kinetic energy");
   int rc = o.weno ? adjw_setup(e) : adj_setup(e);
   if (rc) return rc;
   const int64_t n = e->n;
@@ -1613,7 +1644,9 @@ extern "C" {
 
 int ucg_force(ucg_engine* e, double* fx) {
   if (!e || !fx) return fail(e, UCG_EINVAL, "null argument");
-  int rc = adj_setup(e);
+  int rc = e->cfg.scheme == 3 ? adjw_setup(e) : adj_setup(e);
+  rc = rc ? rc : alloc(e, e->adj_bar, (size_t)4 * e->n * NV * 8 + 64 * 8);
+  rc = rc ? rc : alloc(e, e->adj_fcell, (size_t)e->n * 8);
   if (rc) return rc;
   cudaSetDevice(e->device);
   Problem p = make_problem(e);
@@ -1626,12 +1659,15 @@ int ucg_force(ucg_engine* e, double* fx) {
 
 int ucg_force_vjp(ucg_engine* e, double* dJdU) {
   if (!e || !dJdU) return fail(e, UCG_EINVAL, "null argument");
-  int rc = adj_setup(e);
+  const bool weno = e->cfg.scheme == 3;
+  int rc = weno ? adjw_setup(e) : adj_setup(e);
+  rc = rc ? rc : alloc(e, e->adj_fcell, (size_t)e->n * 8);
   if (rc) return rc;
   cudaSetDevice(e->device);
   Problem p = make_problem(e);
-  if ((rc = force_vjp_device(e, p, (const double*)e->Un.p, (double*)e->adj_mu.p))) return rc;
-  if ((rc = copy_out(e, dJdU, (const double*)e->adj_mu.p, (size_t)e->n * NV))) return rc;
+  double* g = weno ? (double*)e->adjw_mu.p : (double*)e->adj_mu.p;
+  if ((rc = force_vjp_device(e, p, (const double*)e->Un.p, g))) return rc;
+  if ((rc = copy_out(e, dJdU, g, (size_t)e->n * NV))) return rc;
   CK(cudaStreamSynchronize(e->stream));
   return UCG_OK;
 }
