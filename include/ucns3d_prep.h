@@ -58,11 +58,21 @@ ucp_mesh* ucp_mixed_box(int32_t n, double L, uint64_t seed);
  * reader of OPEN_ARBITRARY / FIND_SHAPE / READ_BOUND, src/io.f90:4157-4304,
  * src/grid_p.f90:1652-1743, src/bc_p.f90:36-130): hexahedra, tetrahedra,
  * pyramids and prisms in the 8-node encoding with repeated nodes, boundary
- * faces with their codes.  Periodic faces (codes 5, 50) are refused.  The
- * mesh is then prepared like any other; every boundary face must appear in
- * GRID.bnd.  ucp_write_grid writes a prepared, non-periodic mesh in the same
+ * faces with their codes.  Periodic faces (codes 5, 50) are paired as
+ * APPLY_BOUNDARY does (src/bc_p.f90:499-620): a face whose centroid lies on
+ * the low side of the nodes' bounding box in one axis pairs with the face of
+ * the same shape on the high side whose centroid has the same other two
+ * coordinates (within 1e-13 of the coordinates' size), the axis becomes
+ * periodic with the box's extent as the period (XPER, YPER, ZPER of
+ * src/io.f90:4977-4979), and the two faces meet like interior faces.  A
+ * periodic face off the box's sides or without a partner is refused.  The
+ * mesh is then prepared like any other; every other boundary face must
+ * appear in GRID.bnd.  ucp_write_grid writes a prepared mesh in the same
  * format (coordinates with 17 significant digits, so a read-back prepares
- * to the same tables).                                                    */
+ * to the same tables); on a periodic mesh the faces on the periodic sides
+ * get code 5 and the nodes a cell sees across them image nodes of their
+ * own, and a mesh whose periodic faces are off the box's sides (a jittered
+ * periodic box) is refused with UCG_EINVAL.                               */
 ucp_mesh* ucp_read_grid(const char* prefix);
 int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix);
 

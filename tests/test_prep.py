@@ -162,6 +162,61 @@ def test_grid_files_round_trip(kind, tmp_path):
     assert len([x for x in lines if x]) == int(((ga["neigh"] < 0) & (np.arange(6)[None, :] < ga["nfaces"][:, None])).sum())
 
 
+@pytest.mark.parametrize("kind", ["hex", "tet", "mixed", "hex_xz"])
+def test_periodic_grid_files_round_trip(kind, tmp_path):
+    """Periodic meshes in GRID files: the writer gives each node that a cell
+    sees across a periodic side its own image node and writes the faces on
+    the periodic sides with code 5; the reader pairs them as APPLY_BOUNDARY
+    does (same shape, centroids on opposite sides of the bounding box with
+    the same other two coordinates, period = the box's extent) and prepares
+    to the same geometry, stencils, tables and oracle residual, bit for bit."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    from oracle import Oracle
+    from ucns3d_b200.config import EULER, make_config
+    from ucns3d_b200.mesh import IC_TGV
+    m = {"hex": lambda: Mesh.box_hex(6, 5, 4),
+         "tet": lambda: Mesh.box_tet(4, 4, 4, jitter=0.0, seed=3),
+         "mixed": lambda: Mesh.mixed_box(6),
+         "hex_xz": lambda: Mesh.box_hex(6, 5, 4, periodic=(1, 0, 1), bc=(0, 0, 4, 4, 0, 0))}[kind]()
+    m = m.prepare(SCHEME_WENO, 2)
+    prefix = str(tmp_path) + "/"
+    m.write_grid(prefix)
+    codes = np.loadtxt(prefix + "GRID.bnd", dtype=np.int64, ndmin=2)[:, 5]
+    assert (codes == 5).sum() > 0
+    r = Mesh.read_grid(prefix).prepare(SCHEME_WENO, 2)
+    ga, gb = m.geometry(), r.geometry()
+    for k in ("nfaces", "face_type", "neigh", "neigh_face", "bc", "qperm", "face_angle", "face_area", "dih",
+              "qpoints", "volume", "minedge", "invccjac", "basis_mean", "admis", "full"):
+        assert np.array_equal(ga[k], gb[k]), k
+    ra, rb = m.recon(), r.recon()
+    assert np.array_equal(ra["stencil"], rb["stencil"])
+    ia = ra["invmat"][ra["table_id"]] if ra["table_id"] is not None else ra["invmat"]
+    ib = rb["invmat"][rb["table_id"]] if rb["table_id"] is not None else rb["invmat"]
+    assert np.array_equal(ia, ib)
+    cfg = make_config(m, governing=EULER)
+    U = m.initial_condition(IC_TGV, [1.4, 5.0, 1.0])
+    assert np.array_equal(Oracle(r, cfg).residual(U), Oracle(m, cfg).residual(U))
+
+
+def test_periodic_grid_errors(tmp_path):
+    """Periodic sides the GRID format cannot pair are refused: a jittered
+    periodic box (faces off the box's sides) is not written, and a code 5
+    face without a partner on the opposite side is not read."""
+    m = Mesh.box_tet(4, 4, 4, jitter=0.15, seed=3).prepare(SCHEME_WENO, 2)
+    with pytest.raises(RuntimeError, match="off the sides"):
+        m.write_grid(str(tmp_path) + "/j_")
+    m = Mesh.box_hex(4, 4, 4).prepare(SCHEME_MUSCL, 1)
+    prefix = str(tmp_path) + "/h_"
+    m.write_grid(prefix)
+    lines = open(prefix + "GRID.bnd").read().split("\n")
+    with open(prefix + "GRID.bnd", "w") as f:
+        f.write("\n".join(lines[1:]))  # one face of a periodic pair dropped
+    with pytest.raises(RuntimeError, match="periodic"):
+        Mesh.read_grid(prefix)
+
+
 def test_grid_reader_shapes_and_errors(tmp_path):
     """The 8-node encoding of the four cell shapes, told apart by repeated
     nodes as FIND_SHAPE does: a pyramid on a hexahedron's top with a

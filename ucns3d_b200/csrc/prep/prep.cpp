@@ -1288,25 +1288,24 @@ ucp_mesh* ucp_read_grid(const char* prefix) {
     }
     if (ok) set_cell(m, c, type, ids, pts);
   }
+  struct BndFace {
+    std::array<int64_t, 4> k;  // 0-based node ids in file order, -1 for a triangle's fourth
+    int nv, code;
+  };
+  std::vector<BndFace> bnd;
   long long b[4];
   int code;
   while (ok && std::fscanf(fb, "%lld %lld %lld %lld %lld %d", &id, &b[0], &b[1], &b[2], &b[3], &code) == 6) {
-    if (code == 5 || code == 50) {
-      set_err("GRID.bnd: periodic faces (codes 5, 50) are not supported by this reader");
-      ok = false;
-      break;
-    }
-    std::array<int64_t, 4> k = {b[0] - 1, b[1] - 1, b[2] - 1, b[2] == b[3] ? -1 : b[3] - 1};
     const int nv = b[2] == b[3] ? 3 : 4;
-    std::sort(k.begin(), k.begin() + nv);
-    m->bnd_code[k] = code;
+    BndFace r{{b[0] - 1, b[1] - 1, b[2] - 1, nv == 3 ? -1 : b[3] - 1}, nv, code};
+    for (int k = 0; k < nv; ++k)
+      if (r.k[k] < 0 || (size_t)r.k[k] >= node.size() || std::isnan(node[r.k[k]].x)) {
+        set_err("GRID.bnd: face " + std::to_string(id) + " names a node missing from GRID.vrt");
+        ok = false;
+      }
+    bnd.push_back(r);
   }
   close_all();
-  if (!ok) {
-    delete m;
-    return nullptr;
-  }
-  m->has_bnd = true;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (const V3& p : node)
     if (!std::isnan(p.x)) {
@@ -1317,7 +1316,117 @@ ucp_mesh* ucp_read_grid(const char* prefix) {
   for (int k = 0; k < 3; ++k) {
     m->box_lo[k] = lo[k];
     m->box_hi[k] = hi[k];
+    m->L[k] = hi[k] - lo[k];  // XPER, YPER, ZPER of READ_INPUT (io.f90:4977-4979)
   }
+  // Periodic faces (codes 5 and 50; APPLY_BOUNDARY, bc_p.f90:499-620): a
+  // face whose centroid lies on the low side of the bounding box in one
+  // axis pairs with the face of the same shape on the high side whose
+  // centroid has the same other two coordinates.  The pair's nodes are
+  // then one node each (matched by those two coordinates), so the faces
+  // meet like interior faces and the axis is periodic with the box's
+  // extent as the period.
+  std::vector<int64_t> rep(node.size());
+  std::iota(rep.begin(), rep.end(), 0);
+  auto find = [&](int64_t a) {
+    while (rep[a] != a) a = rep[a] = rep[rep[a]];
+    return a;
+  };
+  auto coord = [](const V3& p, int k) { return k == 0 ? p.x : k == 1 ? p.y : p.z; };
+  const double ext = std::max({1.0, std::fabs(lo[0]), std::fabs(lo[1]), std::fabs(lo[2]), std::fabs(hi[0]),
+                               std::fabs(hi[1]), std::fabs(hi[2])});
+  const double tol = 1e-13 * ext;  // TOLSMALL of the reference, relative to the coordinates' size
+  struct PerFace {
+    V3 c;
+    size_t i;
+  };
+  std::vector<PerFace> side[3][2];
+  for (size_t i = 0; ok && i < bnd.size(); ++i) {
+    if (bnd[i].code != 5 && bnd[i].code != 50) continue;
+    V3 c = {0, 0, 0};
+    for (int k = 0; k < bnd[i].nv; ++k) c = c + node[bnd[i].k[k]];
+    c = (1.0 / bnd[i].nv) * c;
+    int axis = -1, hiside = 0;
+    for (int a = 0; a < 3 && axis < 0; ++a) {
+      if (std::fabs(coord(c, a) - lo[a]) < tol) axis = a, hiside = 0;
+      else if (std::fabs(coord(c, a) - hi[a]) < tol) axis = a, hiside = 1;
+    }
+    if (axis < 0) {
+      set_err("GRID.bnd: periodic face " + std::to_string(i + 1) + " does not lie on a side of the bounding box");
+      ok = false;
+      break;
+    }
+    side[axis][hiside].push_back({c, i});
+  }
+  for (int a = 0; ok && a < 3; ++a) {
+    if (side[a][0].empty() && side[a][1].empty()) continue;
+    const int a1 = (a + 1) % 3, a2 = (a + 2) % 3;
+    auto& H = side[a][1];
+    std::sort(H.begin(), H.end(), [&](const PerFace& u, const PerFace& v) { return coord(u.c, a1) < coord(v.c, a1); });
+    std::vector<char> used(H.size(), 0);
+    size_t paired = 0;
+    for (const PerFace& f : side[a][0]) {
+      const BndFace& A = bnd[f.i];
+      size_t j = std::lower_bound(H.begin(), H.end(), coord(f.c, a1) - tol,
+                                  [&](const PerFace& u, double x) { return coord(u.c, a1) < x; }) -
+                 H.begin();
+      for (; j < H.size() && coord(H[j].c, a1) <= coord(f.c, a1) + tol; ++j)
+        if (!used[j] && bnd[H[j].i].nv == A.nv && std::fabs(coord(H[j].c, a2) - coord(f.c, a2)) < tol) break;
+      if (j >= H.size() || coord(H[j].c, a1) > coord(f.c, a1) + tol) {
+        set_err("GRID.bnd: periodic face " + std::to_string(f.i + 1) + " has no partner on the opposite side");
+        ok = false;
+        break;
+      }
+      used[j] = 1;
+      ++paired;
+      const BndFace& B = bnd[H[j].i];
+      for (int u = 0; u < B.nv && ok; ++u) {
+        const V3& q = node[B.k[u]];
+        int match = -1;
+        for (int v = 0; v < A.nv; ++v) {
+          const V3& pa = node[A.k[v]];
+          if (std::fabs(coord(pa, a1) - coord(q, a1)) < tol && std::fabs(coord(pa, a2) - coord(q, a2)) < tol) match = v;
+        }
+        if (match < 0) {
+          set_err("GRID.bnd: the nodes of periodic faces " + std::to_string(f.i + 1) + " and " +
+                  std::to_string(H[j].i + 1) + " do not match");
+          ok = false;
+          break;
+        }
+        const int64_t x = find(A.k[match]), y = find(B.k[u]);
+        if (x != y) rep[std::max(x, y)] = std::min(x, y);
+      }
+    }
+    if (ok && paired != H.size()) {
+      set_err("GRID.bnd: a periodic face on the high side of axis " + std::to_string(a) + " has no partner");
+      ok = false;
+    }
+    if (ok) m->per[a] = 1;
+  }
+  if (ok && (m->per[0] || m->per[1] || m->per[2]))
+    for (int64_t c = 0; c < m->nc && ok; ++c) {
+      const int nv = topo(m->type[c]).nv;
+      for (int k = 0; k < nv; ++k) m->gnode[c * 8 + k] = find(m->gnode[c * 8 + k]);
+      for (int k = 0; k < nv && ok; ++k)
+        for (int l = k + 1; l < nv; ++l)
+          if (m->gnode[c * 8 + k] == m->gnode[c * 8 + l]) {
+            set_err("GRID: cell " + std::to_string(c + 1) + " meets its own periodic image");
+            ok = false;
+            break;
+          }
+    }
+  for (const BndFace& r : bnd) {
+    if (!ok) break;
+    if (r.code == 5 || r.code == 50) continue;
+    std::array<int64_t, 4> k = r.k;
+    for (int v = 0; v < r.nv; ++v) k[v] = find(k[v]);
+    std::sort(k.begin(), k.begin() + r.nv);
+    m->bnd_code[k] = r.code;
+  }
+  if (!ok) {
+    delete m;
+    return nullptr;
+  }
+  m->has_bnd = true;
   return m;
 }
 
@@ -1326,9 +1435,72 @@ int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix) {
     set_err("write_grid needs a prepared mesh (its boundary faces and codes)");
     return UCG_ESTATE;
   }
-  if (m->per[0] || m->per[1] || m->per[2]) {
-    set_err("write_grid: periodic meshes are not written (their faces would need codes 5/50 and pairing)");
-    return UCG_EINVAL;
+  const bool periodic = m->per[0] || m->per[1] || m->per[2];
+  // nodes by global id (each node's position as its first cell sees it);
+  // on a periodic mesh a node seen by a cell across a periodic side (shifted
+  // by a whole period) is written again as its own image node
+  int64_t nn = 0;
+  for (int64_t c = 0; c < m->nc; ++c)
+    for (int k = 0; k < topo(m->type[c]).nv; ++k) nn = std::max(nn, m->gnode[c * 8 + k] + 1);
+  std::vector<V3> pos(nn);
+  std::vector<char> seen(nn, 0);
+  std::map<std::array<int64_t, 4>, int64_t> image;  // (global id, shift in x, y, z) -> 0-based output id
+  std::vector<V3> ipos;
+  std::vector<int64_t> cid((size_t)m->nc * 8, -1);  // output node id of each cell vertex
+  for (int64_t c = 0; c < m->nc; ++c)
+    for (int k = 0; k < topo(m->type[c]).nv; ++k) {
+      const int64_t g = m->gnode[c * 8 + k];
+      const V3 p = vtx(*m, c, k);
+      if (!seen[g]) {
+        seen[g] = 1;
+        pos[g] = p;
+      }
+      const V3 d = p - pos[g];
+      const std::array<int64_t, 4> key = {g, m->per[0] ? std::llround(d.x / m->L[0]) : 0,
+                                          m->per[1] ? std::llround(d.y / m->L[1]) : 0,
+                                          m->per[2] ? std::llround(d.z / m->L[2]) : 0};
+      if (key[1] == 0 && key[2] == 0 && key[3] == 0) {
+        cid[c * 8 + k] = g;
+        continue;
+      }
+      auto it = image.find(key);
+      if (it == image.end()) {
+        it = image.emplace(key, nn + (int64_t)ipos.size()).first;
+        ipos.push_back(p);
+      }
+      cid[c * 8 + k] = it->second;
+    }
+  // faces across a periodic side: the neighbour sees them shifted by a period
+  auto face_centre = [&](int64_t c, int f) {
+    const int nv = m->face_type[c * 6 + f] == 5 ? 4 : 3;
+    V3 s = {0, 0, 0};
+    for (int k = 0; k < nv; ++k) s = s + vtx(*m, c, m->fnode[c * 24 + f * 4 + k]);
+    return (1.0 / nv) * s;
+  };
+  auto across = [&](int64_t c, int f) {
+    const int64_t nb = m->neigh[c * 6 + f];
+    if (!periodic || nb < 0) return false;
+    const V3 d = face_centre(c, f) - face_centre(nb, m->neigh_face[c * 6 + f]);
+    return norm(d) > 1e-9 * std::max({m->L[0], m->L[1], m->L[2]});
+  };
+  if (periodic) {
+    const double tol = 1e-13 * std::max({1.0, std::fabs(m->box_lo[0]), std::fabs(m->box_lo[1]),
+                                         std::fabs(m->box_lo[2]), std::fabs(m->box_hi[0]), std::fabs(m->box_hi[1]),
+                                         std::fabs(m->box_hi[2])});
+    for (int64_t c = 0; c < m->nc; ++c)
+      for (int f = 0; f < m->nfaces[c]; ++f) {
+        if (!across(c, f)) continue;
+        const V3 fc = face_centre(c, f);
+        const double x[3] = {fc.x, fc.y, fc.z};
+        bool side = false;
+        for (int a = 0; a < 3; ++a)
+          side = side || (m->per[a] && (std::fabs(x[a] - m->box_lo[a]) < tol || std::fabs(x[a] - m->box_hi[a]) < tol));
+        if (!side) {
+          set_err("write_grid: a periodic face of cell " + std::to_string(c + 1) +
+                  " is off the sides of the box, where the GRID format's periodic pairing looks for it");
+          return UCG_EINVAL;
+        }
+      }
   }
   const std::string pre = prefix ? prefix : "";
   FILE* fv = std::fopen((pre + "GRID.vrt").c_str(), "w");
@@ -1341,24 +1513,12 @@ int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix) {
     set_err("cannot create " + pre + "GRID.vrt, GRID.cel or GRID.bnd");
     return UCG_EINVAL;
   }
-  // nodes by global id (each node's position as its first cell sees it)
-  int64_t nn = 0;
-  for (int64_t c = 0; c < m->nc; ++c)
-    for (int k = 0; k < topo(m->type[c]).nv; ++k) nn = std::max(nn, m->gnode[c * 8 + k] + 1);
-  std::vector<V3> pos(nn);
-  std::vector<char> seen(nn, 0);
-  for (int64_t c = 0; c < m->nc; ++c)
-    for (int k = 0; k < topo(m->type[c]).nv; ++k) {
-      const int64_t g = m->gnode[c * 8 + k];
-      if (!seen[g]) {
-        seen[g] = 1;
-        pos[g] = vtx(*m, c, k);
-      }
-    }
   for (int64_t g = 0; g < nn; ++g)
     if (seen[g]) std::fprintf(fv, "%lld %.17g %.17g %.17g\n", (long long)(g + 1), pos[g].x, pos[g].y, pos[g].z);
+  for (size_t i = 0; i < ipos.size(); ++i)
+    std::fprintf(fv, "%lld %.17g %.17g %.17g\n", (long long)(nn + i + 1), ipos[i].x, ipos[i].y, ipos[i].z);
   for (int64_t c = 0; c < m->nc; ++c) {
-    const int64_t* gn = &m->gnode[c * 8];
+    const int64_t* gn = &cid[c * 8];
     long long s[8];
     switch (m->type[c]) {
       case 1: for (int k = 0; k < 8; ++k) s[k] = gn[k]; break;
@@ -1372,12 +1532,13 @@ int32_t ucp_write_grid(const ucp_mesh* m, const char* prefix) {
   long long ib = 0;
   for (int64_t c = 0; c < m->nc; ++c)
     for (int f = 0; f < m->nfaces[c]; ++f) {
-      if (m->neigh[c * 6 + f] >= 0) continue;
+      const bool per_face = across(c, f);
+      if (m->neigh[c * 6 + f] >= 0 && !per_face) continue;
       const int nv = m->face_type[c * 6 + f] == 5 ? 4 : 3;
       long long g[4];
-      for (int k = 0; k < nv; ++k) g[k] = m->gnode[c * 8 + m->fnode[c * 24 + f * 4 + k]] + 1;
+      for (int k = 0; k < nv; ++k) g[k] = cid[c * 8 + m->fnode[c * 24 + f * 4 + k]] + 1;
       if (nv == 3) g[3] = g[2];
-      std::fprintf(fb, "%lld %lld %lld %lld %lld %d\n", ++ib, g[0], g[1], g[2], g[3], m->bc[c * 6 + f]);
+      std::fprintf(fb, "%lld %lld %lld %lld %lld %d\n", ++ib, g[0], g[1], g[2], g[3], per_face ? 5 : m->bc[c * 6 + f]);
     }
   const bool bad = std::ferror(fv) || std::ferror(fc) || std::ferror(fb);
   std::fclose(fv);
