@@ -463,6 +463,19 @@ int ucg_residual_muscl_static(const ucg_config* cfg, const ucg_geometry* geo, co
  *   dJ = <dJ/dU0, dU0> + <dJ/dp, dp> by forward mode; state as above.    */
 int ucg_force(ucg_engine* e, double* fx);
 int ucg_force_vjp(ucg_engine* e, double* dJdU);
+/* ucg_wall_loads: COMPUTEFORCE (src/io.f90:18752-19000) in full at the
+ *   current state, any scheme and precision form (not MOOD):
+ *   out[6] = FX, FY, FZ, MX, MY, MZ.  Per wall face (BC code 4),
+ *   SSP = sum_q w_q p_q - pres adds SSP * area * n, and with Navier-Stokes
+ *   the shear SS = -sum_q mu_q (n . tau_q) w_q adds SS * area, tau from the
+ *   cell's own face-point velocity gradients (ULEFTV) and mu from SUTHERLAND
+ *   at the face state.  The moments are those of the pressure part about
+ *   the cell centres, as the reference takes them: `centre` [n][3] (host,
+ *   the caller's cell order), or NULL for zero moments.  Lift and drag
+ *   coefficients follow on the host from FX, FY, FZ, the angle of attack
+ *   and the free stream.  With partition roles only the faces of the stepped
+ *   cells count (the ranks' sums add up to the whole mesh's).             */
+int ucg_wall_loads(ucg_engine* e, const double* centre, double* out);
 int ucg_residual_vjp(ucg_engine* e, const double* lambda, double* mu, double* pbar);
 int ucg_residual_jvp(ucg_engine* e, const double* du, const double* dp, double* drhs);
 int ucg_adjoint_run(ucg_engine* e, int32_t nsteps, double dt, int32_t every, double* J, double* dJdU0,

@@ -61,6 +61,8 @@ def lib():
         L.orc_reduce.argtypes = [geop, f64p, C.c_int, f64p]
         L.orc_force.restype = C.c_int
         L.orc_force.argtypes = [cfgp, geop, recp, f64p, f64p]
+        L.orc_wall_loads.restype = C.c_int
+        L.orc_wall_loads.argtypes = [cfgp, geop, recp, f64p, f64p, f64p]
         L.orc_enstrophy.restype = C.c_int
         L.orc_enstrophy.argtypes = [cfgp, geop, recp, f64p, f64p]
         _lib = L
@@ -206,6 +208,19 @@ class Oracle:
         if rc:
             raise RuntimeError(f"orc_force failed: {rc}")
         return out.value
+
+    def wall_loads(self, U: np.ndarray, centre=None) -> np.ndarray:
+        """COMPUTEFORCE: FX, FY, FZ (pressure and, Navier-Stokes, shear) and
+        the pressure moments MX, MY, MZ about the cell centres (zero without
+        `centre` [n][3])."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        out = np.zeros(6)
+        cen = None if centre is None else np.ascontiguousarray(centre, dtype=np.float64)
+        rc = lib().orc_wall_loads(C.byref(self.cfg), C.byref(self.geo), C.byref(self.rec), _p(U),
+                                  None if cen is None else _p(cen), _p(out))
+        if rc:
+            raise RuntimeError(f"orc_wall_loads failed: {rc}")
+        return out
 
     def enstrophy(self, U: np.ndarray) -> float:
         """TOTENS of a periodic TGV run (ENSTROPHY_CALC), Navier-Stokes MUSCL."""

@@ -1627,6 +1627,68 @@ int orc_force(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, 
   return UCG_OK;
 }
 
+// COMPUTEFORCE (io.f90:18752-19000) in full: out = FX, FY, FZ, MX, MY, MZ.
+// Per wall face (code 4): SSP = sum_q w_q p_q - PRES and, Navier-Stokes,
+// SS = -sum_q mu_q (n . tau_q) w_q with tau from the cell's own face-point
+// velocity gradients (ULEFTV rows u, v, w) and mu from SUTHERLAND at the
+// face state; F += SSP * S * n + SS * S; the moments take the pressure
+// part about the cell centre (IELEM%XXC, YYC, ZZC), centre NULL = none.
+int orc_wall_loads(const ucg_config* cfg, const ucg_geometry* g, const ucg_recon* r, const double* U,
+                   const double* centre, double* out) {
+  if (!check_ctx(cfg, g, r) || !U || !out) return UCG_EINVAL;
+  const int64_t n = g->ncells;
+  const bool ns = cfg->governing == 1;
+  Ctx x{cfg, g, r, n, monos(cfg->iorder)};
+  std::vector<double> ul((size_t)n * F * Q * NV, 0.0), ulv(ns ? (size_t)n * F * Q * 12 : 1, 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < n; ++c)
+    reconstruct_cell(x, c, U, &ul[(size_t)c * F * Q * NV], ns ? &ulv[(size_t)c * F * Q * 12] : nullptr);
+  double fx = 0.0, fy = 0.0, fz = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+  for (int64_t c = 0; c < n; ++c)
+    for (int f = 0; f < g->nfaces[c]; ++f) {
+      if (g->neigh[c * F + f] >= 0 || g->bc[c * F + f] != 4) continue;
+      const bool quad = g->face_type[c * F + f] == 5;
+      const int nq = quad ? cfg->nq_quad : cfg->nq_tri;
+      const double* w = quad ? cfg->quad_w : cfg->tri_w;
+      const double a1 = g->face_angle[(c * F + f) * 2], a2 = g->face_angle[(c * F + f) * 2 + 1];
+      const double nx = std::cos(a1) * std::sin(a2), ny = std::sin(a1) * std::sin(a2), nz = std::cos(a2);
+      const double S = g->face_area[c * F + f];
+      double ssp = 0.0, ssx = 0.0, ssy = 0.0, ssz = 0.0;
+      for (int q = 0; q < nq; ++q) {
+        const size_t k = (((size_t)c * F + f) * Q + q);
+        double pm[NV];
+        cons2prim(x, &ul[k * NV], pm);
+        ssp = ssp + (pm[4] * w[q]);
+        if (ns) {
+          const double* gv = &ulv[k * 12];  // rows T, u, v, w; columns x, y, z
+          const double ux = gv[3], uy = gv[4], uz = gv[5], vx = gv[6], vy = gv[7], vz = gv[8];
+          const double wx = gv[9], wy = gv[10], wz = gv[11];
+          double mu, lam;
+          sutherland(cfg, pm[0], pm[4], &mu, &lam);
+          const double txx = (4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz;
+          const double tyy = (4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz;
+          const double tzz = (4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy;
+          const double tyx = uy + vx, tzx = wx + uz, tzy = vz + wy;
+          ssx = ssx - ((mu * ((nx * txx) + (ny * tyx) + (nz * tzx))) * w[q]);
+          ssy = ssy - ((mu * ((nx * tyx) + (ny * tyy) + (nz * tzy))) * w[q]);
+          ssz = ssz - ((mu * ((nx * tzx) + (ny * tzy) + (nz * tzz))) * w[q]);
+        }
+      }
+      ssp = ssp - cfg->pres;
+      fx = fx + ((ssp * S * nx)) + (ssx * S);
+      fy = fy + ((ssp * S * ny)) + (ssy * S);
+      fz = fz + ((ssp * S * nz)) + (ssz * S);
+      if (centre) {
+        const double xc = centre[c * 3], yc = centre[c * 3 + 1], zc = centre[c * 3 + 2];
+        mx = mx + ((ssp * S * nz)) * yc - ((ssp * S * ny)) * zc;
+        my = my + ((ssp * S * nx)) * zc - ((ssp * S * nz)) * xc;
+        mz = mz + ((ssp * S * ny)) * xc - ((ssp * S * nx)) * yc;
+      }
+    }
+  out[0] = fx, out[1] = fy, out[2] = fz, out[3] = mx, out[4] = my, out[5] = mz;
+  return UCG_OK;
+}
+
 // HLLC flux of two conserved states in the face frame (known-answer tests).
 int orc_hllc(double gamma, const double* cl, const double* cr, double* flux) {
   hllc(gamma, cl, cr, flux);

@@ -156,7 +156,7 @@ ENGINE_SYMBOLS = [
     "ucg_tangent_run", "ucg_time_adjoint", "ucg_cell_order", "ucg_adjoint_run_obj", "ucg_tangent_run_obj",
     "ucg_set_wait_limit", "ucg_mood_state", "ucg_build_recon", "ucg_implicit_step",
     "ucg_dual_time_step", "ucg_rk3_stage", "ucg_halo_set", "ucg_halo_pack", "ucg_halo_unpack",
-    "ucg_set_cell_roles", "ucg_dual_time_step_explicit",
+    "ucg_set_cell_roles", "ucg_dual_time_step_explicit", "ucg_wall_loads",
 ]
 
 
@@ -210,6 +210,8 @@ def engine() -> C.CDLL:
         lib.ucg_force.argtypes = [vp, _f64p]
         lib.ucg_force_vjp.restype = C.c_int
         lib.ucg_force_vjp.argtypes = [vp, _f64p]
+        lib.ucg_wall_loads.restype = C.c_int
+        lib.ucg_wall_loads.argtypes = [vp, _f64p, _f64p]
         lib.ucg_residual_vjp.restype = C.c_int
         lib.ucg_residual_vjp.argtypes = [vp, _f64p, _f64p, _f64p]
         lib.ucg_residual_jvp.restype = C.c_int

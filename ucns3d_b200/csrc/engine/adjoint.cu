@@ -1345,6 +1345,69 @@ int jvp_device(ucg_engine* e, const Problem& p, const double* U, const double* d
 }
 
 // J at state U into *out (device); with dU the tangent dJ instead
+// COMPUTEFORCE (io.f90:18752-19000) in full, one thread per owned face:
+// on a wall face (code 4), SSP = sum_q w_q p_q - PRES and, Navier-Stokes,
+// SS = -sum_q mu_q (n . tau_q) w_q from the cell's own face-point velocity
+// gradients (ULEFTV: ulv for MUSCL; for WENO fgrad, which on a physical
+// boundary face holds the own side's gradient) and SUTHERLAND at the face
+// state; columns [6][nown]: SSP S n + SS S, and the pressure moments about
+// the cell centre (cen [n][3], or none).  Face values in T (FP32 in the
+// mixed form), everything after in FP64.
+template <typename T>
+__global__ void k_wall_loads(Problem p, const double* __restrict__ U, const double* __restrict__ cen,
+                             double* __restrict__ cols) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.nown) return;
+  const int32_t code = p.own[i];
+  const int64_t c = code >> 3;
+  const int f = code & 7;
+  double r[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (p.neigh[c * MF + f] < 0 && p.bc[c * MF + f] == 4) {
+    const int QS = p.nq_quad > p.nq_tri ? p.nq_quad : p.nq_tri;
+    const int ft = p.ftype[c * MF + f], nq = face_nq(p, ft);
+    const double* rt = p.rot + (c * MF + f) * 4;
+    const double nx = rt[0] * rt[3], ny = rt[1] * rt[3], nz = rt[2];
+    const double S = p.area[c * MF + f];
+    const T* dul = (const T*)p.dul;
+    double ssp = 0.0, ssx = 0.0, ssy = 0.0, ssz = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      const int64_t s = (c * MF + f) * QS + q;
+      double u[NV], pr[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) u[v] = U[c * NV + v] + (double)dul[s * NV + v];
+      cons2prim(p.gamma, u, pr);
+      const double w = face_weight(p, ft, q);
+      ssp = ssp + (pr[4] * w);
+      if (p.governing == 1) {
+        const double* g = p.fgrad ? p.fgrad + (i * QS + q) * 12 : p.ulv + s * 12;  // rows T, u, v, w
+        const double ux = g[3], uy = g[4], uz = g[5], vx = g[6], vy = g[7], vz = g[8];
+        const double wx = g[9], wy = g[10], wz = g[11];
+        double mu, lam;
+        sutherland(p, pr[0], pr[4], &mu, &lam);
+        const double txx = (4.0 / 3.0) * ux - (2.0 / 3.0) * vy - (2.0 / 3.0) * wz;
+        const double tyy = (4.0 / 3.0) * vy - (2.0 / 3.0) * ux - (2.0 / 3.0) * wz;
+        const double tzz = (4.0 / 3.0) * wz - (2.0 / 3.0) * ux - (2.0 / 3.0) * vy;
+        const double tyx = uy + vx, tzx = wx + uz, tzy = vz + wy;
+        ssx = ssx - ((mu * ((nx * txx) + (ny * tyx) + (nz * tzx))) * w);
+        ssy = ssy - ((mu * ((nx * tyx) + (ny * tyy) + (nz * tzy))) * w);
+        ssz = ssz - ((mu * ((nx * tzx) + (ny * tzy) + (nz * tzz))) * w);
+      }
+    }
+    ssp = ssp - p.pres;
+    r[0] = (ssp * S * nx) + (ssx * S);
+    r[1] = (ssp * S * ny) + (ssy * S);
+    r[2] = (ssp * S * nz) + (ssz * S);
+    if (cen) {
+      const double xc = cen[c * 3], yc = cen[c * 3 + 1], zc = cen[c * 3 + 2];
+      r[3] = (ssp * S * nz) * yc - (ssp * S * ny) * zc;
+      r[4] = (ssp * S * nx) * zc - (ssp * S * nz) * xc;
+      r[5] = (ssp * S * ny) * xc - (ssp * S * nx) * yc;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) cols[k * p.nown + i] = r[k];
+}
+
 int force_device(ucg_engine* e, const Problem& p, const double* U, const double* dU, double* out) {
   int rc = launch_recon(e, p, U);
   if (rc) return rc;
@@ -1668,6 +1731,43 @@ int ucg_force_vjp(ucg_engine* e, double* dJdU) {
   double* g = weno ? (double*)e->adjw_mu.p : (double*)e->adj_mu.p;
   if ((rc = force_vjp_device(e, p, (const double*)e->Un.p, g))) return rc;
   if ((rc = copy_out(e, dJdU, g, (size_t)e->n * NV))) return rc;
+  CK(cudaStreamSynchronize(e->stream));
+  return UCG_OK;
+}
+
+int ucg_wall_loads(ucg_engine* e, const double* centre, double* out) {
+  if (!e || !out) return fail(e, UCG_EINVAL, "null argument");
+  if (!ready(e) || !e->have_state) return fail(e, UCG_ESTATE, "geometry, tables and state are needed");
+  if (e->cfg.mood) return fail(e, UCG_EINVAL, "the wall loads take the plain reconstruction (no MOOD)");
+  const int64_t n = e->n, nown = e->nown;
+  cudaSetDevice(e->device);
+  int rc = alloc(e, e->wl_buf, ((size_t)6 * std::max<int64_t>(nown, 1) + 8 + (size_t)3 * n) * 8);
+  if (rc) return rc;
+  double* cols = (double*)e->wl_buf.p;
+  double* sums = cols + 6 * std::max<int64_t>(nown, 1);
+  double* cen = sums + 8;
+  if (centre) {  // into the engine's cell order
+    if (e->n2o.empty()) {
+      CK(cudaMemcpyAsync(cen, centre, (size_t)n * 3 * 8, cudaMemcpyHostToDevice, e->stream));
+    } else {
+      std::vector<double> h((size_t)n * 3);
+      for (int64_t c = 0; c < n; ++c)
+        for (int k = 0; k < 3; ++k) h[c * 3 + k] = centre[(size_t)e->n2o[c] * 3 + k];
+      CK(cudaMemcpyAsync(cen, h.data(), h.size() * 8, cudaMemcpyHostToDevice, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+    }
+  }
+  Problem p = make_problem(e);
+  if ((rc = launch_recon(e, p, (const double*)e->Un.p))) return rc;
+  const unsigned nb = blocks_for(std::max<int64_t>(nown, 1), 128);
+  if (e->cfg.precision == UCG_FP64)
+    k_wall_loads<double><<<nb, 128, 0, e->stream>>>(p, (const double*)e->Un.p, centre ? cen : nullptr, cols);
+  else
+    k_wall_loads<float><<<nb, 128, 0, e->stream>>>(p, (const double*)e->Un.p, centre ? cen : nullptr, cols);
+  for (int k = 0; k < 6; ++k) k_sum1<<<1, 1024, 0, e->stream>>>(cols + k * nown, nown, sums + k);
+  e->launches += 7;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, sums, 6 * 8, cudaMemcpyDeviceToHost, e->stream));
   CK(cudaStreamSynchronize(e->stream));
   return UCG_OK;
 }

@@ -615,7 +615,7 @@ void ucg_destroy(ucg_engine* e) {
                    &e->health, &e->dt, &e->partial, &e->red, &e->staging, &e->own, &e->fflux, &e->vflux, &e->gbuf,
                    &e->qbuf, &e->d_n2o, &e->permbuf, &e->fgrad, &e->isb, &e->wflag, &e->mprev, &e->mflag,
                    &e->msel, &e->mmus, &e->mord, &e->Um, &e->imp_dtl, &e->imp_dinv, &e->imp_off, &e->imp_du,
-                   &e->dual_hist, &e->dual_part, &e->halo_send, &e->halo_recv};
+                   &e->dual_hist, &e->dual_part, &e->halo_send, &e->halo_recv, &e->wl_buf};
   for (DevBuf* b : all) release(*b);
   adjoint_release(e);
   if (e->stream) cudaStreamDestroy(e->stream);

@@ -83,6 +83,7 @@ struct ucg_engine {
   int64_t n_recon = 0, n_update = 0;
   // halo lists of a partition (ucg_halo_set), in the engine's order
   DevBuf halo_send, halo_recv;
+  DevBuf wl_buf;  // ucg_wall_loads: [6][nown] face columns, sums, cell centres
   int64_t halo_nsend = 0, halo_nrecv = 0;
   double cost_caller = 0.0, cost_rcm = 0.0;  // gather cost of both orders (reorder 1)
   // discrete adjoint / tangent (adjoint.cu)

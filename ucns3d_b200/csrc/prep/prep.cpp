@@ -39,6 +39,14 @@ namespace {
 
 thread_local std::string g_err;
 void set_err(const std::string& s) { g_err = s; }
+// a message set by an OpenMP worker (inside a critical section) goes to the
+// calling thread's error when the parallel loop's result comes back
+std::string g_err_par;
+void set_err_par(const std::string& s) { g_err_par = s; }
+bool par_result(bool ok) {
+  if (!ok) set_err(g_err_par);
+  return ok;
+}
 
 struct V3 {
   double x, y, z;
@@ -557,14 +565,14 @@ bool build_geometry(ucp_mesh& m) {
 #pragma omp critical
           {
             ok = false;
-            set_err("face quadrature points of neighbouring cells do not coincide");
+            set_err_par("face quadrature points of neighbouring cells do not coincide");
           }
         }
         m.qperm[(c * 6 + f) * Q + q] = best;
       }
     }
   }
-  return ok;
+  return par_result(ok);
 }
 
 // ------------------------------------------------------------- stencils
@@ -665,7 +673,7 @@ bool build_stencils(ucp_mesh& m) {
 #pragma omp critical
         {
           ok = false;
-          set_err("mesh too small for the central stencil");
+          set_err_par("mesh too small for the central stencil");
         }
       }
       // directional stencils (STENCIILSX): candidates inside the cone of each face
@@ -696,7 +704,7 @@ bool build_stencils(ucp_mesh& m) {
       m.full[c] = (s.scheme == 3 && nadm >= m.nfaces[c] + 1) ? 1 : 0;
     }
   }
-  return ok;
+  return par_result(ok);
 }
 
 // ------------------------------------------------------------- tables
@@ -905,7 +913,7 @@ bool build_tables(ucp_mesh& m) {
 #pragma omp critical
           {
             ok = false;
-            set_err("singular least-squares normal matrix");
+            set_err_par("singular least-squares normal matrix");
           }
           continue;
         }
@@ -921,7 +929,7 @@ bool build_tables(ucp_mesh& m) {
       if (s.ees == 5) indicator_matrix(m, c, F, s.iorder2, Ri, &m.indicator2[t * s.ideg2 * s.ideg2]);
     }
   }
-  return ok;
+  return par_result(ok);
 }
 
 // ---------------------------------------------------------- IC helpers

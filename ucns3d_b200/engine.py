@@ -159,6 +159,16 @@ class Engine:
         """TOTENS of a periodic TGV run (ENSTROPHY_CALC); Navier-Stokes MUSCL."""
         return self.reduce(N.UCG_REDUCE_ENSTROPHY)
 
+    def wall_loads(self, centre=None) -> np.ndarray:
+        """COMPUTEFORCE in full (src/io.f90:18752-19000): FX, FY, FZ (pressure
+        and, Navier-Stokes, viscous shear) and the pressure moments MX, MY,
+        MZ about the cell centres `centre` (n, 3) (zero when None)."""
+        out = np.zeros(6)
+        cen = None if centre is None else np.ascontiguousarray(centre, dtype=np.float64)
+        self._check(self.lib.ucg_wall_loads(self._h, None if cen is None else N.ptr(cen, C.c_double),
+                                            N.ptr(out, C.c_double)))
+        return out
+
     # ------------------------------------------- adjoint and tangent (FP64 MUSCL, Euler)
     def force(self) -> float:
         """Wall pressure force in x at the current state (COMPUTEFORCE, src/io.f90:18752)."""
@@ -282,3 +292,15 @@ class Engine:
     @property
     def device_bytes(self) -> int:
         return int(self.lib.ucg_device_bytes(self._h))
+
+
+def lift_drag(loads, aoa_deg: float, rres: float, ufreestream: float, vector=(1.0, 1.0, 1.0)):
+    """CL and CD from the wall loads as COMPUTEFORCE forms them in the body
+    frame (RFRAME 0, src/io.f90:18933-18941): the forces scaled by VECTORX,
+    Y, Z, then lift = FZ cos a + FY cos a - FX sin a, drag = FX cos a +
+    FY sin a + FZ sin a, and C = 2 force / (RRES u_inf^2)."""
+    fx, fy, fz = (float(loads[k]) * float(vector[k]) for k in range(3))
+    a = (aoa_deg / 180.0) * np.pi
+    lift = (fz * np.cos(a)) + (fy * np.cos(a)) - (fx * np.sin(a))
+    drag = (fx * np.cos(a)) + (fy * np.sin(a)) + (fz * np.sin(a))
+    return (2.0 * lift) / (rres * ufreestream ** 2), (2.0 * drag) / (rres * ufreestream ** 2)
