@@ -312,6 +312,7 @@ class HaloEngine:
         self.recvbuf = torch.empty((len(self.lists.recv), 5), dtype=torch.float64, device=dev)
         self.stream = torch.cuda.ExternalStream(self.engine.stream_ptr, device=dev)
         self.comm = comm
+        self.restrict = restrict
 
     def close(self):
         self.engine.close()
@@ -369,6 +370,24 @@ class HaloEngine:
         return float(t.item())
 
 
+    def wall_loads(self, centre=None) -> np.ndarray:
+        """COMPUTEFORCE of the whole mesh: the halo of U^n brought up to date,
+        this rank's walls (those of its owned cells: the engine has the
+        roles), then the sum over the ranks.  `centre` is the whole mesh's
+        cell centres (n, 3) for the moments, or None."""
+        import torch
+        import torch.distributed as dist
+        if not self.restrict:
+            raise ValueError("the wall loads of a rank need the cell roles (restrict=True)")
+        self.exchange(1)
+        loads = self.engine.wall_loads(None if centre is None else self.plan.local(self.rank, centre))
+        if not dist.is_initialized():
+            return loads
+        t = torch.tensor(loads, dtype=torch.float64, device=self.sendbuf.device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.comm)
+        return t.cpu().numpy()
+
+
 class LocalCluster:
     """All ranks of a plan as engines in this process on one device: each
     stage packs every rank, copies the rows between the ranks' buffers, then
@@ -413,3 +432,12 @@ class LocalCluster:
     def compute_dt(self, cfl: float) -> float:
         self.exchange(1)
         return min(h.engine.calculate_cfl(cfl) for h in self.ranks)
+
+    def wall_loads(self, centre=None) -> np.ndarray:
+        """The ranks' wall loads added in rank order (the engines need the
+        roles: restrict=True)."""
+        if not all(h.restrict for h in self.ranks):
+            raise ValueError("the wall loads of a rank need the cell roles (restrict=True)")
+        self.exchange(1)
+        return sum(h.engine.wall_loads(None if centre is None else self.plan.local(h.rank, centre))
+                   for h in self.ranks)
